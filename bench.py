@@ -1,0 +1,365 @@
+#!/usr/bin/env python
+"""Coulomb pair-evaluation throughput of the B200 hot path.
+
+One step = the potentials at the current and proposed sites of every carrier
+(the kernel-2 packing of OpenClHelper::launchCoulombKernel2,
+openclhelper.cpp:372-457) from all carriers, with the workload's image terms.
+Default workload: 256x256x16 lattice, 2% occupancy split 50/50 electrons and
+holes (20,970 charges, 41,940 targets), cutoff 50, image charges at both x
+electrodes -- seeded synthetic placement.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+N > 1 (under torchrun): independent replicas, one per GPU (the path does not
+shard); value = pairs of all ranks / max over ranks of the timed span.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOADS = {
+    # name: lattice, cutoff, occupancy, image terms, sigma
+    "cfg2_3d_eh_images": dict(X=256, Y=256, Z=16, cutoff=50, e=0.01, h=0.01, terms=7, sigma=0.0,
+                              desc="256x256x16, 2% e/h 50/50, cutoff 50, images at both x "
+                                   "electrodes"),
+    "cfg1_2d_holes": dict(X=128, Y=128, Z=1, cutoff=50, e=0.0, h=0.01, terms=1, sigma=0.0,
+                          desc="128x128x1, 1% holes, cutoff 50, no images"),
+    "cfg3_gauss": dict(X=128, Y=128, Z=64, cutoff=30, e=0.01, h=0.01, terms=1, sigma=1.0,
+                       desc="128x128x64, 1%+1% e/h, Gaussian sigma 1, cutoff 30"),
+}
+DEFAULT_WORKLOAD = "cfg2_3d_eh_images"
+
+# FLOP per pair evaluation counted for the roofline: dx,dy,dz (3), r^2 (3 mul
+# + 2 add), 1/sqrt (1), q*w + acc (2).
+FLOP_PER_PAIR = 11
+# DRAM bytes per launch of the pair kernel from one ncu capture of this
+# workload (profiles/pair_kernel_cfg2.md); None until captured.
+PAIR_KERNEL_DRAM_BYTES = None
+
+
+def make_inputs(w, seed):
+    """Seeded uniform placement and one nearest-neighbour proposal per carrier."""
+    rng = np.random.default_rng(seed)
+    X, Y, Z = w["X"], w["Y"], w["Z"]
+    vol = X * Y * Z
+    ne, nh = int(w["e"] * vol), int(w["h"] * vol)
+    sites = rng.choice(vol, ne + nh, replace=False).astype(np.int64)
+    q = np.concatenate([-np.ones(ne), np.ones(nh)]).astype(np.int32)
+    x, y, z = sites % X, (sites // X) % Y, sites // (X * Y)
+    coords = np.stack([x, y, z], 1)
+    dims = np.array([X, Y, Z])
+    axis = rng.integers(0, 3 if Z > 1 else 2, len(sites))
+    step = rng.choice([-1, 1], len(sites))
+    fut = coords.copy()
+    fut[np.arange(len(sites)), axis] += step
+    off = (fut < 0) | (fut >= dims)
+    fut[off] = coords[off] - (fut[off] - coords[off])  # reflect at the faces
+    fsites = fut[:, 0] + X * (fut[:, 1] + Y * fut[:, 2])
+    s_all = np.concatenate([sites, fsites]).astype(np.int32)
+    q_all = np.concatenate([q, q]).astype(np.int32)
+    return s_all, q_all, ne + nh
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return json.load(f)
+    return {}
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        rows = []
+        if self.path and os.path.exists(self.path):
+            for line in open(self.path):
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+            os.remove(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i] == "Active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(rows)}
+
+
+def cpu_baseline_run(w, s_all, q_all, n, seconds, threads):
+    """The oracle (C++ FP64 restatement of the reference's CPU Coulomb path) on a
+    bounded sample of targets: pairs/s, threads used, sample description."""
+    from oracle import oracle as O
+    orc = O.Oracle(w["X"], w["Y"], w["Z"], cutoff=w["cutoff"], sigma=w["sigma"])
+    src, q = s_all[:n], q_all[:n]
+    nterms = bin(w["terms"]).count("1")
+    probe = s_all[: min(64, len(s_all))]
+    t0 = time.perf_counter()
+    orc.potentials(src, q, probe, gauss=w["sigma"] > 0, terms=w["terms"], threads=threads)
+    rate = len(probe) * n * nterms / max(time.perf_counter() - t0, 1e-6)
+    k = int(np.clip(rate * seconds / (n * nterms), 64, len(s_all)))
+    tgt = s_all[:k]
+    t0 = time.perf_counter()
+    orc.potentials(src, q, tgt, gauss=w["sigma"] > 0, terms=w["terms"], threads=threads)
+    dt = time.perf_counter() - t0
+    pairs = k * n * nterms
+    return pairs / dt, dt, f"{k} of {len(s_all)} targets x {n} sources x {nterms} terms"
+
+
+def reference_arm(args, w, rank):
+    """--impl reference: the CPU path on the host cores, rank 0 only."""
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    s_all, q_all, n = make_inputs(w, seed=2)
+    from oracle import oracle as O
+    orc = O.Oracle(w["X"], w["Y"], w["Z"], cutoff=w["cutoff"], sigma=w["sigma"])
+    nterms = bin(w["terms"]).count("1")
+    # each step: a bounded slice of the targets (about 2 s of CPU work)
+    probe = s_all[:64]
+    t0 = time.perf_counter()
+    orc.potentials(s_all[:n], q_all[:n], probe, w["sigma"] > 0, w["terms"], threads)
+    rate = 64 * n * nterms / max(time.perf_counter() - t0, 1e-6)
+    k = int(np.clip(rate * 2.0 / (n * nterms), 64, len(s_all)))
+    times = []
+    for i in range(args.warmup + args.steps):
+        lo = (i * k) % max(1, len(s_all) - k)
+        tgt = s_all[lo:lo + k]
+        t0 = time.perf_counter()
+        orc.potentials(s_all[:n], q_all[:n], tgt, w["sigma"] > 0, w["terms"], threads)
+        if i >= args.warmup:
+            times.append(time.perf_counter() - t0)
+    pairs = k * n * nterms
+    value = pairs * len(times) / sum(times)
+    sample = (f"{k} of {len(s_all)} targets per step x {n} sources x {nterms} terms "
+              "(C++ FP64 restatement of Potential::coulomb*/coulombImage*, table gathers)")
+    line = {
+        "impl": "reference", "metric": "Coulomb pair-evals/s", "value": value,
+        "unit": "pair-evals/s", "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * sum(times) / len(times),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "config": {"workload": args.workload, "desc": w["desc"]},
+        "cpu_baseline": {"value": value, "unit": "pair-evals/s", "cores": threads,
+                         "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": "pair-evals/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=list(WORKLOADS))
+    ap.add_argument("--path", type=int, default=0, help="0 MUFU rsqrt, 1 1/sqrt(k) table")
+    ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        ap.error("--warmup must be >= 3")
+    w = WORKLOADS[args.workload]
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        reference_arm(args, w, rank)
+        return
+
+    import torch
+    import langmuir_b200 as L
+
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local_rank))
+
+    s_all, q_all, n = make_inputs(w, seed=2 + rank)
+    T = len(s_all)
+    nterms = bin(w["terms"]).count("1")
+    pairs_per_step = nterms * T * n
+
+    ctx = L.Coulomb(w["X"], w["Y"], w["Z"], cutoff=w["cutoff"], sigma=w["sigma"],
+                    device=local_rank, path=args.path)
+    kind = L.GAUSS if w["sigma"] > 0 else L.POINT
+    dev = torch.device("cuda", local_rank)
+    d_s = torch.from_numpy(s_all).to(dev)
+    d_q = torch.from_numpy(q_all).to(dev)
+    d_out = torch.empty(T, dtype=torch.float64, device=dev)
+    stream = torch.cuda.Stream(dev)  # a real stream: handle 0 would mean the context's own
+    torch.cuda.set_stream(stream)
+    sp = stream.cuda_stream
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)  # > L2
+
+    def step():
+        ctx.potentials_async(d_s.data_ptr(), d_q.data_ptr(), n, d_s.data_ptr(), T,
+                             d_out.data_ptr(), kind, w["terms"], sp)
+
+    ctx.set_timing(True)
+    for _ in range(args.warmup):
+        step()
+    ctx.sync(sp)
+    torch.cuda.synchronize(dev)
+    if dist:
+        dist.barrier()
+
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(args.steps)]
+    pair_ms = []
+    launches = 0
+    with ClockSampler(local_rank) as clk:
+        torch.cuda.synchronize(dev)
+        for i in range(args.steps):
+            flush.zero_()  # L2 flush between timed steps (outside the events)
+            ev[i][0].record(stream)
+            step()
+            ev[i][1].record(stream)
+            info = ctx.last_launch()
+            pair_ms.append(info["pair_kernel_ms"])
+            launches += info["kernel_launches"]
+        torch.cuda.synchronize(dev)
+    ctx.sync(sp)
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    span_ms = float(sum(step_ms))
+    if dist:
+        t = torch.tensor([span_ms], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        span_ms = float(t.item())
+        dist.barrier()
+    clocks = clk.summary()
+    ms_per_step = span_ms / args.steps
+    value = pairs_per_step * world / (ms_per_step * 1e-3)
+
+    # accuracy on a sample of targets against the FP64 oracle (the checker)
+    o = d_out.cpu().numpy()
+    acc = None
+    if rank == 0:
+        from oracle import oracle as O
+        orc = O.Oracle(w["X"], w["Y"], w["Z"], cutoff=w["cutoff"], sigma=w["sigma"])
+        idx = np.linspace(0, T - 1, 512).astype(int)
+        want = orc.potentials(s_all[:n], q_all[:n], s_all[idx], w["sigma"] > 0, w["terms"])
+        nrm = orc.potentials(s_all[:n], np.abs(q_all[:n]), s_all[idx], w["sigma"] > 0, 1)
+        if w["terms"] & 2:
+            nrm -= orc.potentials(s_all[:n], np.abs(q_all[:n]), s_all[idx], w["sigma"] > 0, 2)
+        if w["terms"] & 4:
+            nrm -= orc.potentials(s_all[:n], np.abs(q_all[:n]), s_all[idx], w["sigma"] > 0, 4)
+        err = np.abs(o[idx] - want)
+        acc = {"targets_checked": len(idx), "max_err_over_norm": float((err / nrm).max()),
+               "max_rel_err": float((err / np.maximum(np.abs(want), 1e-3 * nrm)).max()),
+               "tolerance_over_norm": 1e-6}
+
+    # end to end through the host-buffer ABI: H2D inputs, kernels, D2H result
+    e2e = None
+    if rank == 0:
+        h_s = s_all.copy()
+        h_q = q_all.copy()
+        for _ in range(3):
+            ctx.potentials(h_s[:n], h_q[:n], h_s, kind, w["terms"])
+        t0 = time.perf_counter()
+        k_e2e = max(3, args.steps // 2)
+        for _ in range(k_e2e):
+            ctx.potentials(h_s[:n], h_q[:n], h_s, kind, w["terms"])
+        dt = (time.perf_counter() - t0) / k_e2e
+        e2e = {"value": pairs_per_step / dt, "unit": "pair-evals/s",
+               "h2d_bytes_per_step": int(4 * (2 * n + T)), "d2h_bytes_per_step": int(8 * T)}
+
+    peaks = measured_peaks()
+    props = torch.cuda.get_device_properties(dev)
+    sms = props.multi_processor_count
+    clk_max = float(peaks.get("sm_max_mhz", 1965.0))
+    fp32_peak = sms * 128 * 2 * clk_max * 1e6 / 1e12          # TFLOP/s, derived
+    sfu_peak = sms * 16 * clk_max * 1e6                        # rsqrt/s, derived
+    pk = float(np.median(pair_ms))
+    achieved = FLOP_PER_PAIR * pairs_per_step / (pk * 1e-3) / 1e12
+    roof = {
+        "bound": "fp32", "kernel": "pair_kernel", "achieved": achieved, "peak": fp32_peak,
+        "unit": "TFLOP/s", "frac": achieved / fp32_peak,
+        "peak_source": (f"derived: {sms} SMs x 128 FP32 lanes x 2 x {clk_max:.0f} MHz "
+                        "(sm_max_mhz of MEASURED_PEAKS.json); no measured FP32 figure exists"),
+        "sfu_frac": (pairs_per_step / (pk * 1e-3)) / sfu_peak,
+        "pair_kernel_ms": pk, "flop_per_pair": FLOP_PER_PAIR,
+        "traffic": PAIR_KERNEL_DRAM_BYTES,
+    }
+    if clocks.get("sm_mhz"):
+        roof["frac_at_sampled_clock"] = achieved / (sms * 256 * clocks["sm_mhz"] * 1e6 / 1e12)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        v, dt, sample = cpu_baseline_run(w, s_all, q_all, n, args.cpu_seconds, threads)
+        cpu = {"value": v, "unit": "pair-evals/s", "cores": threads, "kind": "port",
+               "sample": sample + f" ({dt:.1f} s)"}
+
+    if rank == 0:
+        line = {
+            "metric": "Coulomb pair-evals/s", "value": value, "unit": "pair-evals/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "fp32", "data": "synthetic",
+            "config": {"workload": args.workload, "desc": w["desc"], "sources": n,
+                       "targets": T, "terms": nterms, "pairs_per_step": pairs_per_step,
+                       "path": "table" if args.path else "rsqrt", "l2": "flushed between steps",
+                       "parallelism": "replicas" if world > 1 else "single"},
+            "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
+            "gpu_launches": launches, "accuracy": acc,
+        }
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,162 @@
+/*
+ * langmuir_b200.h -- C ABI of the B200 Coulomb hot path for Langmuir.
+ *
+ * Drop-in for the engine's OpenCL helper (class OpenClHelper,
+ * src/langmuirCore/include/openclhelper.h:22-241 in the reference): the same
+ * packed site/charge buffers, the same kernel-1 / kernel-2 results, status
+ * codes instead of qFatal, no exceptions across the boundary, caller-owned
+ * buffers.  Plain C types only; a CUDA stream travels as `void*`.
+ *
+ * Threading: one lgm_ctx is used by one host thread at a time.  Results
+ * written to caller buffers are plain memory once a synchronous call returns
+ * and may be read concurrently (as the reference's QtConcurrent workers read
+ * getOutputHost, simulation.cpp:77-80).
+ *
+ * Units: potentials in volts (prefactor * sum q_j w(r_ij)), as the reference.
+ */
+#ifndef LANGMUIR_B200_H
+#define LANGMUIR_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LGM_ABI_VERSION 1
+
+/* ---- status codes ------------------------------------------------------- */
+typedef int32_t lgm_status;
+#define LGM_OK                     0
+#define LGM_ERR_INVALID_ARGUMENT   1  /* null pointer, bad size or enum         */
+#define LGM_ERR_OUT_OF_RANGE       2  /* a site id outside the lattice          */
+#define LGM_ERR_CUDA               3  /* a CUDA runtime call failed              */
+#define LGM_ERR_NO_DEVICE          4  /* no usable sm_100 device                 */
+#define LGM_ERR_CAPACITY           5  /* more charges/targets than configured    */
+#define LGM_ERR_TIMEOUT            6  /* a bounded device wait ran out           */
+#define LGM_ERR_PARSE              7  /* input-file key/value error              */
+#define LGM_ERR_UNSUPPORTED        8  /* valid in the reference, not supported   */
+#define LGM_ERR_STATE              9  /* call out of order                       */
+
+/* ---- enums --------------------------------------------------------------- */
+/* Interaction kind: point charges (coulomb1/coulomb2, kernel.cl:56,222) or
+ * Gaussian-smeared charges (gauss1/gauss2, kernel.cl:139,296). */
+typedef enum lgm_kind { LGM_POINT = 0, LGM_GAUSS = 1 } lgm_kind;
+
+/* Pair-sum arithmetic.  FP32C: FP32 terms, FP32 runs of 8 positive terms
+ * folded into FP64 accumulators.  FP64: every term in FP64 (the guard-band and
+ * reference-precision path). */
+typedef enum lgm_precision { LGM_PREC_FP32C = 0, LGM_PREC_FP64 = 1 } lgm_precision;
+
+/* How 1/r is formed in FP32C: MUFU reciprocal square root, or a per-r^2
+ * shared-memory table of correctly rounded values (r^2 is an integer). */
+typedef enum lgm_path { LGM_PATH_RSQRT = 0, LGM_PATH_TABLE = 1 } lgm_path;
+
+/* Terms of lgm_potentials: direct sum, and the images of the sources in the
+ * x = -1/2 electrode (Potential::coulombImage*, potential.cpp:384-753) and,
+ * as an extension, in the x = X - 1/2 electrode.  Image terms enter with the
+ * opposite sign, as in the reference. */
+#define LGM_TERM_DIRECT       1u
+#define LGM_TERM_IMAGE_LEFT   2u
+#define LGM_TERM_IMAGE_RIGHT  4u
+
+/* ---- configuration -------------------------------------------------------- */
+/* The input keys of the reference that reach its OpenCL path
+ * (include/parameters.h:205-223, 241-244; openclhelper.cpp:125-168). */
+typedef struct lgm_config {
+    int32_t grid_x, grid_y, grid_z;     /* grid.x / grid.y / grid.z                    */
+    int32_t electrostatic_cutoff;       /* electrostatic.cutoff (sites, default 50)    */
+    double  electrostatic_prefactor;    /* electrostatic.prefactor (V, see below)      */
+    double  coulomb_gaussian_sigma;     /* coulomb.gaussian.sigma (sites)              */
+    int32_t work_x, work_y, work_z;     /* work.x/y/z  (accepted; tiles are autotuned) */
+    int32_t work_size;                  /* work.size   (accepted; tiles are autotuned) */
+    int32_t opencl_threshold;           /* opencl.threshold (used by the shim)         */
+    int32_t max_charges;                /* capacity: sources per call                  */
+    int32_t max_targets;                /* capacity: targets per call                  */
+    int32_t precision;                  /* lgm_precision                               */
+    int32_t path;                       /* lgm_path                                    */
+} lgm_config;
+
+/* Defaults of SimulationParameters (parameters.h:285-378) for these keys;
+ * electrostatic_prefactor = e / (4 pi eps_r eps_0 a) with eps_r = 3.5
+ * (setCalculatedValues, parameters.h:384-390). */
+void lgm_config_default(lgm_config* cfg);
+
+typedef struct lgm_ctx lgm_ctx;
+
+/* OpenClHelper::OpenClHelper + initializeOpenCL(gpuID) (openclhelper.cpp:12-187).
+ * device < 0 selects device 0.  Allocates the device buffers for the
+ * configured capacities. */
+lgm_status lgm_create(const lgm_config* cfg, int32_t device, lgm_ctx** out);
+lgm_status lgm_destroy(lgm_ctx* ctx);
+
+/* Text of the last error on this context (ctx == NULL: last error of a failed
+ * lgm_create on this thread).  Valid until the next call on the context. */
+const char* lgm_last_error(const lgm_ctx* ctx);
+const char* lgm_status_string(lgm_status status);
+int32_t lgm_abi_version(void);
+
+/* Potentials at t target sites from n source charges:
+ *   out[g] = prefactor * sum_j q_j w(r(tgt_site[g], src_site[j])), 0 < r^2 < cutoff^2,
+ *   w = 1/r (LGM_POINT) or erf(r / (sqrt(2) sigma)) / r (LGM_GAUSS),
+ * plus the image terms selected by `terms` (subtracted).  Sources must be
+ * lattice sites [0, volume); targets may also be the electrode ids
+ * [volume, volume + 35) that the reference packs for drains
+ * (openclhelper.cpp:411-424), whose values are defined but meaningless.
+ * Host buffers, synchronous. */
+lgm_status lgm_potentials(lgm_ctx* ctx, lgm_kind kind, uint32_t terms,
+                          const int32_t* src_site, const int32_t* src_q, int32_t n,
+                          const int32_t* tgt_site, int32_t t, double* out);
+
+/* The same on device buffers, ordered on `stream` (a cudaStream_t; NULL =
+ * the context's stream).  Returns once the work is enqueued; range errors
+ * found on the device are reported by lgm_sync. */
+lgm_status lgm_potentials_async(lgm_ctx* ctx, lgm_kind kind, uint32_t terms,
+                                const int32_t* d_src_site, const int32_t* d_src_q, int32_t n,
+                                const int32_t* d_tgt_site, int32_t t, double* d_out,
+                                void* stream);
+
+/* Wait for the context's work on `stream` and report device-side errors. */
+lgm_status lgm_sync(lgm_ctx* ctx, void* stream);
+
+/* OpenClHelper::launchCoulombKernel2 / launchGaussKernel2
+ * (openclhelper.cpp:372-544, kernel.cl:222-369): s[total], q[total] packed as
+ * the reference packs them (current sites of electrons, holes, charged
+ * defects = the n sources, then the future sites of electrons and holes);
+ * o[g] is the potential at s[g] from the n sources, for all g < total. */
+lgm_status lgm_coulomb_kernel2(lgm_ctx* ctx, lgm_kind kind, const int32_t* s,
+                               const int32_t* q, int32_t n, int32_t total, double* o);
+
+/* OpenClHelper::launchCoulombKernel1 / launchGaussKernel1
+ * (openclhelper.cpp:220-370, kernel.cl:56-220): potential at every lattice
+ * site k < volume from the n charges (s, q); o holds `volume` values (the
+ * reference reads back only n of them, openclhelper.cpp:261,284). */
+lgm_status lgm_coulomb_kernel1(lgm_ctx* ctx, lgm_kind kind, const int32_t* s,
+                               const int32_t* q, int32_t n, double* o);
+lgm_status lgm_coulomb_kernel1_async(lgm_ctx* ctx, lgm_kind kind, const int32_t* d_s,
+                                     const int32_t* d_q, int32_t n, double* d_o,
+                                     void* stream);
+
+/* Launch statistics of the last pair-sum launch on the context. */
+typedef struct lgm_launch_info {
+    int64_t pairs_tested;      /* (physical targets) x (sources), padding excluded */
+    int32_t ctas;              /* CTAs of the pair kernel                          */
+    int32_t splits;            /* source splits                                     */
+    int32_t threads;           /* threads per CTA                                   */
+    int32_t targets_per_thread;
+    int32_t kernel_launches;   /* kernels launched by the call                      */
+    float pair_kernel_ms;      /* device time of the pair kernel (timing on), else -1 */
+} lgm_launch_info;
+/* Waits for the last launch when timing is on. */
+lgm_status lgm_last_launch(lgm_ctx* ctx, lgm_launch_info* info);
+
+/* Timing on: CUDA events on the launch stream bracket the pair kernel of
+ * every call, read back by lgm_last_launch. */
+lgm_status lgm_set_timing(lgm_ctx* ctx, int32_t enable);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* LANGMUIR_B200_H */

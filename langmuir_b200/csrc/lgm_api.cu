@@ -1,0 +1,701 @@
+// lgm_api.cu -- C ABI of the Coulomb path: context, buffers, launches.
+//
+// Host side of the drop-in for OpenClHelper (src/langmuirCore/openclhelper.cpp):
+// validation with status codes instead of qFatal, device buffers that stay
+// resident, and the prep -> pair -> finalize launch sequence on one stream.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+
+#include "langmuir_b200.h"
+#include "lgm_context.hpp"
+#include "lgm_pairs.cuh"
+
+using namespace lgm;
+
+namespace {
+
+thread_local std::string g_create_error;
+
+constexpr int kPairThreads = 128;   // NT
+constexpr int kPairRP = 4;          // target pairs per thread
+constexpr int kTile = kPairThreads * 2 * kPairRP;  // targets per CTA
+constexpr int kMaxSplits = 64;
+constexpr int kDrainIds = 35;       // Grid::m_specialAgentReserve (cubicgrid.cpp:22)
+
+lgm_status fail(lgm_ctx* c, lgm_status st, const std::string& msg) {
+    if (c) c->err = msg;
+    return st;
+}
+
+lgm_status cuda_fail(lgm_ctx* c, cudaError_t e, const char* what) {
+    std::string m = std::string(what) + ": " + cudaGetErrorString(e);
+    return fail(c, LGM_ERR_CUDA, m);
+}
+
+#define LGM_CUDA(c, call)                                    \
+    do {                                                     \
+        cudaError_t e_ = (call);                             \
+        if (e_ != cudaSuccess) return cuda_fail((c), e_, #call); \
+    } while (0)
+
+template <class T>
+lgm_status grow_device(lgm_ctx* c, T** p, size_t* cap, size_t need) {
+    if (need <= *cap && *p) return LGM_OK;
+    size_t n = std::max(need, (size_t)(*cap * 3 / 2));
+    n = std::max<size_t>(n, 256);
+    if (*p) LGM_CUDA(c, cudaFree(*p));
+    *p = nullptr;
+    *cap = 0;
+    LGM_CUDA(c, cudaMalloc(reinterpret_cast<void**>(p), n * sizeof(T)));
+    *cap = n;
+    return LGM_OK;
+}
+
+template <class T>
+lgm_status grow_host(lgm_ctx* c, T** p, size_t* cap, size_t need) {
+    if (need <= *cap && *p) return LGM_OK;
+    size_t n = std::max(need, (size_t)(*cap * 3 / 2));
+    n = std::max<size_t>(n, 256);
+    if (*p) LGM_CUDA(c, cudaFreeHost(*p));
+    *p = nullptr;
+    *cap = 0;
+    LGM_CUDA(c, cudaMallocHost(reinterpret_cast<void**>(p), n * sizeof(T)));
+    *cap = n;
+    return LGM_OK;
+}
+
+// ---- prep kernels ---------------------------------------------------------
+
+// Source records (see lgm_pairs.cuh).  Entries n .. n_pad-1 are zero-charge
+// padding at the origin; their weight is (q*m) * y = 0 * finite = 0.
+__global__ void prep_sources(const int32_t* __restrict__ s, const int32_t* __restrict__ q, int n,
+                             int n_pad, int X, int Y, int XY, int volume, float4* __restrict__ geo,
+                             float2* __restrict__ qq, unsigned* err) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n_pad) return;
+    float a = 0.f, b = 0.f, cc = 0.f, d = 0.f, qf = 0.f;
+    if (j < n) {
+        const int sj = s[j];
+        if (sj < 0 || sj >= volume) {
+            atomicOr(err, DEVERR_SOURCE_RANGE);
+        } else {
+            // Grid::getIndexX/Y/Z (cubicgrid.cpp:132-145), as kernel.cl:266-268.
+            const int z = sj / XY, y = sj / X - z * Y, x = sj % X;
+            a = -2.f * x; b = -2.f * y; cc = -2.f * z;
+            d = (float)(x * x + y * y + z * z);
+            qf = (float)q[j];
+        }
+    }
+    geo[2 * j] = make_float4(a, a, b, b);
+    geo[2 * j + 1] = make_float4(cc, cc, d, d);
+    qq[j] = make_float2(qf, qf);
+}
+
+// Physical targets: for each requested term the (possibly mirrored) target
+// position.  Term order in `tgt`: direct, left image, right image (present
+// ones only), each block t_pad long.  A left image is the direct sum at
+// x' = -1 - x (distance x_i + x_j + 1, cubicgrid.cpp:117-120); a right image
+// at x' = 2X - 1 - x.  all_sites != 0: target g is lattice site g (kernel 1).
+__global__ void prep_targets(const int32_t* __restrict__ ts, int t, int t_pad, int all_sites,
+                             unsigned terms, int X, int Y, int XY, int volume,
+                             float4* __restrict__ tgt, unsigned* err) {
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= t_pad) return;
+    int x = 0, y = 0, z = 0;
+    if (g < t) {
+        const int sg = all_sites ? g : ts[g];
+        if (sg < 0 || sg >= volume + kDrainIds) {
+            atomicOr(err, DEVERR_TARGET_RANGE);
+        } else {
+            z = sg / XY; y = sg / X - z * Y; x = sg % X;
+        }
+    }
+    int slot = 0;
+    for (int term = 0; term < 3; ++term) {
+        if (!(terms & (1u << term))) continue;
+        int xp = x;
+        if (term == 1) xp = -1 - x;
+        if (term == 2) xp = 2 * X - 1 - x;
+        const float fx = (float)xp, fy = (float)y, fz = (float)z;
+        tgt[(size_t)slot * t_pad + g] =
+            make_float4(fx, fy, fz, (float)(xp * xp + y * y + z * z));
+        ++slot;
+    }
+}
+
+// out[g] = prefactor * (sum over splits of the direct block - image blocks).
+__global__ void finalize(const double* __restrict__ part, int splits, int t_phys, int t,
+                         int t_pad, int nterms, double prefactor, double* __restrict__ out) {
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= t) return;
+    double total = 0.0;
+    for (int slot = 0; slot < nterms; ++slot) {
+        double s = 0.0;
+        const double* p = part + (size_t)slot * t_pad + g;
+        for (int sp = 0; sp < splits; ++sp) s += p[(size_t)sp * t_phys];
+        total = (slot == 0) ? s : total - s;
+    }
+    out[g] = prefactor * total;
+}
+
+__global__ void fill_zero(double* out, int t) {
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g < t) out[g] = 0.0;
+}
+
+// FP64 path: every term in double, 1/sqrt and erf of the CUDA runtime.
+// Sources staged in shared memory by plain loads; one thread per physical
+// target and split.
+constexpr int kF64Threads = 256;
+constexpr int kF64Tile = 512;
+
+__global__ void __launch_bounds__(kF64Threads)
+pair_kernel_f64(const float4* __restrict__ geo, const float2* __restrict__ qq, int n_pad,
+                int splits, const float4* __restrict__ tgt, int t_phys, double* __restrict__ part,
+                int c2, int kind, double erffactor) {
+    __shared__ int4 s_g[kF64Tile];  // x, y, z, q
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    const int split = blockIdx.y;
+    const int j_begin = (int)((long long)split * n_pad / splits);
+    const int j_end = (int)((long long)(split + 1) * n_pad / splits);
+    float4 tp = p < t_phys ? tgt[p] : make_float4(0.f, 0.f, 0.f, 0.f);
+    // target coordinates are exact small integers
+    const int tx = (int)tp.x, ty = (int)tp.y, tz = (int)tp.z;
+    double acc = 0.0;
+    for (int j0 = j_begin; j0 < j_end; j0 += kF64Tile) {
+        const int m = min(kF64Tile, j_end - j0);
+        __syncthreads();
+        for (int k = threadIdx.x; k < m; k += blockDim.x) {
+            const float4 g0 = geo[2 * (j0 + k)], g1 = geo[2 * (j0 + k) + 1];
+            s_g[k] = make_int4((int)(-0.5f * g0.x), (int)(-0.5f * g0.z), (int)(-0.5f * g1.x),
+                               (int)qq[j0 + k].x);
+        }
+        __syncthreads();
+        for (int k = 0; k < m; ++k) {
+            const int4 sk = s_g[k];
+            const int dx = tx - sk.x, dy = ty - sk.y, dz = tz - sk.z;
+            const int r2 = dx * dx + dy * dy + dz * dz;
+            if (r2 > 0 && r2 < c2) {
+                const double r = (double)r2;
+                if (kind == 0) {
+                    acc += (double)sk.w * (1.0 / sqrt(r));
+                } else {
+                    const double rr = sqrt(r);
+                    acc += (double)sk.w * erf(erffactor * rr) / rr;
+                }
+            }
+        }
+    }
+    if (p < t_phys) part[(size_t)split * t_phys + p] = acc;
+}
+
+// ---- launch plumbing --------------------------------------------------------
+
+using PairFn = void (*)(PairArgs);
+
+PairFn pick_pair_kernel(int kind, int path) {
+    if (path == LGM_PATH_TABLE) return &pair_kernel<0, 1, kPairThreads, kPairRP>;
+    if (kind == LGM_GAUSS) return &pair_kernel<1, 0, kPairThreads, kPairRP>;
+    return &pair_kernel<0, 0, kPairThreads, kPairRP>;
+}
+
+int popcount3(unsigned terms) {
+    return ((terms & 1u) ? 1 : 0) + ((terms & 2u) ? 1 : 0) + ((terms & 4u) ? 1 : 0);
+}
+
+// Shared launch sequence.  d_src/d_q: n sources; d_tgt_site: t targets (or
+// all lattice sites when all_sites).  Everything on `st`.
+lgm_status launch_potentials(lgm_ctx* c, int kind, unsigned terms, const int32_t* d_src,
+                             const int32_t* d_q, int n, const int32_t* d_tgt_site, int t,
+                             int all_sites, double* d_out, cudaStream_t st) {
+    const lgm_config& cf = c->cfg;
+    c->last = lgm_launch_info{};
+    c->last.pair_kernel_ms = -1.f;
+    c->timed_pending = false;
+    if (t == 0) return LGM_OK;
+    if (n == 0) {
+        fill_zero<<<(t + 255) / 256, 256, 0, st>>>(d_out, t);
+        LGM_CUDA(c, cudaGetLastError());
+        c->last.kernel_launches = 1;
+        return LGM_OK;
+    }
+    const int nterms = popcount3(terms);
+    const int n_pad = (n + CH - 1) / CH * CH;
+    const int n_chunks = n_pad / CH;
+    const int t_pad = (t + 63) / 64 * 64;
+    const int t_phys = nterms * t_pad;
+    const int tiles = (t_phys + kTile - 1) / kTile;
+    const bool f64 = cf.precision == LGM_PREC_FP64;
+
+    // Splits: fill the SMs with one wave of CTAs (4 resident per SM for the
+    // FP32 kernel), never more splits than source chunks.
+    int splits;
+    if (f64) {
+        const int ctas = (t_phys + kF64Threads - 1) / kF64Threads;
+        splits = std::max(1, std::min({kMaxSplits, (c->sm_count * 8) / std::max(1, ctas),
+                                       (n_pad + kF64Tile - 1) / kF64Tile}));
+    } else {
+        splits = std::max(1, std::min({kMaxSplits, (c->sm_count * 4) / tiles, n_chunks}));
+    }
+
+    lgm_status s;
+    if ((s = grow_device(c, &c->d_geo, &c->geo_cap, (size_t)n_pad * 2)) != LGM_OK) return s;
+    if ((s = grow_device(c, &c->d_qq, &c->qq_cap, (size_t)n_pad)) != LGM_OK) return s;
+    if ((s = grow_device(c, &c->d_tgt, &c->tgt_cap, (size_t)std::max(t_phys, tiles * kTile))) != LGM_OK)
+        return s;
+    if ((s = grow_device(c, &c->d_part, &c->part_cap, (size_t)splits * t_phys)) != LGM_OK) return s;
+
+    prep_sources<<<(n_pad + 255) / 256, 256, 0, st>>>(d_src, d_q, n, n_pad, cf.grid_x, cf.grid_y,
+                                                       c->xy, c->volume, c->d_geo, c->d_qq,
+                                                       c->d_err);
+    LGM_CUDA(c, cudaGetLastError());
+    prep_targets<<<(t_pad + 255) / 256, 256, 0, st>>>(d_tgt_site, t, t_pad, all_sites, terms,
+                                                       cf.grid_x, cf.grid_y, c->xy, c->volume,
+                                                       c->d_tgt, c->d_err);
+    LGM_CUDA(c, cudaGetLastError());
+
+    const int c2 = cf.electrostatic_cutoff * cf.electrostatic_cutoff;
+    if (c->timing) LGM_CUDA(c, cudaEventRecord(c->ev_pair0, st));
+    if (f64) {
+        const double erffactor =
+            cf.coulomb_gaussian_sigma > 0 ? 1.0 / (std::sqrt(2.0) * cf.coulomb_gaussian_sigma) : 0.0;
+        dim3 grid((t_phys + kF64Threads - 1) / kF64Threads, splits);
+        pair_kernel_f64<<<grid, kF64Threads, 0, st>>>(c->d_geo, c->d_qq, n_pad, splits, c->d_tgt,
+                                                      t_phys, c->d_part, c2, kind, erffactor);
+        LGM_CUDA(c, cudaGetLastError());
+        c->last.ctas = grid.x * grid.y;
+        c->last.threads = kF64Threads;
+        c->last.targets_per_thread = 1;
+    } else {
+        PairArgs A;
+        A.geo = c->d_geo; A.qq = c->d_qq; A.n_chunks = n_chunks; A.splits = splits;
+        A.tgt = c->d_tgt; A.t_phys = t_phys; A.part = c->d_part; A.c2 = (float)c2;
+        A.err = c->d_err;
+        if (cf.path == LGM_PATH_TABLE) {
+            A.tab = kind == LGM_GAUSS ? c->d_gtab + 0 : c->d_rtab;  // both full tables
+            A.tab_k = kind == LGM_GAUSS ? c->gtab_k : c->rtab_k;
+        } else {
+            A.tab = c->d_gtab; A.tab_k = kind == LGM_GAUSS ? c->gtab_k : 0;
+        }
+        PairFn fn = pick_pair_kernel(kind, cf.path);
+        const size_t smem = pair_smem_bytes(A.tab_k);
+        dim3 grid(tiles, splits);
+        fn<<<grid, kPairThreads, smem, st>>>(A);
+        LGM_CUDA(c, cudaGetLastError());
+        c->last.ctas = grid.x * grid.y;
+        c->last.threads = kPairThreads;
+        c->last.targets_per_thread = 2 * kPairRP;
+    }
+    if (c->timing) {
+        LGM_CUDA(c, cudaEventRecord(c->ev_pair1, st));
+        c->timed_pending = true;
+    }
+    finalize<<<(t + 255) / 256, 256, 0, st>>>(c->d_part, splits, t_phys, t, t_pad, nterms,
+                                               cf.electrostatic_prefactor, d_out);
+    LGM_CUDA(c, cudaGetLastError());
+    c->last.pairs_tested = (int64_t)nterms * t * (int64_t)n;
+    c->last.splits = splits;
+    c->last.kernel_launches = 4;
+    return LGM_OK;
+}
+
+lgm_status check_device_error(lgm_ctx* c, cudaStream_t st) {
+    LGM_CUDA(c, cudaMemcpyAsync(c->h_err, c->d_err, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+    LGM_CUDA(c, cudaStreamSynchronize(st));
+    const unsigned e = *c->h_err;
+    if (e == 0) return LGM_OK;
+    LGM_CUDA(c, cudaMemsetAsync(c->d_err, 0, sizeof(unsigned), st));
+    LGM_CUDA(c, cudaStreamSynchronize(st));
+    if (e & DEVERR_TIMEOUT) return fail(c, LGM_ERR_TIMEOUT, "a bounded device wait ran out");
+    if (e & DEVERR_SOURCE_RANGE)
+        return fail(c, LGM_ERR_OUT_OF_RANGE, "a source site lies outside [0, volume)");
+    if (e & DEVERR_TARGET_RANGE)
+        return fail(c, LGM_ERR_OUT_OF_RANGE, "a target site lies outside [0, volume + 35)");
+    return fail(c, LGM_ERR_STATE, "device reported an inconsistent state");
+}
+
+lgm_status check_common(lgm_ctx* c, int kind, unsigned terms, int n, int t) {
+    if (!c) return LGM_ERR_INVALID_ARGUMENT;
+    c->err.clear();
+    if (kind != LGM_POINT && kind != LGM_GAUSS)
+        return fail(c, LGM_ERR_INVALID_ARGUMENT, "kind must be LGM_POINT or LGM_GAUSS");
+    if (kind == LGM_GAUSS && !(c->cfg.coulomb_gaussian_sigma > 0))
+        return fail(c, LGM_ERR_INVALID_ARGUMENT, "LGM_GAUSS needs coulomb.gaussian.sigma > 0");
+    if (terms == 0 || (terms & ~7u) || !(terms & LGM_TERM_DIRECT))
+        return fail(c, LGM_ERR_INVALID_ARGUMENT,
+                    "terms must include LGM_TERM_DIRECT and only the three term bits");
+    if (n < 0 || t < 0) return fail(c, LGM_ERR_INVALID_ARGUMENT, "negative size");
+    if (c->cfg.max_charges > 0 && n > c->cfg.max_charges)
+        return fail(c, LGM_ERR_CAPACITY, "more sources than max_charges");
+    if (c->cfg.max_targets > 0 && t > c->cfg.max_targets)
+        return fail(c, LGM_ERR_CAPACITY, "more targets than max_targets");
+    return LGM_OK;
+}
+
+// Host-side range checks for the host-buffer entry points (the reference
+// would index garbage; here the call fails before any work).
+lgm_status check_sites(lgm_ctx* c, const int32_t* src, int n, const int32_t* tgt, int t) {
+    for (int j = 0; j < n; ++j)
+        if (src[j] < 0 || src[j] >= c->volume) {
+            char b[128];
+            std::snprintf(b, sizeof b, "source %d: site %d outside [0, %d)", j, src[j], c->volume);
+            return fail(c, LGM_ERR_OUT_OF_RANGE, b);
+        }
+    for (int g = 0; g < t; ++g)
+        if (tgt[g] < 0 || tgt[g] >= c->volume + kDrainIds) {
+            char b[128];
+            std::snprintf(b, sizeof b, "target %d: site %d outside [0, %d)", g, tgt[g],
+                          c->volume + kDrainIds);
+            return fail(c, LGM_ERR_OUT_OF_RANGE, b);
+        }
+    return LGM_OK;
+}
+
+}  // namespace
+
+// ---- ABI ----------------------------------------------------------------------
+
+extern "C" {
+
+int32_t lgm_abi_version(void) { return LGM_ABI_VERSION; }
+
+const char* lgm_status_string(lgm_status s) {
+    switch (s) {
+    case LGM_OK: return "ok";
+    case LGM_ERR_INVALID_ARGUMENT: return "invalid argument";
+    case LGM_ERR_OUT_OF_RANGE: return "site out of range";
+    case LGM_ERR_CUDA: return "CUDA error";
+    case LGM_ERR_NO_DEVICE: return "no usable sm_100 device";
+    case LGM_ERR_CAPACITY: return "capacity exceeded";
+    case LGM_ERR_TIMEOUT: return "device wait timed out";
+    case LGM_ERR_PARSE: return "parse error";
+    case LGM_ERR_UNSUPPORTED: return "unsupported";
+    case LGM_ERR_STATE: return "invalid state";
+    default: return "unknown status";
+    }
+}
+
+void lgm_config_default(lgm_config* cfg) {
+    if (!cfg) return;
+    std::memset(cfg, 0, sizeof *cfg);
+    // SimulationParameters() defaults (parameters.h:285-378)
+    cfg->grid_x = 128; cfg->grid_y = 128; cfg->grid_z = 1;
+    cfg->electrostatic_cutoff = 50;
+    // setCalculatedValues (parameters.h:384-390) with the constants of
+    // parameters.h:358-362 and dielectric.constant 3.5.
+    const double e = 1.60217646e-19, eps0 = 8.854187817e-12, a = 1e-9, epsr = 3.5;
+    cfg->electrostatic_prefactor = e / (4.0 * M_PI * epsr * eps0 * a);
+    cfg->coulomb_gaussian_sigma = 0.0;
+    cfg->work_x = cfg->work_y = cfg->work_z = 4;
+    cfg->work_size = 256;
+    cfg->opencl_threshold = 256;
+    cfg->max_charges = 0;
+    cfg->max_targets = 0;
+    cfg->precision = LGM_PREC_FP32C;
+    cfg->path = LGM_PATH_RSQRT;
+}
+
+lgm_status lgm_create(const lgm_config* cfg, int32_t device, lgm_ctx** out) {
+    g_create_error.clear();
+    if (!cfg || !out) {
+        g_create_error = "null argument";
+        return LGM_ERR_INVALID_ARGUMENT;
+    }
+    *out = nullptr;
+    const lgm_config& cf = *cfg;
+    if (cf.grid_x < 1 || cf.grid_y < 1 || cf.grid_z < 1) {
+        g_create_error = "grid.x, grid.y and grid.z must be >= 1 (parameters.h:403-414)";
+        return LGM_ERR_INVALID_ARGUMENT;
+    }
+    if (cf.electrostatic_cutoff < 1 || cf.electrostatic_cutoff > 1000) {
+        g_create_error = "electrostatic.cutoff must be in [1, 1000]";
+        return LGM_ERR_INVALID_ARGUMENT;
+    }
+    if (!(cf.coulomb_gaussian_sigma >= 0) || !std::isfinite(cf.electrostatic_prefactor)) {
+        g_create_error = "coulomb.gaussian.sigma must be >= 0 and the prefactor finite";
+        return LGM_ERR_INVALID_ARGUMENT;
+    }
+    if (cf.precision != LGM_PREC_FP32C && cf.precision != LGM_PREC_FP64) {
+        g_create_error = "unknown precision";
+        return LGM_ERR_INVALID_ARGUMENT;
+    }
+    if (cf.path != LGM_PATH_RSQRT && cf.path != LGM_PATH_TABLE) {
+        g_create_error = "unknown path";
+        return LGM_ERR_INVALID_ARGUMENT;
+    }
+    // FP32 exactness of r^2 in expanded form: every intermediate below 2^23
+    // with the right-image targets at x' < 2X (3 L^2 < 2^23).
+    const long long L = std::max<long long>({2LL * cf.grid_x, cf.grid_y, cf.grid_z + 1});
+    if (3 * L * L >= (1LL << 23) ||
+        (long long)cf.grid_x * cf.grid_y * cf.grid_z + kDrainIds > INT32_MAX) {
+        g_create_error = "lattice too large for exact FP32 r^2 (need 3*max(2X,Y,Z+1)^2 < 2^23)";
+        return LGM_ERR_UNSUPPORTED;
+    }
+    int ndev = 0;
+    cudaError_t e = cudaGetDeviceCount(&ndev);
+    if (e != cudaSuccess || ndev == 0) {
+        g_create_error = std::string("no CUDA device: ") + cudaGetErrorString(e);
+        return LGM_ERR_NO_DEVICE;
+    }
+    const int dev = device < 0 ? 0 : device;
+    if (dev >= ndev) {
+        g_create_error = "device id out of range";
+        return LGM_ERR_NO_DEVICE;
+    }
+    cudaDeviceProp prop;
+    if ((e = cudaGetDeviceProperties(&prop, dev)) != cudaSuccess) {
+        g_create_error = std::string("cudaGetDeviceProperties: ") + cudaGetErrorString(e);
+        return LGM_ERR_NO_DEVICE;
+    }
+    if (prop.major != 10) {
+        g_create_error = "device is not sm_100 (B200); this library is built for sm_100a only";
+        return LGM_ERR_NO_DEVICE;
+    }
+    lgm_ctx* c = new (std::nothrow) lgm_ctx();
+    if (!c) {
+        g_create_error = "out of host memory";
+        return LGM_ERR_INVALID_ARGUMENT;
+    }
+    c->cfg = cf;
+    c->device = dev;
+    c->sm_count = prop.multiProcessorCount;
+    c->xy = cf.grid_x * cf.grid_y;
+    c->volume = c->xy * cf.grid_z;
+    auto bail = [&](const char* what, cudaError_t err) {
+        g_create_error = std::string(what) + ": " + cudaGetErrorString(err);
+        lgm_destroy(c);
+        return LGM_ERR_CUDA;
+    };
+    if ((e = cudaSetDevice(dev)) != cudaSuccess) return bail("cudaSetDevice", e);
+    if ((e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking)) != cudaSuccess)
+        return bail("cudaStreamCreate", e);
+    if ((e = cudaMalloc(&c->d_err, sizeof(unsigned))) != cudaSuccess) return bail("cudaMalloc", e);
+    if ((e = cudaMemset(c->d_err, 0, sizeof(unsigned))) != cudaSuccess) return bail("cudaMemset", e);
+    if ((e = cudaMallocHost(&c->h_err, sizeof(unsigned))) != cudaSuccess)
+        return bail("cudaMallocHost", e);
+
+    // Tables indexed by the integer r^2 (potential.cpp:268-308 restated per r^2):
+    //   rtab[k] = 1/sqrt(k) for 0 < k < c^2, 0 at k = 0 and k = c^2 (point, table path);
+    //   gauss: gtab[k] = erf(f sqrt(k))/sqrt(k); with the rsqrt path only the
+    //   k where it differs from 1/sqrt(k) in FP32 are kept and entry gtab_k
+    //   is NaN (the kernel then falls back to 1/r).
+    const int c2 = cf.electrostatic_cutoff * cf.electrostatic_cutoff;
+    {
+        std::vector<float> rt(c2 + 1, 0.f);
+        for (int k = 1; k < c2; ++k) rt[k] = (float)(1.0 / std::sqrt((double)k));
+        c->rtab_k = c2;
+        if ((e = cudaMalloc(&c->d_rtab, rt.size() * sizeof(float))) != cudaSuccess)
+            return bail("cudaMalloc", e);
+        if ((e = cudaMemcpy(c->d_rtab, rt.data(), rt.size() * sizeof(float),
+                            cudaMemcpyHostToDevice)) != cudaSuccess)
+            return bail("cudaMemcpy", e);
+    }
+    {
+        const double sig = cf.coulomb_gaussian_sigma;
+        std::vector<float> gt;
+        if (sig > 0) {
+            const double f = 1.0 / (std::sqrt(2.0) * sig);
+            int kmax = c2;
+            if (cf.path == LGM_PATH_RSQRT) {
+                // erfc(f sqrt(k)) < 2^-30 beyond kmax: erf rounds to 1 in FP32
+                kmax = 1;
+                while (kmax < c2 && std::erfc(f * std::sqrt((double)kmax)) >= 0x1p-30) ++kmax;
+            }
+            gt.assign(kmax + 1, 0.f);
+            for (int k = 1; k < kmax; ++k) {
+                const double r = std::sqrt((double)k);
+                gt[k] = (float)(std::erf(f * r) / r);
+            }
+            gt[kmax] = cf.path == LGM_PATH_RSQRT ? std::nanf("") : 0.f;
+            c->gtab_k = kmax;
+        } else {
+            gt.assign(2, 0.f);
+            c->gtab_k = 0;
+        }
+        if ((e = cudaMalloc(&c->d_gtab, gt.size() * sizeof(float))) != cudaSuccess)
+            return bail("cudaMalloc", e);
+        if ((e = cudaMemcpy(c->d_gtab, gt.data(), gt.size() * sizeof(float),
+                            cudaMemcpyHostToDevice)) != cudaSuccess)
+            return bail("cudaMemcpy", e);
+    }
+    // Shared memory above the 48 KB default for large cutoffs.
+    {
+        const int tk = std::max(c->rtab_k, c->gtab_k);
+        const size_t smem = pair_smem_bytes(tk);
+        if (smem > 48 * 1024) {
+            if (smem > (size_t)prop.sharedMemPerBlockOptin) {
+                g_create_error = "cutoff too large for the shared-memory tables";
+                lgm_destroy(c);
+                return LGM_ERR_UNSUPPORTED;
+            }
+            PairFn fns[3] = {&pair_kernel<0, 0, kPairThreads, kPairRP>,
+                             &pair_kernel<1, 0, kPairThreads, kPairRP>,
+                             &pair_kernel<0, 1, kPairThreads, kPairRP>};
+            for (PairFn fn : fns)
+                if ((e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                              (int)smem)) != cudaSuccess)
+                    return bail("cudaFuncSetAttribute", e);
+        }
+    }
+    *out = c;
+    return LGM_OK;
+}
+
+lgm_status lgm_destroy(lgm_ctx* c) {
+    if (!c) return LGM_OK;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    void* dev_ptrs[] = {c->d_geo, c->d_qq, c->d_tgt, c->d_part, c->d_s, c->d_q,
+                        c->d_t, c->d_o, c->d_gtab, c->d_rtab, c->d_err};
+    for (void* p : dev_ptrs)
+        if (p) cudaFree(p);
+    void* host_ptrs[] = {c->h_s, c->h_q, c->h_t, c->h_o, c->h_err};
+    for (void* p : host_ptrs)
+        if (p) cudaFreeHost(p);
+    if (c->ev_pair0) cudaEventDestroy(c->ev_pair0);
+    if (c->ev_pair1) cudaEventDestroy(c->ev_pair1);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return LGM_OK;
+}
+
+const char* lgm_last_error(const lgm_ctx* c) {
+    if (!c) return g_create_error.c_str();
+    return c->err.c_str();
+}
+
+lgm_status lgm_last_launch(lgm_ctx* c, lgm_launch_info* info) {
+    if (!c || !info) return LGM_ERR_INVALID_ARGUMENT;
+    if (c->timed_pending) {
+        LGM_CUDA(c, cudaEventSynchronize(c->ev_pair1));
+        float ms = -1.f;
+        LGM_CUDA(c, cudaEventElapsedTime(&ms, c->ev_pair0, c->ev_pair1));
+        c->last.pair_kernel_ms = ms;
+        c->timed_pending = false;
+    }
+    *info = c->last;
+    return LGM_OK;
+}
+
+lgm_status lgm_set_timing(lgm_ctx* c, int32_t enable) {
+    if (!c) return LGM_ERR_INVALID_ARGUMENT;
+    LGM_CUDA(c, cudaSetDevice(c->device));
+    if (enable && !c->ev_pair0) {
+        LGM_CUDA(c, cudaEventCreate(&c->ev_pair0));
+        LGM_CUDA(c, cudaEventCreate(&c->ev_pair1));
+    }
+    c->timing = enable != 0;
+    c->timed_pending = false;
+    return LGM_OK;
+}
+
+lgm_status lgm_potentials_async(lgm_ctx* c, lgm_kind kind, uint32_t terms,
+                                const int32_t* d_src_site, const int32_t* d_src_q, int32_t n,
+                                const int32_t* d_tgt_site, int32_t t, double* d_out,
+                                void* stream) {
+    lgm_status s = check_common(c, kind, terms, n, t);
+    if (s != LGM_OK) return s;
+    if ((n > 0 && (!d_src_site || !d_src_q)) || (t > 0 && (!d_tgt_site || !d_out)))
+        return fail(c, LGM_ERR_INVALID_ARGUMENT, "null buffer");
+    LGM_CUDA(c, cudaSetDevice(c->device));
+    cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
+    return launch_potentials(c, kind, terms, d_src_site, d_src_q, n, d_tgt_site, t, 0, d_out, st);
+}
+
+lgm_status lgm_sync(lgm_ctx* c, void* stream) {
+    if (!c) return LGM_ERR_INVALID_ARGUMENT;
+    LGM_CUDA(c, cudaSetDevice(c->device));
+    cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
+    return check_device_error(c, st);
+}
+
+lgm_status lgm_potentials(lgm_ctx* c, lgm_kind kind, uint32_t terms, const int32_t* src_site,
+                          const int32_t* src_q, int32_t n, const int32_t* tgt_site, int32_t t,
+                          double* out) {
+    lgm_status s = check_common(c, kind, terms, n, t);
+    if (s != LGM_OK) return s;
+    if ((n > 0 && (!src_site || !src_q)) || (t > 0 && (!tgt_site || !out)))
+        return fail(c, LGM_ERR_INVALID_ARGUMENT, "null buffer");
+    if ((s = check_sites(c, src_site, n, tgt_site, t)) != LGM_OK) return s;
+    LGM_CUDA(c, cudaSetDevice(c->device));
+    cudaStream_t st = c->stream;
+    const size_t nn = std::max(n, 1), tt = std::max(t, 1);
+    if ((s = grow_host(c, &c->h_s, &c->hs_cap, nn)) != LGM_OK) return s;
+    if ((s = grow_host(c, &c->h_q, &c->hq_cap, nn)) != LGM_OK) return s;
+    if ((s = grow_host(c, &c->h_t, &c->ht_cap, tt)) != LGM_OK) return s;
+    if ((s = grow_host(c, &c->h_o, &c->ho_cap, tt)) != LGM_OK) return s;
+    if ((s = grow_device(c, &c->d_s, &c->s_cap, nn)) != LGM_OK) return s;
+    if ((s = grow_device(c, &c->d_q, &c->q_cap, nn)) != LGM_OK) return s;
+    if ((s = grow_device(c, &c->d_t, &c->t_cap, tt)) != LGM_OK) return s;
+    if ((s = grow_device(c, &c->d_o, &c->o_cap, tt)) != LGM_OK) return s;
+    std::memcpy(c->h_s, src_site, sizeof(int32_t) * n);
+    std::memcpy(c->h_q, src_q, sizeof(int32_t) * n);
+    std::memcpy(c->h_t, tgt_site, sizeof(int32_t) * t);
+    LGM_CUDA(c, cudaMemcpyAsync(c->d_s, c->h_s, sizeof(int32_t) * n, cudaMemcpyHostToDevice, st));
+    LGM_CUDA(c, cudaMemcpyAsync(c->d_q, c->h_q, sizeof(int32_t) * n, cudaMemcpyHostToDevice, st));
+    LGM_CUDA(c, cudaMemcpyAsync(c->d_t, c->h_t, sizeof(int32_t) * t, cudaMemcpyHostToDevice, st));
+    if ((s = launch_potentials(c, kind, terms, c->d_s, c->d_q, n, c->d_t, t, 0, c->d_o, st)) !=
+        LGM_OK)
+        return s;
+    LGM_CUDA(c, cudaMemcpyAsync(c->h_o, c->d_o, sizeof(double) * t, cudaMemcpyDeviceToHost, st));
+    if ((s = check_device_error(c, st)) != LGM_OK) return s;
+    std::memcpy(out, c->h_o, sizeof(double) * t);
+    return LGM_OK;
+}
+
+lgm_status lgm_coulomb_kernel2(lgm_ctx* c, lgm_kind kind, const int32_t* s, const int32_t* q,
+                               int32_t n, int32_t total, double* o) {
+    if (c && (n < 0 || n > total)) return fail(c, LGM_ERR_INVALID_ARGUMENT, "need 0 <= n <= total");
+    // kernel 2: w aliases s (openclhelper.cpp:154), the first n entries are
+    // the sources, every entry is a target.
+    return lgm_potentials(c, kind, LGM_TERM_DIRECT, s, q, n, s, total, o);
+}
+
+lgm_status lgm_coulomb_kernel1_async(lgm_ctx* c, lgm_kind kind, const int32_t* d_s,
+                                     const int32_t* d_q, int32_t n, double* d_o, void* stream) {
+    if (!c) return LGM_ERR_INVALID_ARGUMENT;
+    lgm_status st = check_common(c, kind, LGM_TERM_DIRECT, n, 0);
+    if (st != LGM_OK) return st;
+    if ((n > 0 && (!d_s || !d_q)) || !d_o) return fail(c, LGM_ERR_INVALID_ARGUMENT, "null buffer");
+    LGM_CUDA(c, cudaSetDevice(c->device));
+    cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
+    return launch_potentials(c, kind, LGM_TERM_DIRECT, d_s, d_q, n, nullptr, c->volume, 1, d_o, s);
+}
+
+lgm_status lgm_coulomb_kernel1(lgm_ctx* c, lgm_kind kind, const int32_t* s, const int32_t* q,
+                               int32_t n, double* o) {
+    if (!c) return LGM_ERR_INVALID_ARGUMENT;
+    lgm_status st = check_common(c, kind, LGM_TERM_DIRECT, n, 0);
+    if (st != LGM_OK) return st;
+    if ((n > 0 && (!s || !q)) || !o) return fail(c, LGM_ERR_INVALID_ARGUMENT, "null buffer");
+    if ((st = check_sites(c, s, n, nullptr, 0)) != LGM_OK) return st;
+    LGM_CUDA(c, cudaSetDevice(c->device));
+    cudaStream_t str = c->stream;
+    const size_t nn = std::max(n, 1);
+    const size_t vv = (size_t)c->volume;
+    if ((st = grow_host(c, &c->h_s, &c->hs_cap, nn)) != LGM_OK) return st;
+    if ((st = grow_host(c, &c->h_q, &c->hq_cap, nn)) != LGM_OK) return st;
+    if ((st = grow_host(c, &c->h_o, &c->ho_cap, vv)) != LGM_OK) return st;
+    if ((st = grow_device(c, &c->d_s, &c->s_cap, nn)) != LGM_OK) return st;
+    if ((st = grow_device(c, &c->d_q, &c->q_cap, nn)) != LGM_OK) return st;
+    if ((st = grow_device(c, &c->d_o, &c->o_cap, vv)) != LGM_OK) return st;
+    std::memcpy(c->h_s, s, sizeof(int32_t) * n);
+    std::memcpy(c->h_q, q, sizeof(int32_t) * n);
+    LGM_CUDA(c, cudaMemcpyAsync(c->d_s, c->h_s, sizeof(int32_t) * n, cudaMemcpyHostToDevice, str));
+    LGM_CUDA(c, cudaMemcpyAsync(c->d_q, c->h_q, sizeof(int32_t) * n, cudaMemcpyHostToDevice, str));
+    if ((st = launch_potentials(c, kind, LGM_TERM_DIRECT, c->d_s, c->d_q, n, nullptr, c->volume, 1,
+                                c->d_o, str)) != LGM_OK)
+        return st;
+    LGM_CUDA(c, cudaMemcpyAsync(c->h_o, c->d_o, sizeof(double) * vv, cudaMemcpyDeviceToHost, str));
+    if ((st = check_device_error(c, str)) != LGM_OK) return st;
+    std::memcpy(o, c->h_o, sizeof(double) * vv);
+    return LGM_OK;
+}
+
+}  // extern "C"

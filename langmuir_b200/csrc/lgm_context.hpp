@@ -1,0 +1,45 @@
+// lgm_context.hpp -- host-side state behind an lgm_ctx handle.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "langmuir_b200.h"
+
+struct lgm_ctx {
+    lgm_config cfg{};
+    int device = 0;
+    int sm_count = 0;
+    int volume = 0;
+    int xy = 0;
+    cudaStream_t stream = nullptr;
+
+    // Device work buffers, grown on demand (never inside stream capture).
+    float4* d_geo = nullptr;  size_t geo_cap = 0;   // 2 float4 per source
+    float2* d_qq = nullptr;   size_t qq_cap = 0;    // 1 float2 per source
+    float4* d_tgt = nullptr;  size_t tgt_cap = 0;   // per physical target
+    double* d_part = nullptr; size_t part_cap = 0;  // split partial sums
+    int32_t* d_s = nullptr;   size_t s_cap = 0;     // staging for host-buffer calls
+    int32_t* d_q = nullptr;   size_t q_cap = 0;
+    int32_t* d_t = nullptr;   size_t t_cap = 0;
+    double* d_o = nullptr;    size_t o_cap = 0;
+    float* d_gtab = nullptr;  int gtab_k = 0;       // gauss correction table
+    float* d_rtab = nullptr;  int rtab_k = 0;       // 1/sqrt(k) table
+    unsigned* d_err = nullptr;                       // device error word
+
+    // Pinned host staging for the host-buffer entry points.
+    int32_t* h_s = nullptr;   size_t hs_cap = 0;
+    int32_t* h_q = nullptr;   size_t hq_cap = 0;
+    int32_t* h_t = nullptr;   size_t ht_cap = 0;
+    double* h_o = nullptr;    size_t ho_cap = 0;
+    unsigned* h_err = nullptr;
+
+    bool timing = false;
+    cudaEvent_t ev_pair0 = nullptr, ev_pair1 = nullptr;  // bracket the pair kernel
+    bool timed_pending = false;
+
+    std::string err;
+    lgm_launch_info last{};
+};

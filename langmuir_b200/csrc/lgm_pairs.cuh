@@ -1,0 +1,205 @@
+// lgm_pairs.cuh -- the all-pairs Coulomb sum on sm_100a.
+//
+// Replaces the reference's coulomb2/gauss2 (and coulomb1/gauss1) OpenCL
+// kernels (src/langmuirCore/kernel.cl:56-369): for every target site the sum
+// over all source charges of q_j w(r), 0 < r^2 < cutoff^2.
+//
+// Layout (built by the prep kernels in lgm_api.cu):
+//   source j  -> two float4 {a,a,b,b},{c,c,d,d} with a,b,c = -2x,-2y,-2z and
+//                d = x^2+y^2+z^2, and one float2 {q,q};
+//   target p  -> float4 {x, y, z, x^2+y^2+z^2}.
+// Then r^2 = d + tt + x*a + y*b + z*c: one add and three FMAs, every
+// intermediate an integer below 2^24, so r^2 is exact in FP32.  Each
+// component is stored twice so that one packed FP32x2 instruction serves two
+// targets of a thread.
+//
+// Per pair:  v = r^2 (exact), m = sat(v * (c^2 - v)) is 1 for 1 <= v < c^2
+// and 0 for v = 0 or v >= c^2 (exact on integers), y = min(rsqrt(v), 1)
+// (MUFU; the clamp keeps v = 0 finite), acc += (q*m) * y.
+// Accumulation: runs of 8 sources in FP32 (positive-weighted terms), each run
+// folded into an FP64 accumulator per target; split partials summed in FP64
+// in a fixed order.
+//
+// Sources are staged through shared memory in chunks of CH by bulk TMA copies
+// (cp.async.bulk, no multicast) on two mbarrier-tracked stages; all threads
+// read each source by broadcast.
+#pragma once
+
+#include "lgm_device.cuh"
+
+namespace lgm {
+
+constexpr int CH = 128;   // sources per shared-memory stage
+constexpr int SUB = 8;    // FP32 run length before folding into FP64
+
+struct PairArgs {
+    const float4* geo;      // [n_pad * 2]
+    const float2* qq;       // [n_pad]
+    int n_chunks;           // n_pad / CH
+    int splits;             // source splits (gridDim.y)
+    const float4* tgt;      // [t_phys]
+    int t_phys;             // physical targets (padded)
+    double* part;           // [splits][t_phys]
+    float c2;               // cutoff^2
+    const float* tab;       // gauss correction table or 1/sqrt(k) table
+    int tab_k;              // last valid table index (clamp)
+    unsigned* err;
+};
+
+// Kernel launched with dynamic shared memory pair_smem_bytes(tab_k).
+__host__ __device__ constexpr size_t pair_stage_bytes() {
+    return (size_t)CH * (2 * sizeof(float4) + sizeof(float2));
+}
+inline size_t pair_smem_bytes(int tab_k) {
+    return 2 * pair_stage_bytes() + 16 + (size_t)(tab_k + 1) * sizeof(float) + 16;
+}
+
+// KIND 0 point, 1 gauss.  PATH 0 MUFU rsqrt, 1 shared-memory 1/sqrt(k) table
+// (point only).  NT threads, RP target pairs per thread.
+template <int KIND, int PATH, int NT, int RP>
+__global__ void __launch_bounds__(NT) pair_kernel(PairArgs A) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    float4* s_geo = reinterpret_cast<float4*>(smem);                       // [2][CH*2]
+    float2* s_qq = reinterpret_cast<float2*>(smem + 2 * CH * 2 * sizeof(float4));  // [2][CH]
+    uint64_t* s_bar = reinterpret_cast<uint64_t*>(smem + 2 * pair_stage_bytes());
+    float* s_tab = reinterpret_cast<float*>(smem + 2 * pair_stage_bytes() + 16);
+
+    const int tid = threadIdx.x;
+    const int split = blockIdx.y;
+    const int c_begin = (int)((long long)split * A.n_chunks / A.splits);
+    const int c_end = (int)((long long)(split + 1) * A.n_chunks / A.splits);
+    const int nck = c_end - c_begin;
+
+    if (tid == 0) {
+        mbar_init(&s_bar[0], 1);
+        mbar_init(&s_bar[1], 1);
+        fence_mbar_init();
+    }
+    if (KIND == 1 || PATH == 1)
+        for (int k = tid; k <= A.tab_k; k += NT) s_tab[k] = A.tab[k];
+    __syncthreads();
+
+    auto issue = [&](int i) {
+        const int st = i & 1;
+        const int chunk = c_begin + i;
+        mbar_arrive_expect_tx(&s_bar[st], (uint32_t)pair_stage_bytes());
+        bulk_g2s(s_geo + st * CH * 2, A.geo + (size_t)chunk * CH * 2,
+                 (uint32_t)(CH * 2 * sizeof(float4)), &s_bar[st]);
+        bulk_g2s(s_qq + st * CH, A.qq + (size_t)chunk * CH, (uint32_t)(CH * sizeof(float2)),
+                 &s_bar[st]);
+    };
+    if (tid == 0) {
+        if (nck > 0) issue(0);
+        if (nck > 1) issue(1);
+    }
+
+    // Targets of this thread: p = base + tid + k*NT, k = 0 .. 2*RP-1; pair k
+    // packs targets 2k and 2k+1.
+    const int base = blockIdx.x * (NT * 2 * RP);
+    float2 tx[RP], ty[RP], tz[RP], tt[RP];
+#pragma unroll
+    for (int k = 0; k < RP; ++k) {
+        const int p0 = base + tid + (2 * k) * NT;
+        const int p1 = p0 + NT;
+        const float4 a = p0 < A.t_phys ? A.tgt[p0] : make_float4(0.f, 0.f, 0.f, 0.f);
+        const float4 b = p1 < A.t_phys ? A.tgt[p1] : make_float4(0.f, 0.f, 0.f, 0.f);
+        tx[k] = f2(a.x, b.x); ty[k] = f2(a.y, b.y); tz[k] = f2(a.z, b.z); tt[k] = f2(a.w, b.w);
+    }
+    double acc64[2 * RP];
+#pragma unroll
+    for (int k = 0; k < 2 * RP; ++k) acc64[k] = 0.0;
+
+    const float2 c2v = f2(A.c2, A.c2);
+    const float2 m1 = f2(-1.f, -1.f);
+    int failed_at = -1;
+
+    for (int i = 0; i < nck; ++i) {
+        const int st = i & 1;
+        const uint32_t parity = (uint32_t)((i >> 1) & 1);
+        bool mine = mbar_wait_bounded(&s_bar[st], parity, A.err);
+        if (!__syncthreads_and(mine)) { failed_at = i; break; }
+        const float4* sg = s_geo + st * CH * 2;
+        const float2* sq = s_qq + st * CH;
+
+#pragma unroll 1
+        for (int j0 = 0; j0 < CH; j0 += SUB) {
+            float2 acc[RP];
+#pragma unroll
+            for (int k = 0; k < RP; ++k) acc[k] = f2(0.f, 0.f);
+#pragma unroll
+            for (int jj = 0; jj < SUB; ++jj) {
+                const int j = j0 + jj;
+                const float4 g0 = sg[2 * j];
+                const float4 g1 = sg[2 * j + 1];
+                const float2 qv = sq[j];
+                const float2 av = f2(g0.x, g0.y), bv = f2(g0.z, g0.w);
+                const float2 cv = f2(g1.x, g1.y), dv = f2(g1.z, g1.w);
+#pragma unroll
+                for (int k = 0; k < RP; ++k) {
+                    float2 v = __fadd2_rn(dv, tt[k]);
+                    v = __ffma2_rn(tx[k], av, v);
+                    v = __ffma2_rn(ty[k], bv, v);
+                    v = __ffma2_rn(tz[k], cv, v);  // r^2, exact
+                    if (PATH == 1) {
+                        // 1/sqrt(k) from the table; entries 0 and c^2 are 0, so
+                        // the clamp also applies the cutoff and the r = 0 skip.
+                        const int ix = min(__float_as_int(v.x + 8388608.f) & 0x7fffff, A.tab_k);
+                        const int iy = min(__float_as_int(v.y + 8388608.f) & 0x7fffff, A.tab_k);
+                        acc[k] = __ffma2_rn(qv, f2(s_tab[ix], s_tab[iy]), acc[k]);
+                    } else {
+                        const float2 t = __ffma2_rn(v, m1, c2v);  // c^2 - r^2
+                        const float mx = mul_sat(v.x, t.x);
+                        const float my = mul_sat(v.y, t.y);
+                        float yx = fminf(rsqrt_mufu(v.x), 1.f);
+                        float yy = fminf(rsqrt_mufu(v.y), 1.f);
+                        if (KIND == 1) {
+                            // erf(f r)/r = the tabulated value for r^2 < tab_k,
+                            // else 1/r (entry tab_k is NaN: fminf returns 1/r).
+                            const int ix =
+                                min(__float_as_int(v.x + 8388608.f) & 0x7fffff, A.tab_k);
+                            const int iy =
+                                min(__float_as_int(v.y + 8388608.f) & 0x7fffff, A.tab_k);
+                            yx = fminf(s_tab[ix], yx);
+                            yy = fminf(s_tab[iy], yy);
+                        }
+                        const float2 qm = __fmul2_rn(qv, f2(mx, my));
+                        acc[k] = __ffma2_rn(qm, f2(yx, yy), acc[k]);
+                    }
+                }
+            }
+#pragma unroll
+            for (int k = 0; k < RP; ++k) {
+                acc64[2 * k] += (double)acc[k].x;
+                acc64[2 * k + 1] += (double)acc[k].y;
+            }
+        }
+        __syncthreads();  // every thread is done with stage st
+        if (tid == 0 && i + 2 < nck) {
+            fence_proxy_async_smem();
+            issue(i + 2);
+        }
+    }
+
+    if (failed_at >= 0) {
+        // A stage never completed: wait (bounded) for the copies this CTA
+        // still has in flight -- chunks failed_at and failed_at + 1 -- then
+        // leave without writing results; the host sees DEVERR_TIMEOUT.
+        if (tid == 0) {
+            for (int i = failed_at; i < failed_at + 2 && i < nck; ++i) {
+                const uint32_t parity = (uint32_t)((i >> 1) & 1);
+                for (int it = 0; it < kWaitLimit; ++it)
+                    if (mbar_try_wait(&s_bar[i & 1], parity)) break;
+            }
+        }
+        return;
+    }
+
+    double* out = A.part + (size_t)split * A.t_phys;
+#pragma unroll
+    for (int k = 0; k < 2 * RP; ++k) {
+        const int p = base + tid + k * NT;
+        if (p < A.t_phys) out[p] = acc64[k];
+    }
+}
+
+}  // namespace lgm

@@ -1,0 +1,76 @@
+"""The C ABI library: loads without a GPU and exports every declared symbol."""
+import ctypes
+import os
+import re
+
+import pytest
+
+from langmuir_b200 import _native as N
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "langmuir_b200.h")
+
+
+def declared_functions():
+    text = open(HEADER).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(lgm_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_library_builds_and_loads():
+    from langmuir_b200 import build
+    build.build()
+    assert os.path.exists(N.LIB_PATH)
+    N.lib()
+
+
+def test_every_declared_symbol_is_exported():
+    L = ctypes.CDLL(N.LIB_PATH)
+    names = declared_functions()
+    assert "lgm_coulomb_kernel2" in names and "lgm_create" in names
+    missing = [n for n in names if not hasattr(L, n)]
+    assert not missing, missing
+    # the Python binding covers the whole header
+    assert set(names) <= set(N.SIGNATURES), set(names) - set(N.SIGNATURES)
+
+
+def test_abi_version_and_status_strings():
+    assert N.lib().lgm_abi_version() == 1
+    assert N.lib().lgm_status_string(0) == b"ok"
+    assert N.lib().lgm_status_string(N.ERR_OUT_OF_RANGE) == b"site out of range"
+
+
+def test_config_defaults_match_reference():
+    cfg = N.default_config()
+    # parameters.h:285-378 defaults
+    assert (cfg.grid_x, cfg.grid_y, cfg.grid_z) == (128, 128, 1)
+    assert cfg.electrostatic_cutoff == 50
+    assert cfg.work_size == 256 and cfg.opencl_threshold == 256
+    assert (cfg.work_x, cfg.work_y, cfg.work_z) == (4, 4, 4)
+    assert cfg.electrostatic_prefactor == pytest.approx(0.4114184, rel=1e-6)
+
+
+def test_create_validates_before_touching_a_device():
+    cfg = N.default_config(grid_x=0)
+    h = ctypes.c_void_p()
+    st = N.lib().lgm_create(ctypes.byref(cfg), 0, ctypes.byref(h))
+    assert st == N.ERR_INVALID_ARGUMENT
+    assert b"grid" in N.lib().lgm_last_error(None)
+    cfg = N.default_config(grid_x=4000)
+    assert N.lib().lgm_create(ctypes.byref(cfg), 0, ctypes.byref(h)) == N.ERR_UNSUPPORTED
+
+
+def test_create_without_gpu_reports_no_device():
+    from tests.conftest import HAS_GPU
+    if HAS_GPU:
+        pytest.skip("a GPU is present")
+    cfg = N.default_config()
+    h = ctypes.c_void_p()
+    st = N.lib().lgm_create(ctypes.byref(cfg), 0, ctypes.byref(h))
+    assert st == N.ERR_NO_DEVICE
+    assert not h.value
+
+
+def test_null_context_is_rejected():
+    assert N.lib().lgm_destroy(None) == N.OK
+    assert N.lib().lgm_sync(None, None) == N.ERR_INVALID_ARGUMENT

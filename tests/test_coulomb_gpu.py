@@ -1,0 +1,284 @@
+"""GPU parity of the Coulomb pair sums against the FP64 oracle, through the C ABI.
+
+Tolerance (FP32C path), per target g:
+    |V_gpu - V_oracle| <= 1e-6 * N_g,   N_g = prefactor * sum_j |q_j| w(r_gj)
+(the condition-aware bound: FP32 terms with FP32 runs of 8 folded into FP64);
+FP64 path: 1e-12 relative to N_g.  The reference's own acceptance test
+(ChargeAgent::compareCoulomb, chargeagent.cpp:364-370) asks 1e-4 % = 1e-6
+relative per site potential.
+"""
+import os
+import zlib
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+TOL32 = 1e-6
+TOL64 = 1e-12
+
+
+def golden(name):
+    return dict(np.load(os.path.join(GOLDEN, name + ".npz")))
+
+
+@pytest.fixture(scope="module")
+def lgm():
+    import langmuir_b200
+    return langmuir_b200
+
+
+def norm_of(orc, s, q, n, gauss=False):
+    return orc.kernel2(s, np.abs(np.asarray(q)), n, gauss=gauss)
+
+
+def assert_close(got, want, norm, tol):
+    err = np.abs(got - want)
+    bound = tol * norm + 1e-13
+    bad = np.nonzero(err > bound)[0]
+    assert bad.size == 0, (f"{bad.size} targets off; worst idx {bad[np.argmax(err[bad] / bound[bad])]} "
+                           f"err {err[bad].max():.3e} norm {norm[bad].min():.3e}")
+
+
+def packed_case(orc, rng, ne, nh, nd=0, dq=0, drains=0):
+    """Reference kernel-2 packing (openclhelper.cpp:380-424)."""
+    vol = orc.volume
+    sites = rng.choice(vol, ne + nh + nd, replace=False).astype(np.int32)
+    q = np.concatenate([-np.ones(ne), np.ones(nh), np.full(nd, dq)]).astype(np.int32)
+    fut = []
+    for s in sites[: ne + nh]:
+        nb = orc.neighbors(int(s), 1)
+        fut.append(nb[rng.integers(len(nb))])
+    fut = np.asarray(fut, dtype=np.int32)
+    if drains:
+        fut[rng.choice(len(fut), drains, replace=False)] = vol + rng.integers(0, 35, drains)
+    s_all = np.concatenate([sites, fut]).astype(np.int32)
+    q_all = np.concatenate([q, q[: ne + nh]]).astype(np.int32)
+    return s_all, q_all, ne + nh + nd
+
+
+# ---- golden fixtures (the reference's kernel.cl compiled as C) ----------------------
+@pytest.mark.parametrize("name", ["k2_point_2d", "k2_point_3d_cut", "k2_gauss_3d",
+                                  "k2_gauss_3d_defects"])
+@pytest.mark.parametrize("precision", [0, 1])
+def test_kernel2_golden(lgm, oracle_mod, name, precision):
+    g = golden(name)
+    X, Y, Z = (int(v) for v in g["dims"])
+    sigma = float(g["sigma"])
+    kind = lgm.GAUSS if sigma > 0 else lgm.POINT
+    with lgm.Coulomb(X, Y, Z, cutoff=int(g["cutoff"]), prefactor=float(g["prefactor"]),
+                     sigma=sigma, precision=precision) as c:
+        o = c.kernel2(g["s"], g["q"], int(g["n"]), kind)
+    orc = oracle_mod.Oracle(X, Y, Z, cutoff=int(g["cutoff"]), sigma=sigma,
+                            prefactor=float(g["prefactor"]))
+    nrm = norm_of(orc, g["s"], g["q"], int(g["n"]), gauss=sigma > 0)
+    assert_close(o, g["o"], nrm, TOL32 if precision == 0 else TOL64)
+
+
+@pytest.mark.parametrize("name", ["k1_point", "k1_gauss"])
+def test_kernel1_golden(lgm, oracle_mod, name):
+    g = golden(name)
+    X, Y, Z = (int(v) for v in g["dims"])
+    sigma = float(g["sigma"])
+    kind = lgm.GAUSS if sigma > 0 else lgm.POINT
+    with lgm.Coulomb(X, Y, Z, cutoff=int(g["cutoff"]), prefactor=float(g["prefactor"]),
+                     sigma=sigma) as c:
+        o = c.kernel1(g["s"], g["q"], kind)
+    orc = oracle_mod.Oracle(X, Y, Z, cutoff=int(g["cutoff"]), sigma=sigma,
+                            prefactor=float(g["prefactor"]))
+    nrm = orc.kernel1(g["s"], np.abs(g["q"]), gauss=sigma > 0)
+    assert_close(o, g["o"], nrm, TOL32)
+
+
+# ---- seeded random cases against the oracle ------------------------------------------
+CASES = {
+    # name: X, Y, Z, cutoff, ne, nh, nd, dq, sigma, drains
+    "2d_small": (64, 48, 1, 50, 150, 0, 0, 0, 0.0, 3),
+    "2d_mixed": (128, 128, 1, 50, 82, 81, 0, 0, 0.0, 2),
+    "3d_cut": (40, 36, 20, 12, 300, 280, 40, 1, 0.0, 5),
+    "3d_gauss": (48, 40, 24, 30, 500, 500, 0, 0, 1.0, 4),
+    "3d_gauss_wide": (32, 32, 16, 10, 200, 150, 30, -2, 2.5, 0),
+    "ragged": (17, 13, 7, 5, 37, 29, 3, 1, 0.0, 1),
+}
+
+
+@pytest.mark.parametrize("name", list(CASES))
+@pytest.mark.parametrize("path", [0, 1])
+def test_kernel2_random(lgm, oracle_mod, name, path):
+    X, Y, Z, c, ne, nh, nd, dq, sigma, drains = CASES[name]
+    rng = np.random.default_rng(zlib.crc32(name.encode()))
+    orc = oracle_mod.Oracle(X, Y, Z, cutoff=c, sigma=sigma)
+    s, q, n = packed_case(orc, rng, ne, nh, nd, dq, drains)
+    kind = lgm.GAUSS if sigma > 0 else lgm.POINT
+    with lgm.Coulomb(X, Y, Z, cutoff=c, sigma=sigma, path=path) as ctx:
+        o = ctx.kernel2(s, q, n, kind)
+    want = orc.kernel2(s, q, n, gauss=sigma > 0)
+    assert_close(o, want, norm_of(orc, s, q, n, sigma > 0), TOL32)
+
+
+@pytest.mark.parametrize("terms", [3, 5, 7])
+def test_image_terms(lgm, oracle_mod, terms):
+    X, Y, Z, c = 50, 30, 6, 20
+    rng = np.random.default_rng(terms)
+    orc = oracle_mod.Oracle(X, Y, Z, cutoff=c)
+    src = rng.choice(X * Y * Z, 120, replace=False).astype(np.int32)
+    q = rng.choice([-1, 1], 120).astype(np.int32)
+    tgt = rng.choice(X * Y * Z, 90).astype(np.int32)
+    with lgm.Coulomb(X, Y, Z, cutoff=c) as ctx:
+        o = ctx.potentials(src, q, tgt, lgm.POINT, terms)
+    for g, t in enumerate(tgt):
+        want = orc.species_potential(int(t), src, q)
+        nrm = orc.species_potential(int(t), src, np.abs(q))
+        if terms & 2:
+            want += orc.species_potential(int(t), src, q, image=True)
+            nrm -= orc.species_potential(int(t), src, np.abs(q), image=True)
+        if terms & 4:
+            want += orc.species_potential_right_image(int(t), src, q)
+            nrm -= orc.species_potential_right_image(int(t), src, np.abs(q))
+        assert abs(o[g] - want) <= TOL32 * nrm + 1e-13
+
+
+def test_kernel1_random_3d(lgm, oracle_mod):
+    X, Y, Z, c = 30, 28, 10, 15
+    rng = np.random.default_rng(7)
+    orc = oracle_mod.Oracle(X, Y, Z, cutoff=c)
+    s = rng.choice(X * Y * Z, 400, replace=False).astype(np.int32)
+    q = rng.choice([-1, 1], 400).astype(np.int32)
+    with lgm.Coulomb(X, Y, Z, cutoff=c) as ctx:
+        o = ctx.kernel1(s, q)
+    assert_close(o, orc.kernel1(s, q), orc.kernel1(s, np.abs(q)), TOL32)
+
+
+# ---- edge cases ----------------------------------------------------------------------
+def test_empty_inputs(lgm):
+    with lgm.Coulomb(16, 16, 4, cutoff=8) as ctx:
+        assert ctx.kernel2(np.zeros(0, np.int32), np.zeros(0, np.int32), 0).size == 0
+        o = ctx.potentials(np.zeros(0, np.int32), np.zeros(0, np.int32), [5, 6, 7])
+        np.testing.assert_array_equal(o, 0.0)
+        assert ctx.potentials([3], [1], np.zeros(0, np.int32)).size == 0
+
+
+def test_colocated_and_shell(lgm, oracle_mod):
+    """r = 0 pairs (a charge at its own site, an electron and a hole sharing a
+    site) contribute nothing; a charge exactly at r = cutoff is excluded."""
+    X, Y, Z, c = 40, 8, 4, 10
+    orc = oracle_mod.Oracle(X, Y, Z, cutoff=c)
+    a = orc.site(5, 3, 1)
+    src = np.array([a, a, orc.site(15, 3, 1), orc.site(14, 3, 1), orc.site(6, 3, 1)], np.int32)
+    q = np.array([-1, 1, 1, 2, -1], np.int32)
+    tgt = np.array([a, orc.site(5, 3, 2), X * Y * Z + 3], np.int32)
+    with lgm.Coulomb(X, Y, Z, cutoff=c) as ctx:
+        o = ctx.potentials(src, q, tgt)
+    for g, t in enumerate(tgt):
+        want = orc.species_potential(int(t), src, q)
+        assert abs(o[g] - want) <= TOL32 * max(orc.species_potential(int(t), src, np.abs(q)),
+                                               1e-12) + 1e-13
+    # at site a: r=0 pairs skipped, (15,3,1) at r = 10 = cutoff excluded,
+    # (14,3,1) at r = 9 (q=2), (6,3,1) at r = 1 (q=-1)
+    assert o[0] == pytest.approx(orc.prefactor * (2 / 9 - 1.0), rel=1e-6)
+
+
+def test_full_lattice_of_charges(lgm, oracle_mod):
+    X, Y, Z, c = 12, 10, 6, 7
+    orc = oracle_mod.Oracle(X, Y, Z, cutoff=c)
+    s = np.arange(X * Y * Z, dtype=np.int32)
+    q = np.where(s % 3 == 0, 1, -1).astype(np.int32)
+    with lgm.Coulomb(X, Y, Z, cutoff=c) as ctx:
+        o = ctx.kernel2(s, q, len(s))
+    assert_close(o, orc.kernel2(s, q, len(s)), norm_of(orc, s, q, len(s)), TOL32)
+
+
+def test_range_errors(lgm):
+    import langmuir_b200._native as N
+    with lgm.Coulomb(8, 8, 2, cutoff=5) as ctx:
+        with pytest.raises(lgm.LgmError) as e:
+            ctx.potentials([8 * 8 * 2], [1], [0])
+        assert e.value.status == N.ERR_OUT_OF_RANGE
+        with pytest.raises(lgm.LgmError) as e:
+            ctx.potentials([0], [1], [8 * 8 * 2 + 35])
+        assert e.value.status == N.ERR_OUT_OF_RANGE
+        # drain ids volume .. volume+34 are valid targets
+        ctx.potentials([0], [1], [8 * 8 * 2 + 34])
+        with pytest.raises(lgm.LgmError):
+            ctx.kernel2([1, 2], [1, 1], 3)
+
+
+def test_async_range_error_reported_by_sync(lgm):
+    import torch
+    import langmuir_b200._native as N
+    with lgm.Coulomb(8, 8, 2, cutoff=5) as ctx:
+        s = torch.tensor([1, 2, 500], dtype=torch.int32, device="cuda")
+        q = torch.tensor([1, -1, 1], dtype=torch.int32, device="cuda")
+        o = torch.empty(3, dtype=torch.float64, device="cuda")
+        ctx.potentials_async(s.data_ptr(), q.data_ptr(), 3, s.data_ptr(), 3, o.data_ptr(),
+                             stream=torch.cuda.current_stream().cuda_stream)
+        with pytest.raises(lgm.LgmError) as e:
+            ctx.sync(torch.cuda.current_stream().cuda_stream)
+        assert e.value.status == N.ERR_OUT_OF_RANGE
+        # the context stays usable
+        ctx.potentials_async(s.data_ptr(), q.data_ptr(), 2, s.data_ptr(), 2, o.data_ptr(),
+                             stream=torch.cuda.current_stream().cuda_stream)
+        ctx.sync(torch.cuda.current_stream().cuda_stream)
+
+
+# ---- OpenClHelper mirror: the coulombGPU assembly equals coulombCPU ---------------------
+def test_openclhelper_mirror_matches_coulomb_cpu(lgm, oracle_mod):
+    X, Y, Z, c = 64, 64, 4, 50
+    rng = np.random.default_rng(21)
+    orc = oracle_mod.Oracle(X, Y, Z, cutoff=c)
+    vol = X * Y * Z
+    sites = rng.choice(vol, 700, replace=False).astype(np.int32)
+    e_site, h_site, d_site = sites[:300], sites[300:680], sites[680:]
+    e_f = np.array([rng.choice(orc.neighbors(int(s))) for s in e_site], np.int32)
+    h_f = np.array([rng.choice(orc.neighbors(int(s))) for s in h_site], np.int32)
+
+    class World:
+        parameters = {"grid.x": X, "grid.y": Y, "grid.z": Z, "electrostatic.cutoff": c,
+                      "defects.charge": 1, "use.opencl": True, "coulomb.carriers": True}
+        electrons = [lgm.Carrier(s, -1, f) for s, f in zip(e_site, e_f)]
+        holes = [lgm.Carrier(s, 1, f) for s, f in zip(h_site, h_f)]
+        defect_site_ids = list(d_site)
+
+    w = World()
+    helper = lgm.OpenClHelper(w)
+    helper.initializeOpenCL(0)
+    assert helper.toggleOpenCL(True)
+    helper.launchCoulombKernel2()
+    de_cpu, p1, p2 = orc.coulomb_cpu(e_site, e_f, h_site, h_f, d_site, defects_charge=1,
+                                     want_potentials=True)
+    sI = orc.self_table()[1, 0, 0]
+    for i, ch in enumerate(w.electrons + w.holes):
+        g1 = helper.getOutputHost(ch.opencl_id)
+        g2 = helper.getOutputHostFuture(ch.opencl_id) - sI * ch.charge
+        de_gpu = ch.charge * (g2 - g1)  # chargeagent.cpp:273-296, no binding here
+        # compareCoulomb thresholds (chargeagent.cpp:364-370): 1e-4 absolute on
+        # dE, 1e-4 % on each site potential
+        assert abs(de_gpu - de_cpu[i]) <= 1e-4
+        assert abs(g1 - p1[i]) <= 1e-6 * max(abs(p1[i]), 1e-3)
+        assert abs(g2 - p2[i]) <= 1e-6 * max(abs(p2[i]), 1e-3)
+
+
+# ---- full-size configuration: parity and size-independent properties --------------------
+def test_full_size_3d_config_parity_and_symmetry(lgm, oracle_mod):
+    """256x256x16, 2% occupancy split e/h (~21k charges): FP32C against the
+    FP64 oracle on every target, the sign-flip identity V(-q) = -V(q) bit for
+    bit, and FP64 GPU path against the oracle."""
+    X, Y, Z, c = 256, 256, 16, 50
+    rng = np.random.default_rng(2)
+    orc = oracle_mod.Oracle(X, Y, Z, cutoff=c)
+    ne = nh = int(0.01 * X * Y * Z)
+    s, q, n = packed_case(orc, rng, ne, nh, drains=10)
+    with lgm.Coulomb(X, Y, Z, cutoff=c) as ctx:
+        o = ctx.kernel2(s, q, n)
+        o_neg = ctx.kernel2(s, -q, n)
+    want = orc.kernel2(s, q, n)
+    nrm = norm_of(orc, s, q, n)
+    assert_close(o, want, nrm, TOL32)
+    np.testing.assert_array_equal(o_neg, -o)
+    rel = np.abs(o - want) / nrm
+    assert rel.max() < 1e-6
+    with lgm.Coulomb(X, Y, Z, cutoff=c, precision=1) as ctx:
+        o64 = ctx.kernel2(s, q, n)
+    assert_close(o64, want, nrm, TOL64)
