@@ -200,6 +200,7 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=list(WORKLOADS))
     ap.add_argument("--path", type=int, default=0, help="0 MUFU rsqrt, 1 1/sqrt(k) table")
+    ap.add_argument("--variant", type=int, default=-1, help="tile variant, -1 = autotune")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
@@ -246,6 +247,8 @@ def main():
         ctx.potentials_async(d_s.data_ptr(), d_q.data_ptr(), n, d_s.data_ptr(), T,
                              d_out.data_ptr(), kind, w["terms"], sp)
 
+    variant = ctx.autotune(n, T, kind, w["terms"]) if args.variant < 0 else args.variant
+    ctx.set_variant(variant)
     ctx.set_timing(True)
     for _ in range(args.warmup):
         step()
@@ -350,6 +353,7 @@ def main():
             "config": {"workload": args.workload, "desc": w["desc"], "sources": n,
                        "targets": T, "terms": nterms, "pairs_per_step": pairs_per_step,
                        "path": "table" if args.path else "rsqrt", "l2": "flushed between steps",
+                       "tile_variant": dict(ctx.variants()[variant], id=variant),
                        "parallelism": "replicas" if world > 1 else "single"},
             "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
             "gpu_launches": launches, "accuracy": acc,

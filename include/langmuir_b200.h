@@ -147,6 +147,7 @@ typedef struct lgm_launch_info {
     int32_t targets_per_thread;
     int32_t kernel_launches;   /* kernels launched by the call                      */
     float pair_kernel_ms;      /* device time of the pair kernel (timing on), else -1 */
+    int32_t variant;           /* tile variant of the pair kernel, -1 if none ran   */
 } lgm_launch_info;
 /* Waits for the last launch when timing is on. */
 lgm_status lgm_last_launch(lgm_ctx* ctx, lgm_launch_info* info);
@@ -154,6 +155,21 @@ lgm_status lgm_last_launch(lgm_ctx* ctx, lgm_launch_info* info);
 /* Timing on: CUDA events on the launch stream bracket the pair kernel of
  * every call, read back by lgm_last_launch. */
 lgm_status lgm_set_timing(lgm_ctx* ctx, int32_t enable);
+
+/* ---- tile autotuner --------------------------------------------------------
+ * The pair kernel is compiled in several tile shapes (threads per CTA, target
+ * pairs per thread, FP32 run length).  lgm_autotune times each on synthetic
+ * charges of the given size (n sources, t targets, `terms`) with CUDA events,
+ * remembers the fastest for that size bucket (half-octaves of targets and
+ * source chunks) on this context, and reports it; calls in an untuned bucket
+ * use variant 0.  It allocates, so call it before any stream capture. */
+lgm_status lgm_autotune(lgm_ctx* ctx, lgm_kind kind, uint32_t terms, int32_t n, int32_t t,
+                        int32_t* chosen);
+/* Force a variant (0 .. lgm_variant_count()-1) for every call, -1 = automatic. */
+lgm_status lgm_set_variant(lgm_ctx* ctx, int32_t variant);
+int32_t lgm_variant_count(void);
+lgm_status lgm_variant_info(int32_t variant, int32_t* threads, int32_t* target_pairs,
+                            int32_t* run);
 
 #ifdef __cplusplus
 }

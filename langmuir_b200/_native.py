@@ -63,6 +63,7 @@ class LaunchInfo(ctypes.Structure):
         ("targets_per_thread", ctypes.c_int32),
         ("kernel_launches", ctypes.c_int32),
         ("pair_kernel_ms", ctypes.c_float),
+        ("variant", ctypes.c_int32),
     ]
 
 
@@ -91,6 +92,13 @@ SIGNATURES = {
                                                    ctypes.c_int32, _vp, _vp]),
     "lgm_last_launch": (ctypes.c_int32, [_vp, ctypes.POINTER(LaunchInfo)]),
     "lgm_set_timing": (ctypes.c_int32, [_vp, ctypes.c_int32]),
+    "lgm_autotune": (ctypes.c_int32, [_vp, ctypes.c_int32, ctypes.c_uint32, ctypes.c_int32,
+                                      ctypes.c_int32, ctypes.POINTER(ctypes.c_int32)]),
+    "lgm_set_variant": (ctypes.c_int32, [_vp, ctypes.c_int32]),
+    "lgm_variant_count": (ctypes.c_int32, []),
+    "lgm_variant_info": (ctypes.c_int32, [ctypes.c_int32, ctypes.POINTER(ctypes.c_int32),
+                                          ctypes.POINTER(ctypes.c_int32),
+                                          ctypes.POINTER(ctypes.c_int32)]),
 }
 
 _lib = None

@@ -101,6 +101,24 @@ class Coulomb:
     def sync(self, stream=0):
         self._check(N.lib().lgm_sync(self._h, stream or None))
 
+    def autotune(self, n, t, kind=N.POINT, terms=N.TERM_DIRECT) -> int:
+        v = ctypes.c_int32(-1)
+        self._check(N.lib().lgm_autotune(self._h, int(kind), int(terms), int(n), int(t),
+                                         ctypes.byref(v)))
+        return v.value
+
+    def set_variant(self, v: int):
+        self._check(N.lib().lgm_set_variant(self._h, int(v)))
+
+    @staticmethod
+    def variants():
+        out = []
+        for v in range(N.lib().lgm_variant_count()):
+            a, b, c = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32()
+            N.lib().lgm_variant_info(v, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c))
+            out.append({"threads": a.value, "target_pairs": b.value, "run": c.value})
+        return out
+
     def set_timing(self, on: bool = True):
         self._check(N.lib().lgm_set_timing(self._h, int(bool(on))))
 

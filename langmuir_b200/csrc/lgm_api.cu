@@ -11,6 +11,7 @@
 #include <cstring>
 #include <new>
 #include <string>
+#include <vector>
 
 #include "langmuir_b200.h"
 #include "lgm_context.hpp"
@@ -22,9 +23,6 @@ namespace {
 
 thread_local std::string g_create_error;
 
-constexpr int kPairThreads = 128;   // NT
-constexpr int kPairRP = 4;          // target pairs per thread
-constexpr int kTile = kPairThreads * 2 * kPairRP;  // targets per CTA
 constexpr int kMaxSplits = 64;
 constexpr int kDrainIds = 35;       // Grid::m_specialAgentReserve (cubicgrid.cpp:22)
 
@@ -199,14 +197,124 @@ pair_kernel_f64(const float4* __restrict__ geo, const float2* __restrict__ qq, i
 
 using PairFn = void (*)(PairArgs);
 
-PairFn pick_pair_kernel(int kind, int path) {
-    if (path == LGM_PATH_TABLE) return &pair_kernel<0, 1, kPairThreads, kPairRP>;
-    if (kind == LGM_GAUSS) return &pair_kernel<1, 0, kPairThreads, kPairRP>;
-    return &pair_kernel<0, 0, kPairThreads, kPairRP>;
+// Compiled tile variants of the pair kernel: threads per CTA, target pairs per
+// thread, FP32 run length.  fn[0] point/rsqrt, fn[1] gauss/rsqrt, fn[2] table.
+struct Variant {
+    int nt, rp, sub;
+    PairFn fn[3];
+};
+#define LGM_VARIANT(NT, RP, SUB)                                                  \
+    Variant {                                                                     \
+        NT, RP, SUB, {                                                            \
+            &pair_kernel<0, 0, NT, RP, SUB>, &pair_kernel<1, 0, NT, RP, SUB>,     \
+                &pair_kernel<0, 1, NT, RP, SUB>                                   \
+        }                                                                         \
+    }
+const Variant kVariants[] = {
+    LGM_VARIANT(128, 4, 16), LGM_VARIANT(128, 4, 8),  LGM_VARIANT(128, 2, 16),
+    LGM_VARIANT(128, 8, 16), LGM_VARIANT(256, 4, 16), LGM_VARIANT(64, 4, 16),
+    LGM_VARIANT(128, 4, 32), LGM_VARIANT(256, 2, 16),
+};
+constexpr int kNumVariants = (int)(sizeof(kVariants) / sizeof(kVariants[0]));
+constexpr int kDefaultVariant = 0;
+
+int fn_index(int kind, int path) {
+    if (path == LGM_PATH_TABLE) return 2;
+    return kind == LGM_GAUSS ? 1 : 0;
+}
+
+// Size bucket of a pair launch: half-octaves of physical targets and chunks.
+uint64_t tune_key(int kind, int path, int t_phys, int n_chunks) {
+    auto hb = [](int x) { return (uint64_t)std::lround(2.0 * std::log2((double)std::max(x, 1))); };
+    return ((uint64_t)kind << 60) | ((uint64_t)path << 56) | (hb(t_phys) << 28) | hb(n_chunks);
 }
 
 int popcount3(unsigned terms) {
     return ((terms & 1u) ? 1 : 0) + ((terms & 2u) ? 1 : 0) + ((terms & 4u) ? 1 : 0);
+}
+
+// Source and target records for a call (see lgm_pairs.cuh).
+struct Shape {
+    int nterms, n_pad, n_chunks, t_pad, t_phys;
+};
+
+Shape shape_of(int n, int t, unsigned terms) {
+    Shape sh;
+    sh.nterms = popcount3(terms);
+    sh.n_pad = (n + CH - 1) / CH * CH;
+    sh.n_chunks = sh.n_pad / CH;
+    sh.t_pad = (t + 63) / 64 * 64;
+    sh.t_phys = sh.nterms * sh.t_pad;
+    return sh;
+}
+
+lgm_status prep(lgm_ctx* c, unsigned terms, const int32_t* d_src, const int32_t* d_q, int n,
+                const int32_t* d_tgt_site, int t, int all_sites, const Shape& sh,
+                cudaStream_t st) {
+    const lgm_config& cf = c->cfg;
+    lgm_status s;
+    if ((s = grow_device(c, &c->d_geo, &c->geo_cap, (size_t)sh.n_pad * 2)) != LGM_OK) return s;
+    if ((s = grow_device(c, &c->d_qq, &c->qq_cap, (size_t)sh.n_pad)) != LGM_OK) return s;
+    // room for the widest target tile of any variant
+    if ((s = grow_device(c, &c->d_tgt, &c->tgt_cap, (size_t)sh.t_phys + 4096)) != LGM_OK) return s;
+    prep_sources<<<(sh.n_pad + 255) / 256, 256, 0, st>>>(d_src, d_q, n, sh.n_pad, cf.grid_x,
+                                                          cf.grid_y, c->xy, c->volume, c->d_geo,
+                                                          c->d_qq, c->d_err);
+    LGM_CUDA(c, cudaGetLastError());
+    prep_targets<<<(sh.t_pad + 255) / 256, 256, 0, st>>>(d_tgt_site, t, sh.t_pad, all_sites, terms,
+                                                          cf.grid_x, cf.grid_y, c->xy, c->volume,
+                                                          c->d_tgt, c->d_err);
+    LGM_CUDA(c, cudaGetLastError());
+    return LGM_OK;
+}
+
+// Splits of the source range for variant v: as many as fill one wave of
+// resident CTAs, never more than the chunks.
+int splits_for(const lgm_ctx* c, int v, int fi, const Shape& sh, int* tiles_out) {
+    const Variant& V = kVariants[v];
+    const int tiles = (sh.t_phys + V.nt * 2 * V.rp - 1) / (V.nt * 2 * V.rp);
+    const int capacity = c->sm_count * std::max(1, c->bps[v][fi]);
+    *tiles_out = tiles;
+    return std::max(1, std::min({kMaxSplits, capacity / tiles, sh.n_chunks}));
+}
+
+lgm_status launch_pair(lgm_ctx* c, int kind, int v, const Shape& sh, cudaStream_t st,
+                       int* splits_out) {
+    const lgm_config& cf = c->cfg;
+    const int fi = fn_index(kind, cf.path);
+    int tiles;
+    const int splits = splits_for(c, v, fi, sh, &tiles);
+    lgm_status s;
+    if ((s = grow_device(c, &c->d_part, &c->part_cap, (size_t)splits * sh.t_phys)) != LGM_OK)
+        return s;
+    PairArgs A;
+    A.geo = c->d_geo; A.qq = c->d_qq; A.n_chunks = sh.n_chunks; A.splits = splits;
+    A.tgt = c->d_tgt; A.t_phys = sh.t_phys; A.part = c->d_part;
+    A.c2 = (float)(cf.electrostatic_cutoff * cf.electrostatic_cutoff);
+    A.err = c->d_err;
+    if (cf.path == LGM_PATH_TABLE) {
+        A.tab = kind == LGM_GAUSS ? c->d_gtab : c->d_rtab;  // both hold every r^2 < c^2
+        A.tab_k = kind == LGM_GAUSS ? c->gtab_k : c->rtab_k;
+    } else {
+        A.tab = c->d_gtab;
+        A.tab_k = kind == LGM_GAUSS ? c->gtab_k : 0;
+    }
+    const Variant& V = kVariants[v];
+    dim3 grid(tiles, splits);
+    V.fn[fi]<<<grid, V.nt, pair_smem_bytes(A.tab_k), st>>>(A);
+    LGM_CUDA(c, cudaGetLastError());
+    c->last.ctas = grid.x * grid.y;
+    c->last.threads = V.nt;
+    c->last.targets_per_thread = 2 * V.rp;
+    c->last.variant = v;
+    *splits_out = splits;
+    return LGM_OK;
+}
+
+int choose_variant(const lgm_ctx* c, int kind, const Shape& sh) {
+    if (c->forced_variant >= 0) return c->forced_variant;
+    auto it = c->tune_cache.find(tune_key(kind, c->cfg.path, sh.t_phys, sh.n_chunks));
+    return it == c->tune_cache.end() ? kDefaultVariant : it->second;
 }
 
 // Shared launch sequence.  d_src/d_q: n sources; d_tgt_site: t targets (or
@@ -217,6 +325,7 @@ lgm_status launch_potentials(lgm_ctx* c, int kind, unsigned terms, const int32_t
     const lgm_config& cf = c->cfg;
     c->last = lgm_launch_info{};
     c->last.pair_kernel_ms = -1.f;
+    c->last.variant = -1;
     c->timed_pending = false;
     if (t == 0) return LGM_OK;
     if (n == 0) {
@@ -225,81 +334,40 @@ lgm_status launch_potentials(lgm_ctx* c, int kind, unsigned terms, const int32_t
         c->last.kernel_launches = 1;
         return LGM_OK;
     }
-    const int nterms = popcount3(terms);
-    const int n_pad = (n + CH - 1) / CH * CH;
-    const int n_chunks = n_pad / CH;
-    const int t_pad = (t + 63) / 64 * 64;
-    const int t_phys = nterms * t_pad;
-    const int tiles = (t_phys + kTile - 1) / kTile;
-    const bool f64 = cf.precision == LGM_PREC_FP64;
-
-    // Splits: fill the SMs with one wave of CTAs (4 resident per SM for the
-    // FP32 kernel), never more splits than source chunks.
-    int splits;
-    if (f64) {
-        const int ctas = (t_phys + kF64Threads - 1) / kF64Threads;
-        splits = std::max(1, std::min({kMaxSplits, (c->sm_count * 8) / std::max(1, ctas),
-                                       (n_pad + kF64Tile - 1) / kF64Tile}));
-    } else {
-        splits = std::max(1, std::min({kMaxSplits, (c->sm_count * 4) / tiles, n_chunks}));
-    }
-
+    const Shape sh = shape_of(n, t, terms);
     lgm_status s;
-    if ((s = grow_device(c, &c->d_geo, &c->geo_cap, (size_t)n_pad * 2)) != LGM_OK) return s;
-    if ((s = grow_device(c, &c->d_qq, &c->qq_cap, (size_t)n_pad)) != LGM_OK) return s;
-    if ((s = grow_device(c, &c->d_tgt, &c->tgt_cap, (size_t)std::max(t_phys, tiles * kTile))) != LGM_OK)
-        return s;
-    if ((s = grow_device(c, &c->d_part, &c->part_cap, (size_t)splits * t_phys)) != LGM_OK) return s;
-
-    prep_sources<<<(n_pad + 255) / 256, 256, 0, st>>>(d_src, d_q, n, n_pad, cf.grid_x, cf.grid_y,
-                                                       c->xy, c->volume, c->d_geo, c->d_qq,
-                                                       c->d_err);
-    LGM_CUDA(c, cudaGetLastError());
-    prep_targets<<<(t_pad + 255) / 256, 256, 0, st>>>(d_tgt_site, t, t_pad, all_sites, terms,
-                                                       cf.grid_x, cf.grid_y, c->xy, c->volume,
-                                                       c->d_tgt, c->d_err);
-    LGM_CUDA(c, cudaGetLastError());
-
-    const int c2 = cf.electrostatic_cutoff * cf.electrostatic_cutoff;
+    if ((s = prep(c, terms, d_src, d_q, n, d_tgt_site, t, all_sites, sh, st)) != LGM_OK) return s;
+    int splits = 1;
     if (c->timing) LGM_CUDA(c, cudaEventRecord(c->ev_pair0, st));
-    if (f64) {
+    if (cf.precision == LGM_PREC_FP64) {
         const double erffactor =
             cf.coulomb_gaussian_sigma > 0 ? 1.0 / (std::sqrt(2.0) * cf.coulomb_gaussian_sigma) : 0.0;
-        dim3 grid((t_phys + kF64Threads - 1) / kF64Threads, splits);
-        pair_kernel_f64<<<grid, kF64Threads, 0, st>>>(c->d_geo, c->d_qq, n_pad, splits, c->d_tgt,
-                                                      t_phys, c->d_part, c2, kind, erffactor);
+        const int ctas = (sh.t_phys + kF64Threads - 1) / kF64Threads;
+        splits = std::max(1, std::min({kMaxSplits, (c->sm_count * 8) / std::max(1, ctas),
+                                       (sh.n_pad + kF64Tile - 1) / kF64Tile}));
+        if ((s = grow_device(c, &c->d_part, &c->part_cap, (size_t)splits * sh.t_phys)) != LGM_OK)
+            return s;
+        dim3 grid(ctas, splits);
+        pair_kernel_f64<<<grid, kF64Threads, 0, st>>>(c->d_geo, c->d_qq, sh.n_pad, splits, c->d_tgt,
+                                                      sh.t_phys, c->d_part,
+                                                      cf.electrostatic_cutoff * cf.electrostatic_cutoff,
+                                                      kind, erffactor);
         LGM_CUDA(c, cudaGetLastError());
         c->last.ctas = grid.x * grid.y;
         c->last.threads = kF64Threads;
         c->last.targets_per_thread = 1;
     } else {
-        PairArgs A;
-        A.geo = c->d_geo; A.qq = c->d_qq; A.n_chunks = n_chunks; A.splits = splits;
-        A.tgt = c->d_tgt; A.t_phys = t_phys; A.part = c->d_part; A.c2 = (float)c2;
-        A.err = c->d_err;
-        if (cf.path == LGM_PATH_TABLE) {
-            A.tab = kind == LGM_GAUSS ? c->d_gtab + 0 : c->d_rtab;  // both full tables
-            A.tab_k = kind == LGM_GAUSS ? c->gtab_k : c->rtab_k;
-        } else {
-            A.tab = c->d_gtab; A.tab_k = kind == LGM_GAUSS ? c->gtab_k : 0;
-        }
-        PairFn fn = pick_pair_kernel(kind, cf.path);
-        const size_t smem = pair_smem_bytes(A.tab_k);
-        dim3 grid(tiles, splits);
-        fn<<<grid, kPairThreads, smem, st>>>(A);
-        LGM_CUDA(c, cudaGetLastError());
-        c->last.ctas = grid.x * grid.y;
-        c->last.threads = kPairThreads;
-        c->last.targets_per_thread = 2 * kPairRP;
+        if ((s = launch_pair(c, kind, choose_variant(c, kind, sh), sh, st, &splits)) != LGM_OK)
+            return s;
     }
     if (c->timing) {
         LGM_CUDA(c, cudaEventRecord(c->ev_pair1, st));
         c->timed_pending = true;
     }
-    finalize<<<(t + 255) / 256, 256, 0, st>>>(c->d_part, splits, t_phys, t, t_pad, nterms,
+    finalize<<<(t + 255) / 256, 256, 0, st>>>(c->d_part, splits, sh.t_phys, t, sh.t_pad, sh.nterms,
                                                cf.electrostatic_prefactor, d_out);
     LGM_CUDA(c, cudaGetLastError());
-    c->last.pairs_tested = (int64_t)nterms * t * (int64_t)n;
+    c->last.pairs_tested = (int64_t)sh.nterms * t * (int64_t)n;
     c->last.splits = splits;
     c->last.kernel_launches = 4;
     return LGM_OK;
@@ -524,24 +592,31 @@ lgm_status lgm_create(const lgm_config* cfg, int32_t device, lgm_ctx** out) {
                             cudaMemcpyHostToDevice)) != cudaSuccess)
             return bail("cudaMemcpy", e);
     }
-    // Shared memory above the 48 KB default for large cutoffs.
+    // Shared memory above the 48 KB default for large cutoffs, and the
+    // resident CTAs per SM of every variant (the split count fills one wave).
     {
-        const int tk = std::max(c->rtab_k, c->gtab_k);
-        const size_t smem = pair_smem_bytes(tk);
-        if (smem > 48 * 1024) {
-            if (smem > (size_t)prop.sharedMemPerBlockOptin) {
-                g_create_error = "cutoff too large for the shared-memory tables";
-                lgm_destroy(c);
-                return LGM_ERR_UNSUPPORTED;
+        const size_t smem_tab[3] = {pair_smem_bytes(0), pair_smem_bytes(c->gtab_k),
+                                    pair_smem_bytes(std::max(c->rtab_k, c->gtab_k))};
+        for (int v = 0; v < kNumVariants; ++v)
+            for (int fi = 0; fi < 3; ++fi) {
+                const size_t smem = smem_tab[fi];
+                if (smem > 48 * 1024) {
+                    if (smem > (size_t)prop.sharedMemPerBlockOptin) {
+                        g_create_error = "cutoff too large for the shared-memory tables";
+                        lgm_destroy(c);
+                        return LGM_ERR_UNSUPPORTED;
+                    }
+                    if ((e = cudaFuncSetAttribute(kVariants[v].fn[fi],
+                                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                  (int)smem)) != cudaSuccess)
+                        return bail("cudaFuncSetAttribute", e);
+                }
+                int bps = 0;
+                if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                         &bps, kVariants[v].fn[fi], kVariants[v].nt, smem)) != cudaSuccess)
+                    return bail("cudaOccupancyMaxActiveBlocksPerMultiprocessor", e);
+                c->bps[v][fi] = bps;
             }
-            PairFn fns[3] = {&pair_kernel<0, 0, kPairThreads, kPairRP>,
-                             &pair_kernel<1, 0, kPairThreads, kPairRP>,
-                             &pair_kernel<0, 1, kPairThreads, kPairRP>};
-            for (PairFn fn : fns)
-                if ((e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                              (int)smem)) != cudaSuccess)
-                    return bail("cudaFuncSetAttribute", e);
-        }
     }
     *out = c;
     return LGM_OK;
@@ -592,6 +667,73 @@ lgm_status lgm_set_timing(lgm_ctx* c, int32_t enable) {
     }
     c->timing = enable != 0;
     c->timed_pending = false;
+    return LGM_OK;
+}
+
+int32_t lgm_variant_count(void) { return kNumVariants; }
+
+lgm_status lgm_variant_info(int32_t v, int32_t* threads, int32_t* target_pairs, int32_t* run) {
+    if (v < 0 || v >= kNumVariants) return LGM_ERR_INVALID_ARGUMENT;
+    if (threads) *threads = kVariants[v].nt;
+    if (target_pairs) *target_pairs = kVariants[v].rp;
+    if (run) *run = kVariants[v].sub;
+    return LGM_OK;
+}
+
+lgm_status lgm_set_variant(lgm_ctx* c, int32_t v) {
+    if (!c) return LGM_ERR_INVALID_ARGUMENT;
+    if (v < -1 || v >= kNumVariants) return fail(c, LGM_ERR_INVALID_ARGUMENT, "no such variant");
+    c->forced_variant = v;
+    return LGM_OK;
+}
+
+lgm_status lgm_autotune(lgm_ctx* c, lgm_kind kind, uint32_t terms, int32_t n, int32_t t,
+                        int32_t* chosen) {
+    lgm_status s = check_common(c, kind, terms, n, t);
+    if (s != LGM_OK) return s;
+    if (n < 1 || t < 1) return fail(c, LGM_ERR_INVALID_ARGUMENT, "autotune needs n, t >= 1");
+    LGM_CUDA(c, cudaSetDevice(c->device));
+    cudaStream_t st = c->stream;
+    // Synthetic charges of this size: sites spread over the lattice, q = +-1.
+    std::vector<int32_t> hs(n), hq(n), ht(t);
+    uint64_t x = 0x9E3779B97F4A7C15ull;
+    auto next = [&]() { x ^= x << 13; x ^= x >> 7; x ^= x << 17; return x; };
+    for (int j = 0; j < n; ++j) { hs[j] = (int32_t)(next() % c->volume); hq[j] = (next() & 1) ? 1 : -1; }
+    for (int g = 0; g < t; ++g) ht[g] = (int32_t)(next() % c->volume);
+    if ((s = grow_device(c, &c->d_s, &c->s_cap, (size_t)n)) != LGM_OK) return s;
+    if ((s = grow_device(c, &c->d_q, &c->q_cap, (size_t)n)) != LGM_OK) return s;
+    if ((s = grow_device(c, &c->d_t, &c->t_cap, (size_t)t)) != LGM_OK) return s;
+    LGM_CUDA(c, cudaMemcpyAsync(c->d_s, hs.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice, st));
+    LGM_CUDA(c, cudaMemcpyAsync(c->d_q, hq.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice, st));
+    LGM_CUDA(c, cudaMemcpyAsync(c->d_t, ht.data(), sizeof(int32_t) * t, cudaMemcpyHostToDevice, st));
+    const Shape sh = shape_of(n, t, terms);
+    if ((s = prep(c, terms, c->d_s, c->d_q, n, c->d_t, t, 0, sh, st)) != LGM_OK) return s;
+    cudaEvent_t e0, e1;
+    LGM_CUDA(c, cudaEventCreate(&e0));
+    LGM_CUDA(c, cudaEventCreate(&e1));
+    int best = kDefaultVariant;
+    float best_ms = 1e30f;
+    for (int v = 0; v < kNumVariants; ++v) {
+        int splits;
+        if ((s = launch_pair(c, kind, v, sh, st, &splits)) != LGM_OK) break;  // warm
+        float ms[3];
+        for (int r = 0; r < 3; ++r) {
+            cudaEventRecord(e0, st);
+            if ((s = launch_pair(c, kind, v, sh, st, &splits)) != LGM_OK) break;
+            cudaEventRecord(e1, st);
+            cudaEventSynchronize(e1);
+            cudaEventElapsedTime(&ms[r], e0, e1);
+        }
+        if (s != LGM_OK) break;
+        std::sort(ms, ms + 3);
+        if (ms[1] < best_ms) { best_ms = ms[1]; best = v; }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (s != LGM_OK) return s;
+    if ((s = check_device_error(c, st)) != LGM_OK) return s;
+    c->tune_cache[tune_key(kind, c->cfg.path, sh.t_phys, sh.n_chunks)] = best;
+    if (chosen) *chosen = best;
     return LGM_OK;
 }
 

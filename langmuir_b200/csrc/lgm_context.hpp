@@ -3,6 +3,7 @@
 
 #include <cuda_runtime.h>
 
+#include <map>
 #include <string>
 #include <vector>
 
@@ -35,6 +36,10 @@ struct lgm_ctx {
     int32_t* h_t = nullptr;   size_t ht_cap = 0;
     double* h_o = nullptr;    size_t ho_cap = 0;
     unsigned* h_err = nullptr;
+
+    int bps[16][3] = {};                 // resident CTAs per SM, per variant and kernel
+    int forced_variant = -1;             // -1: autotuned / default
+    std::map<uint64_t, int> tune_cache;  // size bucket -> fastest variant
 
     bool timing = false;
     cudaEvent_t ev_pair0 = nullptr, ev_pair1 = nullptr;  // bracket the pair kernel

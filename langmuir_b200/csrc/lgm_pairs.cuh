@@ -16,8 +16,8 @@
 // Per pair:  v = r^2 (exact), m = sat(v * (c^2 - v)) is 1 for 1 <= v < c^2
 // and 0 for v = 0 or v >= c^2 (exact on integers), y = min(rsqrt(v), 1)
 // (MUFU; the clamp keeps v = 0 finite), acc += (q*m) * y.
-// Accumulation: runs of 8 sources in FP32 (positive-weighted terms), each run
-// folded into an FP64 accumulator per target; split partials summed in FP64
+// Accumulation: runs of SUB sources in FP32, each run folded into an FP64
+// accumulator per target; split partials summed in FP64
 // in a fixed order.
 //
 // Sources are staged through shared memory in chunks of CH by bulk TMA copies
@@ -30,7 +30,6 @@
 namespace lgm {
 
 constexpr int CH = 128;   // sources per shared-memory stage
-constexpr int SUB = 8;    // FP32 run length before folding into FP64
 
 struct PairArgs {
     const float4* geo;      // [n_pad * 2]
@@ -54,10 +53,12 @@ inline size_t pair_smem_bytes(int tab_k) {
     return 2 * pair_stage_bytes() + 16 + (size_t)(tab_k + 1) * sizeof(float) + 16;
 }
 
-// KIND 0 point, 1 gauss.  PATH 0 MUFU rsqrt, 1 shared-memory 1/sqrt(k) table
-// (point only).  NT threads, RP target pairs per thread.
-template <int KIND, int PATH, int NT, int RP>
+// KIND 0 point, 1 gauss.  PATH 0 MUFU rsqrt, 1 shared-memory table of w(k)
+// for every integer r^2 = k (entries 0 and c^2 are 0).  NT threads, RP target
+// pairs per thread, SUB sources per FP32 run (SUB divides CH).
+template <int KIND, int PATH, int NT, int RP, int SUB>
 __global__ void __launch_bounds__(NT) pair_kernel(PairArgs A) {
+    static_assert(CH % SUB == 0, "SUB must divide CH");
     extern __shared__ __align__(128) unsigned char smem[];
     float4* s_geo = reinterpret_cast<float4*>(smem);                       // [2][CH*2]
     float2* s_qq = reinterpret_cast<float2*>(smem + 2 * CH * 2 * sizeof(float4));  // [2][CH]

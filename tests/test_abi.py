@@ -74,3 +74,14 @@ def test_create_without_gpu_reports_no_device():
 def test_null_context_is_rejected():
     assert N.lib().lgm_destroy(None) == N.OK
     assert N.lib().lgm_sync(None, None) == N.ERR_INVALID_ARGUMENT
+
+
+def test_variant_table():
+    n = N.lib().lgm_variant_count()
+    assert n >= 4
+    import ctypes as C
+    a, b, c = C.c_int32(), C.c_int32(), C.c_int32()
+    for v in range(n):
+        assert N.lib().lgm_variant_info(v, C.byref(a), C.byref(b), C.byref(c)) == N.OK
+        assert a.value % 32 == 0 and b.value >= 1 and 128 % c.value == 0
+    assert N.lib().lgm_variant_info(n, None, None, None) == N.ERR_INVALID_ARGUMENT

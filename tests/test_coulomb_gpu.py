@@ -248,16 +248,29 @@ def test_openclhelper_mirror_matches_coulomb_cpu(lgm, oracle_mod):
     helper.launchCoulombKernel2()
     de_cpu, p1, p2 = orc.coulomb_cpu(e_site, e_f, h_site, h_f, d_site, defects_charge=1,
                                      want_potentials=True)
+    # condition numbers: the same sums with |q| (the per-target error scale)
+    s_src = np.concatenate([e_site, h_site, d_site]).astype(np.int32)
+    n1 = orc.potentials(s_src, np.ones(len(s_src), np.int32),
+                        np.concatenate([e_site, h_site]))
+    n2 = orc.potentials(s_src, np.ones(len(s_src), np.int32), np.concatenate([e_f, h_f]))
     sI = orc.self_table()[1, 0, 0]
+    e_occ, h_occ = set(e_site.tolist()), set(h_site.tolist())
+
+    def bind(ch, site):  # bindingPotential, chargeagent.cpp:463-481 (exciton.binding 0)
+        other = h_occ if ch.charge < 0 else e_occ
+        return sI if site in other else 0.0
+
     for i, ch in enumerate(w.electrons + w.holes):
-        g1 = helper.getOutputHost(ch.opencl_id)
-        g2 = helper.getOutputHostFuture(ch.opencl_id) - sI * ch.charge
-        de_gpu = ch.charge * (g2 - g1)  # chargeagent.cpp:273-296, no binding here
+        # ChargeAgent::coulombGPU (chargeagent.cpp:273-296)
+        g1 = helper.getOutputHost(ch.opencl_id) + bind(ch, ch.site)
+        g2 = (helper.getOutputHostFuture(ch.opencl_id) - sI * ch.charge
+              + bind(ch, ch.future_site))
+        de_gpu = ch.charge * (g2 - g1)
         # compareCoulomb thresholds (chargeagent.cpp:364-370): 1e-4 absolute on
         # dE, 1e-4 % on each site potential
         assert abs(de_gpu - de_cpu[i]) <= 1e-4
-        assert abs(g1 - p1[i]) <= 1e-6 * max(abs(p1[i]), 1e-3)
-        assert abs(g2 - p2[i]) <= 1e-6 * max(abs(p2[i]), 1e-3)
+        assert abs(g1 - p1[i]) <= TOL32 * n1[i] + 1e-13
+        assert abs(g2 - p2[i]) <= TOL32 * n2[i] + 1e-13
 
 
 # ---- full-size configuration: parity and size-independent properties --------------------
@@ -282,3 +295,23 @@ def test_full_size_3d_config_parity_and_symmetry(lgm, oracle_mod):
     with lgm.Coulomb(X, Y, Z, cutoff=c, precision=1) as ctx:
         o64 = ctx.kernel2(s, q, n)
     assert_close(o64, want, nrm, TOL64)
+
+
+# ---- every compiled tile variant is exact to the same bound --------------------------
+def test_every_variant_and_autotune(lgm, oracle_mod):
+    X, Y, Z, c = 96, 80, 12, 30
+    rng = np.random.default_rng(99)
+    orc = oracle_mod.Oracle(X, Y, Z, cutoff=c)
+    s, q, n = packed_case(orc, rng, 1500, 1400, 100, 1, drains=3)
+    want = orc.kernel2(s, q, n)
+    nrm = norm_of(orc, s, q, n)
+    with lgm.Coulomb(X, Y, Z, cutoff=c) as ctx:
+        for v in range(len(ctx.variants())):
+            ctx.set_variant(v)
+            assert_close(ctx.kernel2(s, q, n), want, nrm, TOL32)
+            assert ctx.last_launch()["variant"] == v
+        ctx.set_variant(-1)
+        best = ctx.autotune(n, len(s))
+        assert 0 <= best < len(ctx.variants())
+        assert_close(ctx.kernel2(s, q, n), want, nrm, TOL32)
+        assert ctx.last_launch()["variant"] == best
