@@ -77,7 +77,7 @@ __global__ void prep_sources(const int32_t* __restrict__ s, const int32_t* __res
                              float2* __restrict__ qq, unsigned* err) {
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= n_pad) return;
-    float a = 0.f, b = 0.f, cc = 0.f, d = 0.f, qf = 0.f;
+    float a = 0.f, b = 0.f, cc = 0.f, d = -0.5f, qf = 0.f;
     if (j < n) {
         const int sj = s[j];
         if (sj < 0 || sj >= volume) {
@@ -86,7 +86,7 @@ __global__ void prep_sources(const int32_t* __restrict__ s, const int32_t* __res
             // Grid::getIndexX/Y/Z (cubicgrid.cpp:132-145), as kernel.cl:266-268.
             const int z = sj / XY, y = sj / X - z * Y, x = sj % X;
             a = -2.f * x; b = -2.f * y; cc = -2.f * z;
-            d = (float)(x * x + y * y + z * z);
+            d = (float)(x * x + y * y + z * z) - 0.5f;
             qf = (float)q[j];
         }
     }
@@ -497,12 +497,13 @@ lgm_status lgm_create(const lgm_config* cfg, int32_t device, lgm_ctx** out) {
         g_create_error = "unknown path";
         return LGM_ERR_INVALID_ARGUMENT;
     }
-    // FP32 exactness of r^2 in expanded form: every intermediate below 2^23
-    // with the right-image targets at x' < 2X (3 L^2 < 2^23).
+    // FP32 exactness of r^2 - 1/2 in expanded form: every intermediate a
+    // half-integer below 2^22 with the right-image targets at x' < 2X
+    // (6 L^2 < 2^22).
     const long long L = std::max<long long>({2LL * cf.grid_x, cf.grid_y, cf.grid_z + 1});
-    if (3 * L * L >= (1LL << 23) ||
+    if (6 * L * L >= (1LL << 22) ||
         (long long)cf.grid_x * cf.grid_y * cf.grid_z + kDrainIds > INT32_MAX) {
-        g_create_error = "lattice too large for exact FP32 r^2 (need 3*max(2X,Y,Z+1)^2 < 2^23)";
+        g_create_error = "lattice too large for exact FP32 r^2 (need 6*max(2X,Y,Z+1)^2 < 2^22)";
         return LGM_ERR_UNSUPPORTED;
     }
     int ndev = 0;

@@ -89,11 +89,14 @@ __device__ __forceinline__ float rsqrt_mufu(float x) {
     return y;
 }
 
-// x * y clamped to [0, 1] (FMUL.SAT).
-__device__ __forceinline__ float mul_sat(float x, float y) {
-    float r;
-    asm("mul.rn.sat.f32 %0, %1, %2;" : "=f"(r) : "f"(x), "f"(y));
-    return r;
+// acc += q * w if key < lim (unsigned): one compare, one predicated FFMA.
+__device__ __forceinline__ void fma_if_below(float& acc, float q, float w, unsigned key,
+                                             unsigned lim) {
+    asm("{\n\t.reg .pred p;\n\t"
+        "setp.lt.u32 p, %1, %2;\n\t"
+        "@p fma.rn.f32 %0, %3, %4, %0;\n\t}"
+        : "+f"(acc)
+        : "r"(key), "r"(lim), "f"(q), "f"(w));
 }
 
 __device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }

@@ -6,19 +6,20 @@
 //
 // Layout (built by the prep kernels in lgm_api.cu):
 //   source j  -> two float4 {a,a,b,b},{c,c,d,d} with a,b,c = -2x,-2y,-2z and
-//                d = x^2+y^2+z^2, and one float2 {q,q};
+//                d = x^2+y^2+z^2 - 1/2, and one float2 {q,q};
 //   target p  -> float4 {x, y, z, x^2+y^2+z^2}.
-// Then r^2 = d + tt + x*a + y*b + z*c: one add and three FMAs, every
-// intermediate an integer below 2^24, so r^2 is exact in FP32.  Each
+// Then u = d + tt + x*a + y*b + z*c = r^2 - 1/2: one add and three FMAs,
+// every intermediate a half-integer below 2^22, so u is exact in FP32.  Each
 // component is stored twice so that one packed FP32x2 instruction serves two
 // targets of a thread.
 //
-// Per pair:  v = r^2 (exact), m = sat(v * (c^2 - v)) is 1 for 1 <= v < c^2
-// and 0 for v = 0 or v >= c^2 (exact on integers), y = min(rsqrt(v), 1)
-// (MUFU; the clamp keeps v = 0 finite), acc += (q*m) * y.
+// Per pair:  u = r^2 - 1/2 (exact), r^2 = u + 1/2, y = rsqrt(r^2) (MUFU) and,
+// predicated on 0 < u < c^2 - 1/2, acc += q * y.  The predicate is one
+// unsigned compare of u's bit pattern (negative u has the sign bit set, so
+// r = 0 fails it as r^2 >= c^2 does): the cutoff and the reference's r = 0
+// skip cost one ALU instruction, and the accumulate is a predicated FFMA.
 // Accumulation: runs of SUB sources in FP32, each run folded into an FP64
-// accumulator per target; split partials summed in FP64
-// in a fixed order.
+// accumulator per target; split partials summed in FP64 in a fixed order.
 //
 // Sources are staged through shared memory in chunks of CH by bulk TMA copies
 // (cp.async.bulk, no multicast) on two mbarrier-tracked stages; all threads
@@ -109,9 +110,9 @@ __global__ void __launch_bounds__(NT) pair_kernel(PairArgs A) {
     double acc64[2 * RP];
 #pragma unroll
     for (int k = 0; k < 2 * RP; ++k) acc64[k] = 0.0;
+    const unsigned ulim = __float_as_uint(A.c2 - 0.5f);
+    const float2 half2 = f2(0.5f, 0.5f);
 
-    const float2 c2v = f2(A.c2, A.c2);
-    const float2 m1 = f2(-1.f, -1.f);
     int failed_at = -1;
 
     for (int i = 0; i < nck; ++i) {
@@ -124,55 +125,52 @@ __global__ void __launch_bounds__(NT) pair_kernel(PairArgs A) {
 
 #pragma unroll 1
         for (int j0 = 0; j0 < CH; j0 += SUB) {
-            float2 acc[RP];
+            float acc[2 * RP];
 #pragma unroll
-            for (int k = 0; k < RP; ++k) acc[k] = f2(0.f, 0.f);
+            for (int k = 0; k < 2 * RP; ++k) acc[k] = 0.f;
 #pragma unroll
             for (int jj = 0; jj < SUB; ++jj) {
                 const int j = j0 + jj;
                 const float4 g0 = sg[2 * j];
                 const float4 g1 = sg[2 * j + 1];
-                const float2 qv = sq[j];
+                const float qs = sq[j].x;
                 const float2 av = f2(g0.x, g0.y), bv = f2(g0.z, g0.w);
                 const float2 cv = f2(g1.x, g1.y), dv = f2(g1.z, g1.w);
 #pragma unroll
                 for (int k = 0; k < RP; ++k) {
-                    float2 v = __fadd2_rn(dv, tt[k]);
-                    v = __ffma2_rn(tx[k], av, v);
-                    v = __ffma2_rn(ty[k], bv, v);
-                    v = __ffma2_rn(tz[k], cv, v);  // r^2, exact
+                    float2 u = __fadd2_rn(dv, tt[k]);
+                    u = __ffma2_rn(tx[k], av, u);
+                    u = __ffma2_rn(ty[k], bv, u);
+                    u = __ffma2_rn(tz[k], cv, u);  // r^2 - 1/2, exact
+                    const float2 r2 = __fadd2_rn(u, half2);
+                    float wx, wy;
                     if (PATH == 1) {
-                        // 1/sqrt(k) from the table; entries 0 and c^2 are 0, so
-                        // the clamp also applies the cutoff and the r = 0 skip.
-                        const int ix = min(__float_as_int(v.x + 8388608.f) & 0x7fffff, A.tab_k);
-                        const int iy = min(__float_as_int(v.y + 8388608.f) & 0x7fffff, A.tab_k);
-                        acc[k] = __ffma2_rn(qv, f2(s_tab[ix], s_tab[iy]), acc[k]);
+                        // w(k) from the table; entries 0 and c^2 are 0, so the
+                        // clamp also applies the cutoff and the r = 0 skip.
+                        const int ix = min(__float_as_int(r2.x + 8388608.f) & 0x7fffff, A.tab_k);
+                        const int iy = min(__float_as_int(r2.y + 8388608.f) & 0x7fffff, A.tab_k);
+                        wx = s_tab[ix];
+                        wy = s_tab[iy];
                     } else {
-                        const float2 t = __ffma2_rn(v, m1, c2v);  // c^2 - r^2
-                        const float mx = mul_sat(v.x, t.x);
-                        const float my = mul_sat(v.y, t.y);
-                        float yx = fminf(rsqrt_mufu(v.x), 1.f);
-                        float yy = fminf(rsqrt_mufu(v.y), 1.f);
+                        wx = rsqrt_mufu(r2.x);
+                        wy = rsqrt_mufu(r2.y);
                         if (KIND == 1) {
-                            // erf(f r)/r = the tabulated value for r^2 < tab_k,
+                            // erf(f r)/r: the tabulated value for r^2 < tab_k,
                             // else 1/r (entry tab_k is NaN: fminf returns 1/r).
                             const int ix =
-                                min(__float_as_int(v.x + 8388608.f) & 0x7fffff, A.tab_k);
+                                min(__float_as_int(r2.x + 8388608.f) & 0x7fffff, A.tab_k);
                             const int iy =
-                                min(__float_as_int(v.y + 8388608.f) & 0x7fffff, A.tab_k);
-                            yx = fminf(s_tab[ix], yx);
-                            yy = fminf(s_tab[iy], yy);
+                                min(__float_as_int(r2.y + 8388608.f) & 0x7fffff, A.tab_k);
+                            wx = fminf(s_tab[ix], wx);
+                            wy = fminf(s_tab[iy], wy);
                         }
-                        const float2 qm = __fmul2_rn(qv, f2(mx, my));
-                        acc[k] = __ffma2_rn(qm, f2(yx, yy), acc[k]);
                     }
+                    fma_if_below(acc[2 * k], qs, wx, __float_as_uint(u.x), ulim);
+                    fma_if_below(acc[2 * k + 1], qs, wy, __float_as_uint(u.y), ulim);
                 }
             }
 #pragma unroll
-            for (int k = 0; k < RP; ++k) {
-                acc64[2 * k] += (double)acc[k].x;
-                acc64[2 * k + 1] += (double)acc[k].y;
-            }
+            for (int k = 0; k < 2 * RP; ++k) acc64[k] += (double)acc[k];
         }
         __syncthreads();  // every thread is done with stage st
         if (tid == 0 && i + 2 < nck) {
