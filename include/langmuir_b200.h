@@ -138,6 +138,37 @@ lgm_status lgm_coulomb_kernel1_async(lgm_ctx* ctx, lgm_kind kind, const int32_t*
                                      const int32_t* d_q, int32_t n, double* d_o,
                                      void* stream);
 
+/* Kernel-2 potentials that allocate no device memory.  No counterpart in the
+ * reference: its OpenCL helper always allocated its own buffers.
+ *
+ * For callers that cannot call cudaMalloc: a host engine that sets up all of
+ * its device memory once at start-up and forbids allocations afterwards, a
+ * plugin whose device memory is owned by the application that loads it, or
+ * code running where an allocation could stall or fail.  Such a caller owns
+ * the inputs and the output; this entry needs no lgm_ctx.  Its working memory
+ * is one fixed array of LGM_NOALLOC_SCRATCH_BYTES (4.25 MiB) in the library,
+ * which every GPU that loads the library holds until the process exits.
+ *
+ * Same results as lgm_coulomb_kernel2 with LGM_POINT and the default FP32C
+ * precision: d_s[total] / d_q[total] are device buffers packed as for
+ * kernel 2 (the first n entries are the sources), d_o[total] receives the
+ * potentials.  Limits: n <= LGM_NOALLOC_MAX_SOURCES and total <=
+ * LGM_NOALLOC_MAX_TARGETS, else LGM_ERR_CAPACITY (nothing is launched).
+ * Runs on `stream` (a cudaStream_t, NULL = legacy default) on the current
+ * device and returns when the result is in d_o, with LGM_ERR_OUT_OF_RANGE
+ * for a site outside the lattice.
+ *
+ * The first call on a device looks up the array's device address and caches
+ * it; make that first call before any stream capture.  All calls share the
+ * array, so calls that overlap on the GPU race: serialize them. */
+#define LGM_NOALLOC_MAX_SOURCES 32768
+#define LGM_NOALLOC_MAX_TARGETS 65536
+#define LGM_NOALLOC_SCRATCH_BYTES 4456704
+lgm_status lgm_coulomb_kernel2_noalloc(int32_t grid_x, int32_t grid_y, int32_t grid_z,
+                                       int32_t cutoff, double prefactor, const int32_t* d_s,
+                                       const int32_t* d_q, int32_t n, int32_t total,
+                                       double* d_o, void* stream);
+
 /* Launch statistics of the last pair-sum launch on the context. */
 typedef struct lgm_launch_info {
     int64_t pairs_tested;      /* (physical targets) x (sources), padding excluded */

@@ -95,6 +95,10 @@ SIGNATURES = {
     "lgm_autotune": (ctypes.c_int32, [_vp, ctypes.c_int32, ctypes.c_uint32, ctypes.c_int32,
                                       ctypes.c_int32, ctypes.POINTER(ctypes.c_int32)]),
     "lgm_set_variant": (ctypes.c_int32, [_vp, ctypes.c_int32]),
+    "lgm_coulomb_kernel2_noalloc": (ctypes.c_int32, [ctypes.c_int32, ctypes.c_int32,
+                                                     ctypes.c_int32, ctypes.c_int32,
+                                                     ctypes.c_double, _vp, _vp, ctypes.c_int32,
+                                                     ctypes.c_int32, _vp, _vp]),
     "lgm_variant_count": (ctypes.c_int32, []),
     "lgm_variant_info": (ctypes.c_int32, [ctypes.c_int32, ctypes.POINTER(ctypes.c_int32),
                                           ctypes.POINTER(ctypes.c_int32),
