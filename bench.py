@@ -44,8 +44,8 @@ DEFAULT_WORKLOAD = "cfg2_3d_eh_images"
 # + 2 add), 1/sqrt (1), q*w + acc (2).
 FLOP_PER_PAIR = 11
 # DRAM bytes per launch of the pair kernel from one ncu capture of this
-# workload (profiles/pair_kernel_cfg2.md); None until captured.
-PAIR_KERNEL_DRAM_BYTES = None
+# workload (profiles/pair_kernel_cfg2.md): dram__bytes_read + dram__bytes_write.
+PAIR_KERNEL_DRAM_BYTES = 2891264
 
 
 def make_inputs(w, seed):

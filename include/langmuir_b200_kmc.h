@@ -1,0 +1,140 @@
+/*
+ * langmuir_b200_kmc.h -- input keys and the GPU kMC step (C ABI).
+ *
+ * lgm_params carries every key the reference registers
+ * (src/langmuirCore/keyvalueparser.cpp:15-105) with the defaults of
+ * SimulationParameters (include/parameters.h:285-378).  lgm_params_parse reads
+ * the [Parameters] section of a Langmuir input or checkpoint file with the
+ * reference's rules (KeyValueParser::parse, keyvalueparser.cpp:112-173;
+ * CheckPointer::loadParameters, checkpointer.cpp:403-429) and lgm_params_check
+ * applies setCalculatedValues / checkSimulationParameters (parameters.h:384-646),
+ * returning a status and a message where the reference called qFatal.
+ *
+ * lgm_kmc is one simulation replica whose whole step -- proposals, Coulomb
+ * energy changes, Metropolis decisions, conflict resolution, drains and the
+ * electrode sources -- runs on the GPU (Simulation::performIterations,
+ * simulation.cpp:34-111, transistor set-up).
+ */
+#ifndef LANGMUIR_B200_KMC_H
+#define LANGMUIR_B200_KMC_H
+
+#include "langmuir_b200.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct lgm_params {
+    char simulation_type[16];           /* simulation.type: transistor | solarcell */
+    uint32_t current_step;              /* current.step        */
+    int32_t iterations_real;            /* iterations.real     */
+    uint64_t random_seed;               /* random.seed         */
+    int32_t grid_z, grid_y, grid_x;     /* grid.z, grid.y, grid.x */
+    int32_t hopping_range;              /* hopping.range       */
+    int32_t output_is_on;               /* output.is.on        */
+    int32_t iterations_print;           /* iterations.print    */
+    int32_t output_precision, output_width;
+    char output_stub[64];               /* output.stub         */
+    int32_t output_ids_on_delete, output_ids_on_encounter, output_coulomb, output_step_chk;
+    int32_t output_chk_trap_potential, output_potential;
+    int32_t output_xyz, output_xyz_e, output_xyz_h, output_xyz_d, output_xyz_t, output_xyz_mode;
+    int32_t image_traps, image_defects, image_carriers;
+    double electron_percentage, hole_percentage, seed_charges, defect_percentage;
+    double trap_percentage, trap_potential, gaussian_stdev, seed_percentage;
+    double voltage_right, voltage_left, slope_z;
+    int32_t coulomb_carriers;           /* coulomb.carriers        */
+    double coulomb_gaussian_sigma;      /* coulomb.gaussian.sigma  */
+    int32_t defects_charge;             /* defects.charge          */
+    double exciton_binding, temperature_kelvin;
+    double source_rate, e_source_l_rate, e_source_r_rate, h_source_l_rate, h_source_r_rate;
+    double generation_rate;
+    int32_t source_metropolis, source_coulomb;
+    double source_scale_area;
+    int32_t balance_charges;
+    double drain_rate, e_drain_l_rate, e_drain_r_rate, h_drain_l_rate, h_drain_r_rate;
+    double recombination_rate;
+    int32_t recombination_range;
+    int32_t use_opencl, work_x, work_y, work_z, work_size, opencl_threshold, opencl_device_id;
+    int32_t max_threads;
+    /* constants: registered as Constant in the reference, so an input file
+     * cannot change them (variable.h:267-276); set them here directly */
+    double boltzmann_constant, dielectric_constant, elementary_charge, permittivity_space;
+    double grid_factor;
+    int32_t electrostatic_cutoff;
+    double electrostatic_prefactor, inverse_kt;
+    /* extensions (keys the reference does not have):
+     *   image.charges: electrode images in the hop energy, 0 none, 1 x = -1/2,
+     *                  2 x = X - 1/2, 3 both;
+     *   site.disorder: standard deviation (eV) of a Gaussian energy on every site */
+    int32_t image_charges;
+    double site_disorder;
+} lgm_params;
+
+void lgm_params_default(lgm_params* p);
+/* sizeof(lgm_params), for bindings that declare the struct themselves. */
+int32_t lgm_params_size(void);
+
+/* Parse `text` (an input file, or a checkpoint whose first section is
+ * [Parameters]) into *p, starting from its current values.  Rules of the
+ * reference: '#' starts a comment, one '=' per line, keys case-insensitive,
+ * values may be quoted, empty values are skipped, the section ends at a line
+ * "end" or at the end of the text, and -- as std::getline at EOF does there
+ * -- a last line without a trailing newline is not read.  Unknown keys and
+ * malformed lines fail with LGM_ERR_PARSE and a message in err. */
+lgm_status lgm_params_parse(const char* text, lgm_params* p, char* err, int32_t err_len);
+
+/* setCalculatedValues + checkSimulationParameters: derives
+ * electrostatic_prefactor and inverse_kt, then validates; LGM_ERR_INVALID_ARGUMENT
+ * with the reference's message on failure. */
+lgm_status lgm_params_check(lgm_params* p, char* err, int32_t err_len);
+
+/* ---- one replica on the GPU ------------------------------------------------ */
+typedef struct lgm_kmc lgm_kmc;
+
+/* Builds the world on the host -- defects, traps (seeds and growth,
+ * potential.cpp:74-244), site energies (linear field, gate, traps,
+ * potential.cpp:17-72), seeded carriers (world.cpp:759-959) -- from a
+ * Philox stream keyed by (random.seed, replica), then uploads it.  Only the
+ * transistor set-up with source.metropolis off is supported
+ * (LGM_ERR_UNSUPPORTED otherwise). */
+lgm_status lgm_kmc_create(const lgm_params* p, int32_t device, uint32_t replica, lgm_kmc** out);
+lgm_status lgm_kmc_destroy(lgm_kmc* k);
+/* Text of the last error on `k`; k == NULL: why lgm_kmc_create failed on this thread. */
+const char* lgm_kmc_last_error(const lgm_kmc* k);
+
+/* Advance `steps` steps.  The first call records one step as a CUDA graph;
+ * later steps replay it.  Synchronous. */
+lgm_status lgm_kmc_run(lgm_kmc* k, int32_t steps);
+
+typedef struct lgm_kmc_stats {
+    uint32_t step;                 /* current.step                                       */
+    int32_t electrons, holes;      /* carriers now                                       */
+    int32_t max_electrons, max_holes;
+    int32_t defects, traps;
+    uint64_t proposals;            /* carrier proposals processed (hops attempted)        */
+    uint64_t accepted;             /* proposals that moved a carrier or left by a drain   */
+    uint64_t guard_evaluations;    /* decisions re-evaluated in FP64 (near the threshold) */
+    uint64_t counters[16];         /* (attempts, successes) of eSourceL, eSourceR,
+                                      hSourceL, hSourceR, eDrainL, eDrainR, hDrainL, hDrainR */
+} lgm_kmc_stats;
+lgm_status lgm_kmc_stats_get(lgm_kmc* k, lgm_kmc_stats* s);
+
+/* Carrier lists in list order (capacities in entries). */
+lgm_status lgm_kmc_get_carriers(lgm_kmc* k, int32_t* e_sites, int32_t e_cap, int32_t* h_sites,
+                                int32_t h_cap);
+/* Replace the carriers (distinct sites per species, no defect sites). */
+lgm_status lgm_kmc_set_carriers(lgm_kmc* k, const int32_t* e_sites, int32_t ne,
+                                const int32_t* h_sites, int32_t nh);
+/* Site energies (volume values), defect sites, trap sites and potentials. */
+lgm_status lgm_kmc_get_world(lgm_kmc* k, double* site_energy, int32_t* defects, int32_t d_cap,
+                             int32_t* traps, double* trap_potentials, int32_t t_cap);
+/* Per-carrier outcome of the last step (electrons then holes as listed at its
+ * start: 0 occupied, 1 Metropolis accept, 2 Metropolis reject, 3 drain
+ * accept, 4 drain reject) and the Coulomb energy change used. */
+lgm_status lgm_kmc_last_outcomes(lgm_kmc* k, int32_t* outcome, double* de, int32_t cap);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* LANGMUIR_B200_KMC_H */

@@ -1,0 +1,1015 @@
+// lgm_kmc.cu -- one Langmuir kMC replica stepped entirely on the GPU.
+//
+// Step (Simulation::performIterations, transistor set-up, simulation.cpp:34-111),
+// as a chain of kernels that read every count from device memory, so one
+// step is captured once as a CUDA graph and replayed:
+//   choose     proposals, ChargeAgent::chooseFuture (chargeagent.cpp:73-78)
+//   pack       source / target records for the Coulomb sums (kernel-2 layout)
+//   pair       FP32 pair sums + per-target error scale N (lgm_pairs.cuh)
+//   finalize   potentials V and N per target
+//   decide     ChargeAgent::decideFuture (chargeagent.cpp:90-161): Metropolis
+//              with coupling, drains; decisions whose energy lies within the
+//              FP32 error bound of the acceptance threshold are queued
+//   guard      those decisions redone with FP64 sums (the oracle's arithmetic)
+//   claim/move completeTick in list order (chargeagent.cpp:163-199): the lowest
+//              list index wins a contested site; drains remove the carrier
+//   compact    Simulation::nextTick list removal + the four electrode sources'
+//              tryToInject (sourceagent.cpp:92-103) + currentStep += 1
+// Random numbers come from the counter-based stream of lgm_rng.cuh, the
+// stream the oracle (oracle/lgm_oracle_kmc.cpp) uses, so occupancies and
+// decisions compare bit for bit.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <climits>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "langmuir_b200_kmc.h"
+#include "lgm_pairs.cuh"
+#include "lgm_rng.cuh"
+
+using namespace lgm;
+
+namespace {
+
+// Agent::Type (include/agent.h:33-55) in the per-site type arrays.
+enum : uint8_t { T_EMPTY = 0, T_ELECTRON = 1, T_HOLE = 2, T_DEFECT = 3, T_SOURCE = 4, T_DRAIN = 5 };
+// Special agent ids above the lattice (Grid::registerSpecialAgent in the order
+// of World::createSources/createDrains, world.cpp:961-1187).
+constexpr int kSpecial = 35;
+constexpr int E_DRAIN_L = 3, E_DRAIN_R = 4, H_DRAIN_L = 2, H_DRAIN_R = 3;
+// Outcomes (same codes as the oracle).
+enum : int32_t { O_OCCUPIED = 0, O_MET_ACCEPT = 1, O_MET_REJECT = 2, O_DRAIN_ACCEPT = 3,
+                 O_DRAIN_REJECT = 4 };
+// Device counters: 16 flux (attempts, successes) + proposals + accepted + guard.
+enum { C_PROPOSALS = 16, C_ACCEPTED = 17, C_GUARD = 18, C_NUM = 19 };
+// Device ints.
+enum { I_NE = 0, I_NH, I_STEP, I_NFLAG, I_REMOVED, I_NE0, I_NH0, I_NCHUNK, I_TPHYS, I_TPAD,
+       I_NUM };
+
+// Guard band: FP32C potentials carry at most (2 ulp rsqrt + 31 u run sums)
+// ~ 2.1e-6 N of error each; a decision whose energy lies within kGuard*(N_c +
+// N_f) of the threshold is redone in FP64.
+constexpr double kGuard = 8e-6;
+
+constexpr int kNT = 128, kRP = 4, kSUB = 32;
+constexpr int kTile = kNT * 2 * kRP;
+
+struct Dev {
+    int X, Y, Z, XY, V, hr;
+    int cap_e, cap_h, nd, dq;
+    uint32_t seed, replica;
+    double beta, exciton_binding, sI100, prefactor, erffactor;
+    double coupling[27];
+    double rate_src[4], rate_drain[4];  // eL eR hL hR
+    int coulomb, gauss;
+    unsigned terms;  // LGM_TERM_* bits
+    int nterms;
+    int cutoff2;
+    double* pot;
+    uint8_t *et, *ht;
+    int32_t *e_site, *h_site, *e_f, *h_f, *defects;
+    int32_t *claim_e, *claim_h;
+    int32_t* outcome;
+    double* de;
+    uint8_t* accept;
+    int32_t* flagged;
+    int32_t* cnt;
+    unsigned long long* ctr;
+    float4* geo;
+    float2* qq;
+    float4* tgt;
+    double* part;
+    float* part_norm;
+    double *Vt, *Nt;
+    int splits;
+    int src_cap;   // source records capacity (multiple of CH)
+    int tpad_cap;  // per-term target block capacity
+    unsigned* err;
+};
+
+// ---- lattice helpers (cubicgrid.cpp:132-165, 207-471) ---------------------------
+__device__ __forceinline__ void xyz(const Dev& D, int s, int& x, int& y, int& z) {
+    z = s / D.XY;
+    y = s / D.X - z * D.Y;
+    x = s % D.X;
+}
+__device__ __forceinline__ int sidx(const Dev& D, int x, int y, int z) {
+    return D.X * (y + z * D.Y) + x;
+}
+
+// Grid::neighborsSite in the reference's push order, then the face drains.
+__device__ int neighbors(const Dev& D, int site, bool electron, int* nb) {
+    int x, y, z;
+    xyz(D, site, x, y, z);
+    const int X = D.X, Y = D.Y, Z = D.Z;
+    int n = 0;
+    auto S = [&](int a, int b, int c) { nb[n++] = sidx(D, a, b, c); };
+    if (D.hr == 1) {
+        if (x > 0) S(x - 1, y, z);
+        if (x < X - 1) S(x + 1, y, z);
+        if (y > 0) S(x, y - 1, z);
+        if (y < Y - 1) S(x, y + 1, z);
+        if (z > 0) S(x, y, z - 1);
+        if (z < Z - 1) S(x, y, z + 1);
+    } else if (Z == 1) {
+        if (x > 0) { S(x - 1, y, z); if (y > 0) S(x - 1, y - 1, z); if (y < Y - 1) S(x - 1, y + 1, z); if (x > 1) S(x - 2, y, z); }
+        if (x < X - 1) { S(x + 1, y, z); if (y > 0) S(x + 1, y - 1, z); if (y < Y - 1) S(x + 1, y + 1, z); if (x < X - 2) S(x + 2, y, z); }
+        if (y > 0) { S(x, y - 1, z); if (y > 1) S(x, y - 2, z); }
+        if (y < Y - 1) { S(x, y + 1, z); if (y < Y - 2) S(x, y + 2, z); }
+    } else {
+        if (x > 0) {
+            S(x - 1, y, z);
+            if (y > 0) { S(x - 1, y - 1, z); if (z > 0) S(x - 1, y - 1, z - 1); if (z < Z - 1) S(x - 1, y - 1, z + 1); }
+            if (y < Y - 1) { S(x - 1, y + 1, z); if (z > 0) S(x - 1, y + 1, z - 1); if (z < Z - 1) S(x - 1, y + 1, z + 1); }
+            if (z > 0) S(x - 1, y, z - 1);
+            if (z < Z - 1) S(x - 1, y, z + 1);
+            if (x > 1) S(x - 2, y, z);
+        }
+        if (x < X - 1) {
+            S(x + 1, y, z);
+            if (y > 0) { S(x + 1, y - 1, z); if (z > 0) S(x + 1, y - 1, z - 1); if (z < Z - 1) S(x + 1, y - 1, z + 1); }
+            if (y < Y - 1) { S(x + 1, y + 1, z); if (z > 0) S(x + 1, y + 1, z - 1); if (z < Z - 1) S(x + 1, y + 1, z + 1); }
+            if (z > 0) S(x + 1, y, z - 1);
+            if (z < Z - 1) S(x + 1, y, z + 1);
+            if (x < X - 2) S(x + 2, y, z);
+        }
+        if (z > 0) { S(x, y, z - 1); if (y > 0) S(x, y - 1, z - 1); if (y < Y - 1) S(x, y + 1, z - 1); if (z > 1) S(x, y, z - 2); }
+        if (z < Z - 1) { S(x, y, z + 1); if (y > 0) S(x, y - 1, z + 1); if (y < Y - 1) S(x, y + 1, z + 1); if (z < Z - 2) S(x, y, z + 2); }
+        if (y > 0) { S(x, y - 1, z); if (y > 1) S(x, y - 2, z); }
+        if (y < Y - 1) { S(x, y + 1, z); if (y < Y - 2) S(x, y + 2, z); }
+    }
+    if (x == 0) nb[n++] = D.V + (electron ? E_DRAIN_L : H_DRAIN_L);
+    if (x == X - 1) nb[n++] = D.V + (electron ? E_DRAIN_R : H_DRAIN_R);
+    return n;
+}
+
+__device__ __forceinline__ Philox4 draw(const Dev& D, uint32_t step, uint32_t index,
+                                        uint32_t purpose) {
+    return philox4x32_10(step, index, purpose, 0u, D.seed, D.replica);
+}
+
+// ---- kernels ----------------------------------------------------------------------
+
+// Proposals; also snapshots the step's carrier counts.
+__global__ void k_choose(Dev D) {
+    const int ne = D.cnt[I_NE], nh = D.cnt[I_NH];
+    const uint32_t step = (uint32_t)D.cnt[I_STEP];
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i == 0) {
+        D.cnt[I_NE0] = ne;
+        D.cnt[I_NH0] = nh;
+        D.cnt[I_NFLAG] = 0;
+        D.cnt[I_REMOVED] = 0;
+    }
+    if (i >= ne + nh) return;
+    const bool e = i < ne;
+    const int k = e ? i : i - ne;
+    const int site = e ? D.e_site[k] : D.h_site[k];
+    int nb[40];
+    const int n = neighbors(D, site, e, nb);
+    const Philox4 r = draw(D, step, (uint32_t)k, e ? RNG_CHOOSE_E : RNG_CHOOSE_H);
+    const int f = nb[uint_below(r.w[0], (uint32_t)n)];
+    (e ? D.e_f : D.h_f)[k] = f;
+}
+
+// Source records (electrons, holes, defects, each padded to whole chunks so
+// that every FP32 run holds one charge sign) and target records (current sites
+// then future sites, one block per term).
+__global__ void k_pack(Dev D) {
+    const int ne = D.cnt[I_NE], nh = D.cnt[I_NH];
+    const int nd = D.dq != 0 ? D.nd : 0;
+    const int pe = (ne + CH - 1) / CH * CH, ph = (nh + CH - 1) / CH * CH,
+              pd = (nd + CH - 1) / CH * CH;
+    const int nsrc = pe + ph + pd;
+    const int t = 2 * (ne + nh);
+    const int tpad = (t + 63) / 64 * 64;
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j == 0) {
+        D.cnt[I_NCHUNK] = nsrc / CH;
+        D.cnt[I_TPHYS] = D.nterms * tpad;
+        D.cnt[I_TPAD] = tpad;
+    }
+    if (j < D.src_cap) {
+        float a = 0.f, b = 0.f, c = 0.f, d = -0.5f, q = 0.f;
+        int s = -1;
+        if (j < pe) { if (j < ne) { s = D.e_site[j]; q = -1.f; } }
+        else if (j < pe + ph) { const int k = j - pe; if (k < nh) { s = D.h_site[k]; q = 1.f; } }
+        else if (j < nsrc) { const int k = j - pe - ph; if (k < nd) { s = D.defects[k]; q = (float)D.dq; } }
+        if (s >= 0) {
+            int x, y, z;
+            xyz(D, s, x, y, z);
+            a = -2.f * x; b = -2.f * y; c = -2.f * z;
+            d = (float)(x * x + y * y + z * z) - 0.5f;
+        }
+        D.geo[2 * j] = make_float4(a, a, b, b);
+        D.geo[2 * j + 1] = make_float4(c, c, d, d);
+        D.qq[j] = make_float2(q, q);
+    }
+    if (j < tpad) {
+        int s = -1;
+        if (j < ne) s = D.e_site[j];
+        else if (j < ne + nh) s = D.h_site[j - ne];
+        else if (j < 2 * ne + nh) s = D.e_f[j - ne - nh];
+        else if (j < t) s = D.h_f[j - 2 * ne - nh];
+        int x = 0, y = 0, z = 0;
+        if (s >= 0) xyz(D, s, x, y, z);  // drain ids decode beyond the lattice: unused
+        int slot = 0;
+        for (int term = 0; term < 3; ++term) {
+            if (!(D.terms & (1u << term))) continue;
+            const int xp = term == 0 ? x : (term == 1 ? -1 - x : 2 * D.X - 1 - x);
+            D.tgt[(size_t)slot * tpad + j] =
+                make_float4((float)xp, (float)y, (float)z, (float)(xp * xp + y * y + z * z));
+            ++slot;
+        }
+    }
+}
+
+__global__ void k_finalize(Dev D) {
+    const int t = 2 * (D.cnt[I_NE] + D.cnt[I_NH]);
+    const int tpad = D.cnt[I_TPAD], tphys = D.cnt[I_TPHYS];
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= t) return;
+    double v = 0.0, n = 0.0;
+    for (int slot = 0; slot < D.nterms; ++slot) {
+        double s = 0.0, m = 0.0;
+        for (int sp = 0; sp < D.splits; ++sp) {
+            const size_t o = (size_t)sp * tphys + (size_t)slot * tpad + g;
+            s += D.part[o];
+            m += (double)D.part_norm[o];
+        }
+        v = slot == 0 ? s : v - s;
+        n += m;
+    }
+    D.Vt[g] = D.prefactor * v;
+    D.Nt[g] = D.prefactor * n;
+}
+
+// ChargeAgent::bindingPotential (chargeagent.cpp:463-481)
+__device__ __forceinline__ double binding(const Dev& D, bool e, int site) {
+    if (e) return D.ht[site] == T_HOLE ? D.sI100 + D.exciton_binding : 0.0;
+    return D.et[site] == T_ELECTRON ? D.sI100 - D.exciton_binding : 0.0;
+}
+
+__device__ __forceinline__ double coupling_of(const Dev& D, int s, int f) {
+    int x0, y0, z0, x1, y1, z1;
+    xyz(D, s, x0, y0, z0);
+    xyz(D, f, x1, y1, z1);
+    const int dx = abs(x0 - x1), dy = abs(y0 - y1), dz = abs(z0 - z1);
+    const int h = D.hr + 1;
+    return D.coupling[(dx * h + dy) * h + dz];
+}
+
+// Random::metropolisWithCoupling (rand.cpp:91-106) on an FP64 energy.
+__device__ __forceinline__ bool metropolis(double pd, double beta, double c, double u) {
+    if (pd > 0.0) return c * exp(-pd * beta) > u;
+    return c > u;
+}
+
+__global__ void k_decide(Dev D) {
+    const int ne = D.cnt[I_NE0], nh = D.cnt[I_NH0];
+    const uint32_t step = (uint32_t)D.cnt[I_STEP];
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= ne + nh) return;
+    const bool e = i < ne;
+    const int k = e ? i : i - ne;
+    const int site = e ? D.e_site[k] : D.h_site[k];
+    int f = e ? D.e_f[k] : D.h_f[k];
+    const uint8_t type = (e ? D.et : D.ht)[f];
+    const double q = e ? -1.0 : 1.0;
+    int32_t out = O_OCCUPIED;
+    uint8_t acc = 0;
+    double de = 0.0;
+    if (type == T_EMPTY) {
+        const double c = coupling_of(D, site, f);
+        const Philox4 r = draw(D, step, (uint32_t)k, e ? RNG_DECIDE_E : RNG_DECIDE_H);
+        const double u = unit_double(r.w[0], r.w[1]);
+        double pd = (D.pot[f] - D.pot[site]) * q;
+        bool flag = false;
+        if (D.coulomb) {
+            const int t = ne + nh;
+            const double p1 = D.Vt[i] + binding(D, e, site);
+            const double p2 = D.Vt[t + i] - D.sI100 * q + binding(D, e, f);
+            de = q * (p2 - p1);
+            pd += de;
+            if (u < c) {
+                const double tau = log(c / u) / D.beta;
+                const double g = kGuard * (D.Nt[i] + D.Nt[t + i]) + 1e-12 * (1.0 + fabs(pd));
+                if (fabs(pd - tau) <= g) flag = true;
+                else acc = pd < tau;
+            }
+        } else {
+            acc = metropolis(pd, D.beta, c, u);
+        }
+        if (flag) {
+            const int slot = atomicAdd(&D.cnt[I_NFLAG], 1);
+            D.flagged[slot] = i;
+            out = -1;  // pending
+        } else {
+            out = acc ? O_MET_ACCEPT : O_MET_REJECT;
+        }
+    } else if (type == T_DRAIN) {
+        const int which = f - D.V;
+        const int agent = e ? (which == E_DRAIN_L ? 0 : 1) : (which == H_DRAIN_L ? 2 : 3);
+        atomicAdd(&D.ctr[2 * (4 + agent)], 1ull);
+        const Philox4 r = draw(D, step, (uint32_t)k, e ? RNG_DECIDE_E : RNG_DECIDE_H);
+        const double u = unit_double(r.w[0], r.w[1]);
+        if (D.rate_drain[agent] > u) {  // chooseYes (fluxagent.cpp:125-130)
+            atomicAdd(&D.ctr[2 * (4 + agent) + 1], 1ull);
+            acc = 1;
+            out = O_DRAIN_ACCEPT;
+        } else {
+            out = O_DRAIN_REJECT;
+        }
+    }
+    D.outcome[i] = out;
+    D.de[i] = de;
+    D.accept[i] = acc;
+}
+
+// FP64 re-evaluation of queued decisions: the potentials at the current and
+// future site summed in double over all charges (and their images), then the
+// reference's test on the FP64 energy.  One block per queued decision,
+// grid-stride over the queue.
+constexpr int kGuardThreads = 256;
+
+__device__ double fp64_potential(const Dev& D, int ne, int nh, int site, double* red) {
+    int xi, yi, zi;
+    xyz(D, site, xi, yi, zi);
+    const int nd = D.dq != 0 ? D.nd : 0;
+    const int n = ne + nh + nd;
+    double acc = 0.0;
+    for (int j = threadIdx.x; j < n; j += blockDim.x) {
+        int s;
+        double q;
+        if (j < ne) { s = D.e_site[j]; q = -1.0; }
+        else if (j < ne + nh) { s = D.h_site[j - ne]; q = 1.0; }
+        else { s = D.defects[j - ne - nh]; q = (double)D.dq; }
+        int xj, yj, zj;
+        xyz(D, s, xj, yj, zj);
+        const int dy = yi - yj, dz = zi - zj;
+        for (int term = 0; term < 3; ++term) {
+            if (!(D.terms & (1u << term))) continue;
+            const int dx = term == 0 ? xi - xj : (term == 1 ? xi + xj + 1 : 2 * D.X - 1 - xi - xj);
+            const int r2 = dx * dx + dy * dy + dz * dz;
+            if (r2 > 0 && r2 < D.cutoff2) {
+                const double r = sqrt((double)r2);
+                const double w = D.gauss ? erf(D.erffactor * r) / r : 1.0 / r;
+                acc += term == 0 ? q * w : -q * w;
+            }
+        }
+    }
+    red[threadIdx.x] = acc;
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if ((int)threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+        __syncthreads();
+    }
+    const double v = red[0];
+    __syncthreads();
+    return D.prefactor * v;
+}
+
+__global__ void __launch_bounds__(kGuardThreads) k_guard(Dev D) {
+    __shared__ double red[kGuardThreads];
+    const int ne = D.cnt[I_NE0], nh = D.cnt[I_NH0];
+    const int nflag = D.cnt[I_NFLAG];
+    const uint32_t step = (uint32_t)D.cnt[I_STEP];
+    for (int q_i = blockIdx.x; q_i < nflag; q_i += gridDim.x) {
+        const int i = D.flagged[q_i];
+        const bool e = i < ne;
+        const int k = e ? i : i - ne;
+        const int site = e ? D.e_site[k] : D.h_site[k];
+        const int f = e ? D.e_f[k] : D.h_f[k];
+        const double q = e ? -1.0 : 1.0;
+        const double v1 = fp64_potential(D, ne, nh, site, red);
+        const double v2 = fp64_potential(D, ne, nh, f, red);
+        if (threadIdx.x == 0) {
+            const double p1 = v1 + binding(D, e, site);
+            const double p2 = v2 - D.sI100 * q + binding(D, e, f);
+            const double de = q * (p2 - p1);
+            double pd = (D.pot[f] - D.pot[site]) * q;
+            pd += de;
+            const Philox4 r = draw(D, step, (uint32_t)k, e ? RNG_DECIDE_E : RNG_DECIDE_H);
+            const double u = unit_double(r.w[0], r.w[1]);
+            const bool acc = metropolis(pd, D.beta, coupling_of(D, site, f), u);
+            D.outcome[i] = acc ? O_MET_ACCEPT : O_MET_REJECT;
+            D.accept[i] = acc;
+            D.de[i] = de;
+            atomicAdd(&D.ctr[C_GUARD], 1ull);
+        }
+    }
+}
+
+// completeTick, part 1: contested empty sites go to the lowest list index.
+__global__ void k_claim(Dev D) {
+    const int ne = D.cnt[I_NE0], nh = D.cnt[I_NH0];
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= ne + nh || !D.accept[i]) return;
+    const bool e = i < ne;
+    const int k = e ? i : i - ne;
+    const int f = e ? D.e_f[k] : D.h_f[k];
+    if (f < D.V) atomicMin(&(e ? D.claim_e : D.claim_h)[f], k);
+}
+
+// completeTick, part 2: winners move, drains remove (site marked -1).
+__global__ void k_move(Dev D) {
+    const int ne = D.cnt[I_NE0], nh = D.cnt[I_NH0];
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    unsigned long long moved = 0, props = 0;
+    if (i < ne + nh) {
+        props = 1;
+        if (D.accept[i]) {
+            const bool e = i < ne;
+            const int k = e ? i : i - ne;
+            int32_t* sites = e ? D.e_site : D.h_site;
+            uint8_t* own = e ? D.et : D.ht;
+            const int s = sites[k];
+            const int f = (e ? D.e_f : D.h_f)[k];
+            if (f >= D.V) {
+                own[s] = T_EMPTY;
+                sites[k] = -1;
+                D.cnt[I_REMOVED] = 1;
+                moved = 1;
+            } else if ((e ? D.claim_e : D.claim_h)[f] == k) {
+                own[s] = T_EMPTY;
+                own[f] = e ? T_ELECTRON : T_HOLE;
+                sites[k] = f;
+                moved = 1;
+            }
+        }
+    }
+    // warp-aggregated counters
+    for (int o = 16; o > 0; o >>= 1) {
+        moved += __shfl_down_sync(0xffffffffu, moved, o);
+        props += __shfl_down_sync(0xffffffffu, props, o);
+    }
+    if ((threadIdx.x & 31) == 0 && props) {
+        atomicAdd(&D.ctr[C_PROPOSALS], props);
+        if (moved) atomicAdd(&D.ctr[C_ACCEPTED], moved);
+    }
+}
+
+__global__ void k_unclaim(Dev D) {
+    const int ne = D.cnt[I_NE0], nh = D.cnt[I_NH0];
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= ne + nh || !D.accept[i]) return;
+    const bool e = i < ne;
+    const int k = e ? i : i - ne;
+    const int f = e ? D.e_f[k] : D.h_f[k];
+    if (f < D.V) (e ? D.claim_e : D.claim_h)[f] = INT_MAX;
+}
+
+// Stable removal of drained carriers (Simulation::nextTick removeAt), then the
+// electrode sources (simulation.cpp:246-249) and currentStep += 1.  One block.
+constexpr int kCompactThreads = 1024;
+
+__device__ int compact(int32_t* a, int n, int* warp_sums) {
+    int base = 0;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int t0 = 0; t0 < n; t0 += blockDim.x) {
+        const int i = t0 + threadIdx.x;
+        const int v = i < n ? a[i] : -1;
+        const bool keep = v >= 0;
+        const unsigned m = __ballot_sync(0xffffffffu, keep);
+        if (lane == 0) warp_sums[warp] = __popc(m);
+        __syncthreads();
+        int before = 0, total = 0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+            if (w < warp) before += warp_sums[w];
+            total += warp_sums[w];
+        }
+        before += __popc(m & ((1u << lane) - 1u));
+        __syncthreads();
+        if (keep) a[base + before] = v;
+        base += total;
+        __syncthreads();
+    }
+    return base;
+}
+
+__global__ void __launch_bounds__(kCompactThreads) k_compact_inject(Dev D) {
+    __shared__ int warp_sums[32];
+    int ne = D.cnt[I_NE0], nh = D.cnt[I_NH0];
+    if (D.cnt[I_REMOVED]) {
+        ne = compact(D.e_site, ne, warp_sums);
+        nh = compact(D.h_site, nh, warp_sums);
+    }
+    if (threadIdx.x != 0) return;
+    const uint32_t step = (uint32_t)D.cnt[I_STEP];
+    for (int s = 0; s < 4; ++s) {
+        const bool e = s < 2, left = (s % 2) == 0;
+        D.ctr[2 * s] += 1;  // attempts (sourceagent.cpp:94)
+        const Philox4 r = draw(D, step, 0u, RNG_SOURCE + (uint32_t)s);
+        const int idx = (int)uint_below(r.w[0], (uint32_t)(D.Y * D.Z));
+        const int site = D.X * idx + (left ? 0 : D.X - 1);
+        uint8_t* own = e ? D.et : D.ht;
+        const int count = e ? ne : nh;
+        const int cap = e ? D.cap_e : D.cap_h;
+        if (!(count < cap && D.rate_src[s] > 0 && own[site] == T_EMPTY)) continue;
+        const double u = unit_double(r.w[1], r.w[2]);
+        if (D.rate_src[s] > u) {
+            D.ctr[2 * s + 1] += 1;
+            own[site] = e ? T_ELECTRON : T_HOLE;
+            if (e) D.e_site[ne++] = site;
+            else D.h_site[nh++] = site;
+        }
+    }
+    D.cnt[I_NE] = ne;
+    D.cnt[I_NH] = nh;
+    D.cnt[I_STEP] = (int32_t)(step + 1);
+}
+
+// ---- host side -------------------------------------------------------------------
+
+struct Stream {
+    uint32_t seed, replica, purpose;
+    uint32_t next = 0;
+    Philox4 draw() { return philox4x32_10(next++, 0u, purpose, 0u, seed, replica); }
+    uint32_t below(uint32_t n) { return uint_below(draw().w[0], n); }
+    // Box-Muller (the reference draws boost::normal_distribution, rand.cpp:61-66)
+    double normal(double mean, double sigma) {
+        const Philox4 r = draw();
+        const double u1 = (unit_double(r.w[0], r.w[1]) * 9007199254740991.0 + 1.0) / 9007199254740992.0;
+        const double u2 = unit_double(r.w[2], r.w[3]);
+        return mean + sigma * std::sqrt(-2.0 * std::log(u1)) * std::cos(2.0 * M_PI * u2);
+    }
+};
+
+void host_neighbors1(int X, int Y, int Z, int site, std::vector<int>& nb) {
+    nb.clear();
+    const int XY = X * Y;
+    const int z = site / XY, y = site / X - z * Y, x = site % X;
+    auto S = [&](int a, int b, int c) { nb.push_back(X * (b + c * Y) + a); };
+    if (x > 0) S(x - 1, y, z);
+    if (x < X - 1) S(x + 1, y, z);
+    if (y > 0) S(x, y - 1, z);
+    if (y < Y - 1) S(x, y + 1, z);
+    if (z > 0) S(x, y, z - 1);
+    if (z < Z - 1) S(x, y, z + 1);
+    const int V = X * Y * Z;
+    if (x == 0) nb.push_back(V + E_DRAIN_L);  // electron grid drains (cubicgrid.cpp:447-468)
+    if (x == X - 1) nb.push_back(V + E_DRAIN_R);
+}
+
+}  // namespace
+
+struct lgm_kmc {
+    lgm_params p{};
+    int device = 0;
+    uint32_t replica = 0;
+    int V = 0, max_e = 0, max_h = 0;
+    std::vector<double> pot;
+    std::vector<int32_t> defects, traps, e0, h0;
+    std::vector<double> trap_pots;
+    Dev D{};
+    cudaStream_t stream = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    std::vector<void*> allocs;
+    float* gtab = nullptr;
+    int gtab_k = 0;
+    int pair_blocks = 0, pair_tiles = 0;
+    std::string err;
+};
+
+namespace {
+
+thread_local std::string g_kmc_create_error;
+
+lgm_status kfail(lgm_kmc* k, lgm_status s, const std::string& m) {
+    if (k) k->err = m;
+    return s;
+}
+
+#define KCUDA(k, call)                                                                   \
+    do {                                                                                 \
+        cudaError_t e_ = (call);                                                         \
+        if (e_ != cudaSuccess) return kfail((k), LGM_ERR_CUDA, std::string(#call ": ") + \
+                                                               cudaGetErrorString(e_));  \
+    } while (0)
+
+template <class T>
+lgm_status dalloc(lgm_kmc* k, T** p, size_t n) {
+    KCUDA(k, cudaMalloc(reinterpret_cast<void**>(p), std::max<size_t>(n, 1) * sizeof(T)));
+    k->allocs.push_back(*p);
+    return LGM_OK;
+}
+
+// World::initialize order (world.cpp:625-643) on a Philox stream.
+lgm_status build_world(lgm_kmc* k) {
+    const lgm_params& p = k->p;
+    const int X = p.grid_x, Y = p.grid_y, Z = p.grid_z, V = X * Y * Z;
+    k->V = V;
+    const uint32_t seed = (uint32_t)(p.random_seed & 0xffffffffu);
+    k->max_e = (int)(p.electron_percentage * (double)V);
+    k->max_h = (int)(p.hole_percentage * (double)V);
+    const int max_d = (int)(p.defect_percentage * (double)V);
+    const int max_t = (int)(p.trap_percentage * (double)V);
+    std::vector<uint8_t> is_def(V, 0), is_trap(V, 0);
+    // placeDefects (world.cpp:659-757)
+    {
+        Stream r{seed, k->replica, RNG_SETUP + 0};
+        long tries = 0;
+        while ((int)k->defects.size() < max_d) {
+            if (++tries > 10L * V) return kfail(k, LGM_ERR_INVALID_ARGUMENT, "can not seed defects");
+            const int s = (int)r.below((uint32_t)V);
+            if (!is_def[s]) { is_def[s] = 1; k->defects.push_back(s); }
+        }
+    }
+    // setPotentialTraps (potential.cpp:74-244): seeds, then growth onto neighbours
+    {
+        Stream r{seed, k->replica, RNG_SETUP + 1};
+        int seeds = (int)(max_t * p.seed_percentage);
+        int grown = max_t - seeds;
+        if (max_t <= 0) { seeds = 0; grown = 0; }
+        if (seeds == 0 && grown > 0) { seeds = grown; grown = 0; }
+        long tries = 0;
+        while ((int)k->traps.size() < seeds) {
+            if (++tries > 100L * V + 1000) return kfail(k, LGM_ERR_INVALID_ARGUMENT, "can not seed traps");
+            const int s = (int)r.below((uint32_t)V);
+            if (!is_trap[s]) { is_trap[s] = 1; k->traps.push_back(s); }
+        }
+        std::vector<int> nb;
+        int progress = 0;
+        while (progress < grown) {
+            if (++tries > 100L * V + 1000) return kfail(k, LGM_ERR_INVALID_ARGUMENT, "can not grow traps");
+            const int seed_site = k->traps[r.below((uint32_t)k->traps.size())];
+            host_neighbors1(X, Y, Z, seed_site, nb);
+            const int s = nb[r.below((uint32_t)nb.size())];
+            if (s < V && !is_trap[s]) { is_trap[s] = 1; k->traps.push_back(s); ++progress; }
+        }
+        k->trap_pots.assign(k->traps.size(), p.trap_potential);
+        if (std::fabs(p.gaussian_stdev) > 0)
+            for (double& v : k->trap_pots) v += r.normal(0.0, p.gaussian_stdev);
+    }
+    // setPotentialZero / Linear / Gate (potential.cpp:17-72), traps, disorder
+    k->pot.assign(V, 0.0);
+    const double m = (p.voltage_right - p.voltage_left) / (double)X, b = p.voltage_left;
+    for (int i = 0; i < X; ++i)
+        for (int j = 0; j < Y; ++j)
+            for (int z = 0; z < Z; ++z) k->pot[X * (j + z * Y) + i] += m * (i + 0.5) + b;
+    if (!(Z == 1 || p.slope_z == 0))
+        for (int i = 0; i < X; ++i)
+            for (int j = 0; j < Y; ++j)
+                for (int z = 0; z < Z; ++z) k->pot[X * (j + z * Y) + i] += p.slope_z * (z + 0.5);
+    for (size_t i = 0; i < k->traps.size(); ++i) k->pot[k->traps[i]] += k->trap_pots[i];
+    if (p.site_disorder > 0) {
+        Stream r{seed, k->replica, RNG_SETUP + 2};
+        for (int s = 0; s < V; ++s) k->pot[s] += r.normal(0.0, p.site_disorder);
+    }
+    // placeElectrons / placeHoles (world.cpp:759-959): tryToSeed at uniform sites
+    auto seed_carriers = [&](int max, uint32_t purpose, std::vector<int32_t>& out) -> bool {
+        Stream r{seed, k->replica, purpose};
+        std::vector<uint8_t> occ(V, 0);
+        long tries = 0;
+        for (int i = 0; i < max * p.seed_charges;) {
+            if (++tries > 10L * V) return false;
+            const int s = (int)r.below((uint32_t)V);
+            if (!occ[s] && !is_def[s] && (int)out.size() < max) {
+                occ[s] = 1;
+                out.push_back(s);
+                ++i;
+            }
+        }
+        return true;
+    };
+    if (!seed_carriers(k->max_e, RNG_SETUP + 3, k->e0))
+        return kfail(k, LGM_ERR_INVALID_ARGUMENT, "can not seed electrons");
+    if (!seed_carriers(k->max_h, RNG_SETUP + 4, k->h0))
+        return kfail(k, LGM_ERR_INVALID_ARGUMENT, "can not seed holes");
+    return LGM_OK;
+}
+
+lgm_status upload_carriers(lgm_kmc* k, const int32_t* e, int ne, const int32_t* h, int nh) {
+    Dev& D = k->D;
+    std::vector<uint8_t> et(k->V + kSpecial, T_EMPTY), ht(k->V + kSpecial, T_EMPTY);
+    for (int s : k->defects) et[s] = ht[s] = T_DEFECT;
+    for (int i = 0; i < ne; ++i) {
+        if (e[i] < 0 || e[i] >= k->V || et[e[i]] != T_EMPTY)
+            return kfail(k, LGM_ERR_OUT_OF_RANGE, "electron site invalid or occupied");
+        et[e[i]] = T_ELECTRON;
+    }
+    for (int i = 0; i < nh; ++i) {
+        if (h[i] < 0 || h[i] >= k->V || ht[h[i]] != T_EMPTY)
+            return kfail(k, LGM_ERR_OUT_OF_RANGE, "hole site invalid or occupied");
+        ht[h[i]] = T_HOLE;
+    }
+    const int V = k->V;
+    et[V + 0] = et[V + 1] = et[V + 2] = T_SOURCE;
+    et[V + 3] = et[V + 4] = et[V + 5] = T_DRAIN;
+    ht[V + 0] = ht[V + 1] = T_SOURCE;
+    ht[V + 2] = ht[V + 3] = T_DRAIN;
+    KCUDA(k, cudaMemcpy(D.et, et.data(), et.size(), cudaMemcpyHostToDevice));
+    KCUDA(k, cudaMemcpy(D.ht, ht.data(), ht.size(), cudaMemcpyHostToDevice));
+    if (ne) KCUDA(k, cudaMemcpy(D.e_site, e, sizeof(int32_t) * ne, cudaMemcpyHostToDevice));
+    if (nh) KCUDA(k, cudaMemcpy(D.h_site, h, sizeof(int32_t) * nh, cudaMemcpyHostToDevice));
+    int32_t c[2] = {ne, nh};
+    KCUDA(k, cudaMemcpy(D.cnt + I_NE, c, sizeof c, cudaMemcpyHostToDevice));
+    return LGM_OK;
+}
+
+using KPairFn = void (*)(PairArgs);
+
+KPairFn kmc_pair(int gauss) {
+    return gauss ? &pair_kernel<1, 0, kNT, kRP, kSUB, true> : &pair_kernel<0, 0, kNT, kRP, kSUB, true>;
+}
+
+// One step: kernels in order on k->stream (captured into the graph).
+lgm_status enqueue_step(lgm_kmc* k) {
+    const Dev& D = k->D;
+    cudaStream_t st = k->stream;
+    const int nc = std::max(1, D.cap_e + D.cap_h);
+    const int blk = 256;
+    k_choose<<<(nc + blk - 1) / blk, blk, 0, st>>>(D);
+    if (D.coulomb) {
+        const int npack = std::max(D.src_cap, D.tpad_cap);
+        k_pack<<<(npack + blk - 1) / blk, blk, 0, st>>>(D);
+        PairArgs A;
+        A.geo = D.geo; A.qq = D.qq; A.splits = D.splits; A.tgt = D.tgt; A.part = D.part;
+        A.part_norm = D.part_norm;
+        A.c2 = (float)D.cutoff2; A.tab = k->gtab; A.tab_k = D.gauss ? k->gtab_k : 0;
+        A.err = D.err; A.dyn = D.cnt + I_NCHUNK;  // dyn[0] = n_chunks, dyn[1] = t_phys
+        kmc_pair(D.gauss)<<<dim3(k->pair_tiles, D.splits), kNT, pair_smem_bytes(A.tab_k), st>>>(A);
+        k_finalize<<<(2 * nc + blk - 1) / blk, blk, 0, st>>>(D);
+    }
+    k_decide<<<(nc + blk - 1) / blk, blk, 0, st>>>(D);
+    if (D.coulomb) k_guard<<<2 * 148, kGuardThreads, 0, st>>>(D);
+    k_claim<<<(nc + blk - 1) / blk, blk, 0, st>>>(D);
+    k_move<<<(nc + blk - 1) / blk, blk, 0, st>>>(D);
+    k_unclaim<<<(nc + blk - 1) / blk, blk, 0, st>>>(D);
+    k_compact_inject<<<1, kCompactThreads, 0, st>>>(D);
+    KCUDA(k, cudaGetLastError());
+    return LGM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+lgm_status lgm_kmc_create(const lgm_params* pin, int32_t device, uint32_t replica, lgm_kmc** out) {
+    if (!pin || !out) return LGM_ERR_INVALID_ARGUMENT;
+    *out = nullptr;
+    lgm_kmc* k = new (std::nothrow) lgm_kmc();
+    if (!k) return LGM_ERR_INVALID_ARGUMENT;
+    k->p = *pin;
+    k->replica = replica;
+    char msg[256] = {0};
+    lgm_status s = lgm_params_check(&k->p, msg, sizeof msg);
+    auto bail = [&](lgm_status st, const std::string& m) {
+        g_kmc_create_error = m;
+        lgm_kmc_destroy(k);
+        return st;
+    };
+    g_kmc_create_error.clear();
+    if (s != LGM_OK) return bail(s, msg);
+    const lgm_params& p = k->p;
+    if (std::string(p.simulation_type) != "transistor" || p.source_metropolis)
+        return bail(LGM_ERR_UNSUPPORTED, "only the transistor set-up without source.metropolis");
+    if (p.hopping_range < 1) return bail(LGM_ERR_UNSUPPORTED, "hopping.range 0 has no moves");
+    const long long L = std::max<long long>({2LL * p.grid_x, p.grid_y, p.grid_z + 1});
+    if (6 * L * L >= (1LL << 22)) return bail(LGM_ERR_UNSUPPORTED, "lattice too large");
+    if ((s = build_world(k)) != LGM_OK) return bail(s, k->err);
+    k->device = device < 0 ? 0 : device;
+    if (cudaSetDevice(k->device) != cudaSuccess) return bail(LGM_ERR_NO_DEVICE, "no device");
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, k->device) != cudaSuccess || prop.major != 10)
+        return bail(LGM_ERR_NO_DEVICE, "device is not sm_100 (B200)");
+    if (cudaStreamCreateWithFlags(&k->stream, cudaStreamNonBlocking) != cudaSuccess)
+        return bail(LGM_ERR_CUDA, "stream");
+
+    Dev& D = k->D;
+    D.X = p.grid_x; D.Y = p.grid_y; D.Z = p.grid_z; D.XY = D.X * D.Y; D.V = k->V;
+    D.hr = p.hopping_range;
+    D.cap_e = k->max_e; D.cap_h = k->max_h;
+    D.nd = (int)k->defects.size(); D.dq = p.defects_charge;
+    D.seed = (uint32_t)(p.random_seed & 0xffffffffu); D.replica = replica;
+    D.beta = p.inverse_kt; D.exciton_binding = p.exciton_binding;
+    D.prefactor = p.electrostatic_prefactor;
+    D.erffactor = p.coulomb_gaussian_sigma > 0 ? 1.0 / (std::sqrt(2.0) * p.coulomb_gaussian_sigma) : 0.0;
+    D.gauss = p.coulomb_gaussian_sigma > 0;
+    // sI[1][0][0] = prefactor * iR * eR at r = 1 (potential.cpp:311-323)
+    D.sI100 = p.electrostatic_prefactor * (D.gauss ? std::erf(D.erffactor * 1.0) : 1.0);
+    // coupling (potential.cpp:326-349)
+    {
+        const int h = D.hr + 1;
+        for (int dx = 0; dx < h; ++dx)
+            for (int dy = 0; dy < h; ++dy)
+                for (int dz = 0; dz < h; ++dz) {
+                    const double r = std::sqrt((double)(dx * dx + dy * dy + dz * dz));
+                    D.coupling[(dx * h + dy) * h + dz] =
+                        (1.0 / 3.0) * std::pow(3.0, r - 1) * std::pow(1.0 / 27.0, r - 1);
+                }
+        D.coupling[0] = 0.0;
+    }
+    // World::createSources/createDrains rates, transistor (world.cpp:990-1000, 1116-1124)
+    auto smart = [](double r, double dflt) { return r < 0 ? dflt : r; };
+    D.rate_src[0] = smart(p.e_source_l_rate, p.source_rate);
+    D.rate_src[1] = smart(p.e_source_r_rate, 0.0);
+    D.rate_src[2] = smart(p.h_source_l_rate, 0.0);
+    D.rate_src[3] = smart(p.h_source_r_rate, 0.0);
+    D.rate_drain[0] = smart(p.e_drain_l_rate, 0.0);
+    D.rate_drain[1] = smart(p.e_drain_r_rate, p.drain_rate);
+    D.rate_drain[2] = smart(p.h_drain_l_rate, 0.0);
+    D.rate_drain[3] = smart(p.h_drain_r_rate, 0.0);
+    // createSources / createDrains sanity checks (world.cpp:1032-1068, 1158-1186)
+    if (D.rate_src[0] == 0 && D.rate_src[1] == 0 && D.rate_src[2] == 0 && D.rate_src[3] == 0)
+        return bail(LGM_ERR_INVALID_ARGUMENT, "langmuir: all sources have zero rate");
+    if (k->max_e == 0 && (D.rate_src[0] > 0 || D.rate_src[1] > 0))
+        return bail(LGM_ERR_INVALID_ARGUMENT,
+                    "langmuir: an electron source rate > 0, yet maxElectronAgents() == 0");
+    if (k->max_h == 0 && (D.rate_src[2] > 0 || D.rate_src[3] > 0))
+        return bail(LGM_ERR_INVALID_ARGUMENT,
+                    "langmuir: a hole source rate > 0, yet maxHoleAgents() == 0");
+    if (D.rate_drain[0] == 0 && D.rate_drain[1] == 0 && D.rate_drain[2] == 0 && D.rate_drain[3] == 0)
+        return bail(LGM_ERR_INVALID_ARGUMENT, "langmuir: all drains have zero rate");
+    if (k->max_e > 0 && D.rate_drain[0] <= 0 && D.rate_drain[1] <= 0)
+        return bail(LGM_ERR_INVALID_ARGUMENT,
+                    "langmuir: all electron drain rates are zero, yet maxElectronAgents() > 0");
+    if (k->max_h > 0 && D.rate_drain[2] <= 0 && D.rate_drain[3] <= 0)
+        return bail(LGM_ERR_INVALID_ARGUMENT,
+                    "langmuir: all hole drain rates are zero, yet maxHoleAgents() > 0");
+    D.coulomb = p.coulomb_carriers;
+    D.terms = LGM_TERM_DIRECT | ((p.image_charges & 1) ? LGM_TERM_IMAGE_LEFT : 0u) |
+              ((p.image_charges & 2) ? LGM_TERM_IMAGE_RIGHT : 0u);
+    D.nterms = 1 + ((p.image_charges & 1) ? 1 : 0) + ((p.image_charges & 2) ? 1 : 0);
+    D.cutoff2 = p.electrostatic_cutoff * p.electrostatic_cutoff;
+
+    const int ncap = std::max(1, D.cap_e + D.cap_h);
+    const int nd_src = D.dq != 0 ? D.nd : 0;
+    D.src_cap = ((D.cap_e + CH - 1) / CH + (D.cap_h + CH - 1) / CH + (nd_src + CH - 1) / CH) * CH;
+    D.src_cap = std::max(D.src_cap, CH);
+    D.tpad_cap = (2 * ncap + 63) / 64 * 64;
+    const int tphys_cap = D.nterms * D.tpad_cap;
+    k->pair_tiles = (tphys_cap + kTile - 1) / kTile;
+    int bps = 1;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, kmc_pair(D.gauss), kNT, pair_smem_bytes(64));
+    D.splits = std::max(1, std::min({64, prop.multiProcessorCount * std::max(1, bps) / k->pair_tiles,
+                                     D.src_cap / CH}));
+    lgm_status st;
+#define DA(ptr, n) if ((st = dalloc(k, &(ptr), (size_t)(n))) != LGM_OK) return bail(st, k->err)
+    DA(D.pot, k->V);
+    DA(D.et, k->V + kSpecial);
+    DA(D.ht, k->V + kSpecial);
+    DA(D.e_site, std::max(D.cap_e, 1)); DA(D.h_site, std::max(D.cap_h, 1));
+    DA(D.e_f, std::max(D.cap_e, 1)); DA(D.h_f, std::max(D.cap_h, 1));
+    DA(D.defects, std::max(D.nd, 1));
+    DA(D.claim_e, k->V); DA(D.claim_h, k->V);
+    DA(D.outcome, ncap); DA(D.de, ncap); DA(D.accept, ncap); DA(D.flagged, ncap);
+    DA(D.cnt, I_NUM); DA(D.ctr, C_NUM);
+    DA(D.geo, 2 * D.src_cap); DA(D.qq, D.src_cap);
+    DA(D.tgt, tphys_cap + kTile);
+    DA(D.part, (size_t)D.splits * tphys_cap); DA(D.part_norm, (size_t)D.splits * tphys_cap);
+    DA(D.Vt, 2 * ncap); DA(D.Nt, 2 * ncap);
+    DA(D.err, 1);
+#undef DA
+    if (D.gauss) {
+        // erf(f sqrt(k))/sqrt(k) where it differs from 1/sqrt(k) in FP32; NaN past it
+        const int c2 = D.cutoff2;
+        int kmax = 1;
+        while (kmax < c2 && std::erfc(D.erffactor * std::sqrt((double)kmax)) >= 0x1p-30) ++kmax;
+        std::vector<float> gt(kmax + 1, 0.f);
+        for (int i = 1; i < kmax; ++i) {
+            const double r = std::sqrt((double)i);
+            gt[i] = (float)(std::erf(D.erffactor * r) / r);
+        }
+        gt[kmax] = std::nanf("");
+        k->gtab_k = kmax;
+        if ((st = dalloc(k, &k->gtab, gt.size())) != LGM_OK) return bail(st, k->err);
+        if (cudaMemcpy(k->gtab, gt.data(), gt.size() * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess)
+            return bail(LGM_ERR_CUDA, "table upload");
+        cudaFuncSetAttribute(kmc_pair(1), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)pair_smem_bytes(kmax));
+    }
+    cudaMemcpy(D.pot, k->pot.data(), sizeof(double) * k->V, cudaMemcpyHostToDevice);
+    if (D.nd) cudaMemcpy(D.defects, k->defects.data(), sizeof(int32_t) * D.nd, cudaMemcpyHostToDevice);
+    std::vector<int32_t> claims(k->V, INT_MAX);
+    cudaMemcpy(D.claim_e, claims.data(), sizeof(int32_t) * k->V, cudaMemcpyHostToDevice);
+    cudaMemcpy(D.claim_h, claims.data(), sizeof(int32_t) * k->V, cudaMemcpyHostToDevice);
+    cudaMemset(D.cnt, 0, sizeof(int32_t) * I_NUM);
+    cudaMemset(D.ctr, 0, sizeof(unsigned long long) * C_NUM);
+    cudaMemset(D.err, 0, sizeof(unsigned));
+    int32_t step0 = (int32_t)p.current_step;
+    cudaMemcpy(D.cnt + I_STEP, &step0, sizeof step0, cudaMemcpyHostToDevice);
+    if ((st = upload_carriers(k, k->e0.data(), (int)k->e0.size(), k->h0.data(),
+                              (int)k->h0.size())) != LGM_OK)
+        return bail(st, k->err);
+    if (cudaDeviceSynchronize() != cudaSuccess) return bail(LGM_ERR_CUDA, "set-up");
+    *out = k;
+    return LGM_OK;
+}
+
+lgm_status lgm_kmc_destroy(lgm_kmc* k) {
+    if (!k) return LGM_OK;
+    cudaSetDevice(k->device);
+    if (k->stream) cudaStreamSynchronize(k->stream);
+    if (k->exec) cudaGraphExecDestroy(k->exec);
+    if (k->graph) cudaGraphDestroy(k->graph);
+    for (void* p : k->allocs) cudaFree(p);
+    if (k->stream) cudaStreamDestroy(k->stream);
+    delete k;
+    return LGM_OK;
+}
+
+const char* lgm_kmc_last_error(const lgm_kmc* k) {
+    return k ? k->err.c_str() : g_kmc_create_error.c_str();
+}
+
+lgm_status lgm_kmc_run(lgm_kmc* k, int32_t steps) {
+    if (!k || steps < 0) return LGM_ERR_INVALID_ARGUMENT;
+    KCUDA(k, cudaSetDevice(k->device));
+    if (!k->exec && steps > 0) {
+        KCUDA(k, cudaStreamBeginCapture(k->stream, cudaStreamCaptureModeThreadLocal));
+        lgm_status s = enqueue_step(k);
+        cudaGraph_t g = nullptr;
+        cudaError_t e = cudaStreamEndCapture(k->stream, &g);
+        if (s != LGM_OK) { if (g) cudaGraphDestroy(g); return s; }
+        if (e != cudaSuccess) return kfail(k, LGM_ERR_CUDA, "graph capture failed");
+        k->graph = g;
+        KCUDA(k, cudaGraphInstantiate(&k->exec, g, 0));
+    }
+    for (int i = 0; i < steps; ++i) KCUDA(k, cudaGraphLaunch(k->exec, k->stream));
+    KCUDA(k, cudaStreamSynchronize(k->stream));
+    unsigned e = 0;
+    KCUDA(k, cudaMemcpy(&e, k->D.err, sizeof e, cudaMemcpyDeviceToHost));
+    if (e) return kfail(k, LGM_ERR_TIMEOUT, "device reported an error during the step");
+    return LGM_OK;
+}
+
+lgm_status lgm_kmc_stats_get(lgm_kmc* k, lgm_kmc_stats* s) {
+    if (!k || !s) return LGM_ERR_INVALID_ARGUMENT;
+    KCUDA(k, cudaSetDevice(k->device));
+    KCUDA(k, cudaStreamSynchronize(k->stream));
+    int32_t c[I_NUM];
+    unsigned long long ctr[C_NUM];
+    KCUDA(k, cudaMemcpy(c, k->D.cnt, sizeof c, cudaMemcpyDeviceToHost));
+    KCUDA(k, cudaMemcpy(ctr, k->D.ctr, sizeof ctr, cudaMemcpyDeviceToHost));
+    std::memset(s, 0, sizeof *s);
+    s->step = (uint32_t)c[I_STEP];
+    s->electrons = c[I_NE];
+    s->holes = c[I_NH];
+    s->max_electrons = k->max_e;
+    s->max_holes = k->max_h;
+    s->defects = (int32_t)k->defects.size();
+    s->traps = (int32_t)k->traps.size();
+    s->proposals = ctr[C_PROPOSALS];
+    s->accepted = ctr[C_ACCEPTED];
+    s->guard_evaluations = ctr[C_GUARD];
+    for (int i = 0; i < 16; ++i) s->counters[i] = ctr[i];
+    return LGM_OK;
+}
+
+lgm_status lgm_kmc_get_carriers(lgm_kmc* k, int32_t* e, int32_t e_cap, int32_t* h, int32_t h_cap) {
+    if (!k) return LGM_ERR_INVALID_ARGUMENT;
+    KCUDA(k, cudaStreamSynchronize(k->stream));
+    int32_t c[2];
+    KCUDA(k, cudaMemcpy(c, k->D.cnt + I_NE, sizeof c, cudaMemcpyDeviceToHost));
+    if (c[0] > e_cap || c[1] > h_cap) return kfail(k, LGM_ERR_CAPACITY, "buffers too small");
+    if (c[0]) KCUDA(k, cudaMemcpy(e, k->D.e_site, sizeof(int32_t) * c[0], cudaMemcpyDeviceToHost));
+    if (c[1]) KCUDA(k, cudaMemcpy(h, k->D.h_site, sizeof(int32_t) * c[1], cudaMemcpyDeviceToHost));
+    return LGM_OK;
+}
+
+lgm_status lgm_kmc_set_carriers(lgm_kmc* k, const int32_t* e, int32_t ne, const int32_t* h,
+                                int32_t nh) {
+    if (!k || ne < 0 || nh < 0 || (ne && !e) || (nh && !h)) return LGM_ERR_INVALID_ARGUMENT;
+    if (ne > k->max_e || nh > k->max_h) return kfail(k, LGM_ERR_CAPACITY, "more carriers than the maxima");
+    KCUDA(k, cudaSetDevice(k->device));
+    KCUDA(k, cudaStreamSynchronize(k->stream));
+    return upload_carriers(k, e, ne, h, nh);
+}
+
+lgm_status lgm_kmc_get_world(lgm_kmc* k, double* pot, int32_t* defects, int32_t d_cap,
+                             int32_t* traps, double* trap_pots, int32_t t_cap) {
+    if (!k) return LGM_ERR_INVALID_ARGUMENT;
+    if (pot) std::memcpy(pot, k->pot.data(), sizeof(double) * k->V);
+    if (defects) {
+        if ((int)k->defects.size() > d_cap) return kfail(k, LGM_ERR_CAPACITY, "defect buffer too small");
+        std::memcpy(defects, k->defects.data(), sizeof(int32_t) * k->defects.size());
+    }
+    if (traps || trap_pots) {
+        if ((int)k->traps.size() > t_cap) return kfail(k, LGM_ERR_CAPACITY, "trap buffer too small");
+        if (traps) std::memcpy(traps, k->traps.data(), sizeof(int32_t) * k->traps.size());
+        if (trap_pots) std::memcpy(trap_pots, k->trap_pots.data(), sizeof(double) * k->traps.size());
+    }
+    return LGM_OK;
+}
+
+lgm_status lgm_kmc_last_outcomes(lgm_kmc* k, int32_t* outcome, double* de, int32_t cap) {
+    if (!k) return LGM_ERR_INVALID_ARGUMENT;
+    KCUDA(k, cudaStreamSynchronize(k->stream));
+    int32_t c[2];
+    KCUDA(k, cudaMemcpy(c, k->D.cnt + I_NE0, sizeof c, cudaMemcpyDeviceToHost));
+    const int n = c[0] + c[1];
+    if (n > cap) return kfail(k, LGM_ERR_CAPACITY, "buffer too small");
+    if (n && outcome) KCUDA(k, cudaMemcpy(outcome, k->D.outcome, sizeof(int32_t) * n, cudaMemcpyDeviceToHost));
+    if (n && de) KCUDA(k, cudaMemcpy(de, k->D.de, sizeof(double) * n, cudaMemcpyDeviceToHost));
+    return LGM_OK;
+}
+
+}  // extern "C"

@@ -33,17 +33,25 @@ namespace lgm {
 constexpr int CH = 128;   // sources per shared-memory stage
 
 struct PairArgs {
-    const float4* geo;      // [n_pad * 2]
-    const float2* qq;       // [n_pad]
-    int n_chunks;           // n_pad / CH
-    int splits;             // source splits (gridDim.y)
-    const float4* tgt;      // [t_phys]
-    int t_phys;             // physical targets (padded)
-    double* part;           // [splits][t_phys]
-    float c2;               // cutoff^2
-    const float* tab;       // gauss correction table or 1/sqrt(k) table
-    int tab_k;              // last valid table index (clamp)
-    unsigned* err;
+    const float4* geo = nullptr;      // [n_pad * 2]
+    const float2* qq = nullptr;       // [n_pad]
+    int n_chunks = 0;                 // n_pad / CH
+    int splits = 1;                   // source splits (gridDim.y)
+    const float4* tgt = nullptr;      // [t_phys]
+    int t_phys = 0;                   // physical targets (padded)
+    double* part = nullptr;           // [splits][t_phys]
+    float c2 = 0.f;                   // cutoff^2
+    const float* tab = nullptr;       // gauss correction table or 1/sqrt(k) table
+    int tab_k = 0;                    // last valid table index (clamp)
+    unsigned* err = nullptr;
+    // Optional: counts read on the device (dyn[0] = n_chunks, dyn[1] = t_phys)
+    // so one launch shape serves every step of a simulation.
+    const int* dyn = nullptr;
+    // NORM kernels: sum over FP32 runs of |run sum| per target.  When every
+    // run holds charges of one sign (charge classes padded to whole chunks)
+    // this is prefactor-free N = sum_j |q_j| w(r_j), the error scale of the
+    // target's potential.  Layout [splits][t_phys].
+    float* part_norm = nullptr;
 };
 
 // Kernel launched with dynamic shared memory pair_smem_bytes(tab_k).
@@ -57,9 +65,14 @@ inline size_t pair_smem_bytes(int tab_k) {
 // KIND 0 point, 1 gauss.  PATH 0 MUFU rsqrt, 1 shared-memory table of w(k)
 // for every integer r^2 = k (entries 0 and c^2 are 0).  NT threads, RP target
 // pairs per thread, SUB sources per FP32 run (SUB divides CH).
-template <int KIND, int PATH, int NT, int RP, int SUB>
+template <int KIND, int PATH, int NT, int RP, int SUB, bool NORM = false>
 __global__ void __launch_bounds__(NT) pair_kernel(PairArgs A) {
     static_assert(CH % SUB == 0, "SUB must divide CH");
+    if (A.dyn) {
+        A.n_chunks = A.dyn[0];
+        A.t_phys = A.dyn[1];
+    }
+    if ((int)blockIdx.x * (NT * 2 * RP) >= A.t_phys) return;  // tile beyond this launch's targets
     extern __shared__ __align__(128) unsigned char smem[];
     float4* s_geo = reinterpret_cast<float4*>(smem);                       // [2][CH*2]
     float2* s_qq = reinterpret_cast<float2*>(smem + 2 * CH * 2 * sizeof(float4));  // [2][CH]
@@ -108,8 +121,11 @@ __global__ void __launch_bounds__(NT) pair_kernel(PairArgs A) {
         tx[k] = f2(a.x, b.x); ty[k] = f2(a.y, b.y); tz[k] = f2(a.z, b.z); tt[k] = f2(a.w, b.w);
     }
     double acc64[2 * RP];
+    float nrm[NORM ? 2 * RP : 1];
 #pragma unroll
     for (int k = 0; k < 2 * RP; ++k) acc64[k] = 0.0;
+#pragma unroll
+    for (int k = 0; k < (NORM ? 2 * RP : 1); ++k) nrm[k] = 0.f;
     const unsigned ulim = __float_as_uint(A.c2 - 0.5f);
     const float2 half2 = f2(0.5f, 0.5f);
 
@@ -171,6 +187,10 @@ __global__ void __launch_bounds__(NT) pair_kernel(PairArgs A) {
             }
 #pragma unroll
             for (int k = 0; k < 2 * RP; ++k) acc64[k] += (double)acc[k];
+            if (NORM) {
+#pragma unroll
+                for (int k = 0; k < 2 * RP; ++k) nrm[NORM ? k : 0] += fabsf(acc[k]);
+            }
         }
         __syncthreads();  // every thread is done with stage st
         if (tid == 0 && i + 2 < nck) {
@@ -197,7 +217,10 @@ __global__ void __launch_bounds__(NT) pair_kernel(PairArgs A) {
 #pragma unroll
     for (int k = 0; k < 2 * RP; ++k) {
         const int p = base + tid + k * NT;
-        if (p < A.t_phys) out[p] = acc64[k];
+        if (p < A.t_phys) {
+            out[p] = acc64[k];
+            if (NORM) A.part_norm[(size_t)split * A.t_phys + p] = nrm[NORM ? k : 0];
+        }
     }
 }
 

@@ -1,0 +1,198 @@
+"""Input keys and the GPU kMC step (include/langmuir_b200_kmc.h) from Python.
+
+``Params`` mirrors ``lgm_params``: every key of the reference's KeyValueParser
+(keyvalueparser.cpp:15-105) as an attribute named with underscores
+(``grid.x`` -> ``grid_x``), defaults from SimulationParameters
+(parameters.h:285-378).  ``Params.parse(text)`` reads a Langmuir input file;
+``check()`` derives the prefactor and 1/kT and validates.
+
+``KMC`` is one replica stepped on the GPU.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _native as N
+
+_i32 = ctypes.c_int32
+_f64 = ctypes.c_double
+
+
+class Params(ctypes.Structure):
+    _fields_ = [
+        ("simulation_type", ctypes.c_char * 16), ("current_step", ctypes.c_uint32),
+        ("iterations_real", _i32), ("random_seed", ctypes.c_uint64),
+        ("grid_z", _i32), ("grid_y", _i32), ("grid_x", _i32), ("hopping_range", _i32),
+        ("output_is_on", _i32), ("iterations_print", _i32), ("output_precision", _i32),
+        ("output_width", _i32), ("output_stub", ctypes.c_char * 64),
+        ("output_ids_on_delete", _i32), ("output_ids_on_encounter", _i32),
+        ("output_coulomb", _i32), ("output_step_chk", _i32),
+        ("output_chk_trap_potential", _i32), ("output_potential", _i32),
+        ("output_xyz", _i32), ("output_xyz_e", _i32), ("output_xyz_h", _i32),
+        ("output_xyz_d", _i32), ("output_xyz_t", _i32), ("output_xyz_mode", _i32),
+        ("image_traps", _i32), ("image_defects", _i32), ("image_carriers", _i32),
+        ("electron_percentage", _f64), ("hole_percentage", _f64), ("seed_charges", _f64),
+        ("defect_percentage", _f64), ("trap_percentage", _f64), ("trap_potential", _f64),
+        ("gaussian_stdev", _f64), ("seed_percentage", _f64),
+        ("voltage_right", _f64), ("voltage_left", _f64), ("slope_z", _f64),
+        ("coulomb_carriers", _i32), ("coulomb_gaussian_sigma", _f64), ("defects_charge", _i32),
+        ("exciton_binding", _f64), ("temperature_kelvin", _f64),
+        ("source_rate", _f64), ("e_source_l_rate", _f64), ("e_source_r_rate", _f64),
+        ("h_source_l_rate", _f64), ("h_source_r_rate", _f64), ("generation_rate", _f64),
+        ("source_metropolis", _i32), ("source_coulomb", _i32), ("source_scale_area", _f64),
+        ("balance_charges", _i32),
+        ("drain_rate", _f64), ("e_drain_l_rate", _f64), ("e_drain_r_rate", _f64),
+        ("h_drain_l_rate", _f64), ("h_drain_r_rate", _f64),
+        ("recombination_rate", _f64), ("recombination_range", _i32),
+        ("use_opencl", _i32), ("work_x", _i32), ("work_y", _i32), ("work_z", _i32),
+        ("work_size", _i32), ("opencl_threshold", _i32), ("opencl_device_id", _i32),
+        ("max_threads", _i32),
+        ("boltzmann_constant", _f64), ("dielectric_constant", _f64),
+        ("elementary_charge", _f64), ("permittivity_space", _f64), ("grid_factor", _f64),
+        ("electrostatic_cutoff", _i32), ("electrostatic_prefactor", _f64), ("inverse_kt", _f64),
+        ("image_charges", _i32), ("site_disorder", _f64),
+    ]
+
+    @classmethod
+    def default(cls, **keys) -> "Params":
+        p = cls()
+        N.lib().lgm_params_default(ctypes.byref(p))
+        for k, v in keys.items():
+            p.set(k, v)
+        return p
+
+    def set(self, key: str, value):
+        name = key.replace(".", "_")
+        if not hasattr(self, name):
+            raise KeyError(key)
+        if isinstance(getattr(self, name), bytes):
+            value = value.encode() if isinstance(value, str) else value
+        setattr(self, name, value)
+
+    def parse(self, text: str) -> "Params":
+        err = ctypes.create_string_buffer(512)
+        st = N.lib().lgm_params_parse(text.encode(), ctypes.byref(self), err, len(err))
+        if st != N.OK:
+            raise N.LgmError(st, err.value.decode())
+        return self
+
+    @classmethod
+    def from_text(cls, text: str) -> "Params":
+        return cls.default().parse(text)
+
+    def check(self) -> "Params":
+        err = ctypes.create_string_buffer(512)
+        st = N.lib().lgm_params_check(ctypes.byref(self), err, len(err))
+        if st != N.OK:
+            raise N.LgmError(st, err.value.decode())
+        return self
+
+
+class Stats(ctypes.Structure):
+    _fields_ = [("step", ctypes.c_uint32), ("electrons", _i32), ("holes", _i32),
+                ("max_electrons", _i32), ("max_holes", _i32), ("defects", _i32),
+                ("traps", _i32), ("proposals", ctypes.c_uint64), ("accepted", ctypes.c_uint64),
+                ("guard_evaluations", ctypes.c_uint64), ("counters", ctypes.c_uint64 * 16)]
+
+
+_vp = ctypes.c_void_p
+_i32p = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+_f64p = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+
+N.SIGNATURES.update({
+    "lgm_params_default": (None, [ctypes.POINTER(Params)]),
+    "lgm_params_size": (_i32, []),
+    "lgm_params_parse": (_i32, [ctypes.c_char_p, ctypes.POINTER(Params), ctypes.c_char_p, _i32]),
+    "lgm_params_check": (_i32, [ctypes.POINTER(Params), ctypes.c_char_p, _i32]),
+    "lgm_kmc_create": (_i32, [ctypes.POINTER(Params), _i32, ctypes.c_uint32,
+                              ctypes.POINTER(_vp)]),
+    "lgm_kmc_destroy": (_i32, [_vp]),
+    "lgm_kmc_last_error": (ctypes.c_char_p, [_vp]),
+    "lgm_kmc_run": (_i32, [_vp, _i32]),
+    "lgm_kmc_stats_get": (_i32, [_vp, ctypes.POINTER(Stats)]),
+    "lgm_kmc_get_carriers": (_i32, [_vp, _i32p, _i32, _i32p, _i32]),
+    "lgm_kmc_set_carriers": (_i32, [_vp, _i32p, _i32, _i32p, _i32]),
+    "lgm_kmc_get_world": (_i32, [_vp, _vp, _vp, _i32, _vp, _vp, _i32]),
+    "lgm_kmc_last_outcomes": (_i32, [_vp, _vp, _vp, _i32]),
+})
+if N._lib is not None:  # bind the new symbols if the library was already loaded
+    for _name in ("lgm_params_default", "lgm_params_size", "lgm_params_parse",
+                  "lgm_params_check", "lgm_kmc_create", "lgm_kmc_destroy", "lgm_kmc_last_error",
+                  "lgm_kmc_run", "lgm_kmc_stats_get", "lgm_kmc_get_carriers",
+                  "lgm_kmc_set_carriers", "lgm_kmc_get_world", "lgm_kmc_last_outcomes"):
+        _fn = getattr(N._lib, _name)
+        _fn.restype, _fn.argtypes = N.SIGNATURES[_name]
+
+
+class KMC:
+    """One replica on the GPU: the world is built from ``params`` and the
+    (random.seed, replica) Philox stream."""
+
+    def __init__(self, params: Params, device: int = 0, replica: int = 0):
+        h = ctypes.c_void_p()
+        st = N.lib().lgm_kmc_create(ctypes.byref(params), int(device), int(replica),
+                                    ctypes.byref(h))
+        if st != N.OK:
+            raise N.LgmError(st, N.lib().lgm_kmc_last_error(None).decode())
+        self._h = h
+        self.params = params
+        self.volume = params.grid_x * params.grid_y * params.grid_z
+
+    def _check(self, st):
+        if st != N.OK:
+            raise N.LgmError(st, N.lib().lgm_kmc_last_error(self._h).decode())
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value and N._lib is not None:
+            N._lib.lgm_kmc_destroy(self._h)
+        self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def run(self, steps: int):
+        self._check(N.lib().lgm_kmc_run(self._h, int(steps)))
+
+    def stats(self) -> dict:
+        s = Stats()
+        self._check(N.lib().lgm_kmc_stats_get(self._h, ctypes.byref(s)))
+        d = {k: getattr(s, k) for k, _ in Stats._fields_ if k != "counters"}
+        d["counters"] = list(s.counters)
+        return d
+
+    def carriers(self):
+        s = self.stats()
+        e = np.zeros(max(s["max_electrons"], 1), np.int32)
+        h = np.zeros(max(s["max_holes"], 1), np.int32)
+        self._check(N.lib().lgm_kmc_get_carriers(self._h, e, len(e), h, len(h)))
+        return e[: s["electrons"]].copy(), h[: s["holes"]].copy()
+
+    def set_carriers(self, e, h):
+        e = np.ascontiguousarray(e, dtype=np.int32)
+        h = np.ascontiguousarray(h, dtype=np.int32)
+        self._check(N.lib().lgm_kmc_set_carriers(self._h, e, len(e), h, len(h)))
+
+    def world(self):
+        s = self.stats()
+        pot = np.zeros(self.volume, np.float64)
+        d = np.zeros(max(s["defects"], 1), np.int32)
+        t = np.zeros(max(s["traps"], 1), np.int32)
+        tp = np.zeros(max(s["traps"], 1), np.float64)
+        self._check(N.lib().lgm_kmc_get_world(self._h, pot.ctypes.data, d.ctypes.data, len(d),
+                                              t.ctypes.data, tp.ctypes.data, len(t)))
+        return dict(site_energy=pot, defects=d[: s["defects"]].copy(),
+                    traps=t[: s["traps"]].copy(), trap_potentials=tp[: s["traps"]].copy())
+
+    def last_outcomes(self, n):
+        o = np.zeros(max(n, 1), np.int32)
+        de = np.zeros(max(n, 1), np.float64)
+        self._check(N.lib().lgm_kmc_last_outcomes(self._h, o.ctypes.data, de.ctypes.data, len(o)))
+        return o[:n].copy(), de[:n].copy()

@@ -178,6 +178,10 @@ void orc_coupling_table(const orc_ctx* c, double* out) {
     std::memcpy(out, c->coupling.data(), c->coupling.size() * sizeof(double));
 }
 
+void orc_dims(const orc_ctx* c, int dims[3]) { dims[0] = c->X; dims[1] = c->Y; dims[2] = c->Z; }
+int orc_hopping_range(const orc_ctx* c) { return c->hopping_range; }
+double orc_sigma(const orc_ctx* c) { return c->sigma; }
+
 int orc_index_x(const orc_ctx* c, int s) { return gx(c, s); }
 int orc_index_y(const orc_ctx* c, int s) { return gy(c, s); }
 int orc_index_z(const orc_ctx* c, int s) { return gz(c, s); }

@@ -54,7 +54,7 @@ int orc_index_z(const orc_ctx* ctx, int site);
 int orc_index_s(const orc_ctx* ctx, int x, int y, int z);
 
 /* Grid::neighborsSite (cubicgrid.cpp:207-471) without the drain entries:
- * writes up to 18 site ids, returns the count. */
+ * writes up to 32 site ids (range 2 in 3-D), returns the count. */
 int orc_neighbors(const orc_ctx* ctx, int site, int hopping_range, int* out);
 
 /* One species sum as Potential::coulombE/H/D, gaussE/H/D and the Image
@@ -124,6 +124,39 @@ enum orc_agent_type {
 /* Philox4x32-10 counter-based generator (Salmon et al., SC'11), the
  * random stream shared by the GPU kMC and this oracle. */
 void orc_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);
+
+/* Context accessors. */
+void orc_dims(const orc_ctx* ctx, int dims[3]);
+int orc_hopping_range(const orc_ctx* ctx);
+double orc_sigma(const orc_ctx* ctx);
+
+/* ---- one kMC step (transistor set-up), see lgm_oracle_kmc.cpp ------------- */
+typedef struct orc_kmc_config {
+    double inverse_kt;          /* inverse.kt = e / (k_B T) (parameters.h:387)   */
+    double exciton_binding;     /* exciton.binding                               */
+    int32_t coulomb_carriers;   /* coulomb.carriers                              */
+    int32_t defects_charge;     /* defects.charge                                */
+    uint32_t image_terms;       /* 2: left, 4: right electrode images (extension) */
+    double rate_e_source_l, rate_e_source_r, rate_h_source_l, rate_h_source_r;
+    double rate_e_drain_l, rate_e_drain_r, rate_h_drain_l, rate_h_drain_r;
+    int32_t max_electrons, max_holes;
+    uint32_t seed, replica;     /* Philox key                                    */
+} orc_kmc_config;
+
+/* decideFuture outcomes per carrier */
+enum orc_outcome { ORC_OCCUPIED = 0, ORC_MET_ACCEPT = 1, ORC_MET_REJECT = 2,
+                   ORC_DRAIN_ACCEPT = 3, ORC_DRAIN_REJECT = 4 };
+
+/* Advance one step.  pot: site energies (volume entries); defects: nd sites.
+ * e_site/h_site: in/out carrier lists in list order (capacity max_electrons /
+ * max_holes), with their lengths in ne_io and nh_io.  counters: 16 uint64, (attempts,
+ * successes) of eSourceL, eSourceR, hSourceL, hSourceR, eDrainL, eDrainR,
+ * hDrainL, hDrainR.  outcome / de_out (optional): per carrier of the lists as
+ * they were at the start of the step, electrons then holes. */
+int orc_kmc_step(const orc_ctx* ctx, const orc_kmc_config* cfg, const double* pot,
+                 const int32_t* defects, int nd, uint32_t step, int32_t* e_site, int32_t* ne_io,
+                 int32_t* h_site, int32_t* nh_io, uint64_t* counters, int32_t* outcome,
+                 double* de_out, int threads);
 
 #ifdef __cplusplus
 }

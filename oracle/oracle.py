@@ -38,6 +38,19 @@ _lib = None
 _ref = None
 
 
+class KmcConfig(ctypes.Structure):
+    """orc_kmc_config (lgm_oracle.h)."""
+    _fields_ = [("inverse_kt", ctypes.c_double), ("exciton_binding", ctypes.c_double),
+                ("coulomb_carriers", ctypes.c_int32), ("defects_charge", ctypes.c_int32),
+                ("image_terms", ctypes.c_uint32),
+                ("rate_e_source_l", ctypes.c_double), ("rate_e_source_r", ctypes.c_double),
+                ("rate_h_source_l", ctypes.c_double), ("rate_h_source_r", ctypes.c_double),
+                ("rate_e_drain_l", ctypes.c_double), ("rate_e_drain_r", ctypes.c_double),
+                ("rate_h_drain_l", ctypes.c_double), ("rate_h_drain_r", ctypes.c_double),
+                ("max_electrons", ctypes.c_int32), ("max_holes", ctypes.c_int32),
+                ("seed", ctypes.c_uint32), ("replica", ctypes.c_uint32)]
+
+
 def lib():
     global _lib
     if _lib is None:
@@ -72,6 +85,12 @@ def lib():
                                       ctypes.c_double, _f64p, ctypes.c_void_p, ctypes.c_void_p,
                                       ctypes.c_int]
         L.orc_philox4x32_10.argtypes = [_u32p, _u32p, _u32p]
+        L.orc_kmc_step.argtypes = [ctypes.c_void_p, ctypes.POINTER(KmcConfig), _f64p, _i32p,
+                                   ctypes.c_int, ctypes.c_uint32, _i32p,
+                                   ctypes.POINTER(ctypes.c_int32), _i32p,
+                                   ctypes.POINTER(ctypes.c_int32),
+                                   np.ctypeslib.ndpointer(dtype=np.uint64, flags="C_CONTIGUOUS"),
+                                   ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]
         L.orc_potentials.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_uint, _i32p, _i32p,
                                      ctypes.c_int, _i32p, ctypes.c_int, _f64p, ctypes.c_int]
         _lib = L
@@ -213,6 +232,39 @@ class Oracle:
         if want_potentials:
             return de, p1, p2
         return de
+
+
+class KmcOracle:
+    """The oracle's kMC step on a world (site energies, defects, carriers)."""
+
+    def __init__(self, orc: "Oracle", site_energy, defects, electrons, holes, cfg: KmcConfig,
+                 step=0):
+        self.orc = orc
+        self.cfg = cfg
+        self.pot = np.ascontiguousarray(site_energy, dtype=np.float64)
+        self.defects = np.ascontiguousarray(defects, dtype=np.int32)
+        self.e = np.zeros(max(cfg.max_electrons, 1), np.int32)
+        self.h = np.zeros(max(cfg.max_holes, 1), np.int32)
+        self.ne = ctypes.c_int32(len(electrons))
+        self.nh = ctypes.c_int32(len(holes))
+        self.e[: len(electrons)] = electrons
+        self.h[: len(holes)] = holes
+        self.counters = np.zeros(16, np.uint64)
+        self.step_no = int(step)
+
+    def step(self, threads=0):
+        n = self.ne.value + self.nh.value
+        outcome = np.zeros(max(n, 1), np.int32)
+        de = np.zeros(max(n, 1), np.float64)
+        lib().orc_kmc_step(self.orc._c, ctypes.byref(self.cfg), self.pot, self.defects,
+                           len(self.defects), self.step_no, self.e, ctypes.byref(self.ne), self.h,
+                           ctypes.byref(self.nh), self.counters, outcome.ctypes.data,
+                           de.ctypes.data, int(threads))
+        self.step_no += 1
+        return outcome[:n].copy(), de[:n].copy()
+
+    def carriers(self):
+        return self.e[: self.ne.value].copy(), self.h[: self.nh.value].copy()
 
 
 def philox4x32_10(ctr, key):

@@ -1,0 +1,193 @@
+"""The kMC step: the oracle's invariants (CPU) and the GPU step against the
+oracle, step by step (GPU).
+
+Parity bar: carrier lists (occupancies, list order), per-carrier outcomes and
+the sixteen flux counters are bit-exact after every step under the shared
+Philox stream; Coulomb energy changes agree to the reference's own
+compareCoulomb threshold (|dE_gpu - dE_cpu| <= 1e-4, chargeagent.cpp:368).
+Decisions whose FP32 energy lies inside the guard band of the threshold are
+redone in FP64 on the GPU; the tests report how many.
+"""
+import numpy as np
+import pytest
+
+import langmuir_b200 as L
+
+
+def make_params(**keys):
+    base = dict(simulation_type="transistor", random_seed=7, seed_charges=1.0,
+                coulomb_carriers=1, iterations_real=1000, iterations_print=10)
+    base.update(keys)
+    p = L.Params.default()
+    for k, v in base.items():
+        p.set(k, v)
+    return p
+
+
+def rates(p):
+    """World::createSources / createDrains, transistor (world.cpp:990-1000, 1116-1124)."""
+    smart = lambda r, d: d if r < 0 else r
+    return dict(rate_e_source_l=smart(p.e_source_l_rate, p.source_rate),
+                rate_e_source_r=smart(p.e_source_r_rate, 0.0),
+                rate_h_source_l=smart(p.h_source_l_rate, 0.0),
+                rate_h_source_r=smart(p.h_source_r_rate, 0.0),
+                rate_e_drain_l=smart(p.e_drain_l_rate, 0.0),
+                rate_e_drain_r=smart(p.e_drain_r_rate, p.drain_rate),
+                rate_h_drain_l=smart(p.h_drain_l_rate, 0.0),
+                rate_h_drain_r=smart(p.h_drain_r_rate, 0.0))
+
+
+def oracle_for(O, p, world, e, h, max_e, max_h, replica=0, step=0):
+    q = L.Params.from_text("[Parameters]\n")  # fresh copy for the derived constants
+    for name, _ in L.Params._fields_:
+        setattr(q, name, getattr(p, name))
+    q.check()
+    orc = O.Oracle(q.grid_x, q.grid_y, q.grid_z, cutoff=q.electrostatic_cutoff,
+                   hopping_range=q.hopping_range, sigma=q.coulomb_gaussian_sigma,
+                   prefactor=q.electrostatic_prefactor)
+    cfg = O.KmcConfig(inverse_kt=q.inverse_kt, exciton_binding=q.exciton_binding,
+                      coulomb_carriers=q.coulomb_carriers, defects_charge=q.defects_charge,
+                      image_terms=(2 if q.image_charges & 1 else 0) | (4 if q.image_charges & 2 else 0),
+                      max_electrons=max_e, max_holes=max_h,
+                      seed=q.random_seed & 0xFFFFFFFF, replica=replica, **rates(q))
+    return O.KmcOracle(orc, world["site_energy"], world["defects"], e, h, cfg, step)
+
+
+# ---- CPU: the oracle step's invariants ------------------------------------------------
+def test_oracle_step_invariants(oracle_mod):
+    O = oracle_mod
+    rng = np.random.default_rng(3)
+    X, Y, Z = 20, 16, 3
+    V = X * Y * Z
+    orc = O.Oracle(X, Y, Z, cutoff=50)
+    pot = np.linspace(0, 1, X)[np.arange(V) % X] + rng.normal(0, 0.02, V)
+    defects = rng.choice(V, 10, replace=False)
+    free = np.setdiff1d(np.arange(V), defects)
+    e = rng.choice(free, 30, replace=False)
+    h = rng.choice(free, 25, replace=False)
+    cfg = O.KmcConfig(inverse_kt=O.inverse_kt(300.0), coulomb_carriers=1, max_electrons=60,
+                      max_holes=60, rate_e_source_l=0.9, rate_e_drain_r=0.9, rate_h_source_r=0.5,
+                      rate_h_drain_l=0.9, seed=5)
+    k = O.KmcOracle(orc, pot, defects, e, h, cfg)
+    for _ in range(40):
+        outcome, de = k.step(threads=2)
+        e_now, h_now = k.carriers()
+        assert len(set(e_now)) == len(e_now) and len(set(h_now)) == len(h_now)
+        assert not set(e_now) & set(defects) and not set(h_now) & set(defects)
+        assert np.all((outcome >= 0) & (outcome <= 4))
+    c = k.counters.astype(np.int64)
+    # carriers = start + injected - drained
+    assert len(k.carriers()[0]) == 30 + c[1] + c[3] - c[9] - c[11]
+    assert len(k.carriers()[1]) == 25 + c[5] + c[7] - c[13] - c[15]
+    assert c[0] == c[2] == c[4] == c[6] == 40  # one attempt per source per step
+
+
+def test_oracle_step_is_deterministic(oracle_mod):
+    O = oracle_mod
+    orc = O.Oracle(16, 16, 2, cutoff=50)
+    V = 16 * 16 * 2
+    pot = np.zeros(V)
+    e = np.arange(0, V, 23)[:15]
+    cfg = O.KmcConfig(inverse_kt=38.68, coulomb_carriers=1, max_electrons=40, max_holes=0,
+                      rate_e_source_l=0.9, rate_e_drain_r=0.9, seed=11)
+    runs = []
+    for _ in range(2):
+        k = O.KmcOracle(orc, pot, [], e, [], cfg)
+        for _ in range(25):
+            k.step()
+        runs.append(k.carriers()[0])
+    np.testing.assert_array_equal(runs[0], runs[1])
+
+
+# ---- GPU: bit-exact parity of the fused step ------------------------------------------
+CASES = {
+    "2d_holes_traps": dict(grid_x=48, grid_y=40, grid_z=1, hole_percentage=0.02,
+                           electron_percentage=0.0, trap_percentage=0.05, trap_potential=0.1,
+                           voltage_left=1.0, e_source_l_rate=0.0, h_source_l_rate=0.5,
+                           h_drain_r_rate=0.9, steps=150),
+    "3d_eh_images_disorder": dict(grid_x=32, grid_y=28, grid_z=8, electron_percentage=0.02,
+                                  hole_percentage=0.02, trap_percentage=0.02,
+                                  trap_potential=0.2, site_disorder=0.05, image_charges=3,
+                                  voltage_right=1.0, h_source_r_rate=0.5, h_drain_l_rate=0.9,
+                                  steps=80),
+    "range2_charged_defects": dict(grid_x=24, grid_y=24, grid_z=6, electron_percentage=0.03,
+                                   hole_percentage=0.01, defect_percentage=0.02,
+                                   defects_charge=1, hopping_range=2, voltage_right=0.5,
+                                   h_source_l_rate=0.3, h_drain_r_rate=0.9, steps=80),
+    "gauss_cutoff30": dict(grid_x=20, grid_y=20, grid_z=20, electron_percentage=0.01,
+                           hole_percentage=0.01, coulomb_gaussian_sigma=1.0,
+                           electrostatic_cutoff=30, h_source_l_rate=0.3, h_drain_r_rate=0.9,
+                           steps=50),
+    "no_coulomb": dict(grid_x=40, grid_y=30, grid_z=2, electron_percentage=0.05,
+                       coulomb_carriers=0, voltage_right=2.0, steps=100),
+    "2d_128_holes_1pct": dict(grid_x=128, grid_y=128, grid_z=1, hole_percentage=0.01,
+                              electron_percentage=0.0, trap_percentage=0.05,
+                              trap_potential=0.1, voltage_left=1.0, e_source_l_rate=0.0,
+                              h_source_l_rate=0.9, h_drain_r_rate=0.9, steps=200),
+}
+
+
+def run_parity(O, name, keys, replica=0):
+    keys = dict(keys)
+    steps = keys.pop("steps")
+    p = make_params(**keys)
+    with L.KMC(p, device=0, replica=replica) as g:
+        st = g.stats()
+        e0, h0 = g.carriers()
+        k = oracle_for(O, p, g.world(), e0, h0, st["max_electrons"], st["max_holes"], replica)
+        worst = 0.0
+        for s in range(steps):
+            n0 = len(k.carriers()[0]) + len(k.carriers()[1])
+            out_o, de_o = k.step()
+            g.run(1)
+            out_g, de_g = g.last_outcomes(n0)
+            np.testing.assert_array_equal(out_g, out_o, err_msg=f"{name}: outcomes, step {s}")
+            e_g, h_g = g.carriers()
+            e_o, h_o = k.carriers()
+            np.testing.assert_array_equal(e_g, e_o, err_msg=f"{name}: electrons, step {s}")
+            np.testing.assert_array_equal(h_g, h_o, err_msg=f"{name}: holes, step {s}")
+            met = (out_o == 1) | (out_o == 2)  # dE enters only Metropolis decisions
+            if met.any():
+                worst = max(worst, float(np.abs(de_g[met] - de_o[met]).max()))
+        stg = g.stats()
+        np.testing.assert_array_equal(np.array(stg["counters"], np.uint64), k.counters)
+        assert stg["step"] == steps
+        assert worst <= 1e-4, f"{name}: max |dE_gpu - dE_oracle| = {worst:.3e}"
+        return stg, worst
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", list(CASES))
+def test_gpu_step_matches_oracle(oracle_mod, name):
+    stg, worst = run_parity(oracle_mod, name, CASES[name])
+    assert stg["proposals"] > 0
+
+
+@pytest.mark.gpu
+def test_gpu_step_replicas_differ_and_repeat(oracle_mod):
+    keys = dict(CASES["no_coulomb"])
+    keys.pop("steps")
+    p = make_params(**keys)
+    out = []
+    for rep in (0, 1, 0):
+        with L.KMC(p, replica=rep) as g:
+            g.run(30)
+            out.append(g.carriers()[0])
+    np.testing.assert_array_equal(out[0], out[2])
+    assert not np.array_equal(out[0], out[1])
+
+
+@pytest.mark.gpu
+def test_gpu_set_carriers_and_errors():
+    p = make_params(**{k: v for k, v in CASES["no_coulomb"].items() if k != "steps"})
+    with L.KMC(p) as g:
+        e, h = g.carriers()
+        g.set_carriers(e[:5], h)
+        assert len(g.carriers()[0]) == 5
+        with pytest.raises(L.LgmError):
+            g.set_carriers([1, 1], [])  # two electrons on one site
+    bad = make_params(grid_x=8, grid_y=8, grid_z=1, electron_percentage=0.0,
+                      hole_percentage=0.0)
+    with pytest.raises(L.LgmError) as e:
+        L.KMC(bad)
+    assert "zero rate" in str(e.value) or "maxElectronAgents" in str(e.value)
