@@ -192,6 +192,43 @@ def reference_arm(args, w, rank):
     print(json.dumps(line), flush=True)
 
 
+def kmc_params(L, w, seed):
+    """The workload's lattice and occupancy as a Langmuir transistor run."""
+    p = L.Params.default()
+    for k, v in dict(grid_x=w["X"], grid_y=w["Y"], grid_z=w["Z"], electron_percentage=w["e"],
+                     hole_percentage=w["h"], seed_charges=1.0, coulomb_carriers=1,
+                     electrostatic_cutoff=w["cutoff"], coulomb_gaussian_sigma=w["sigma"],
+                     trap_percentage=0.02, trap_potential=0.2, site_disorder=0.05,
+                     image_charges=(1 if w["terms"] & 2 else 0) | (2 if w["terms"] & 4 else 0),
+                     voltage_right=1.0, random_seed=seed).items():
+        p.set(k, v)
+    if w["e"] == 0:
+        p.e_source_l_rate = 0.0
+    if w["h"] > 0:
+        p.h_source_r_rate = 0.9
+        p.h_drain_l_rate = 0.9
+    return p
+
+
+def kmc_run(L, w, args, seed, replica):
+    p = kmc_params(L, w, seed)
+    with L.KMC(p, device=int(os.environ.get("LOCAL_RANK", "0")), replica=replica) as k:
+        k.run(args.warmup)
+        s0 = k.stats()
+        t0 = time.perf_counter()
+        k.run(args.kmc_steps)
+        dt = time.perf_counter() - t0
+        s1 = k.stats()
+    hops = s1["proposals"] - s0["proposals"]
+    return {"workload": w["desc"] + ", traps 2% at 0.2 eV, site disorder 0.05 eV, 1 V",
+            "steps": args.kmc_steps, "ms_per_step": 1e3 * dt / args.kmc_steps,
+            "hops_per_s": hops / dt, "accepted_per_s": (s1["accepted"] - s0["accepted"]) / dt,
+            "guard_fp64_per_step": (s1["guard_evaluations"] - s0["guard_evaluations"])
+            / args.kmc_steps,
+            "carriers": s1["electrons"] + s1["holes"],
+            "timing": "host wall clock around graph replays of the whole step"}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -203,6 +240,8 @@ def main():
     ap.add_argument("--variant", type=int, default=-1, help="tile variant, -1 = autotune")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-kmc", action="store_true")
+    ap.add_argument("--kmc-steps", type=int, default=50)
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
@@ -317,6 +356,11 @@ def main():
         e2e = {"value": pairs_per_step / dt, "unit": "pair-evals/s",
                "h2d_bytes_per_step": int(4 * (2 * n + T)), "d2h_bytes_per_step": int(8 * T)}
 
+    # the fused kMC step on the same lattice and occupancy: hops per second
+    kmc = None
+    if not args.no_kmc and w["e"] + w["h"] > 0:
+        kmc = kmc_run(L, w, args, seed=2 + rank, replica=rank)
+
     peaks = measured_peaks()
     props = torch.cuda.get_device_properties(dev)
     sms = props.multi_processor_count
@@ -355,7 +399,7 @@ def main():
                        "path": "table" if args.path else "rsqrt", "l2": "flushed between steps",
                        "tile_variant": dict(ctx.variants()[variant], id=variant),
                        "parallelism": "replicas" if world > 1 else "single"},
-            "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
+            "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks, "kmc": kmc,
             "gpu_launches": launches, "accuracy": acc,
         }
         print(json.dumps(line), flush=True)
