@@ -229,6 +229,68 @@ def kmc_run(L, w, args, seed, replica):
             "timing": "host wall clock around graph replays of the whole step"}
 
 
+def batch_params(L, n, seed=4):
+    """Replicas drawn as the batched configuration draws them: square lattices
+    of side {32,64,128,256} x depth {1,2,4,8}, occupancy U(0.5%, 3%) split
+    between electrons and holes, voltage U(0.1, 2) V, traps U(0, 10%) at depth
+    U(0.05, 0.3) eV, cutoff 50."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(n):
+        xy = int(rng.choice([32, 64, 128, 256]))
+        z = int(rng.choice([1, 2, 4, 8]))
+        occ = float(rng.uniform(0.005, 0.03))
+        p = L.Params.default()
+        for k, v in dict(grid_x=xy, grid_y=xy, grid_z=z, electron_percentage=occ / 2,
+                         hole_percentage=occ / 2, seed_charges=1.0, coulomb_carriers=1,
+                         voltage_right=float(rng.uniform(0.1, 2.0)),
+                         trap_percentage=float(rng.uniform(0.0, 0.10)),
+                         trap_potential=float(rng.uniform(0.05, 0.3)),
+                         h_source_r_rate=0.9, h_drain_l_rate=0.9, random_seed=seed).items():
+            p.set(k, v)
+        out.append(p)
+    return out
+
+
+def batch_run(L, args, rank):
+    """Batched replicas in one graph vs the same replicas stepped one by one."""
+    params = batch_params(L, args.batch_replicas, seed=4 + rank)
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    t0 = time.perf_counter()
+    with L.KMCBatch(params, device=dev, replica0=1000 * rank) as b:
+        build_s = time.perf_counter() - t0
+        b.run(max(1, args.warmup))  # tunes the tile shape, records the graph
+        reps = [b.replica(i) for i in range(len(params))]
+        h0 = sum(r.stats()["proposals"] for r in reps)
+        t0 = time.perf_counter()
+        b.run(args.batch_steps)
+        dt = time.perf_counter() - t0
+        hops = sum(r.stats()["proposals"] for r in reps) - h0
+        charges = sum(r.stats()["electrons"] + r.stats()["holes"] for r in reps)
+        tuning = b.tuning()
+    # the plain single-replica path on a stratified sample of the same replicas
+    sample = list(range(0, len(params), max(1, len(params) // args.batch_sample)))
+    s_hops, s_time = 0, 0.0
+    for i in sample:
+        with L.KMC(params[i], device=dev, replica=1000 * rank + i) as k:
+            k.run(max(1, args.warmup))
+            h = k.stats()["proposals"]
+            t1 = time.perf_counter()
+            k.run(args.batch_steps)
+            s_time += time.perf_counter() - t1
+            s_hops += k.stats()["proposals"] - h
+    single = s_hops / s_time
+    return {"workload": f"{len(params)} replicas, side {{32,64,128,256}} x depth {{1,2,4,8}}, "
+                        "occupancy U(0.5%,3%) e/h, V U(0.1,2), traps U(0,10%) at U(0.05,0.3) eV, "
+                        "cutoff 50",
+            "steps": args.batch_steps, "charges": charges,
+            "ms_per_step": 1e3 * dt / args.batch_steps, "hops_per_s": hops / dt,
+            "single_replica_hops_per_s": single,
+            "single_replica_sample": f"{len(sample)} of {len(params)} replicas stepped one by one",
+            "speedup_vs_single": (hops / dt) / single, "tuning": tuning,
+            "build_s": build_s}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -242,6 +304,10 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-kmc", action="store_true")
     ap.add_argument("--kmc-steps", type=int, default=50)
+    ap.add_argument("--no-batch", action="store_true")
+    ap.add_argument("--batch-replicas", type=int, default=512)
+    ap.add_argument("--batch-steps", type=int, default=20)
+    ap.add_argument("--batch-sample", type=int, default=32)
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
@@ -361,6 +427,10 @@ def main():
     if not args.no_kmc and w["e"] + w["h"] > 0:
         kmc = kmc_run(L, w, args, seed=2 + rank, replica=rank)
 
+    batch = None
+    if not args.no_batch:
+        batch = batch_run(L, args, rank)
+
     peaks = measured_peaks()
     props = torch.cuda.get_device_properties(dev)
     sms = props.multi_processor_count
@@ -400,6 +470,7 @@ def main():
                        "tile_variant": dict(ctx.variants()[variant], id=variant),
                        "parallelism": "replicas" if world > 1 else "single"},
             "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks, "kmc": kmc,
+            "kmc_batched": batch,
             "gpu_launches": launches, "accuracy": acc,
         }
         print(json.dumps(line), flush=True)

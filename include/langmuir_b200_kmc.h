@@ -133,6 +133,30 @@ lgm_status lgm_kmc_get_world(lgm_kmc* k, double* site_energy, int32_t* defects, 
  * accept, 4 drain reject) and the Coulomb energy change used. */
 lgm_status lgm_kmc_last_outcomes(lgm_kmc* k, int32_t* outcome, double* de, int32_t cap);
 
+/* ---- batched replicas --------------------------------------------------------
+ * `count` independent replicas, params[i] for replica i (sizes, occupancies,
+ * voltages and traps may all differ; the interaction kind must not), advanced
+ * together: each phase of the step is one launch over all replicas and a
+ * batched step is one CUDA graph.  Replica i uses the random stream of a
+ * single replica with id replica0 + i, so its trajectory equals that of
+ * lgm_kmc_create(&params[i], device, replica0 + i).  Before the first step the
+ * pair-sum tile shape and work split are tuned on the batch itself. */
+typedef struct lgm_kmc_batch lgm_kmc_batch;
+lgm_status lgm_kmc_batch_create(const lgm_params* params, int32_t count, int32_t device,
+                                uint32_t replica0, lgm_kmc_batch** out);
+lgm_status lgm_kmc_batch_destroy(lgm_kmc_batch* b);
+/* b == NULL: why lgm_kmc_batch_create failed on this thread. */
+const char* lgm_kmc_batch_last_error(const lgm_kmc_batch* b);
+lgm_status lgm_kmc_batch_run(lgm_kmc_batch* b, int32_t steps);
+int32_t lgm_kmc_batch_size(const lgm_kmc_batch* b);
+/* Replica i, owned by the batch: use the lgm_kmc_* accessors on it (stats,
+ * carriers, world, outcomes); do not destroy or run it. */
+lgm_kmc* lgm_kmc_batch_replica(lgm_kmc_batch* b, int32_t i);
+/* The tuned pair-sum shape: threads per CTA, target pairs per thread, source
+ * chunks per work item, and the number of work items. */
+lgm_status lgm_kmc_batch_tuning(const lgm_kmc_batch* b, int32_t* threads, int32_t* target_pairs,
+                                int32_t* chunks_per_item, int32_t* items);
+
 #ifdef __cplusplus
 }
 #endif

@@ -157,10 +157,9 @@ __device__ __forceinline__ Philox4 draw(const Dev& D, uint32_t step, uint32_t in
 // ---- kernels ----------------------------------------------------------------------
 
 // Proposals; also snapshots the step's carrier counts.
-__global__ void k_choose(Dev D) {
+__device__ __forceinline__ void choose_body(const Dev& D, const int i) {
     const int ne = D.cnt[I_NE], nh = D.cnt[I_NH];
     const uint32_t step = (uint32_t)D.cnt[I_STEP];
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i == 0) {
         D.cnt[I_NE0] = ne;
         D.cnt[I_NH0] = nh;
@@ -181,7 +180,7 @@ __global__ void k_choose(Dev D) {
 // Source records (electrons, holes, defects, each padded to whole chunks so
 // that every FP32 run holds one charge sign) and target records (current sites
 // then future sites, one block per term).
-__global__ void k_pack(Dev D) {
+__device__ __forceinline__ void pack_body(const Dev& D, const int j) {
     const int ne = D.cnt[I_NE], nh = D.cnt[I_NH];
     const int nd = D.dq != 0 ? D.nd : 0;
     const int pe = (ne + CH - 1) / CH * CH, ph = (nh + CH - 1) / CH * CH,
@@ -189,7 +188,6 @@ __global__ void k_pack(Dev D) {
     const int nsrc = pe + ph + pd;
     const int t = 2 * (ne + nh);
     const int tpad = (t + 63) / 64 * 64;
-    const int j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j == 0) {
         D.cnt[I_NCHUNK] = nsrc / CH;
         D.cnt[I_TPHYS] = D.nterms * tpad;
@@ -230,10 +228,9 @@ __global__ void k_pack(Dev D) {
     }
 }
 
-__global__ void k_finalize(Dev D) {
+__device__ __forceinline__ void finalize_body(const Dev& D, const int g) {
     const int t = 2 * (D.cnt[I_NE] + D.cnt[I_NH]);
     const int tpad = D.cnt[I_TPAD], tphys = D.cnt[I_TPHYS];
-    const int g = blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= t) return;
     double v = 0.0, n = 0.0;
     for (int slot = 0; slot < D.nterms; ++slot) {
@@ -271,10 +268,9 @@ __device__ __forceinline__ bool metropolis(double pd, double beta, double c, dou
     return c > u;
 }
 
-__global__ void k_decide(Dev D) {
+__device__ __forceinline__ void decide_body(const Dev& D, const int i) {
     const int ne = D.cnt[I_NE0], nh = D.cnt[I_NH0];
     const uint32_t step = (uint32_t)D.cnt[I_STEP];
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= ne + nh) return;
     const bool e = i < ne;
     const int k = e ? i : i - ne;
@@ -375,12 +371,12 @@ __device__ double fp64_potential(const Dev& D, int ne, int nh, int site, double*
     return D.prefactor * v;
 }
 
-__global__ void __launch_bounds__(kGuardThreads) k_guard(Dev D) {
-    __shared__ double red[kGuardThreads];
+__device__ __forceinline__ void guard_body(const Dev& D, const int block, const int nblocks,
+                                           double* red) {
     const int ne = D.cnt[I_NE0], nh = D.cnt[I_NH0];
     const int nflag = D.cnt[I_NFLAG];
     const uint32_t step = (uint32_t)D.cnt[I_STEP];
-    for (int q_i = blockIdx.x; q_i < nflag; q_i += gridDim.x) {
+    for (int q_i = block; q_i < nflag; q_i += nblocks) {
         const int i = D.flagged[q_i];
         const bool e = i < ne;
         const int k = e ? i : i - ne;
@@ -407,9 +403,8 @@ __global__ void __launch_bounds__(kGuardThreads) k_guard(Dev D) {
 }
 
 // completeTick, part 1: contested empty sites go to the lowest list index.
-__global__ void k_claim(Dev D) {
+__device__ __forceinline__ void claim_body(const Dev& D, const int i) {
     const int ne = D.cnt[I_NE0], nh = D.cnt[I_NH0];
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= ne + nh || !D.accept[i]) return;
     const bool e = i < ne;
     const int k = e ? i : i - ne;
@@ -418,9 +413,8 @@ __global__ void k_claim(Dev D) {
 }
 
 // completeTick, part 2: winners move, drains remove (site marked -1).
-__global__ void k_move(Dev D) {
+__device__ __forceinline__ void move_body(const Dev& D, const int i) {
     const int ne = D.cnt[I_NE0], nh = D.cnt[I_NH0];
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
     unsigned long long moved = 0, props = 0;
     if (i < ne + nh) {
         props = 1;
@@ -455,9 +449,8 @@ __global__ void k_move(Dev D) {
     }
 }
 
-__global__ void k_unclaim(Dev D) {
+__device__ __forceinline__ void unclaim_body(const Dev& D, const int i) {
     const int ne = D.cnt[I_NE0], nh = D.cnt[I_NH0];
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= ne + nh || !D.accept[i]) return;
     const bool e = i < ne;
     const int k = e ? i : i - ne;
@@ -493,8 +486,7 @@ __device__ int compact(int32_t* a, int n, int* warp_sums) {
     return base;
 }
 
-__global__ void __launch_bounds__(kCompactThreads) k_compact_inject(Dev D) {
-    __shared__ int warp_sums[32];
+__device__ __forceinline__ void compact_inject_body(const Dev& D, int* warp_sums) {
     int ne = D.cnt[I_NE0], nh = D.cnt[I_NH0];
     if (D.cnt[I_REMOVED]) {
         ne = compact(D.e_site, ne, warp_sums);
@@ -523,6 +515,61 @@ __global__ void __launch_bounds__(kCompactThreads) k_compact_inject(Dev D) {
     D.cnt[I_NE] = ne;
     D.cnt[I_NH] = nh;
     D.cnt[I_STEP] = (int32_t)(step + 1);
+}
+
+// Single-replica kernels: the Dev travels by value.
+#define LGM_THREAD_INDEX (int)(blockIdx.x * blockDim.x + threadIdx.x)
+__global__ void k_choose(Dev D) { choose_body(D, LGM_THREAD_INDEX); }
+__global__ void k_pack(Dev D) { pack_body(D, LGM_THREAD_INDEX); }
+__global__ void k_finalize(Dev D) { finalize_body(D, LGM_THREAD_INDEX); }
+__global__ void k_decide(Dev D) { decide_body(D, LGM_THREAD_INDEX); }
+__global__ void __launch_bounds__(kGuardThreads) k_guard(Dev D) {
+    __shared__ double red[kGuardThreads];
+    guard_body(D, blockIdx.x, gridDim.x, red);
+}
+__global__ void k_claim(Dev D) { claim_body(D, LGM_THREAD_INDEX); }
+__global__ void k_move(Dev D) { move_body(D, LGM_THREAD_INDEX); }
+__global__ void k_unclaim(Dev D) { unclaim_body(D, LGM_THREAD_INDEX); }
+__global__ void __launch_bounds__(kCompactThreads) k_compact_inject(Dev D) {
+    __shared__ int warp_sums[32];
+    compact_inject_body(D, warp_sums);
+}
+
+// Batched kernels: block b works for replica map[b].x as its local block
+// map[b].y (every block lies inside one replica, so warp-level sums stay
+// within a replica).
+#define LGM_BATCH_INDEX(map) ((map).y * (int)blockDim.x + (int)threadIdx.x)
+__global__ void kb_choose(const Dev* R, const int2* map) {
+    const int2 m = map[blockIdx.x]; choose_body(R[m.x], LGM_BATCH_INDEX(m));
+}
+__global__ void kb_pack(const Dev* R, const int2* map) {
+    const int2 m = map[blockIdx.x]; pack_body(R[m.x], LGM_BATCH_INDEX(m));
+}
+__global__ void kb_finalize(const Dev* R, const int2* map) {
+    const int2 m = map[blockIdx.x]; finalize_body(R[m.x], LGM_BATCH_INDEX(m));
+}
+__global__ void kb_decide(const Dev* R, const int2* map) {
+    const int2 m = map[blockIdx.x]; decide_body(R[m.x], LGM_BATCH_INDEX(m));
+}
+// blocks_per_replica consecutive blocks per replica
+__global__ void __launch_bounds__(kGuardThreads) kb_guard(const Dev* R, int blocks_per_replica) {
+    __shared__ double red[kGuardThreads];
+    guard_body(R[blockIdx.x / blocks_per_replica], blockIdx.x % blocks_per_replica,
+               blocks_per_replica, red);
+}
+__global__ void kb_claim(const Dev* R, const int2* map) {
+    const int2 m = map[blockIdx.x]; claim_body(R[m.x], LGM_BATCH_INDEX(m));
+}
+__global__ void kb_move(const Dev* R, const int2* map) {
+    const int2 m = map[blockIdx.x]; move_body(R[m.x], LGM_BATCH_INDEX(m));
+}
+__global__ void kb_unclaim(const Dev* R, const int2* map) {
+    const int2 m = map[blockIdx.x]; unclaim_body(R[m.x], LGM_BATCH_INDEX(m));
+}
+// one block per replica
+__global__ void __launch_bounds__(kCompactThreads) kb_compact_inject(const Dev* R) {
+    __shared__ int warp_sums[32];
+    compact_inject_body(R[blockIdx.x], warp_sums);
 }
 
 // ---- host side -------------------------------------------------------------------
@@ -1009,6 +1056,301 @@ lgm_status lgm_kmc_last_outcomes(lgm_kmc* k, int32_t* outcome, double* de, int32
     if (n > cap) return kfail(k, LGM_ERR_CAPACITY, "buffer too small");
     if (n && outcome) KCUDA(k, cudaMemcpy(outcome, k->D.outcome, sizeof(int32_t) * n, cudaMemcpyDeviceToHost));
     if (n && de) KCUDA(k, cudaMemcpy(de, k->D.de, sizeof(double) * n, cudaMemcpyDeviceToHost));
+    return LGM_OK;
+}
+
+}  // extern "C"
+
+// ---- batched replicas ----------------------------------------------------------------
+//
+// Many independent replicas of uneven size advance together: every phase of
+// the step is one launch over all replicas (a block-to-replica map for the
+// per-carrier phases, a work-item table of (replica, tile, split) for the
+// pair sums), and the whole batched step is one CUDA graph.  Replica i keeps
+// the Philox key of a single replica with id replica0 + i, so a batched run
+// reproduces the single-replica runs bit for bit.
+
+namespace {
+
+struct BatchVariant {
+    int nt, rp;
+    void (*fn[2])(const PairArgs*, const int4*);
+};
+#define LGM_BV(NT, RP)                                                                 \
+    BatchVariant {                                                                     \
+        NT, RP, {                                                                      \
+            &pair_kernel_items<0, 0, NT, RP, kSUB, true>,                              \
+                &pair_kernel_items<1, 0, NT, RP, kSUB, true>                           \
+        }                                                                              \
+    }
+const BatchVariant kBatchVariants[] = {LGM_BV(128, 4), LGM_BV(128, 2), LGM_BV(64, 4),
+                                       LGM_BV(256, 2)};
+constexpr int kNumBatchVariants = 4;
+// Source chunks per pair work item tried by the tuner.
+const int kChunksPerItem[] = {16, 48};
+
+}  // namespace
+
+struct lgm_kmc_batch {
+    std::vector<lgm_kmc*> reps;
+    int device = 0;
+    int gauss = 0;
+    int coulomb = 0;
+    cudaStream_t stream = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    Dev* d_reps = nullptr;
+    PairArgs* d_pargs = nullptr;
+    int4* d_items = nullptr;
+    int n_items = 0;
+    int2 *map_car = nullptr, *map_pack = nullptr, *map_fin = nullptr;
+    int nb_car = 0, nb_pack = 0, nb_fin = 0;
+    int variant = 0, cpi = 16;
+    std::vector<Dev> hD;
+    std::string err;
+};
+
+namespace {
+
+thread_local std::string g_batch_create_error;
+
+lgm_status bfail(lgm_kmc_batch* b, lgm_status s, const std::string& m) {
+    if (b) b->err = m;
+    return s;
+}
+
+#define BCUDA(b, call)                                                                   \
+    do {                                                                                 \
+        cudaError_t e_ = (call);                                                         \
+        if (e_ != cudaSuccess) return bfail((b), LGM_ERR_CUDA, std::string(#call ": ") + \
+                                                               cudaGetErrorString(e_));  \
+    } while (0)
+
+// Pair work items and per-replica split counts for a variant / chunk budget.
+lgm_status build_items(lgm_kmc_batch* b, int v, int cpi) {
+    const BatchVariant& BV = kBatchVariants[v];
+    const int tile = BV.nt * 2 * BV.rp;
+    std::vector<int4> items;
+    std::vector<PairArgs> pargs(b->reps.size());
+    for (size_t r = 0; r < b->reps.size(); ++r) {
+        Dev& D = b->hD[r];
+        const lgm_kmc* k = b->reps[r];
+        const int chunks = D.src_cap / CH;
+        const int splits = std::max(1, std::min(k->D.splits, (chunks + cpi - 1) / cpi));
+        D.splits = splits;
+        const int tiles = (D.nterms * D.tpad_cap + tile - 1) / tile;
+        for (int t = 0; t < tiles; ++t)
+            for (int sp = 0; sp < splits; ++sp) items.push_back(make_int4((int)r, t, sp, splits));
+        PairArgs& A = pargs[r];
+        A.geo = D.geo; A.qq = D.qq; A.splits = splits; A.tgt = D.tgt; A.part = D.part;
+        A.part_norm = D.part_norm; A.c2 = (float)D.cutoff2;
+        A.tab = k->gtab; A.tab_k = D.gauss ? k->gtab_k : 0;
+        A.err = D.err; A.dyn = D.cnt + I_NCHUNK;
+    }
+    if (b->d_items) cudaFree(b->d_items);
+    b->d_items = nullptr;
+    BCUDA(b, cudaMalloc(&b->d_items, sizeof(int4) * std::max<size_t>(items.size(), 1)));
+    BCUDA(b, cudaMemcpy(b->d_items, items.data(), sizeof(int4) * items.size(), cudaMemcpyHostToDevice));
+    BCUDA(b, cudaMemcpy(b->d_pargs, pargs.data(), sizeof(PairArgs) * pargs.size(), cudaMemcpyHostToDevice));
+    BCUDA(b, cudaMemcpy(b->d_reps, b->hD.data(), sizeof(Dev) * b->hD.size(), cudaMemcpyHostToDevice));
+    b->n_items = (int)items.size();
+    return LGM_OK;
+}
+
+size_t batch_smem(const lgm_kmc_batch* b) {
+    int tk = 0;
+    for (const lgm_kmc* k : b->reps) tk = std::max(tk, k->D.gauss ? k->gtab_k : 0);
+    return pair_smem_bytes(tk);
+}
+
+lgm_status enqueue_batch_pair(lgm_kmc_batch* b, cudaStream_t st) {
+    const BatchVariant& BV = kBatchVariants[b->variant];
+    BV.fn[b->gauss]<<<b->n_items, BV.nt, batch_smem(b), st>>>(b->d_pargs, b->d_items);
+    BCUDA(b, cudaGetLastError());
+    return LGM_OK;
+}
+
+lgm_status enqueue_batch_step(lgm_kmc_batch* b) {
+    cudaStream_t st = b->stream;
+    const int R = (int)b->reps.size();
+    kb_choose<<<b->nb_car, 256, 0, st>>>(b->d_reps, b->map_car);
+    if (b->coulomb) {
+        kb_pack<<<b->nb_pack, 256, 0, st>>>(b->d_reps, b->map_pack);
+        lgm_status s = enqueue_batch_pair(b, st);
+        if (s != LGM_OK) return s;
+        kb_finalize<<<b->nb_fin, 256, 0, st>>>(b->d_reps, b->map_fin);
+    }
+    kb_decide<<<b->nb_car, 256, 0, st>>>(b->d_reps, b->map_car);
+    if (b->coulomb) kb_guard<<<2 * R, kGuardThreads, 0, st>>>(b->d_reps, 2);
+    kb_claim<<<b->nb_car, 256, 0, st>>>(b->d_reps, b->map_car);
+    kb_move<<<b->nb_car, 256, 0, st>>>(b->d_reps, b->map_car);
+    kb_unclaim<<<b->nb_car, 256, 0, st>>>(b->d_reps, b->map_car);
+    kb_compact_inject<<<R, kCompactThreads, 0, st>>>(b->d_reps);
+    BCUDA(b, cudaGetLastError());
+    return LGM_OK;
+}
+
+// The project's tile tuner for the batch: times every (variant, chunks per
+// item) pair on the batch's current charges with CUDA events, keeps the best.
+lgm_status tune_batch(lgm_kmc_batch* b) {
+    if (!b->coulomb) return LGM_OK;
+    cudaStream_t st = b->stream;
+    kb_choose<<<b->nb_car, 256, 0, st>>>(b->d_reps, b->map_car);
+    kb_pack<<<b->nb_pack, 256, 0, st>>>(b->d_reps, b->map_pack);
+    BCUDA(b, cudaGetLastError());
+    cudaEvent_t e0, e1;
+    BCUDA(b, cudaEventCreate(&e0));
+    BCUDA(b, cudaEventCreate(&e1));
+    float best = 1e30f;
+    int bv = 0, bc = kChunksPerItem[0];
+    for (int v = 0; v < kNumBatchVariants; ++v)
+        for (int cpi : kChunksPerItem) {
+            b->variant = v;
+            lgm_status s = build_items(b, v, cpi);
+            if (s != LGM_OK) return s;
+            float ms[3];
+            for (int r = 0; r < 3; ++r) {
+                cudaEventRecord(e0, st);
+                if ((s = enqueue_batch_pair(b, st)) != LGM_OK) return s;
+                cudaEventRecord(e1, st);
+                cudaEventSynchronize(e1);
+                cudaEventElapsedTime(&ms[r], e0, e1);
+            }
+            std::sort(ms, ms + 3);
+            if (ms[1] < best) { best = ms[1]; bv = v; bc = cpi; }
+        }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    b->variant = bv;
+    b->cpi = bc;
+    // the step counters advanced by nothing: choose/pack only snapshot counts
+    return build_items(b, bv, bc);
+}
+
+}  // namespace
+
+extern "C" {
+
+lgm_status lgm_kmc_batch_create(const lgm_params* params, int32_t count, int32_t device,
+                                uint32_t replica0, lgm_kmc_batch** out) {
+    g_batch_create_error.clear();
+    if (!params || count < 1 || !out) return LGM_ERR_INVALID_ARGUMENT;
+    *out = nullptr;
+    lgm_kmc_batch* b = new (std::nothrow) lgm_kmc_batch();
+    if (!b) return LGM_ERR_INVALID_ARGUMENT;
+    auto bail = [&](lgm_status s, const std::string& m) {
+        g_batch_create_error = m;
+        lgm_kmc_batch_destroy(b);
+        return s;
+    };
+    b->device = device < 0 ? 0 : device;
+    for (int i = 0; i < count; ++i) {
+        lgm_kmc* k = nullptr;
+        lgm_status s = lgm_kmc_create(&params[i], b->device, replica0 + (uint32_t)i, &k);
+        if (s != LGM_OK) return bail(s, "replica " + std::to_string(i) + ": " + lgm_kmc_last_error(nullptr));
+        b->reps.push_back(k);
+    }
+    // one interaction kind and one cutoff-table layout per batch
+    b->gauss = b->reps[0]->D.gauss;
+    b->coulomb = b->reps[0]->D.coulomb;
+    for (lgm_kmc* k : b->reps)
+        if (k->D.gauss != b->gauss || k->D.coulomb != b->coulomb)
+            return bail(LGM_ERR_UNSUPPORTED,
+                        "a batch mixes point and Gaussian charges or Coulomb on and off");
+    if (cudaSetDevice(b->device) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess)
+        return bail(LGM_ERR_CUDA, "stream");
+    for (lgm_kmc* k : b->reps) b->hD.push_back(k->D);
+    // block maps
+    std::vector<int2> car, pack, fin;
+    for (int r = 0; r < count; ++r) {
+        const Dev& D = b->hD[r];
+        const int ncap = std::max(1, D.cap_e + D.cap_h);
+        for (int i = 0; i < (ncap + 255) / 256; ++i) car.push_back(make_int2(r, i));
+        const int np = std::max(D.src_cap, D.tpad_cap);
+        for (int i = 0; i < (np + 255) / 256; ++i) pack.push_back(make_int2(r, i));
+        for (int i = 0; i < (2 * ncap + 255) / 256; ++i) fin.push_back(make_int2(r, i));
+    }
+    auto upload = [&](int2** dst, const std::vector<int2>& v) -> bool {
+        return cudaMalloc(dst, sizeof(int2) * v.size()) == cudaSuccess &&
+               cudaMemcpy(*dst, v.data(), sizeof(int2) * v.size(), cudaMemcpyHostToDevice) == cudaSuccess;
+    };
+    if (!upload(&b->map_car, car) || !upload(&b->map_pack, pack) || !upload(&b->map_fin, fin))
+        return bail(LGM_ERR_CUDA, "block maps");
+    b->nb_car = (int)car.size();
+    b->nb_pack = (int)pack.size();
+    b->nb_fin = (int)fin.size();
+    if (cudaMalloc(&b->d_reps, sizeof(Dev) * count) != cudaSuccess ||
+        cudaMalloc(&b->d_pargs, sizeof(PairArgs) * count) != cudaSuccess)
+        return bail(LGM_ERR_CUDA, "descriptors");
+    if (b->gauss) {
+        cudaFuncSetAttribute(kBatchVariants[0].fn[1], cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)batch_smem(b));
+        for (const BatchVariant& BV : kBatchVariants)
+            cudaFuncSetAttribute(BV.fn[1], cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)batch_smem(b));
+    }
+    lgm_status s = build_items(b, 0, kChunksPerItem[0]);
+    if (s != LGM_OK) return bail(s, b->err);
+    *out = b;
+    return LGM_OK;
+}
+
+lgm_status lgm_kmc_batch_destroy(lgm_kmc_batch* b) {
+    if (!b) return LGM_OK;
+    cudaSetDevice(b->device);
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    if (b->graph) cudaGraphDestroy(b->graph);
+    void* ptrs[] = {b->d_reps, b->d_pargs, b->d_items, b->map_car, b->map_pack, b->map_fin};
+    for (void* p : ptrs)
+        if (p) cudaFree(p);
+    if (b->stream) cudaStreamDestroy(b->stream);
+    for (lgm_kmc* k : b->reps) lgm_kmc_destroy(k);
+    delete b;
+    return LGM_OK;
+}
+
+const char* lgm_kmc_batch_last_error(const lgm_kmc_batch* b) {
+    return b ? b->err.c_str() : g_batch_create_error.c_str();
+}
+
+int32_t lgm_kmc_batch_size(const lgm_kmc_batch* b) { return b ? (int32_t)b->reps.size() : 0; }
+
+lgm_kmc* lgm_kmc_batch_replica(lgm_kmc_batch* b, int32_t i) {
+    if (!b || i < 0 || i >= (int)b->reps.size()) return nullptr;
+    return b->reps[i];
+}
+
+lgm_status lgm_kmc_batch_run(lgm_kmc_batch* b, int32_t steps) {
+    if (!b || steps < 0) return LGM_ERR_INVALID_ARGUMENT;
+    BCUDA(b, cudaSetDevice(b->device));
+    for (lgm_kmc* k : b->reps) BCUDA(b, cudaStreamSynchronize(k->stream));
+    if (!b->exec && steps > 0) {
+        lgm_status s = tune_batch(b);
+        if (s != LGM_OK) return s;
+        BCUDA(b, cudaStreamSynchronize(b->stream));
+        BCUDA(b, cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+        s = enqueue_batch_step(b);
+        cudaGraph_t g = nullptr;
+        cudaError_t e = cudaStreamEndCapture(b->stream, &g);
+        if (s != LGM_OK) { if (g) cudaGraphDestroy(g); return s; }
+        if (e != cudaSuccess) return bfail(b, LGM_ERR_CUDA, "graph capture failed");
+        b->graph = g;
+        BCUDA(b, cudaGraphInstantiate(&b->exec, g, 0));
+    }
+    for (int i = 0; i < steps; ++i) BCUDA(b, cudaGraphLaunch(b->exec, b->stream));
+    BCUDA(b, cudaStreamSynchronize(b->stream));
+    return LGM_OK;
+}
+
+lgm_status lgm_kmc_batch_tuning(const lgm_kmc_batch* b, int32_t* threads, int32_t* target_pairs,
+                                int32_t* chunks_per_item, int32_t* items) {
+    if (!b) return LGM_ERR_INVALID_ARGUMENT;
+    if (threads) *threads = kBatchVariants[b->variant].nt;
+    if (target_pairs) *target_pairs = kBatchVariants[b->variant].rp;
+    if (chunks_per_item) *chunks_per_item = b->cpi;
+    if (items) *items = b->n_items;
     return LGM_OK;
 }
 

@@ -65,14 +65,15 @@ inline size_t pair_smem_bytes(int tab_k) {
 // KIND 0 point, 1 gauss.  PATH 0 MUFU rsqrt, 1 shared-memory table of w(k)
 // for every integer r^2 = k (entries 0 and c^2 are 0).  NT threads, RP target
 // pairs per thread, SUB sources per FP32 run (SUB divides CH).
-template <int KIND, int PATH, int NT, int RP, int SUB, bool NORM = false>
-__global__ void __launch_bounds__(NT) pair_kernel(PairArgs A) {
+// One CTA's work: target tile `tile`, source split `split` of A.splits.
+template <int KIND, int PATH, int NT, int RP, int SUB, bool NORM>
+__device__ __forceinline__ void pair_tile(PairArgs A, const int tile, const int split) {
     static_assert(CH % SUB == 0, "SUB must divide CH");
     if (A.dyn) {
         A.n_chunks = A.dyn[0];
         A.t_phys = A.dyn[1];
     }
-    if ((int)blockIdx.x * (NT * 2 * RP) >= A.t_phys) return;  // tile beyond this launch's targets
+    if (tile * (NT * 2 * RP) >= A.t_phys) return;  // tile beyond this launch's targets
     extern __shared__ __align__(128) unsigned char smem[];
     float4* s_geo = reinterpret_cast<float4*>(smem);                       // [2][CH*2]
     float2* s_qq = reinterpret_cast<float2*>(smem + 2 * CH * 2 * sizeof(float4));  // [2][CH]
@@ -80,7 +81,6 @@ __global__ void __launch_bounds__(NT) pair_kernel(PairArgs A) {
     float* s_tab = reinterpret_cast<float*>(smem + 2 * pair_stage_bytes() + 16);
 
     const int tid = threadIdx.x;
-    const int split = blockIdx.y;
     const int c_begin = (int)((long long)split * A.n_chunks / A.splits);
     const int c_end = (int)((long long)(split + 1) * A.n_chunks / A.splits);
     const int nck = c_end - c_begin;
@@ -110,7 +110,7 @@ __global__ void __launch_bounds__(NT) pair_kernel(PairArgs A) {
 
     // Targets of this thread: p = base + tid + k*NT, k = 0 .. 2*RP-1; pair k
     // packs targets 2k and 2k+1.
-    const int base = blockIdx.x * (NT * 2 * RP);
+    const int base = tile * (NT * 2 * RP);
     float2 tx[RP], ty[RP], tz[RP], tt[RP];
 #pragma unroll
     for (int k = 0; k < RP; ++k) {
@@ -222,6 +222,24 @@ __global__ void __launch_bounds__(NT) pair_kernel(PairArgs A) {
             if (NORM) A.part_norm[(size_t)split * A.t_phys + p] = nrm[NORM ? k : 0];
         }
     }
+}
+
+// Grid form: blockIdx.x = target tile, blockIdx.y = source split.
+template <int KIND, int PATH, int NT, int RP, int SUB, bool NORM = false>
+__global__ void __launch_bounds__(NT) pair_kernel(PairArgs A) {
+    pair_tile<KIND, PATH, NT, RP, SUB, NORM>(A, blockIdx.x, blockIdx.y);
+}
+
+// Work-item form for many independent problems in one launch (batched
+// replicas): item = {problem, tile, split, splits}; problem p's arguments are
+// args[p].  Items of uneven problems share the grid.
+template <int KIND, int PATH, int NT, int RP, int SUB, bool NORM = false>
+__global__ void __launch_bounds__(NT) pair_kernel_items(const PairArgs* __restrict__ args,
+                                                        const int4* __restrict__ items) {
+    const int4 it = items[blockIdx.x];
+    PairArgs A = args[it.x];
+    A.splits = it.w;
+    pair_tile<KIND, PATH, NT, RP, SUB, NORM>(A, it.y, it.z);
 }
 
 }  // namespace lgm

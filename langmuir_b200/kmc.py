@@ -196,3 +196,87 @@ class KMC:
         de = np.zeros(max(n, 1), np.float64)
         self._check(N.lib().lgm_kmc_last_outcomes(self._h, o.ctypes.data, de.ctypes.data, len(o)))
         return o[:n].copy(), de[:n].copy()
+
+
+N.SIGNATURES.update({
+    "lgm_kmc_batch_create": (_i32, [ctypes.POINTER(Params), _i32, _i32, ctypes.c_uint32,
+                                    ctypes.POINTER(_vp)]),
+    "lgm_kmc_batch_destroy": (_i32, [_vp]),
+    "lgm_kmc_batch_last_error": (ctypes.c_char_p, [_vp]),
+    "lgm_kmc_batch_run": (_i32, [_vp, _i32]),
+    "lgm_kmc_batch_size": (_i32, [_vp]),
+    "lgm_kmc_batch_replica": (_vp, [_vp, _i32]),
+    "lgm_kmc_batch_tuning": (_i32, [_vp, ctypes.POINTER(_i32), ctypes.POINTER(_i32),
+                                    ctypes.POINTER(_i32), ctypes.POINTER(_i32)]),
+})
+if N._lib is not None:
+    for _name in ("lgm_kmc_batch_create", "lgm_kmc_batch_destroy", "lgm_kmc_batch_last_error",
+                  "lgm_kmc_batch_run", "lgm_kmc_batch_size", "lgm_kmc_batch_replica",
+                  "lgm_kmc_batch_tuning"):
+        _fn = getattr(N._lib, _name)
+        _fn.restype, _fn.argtypes = N.SIGNATURES[_name]
+
+
+class _Borrowed(KMC):
+    """A replica owned by a batch (accessors only)."""
+
+    def __init__(self, handle, params):
+        self._h = ctypes.c_void_p(handle)
+        self.params = params
+        self.volume = params.grid_x * params.grid_y * params.grid_z
+
+    def close(self):
+        self._h = None
+
+    def run(self, steps):
+        raise RuntimeError("run the batch, not one of its replicas")
+
+
+class KMCBatch:
+    """Replicas of uneven size advanced together on one GPU; replica i has the
+    random stream of a single replica with id replica0 + i."""
+
+    def __init__(self, params_list, device=0, replica0=0):
+        arr = (Params * len(params_list))(*params_list)
+        h = ctypes.c_void_p()
+        st = N.lib().lgm_kmc_batch_create(arr, len(params_list), int(device), int(replica0),
+                                          ctypes.byref(h))
+        if st != N.OK:
+            raise N.LgmError(st, N.lib().lgm_kmc_batch_last_error(None).decode())
+        self._h = h
+        self._params = list(params_list)
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value and N._lib is not None:
+            N._lib.lgm_kmc_batch_destroy(self._h)
+        self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __len__(self):
+        return N.lib().lgm_kmc_batch_size(self._h)
+
+    def run(self, steps):
+        st = N.lib().lgm_kmc_batch_run(self._h, int(steps))
+        if st != N.OK:
+            raise N.LgmError(st, N.lib().lgm_kmc_batch_last_error(self._h).decode())
+
+    def replica(self, i) -> KMC:
+        ptr = N.lib().lgm_kmc_batch_replica(self._h, int(i))
+        if not ptr:
+            raise IndexError(i)
+        return _Borrowed(ptr, self._params[i])
+
+    def tuning(self) -> dict:
+        a, b, c, d = (ctypes.c_int32() for _ in range(4))
+        N.lib().lgm_kmc_batch_tuning(self._h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c),
+                                     ctypes.byref(d))
+        return {"threads": a.value, "target_pairs": b.value, "chunks_per_item": c.value,
+                "items": d.value}

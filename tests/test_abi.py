@@ -8,13 +8,15 @@ import pytest
 from langmuir_b200 import _native as N
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-HEADER = os.path.join(ROOT, "include", "langmuir_b200.h")
+HEADERS = [os.path.join(ROOT, "include", h) for h in ("langmuir_b200.h", "langmuir_b200_kmc.h")]
 
 
 def declared_functions():
-    text = open(HEADER).read()
-    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
-    return sorted(set(re.findall(r"\b(lgm_[a-z0-9_]+)\s*\(", text)))
+    names = set()
+    for h in HEADERS:
+        text = re.sub(r"/\*.*?\*/", "", open(h).read(), flags=re.S)
+        names |= set(re.findall(r"\b(lgm_[a-z0-9_]+)\s*\(", text))
+    return sorted(names)
 
 
 def test_library_builds_and_loads():
@@ -25,6 +27,7 @@ def test_library_builds_and_loads():
 
 
 def test_every_declared_symbol_is_exported():
+    import langmuir_b200  # noqa: F401  (binds the kMC entry points too)
     L = ctypes.CDLL(N.LIB_PATH)
     names = declared_functions()
     assert "lgm_coulomb_kernel2" in names and "lgm_create" in names

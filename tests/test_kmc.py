@@ -191,3 +191,64 @@ def test_gpu_set_carriers_and_errors():
     with pytest.raises(L.LgmError) as e:
         L.KMC(bad)
     assert "zero rate" in str(e.value) or "maxElectronAgents" in str(e.value)
+
+
+# ---- GPU: batched replicas reproduce single-replica runs ---------------------------------
+def uneven_params(n, seed=1):
+    """Replicas of uneven size, occupancy, voltage and traps (as the batched
+    configuration draws them)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n):
+        xy = int(rng.choice([16, 24, 32, 48]))
+        z = int(rng.choice([1, 2, 4]))
+        occ = float(rng.uniform(0.005, 0.03))
+        out.append(make_params(grid_x=xy, grid_y=xy, grid_z=z, electron_percentage=occ,
+                               hole_percentage=occ / 2, voltage_right=float(rng.uniform(0.1, 2.0)),
+                               trap_percentage=float(rng.uniform(0.0, 0.1)),
+                               trap_potential=float(rng.uniform(0.05, 0.3)),
+                               h_source_r_rate=0.5, h_drain_l_rate=0.9))
+    return out
+
+
+@pytest.mark.gpu
+def test_batch_matches_single_replicas():
+    params = uneven_params(9)
+    steps = 40
+    with L.KMCBatch(params, replica0=100) as b:
+        b.run(steps)
+        got = [b.replica(i).carriers() for i in range(len(params))]
+        stats = [b.replica(i).stats() for i in range(len(params))]
+        assert b.tuning()["items"] > 0
+    for i, p in enumerate(params):
+        with L.KMC(p, replica=100 + i) as g:
+            g.run(steps)
+            e, h = g.carriers()
+            s = g.stats()
+        np.testing.assert_array_equal(got[i][0], e, err_msg=f"replica {i} electrons")
+        np.testing.assert_array_equal(got[i][1], h, err_msg=f"replica {i} holes")
+        assert stats[i]["counters"] == s["counters"] and stats[i]["step"] == steps
+
+
+@pytest.mark.gpu
+def test_batch_replica_matches_oracle(oracle_mod):
+    params = uneven_params(3, seed=5)
+    steps = 25
+    with L.KMCBatch(params, replica0=7) as b:
+        reps = [b.replica(i) for i in range(3)]
+        orcs = []
+        for i, r in enumerate(reps):
+            st = r.stats()
+            e0, h0 = r.carriers()
+            orcs.append(oracle_for(oracle_mod, params[i], r.world(), e0, h0, st["max_electrons"],
+                                   st["max_holes"], replica=7 + i))
+        for _ in range(steps):
+            for k in orcs:
+                k.step()
+            b.run(1)
+        for r, k in zip(reps, orcs):
+            e, h = r.carriers()
+            e_o, h_o = k.carriers()
+            np.testing.assert_array_equal(e, e_o)
+            np.testing.assert_array_equal(h, h_o)
+            np.testing.assert_array_equal(np.array(r.stats()["counters"], np.uint64), k.counters)
