@@ -68,6 +68,11 @@ typedef struct lgm_params {
      *   site.disorder: standard deviation (eV) of a Gaussian energy on every site */
     int32_t image_charges;
     double site_disorder;
+    /*   morphology.confine: holes only on donor, electrons only on acceptor sites
+     *                       (phase from lgm_kmc_set_morphology);
+     *   generation.interface: excitons split across a random donor-acceptor bond */
+    int32_t morphology_confine;
+    int32_t generation_interface;
 } lgm_params;
 
 void lgm_params_default(lgm_params* p);
@@ -94,9 +99,9 @@ typedef struct lgm_kmc lgm_kmc;
 /* Builds the world on the host -- defects, traps (seeds and growth,
  * potential.cpp:74-244), site energies (linear field, gate, traps,
  * potential.cpp:17-72), seeded carriers (world.cpp:759-959) -- from a
- * Philox stream keyed by (random.seed, replica), then uploads it.  Only the
- * transistor set-up with source.metropolis off is supported
- * (LGM_ERR_UNSUPPORTED otherwise). */
+ * Philox stream keyed by (random.seed, replica), then uploads it.  Transistor
+ * and solar-cell set-ups; source.metropolis and balance.charges are not
+ * supported (LGM_ERR_UNSUPPORTED). */
 lgm_status lgm_kmc_create(const lgm_params* p, int32_t device, uint32_t replica, lgm_kmc** out);
 lgm_status lgm_kmc_destroy(lgm_kmc* k);
 /* Text of the last error on `k`; k == NULL: why lgm_kmc_create failed on this thread. */
@@ -114,8 +119,9 @@ typedef struct lgm_kmc_stats {
     uint64_t proposals;            /* carrier proposals processed (hops attempted)        */
     uint64_t accepted;             /* proposals that moved a carrier or left by a drain   */
     uint64_t guard_evaluations;    /* decisions re-evaluated in FP64 (near the threshold) */
-    uint64_t counters[16];         /* (attempts, successes) of eSourceL, eSourceR,
-                                      hSourceL, hSourceR, eDrainL, eDrainR, hDrainL, hDrainR */
+    uint64_t counters[20];         /* (attempts, successes) of eSourceL, eSourceR,
+                                      hSourceL, hSourceR, eDrainL, eDrainR, hDrainL, hDrainR,
+                                      the exciton source and the recombination agent */
 } lgm_kmc_stats;
 lgm_status lgm_kmc_stats_get(lgm_kmc* k, lgm_kmc_stats* s);
 
@@ -128,6 +134,12 @@ lgm_status lgm_kmc_set_carriers(lgm_kmc* k, const int32_t* e_sites, int32_t ne,
 /* Site energies (volume values), defect sites, trap sites and potentials. */
 lgm_status lgm_kmc_get_world(lgm_kmc* k, double* site_energy, int32_t* defects, int32_t d_cap,
                              int32_t* traps, double* trap_potentials, int32_t t_cap);
+/* Donor (0) / acceptor (1) phase of every lattice site, for
+ * morphology.confine and generation.interface (extensions: carriers confined
+ * to their phase, excitons generated across donor-acceptor bonds).  Call
+ * before the first step. */
+lgm_status lgm_kmc_set_morphology(lgm_kmc* k, const uint8_t* phase);
+
 /* Per-carrier outcome of the last step (electrons then holes as listed at its
  * start: 0 occupied, 1 Metropolis accept, 2 Metropolis reject, 3 drain
  * accept, 4 drain reject) and the Coulomb energy change used. */

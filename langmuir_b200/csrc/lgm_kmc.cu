@@ -46,11 +46,13 @@ constexpr int E_DRAIN_L = 3, E_DRAIN_R = 4, H_DRAIN_L = 2, H_DRAIN_R = 3;
 // Outcomes (same codes as the oracle).
 enum : int32_t { O_OCCUPIED = 0, O_MET_ACCEPT = 1, O_MET_REJECT = 2, O_DRAIN_ACCEPT = 3,
                  O_DRAIN_REJECT = 4 };
-// Device counters: 16 flux (attempts, successes) + proposals + accepted + guard.
-enum { C_PROPOSALS = 16, C_ACCEPTED = 17, C_GUARD = 18, C_NUM = 19 };
+// Device counters: 20 flux (attempts, successes) + proposals + accepted + guard.
+enum { C_XSRC = 16, C_RECOMB = 18, C_PROPOSALS = 20, C_ACCEPTED = 21, C_GUARD = 22, C_NUM = 23 };
 // Device ints.
 enum { I_NE = 0, I_NH, I_STEP, I_NFLAG, I_REMOVED, I_NE0, I_NH0, I_NCHUNK, I_TPHYS, I_TPAD,
-       I_NUM };
+       I_NBONDS, I_NUM };
+// Recombination and exciton-source purposes of the random stream.
+constexpr uint32_t RNG_RECOMB = 5, RNG_EXCITON = RNG_SOURCE + 4;
 
 // Guard band: FP32C potentials carry at most (2 ulp rsqrt + 31 u run sums)
 // ~ 2.1e-6 N of error each; a decision whose energy lies within kGuard*(N_c +
@@ -91,6 +93,15 @@ struct Dev {
     int src_cap;   // source records capacity (multiple of CH)
     int tpad_cap;  // per-term target block capacity
     unsigned* err;
+    // solar-cell set-up
+    int solar, rec_range, confine, gen_iface;
+    double gen_rate, rec_rate;
+    uint8_t* phase;       // donor 0 / acceptor 1 per site (extensions)
+    int32_t* bonds;       // donor, acceptor site pairs
+    int32_t* h_at;        // hole index at a site, -1 elsewhere (recombination)
+    int32_t* rclaim;      // per hole: lowest successful recombining electron
+    int32_t* e_rch;       // per electron: chosen hole, -1 if none
+    uint8_t *e_rm, *h_rm; // removed by recombination this step
 };
 
 // ---- lattice helpers (cubicgrid.cpp:132-165, 207-471) ---------------------------
@@ -104,13 +115,13 @@ __device__ __forceinline__ int sidx(const Dev& D, int x, int y, int z) {
 }
 
 // Grid::neighborsSite in the reference's push order, then the face drains.
-__device__ int neighbors(const Dev& D, int site, bool electron, int* nb) {
+__device__ int neighbors(const Dev& D, int site, bool electron, int* nb, int range) {
     int x, y, z;
     xyz(D, site, x, y, z);
     const int X = D.X, Y = D.Y, Z = D.Z;
     int n = 0;
     auto S = [&](int a, int b, int c) { nb[n++] = sidx(D, a, b, c); };
-    if (D.hr == 1) {
+    if (range == 1) {
         if (x > 0) S(x - 1, y, z);
         if (x < X - 1) S(x + 1, y, z);
         if (y > 0) S(x, y - 1, z);
@@ -169,9 +180,10 @@ __device__ __forceinline__ void choose_body(const Dev& D, const int i) {
     if (i >= ne + nh) return;
     const bool e = i < ne;
     const int k = e ? i : i - ne;
+    (e ? D.e_rm : D.h_rm)[k] = 0;
     const int site = e ? D.e_site[k] : D.h_site[k];
     int nb[40];
-    const int n = neighbors(D, site, e, nb);
+    const int n = neighbors(D, site, e, nb, D.hr);
     const Philox4 r = draw(D, step, (uint32_t)k, e ? RNG_CHOOSE_E : RNG_CHOOSE_H);
     const int f = nb[uint_below(r.w[0], (uint32_t)n)];
     (e ? D.e_f : D.h_f)[k] = f;
@@ -276,7 +288,9 @@ __device__ __forceinline__ void decide_body(const Dev& D, const int i) {
     const int k = e ? i : i - ne;
     const int site = e ? D.e_site[k] : D.h_site[k];
     int f = e ? D.e_f[k] : D.h_f[k];
-    const uint8_t type = (e ? D.et : D.ht)[f];
+    uint8_t type = (e ? D.et : D.ht)[f];
+    // extension: a carrier may not enter the other phase (treated as occupied)
+    if (D.confine && f < D.V && type == T_EMPTY && D.phase[f] != (e ? 1 : 0)) type = T_DEFECT;
     const double q = e ? -1.0 : 1.0;
     int32_t out = O_OCCUPIED;
     uint8_t acc = 0;
@@ -408,6 +422,7 @@ __device__ __forceinline__ void claim_body(const Dev& D, const int i) {
     if (i >= ne + nh || !D.accept[i]) return;
     const bool e = i < ne;
     const int k = e ? i : i - ne;
+    if ((e ? D.e_rm : D.h_rm)[k]) return;  // recombined: completeTick only unregisters
     const int f = e ? D.e_f[k] : D.h_f[k];
     if (f < D.V) atomicMin(&(e ? D.claim_e : D.claim_h)[f], k);
 }
@@ -418,7 +433,15 @@ __device__ __forceinline__ void move_body(const Dev& D, const int i) {
     unsigned long long moved = 0, props = 0;
     if (i < ne + nh) {
         props = 1;
-        if (D.accept[i]) {
+        const bool e0 = i < ne;
+        const int k0 = e0 ? i : i - ne;
+        if ((e0 ? D.e_rm : D.h_rm)[k0]) {
+            // recombined: leave the lattice (chargeagent.cpp:166-170)
+            int32_t* sites = e0 ? D.e_site : D.h_site;
+            (e0 ? D.et : D.ht)[sites[k0]] = T_EMPTY;
+            sites[k0] = -1;
+            D.cnt[I_REMOVED] = 1;
+        } else if (D.accept[i]) {
             const bool e = i < ne;
             const int k = e ? i : i - ne;
             int32_t* sites = e ? D.e_site : D.h_site;
@@ -454,8 +477,57 @@ __device__ __forceinline__ void unclaim_body(const Dev& D, const int i) {
     if (i >= ne + nh || !D.accept[i]) return;
     const bool e = i < ne;
     const int k = e ? i : i - ne;
+    if ((e ? D.e_rm : D.h_rm)[k]) return;
     const int f = e ? D.e_f[k] : D.h_f[k];
     if (f < D.V) (e ? D.claim_e : D.claim_h)[f] = INT_MAX;
+}
+
+// RecombinationAgent::tryToAccept for every electron (drainagent.cpp:113-214).
+// The reference walks the electrons in list order and skips a hole already
+// removed by an earlier electron; here every electron draws its candidate and
+// its acceptance from its own counter, and the lowest-index successful electron
+// of each hole is the one that removes it -- the same outcome.
+__device__ __forceinline__ void hmap_body(const Dev& D, const int k, const bool set) {
+    if (k < D.cnt[I_NH0]) D.h_at[D.h_site[k]] = set ? k : -1;
+}
+
+__device__ __forceinline__ void recomb_propose_body(const Dev& D, const int i) {
+    const int ne = D.cnt[I_NE0];
+    if (i >= ne) return;
+    D.e_rch[i] = -1;
+    const int site = D.e_site[i];
+    int cand[48];
+    int n = 0;
+    if (D.ht[site] == T_HOLE) cand[n++] = site;
+    if (D.rec_range > 0) {
+        int nb[40];
+        const int m = neighbors(D, site, true, nb, D.rec_range);
+        for (int j = 0; j < m; ++j)
+            if (D.ht[nb[j]] == T_HOLE) cand[n++] = nb[j];
+    }
+    if (n == 0) return;
+    const Philox4 r = draw(D, (uint32_t)D.cnt[I_STEP], (uint32_t)i, RNG_RECOMB);
+    const int hk = D.h_at[cand[uint_below(r.w[0], (uint32_t)n)]];
+    D.e_rch[i] = hk;
+    if (D.rec_rate > unit_double(r.w[1], r.w[2])) atomicMin(&D.rclaim[hk], i);
+}
+
+__device__ __forceinline__ void recomb_resolve_body(const Dev& D, const int i) {
+    if (i >= D.cnt[I_NE0]) return;
+    const int hk = D.e_rch[i];
+    if (hk < 0) return;
+    const int w = D.rclaim[hk];
+    if (w == INT_MAX || i <= w) atomicAdd(&D.ctr[C_RECOMB], 1ull);  // hole still there
+    if (i == w) {
+        atomicAdd(&D.ctr[C_RECOMB + 1], 1ull);
+        D.e_rm[i] = 1;
+        D.h_rm[hk] = 1;
+    }
+}
+
+__device__ __forceinline__ void recomb_reset_body(const Dev& D, const int i) {
+    if (i < D.cnt[I_NE0] && D.e_rch[i] >= 0) D.rclaim[D.e_rch[i]] = INT_MAX;
+    hmap_body(D, i, false);
 }
 
 // Stable removal of drained carriers (Simulation::nextTick removeAt), then the
@@ -494,6 +566,33 @@ __device__ __forceinline__ void compact_inject_body(const Dev& D, int* warp_sums
     }
     if (threadIdx.x != 0) return;
     const uint32_t step = (uint32_t)D.cnt[I_STEP];
+    if (D.solar) {
+        // ExcitonSourceAgent::tryToInject (sourceagent.cpp:92-103, 120-123, 234-250)
+        D.ctr[C_XSRC] += 1;
+        const Philox4 r = draw(D, step, 0u, RNG_EXCITON);
+        const int nb = D.cnt[I_NBONDS];
+        int es, hs;
+        if (D.gen_iface && nb > 0) {
+            const uint32_t b = uint_below(r.w[0], (uint32_t)nb);
+            hs = D.bonds[2 * b];
+            es = D.bonds[2 * b + 1];
+        } else {
+            es = hs = (int)uint_below(r.w[0], (uint32_t)D.V);
+        }
+        const bool valid = ne < D.cap_e && nh < D.cap_h && D.gen_rate > 0 &&
+                           D.et[es] == T_EMPTY && D.ht[hs] == T_EMPTY;
+        if (valid && D.gen_rate > unit_double(r.w[1], r.w[2])) {
+            D.ctr[C_XSRC + 1] += 1;
+            D.et[es] = T_ELECTRON;
+            D.ht[hs] = T_HOLE;
+            D.e_site[ne++] = es;
+            D.h_site[nh++] = hs;
+        }
+        D.cnt[I_NE] = ne;
+        D.cnt[I_NH] = nh;
+        D.cnt[I_STEP] = (int32_t)(step + 1);
+        return;
+    }
     for (int s = 0; s < 4; ++s) {
         const bool e = s < 2, left = (s % 2) == 0;
         D.ctr[2 * s] += 1;  // attempts (sourceagent.cpp:94)
@@ -527,6 +626,10 @@ __global__ void __launch_bounds__(kGuardThreads) k_guard(Dev D) {
     __shared__ double red[kGuardThreads];
     guard_body(D, blockIdx.x, gridDim.x, red);
 }
+__global__ void k_hmap(Dev D) { hmap_body(D, LGM_THREAD_INDEX, true); }
+__global__ void k_recomb_propose(Dev D) { recomb_propose_body(D, LGM_THREAD_INDEX); }
+__global__ void k_recomb_resolve(Dev D) { recomb_resolve_body(D, LGM_THREAD_INDEX); }
+__global__ void k_recomb_reset(Dev D) { recomb_reset_body(D, LGM_THREAD_INDEX); }
 __global__ void k_claim(Dev D) { claim_body(D, LGM_THREAD_INDEX); }
 __global__ void k_move(Dev D) { move_body(D, LGM_THREAD_INDEX); }
 __global__ void k_unclaim(Dev D) { unclaim_body(D, LGM_THREAD_INDEX); }
@@ -556,6 +659,18 @@ __global__ void __launch_bounds__(kGuardThreads) kb_guard(const Dev* R, int bloc
     __shared__ double red[kGuardThreads];
     guard_body(R[blockIdx.x / blocks_per_replica], blockIdx.x % blocks_per_replica,
                blocks_per_replica, red);
+}
+__global__ void kb_hmap(const Dev* R, const int2* map) {
+    const int2 m = map[blockIdx.x]; hmap_body(R[m.x], LGM_BATCH_INDEX(m), true);
+}
+__global__ void kb_recomb_propose(const Dev* R, const int2* map) {
+    const int2 m = map[blockIdx.x]; recomb_propose_body(R[m.x], LGM_BATCH_INDEX(m));
+}
+__global__ void kb_recomb_resolve(const Dev* R, const int2* map) {
+    const int2 m = map[blockIdx.x]; recomb_resolve_body(R[m.x], LGM_BATCH_INDEX(m));
+}
+__global__ void kb_recomb_reset(const Dev* R, const int2* map) {
+    const int2 m = map[blockIdx.x]; recomb_reset_body(R[m.x], LGM_BATCH_INDEX(m));
 }
 __global__ void kb_claim(const Dev* R, const int2* map) {
     const int2 m = map[blockIdx.x]; claim_body(R[m.x], LGM_BATCH_INDEX(m));
@@ -787,6 +902,12 @@ lgm_status enqueue_step(lgm_kmc* k) {
     }
     k_decide<<<(nc + blk - 1) / blk, blk, 0, st>>>(D);
     if (D.coulomb) k_guard<<<2 * 148, kGuardThreads, 0, st>>>(D);
+    if (D.solar && D.rec_rate > 0) {
+        k_hmap<<<(nc + blk - 1) / blk, blk, 0, st>>>(D);
+        k_recomb_propose<<<(nc + blk - 1) / blk, blk, 0, st>>>(D);
+        k_recomb_resolve<<<(nc + blk - 1) / blk, blk, 0, st>>>(D);
+        k_recomb_reset<<<(nc + blk - 1) / blk, blk, 0, st>>>(D);
+    }
     k_claim<<<(nc + blk - 1) / blk, blk, 0, st>>>(D);
     k_move<<<(nc + blk - 1) / blk, blk, 0, st>>>(D);
     k_unclaim<<<(nc + blk - 1) / blk, blk, 0, st>>>(D);
@@ -816,8 +937,11 @@ lgm_status lgm_kmc_create(const lgm_params* pin, int32_t device, uint32_t replic
     g_kmc_create_error.clear();
     if (s != LGM_OK) return bail(s, msg);
     const lgm_params& p = k->p;
-    if (std::string(p.simulation_type) != "transistor" || p.source_metropolis)
-        return bail(LGM_ERR_UNSUPPORTED, "only the transistor set-up without source.metropolis");
+    if (p.source_metropolis || p.balance_charges)
+        return bail(LGM_ERR_UNSUPPORTED, "source.metropolis and balance.charges are not supported");
+    if (p.recombination_range < 0 || p.recombination_range > 2)
+        return bail(LGM_ERR_INVALID_ARGUMENT, "langmuir: recombination.range must be 0, 1 or 2");
+    const bool solar = std::string(p.simulation_type) == "solarcell";
     if (p.hopping_range < 1) return bail(LGM_ERR_UNSUPPORTED, "hopping.range 0 has no moves");
     const long long L = std::max<long long>({2LL * p.grid_x, p.grid_y, p.grid_z + 1});
     if (6 * L * L >= (1LL << 22)) return bail(LGM_ERR_UNSUPPORTED, "lattice too large");
@@ -854,18 +978,41 @@ lgm_status lgm_kmc_create(const lgm_params* pin, int32_t device, uint32_t replic
                 }
         D.coupling[0] = 0.0;
     }
-    // World::createSources/createDrains rates, transistor (world.cpp:990-1000, 1116-1124)
+    // World::createSources/createDrains rates (world.cpp:982-1030, 1110-1150)
     auto smart = [](double r, double dflt) { return r < 0 ? dflt : r; };
-    D.rate_src[0] = smart(p.e_source_l_rate, p.source_rate);
-    D.rate_src[1] = smart(p.e_source_r_rate, 0.0);
-    D.rate_src[2] = smart(p.h_source_l_rate, 0.0);
-    D.rate_src[3] = smart(p.h_source_r_rate, 0.0);
-    D.rate_drain[0] = smart(p.e_drain_l_rate, 0.0);
-    D.rate_drain[1] = smart(p.e_drain_r_rate, p.drain_rate);
-    D.rate_drain[2] = smart(p.h_drain_l_rate, 0.0);
-    D.rate_drain[3] = smart(p.h_drain_r_rate, 0.0);
+    D.solar = solar;
+    if (!solar) {
+        D.rate_src[0] = smart(p.e_source_l_rate, p.source_rate);
+        D.rate_src[1] = smart(p.e_source_r_rate, 0.0);
+        D.rate_src[2] = smart(p.h_source_l_rate, 0.0);
+        D.rate_src[3] = smart(p.h_source_r_rate, 0.0);
+        D.rate_drain[0] = smart(p.e_drain_l_rate, 0.0);
+        D.rate_drain[1] = smart(p.e_drain_r_rate, p.drain_rate);
+        D.rate_drain[2] = smart(p.h_drain_l_rate, 0.0);
+        D.rate_drain[3] = smart(p.h_drain_r_rate, 0.0);
+        D.gen_rate = 0.0;
+        D.rec_rate = 0.0;
+    } else {
+        D.rate_src[0] = smart(p.e_source_l_rate, 0.0);
+        D.rate_src[1] = smart(p.e_source_r_rate, 0.0);
+        D.rate_src[2] = smart(p.h_source_l_rate, 0.0);
+        D.rate_src[3] = smart(p.h_source_r_rate, 0.0);
+        D.rate_drain[0] = smart(p.e_drain_l_rate, p.drain_rate);
+        D.rate_drain[1] = smart(p.e_drain_r_rate, p.drain_rate);
+        D.rate_drain[2] = smart(p.h_drain_l_rate, p.drain_rate);
+        D.rate_drain[3] = smart(p.h_drain_r_rate, p.drain_rate);
+        D.gen_rate = smart(p.generation_rate, p.source_rate);
+        const double area = (double)p.grid_x * p.grid_y;
+        if (p.source_scale_area > 0 && p.source_scale_area != area)
+            D.gen_rate *= area / p.source_scale_area;
+        D.rec_rate = p.recombination_rate;
+    }
+    D.rec_range = p.recombination_range;
+    D.confine = p.morphology_confine;
+    D.gen_iface = p.generation_interface;
     // createSources / createDrains sanity checks (world.cpp:1032-1068, 1158-1186)
-    if (D.rate_src[0] == 0 && D.rate_src[1] == 0 && D.rate_src[2] == 0 && D.rate_src[3] == 0)
+    if (D.rate_src[0] == 0 && D.rate_src[1] == 0 && D.rate_src[2] == 0 && D.rate_src[3] == 0 &&
+        D.gen_rate == 0)
         return bail(LGM_ERR_INVALID_ARGUMENT, "langmuir: all sources have zero rate");
     if (k->max_e == 0 && (D.rate_src[0] > 0 || D.rate_src[1] > 0))
         return bail(LGM_ERR_INVALID_ARGUMENT,
@@ -873,12 +1020,16 @@ lgm_status lgm_kmc_create(const lgm_params* pin, int32_t device, uint32_t replic
     if (k->max_h == 0 && (D.rate_src[2] > 0 || D.rate_src[3] > 0))
         return bail(LGM_ERR_INVALID_ARGUMENT,
                     "langmuir: a hole source rate > 0, yet maxHoleAgents() == 0");
-    if (D.rate_drain[0] == 0 && D.rate_drain[1] == 0 && D.rate_drain[2] == 0 && D.rate_drain[3] == 0)
+    if (k->max_e == 0 && D.gen_rate > 0)
+        return bail(LGM_ERR_INVALID_ARGUMENT,
+                    "langmuir: generation.rate > 0, yet maxElectronAgents() == 0");
+    if (D.rate_drain[0] == 0 && D.rate_drain[1] == 0 && D.rate_drain[2] == 0 &&
+        D.rate_drain[3] == 0 && D.rec_rate == 0)
         return bail(LGM_ERR_INVALID_ARGUMENT, "langmuir: all drains have zero rate");
-    if (k->max_e > 0 && D.rate_drain[0] <= 0 && D.rate_drain[1] <= 0)
+    if (k->max_e > 0 && D.rate_drain[0] <= 0 && D.rate_drain[1] <= 0 && D.rec_rate <= 0)
         return bail(LGM_ERR_INVALID_ARGUMENT,
                     "langmuir: all electron drain rates are zero, yet maxElectronAgents() > 0");
-    if (k->max_h > 0 && D.rate_drain[2] <= 0 && D.rate_drain[3] <= 0)
+    if (k->max_h > 0 && D.rate_drain[2] <= 0 && D.rate_drain[3] <= 0 && D.rec_rate <= 0)
         return bail(LGM_ERR_INVALID_ARGUMENT,
                     "langmuir: all hole drain rates are zero, yet maxHoleAgents() > 0");
     D.coulomb = p.coulomb_carriers;
@@ -914,6 +1065,13 @@ lgm_status lgm_kmc_create(const lgm_params* pin, int32_t device, uint32_t replic
     DA(D.part, (size_t)D.splits * tphys_cap); DA(D.part_norm, (size_t)D.splits * tphys_cap);
     DA(D.Vt, 2 * ncap); DA(D.Nt, 2 * ncap);
     DA(D.err, 1);
+    DA(D.phase, k->V);
+    DA(D.bonds, (D.gen_iface ? 12 * (size_t)k->V : 2));
+    DA(D.h_at, k->V);
+    DA(D.rclaim, std::max(D.cap_h, 1));
+    DA(D.e_rch, std::max(D.cap_e, 1));
+    DA(D.e_rm, std::max(D.cap_e, 1));
+    DA(D.h_rm, std::max(D.cap_h, 1));
 #undef DA
     if (D.gauss) {
         // erf(f sqrt(k))/sqrt(k) where it differs from 1/sqrt(k) in FP32; NaN past it
@@ -938,6 +1096,11 @@ lgm_status lgm_kmc_create(const lgm_params* pin, int32_t device, uint32_t replic
     std::vector<int32_t> claims(k->V, INT_MAX);
     cudaMemcpy(D.claim_e, claims.data(), sizeof(int32_t) * k->V, cudaMemcpyHostToDevice);
     cudaMemcpy(D.claim_h, claims.data(), sizeof(int32_t) * k->V, cudaMemcpyHostToDevice);
+    cudaMemcpy(D.rclaim, claims.data(), sizeof(int32_t) * std::max(D.cap_h, 1), cudaMemcpyHostToDevice);
+    cudaMemset(D.h_at, 0xff, sizeof(int32_t) * k->V);  // -1
+    cudaMemset(D.phase, 0, k->V);
+    cudaMemset(D.e_rm, 0, std::max(D.cap_e, 1));
+    cudaMemset(D.h_rm, 0, std::max(D.cap_h, 1));
     cudaMemset(D.cnt, 0, sizeof(int32_t) * I_NUM);
     cudaMemset(D.ctr, 0, sizeof(unsigned long long) * C_NUM);
     cudaMemset(D.err, 0, sizeof(unsigned));
@@ -1007,7 +1170,7 @@ lgm_status lgm_kmc_stats_get(lgm_kmc* k, lgm_kmc_stats* s) {
     s->proposals = ctr[C_PROPOSALS];
     s->accepted = ctr[C_ACCEPTED];
     s->guard_evaluations = ctr[C_GUARD];
-    for (int i = 0; i < 16; ++i) s->counters[i] = ctr[i];
+    for (int i = 0; i < 20; ++i) s->counters[i] = ctr[i];
     return LGM_OK;
 }
 
@@ -1044,6 +1207,39 @@ lgm_status lgm_kmc_get_world(lgm_kmc* k, double* pot, int32_t* defects, int32_t 
         if (traps) std::memcpy(traps, k->traps.data(), sizeof(int32_t) * k->traps.size());
         if (trap_pots) std::memcpy(trap_pots, k->trap_pots.data(), sizeof(double) * k->traps.size());
     }
+    return LGM_OK;
+}
+
+lgm_status lgm_kmc_set_morphology(lgm_kmc* k, const uint8_t* phase) {
+    if (!k || !phase) return LGM_ERR_INVALID_ARGUMENT;
+    KCUDA(k, cudaSetDevice(k->device));
+    KCUDA(k, cudaStreamSynchronize(k->stream));
+    const Dev& D = k->D;
+    for (int s = 0; s < k->V; ++s)
+        if (phase[s] > 1) return kfail(k, LGM_ERR_INVALID_ARGUMENT, "phase values must be 0 or 1");
+    KCUDA(k, cudaMemcpy(D.phase, phase, k->V, cudaMemcpyHostToDevice));
+    int32_t nb = 0;
+    if (D.gen_iface) {
+        // donor-acceptor bonds, from each donor site in site order over its
+        // range-1 lattice neighbours in the order of Grid::neighborsSite
+        std::vector<int32_t> bonds;
+        const int X = D.X, Y = D.Y, Z = D.Z;
+        for (int s = 0; s < k->V; ++s) {
+            if (phase[s] != 0) continue;
+            const int z = s / D.XY, y = s / X - z * Y, x = s % X;
+            const int cand[6][3] = {{x - 1, y, z}, {x + 1, y, z}, {x, y - 1, z},
+                                    {x, y + 1, z}, {x, y, z - 1}, {x, y, z + 1}};
+            for (const auto& c : cand) {
+                if (c[0] < 0 || c[0] >= X || c[1] < 0 || c[1] >= Y || c[2] < 0 || c[2] >= Z) continue;
+                const int t = X * (c[1] + c[2] * Y) + c[0];
+                if (phase[t] == 1) { bonds.push_back(s); bonds.push_back(t); }
+            }
+        }
+        nb = (int32_t)(bonds.size() / 2);
+        if (nb) KCUDA(k, cudaMemcpy(D.bonds, bonds.data(), sizeof(int32_t) * bonds.size(),
+                                    cudaMemcpyHostToDevice));
+    }
+    KCUDA(k, cudaMemcpy(D.cnt + I_NBONDS, &nb, sizeof nb, cudaMemcpyHostToDevice));
     return LGM_OK;
 }
 
@@ -1096,6 +1292,7 @@ struct lgm_kmc_batch {
     int device = 0;
     int gauss = 0;
     int coulomb = 0;
+    int recomb = 0;
     cudaStream_t stream = nullptr;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
@@ -1182,6 +1379,12 @@ lgm_status enqueue_batch_step(lgm_kmc_batch* b) {
     }
     kb_decide<<<b->nb_car, 256, 0, st>>>(b->d_reps, b->map_car);
     if (b->coulomb) kb_guard<<<2 * R, kGuardThreads, 0, st>>>(b->d_reps, 2);
+    if (b->recomb) {
+        kb_hmap<<<b->nb_car, 256, 0, st>>>(b->d_reps, b->map_car);
+        kb_recomb_propose<<<b->nb_car, 256, 0, st>>>(b->d_reps, b->map_car);
+        kb_recomb_resolve<<<b->nb_car, 256, 0, st>>>(b->d_reps, b->map_car);
+        kb_recomb_reset<<<b->nb_car, 256, 0, st>>>(b->d_reps, b->map_car);
+    }
     kb_claim<<<b->nb_car, 256, 0, st>>>(b->d_reps, b->map_car);
     kb_move<<<b->nb_car, 256, 0, st>>>(b->d_reps, b->map_car);
     kb_unclaim<<<b->nb_car, 256, 0, st>>>(b->d_reps, b->map_car);
@@ -1253,6 +1456,7 @@ lgm_status lgm_kmc_batch_create(const lgm_params* params, int32_t count, int32_t
     // one interaction kind and one cutoff-table layout per batch
     b->gauss = b->reps[0]->D.gauss;
     b->coulomb = b->reps[0]->D.coulomb;
+    for (lgm_kmc* k : b->reps) b->recomb |= (k->D.solar && k->D.rec_rate > 0);
     for (lgm_kmc* k : b->reps)
         if (k->D.gauss != b->gauss || k->D.coulomb != b->coulomb)
             return bail(LGM_ERR_UNSUPPORTED,

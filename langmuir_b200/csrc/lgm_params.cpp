@@ -102,6 +102,8 @@ const Key kKeys[] = {
     KC("simulation.start", K_STR64, output_stub),  // constant: never written
     K("image.charges", K_I32, image_charges),
     K("site.disorder", K_F64, site_disorder),
+    K("morphology.confine", K_BOOL, morphology_confine),
+    K("generation.interface", K_BOOL, generation_interface),
 };
 
 void set_err(char* err, int len, const std::string& m) {
@@ -359,6 +361,8 @@ lgm_status lgm_params_check(lgm_params* p, char* err, int32_t err_len) {
     if (p->output_ids_on_encounter) return bad("output.ids.on.encouter is deprecated");
     if (p->image_charges < 0 || p->image_charges > 3) return bad("image.charges must be 0..3");
     if (p->site_disorder < 0) return bad("site.disorder < 0");
+    if (p->generation_interface && st != "solarcell")
+        return bad("generation.interface == true, yet simulation.type != solarcell");
     return LGM_OK;
 }
 

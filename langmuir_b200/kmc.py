@@ -53,6 +53,7 @@ class Params(ctypes.Structure):
         ("elementary_charge", _f64), ("permittivity_space", _f64), ("grid_factor", _f64),
         ("electrostatic_cutoff", _i32), ("electrostatic_prefactor", _f64), ("inverse_kt", _f64),
         ("image_charges", _i32), ("site_disorder", _f64),
+        ("morphology_confine", _i32), ("generation_interface", _i32),
     ]
 
     @classmethod
@@ -94,7 +95,7 @@ class Stats(ctypes.Structure):
     _fields_ = [("step", ctypes.c_uint32), ("electrons", _i32), ("holes", _i32),
                 ("max_electrons", _i32), ("max_holes", _i32), ("defects", _i32),
                 ("traps", _i32), ("proposals", ctypes.c_uint64), ("accepted", ctypes.c_uint64),
-                ("guard_evaluations", ctypes.c_uint64), ("counters", ctypes.c_uint64 * 16)]
+                ("guard_evaluations", ctypes.c_uint64), ("counters", ctypes.c_uint64 * 20)]
 
 
 _vp = ctypes.c_void_p
@@ -116,12 +117,15 @@ N.SIGNATURES.update({
     "lgm_kmc_set_carriers": (_i32, [_vp, _i32p, _i32, _i32p, _i32]),
     "lgm_kmc_get_world": (_i32, [_vp, _vp, _vp, _i32, _vp, _vp, _i32]),
     "lgm_kmc_last_outcomes": (_i32, [_vp, _vp, _vp, _i32]),
+    "lgm_kmc_set_morphology": (_i32, [_vp, np.ctypeslib.ndpointer(dtype=np.uint8,
+                                                                  flags="C_CONTIGUOUS")]),
 })
 if N._lib is not None:  # bind the new symbols if the library was already loaded
     for _name in ("lgm_params_default", "lgm_params_size", "lgm_params_parse",
                   "lgm_params_check", "lgm_kmc_create", "lgm_kmc_destroy", "lgm_kmc_last_error",
                   "lgm_kmc_run", "lgm_kmc_stats_get", "lgm_kmc_get_carriers",
-                  "lgm_kmc_set_carriers", "lgm_kmc_get_world", "lgm_kmc_last_outcomes"):
+                  "lgm_kmc_set_carriers", "lgm_kmc_get_world", "lgm_kmc_last_outcomes",
+                  "lgm_kmc_set_morphology"):
         _fn = getattr(N._lib, _name)
         _fn.restype, _fn.argtypes = N.SIGNATURES[_name]
 
@@ -190,6 +194,13 @@ class KMC:
                                               t.ctypes.data, tp.ctypes.data, len(t)))
         return dict(site_energy=pot, defects=d[: s["defects"]].copy(),
                     traps=t[: s["traps"]].copy(), trap_potentials=tp[: s["traps"]].copy())
+
+    def set_morphology(self, phase):
+        """phase[site]: 0 donor, 1 acceptor (x fastest, then y, then z)."""
+        ph = np.ascontiguousarray(np.asarray(phase).reshape(-1), dtype=np.uint8)
+        if ph.size != self.volume:
+            raise ValueError("phase must have one entry per lattice site")
+        self._check(N.lib().lgm_kmc_set_morphology(self._h, ph))
 
     def last_outcomes(self, n):
         o = np.zeros(max(n, 1), np.int32)

@@ -141,6 +141,18 @@ typedef struct orc_kmc_config {
     double rate_e_drain_l, rate_e_drain_r, rate_h_drain_l, rate_h_drain_r;
     int32_t max_electrons, max_holes;
     uint32_t seed, replica;     /* Philox key                                    */
+    /* solar-cell set-up (simulation.cpp:219-243): exciton source at
+     * generation_rate (already scaled by the plane area), recombination */
+    int32_t solar;
+    double generation_rate, recombination_rate;
+    int32_t recombination_range, hopping_range_neighbors;  /* the latter: hopping.range */
+    /* extensions: phase[site] (0 donor, 1 acceptor); confine: holes only on
+     * donor and electrons only on acceptor sites; bonds (donor, acceptor site
+     * pairs): excitons generated across a random bond instead of at one site */
+    const uint8_t* phase;
+    int32_t confine;
+    const int32_t* bonds;
+    int32_t nbonds;
 } orc_kmc_config;
 
 /* decideFuture outcomes per carrier */
@@ -149,9 +161,9 @@ enum orc_outcome { ORC_OCCUPIED = 0, ORC_MET_ACCEPT = 1, ORC_MET_REJECT = 2,
 
 /* Advance one step.  pot: site energies (volume entries); defects: nd sites.
  * e_site/h_site: in/out carrier lists in list order (capacity max_electrons /
- * max_holes), with their lengths in ne_io and nh_io.  counters: 16 uint64, (attempts,
+ * max_holes), with their lengths in ne_io and nh_io.  counters: 20 uint64, (attempts,
  * successes) of eSourceL, eSourceR, hSourceL, hSourceR, eDrainL, eDrainR,
- * hDrainL, hDrainR.  outcome / de_out (optional): per carrier of the lists as
+ * hDrainL, hDrainR, the exciton source and the recombination agent.  outcome / de_out (optional): per carrier of the lists as
  * they were at the start of the step, electrons then holes. */
 int orc_kmc_step(const orc_ctx* ctx, const orc_kmc_config* cfg, const double* pot,
                  const int32_t* defects, int nd, uint32_t step, int32_t* e_site, int32_t* ne_io,

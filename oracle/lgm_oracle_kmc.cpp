@@ -15,7 +15,9 @@
 // be compared bit for bit.  Layout (shared with langmuir_b200/csrc/lgm_rng.cuh):
 //   key = {seed, replica},  counter = {step, index, purpose, 0}
 //   purpose 1/2: choose/decide of electron `index`, 3/4: of hole `index`,
-//   16 + k: electrode source k (0 eL, 1 eR, 2 hL, 3 hR), index 0.
+//   5: recombination of electron `index` (w0: candidate, (w1, w2): accept),
+//   16 + k: electrode source k (0 eL, 1 eR, 2 hL, 3 hR), 20: exciton source,
+//   index 0.
 //   integer in [0, n): (w0 * n) >> 32;  uniform [0,1): ((w_a >> 5) 2^26 + (w_b >> 6)) / 2^53
 //   with (a, b) = (0, 1) for decisions and (1, 2) for sources.
 #include <cmath>
@@ -126,7 +128,11 @@ extern "C" int orc_kmc_step(const orc_ctx* ctx, const orc_kmc_config* k, const d
     auto decide = [&](int site, int32_t& fsite, bool electron, uint32_t index, int32_t* code) {
         const std::vector<uint8_t>& own = electron ? et : ht;
         const int q = electron ? -1 : 1;
-        const uint8_t type = own[fsite];
+        uint8_t type = own[fsite];
+        // extension: a carrier may not enter the other phase (treated as occupied)
+        if (k->confine && k->phase && fsite < V && type == ORC_EMPTY &&
+            k->phase[fsite] != (electron ? 1 : 0))
+            type = ORC_DEFECT;
         if (type == ORC_EMPTY) {
             double pd = pot[fsite] - pot[site];
             pd *= q;
@@ -173,13 +179,52 @@ extern "C" int orc_kmc_step(const orc_ctx* ctx, const orc_kmc_config* k, const d
     for (int i = 0; i < nh; ++i) decide(h_site[i], hf[i], false, (uint32_t)i, &codes[ne + i]);
     if (outcome) std::memcpy(outcome, codes.data(), sizeof(int32_t) * (ne + nh));
 
+    // performRecombinations (simulation.cpp:219-231), RecombinationAgent::tryToAccept
+    // (drainagent.cpp:113-214) for every electron in list order.
+    std::vector<uint8_t> e_rm(ne, 0), h_rm(nh, 0);
+    if (k->solar && k->recombination_rate > 0) {
+        std::vector<int32_t> h_at(V + 35, -1);
+        for (int i = 0; i < nh; ++i) h_at[h_site[i]] = i;
+        int rb[48];
+        for (int i = 0; i < ne; ++i) {
+            const int site = e_site[i];
+            int n = 0;
+            if (ht[site] == ORC_HOLE) rb[n++] = site;
+            if (k->recombination_range > 0) {
+                int nb2[40];
+                int m = orc_neighbors(ctx, site, k->recombination_range, nb2);
+                const int x = orc_index_x(ctx, site);
+                // the electron's neighbour list carries its face drains too
+                if (x == 0) nb2[m++] = V + E_DRAIN_L;
+                if (x == GX - 1) nb2[m++] = V + E_DRAIN_R;
+                for (int j = 0; j < m; ++j)
+                    if (ht[nb2[j]] == ORC_HOLE) rb[n++] = nb2[j];
+            }
+            if (n == 0) continue;
+            const Draw d = draw(k, step, (uint32_t)i, 5u);
+            const int hs = rb[uint_below(d.w[0], (uint32_t)n)];
+            const int hk = h_at[hs];
+            if (h_rm[hk]) continue;  // already recombined
+            counters[18] += 1;
+            if (k->recombination_rate > unit_double(d.w[1], d.w[2])) {
+                counters[19] += 1;
+                e_rm[i] = 1;
+                h_rm[hk] = 1;
+            }
+        }
+    }
+
     // nextTick: completeTick in list order, first mover wins, drains remove.
     auto tick = [&](int32_t* site, const int32_t* fs, int n, std::vector<uint8_t>& own,
-                    uint8_t mine) {
+                    uint8_t mine, const std::vector<uint8_t>& rm) {
         int w = 0;
         for (int i = 0; i < n; ++i) {
             int s = site[i];
             bool removed = false;
+            if (rm[i]) {  // completeTick: removed charges only leave (chargeagent.cpp:166-170)
+                own[s] = ORC_EMPTY;
+                continue;
+            }
             if (s != fs[i]) {
                 if (own[fs[i]] == ORC_EMPTY) {
                     own[s] = ORC_EMPTY;
@@ -194,8 +239,36 @@ extern "C" int orc_kmc_step(const orc_ctx* ctx, const orc_kmc_config* k, const d
         }
         return w;
     };
-    ne = tick(e_site, ef.data(), ne, et, ORC_ELECTRON);
-    nh = tick(h_site, hf.data(), nh, ht, ORC_HOLE);
+    ne = tick(e_site, ef.data(), ne, et, ORC_ELECTRON, e_rm);
+    nh = tick(h_site, hf.data(), nh, ht, ORC_HOLE, h_rm);
+
+    if (k->solar) {
+        // performInjections, solar (simulation.cpp:235-243): the exciton source,
+        // ExcitonSourceAgent::tryToInject (sourceagent.cpp:92-103, 120-123, 234-250).
+        counters[16] += 1;
+        const Draw d = draw(k, step, 0u, 20u);
+        int es, hs;
+        if (k->bonds && k->nbonds > 0) {
+            const uint32_t b = uint_below(d.w[0], (uint32_t)k->nbonds);
+            hs = k->bonds[2 * b];
+            es = k->bonds[2 * b + 1];
+        } else {
+            es = hs = (int)uint_below(d.w[0], (uint32_t)V);
+        }
+        const bool valid = ne < k->max_electrons && nh < k->max_holes &&
+                           k->generation_rate > 0 && et[es] == ORC_EMPTY && ht[hs] == ORC_EMPTY &&
+                           (k->bonds && k->nbonds > 0 ? true : ht[es] == ORC_EMPTY);
+        if (valid && k->generation_rate > unit_double(d.w[1], d.w[2])) {
+            counters[17] += 1;
+            et[es] = ORC_ELECTRON;
+            ht[hs] = ORC_HOLE;
+            e_site[ne++] = es;
+            h_site[nh++] = hs;
+        }
+        *ne_io = ne;
+        *nh_io = nh;
+        return 0;
+    }
 
     // performInjections, transistor (simulation.cpp:246-249): eL, eR, hL, hR.
     const double src_rate[4] = {k->rate_e_source_l, k->rate_e_source_r, k->rate_h_source_l,

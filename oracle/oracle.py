@@ -48,7 +48,12 @@ class KmcConfig(ctypes.Structure):
                 ("rate_e_drain_l", ctypes.c_double), ("rate_e_drain_r", ctypes.c_double),
                 ("rate_h_drain_l", ctypes.c_double), ("rate_h_drain_r", ctypes.c_double),
                 ("max_electrons", ctypes.c_int32), ("max_holes", ctypes.c_int32),
-                ("seed", ctypes.c_uint32), ("replica", ctypes.c_uint32)]
+                ("seed", ctypes.c_uint32), ("replica", ctypes.c_uint32),
+                ("solar", ctypes.c_int32), ("generation_rate", ctypes.c_double),
+                ("recombination_rate", ctypes.c_double), ("recombination_range", ctypes.c_int32),
+                ("hopping_range_neighbors", ctypes.c_int32),
+                ("phase", ctypes.c_void_p), ("confine", ctypes.c_int32),
+                ("bonds", ctypes.c_void_p), ("nbonds", ctypes.c_int32)]
 
 
 def lib():
@@ -238,9 +243,17 @@ class KmcOracle:
     """The oracle's kMC step on a world (site energies, defects, carriers)."""
 
     def __init__(self, orc: "Oracle", site_energy, defects, electrons, holes, cfg: KmcConfig,
-                 step=0):
+                 step=0, phase=None, bonds=None):
         self.orc = orc
         self.cfg = cfg
+        # keep the morphology arrays alive while the config points at them
+        self._phase = None if phase is None else np.ascontiguousarray(phase, dtype=np.uint8)
+        self._bonds = None if bonds is None else np.ascontiguousarray(bonds, dtype=np.int32)
+        if self._phase is not None:
+            cfg.phase = self._phase.ctypes.data
+        if self._bonds is not None and len(self._bonds):
+            cfg.bonds = self._bonds.ctypes.data
+            cfg.nbonds = len(self._bonds) // 2
         self.pot = np.ascontiguousarray(site_energy, dtype=np.float64)
         self.defects = np.ascontiguousarray(defects, dtype=np.int32)
         self.e = np.zeros(max(cfg.max_electrons, 1), np.int32)
@@ -249,7 +262,7 @@ class KmcOracle:
         self.nh = ctypes.c_int32(len(holes))
         self.e[: len(electrons)] = electrons
         self.h[: len(holes)] = holes
-        self.counters = np.zeros(16, np.uint64)
+        self.counters = np.zeros(20, np.uint64)
         self.step_no = int(step)
 
     def step(self, threads=0):

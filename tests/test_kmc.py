@@ -25,8 +25,23 @@ def make_params(**keys):
 
 
 def rates(p):
-    """World::createSources / createDrains, transistor (world.cpp:990-1000, 1116-1124)."""
+    """World::createSources / createDrains (world.cpp:982-1030, 1110-1150)."""
     smart = lambda r, d: d if r < 0 else r
+    if p.simulation_type == b"solarcell":
+        gen = smart(p.generation_rate, p.source_rate)
+        area = p.grid_x * p.grid_y
+        if p.source_scale_area > 0 and p.source_scale_area != area:
+            gen *= area / p.source_scale_area
+        return dict(rate_e_source_l=smart(p.e_source_l_rate, 0.0),
+                    rate_e_source_r=smart(p.e_source_r_rate, 0.0),
+                    rate_h_source_l=smart(p.h_source_l_rate, 0.0),
+                    rate_h_source_r=smart(p.h_source_r_rate, 0.0),
+                    rate_e_drain_l=smart(p.e_drain_l_rate, p.drain_rate),
+                    rate_e_drain_r=smart(p.e_drain_r_rate, p.drain_rate),
+                    rate_h_drain_l=smart(p.h_drain_l_rate, p.drain_rate),
+                    rate_h_drain_r=smart(p.h_drain_r_rate, p.drain_rate),
+                    solar=1, generation_rate=gen, recombination_rate=p.recombination_rate,
+                    recombination_range=p.recombination_range)
     return dict(rate_e_source_l=smart(p.e_source_l_rate, p.source_rate),
                 rate_e_source_r=smart(p.e_source_r_rate, 0.0),
                 rate_h_source_l=smart(p.h_source_l_rate, 0.0),
@@ -37,7 +52,34 @@ def rates(p):
                 rate_h_drain_r=smart(p.h_drain_r_rate, 0.0))
 
 
-def oracle_for(O, p, world, e, h, max_e, max_h, replica=0, step=0):
+def interface_bonds(phase, X, Y, Z):
+    """Donor-acceptor bonds in the order lgm_kmc_set_morphology lists them."""
+    bonds = []
+    for s in range(X * Y * Z):
+        if phase[s] != 0:
+            continue
+        z, y, x = s // (X * Y), (s // X) % Y, s % X
+        for (a, b, c) in ((x - 1, y, z), (x + 1, y, z), (x, y - 1, z), (x, y + 1, z),
+                          (x, y, z - 1), (x, y, z + 1)):
+            if 0 <= a < X and 0 <= b < Y and 0 <= c < Z:
+                t = X * (b + c * Y) + a
+                if phase[t] == 1:
+                    bonds += [s, t]
+    return np.array(bonds, dtype=np.int32)
+
+
+def blob_phase(X, Y, Z, seed):
+    """A seeded two-phase morphology: smoothed noise thresholded at its median."""
+    rng = np.random.default_rng(seed)
+    f = rng.normal(size=(Z, Y, X))
+    for _ in range(3):
+        for ax in range(3):
+            if f.shape[ax] > 1:
+                f = (f + np.roll(f, 1, ax) + np.roll(f, -1, ax)) / 3
+    return (f > np.median(f)).astype(np.uint8).reshape(-1)
+
+
+def oracle_for(O, p, world, e, h, max_e, max_h, replica=0, step=0, phase=None):
     q = L.Params.from_text("[Parameters]\n")  # fresh copy for the derived constants
     for name, _ in L.Params._fields_:
         setattr(q, name, getattr(p, name))
@@ -50,7 +92,13 @@ def oracle_for(O, p, world, e, h, max_e, max_h, replica=0, step=0):
                       image_terms=(2 if q.image_charges & 1 else 0) | (4 if q.image_charges & 2 else 0),
                       max_electrons=max_e, max_holes=max_h,
                       seed=q.random_seed & 0xFFFFFFFF, replica=replica, **rates(q))
-    return O.KmcOracle(orc, world["site_energy"], world["defects"], e, h, cfg, step)
+    bonds = None
+    if phase is not None:
+        cfg.confine = q.morphology_confine
+        if q.generation_interface:
+            bonds = interface_bonds(phase, q.grid_x, q.grid_y, q.grid_z)
+    return O.KmcOracle(orc, world["site_energy"], world["defects"], e, h, cfg, step,
+                       phase=phase, bonds=bonds)
 
 
 # ---- CPU: the oracle step's invariants ------------------------------------------------
@@ -120,6 +168,22 @@ CASES = {
                            steps=50),
     "no_coulomb": dict(grid_x=40, grid_y=30, grid_z=2, electron_percentage=0.05,
                        coulomb_carriers=0, voltage_right=2.0, steps=100),
+    "solar_2d_recombination": dict(simulation_type="solarcell", grid_x=40, grid_y=40,
+                                   grid_z=1, electron_percentage=0.03, hole_percentage=0.03,
+                                   seed_charges=0.5, voltage_right=1.0, generation_rate=0.3,
+                                   source_scale_area=0, recombination_rate=0.2,
+                                   recombination_range=1, steps=120),
+    "solar_3d_same_site": dict(simulation_type="solarcell", grid_x=20, grid_y=20, grid_z=6,
+                               electron_percentage=0.04, hole_percentage=0.04, seed_charges=0.5,
+                               voltage_right=0.5, generation_rate=0.5, source_scale_area=0,
+                               recombination_rate=0.5, recombination_range=0, image_charges=1,
+                               steps=80),
+    "solar_confined_interface": dict(simulation_type="solarcell", grid_x=32, grid_y=24,
+                                     grid_z=4, electron_percentage=0.03, hole_percentage=0.03,
+                                     seed_charges=0.0, voltage_right=0.5, generation_rate=0.6,
+                                     source_scale_area=0, recombination_rate=0.1,
+                                     recombination_range=1, morphology_confine=1,
+                                     generation_interface=1, steps=120, morphology=3),
     "2d_128_holes_1pct": dict(grid_x=128, grid_y=128, grid_z=1, hole_percentage=0.01,
                               electron_percentage=0.0, trap_percentage=0.05,
                               trap_potential=0.1, voltage_left=1.0, e_source_l_rate=0.0,
@@ -130,11 +194,17 @@ CASES = {
 def run_parity(O, name, keys, replica=0):
     keys = dict(keys)
     steps = keys.pop("steps")
+    morph = keys.pop("morphology", None)
     p = make_params(**keys)
     with L.KMC(p, device=0, replica=replica) as g:
+        phase = None
+        if morph is not None:
+            phase = blob_phase(p.grid_x, p.grid_y, p.grid_z, morph)
+            g.set_morphology(phase)
         st = g.stats()
         e0, h0 = g.carriers()
-        k = oracle_for(O, p, g.world(), e0, h0, st["max_electrons"], st["max_holes"], replica)
+        k = oracle_for(O, p, g.world(), e0, h0, st["max_electrons"], st["max_holes"], replica,
+                       phase=phase)
         worst = 0.0
         for s in range(steps):
             n0 = len(k.carriers()[0]) + len(k.carriers()[1])
