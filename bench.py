@@ -291,6 +291,69 @@ def batch_run(L, args, rank):
             "build_s": build_s}
 
 
+def surrogate_run(args, rank):
+    """Morphology screening: the CNN ensemble over fresh GRF candidates vs
+    labelling the same kind of morphology with the batched solar-cell kMC."""
+    import torch
+    from langmuir_b200 import surrogate as S
+    from langmuir_b200.kmc import KMCBatch
+    n = args.surrogate_candidates
+    t0 = time.perf_counter()
+    cand, _, _ = S.grf_morphologies(n, seed=7 + rank)
+    torch.cuda.synchronize()
+    gen_s = time.perf_counter() - t0
+    model = S.Surrogate(members=4, seed=rank)  # throughput does not depend on the weights
+    for _ in range(args.warmup):
+        S.screen(model, cand[:4096])
+    torch.cuda.synchronize()
+    times = []
+    for _ in range(max(1, args.steps // 10)):
+        t0 = time.perf_counter()
+        S.screen(model, cand)
+        torch.cuda.synchronize()
+        times.append(time.perf_counter() - t0)
+    screen_s = float(np.median(times))
+    # kMC labels of the same morphologies: set-up, steady steps, teardown
+    R, K, full = args.surrogate_label_replicas, args.surrogate_label_steps, 50000
+    ph = cand[:R].cpu().numpy()
+    t0 = time.perf_counter()
+    b = KMCBatch([S.solar_label_params(size=128, seed=1) for _ in range(R)], replica0=0)
+    reps = [b.replica(i) for i in range(R)]
+    for i, r in enumerate(reps):
+        r.set_morphology(ph[i].reshape(-1))
+    b.run(args.warmup)
+    setup_s = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    b.run(K)
+    step_s = (time.perf_counter() - t0) / K
+    t0 = time.perf_counter()
+    b.close()
+    teardown_s = time.perf_counter() - t0
+    kmc_label_s = setup_s + teardown_s + full * step_s
+    out = {"workload": f"{n} GRF candidates 128x128, l ~ U(2,16), donor fraction ~ U(0.4,0.6); "
+                       "4-member CNN ensemble, BF16 tensor-core kernels",
+           "surrogate_morphs_per_s": n / screen_s, "screen_ms": 1e3 * screen_s,
+           "generate_ms": 1e3 * gen_s,
+           "kmc_morphs_per_s": R / kmc_label_s,
+           "kmc_label": {"replicas": R, "steps_per_label": full, "timed_steps": K,
+                         "ms_per_batched_step": 1e3 * step_s, "setup_s": setup_s,
+                         "teardown_s": teardown_s,
+                         "note": f"{full}-step label cost = set-up + teardown + {full} x the "
+                                 f"batched step time measured over {K} steps"},
+           "speedup_vs_kmc": (n / screen_s) / (R / kmc_label_s)}
+    if rank == 0 and not args.no_cpu_baseline:
+        # the reference's screening score (ga.py:83-141), restated, on the host
+        from oracle import ga_score as G
+        imgs = [G.phases_to_image(p) for p in ph[:64]]
+        t0 = time.perf_counter()
+        for im in imgs:
+            G.score(im)
+        dt = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": len(imgs) / dt, "unit": "morphs/s", "cores": 1,
+                               "kind": "port", "sample": f"ga.py score of {len(imgs)} candidates"}
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -308,6 +371,10 @@ def main():
     ap.add_argument("--batch-replicas", type=int, default=512)
     ap.add_argument("--batch-steps", type=int, default=20)
     ap.add_argument("--batch-sample", type=int, default=32)
+    ap.add_argument("--no-surrogate", action="store_true")
+    ap.add_argument("--surrogate-candidates", type=int, default=100000)
+    ap.add_argument("--surrogate-label-replicas", type=int, default=4096)
+    ap.add_argument("--surrogate-label-steps", type=int, default=2000)
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
@@ -431,6 +498,10 @@ def main():
     if not args.no_batch:
         batch = batch_run(L, args, rank)
 
+    surrogate = None
+    if not args.no_surrogate:
+        surrogate = surrogate_run(args, rank)
+
     peaks = measured_peaks()
     props = torch.cuda.get_device_properties(dev)
     sms = props.multi_processor_count
@@ -470,7 +541,7 @@ def main():
                        "tile_variant": dict(ctx.variants()[variant], id=variant),
                        "parallelism": "replicas" if world > 1 else "single"},
             "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks, "kmc": kmc,
-            "kmc_batched": batch,
+            "kmc_batched": batch, "surrogate": surrogate,
             "gpu_launches": launches, "accuracy": acc,
         }
         print(json.dumps(line), flush=True)

@@ -763,6 +763,29 @@ lgm_status dalloc(lgm_kmc* k, T** p, size_t n) {
     return LGM_OK;
 }
 
+// Slices of one device allocation: add() records where each pointer goes and
+// its size, commit() makes one cudaMalloc and hands out 256-byte aligned slices.
+struct Arena {
+    std::vector<std::pair<void**, size_t>> slots;
+    template <typename T>
+    void add(T** p, size_t n) {
+        slots.emplace_back(reinterpret_cast<void**>(p), std::max<size_t>(n, 1) * sizeof(T));
+    }
+    lgm_status commit(lgm_kmc* k) {
+        size_t total = 0;
+        for (auto& s : slots) total += (s.second + 255) / 256 * 256;
+        char* base = nullptr;
+        KCUDA(k, cudaMalloc(reinterpret_cast<void**>(&base), std::max<size_t>(total, 256)));
+        k->allocs.push_back(base);
+        size_t off = 0;
+        for (auto& s : slots) {
+            *s.first = base + off;
+            off += (s.second + 255) / 256 * 256;
+        }
+        return LGM_OK;
+    }
+};
+
 // World::initialize order (world.cpp:625-643) on a Philox stream.
 lgm_status build_world(lgm_kmc* k) {
     const lgm_params& p = k->p;
@@ -948,8 +971,11 @@ lgm_status lgm_kmc_create(const lgm_params* pin, int32_t device, uint32_t replic
     if ((s = build_world(k)) != LGM_OK) return bail(s, k->err);
     k->device = device < 0 ? 0 : device;
     if (cudaSetDevice(k->device) != cudaSuccess) return bail(LGM_ERR_NO_DEVICE, "no device");
-    cudaDeviceProp prop;
-    if (cudaGetDeviceProperties(&prop, k->device) != cudaSuccess || prop.major != 10)
+    // attribute reads, not cudaGetDeviceProperties: a batch creates thousands of replicas
+    int cc_major = 0, n_sms = 0;
+    if (cudaDeviceGetAttribute(&cc_major, cudaDevAttrComputeCapabilityMajor, k->device) != cudaSuccess ||
+        cudaDeviceGetAttribute(&n_sms, cudaDevAttrMultiProcessorCount, k->device) != cudaSuccess ||
+        cc_major != 10)
         return bail(LGM_ERR_NO_DEVICE, "device is not sm_100 (B200)");
     if (cudaStreamCreateWithFlags(&k->stream, cudaStreamNonBlocking) != cudaSuccess)
         return bail(LGM_ERR_CUDA, "stream");
@@ -1047,10 +1073,12 @@ lgm_status lgm_kmc_create(const lgm_params* pin, int32_t device, uint32_t replic
     k->pair_tiles = (tphys_cap + kTile - 1) / kTile;
     int bps = 1;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, kmc_pair(D.gauss), kNT, pair_smem_bytes(64));
-    D.splits = std::max(1, std::min({64, prop.multiProcessorCount * std::max(1, bps) / k->pair_tiles,
+    D.splits = std::max(1, std::min({64, n_sms * std::max(1, bps) / k->pair_tiles,
                                      D.src_cap / CH}));
     lgm_status st;
-#define DA(ptr, n) if ((st = dalloc(k, &(ptr), (size_t)(n))) != LGM_OK) return bail(st, k->err)
+    // every buffer of the replica in one allocation (256-byte aligned slices)
+    Arena arena;
+#define DA(ptr, n) arena.add(&(ptr), (size_t)(n))
     DA(D.pot, k->V);
     DA(D.et, k->V + kSpecial);
     DA(D.ht, k->V + kSpecial);
@@ -1073,6 +1101,7 @@ lgm_status lgm_kmc_create(const lgm_params* pin, int32_t device, uint32_t replic
     DA(D.e_rm, std::max(D.cap_e, 1));
     DA(D.h_rm, std::max(D.cap_h, 1));
 #undef DA
+    if ((st = arena.commit(k)) != LGM_OK) return bail(st, k->err);
     if (D.gauss) {
         // erf(f sqrt(k))/sqrt(k) where it differs from 1/sqrt(k) in FP32; NaN past it
         const int c2 = D.cutoff2;

@@ -8,7 +8,8 @@ import pytest
 from langmuir_b200 import _native as N
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-HEADERS = [os.path.join(ROOT, "include", h) for h in ("langmuir_b200.h", "langmuir_b200_kmc.h")]
+HEADERS = [os.path.join(ROOT, "include", h)
+           for h in ("langmuir_b200.h", "langmuir_b200_kmc.h", "langmuir_b200_cnn.h")]
 
 
 def declared_functions():
@@ -28,6 +29,7 @@ def test_library_builds_and_loads():
 
 def test_every_declared_symbol_is_exported():
     import langmuir_b200  # noqa: F401  (binds the kMC entry points too)
+    import langmuir_b200.surrogate  # noqa: F401  (and the CNN kernels)
     L = ctypes.CDLL(N.LIB_PATH)
     names = declared_functions()
     assert "lgm_coulomb_kernel2" in names and "lgm_create" in names
