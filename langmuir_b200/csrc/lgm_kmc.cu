@@ -89,6 +89,7 @@ struct Dev {
     double* part;
     float* part_norm;
     double *Vt, *Nt;
+    double* w64;          // FP64 w(k) for integer r^2 = k < cutoff^2 (w(0) = 0), the guard's table
     int splits;
     int src_cap;   // source records capacity (multiple of CH)
     int tpad_cap;  // per-term target block capacity
@@ -347,13 +348,22 @@ __device__ __forceinline__ void decide_body(const Dev& D, const int i) {
 // reference's test on the FP64 energy.  One block per queued decision,
 // grid-stride over the queue.
 constexpr int kGuardThreads = 256;
+// Blocks per replica of the batched guard: flagged decisions of one replica
+// are spread over them (a replica with M charges flags ~1e-3 M per step).
+constexpr int kGuardBlocksPerReplica = 4;
 
-__device__ double fp64_potential(const Dev& D, int ne, int nh, int site, double* red) {
-    int xi, yi, zi;
-    xyz(D, site, xi, yi, zi);
+// FP64 potentials at two sites in one pass over the sources (the guard's
+// re-evaluation): the same cutoff and image rules as the pair kernel, terms
+// w(r^2) from the FP64 table (1/sqrt(k) or erf(f sqrt(k))/sqrt(k), computed on
+// the host in IEEE double), summed per thread and then across the block.
+__device__ double2 fp64_potential2(const Dev& D, int ne, int nh, int site_a, int site_b,
+                                   double2* red) {
+    int xa, ya, za, xb, yb, zb;
+    xyz(D, site_a, xa, ya, za);
+    xyz(D, site_b, xb, yb, zb);
     const int nd = D.dq != 0 ? D.nd : 0;
     const int n = ne + nh + nd;
-    double acc = 0.0;
+    double acc_a = 0.0, acc_b = 0.0;
     for (int j = threadIdx.x; j < n; j += blockDim.x) {
         int s;
         double q;
@@ -362,31 +372,34 @@ __device__ double fp64_potential(const Dev& D, int ne, int nh, int site, double*
         else { s = D.defects[j - ne - nh]; q = (double)D.dq; }
         int xj, yj, zj;
         xyz(D, s, xj, yj, zj);
-        const int dy = yi - yj, dz = zi - zj;
+        const int dya = ya - yj, dza = za - zj, dyb = yb - yj, dzb = zb - zj;
+        const int ra = dya * dya + dza * dza, rb = dyb * dyb + dzb * dzb;
         for (int term = 0; term < 3; ++term) {
             if (!(D.terms & (1u << term))) continue;
-            const int dx = term == 0 ? xi - xj : (term == 1 ? xi + xj + 1 : 2 * D.X - 1 - xi - xj);
-            const int r2 = dx * dx + dy * dy + dz * dz;
-            if (r2 > 0 && r2 < D.cutoff2) {
-                const double r = sqrt((double)r2);
-                const double w = D.gauss ? erf(D.erffactor * r) / r : 1.0 / r;
-                acc += term == 0 ? q * w : -q * w;
-            }
+            const int dxa = term == 0 ? xa - xj : (term == 1 ? xa + xj + 1 : 2 * D.X - 1 - xa - xj);
+            const int dxb = term == 0 ? xb - xj : (term == 1 ? xb + xj + 1 : 2 * D.X - 1 - xb - xj);
+            const int r2a = dxa * dxa + ra, r2b = dxb * dxb + rb;
+            const double qs = term == 0 ? q : -q;
+            if (r2a > 0 && r2a < D.cutoff2) acc_a += qs * D.w64[r2a];
+            if (r2b > 0 && r2b < D.cutoff2) acc_b += qs * D.w64[r2b];
         }
     }
-    red[threadIdx.x] = acc;
+    red[threadIdx.x] = make_double2(acc_a, acc_b);
     __syncthreads();
     for (int w = blockDim.x / 2; w > 0; w >>= 1) {
-        if ((int)threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+        if ((int)threadIdx.x < w) {
+            red[threadIdx.x].x += red[threadIdx.x + w].x;
+            red[threadIdx.x].y += red[threadIdx.x + w].y;
+        }
         __syncthreads();
     }
-    const double v = red[0];
+    const double2 v = red[0];
     __syncthreads();
-    return D.prefactor * v;
+    return make_double2(D.prefactor * v.x, D.prefactor * v.y);
 }
 
 __device__ __forceinline__ void guard_body(const Dev& D, const int block, const int nblocks,
-                                           double* red) {
+                                           double2* red) {
     const int ne = D.cnt[I_NE0], nh = D.cnt[I_NH0];
     const int nflag = D.cnt[I_NFLAG];
     const uint32_t step = (uint32_t)D.cnt[I_STEP];
@@ -397,8 +410,8 @@ __device__ __forceinline__ void guard_body(const Dev& D, const int block, const 
         const int site = e ? D.e_site[k] : D.h_site[k];
         const int f = e ? D.e_f[k] : D.h_f[k];
         const double q = e ? -1.0 : 1.0;
-        const double v1 = fp64_potential(D, ne, nh, site, red);
-        const double v2 = fp64_potential(D, ne, nh, f, red);
+        const double2 v = fp64_potential2(D, ne, nh, site, f, red);
+        const double v1 = v.x, v2 = v.y;
         if (threadIdx.x == 0) {
             const double p1 = v1 + binding(D, e, site);
             const double p2 = v2 - D.sI100 * q + binding(D, e, f);
@@ -623,7 +636,7 @@ __global__ void k_pack(Dev D) { pack_body(D, LGM_THREAD_INDEX); }
 __global__ void k_finalize(Dev D) { finalize_body(D, LGM_THREAD_INDEX); }
 __global__ void k_decide(Dev D) { decide_body(D, LGM_THREAD_INDEX); }
 __global__ void __launch_bounds__(kGuardThreads) k_guard(Dev D) {
-    __shared__ double red[kGuardThreads];
+    __shared__ double2 red[kGuardThreads];
     guard_body(D, blockIdx.x, gridDim.x, red);
 }
 __global__ void k_hmap(Dev D) { hmap_body(D, LGM_THREAD_INDEX, true); }
@@ -656,7 +669,7 @@ __global__ void kb_decide(const Dev* R, const int2* map) {
 }
 // blocks_per_replica consecutive blocks per replica
 __global__ void __launch_bounds__(kGuardThreads) kb_guard(const Dev* R, int blocks_per_replica) {
-    __shared__ double red[kGuardThreads];
+    __shared__ double2 red[kGuardThreads];
     guard_body(R[blockIdx.x / blocks_per_replica], blockIdx.x % blocks_per_replica,
                blocks_per_replica, red);
 }
@@ -1100,6 +1113,7 @@ lgm_status lgm_kmc_create(const lgm_params* pin, int32_t device, uint32_t replic
     DA(D.e_rch, std::max(D.cap_e, 1));
     DA(D.e_rm, std::max(D.cap_e, 1));
     DA(D.h_rm, std::max(D.cap_h, 1));
+    DA(D.w64, std::max(D.cutoff2, 1));
 #undef DA
     if ((st = arena.commit(k)) != LGM_OK) return bail(st, k->err);
     if (D.gauss) {
@@ -1119,6 +1133,14 @@ lgm_status lgm_kmc_create(const lgm_params* pin, int32_t device, uint32_t replic
             return bail(LGM_ERR_CUDA, "table upload");
         cudaFuncSetAttribute(kmc_pair(1), cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)pair_smem_bytes(kmax));
+    }
+    {
+        std::vector<double> w(std::max(D.cutoff2, 1), 0.0);
+        for (int r2 = 1; r2 < D.cutoff2; ++r2) {
+            const double r = std::sqrt((double)r2);
+            w[r2] = D.gauss ? std::erf(D.erffactor * r) / r : 1.0 / r;
+        }
+        cudaMemcpy(D.w64, w.data(), sizeof(double) * w.size(), cudaMemcpyHostToDevice);
     }
     cudaMemcpy(D.pot, k->pot.data(), sizeof(double) * k->V, cudaMemcpyHostToDevice);
     if (D.nd) cudaMemcpy(D.defects, k->defects.data(), sizeof(int32_t) * D.nd, cudaMemcpyHostToDevice);
@@ -1407,7 +1429,7 @@ lgm_status enqueue_batch_step(lgm_kmc_batch* b) {
         kb_finalize<<<b->nb_fin, 256, 0, st>>>(b->d_reps, b->map_fin);
     }
     kb_decide<<<b->nb_car, 256, 0, st>>>(b->d_reps, b->map_car);
-    if (b->coulomb) kb_guard<<<2 * R, kGuardThreads, 0, st>>>(b->d_reps, 2);
+    if (b->coulomb) kb_guard<<<kGuardBlocksPerReplica * R, kGuardThreads, 0, st>>>(b->d_reps, kGuardBlocksPerReplica);
     if (b->recomb) {
         kb_hmap<<<b->nb_car, 256, 0, st>>>(b->d_reps, b->map_car);
         kb_recomb_propose<<<b->nb_car, 256, 0, st>>>(b->d_reps, b->map_car);

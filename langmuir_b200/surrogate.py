@@ -363,19 +363,38 @@ def kmc_labels(phases, steps=50000, burn_in=10000, seed=1, replica0=0, device=0,
 
 
 # ---- ensemble ------------------------------------------------------------------------------
-class Surrogate:
-    """Ensemble of CNNs on standardised (current, efficiency) targets."""
+def symmetry(x16, k):
+    """The device's symmetries on a bf16 input [B,H,W,1] (x = +-1 per phase):
+    k = 0 identity, 1 mirror in y, 2 mirror in x with the phases exchanged
+    (electrons and holes, collected at opposite electrodes, trade places),
+    3 both.  kMC labels are invariant under all four."""
+    if k & 1:
+        x16 = x16.flip(1)
+    if k & 2:
+        x16 = (-x16).flip(2)
+    return x16.contiguous()
 
-    def __init__(self, members=4, seed=0, device="cuda"):
+
+class Surrogate:
+    """Ensemble of CNNs on standardised log(current), log(efficiency).
+
+    Training draws one of the four device symmetries per mini-batch;
+    ``tta`` > 1 averages predictions over that many symmetries."""
+
+    def __init__(self, members=4, seed=0, device="cuda", log_targets=True, augment=True, tta=1):
         self.device = device
         self.members = [init_params(seed * 1000 + m, device) for m in range(members)]
         self.mean = torch.zeros(OUTPUTS, device=device)
         self.std = torch.ones(OUTPUTS, device=device)
+        self.log_targets, self.augment, self.tta = log_targets, augment, tta
+
+    def _encode(self, y):
+        return torch.log(y.clamp_min(1e-6)) if self.log_targets else y
 
     def fit(self, phases, targets, epochs=30, batch=64, lr=2e-3, seed=0, log=None):
         """phases uint8 [n,H,W], targets float [n,2] (current, efficiency)."""
         x = phases_to_input(phases, self.device)
-        y = torch.as_tensor(np.asarray(targets, np.float32), device=self.device)
+        y = self._encode(torch.as_tensor(np.asarray(targets, np.float32), device=self.device))
         self.mean = y.mean(0)
         self.std = y.std(0).clamp_min(1e-6)
         yn = (y - self.mean) / self.std
@@ -390,7 +409,10 @@ class Surrogate:
                 tot = 0.0
                 for i0 in range(0, n - batch + 1, batch):
                     idx = perm[i0:i0 + batch]
-                    pred = SurrogateFn.apply(x[idx], *params)
+                    xb = x[idx]
+                    if self.augment:
+                        xb = symmetry(xb, int(torch.randint(0, 4, (1,), generator=g)))
+                    pred = SurrogateFn.apply(xb, *params)
                     loss = ((pred - yn[idx]) ** 2).mean()
                     opt.zero_grad(set_to_none=True)
                     loss.backward()
@@ -404,25 +426,37 @@ class Surrogate:
 
     @torch.no_grad()
     def predict(self, phases=None, x16=None, batch=1024):
-        """Mean and spread over the ensemble, in target units: two [n,2] tensors."""
+        """Ensemble mean and spread in target units: two [n,2] tensors.  With
+        log targets the mean is the geometric mean over members and the spread
+        is mean * (std of the log predictions)."""
         if x16 is None:
             x16 = phases_to_input(phases, self.device)
         n = x16.shape[0]
-        preds = torch.empty(len(self.members), n, OUTPUTS, device=self.device)
+        views = max(1, self.tta)
+        preds = torch.zeros(len(self.members), n, OUTPUTS, device=self.device)
         for m, params in enumerate(self.members):
             for i0 in range(0, n, batch):
-                y, _ = network_forward(x16[i0:i0 + batch], params, keep=False)
-                preds[m, i0:i0 + batch] = y
+                xb = x16[i0:i0 + batch]
+                for k in range(views):
+                    y, _ = network_forward(symmetry(xb, k) if k else xb, params, keep=False)
+                    preds[m, i0:i0 + batch] += y / views
         preds = preds * self.std + self.mean
-        return preds.mean(0), preds.std(0) if len(self.members) > 1 else torch.zeros_like(preds[0])
+        mu = preds.mean(0)
+        sd = preds.std(0) if len(self.members) > 1 else torch.zeros_like(mu)
+        if self.log_targets:
+            mu = torch.exp(mu)
+            sd = mu * sd
+        return mu, sd
 
     def state_dict(self):
         return {"members": [[p.detach().cpu() for p in ps] for ps in self.members],
-                "mean": self.mean.cpu(), "std": self.std.cpu()}
+                "mean": self.mean.cpu(), "std": self.std.cpu(), "log_targets": self.log_targets,
+                "tta": self.tta}
 
     def load_state_dict(self, sd):
         self.members = [[p.to(self.device).requires_grad_(True) for p in ps] for ps in sd["members"]]
         self.mean, self.std = sd["mean"].to(self.device), sd["std"].to(self.device)
+        self.log_targets, self.tta = sd.get("log_targets", False), sd.get("tta", 1)
 
 
 def screen(model, candidates, top=256, uncertainty_quantile=0.9975, batch=1024):
@@ -459,27 +493,55 @@ def error_report(pred, truth):
             "spearman": _spearman(pred, truth) if truth.size > 2 else float("nan")}
 
 
+def save_labels(path, phases, labels):
+    """Morphologies (bit-packed) and their kMC labels in one .npz."""
+    ph = phases.cpu().numpy() if torch.is_tensor(phases) else np.asarray(phases)
+    np.savez_compressed(path, bits=np.packbits(ph.astype(bool), axis=None), shape=np.array(ph.shape),
+                        **{k: np.asarray(v) for k, v in labels.items()})
+
+
+def load_labels(path, device="cuda"):
+    d = np.load(path)
+    shape = tuple(int(v) for v in d["shape"])
+    ph = np.unpackbits(d["bits"])[:int(np.prod(shape))].reshape(shape).astype(np.uint8)
+    labels = {k: (d[k] if d[k].ndim else float(d[k])) for k in d.files if k not in ("bits", "shape")}
+    return torch.as_tensor(ph, device=device), labels
+
+
 def run_pipeline(n_train=4096, n_holdout=512, n_candidates=100000, steps=50000, burn_in=10000,
-                 members=4, epochs=60, top=256, seed=0, log=print):
+                 members=4, epochs=300, top=256, seed=0, labels_cache="", lr=4e-3, log=print,
+                 **model_kw):
     """Generate, label, train, evaluate on kMC-labelled holdouts, screen
-    candidates and re-simulate the picks.  Returns a report dict."""
+    candidates and re-simulate the picks.  Returns a report dict.  With
+    ``labels_cache`` the training and holdout labels are read from (or, the
+    first time, written to) that prefix."""
+    import os
     rep = {"config": dict(n_train=n_train, n_holdout=n_holdout, n_candidates=n_candidates,
                           steps=steps, burn_in=burn_in, members=members, epochs=epochs, top=top,
-                          seed=seed, size=128)}
+                          seed=seed, size=128, lr=lr, **model_kw)}
     sync = torch.cuda.synchronize
-    ph_tr, _, _ = grf_morphologies(n_train, seed=seed * 10 + 1)
-    ph_ho, _, _ = grf_morphologies(n_holdout, seed=seed * 10 + 2)
-    lab_tr = kmc_labels(ph_tr, steps=steps, burn_in=burn_in, seed=seed + 1, replica0=0)
-    log(f"labels: {n_train} morphologies x {steps} steps in {lab_tr['seconds']:.1f} s")
-    lab_ho = kmc_labels(ph_ho, steps=steps, burn_in=burn_in, seed=seed + 1, replica0=1 << 24)
+    cached = labels_cache and os.path.exists(labels_cache + "_train.npz")
+    if cached:
+        ph_tr, lab_tr = load_labels(labels_cache + "_train.npz")
+        ph_ho, lab_ho = load_labels(labels_cache + "_holdout.npz")
+    else:
+        ph_tr, _, _ = grf_morphologies(n_train, seed=seed * 10 + 1)
+        ph_ho, _, _ = grf_morphologies(n_holdout, seed=seed * 10 + 2)
+        lab_tr = kmc_labels(ph_tr, steps=steps, burn_in=burn_in, seed=seed + 1, replica0=0)
+        log(f"labels: {n_train} morphologies x {steps} steps in {lab_tr['seconds']:.1f} s")
+        lab_ho = kmc_labels(ph_ho, steps=steps, burn_in=burn_in, seed=seed + 1, replica0=1 << 24)
+        if labels_cache:
+            save_labels(labels_cache + "_train.npz", ph_tr, lab_tr)
+            save_labels(labels_cache + "_holdout.npz", ph_ho, lab_ho)
+    rep["labels_from_cache"] = bool(cached)
     rep["kmc"] = {"train_seconds": lab_tr["seconds"], "holdout_seconds": lab_ho["seconds"],
                   "morphs_per_s": n_train / lab_tr["seconds"],
                   "efficiency_percentiles": np.percentile(lab_tr["efficiency"], [5, 50, 95]).tolist(),
                   "generated_median": float(np.median(lab_tr["generated"]))}
     y_tr = np.stack([lab_tr["current"], lab_tr["efficiency"]], 1)
-    model = Surrogate(members=members, seed=seed)
+    model = Surrogate(members=members, seed=seed, **model_kw)
     t0 = time.perf_counter()
-    hist = model.fit(ph_tr, y_tr, epochs=epochs, batch=64, lr=2e-3, seed=seed)
+    hist = model.fit(ph_tr, y_tr, epochs=epochs, batch=64, lr=lr, seed=seed)
     sync()
     rep["train"] = {"seconds": time.perf_counter() - t0, "final_loss": [h[2] for h in hist
                                                                         if h[1] == epochs - 1]}
@@ -517,6 +579,7 @@ def run_pipeline(n_train=4096, n_holdout=512, n_candidates=100000, steps=50000, 
     log(f"screen: {rep['screen']}")
     rep["_arrays"] = {"holdout_phases": ph_ho.cpu().numpy(), "holdout_eff": lab_ho["efficiency"],
                       "holdout_pred": mean[:, 1]}
+    rep["_model"] = model
     return rep
 
 
@@ -531,19 +594,25 @@ def main(argv=None):
     ap.add_argument("--steps", type=int, default=50000)
     ap.add_argument("--burn-in", type=int, default=10000)
     ap.add_argument("--members", type=int, default=4)
-    ap.add_argument("--epochs", type=int, default=60)
+    ap.add_argument("--epochs", type=int, default=300)
+    ap.add_argument("--lr", type=float, default=4e-3)
     ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--tta", type=int, default=1, help="symmetry views averaged per prediction")
+    ap.add_argument("--labels-cache", default="", help="prefix of cached training/holdout labels")
     ap.add_argument("--out", default="")
     a = ap.parse_args(argv)
     rep = run_pipeline(a.train, a.holdout, a.candidates, a.steps, a.burn_in, a.members, a.epochs,
-                       seed=a.seed)
+                       seed=a.seed, labels_cache=a.labels_cache, lr=a.lr, tta=a.tta)
     arrays = rep.pop("_arrays")
+    model = rep.pop("_model")
     text = json.dumps(rep, indent=1)
     print(text)
     if a.out:
+        stem = a.out.rsplit(".", 1)[0]
         with open(a.out, "w") as fh:
             fh.write(text)
-        np.savez_compressed(a.out.rsplit(".", 1)[0] + "_holdout.npz", **arrays)
+        np.savez_compressed(stem + "_holdout.npz", **arrays)
+        torch.save(model.state_dict(), stem + "_model.pt")
 
 
 if __name__ == "__main__":
