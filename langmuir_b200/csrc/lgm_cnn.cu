@@ -20,6 +20,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <algorithm>
+
 #include "langmuir_b200_cnn.h"
 
 namespace {
@@ -49,142 +51,210 @@ struct ConvShape {
     static constexpr int CPAD = CIN == 1 ? 2 : CIN + 8;   // patch channel stride (bank skew)
     static constexpr int WSTRIDE = KPAD + 8;              // weight row stride
     static constexpr size_t PATCH = (size_t)(TY + 2) * (TX + 2) * CPAD;
-    static constexpr size_t SMEM = (PATCH + (size_t)COUT * WSTRIDE) * sizeof(bf16);
+    static constexpr int OSTR = COUT + 8;                 // staged output pixel stride
+    static constexpr size_t OTILE = (size_t)TY * TX * OSTR;        // full-resolution tile
+    static constexpr size_t PTILE = (size_t)(TY / 2) * (TX / 2) * OSTR;  // pooled tile
+    static constexpr size_t SMEM = (PATCH + (size_t)COUT * WSTRIDE + OTILE + PTILE) * sizeof(bf16);
 };
+
+// Input patch of one 8x16 tile with a one-pixel halo, zero outside the image:
+// patch[(py*(TX+2) + px)*CPAD + c] = x[b][y0+py-1][x0+px-1][c].  CIN = 32 moves
+// 16-byte vectors (8 channels); CIN = 1 single values.
+template <int CIN>
+__device__ __forceinline__ void load_patch(const bf16* __restrict__ x, bf16* patch, int b, int y0,
+                                           int x0, int H, int W, int tid) {
+    using S = ConvShape<CIN>;
+    if constexpr (CIN == 1) {
+        for (int i = tid; i < (TY + 2) * (TX + 2); i += CONV_THREADS) {
+            const int px = i % (TX + 2), py = i / (TX + 2);
+            const int yy = y0 + py - 1, xx = x0 + px - 1;
+            bf16 v = __float2bfloat16(0.f);
+            if (yy >= 0 && yy < H && xx >= 0 && xx < W) v = x[((size_t)b * H + yy) * W + xx];
+            patch[i * S::CPAD] = v;
+        }
+    } else {
+        constexpr int V = CIN / 8;  // 16-byte vectors per pixel
+        for (int i = tid; i < (TY + 2) * (TX + 2) * V; i += CONV_THREADS) {
+            const int c8 = i % V, pix = i / V;
+            const int px = pix % (TX + 2), py = pix / (TX + 2);
+            const int yy = y0 + py - 1, xx = x0 + px - 1;
+            uint4 v = make_uint4(0u, 0u, 0u, 0u);
+            if (yy >= 0 && yy < H && xx >= 0 && xx < W)
+                v = *reinterpret_cast<const uint4*>(x + (((size_t)b * H + yy) * W + xx) * CIN + c8 * 8);
+            *reinterpret_cast<uint4*>(patch + pix * S::CPAD + c8 * 8) = v;
+        }
+    }
+}
 
 // x: [B,H,W,CIN]; w: [COUT][KPAD] (k = (ky*3 + kx)*CIN + c); act: [B,H,W,COUT]
 // (optional); pooled: [B,H/2,W/2,COUT] (optional).  H % 8 == 0, W % 16 == 0.
+// Persistent over tiles: the weights are staged once per CTA, each 8x16 tile's
+// patch is staged with vector loads, and the epilogue stages the output tile
+// in shared memory so that global stores are whole 16-byte vectors.
 template <int CIN>
 __global__ void __launch_bounds__(CONV_THREADS)
 conv3x3_fwd(const bf16* __restrict__ x, const bf16* __restrict__ w, const float* __restrict__ bias,
-            bf16* __restrict__ act, bf16* __restrict__ pooled, int H, int W, int relu) {
+            bf16* __restrict__ act, bf16* __restrict__ pooled, int B, int H, int W, int relu) {
     using S = ConvShape<CIN>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     bf16* patch = reinterpret_cast<bf16*>(smem_raw);
     bf16* ws = patch + S::PATCH;
+    bf16* ost = ws + COUT * S::WSTRIDE;
+    bf16* pst = ost + S::OTILE;
     const int tiles_x = W / TX;
     const int tiles_y = H / TY;
-    const int b = blockIdx.x / (tiles_x * tiles_y);
-    const int rem = blockIdx.x % (tiles_x * tiles_y);
-    const int y0 = (rem / tiles_x) * TY, x0 = (rem % tiles_x) * TX;
+    const int ntiles = B * tiles_x * tiles_y;
     const int tid = threadIdx.x;
+    const int warp = tid >> 5, lane = tid & 31, g = lane >> 2, t = lane & 3;
+    const bf16 zero = __float2bfloat16(0.f);
 
-    // weights -> shared
     for (int i = tid; i < COUT * S::KPAD; i += CONV_THREADS)
         ws[(i / S::KPAD) * S::WSTRIDE + (i % S::KPAD)] = w[i];
-    // input patch (zero outside the image)
-    const bf16 zero = __float2bfloat16(0.f);
-    for (int i = tid; i < (TY + 2) * (TX + 2) * CIN; i += CONV_THREADS) {
-        const int c = i % CIN, px = (i / CIN) % (TX + 2), py = i / (CIN * (TX + 2));
-        const int yy = y0 + py - 1, xx = x0 + px - 1;
-        bf16 v = zero;
-        if (yy >= 0 && yy < H && xx >= 0 && xx < W)
-            v = x[(((size_t)b * H + yy) * W + xx) * CIN + c];
-        patch[(py * (TX + 2) + px) * S::CPAD + c] = v;
+    float bv[4][2];
+#pragma unroll
+    for (int n = 0; n < 4; ++n) {
+        bv[n][0] = bias ? bias[n * 8 + 2 * t] : 0.f;
+        bv[n][1] = bias ? bias[n * 8 + 2 * t + 1] : 0.f;
     }
-    __syncthreads();
 
-    const int warp = tid >> 5, lane = tid & 31, g = lane >> 2, t = lane & 3;
-    float acc[2][4][4];
-#pragma unroll
-    for (int i = 0; i < 2; ++i)
-#pragma unroll
-        for (int n = 0; n < 4; ++n)
-#pragma unroll
-            for (int j = 0; j < 4; ++j) acc[i][n][j] = 0.f;
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const int b = tile / (tiles_x * tiles_y);
+        const int rem = tile % (tiles_x * tiles_y);
+        const int y0 = (rem / tiles_x) * TY, x0 = (rem % tiles_x) * TX;
+        __syncthreads();  // the previous tile is done with patch, ost and pst
+        load_patch<CIN>(x, patch, b, y0, x0, H, W, tid);
+        __syncthreads();
 
-    if (CIN == 1) {
-        // one k16 step: k < 9 -> (ky, kx) = (k / 3, k % 3), else 0
-        auto tap = [&](int row, int col, int k) -> bf16 {
-            if (k >= 9) return zero;
-            return patch[((row + k / 3) * (TX + 2) + (col + k % 3)) * S::CPAD];
-        };
-        uint32_t bb[4][2];
+        float acc[2][4][4];
 #pragma unroll
-        for (int n = 0; n < 4; ++n) {
-            const bf16* wr = ws + (n * 8 + g) * S::WSTRIDE;
-            bb[n][0] = pack2(wr[2 * t], wr[2 * t + 1]);
-            bb[n][1] = pack2(wr[2 * t + 8], wr[2 * t + 9]);
-        }
+        for (int i = 0; i < 2; ++i)
 #pragma unroll
-        for (int i = 0; i < 2; ++i) {
-            const int row = 2 * warp + i;
-            uint32_t a[4];
-            a[0] = pack2(tap(row, g, 2 * t), tap(row, g, 2 * t + 1));
-            a[1] = pack2(tap(row, g + 8, 2 * t), tap(row, g + 8, 2 * t + 1));
-            a[2] = pack2(tap(row, g, 2 * t + 8), tap(row, g, 2 * t + 9));
-            a[3] = pack2(tap(row, g + 8, 2 * t + 8), tap(row, g + 8, 2 * t + 9));
+            for (int n = 0; n < 4; ++n)
 #pragma unroll
-            for (int n = 0; n < 4; ++n) mma16816(acc[i][n], a, bb[n]);
-        }
-    } else {
-#pragma unroll 1
-        for (int s = 0; s < 9 * CIN / 16; ++s) {
-            const int tap = (s * 16) / CIN, c0 = (s * 16) % CIN;
-            const int ky = tap / 3, kx = tap % 3;
+                for (int j = 0; j < 4; ++j) acc[i][n][j] = 0.f;
+
+        if constexpr (CIN == 1) {
+            // one k16 step: the thread's columns k = 2t, 2t+1, 2t+8, 2t+9 are
+            // taps (ky, kx) = (k / 3, k % 3) for k < 9 and zero padding above
             uint32_t bb[4][2];
 #pragma unroll
             for (int n = 0; n < 4; ++n) {
-                const bf16* wr = ws + (n * 8 + g) * S::WSTRIDE + s * 16;
-                bb[n][0] = *reinterpret_cast<const uint32_t*>(wr + 2 * t);
-                bb[n][1] = *reinterpret_cast<const uint32_t*>(wr + 2 * t + 8);
+                const bf16* wr = ws + (n * 8 + g) * S::WSTRIDE;
+                bb[n][0] = pack2(wr[2 * t], wr[2 * t + 1]);
+                bb[n][1] = pack2(wr[2 * t + 8], wr[2 * t + 9]);
+            }
+            int toff[4];
+            bool tok[4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const int k = 2 * t + (j & 1) + (j >> 1) * 8;
+                tok[j] = k < 9;
+                toff[j] = tok[j] ? ((k / 3) * (TX + 2) + k % 3) * S::CPAD : 0;
             }
 #pragma unroll
             for (int i = 0; i < 2; ++i) {
-                const int row = 2 * warp + i + ky;
-                const bf16* p0 = patch + (row * (TX + 2) + g + kx) * S::CPAD + c0;
-                const bf16* p1 = patch + (row * (TX + 2) + g + 8 + kx) * S::CPAD + c0;
+                const int row = 2 * warp + i;
+                const bf16* p0 = patch + (row * (TX + 2) + g) * S::CPAD;
+                const bf16* p1 = p0 + 8 * S::CPAD;
+                bf16 v0[4], v1[4];
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    v0[j] = tok[j] ? p0[toff[j]] : zero;
+                    v1[j] = tok[j] ? p1[toff[j]] : zero;
+                }
                 uint32_t a[4];
-                a[0] = *reinterpret_cast<const uint32_t*>(p0 + 2 * t);
-                a[1] = *reinterpret_cast<const uint32_t*>(p1 + 2 * t);
-                a[2] = *reinterpret_cast<const uint32_t*>(p0 + 2 * t + 8);
-                a[3] = *reinterpret_cast<const uint32_t*>(p1 + 2 * t + 8);
+                a[0] = pack2(v0[0], v0[1]);
+                a[1] = pack2(v1[0], v1[1]);
+                a[2] = pack2(v0[2], v0[3]);
+                a[3] = pack2(v1[2], v1[3]);
 #pragma unroll
                 for (int n = 0; n < 4; ++n) mma16816(acc[i][n], a, bb[n]);
             }
+        } else {
+#pragma unroll 2
+            for (int s = 0; s < 9 * CIN / 16; ++s) {
+                const int tap = (s * 16) / CIN, c0 = (s * 16) % CIN;
+                const int ky = tap / 3, kx = tap % 3;
+                uint32_t bb[4][2];
+#pragma unroll
+                for (int n = 0; n < 4; ++n) {
+                    const bf16* wr = ws + (n * 8 + g) * S::WSTRIDE + s * 16;
+                    bb[n][0] = *reinterpret_cast<const uint32_t*>(wr + 2 * t);
+                    bb[n][1] = *reinterpret_cast<const uint32_t*>(wr + 2 * t + 8);
+                }
+#pragma unroll
+                for (int i = 0; i < 2; ++i) {
+                    const int row = 2 * warp + i + ky;
+                    const bf16* p0 = patch + (row * (TX + 2) + g + kx) * S::CPAD + c0;
+                    const bf16* p1 = patch + (row * (TX + 2) + g + 8 + kx) * S::CPAD + c0;
+                    uint32_t a[4];
+                    a[0] = *reinterpret_cast<const uint32_t*>(p0 + 2 * t);
+                    a[1] = *reinterpret_cast<const uint32_t*>(p1 + 2 * t);
+                    a[2] = *reinterpret_cast<const uint32_t*>(p0 + 2 * t + 8);
+                    a[3] = *reinterpret_cast<const uint32_t*>(p1 + 2 * t + 8);
+#pragma unroll
+                    for (int n = 0; n < 4; ++n) mma16816(acc[i][n], a, bb[n]);
+                }
+            }
         }
-    }
 
-    // epilogue: rows g / g+8 are pixels x0+g / x0+g+8 of tile row 2*warp+i;
-    // columns 2t, 2t+1 of n-tile n are channels n*8+2t, +1
+        // epilogue: rows g / g+8 of the fragment are pixels x0+g / x0+g+8 of
+        // tile row 2*warp+i; columns 2t, 2t+1 of n-tile n are channels n*8+2t, +1
 #pragma unroll
-    for (int n = 0; n < 4; ++n) {
-        const int ch = n * 8 + 2 * t;
-        const float b0 = bias ? bias[ch] : 0.f, b1 = bias ? bias[ch + 1] : 0.f;
-        float v[2][4];
+        for (int n = 0; n < 4; ++n) {
+            const int ch = n * 8 + 2 * t;
+            float v[2][4];
 #pragma unroll
-        for (int i = 0; i < 2; ++i) {
-            v[i][0] = acc[i][n][0] + b0;
-            v[i][1] = acc[i][n][1] + b1;
-            v[i][2] = acc[i][n][2] + b0;
-            v[i][3] = acc[i][n][3] + b1;
-            if (relu)
+            for (int i = 0; i < 2; ++i) {
+                v[i][0] = acc[i][n][0] + bv[n][0];
+                v[i][1] = acc[i][n][1] + bv[n][1];
+                v[i][2] = acc[i][n][2] + bv[n][0];
+                v[i][3] = acc[i][n][3] + bv[n][1];
+                if (relu)
 #pragma unroll
-                for (int j = 0; j < 4; ++j) v[i][j] = fmaxf(v[i][j], 0.f);
-            if (act) {
-                const int yy = y0 + 2 * warp + i;
-                const size_t base = (((size_t)b * H + yy) * W + x0) * COUT;
-                *reinterpret_cast<uint32_t*>(act + base + (size_t)g * COUT + ch) =
-                    pack2(__float2bfloat16(v[i][0]), __float2bfloat16(v[i][1]));
-                *reinterpret_cast<uint32_t*>(act + base + (size_t)(g + 8) * COUT + ch) =
-                    pack2(__float2bfloat16(v[i][2]), __float2bfloat16(v[i][3]));
+                    for (int j = 0; j < 4; ++j) v[i][j] = fmaxf(v[i][j], 0.f);
+                if (act) {
+                    const int r = 2 * warp + i;
+                    *reinterpret_cast<uint32_t*>(ost + (r * TX + g) * S::OSTR + ch) =
+                        pack2(__float2bfloat16(v[i][0]), __float2bfloat16(v[i][1]));
+                    *reinterpret_cast<uint32_t*>(ost + (r * TX + g + 8) * S::OSTR + ch) =
+                        pack2(__float2bfloat16(v[i][2]), __float2bfloat16(v[i][3]));
+                }
+            }
+            if (pooled) {
+                // sum the two tile rows (same thread), then the x pair (lanes g, g^1)
+                float sm[4];
+#pragma unroll
+                for (int j = 0; j < 4; ++j) sm[j] = v[0][j] + v[1][j];
+#pragma unroll
+                for (int j = 0; j < 4; ++j) sm[j] += __shfl_xor_sync(0xffffffffu, sm[j], 4);
+                if ((g & 1) == 0) {
+                    // pooled tile: row warp (0..3), columns g/2 and g/2 + 4 (0..7)
+                    *reinterpret_cast<uint32_t*>(pst + (warp * (TX / 2) + g / 2) * S::OSTR + ch) =
+                        pack2(__float2bfloat16(0.25f * sm[0]), __float2bfloat16(0.25f * sm[1]));
+                    *reinterpret_cast<uint32_t*>(pst + (warp * (TX / 2) + g / 2 + 4) * S::OSTR + ch) =
+                        pack2(__float2bfloat16(0.25f * sm[2]), __float2bfloat16(0.25f * sm[3]));
+                }
+            }
+        }
+        __syncthreads();
+        constexpr int VO = COUT / 8;  // 16-byte vectors per output pixel
+        if (act) {
+            for (int i = tid; i < TY * TX * VO; i += CONV_THREADS) {
+                const int c8 = i % VO, pix = i / VO;
+                const int r = pix / TX, c = pix % TX;
+                *reinterpret_cast<uint4*>(act + (((size_t)b * H + y0 + r) * W + x0 + c) * COUT + c8 * 8) =
+                    *reinterpret_cast<const uint4*>(ost + pix * S::OSTR + c8 * 8);
             }
         }
         if (pooled) {
-            // sum the two tile rows (same thread), then the x pair (lanes g, g^1)
-            float s[4];
-#pragma unroll
-            for (int j = 0; j < 4; ++j) s[j] = v[0][j] + v[1][j];
-#pragma unroll
-            for (int j = 0; j < 4; ++j) s[j] += __shfl_xor_sync(0xffffffffu, s[j], 4);
-            if ((g & 1) == 0) {
-                const int H2 = H / 2, W2 = W / 2;
-                const int py = (y0 + 2 * warp) / 2;
-                const size_t base = (((size_t)b * H2 + py) * W2 + x0 / 2) * COUT;
-                *reinterpret_cast<uint32_t*>(pooled + base + (size_t)(g / 2) * COUT + ch) =
-                    pack2(__float2bfloat16(0.25f * s[0]), __float2bfloat16(0.25f * s[1]));
-                *reinterpret_cast<uint32_t*>(pooled + base + (size_t)(g / 2 + 4) * COUT + ch) =
-                    pack2(__float2bfloat16(0.25f * s[2]), __float2bfloat16(0.25f * s[3]));
+            const int H2 = H / 2, W2 = W / 2;
+            for (int i = tid; i < (TY / 2) * (TX / 2) * VO; i += CONV_THREADS) {
+                const int c8 = i % VO, pix = i / VO;
+                const int r = pix / (TX / 2), c = pix % (TX / 2);
+                *reinterpret_cast<uint4*>(
+                    pooled + (((size_t)b * H2 + y0 / 2 + r) * W2 + x0 / 2 + c) * COUT + c8 * 8) =
+                    *reinterpret_cast<const uint4*>(pst + pix * S::OSTR + c8 * 8);
             }
         }
     }
@@ -223,18 +293,12 @@ conv3x3_wgrad(const bf16* __restrict__ x, const bf16* __restrict__ dA, float* __
         const int rem = tile % (tiles_x * tiles_y);
         const int y0 = (rem / tiles_x) * TY, x0 = (rem % tiles_x) * TX;
         __syncthreads();
-        for (int i = tid; i < (TY + 2) * (TX + 2) * CIN; i += CONV_THREADS) {
-            const int c = i % CIN, px = (i / CIN) % (TX + 2), py = i / (CIN * (TX + 2));
-            const int yy = y0 + py - 1, xx = x0 + px - 1;
-            bf16 v = zero;
-            if (yy >= 0 && yy < H && xx >= 0 && xx < W)
-                v = x[(((size_t)b * H + yy) * W + xx) * CIN + c];
-            patch[(py * (TX + 2) + px) * S::CPAD + c] = v;
-        }
-        for (int i = tid; i < TY * TX * COUT; i += CONV_THREADS) {
-            const int n = i % COUT, p = i / COUT;
+        load_patch<CIN>(x, patch, b, y0, x0, H, W, tid);
+        for (int i = tid; i < TY * TX * (COUT / 8); i += CONV_THREADS) {
+            const int c8 = i % (COUT / 8), p = i / (COUT / 8);
             const int yy = y0 + p / TX, xx = x0 + p % TX;
-            dtile[p * DSTR + n] = dA[(((size_t)b * H + yy) * W + xx) * COUT + n];
+            *reinterpret_cast<uint4*>(dtile + p * DSTR + c8 * 8) =
+                *reinterpret_cast<const uint4*>(dA + (((size_t)b * H + yy) * W + xx) * COUT + c8 * 8);
         }
         __syncthreads();
         if (tid < COUT)
@@ -402,13 +466,29 @@ lgm_status lgm_cnn_conv3x3_fwd(int32_t cin, const void* x, const void* w, const 
         (pooled && (H % 2 || W % 2)) || (!act && !pooled))
         return LGM_ERR_INVALID_ARGUMENT;
     cudaStream_t st = (cudaStream_t)stream;
-    const int grid = B * (H / TY) * (W / TX);
+    const int ntiles = B * (H / TY) * (W / TX);
+    // persistent: at most the CTAs that fit on the device at once
+    static int cap[2] = {0, 0};
+    const int ci = cin == 1 ? 0 : 1;
+    if (!cap[ci]) {
+        int dev = 0, sms = 0, per_sm = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (ci == 0)
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, conv3x3_fwd<1>, CONV_THREADS,
+                                                          ConvShape<1>::SMEM);
+        else
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, conv3x3_fwd<COUT>, CONV_THREADS,
+                                                          ConvShape<COUT>::SMEM);
+        cap[ci] = std::max(1, sms * std::max(1, per_sm));
+    }
+    const int grid = std::min(ntiles, cap[ci]);
     if (cin == 1) {
         conv3x3_fwd<1><<<grid, CONV_THREADS, ConvShape<1>::SMEM, st>>>(
-            (const bf16*)x, (const bf16*)w, bias, (bf16*)act, (bf16*)pooled, H, W, relu);
+            (const bf16*)x, (const bf16*)w, bias, (bf16*)act, (bf16*)pooled, B, H, W, relu);
     } else {
         conv3x3_fwd<COUT><<<grid, CONV_THREADS, ConvShape<COUT>::SMEM, st>>>(
-            (const bf16*)x, (const bf16*)w, bias, (bf16*)act, (bf16*)pooled, H, W, relu);
+            (const bf16*)x, (const bf16*)w, bias, (bf16*)act, (bf16*)pooled, B, H, W, relu);
     }
     return launch_check();
 }

@@ -351,6 +351,8 @@ constexpr int kGuardThreads = 256;
 // Blocks per replica of the batched guard: flagged decisions of one replica
 // are spread over them (a replica with M charges flags ~1e-3 M per step).
 constexpr int kGuardBlocksPerReplica = 4;
+// Indices per thread of the batched element-wise kernels (see LGM_BATCH_LOOP).
+constexpr int kItemsPerThread = 4;
 
 // FP64 potentials at two sites in one pass over the sources (the guard's
 // re-evaluation): the same cutoff and image rules as the pair kernel, terms
@@ -652,48 +654,40 @@ __global__ void __launch_bounds__(kCompactThreads) k_compact_inject(Dev D) {
 }
 
 // Batched kernels: block b works for replica map[b].x as its local block
-// map[b].y (every block lies inside one replica, so warp-level sums stay
-// within a replica).
-#define LGM_BATCH_INDEX(map) ((map).y * (int)blockDim.x + (int)threadIdx.x)
-__global__ void kb_choose(const Dev* R, const int2* map) {
-    const int2 m = map[blockIdx.x]; choose_body(R[m.x], LGM_BATCH_INDEX(m));
-}
-__global__ void kb_pack(const Dev* R, const int2* map) {
-    const int2 m = map[blockIdx.x]; pack_body(R[m.x], LGM_BATCH_INDEX(m));
-}
-__global__ void kb_finalize(const Dev* R, const int2* map) {
-    const int2 m = map[blockIdx.x]; finalize_body(R[m.x], LGM_BATCH_INDEX(m));
-}
-__global__ void kb_decide(const Dev* R, const int2* map) {
-    const int2 m = map[blockIdx.x]; decide_body(R[m.x], LGM_BATCH_INDEX(m));
-}
-// blocks_per_replica consecutive blocks per replica
-__global__ void __launch_bounds__(kGuardThreads) kb_guard(const Dev* R, int blocks_per_replica) {
+// map[b].y of map[b].z blocks, over indices [0, map[b].w) of that replica with
+// a block-uniform stride (every block lies inside one replica, so warp-level
+// sums stay within a replica, and every thread of a block runs the same number
+// of iterations).  A replica gets one block per kItemsPerThread * 256 indices
+// of its capacity, so small replicas in a big batch cost few idle blocks.
+#define LGM_BATCH_LOOP(CALL)                                                          \
+    const int4 m = map[blockIdx.x];                                                   \
+    const Dev& D = R[m.x];                                                            \
+    for (int base = m.y * (int)blockDim.x; base < m.w; base += m.z * (int)blockDim.x) { \
+        const int i = base + (int)threadIdx.x;                                        \
+        CALL;                                                                         \
+    }
+__global__ void kb_choose(const Dev* R, const int4* map) { LGM_BATCH_LOOP(choose_body(D, i)) }
+__global__ void kb_pack(const Dev* R, const int4* map) { LGM_BATCH_LOOP(pack_body(D, i)) }
+__global__ void kb_finalize(const Dev* R, const int4* map) { LGM_BATCH_LOOP(finalize_body(D, i)) }
+__global__ void kb_decide(const Dev* R, const int4* map) { LGM_BATCH_LOOP(decide_body(D, i)) }
+__global__ void __launch_bounds__(kGuardThreads) kb_guard(const Dev* R, const int4* map) {
     __shared__ double2 red[kGuardThreads];
-    guard_body(R[blockIdx.x / blocks_per_replica], blockIdx.x % blocks_per_replica,
-               blocks_per_replica, red);
+    const int4 m = map[blockIdx.x];
+    guard_body(R[m.x], m.y, m.z, red);
 }
-__global__ void kb_hmap(const Dev* R, const int2* map) {
-    const int2 m = map[blockIdx.x]; hmap_body(R[m.x], LGM_BATCH_INDEX(m), true);
+__global__ void kb_hmap(const Dev* R, const int4* map) { LGM_BATCH_LOOP(hmap_body(D, i, true)) }
+__global__ void kb_recomb_propose(const Dev* R, const int4* map) {
+    LGM_BATCH_LOOP(recomb_propose_body(D, i))
 }
-__global__ void kb_recomb_propose(const Dev* R, const int2* map) {
-    const int2 m = map[blockIdx.x]; recomb_propose_body(R[m.x], LGM_BATCH_INDEX(m));
+__global__ void kb_recomb_resolve(const Dev* R, const int4* map) {
+    LGM_BATCH_LOOP(recomb_resolve_body(D, i))
 }
-__global__ void kb_recomb_resolve(const Dev* R, const int2* map) {
-    const int2 m = map[blockIdx.x]; recomb_resolve_body(R[m.x], LGM_BATCH_INDEX(m));
+__global__ void kb_recomb_reset(const Dev* R, const int4* map) {
+    LGM_BATCH_LOOP(recomb_reset_body(D, i))
 }
-__global__ void kb_recomb_reset(const Dev* R, const int2* map) {
-    const int2 m = map[blockIdx.x]; recomb_reset_body(R[m.x], LGM_BATCH_INDEX(m));
-}
-__global__ void kb_claim(const Dev* R, const int2* map) {
-    const int2 m = map[blockIdx.x]; claim_body(R[m.x], LGM_BATCH_INDEX(m));
-}
-__global__ void kb_move(const Dev* R, const int2* map) {
-    const int2 m = map[blockIdx.x]; move_body(R[m.x], LGM_BATCH_INDEX(m));
-}
-__global__ void kb_unclaim(const Dev* R, const int2* map) {
-    const int2 m = map[blockIdx.x]; unclaim_body(R[m.x], LGM_BATCH_INDEX(m));
-}
+__global__ void kb_claim(const Dev* R, const int4* map) { LGM_BATCH_LOOP(claim_body(D, i)) }
+__global__ void kb_move(const Dev* R, const int4* map) { LGM_BATCH_LOOP(move_body(D, i)) }
+__global__ void kb_unclaim(const Dev* R, const int4* map) { LGM_BATCH_LOOP(unclaim_body(D, i)) }
 // one block per replica
 __global__ void __launch_bounds__(kCompactThreads) kb_compact_inject(const Dev* R) {
     __shared__ int warp_sums[32];
@@ -1351,8 +1345,8 @@ struct lgm_kmc_batch {
     PairArgs* d_pargs = nullptr;
     int4* d_items = nullptr;
     int n_items = 0;
-    int2 *map_car = nullptr, *map_pack = nullptr, *map_fin = nullptr;
-    int nb_car = 0, nb_pack = 0, nb_fin = 0;
+    int4 *map_car = nullptr, *map_pack = nullptr, *map_fin = nullptr, *map_guard = nullptr;
+    int nb_car = 0, nb_pack = 0, nb_fin = 0, nb_guard = 0;
     int variant = 0, cpi = 16;
     std::vector<Dev> hD;
     std::string err;
@@ -1429,7 +1423,7 @@ lgm_status enqueue_batch_step(lgm_kmc_batch* b) {
         kb_finalize<<<b->nb_fin, 256, 0, st>>>(b->d_reps, b->map_fin);
     }
     kb_decide<<<b->nb_car, 256, 0, st>>>(b->d_reps, b->map_car);
-    if (b->coulomb) kb_guard<<<kGuardBlocksPerReplica * R, kGuardThreads, 0, st>>>(b->d_reps, kGuardBlocksPerReplica);
+    if (b->coulomb) kb_guard<<<b->nb_guard, kGuardThreads, 0, st>>>(b->d_reps, b->map_guard);
     if (b->recomb) {
         kb_hmap<<<b->nb_car, 256, 0, st>>>(b->d_reps, b->map_car);
         kb_recomb_propose<<<b->nb_car, 256, 0, st>>>(b->d_reps, b->map_car);
@@ -1516,22 +1510,30 @@ lgm_status lgm_kmc_batch_create(const lgm_params* params, int32_t count, int32_t
         cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess)
         return bail(LGM_ERR_CUDA, "stream");
     for (lgm_kmc* k : b->reps) b->hD.push_back(k->D);
-    // block maps
-    std::vector<int2> car, pack, fin;
+    // block maps: {replica, local block, blocks of the replica, index bound}
+    std::vector<int4> car, pack, fin, guard;
+    auto add = [](std::vector<int4>& v, int r, int bound) {
+        const int nb = std::max(1, (bound + kItemsPerThread * 256 - 1) / (kItemsPerThread * 256));
+        for (int i = 0; i < nb; ++i) v.push_back(make_int4(r, i, nb, bound));
+    };
     for (int r = 0; r < count; ++r) {
         const Dev& D = b->hD[r];
         const int ncap = std::max(1, D.cap_e + D.cap_h);
-        for (int i = 0; i < (ncap + 255) / 256; ++i) car.push_back(make_int2(r, i));
-        const int np = std::max(D.src_cap, D.tpad_cap);
-        for (int i = 0; i < (np + 255) / 256; ++i) pack.push_back(make_int2(r, i));
-        for (int i = 0; i < (2 * ncap + 255) / 256; ++i) fin.push_back(make_int2(r, i));
+        add(car, r, ncap);
+        add(pack, r, std::max(D.src_cap, D.tpad_cap));
+        add(fin, r, 2 * ncap);
+        // flagged decisions grow with the charge count: one block per 2048 of capacity
+        const int ng = std::min(kGuardBlocksPerReplica, std::max(1, (ncap + 2047) / 2048));
+        for (int i = 0; i < ng; ++i) guard.push_back(make_int4(r, i, ng, 0));
     }
-    auto upload = [&](int2** dst, const std::vector<int2>& v) -> bool {
-        return cudaMalloc(dst, sizeof(int2) * v.size()) == cudaSuccess &&
-               cudaMemcpy(*dst, v.data(), sizeof(int2) * v.size(), cudaMemcpyHostToDevice) == cudaSuccess;
+    auto upload = [&](int4** dst, const std::vector<int4>& v) -> bool {
+        return cudaMalloc(dst, sizeof(int4) * v.size()) == cudaSuccess &&
+               cudaMemcpy(*dst, v.data(), sizeof(int4) * v.size(), cudaMemcpyHostToDevice) == cudaSuccess;
     };
-    if (!upload(&b->map_car, car) || !upload(&b->map_pack, pack) || !upload(&b->map_fin, fin))
+    if (!upload(&b->map_car, car) || !upload(&b->map_pack, pack) || !upload(&b->map_fin, fin) ||
+        !upload(&b->map_guard, guard))
         return bail(LGM_ERR_CUDA, "block maps");
+    b->nb_guard = (int)guard.size();
     b->nb_car = (int)car.size();
     b->nb_pack = (int)pack.size();
     b->nb_fin = (int)fin.size();
@@ -1557,7 +1559,8 @@ lgm_status lgm_kmc_batch_destroy(lgm_kmc_batch* b) {
     if (b->stream) cudaStreamSynchronize(b->stream);
     if (b->exec) cudaGraphExecDestroy(b->exec);
     if (b->graph) cudaGraphDestroy(b->graph);
-    void* ptrs[] = {b->d_reps, b->d_pargs, b->d_items, b->map_car, b->map_pack, b->map_fin};
+    void* ptrs[] = {b->d_reps, b->d_pargs, b->d_items, b->map_car, b->map_pack, b->map_fin,
+                    b->map_guard};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (b->stream) cudaStreamDestroy(b->stream);

@@ -378,8 +378,10 @@ def symmetry(x16, k):
 class Surrogate:
     """Ensemble of CNNs on standardised log(current), log(efficiency).
 
-    Training draws one of the four device symmetries per mini-batch;
-    ``tta`` > 1 averages predictions over that many symmetries."""
+    Training draws one of the four device symmetries per mini-batch, which is
+    right for kMC labels (invariant under them) and wrong for targets that are
+    not, such as the donor fraction (augment=False there); ``tta`` > 1
+    averages predictions over that many symmetries."""
 
     def __init__(self, members=4, seed=0, device="cuda", log_targets=True, augment=True, tta=1):
         self.device = device

@@ -240,7 +240,9 @@ def test_training_fits_a_morphology_property():
     bonds = ((ph[:, 1:] != ph[:, :-1]).sum(dim=(1, 2)) +
              (ph[:, :, 1:] != ph[:, :, :-1]).sum(dim=(1, 2))).float() / (2 * 128 * 127)
     y = torch.stack([1 - ph.float().mean(dim=(1, 2)), bonds], 1).cpu().numpy()
-    model = S.Surrogate(members=1, seed=2)
+    # the donor fraction is not invariant under the phase exchange, so no
+    # symmetry augmentation and linear targets here
+    model = S.Surrogate(members=1, seed=2, log_targets=False, augment=False)
     hist = model.fit(ph[:512], y[:512], epochs=20, batch=64, lr=3e-3)
     assert hist[-1][2] < 0.5 * hist[0][2]
     mean, _ = model.predict(ph[512:])
