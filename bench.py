@@ -291,6 +291,103 @@ def batch_run(L, args, rank):
             "build_s": build_s}
 
 
+def other_kernels_run(L, args, fp32_peak):
+    """Rows a2 and a3: the Gaussian kernel-2 sum on config 3 (128x128x64,
+    sigma 1, cutoff 30) and the whole-grid kernel 1 (every site of config 1's
+    128x128 lattice) -- pair kernel time from the library's own CUDA events."""
+    import torch
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
+    st = torch.cuda.Stream(dev)
+    out = {}
+    # gauss2, config 3
+    w = WORKLOADS["cfg3_gauss"]
+    s_all, q_all, n = make_inputs(w, 5)
+    T = len(s_all)
+    with L.Coulomb(w["X"], w["Y"], w["Z"], cutoff=w["cutoff"], sigma=w["sigma"],
+                   device=dev.index) as ctx:
+        d_s, d_q = torch.from_numpy(s_all).to(dev), torch.from_numpy(q_all).to(dev)
+        d_o = torch.empty(T, dtype=torch.float64, device=dev)
+        v = ctx.autotune(n, T, L.GAUSS, 1)
+        ctx.set_variant(v)
+        ctx.set_timing(True)
+        ms = []
+        for i in range(args.warmup + args.steps):
+            ctx.potentials_async(d_s.data_ptr(), d_q.data_ptr(), n, d_s.data_ptr(), T,
+                                 d_o.data_ptr(), L.GAUSS, 1, st.cuda_stream)
+            ctx.sync(st.cuda_stream)
+            if i >= args.warmup:
+                ms.append(ctx.last_launch()["pair_kernel_ms"])
+        pk = float(np.median(ms))
+        pairs = n * T
+        achieved = FLOP_PER_PAIR * pairs / (pk * 1e-3) / 1e12
+        out["gauss2_cfg3"] = {
+            "workload": w["desc"], "pairs_per_launch": pairs, "pair_kernel_ms": pk,
+            "pair_evals_per_s": pairs / (pk * 1e-3),
+            "roofline": {"bound": "fp32", "achieved": achieved, "peak": fp32_peak,
+                         "unit": "TFLOP/s", "frac": achieved / fp32_peak,
+                         "note": "11 FLOP per pair as for point charges; erf(f r)/r is a "
+                                 "shared-memory table gather on top"},
+            "tile_variant": dict(ctx.variants()[v], id=v)}
+    # kernel 1, every site of config 1's lattice
+    w = WORKLOADS["cfg1_2d_holes"]
+    s_all, q_all, n = make_inputs(w, 6)
+    vol = w["X"] * w["Y"] * w["Z"]
+    with L.Coulomb(w["X"], w["Y"], w["Z"], cutoff=w["cutoff"], device=dev.index) as ctx:
+        d_s = torch.from_numpy(s_all[:n].copy()).to(dev)
+        d_q = torch.from_numpy(q_all[:n].copy()).to(dev)
+        d_o = torch.empty(vol, dtype=torch.float64, device=dev)
+        ctx.set_timing(True)
+        ms = []
+        for i in range(args.warmup + args.steps):
+            ctx.kernel1_async(d_s.data_ptr(), d_q.data_ptr(), n, d_o.data_ptr(), L.POINT,
+                              st.cuda_stream)
+            ctx.sync(st.cuda_stream)
+            if i >= args.warmup:
+                ms.append(ctx.last_launch()["pair_kernel_ms"])
+        pk = float(np.median(ms))
+        out["kernel1_cfg1"] = {"workload": f"every site of {w['desc']}", "charges": n,
+                               "sites": vol, "pair_kernel_ms": pk,
+                               "site_charge_evals_per_s": vol * n / (pk * 1e-3),
+                               "note": "163 charges: launch- and latency-bound; the "
+                                       "reference runs this only for output.coulomb"}
+    return out
+
+
+def cnn_layers(S, peaks):
+    """Per-layer timing of the surrogate's conv kernels (1024 images, CUDA
+    events): layer 1 against HBM, layer 2 against the measured bf16 GEMM peak."""
+    import torch
+    B = 1024
+    ph, _, _ = S.grf_morphologies(B, seed=11)
+    x16 = S.phases_to_input(ph)
+    prm = S.init_params(0)
+    w1, w2 = S.conv_weights_bf16(prm[0], 1), S.conv_weights_bf16(prm[2], 32)
+    _, p1 = S.conv3x3(x16, w1, prm[1], 128, 128, keep_act=False)
+
+    def timeit(fn, n=20):
+        for _ in range(3):
+            fn()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(n):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / n
+    t1 = timeit(lambda: S.conv3x3(x16, w1, prm[1], 128, 128, keep_act=False))
+    t2 = timeit(lambda: S.conv3x3(p1, w2, prm[3], 64, 64, keep_act=False))
+    b1 = B * 128 * 128 * 2 + B * 64 * 64 * 32 * 2            # image in, pooled map out
+    f2 = 2 * B * 64 * 64 * 32 * 288                            # layer-2 MACs x 2
+    hbm, bf16 = float(peaks.get("hbm_gbs", 6650.0)), float(peaks.get("bf16_tflops", 1590.0))
+    return {"images": B,
+            "conv1_pool": {"ms": t1, "achieved": b1 / (t1 * 1e-3) / 1e9, "peak": hbm,
+                           "unit": "GB/s", "frac": b1 / (t1 * 1e-3) / 1e9 / hbm, "bound": "hbm"},
+            "conv2_pool": {"ms": t2, "achieved": f2 / (t2 * 1e-3) / 1e12, "peak": bf16,
+                           "unit": "TFLOP/s", "frac": f2 / (t2 * 1e-3) / 1e12 / bf16,
+                           "bound": "tensor",
+                           "note": "mma.sync m16n8k16 bf16; peak = measured cuBLAS bf16 GEMM"}}
+
+
 def surrogate_run(args, rank):
     """Morphology screening: the CNN ensemble over fresh GRF candidates vs
     labelling the same kind of morphology with the batched solar-cell kMC."""
@@ -340,7 +437,8 @@ def surrogate_run(args, rank):
                          "teardown_s": teardown_s,
                          "note": f"{full}-step label cost = set-up + teardown + {full} x the "
                                  f"batched step time measured over {K} steps"},
-           "speedup_vs_kmc": (n / screen_s) / (R / kmc_label_s)}
+           "speedup_vs_kmc": (n / screen_s) / (R / kmc_label_s),
+           "cnn_layers": cnn_layers(S, measured_peaks())}
     if rank == 0 and not args.no_cpu_baseline:
         # the reference's screening score (ga.py:83-141), restated, on the host
         from oracle import ga_score as G
@@ -372,6 +470,7 @@ def main():
     ap.add_argument("--batch-steps", type=int, default=20)
     ap.add_argument("--batch-sample", type=int, default=32)
     ap.add_argument("--no-surrogate", action="store_true")
+    ap.add_argument("--no-other-kernels", action="store_true")
     ap.add_argument("--surrogate-candidates", type=int, default=100000)
     ap.add_argument("--surrogate-label-replicas", type=int, default=4096)
     ap.add_argument("--surrogate-label-steps", type=int, default=2000)
@@ -522,6 +621,14 @@ def main():
     if clocks.get("sm_mhz"):
         roof["frac_at_sampled_clock"] = achieved / (sms * 256 * clocks["sm_mhz"] * 1e6 / 1e12)
 
+    others = None if args.no_other_kernels else other_kernels_run(L, args, fp32_peak)
+    if kmc is not None:
+        # pair evaluations the step's Coulomb sums make, over the whole step time
+        kp = kmc["carriers"] * 2 * kmc["carriers"] * nterms
+        kmc["pair_evals_per_s_in_step"] = kp / (kmc["ms_per_step"] * 1e-3)
+        kmc["pair_frac_of_fp32_peak_in_step"] = (FLOP_PER_PAIR * kmc["pair_evals_per_s_in_step"]
+                                                 / 1e12 / fp32_peak)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
@@ -541,7 +648,7 @@ def main():
                        "tile_variant": dict(ctx.variants()[variant], id=variant),
                        "parallelism": "replicas" if world > 1 else "single"},
             "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks, "kmc": kmc,
-            "kmc_batched": batch, "surrogate": surrogate,
+            "kmc_batched": batch, "surrogate": surrogate, "other_kernels": others,
             "gpu_launches": launches, "accuracy": acc,
         }
         print(json.dumps(line), flush=True)

@@ -21,6 +21,7 @@
 #include <stdint.h>
 
 #include <algorithm>
+#include <type_traits>
 
 #include "langmuir_b200_cnn.h"
 
@@ -86,6 +87,50 @@ __device__ __forceinline__ void load_patch(const bf16* __restrict__ x, bf16* pat
     }
 }
 
+// The patch of the next tile, held in registers while the current tile
+// computes (software pipelining of the global loads): load() issues the
+// loads, store() writes them to shared memory at the next tile's start.
+template <int CIN>
+struct PatchPrefetch {
+    static constexpr int V = CIN == 1 ? 1 : CIN / 8;  // values per pixel
+    static constexpr int ITEMS = (TY + 2) * (TX + 2) * V;
+    static constexpr int PER = (ITEMS + CONV_THREADS - 1) / CONV_THREADS;
+    using T = typename std::conditional<CIN == 1, unsigned short, uint4>::type;
+    T r[PER];
+
+    __device__ __forceinline__ void load(const bf16* __restrict__ x, int b, int y0, int x0, int H,
+                                         int W, int tid) {
+#pragma unroll
+        for (int k = 0; k < PER; ++k) {
+            const int i = tid + k * CONV_THREADS;
+            const int c8 = i % V, pix = i / V;
+            const int px = pix % (TX + 2), py = pix / (TX + 2);
+            const int yy = y0 + py - 1, xx = x0 + px - 1;
+            const bool in = i < ITEMS && yy >= 0 && yy < H && xx >= 0 && xx < W;
+            const size_t off = (((size_t)b * H + (in ? yy : 0)) * W + (in ? xx : 0)) * CIN + c8 * 8;
+            if constexpr (CIN == 1) {
+                r[k] = in ? reinterpret_cast<const unsigned short*>(x)[off] : (unsigned short)0;
+            } else {
+                r[k] = in ? *reinterpret_cast<const uint4*>(x + off) : make_uint4(0u, 0u, 0u, 0u);
+            }
+        }
+    }
+    __device__ __forceinline__ void store(bf16* patch, int tid) const {
+        using S = ConvShape<CIN>;
+#pragma unroll
+        for (int k = 0; k < PER; ++k) {
+            const int i = tid + k * CONV_THREADS;
+            if (i >= ITEMS) break;
+            const int c8 = i % V, pix = i / V;
+            if constexpr (CIN == 1) {
+                reinterpret_cast<unsigned short*>(patch)[pix * S::CPAD] = r[k];
+            } else {
+                *reinterpret_cast<uint4*>(patch + pix * S::CPAD + c8 * 8) = r[k];
+            }
+        }
+    }
+};
+
 // x: [B,H,W,CIN]; w: [COUT][KPAD] (k = (ky*3 + kx)*CIN + c); act: [B,H,W,COUT]
 // (optional); pooled: [B,H/2,W/2,COUT] (optional).  H % 8 == 0, W % 16 == 0.
 // Persistent over tiles: the weights are staged once per CTA, each 8x16 tile's
@@ -117,13 +162,29 @@ conv3x3_fwd(const bf16* __restrict__ x, const bf16* __restrict__ w, const float*
         bv[n][1] = bias ? bias[n * 8 + 2 * t + 1] : 0.f;
     }
 
-    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-        const int b = tile / (tiles_x * tiles_y);
+    PatchPrefetch<CIN> pf;
+    auto origin = [&](int tile, int& b, int& y0, int& x0) {
+        b = tile / (tiles_x * tiles_y);
         const int rem = tile % (tiles_x * tiles_y);
-        const int y0 = (rem / tiles_x) * TY, x0 = (rem % tiles_x) * TX;
+        y0 = (rem / tiles_x) * TY;
+        x0 = (rem % tiles_x) * TX;
+    };
+    if ((int)blockIdx.x < ntiles) {
+        int b0, y00, x00;
+        origin(blockIdx.x, b0, y00, x00);
+        pf.load(x, b0, y00, x00, H, W, tid);
+    }
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        int b, y0, x0;
+        origin(tile, b, y0, x0);
         __syncthreads();  // the previous tile is done with patch, ost and pst
-        load_patch<CIN>(x, patch, b, y0, x0, H, W, tid);
+        pf.store(patch, tid);
         __syncthreads();
+        if (tile + (int)gridDim.x < ntiles) {  // next tile's loads overlap this tile's math
+            int bn, yn, xn;
+            origin(tile + gridDim.x, bn, yn, xn);
+            pf.load(x, bn, yn, xn, H, W, tid);
+        }
 
         float acc[2][4][4];
 #pragma unroll

@@ -206,7 +206,7 @@ __device__ __forceinline__ void pack_body(const Dev& D, const int j) {
         D.cnt[I_TPHYS] = D.nterms * tpad;
         D.cnt[I_TPAD] = tpad;
     }
-    if (j < D.src_cap) {
+    if (j < nsrc) {  // records past the live chunks are never read
         float a = 0.f, b = 0.f, c = 0.f, d = -0.5f, q = 0.f;
         int s = -1;
         if (j < pe) { if (j < ne) { s = D.e_site[j]; q = -1.f; } }
@@ -1347,6 +1347,7 @@ struct lgm_kmc_batch {
     int n_items = 0;
     int4 *map_car = nullptr, *map_pack = nullptr, *map_fin = nullptr, *map_guard = nullptr;
     int nb_car = 0, nb_pack = 0, nb_fin = 0, nb_guard = 0;
+    int compact_threads = kCompactThreads;  // block size of the per-replica list compaction
     int variant = 0, cpi = 16;
     std::vector<Dev> hD;
     std::string err;
@@ -1433,7 +1434,7 @@ lgm_status enqueue_batch_step(lgm_kmc_batch* b) {
     kb_claim<<<b->nb_car, 256, 0, st>>>(b->d_reps, b->map_car);
     kb_move<<<b->nb_car, 256, 0, st>>>(b->d_reps, b->map_car);
     kb_unclaim<<<b->nb_car, 256, 0, st>>>(b->d_reps, b->map_car);
-    kb_compact_inject<<<R, kCompactThreads, 0, st>>>(b->d_reps);
+    kb_compact_inject<<<R, b->compact_threads, 0, st>>>(b->d_reps);
     BCUDA(b, cudaGetLastError());
     return LGM_OK;
 }
@@ -1534,6 +1535,10 @@ lgm_status lgm_kmc_batch_create(const lgm_params* params, int32_t count, int32_t
         !upload(&b->map_guard, guard))
         return bail(LGM_ERR_CUDA, "block maps");
     b->nb_guard = (int)guard.size();
+    // the compaction loops over its list in blocks: small replicas need no 1024-thread block
+    int max_cap = 1;
+    for (const Dev& D : b->hD) max_cap = std::max(max_cap, std::max(D.cap_e, D.cap_h));
+    b->compact_threads = max_cap > 4096 ? kCompactThreads : 256;
     b->nb_car = (int)car.size();
     b->nb_pack = (int)pack.size();
     b->nb_fin = (int)fin.size();
