@@ -728,8 +728,41 @@ void host_neighbors1(int X, int Y, int Z, int site, std::vector<int>& nb) {
 
 }  // namespace
 
+// Bump allocator over large device chunks, owned by a batch: its replicas take
+// their buffers from it instead of one cudaMalloc each, and the chunks are
+// freed together when the batch is destroyed.
+struct DevicePool {
+    std::vector<void*> chunks;
+    char* cur = nullptr;
+    size_t left = 0;
+    cudaError_t take(size_t bytes, void** out) {
+        bytes = (bytes + 255) / 256 * 256;
+        if (bytes > left) {
+            const size_t sz = std::max(bytes, (size_t)256 << 20);
+            char* c = nullptr;
+            const cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&c), sz);
+            if (e != cudaSuccess) return e;
+            chunks.push_back(c);
+            cur = c;
+            left = sz;
+        }
+        *out = cur;
+        cur += bytes;
+        left -= bytes;
+        return cudaSuccess;
+    }
+    void release() {
+        for (void* c : chunks) cudaFree(c);
+        chunks.clear();
+        cur = nullptr;
+        left = 0;
+    }
+};
+
 struct lgm_kmc {
     lgm_params p{};
+    DevicePool* pool = nullptr;  // a batch's pool, or null: own allocations
+    bool own_stream = true;
     int device = 0;
     uint32_t replica = 0;
     int V = 0, max_e = 0, max_h = 0;
@@ -765,7 +798,12 @@ lgm_status kfail(lgm_kmc* k, lgm_status s, const std::string& m) {
 
 template <class T>
 lgm_status dalloc(lgm_kmc* k, T** p, size_t n) {
-    KCUDA(k, cudaMalloc(reinterpret_cast<void**>(p), std::max<size_t>(n, 1) * sizeof(T)));
+    const size_t bytes = std::max<size_t>(n, 1) * sizeof(T);
+    if (k->pool) {
+        KCUDA(k, k->pool->take(bytes, reinterpret_cast<void**>(p)));
+        return LGM_OK;
+    }
+    KCUDA(k, cudaMalloc(reinterpret_cast<void**>(p), bytes));
     k->allocs.push_back(*p);
     return LGM_OK;
 }
@@ -782,8 +820,12 @@ struct Arena {
         size_t total = 0;
         for (auto& s : slots) total += (s.second + 255) / 256 * 256;
         char* base = nullptr;
-        KCUDA(k, cudaMalloc(reinterpret_cast<void**>(&base), std::max<size_t>(total, 256)));
-        k->allocs.push_back(base);
+        if (k->pool) {
+            KCUDA(k, k->pool->take(std::max<size_t>(total, 256), reinterpret_cast<void**>(&base)));
+        } else {
+            KCUDA(k, cudaMalloc(reinterpret_cast<void**>(&base), std::max<size_t>(total, 256)));
+            k->allocs.push_back(base);
+        }
         size_t off = 0;
         for (auto& s : slots) {
             *s.first = base + off;
@@ -950,12 +992,16 @@ lgm_status enqueue_step(lgm_kmc* k) {
 
 extern "C" {
 
-lgm_status lgm_kmc_create(const lgm_params* pin, int32_t device, uint32_t replica, lgm_kmc** out) {
+// One replica.  pool / shared: a batch's device pool and stream (the batch
+// synchronises once after creating all replicas), or null for a standalone one.
+static lgm_status kmc_create_impl(const lgm_params* pin, int32_t device, uint32_t replica,
+                                  lgm_kmc** out, DevicePool* pool, cudaStream_t shared) {
     if (!pin || !out) return LGM_ERR_INVALID_ARGUMENT;
     *out = nullptr;
     lgm_kmc* k = new (std::nothrow) lgm_kmc();
     if (!k) return LGM_ERR_INVALID_ARGUMENT;
     k->p = *pin;
+    k->pool = pool;
     k->replica = replica;
     char msg[256] = {0};
     lgm_status s = lgm_params_check(&k->p, msg, sizeof msg);
@@ -984,8 +1030,12 @@ lgm_status lgm_kmc_create(const lgm_params* pin, int32_t device, uint32_t replic
         cudaDeviceGetAttribute(&n_sms, cudaDevAttrMultiProcessorCount, k->device) != cudaSuccess ||
         cc_major != 10)
         return bail(LGM_ERR_NO_DEVICE, "device is not sm_100 (B200)");
-    if (cudaStreamCreateWithFlags(&k->stream, cudaStreamNonBlocking) != cudaSuccess)
+    if (shared) {
+        k->stream = shared;
+        k->own_stream = false;
+    } else if (cudaStreamCreateWithFlags(&k->stream, cudaStreamNonBlocking) != cudaSuccess) {
         return bail(LGM_ERR_CUDA, "stream");
+    }
 
     Dev& D = k->D;
     D.X = p.grid_x; D.Y = p.grid_y; D.Z = p.grid_z; D.XY = D.X * D.Y; D.V = k->V;
@@ -1154,19 +1204,23 @@ lgm_status lgm_kmc_create(const lgm_params* pin, int32_t device, uint32_t replic
     if ((st = upload_carriers(k, k->e0.data(), (int)k->e0.size(), k->h0.data(),
                               (int)k->h0.size())) != LGM_OK)
         return bail(st, k->err);
-    if (cudaDeviceSynchronize() != cudaSuccess) return bail(LGM_ERR_CUDA, "set-up");
+    if (!pool && cudaDeviceSynchronize() != cudaSuccess) return bail(LGM_ERR_CUDA, "set-up");
     *out = k;
     return LGM_OK;
+}
+
+lgm_status lgm_kmc_create(const lgm_params* pin, int32_t device, uint32_t replica, lgm_kmc** out) {
+    return kmc_create_impl(pin, device, replica, out, nullptr, nullptr);
 }
 
 lgm_status lgm_kmc_destroy(lgm_kmc* k) {
     if (!k) return LGM_OK;
     cudaSetDevice(k->device);
-    if (k->stream) cudaStreamSynchronize(k->stream);
+    if (k->stream && k->own_stream) cudaStreamSynchronize(k->stream);
     if (k->exec) cudaGraphExecDestroy(k->exec);
     if (k->graph) cudaGraphDestroy(k->graph);
     for (void* p : k->allocs) cudaFree(p);
-    if (k->stream) cudaStreamDestroy(k->stream);
+    if (k->stream && k->own_stream) cudaStreamDestroy(k->stream);
     delete k;
     return LGM_OK;
 }
@@ -1348,6 +1402,7 @@ struct lgm_kmc_batch {
     int4 *map_car = nullptr, *map_pack = nullptr, *map_fin = nullptr, *map_guard = nullptr;
     int nb_car = 0, nb_pack = 0, nb_fin = 0, nb_guard = 0;
     int compact_threads = kCompactThreads;  // block size of the per-replica list compaction
+    DevicePool pool;                         // every replica's buffers
     int variant = 0, cpi = 16;
     std::vector<Dev> hD;
     std::string err;
@@ -1493,12 +1548,18 @@ lgm_status lgm_kmc_batch_create(const lgm_params* params, int32_t count, int32_t
         return s;
     };
     b->device = device < 0 ? 0 : device;
+    if (cudaSetDevice(b->device) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess)
+        return bail(LGM_ERR_CUDA, "stream");
+    // replicas share the batch's stream and take their buffers from its pool
     for (int i = 0; i < count; ++i) {
         lgm_kmc* k = nullptr;
-        lgm_status s = lgm_kmc_create(&params[i], b->device, replica0 + (uint32_t)i, &k);
+        lgm_status s = kmc_create_impl(&params[i], b->device, replica0 + (uint32_t)i, &k,
+                                       &b->pool, b->stream);
         if (s != LGM_OK) return bail(s, "replica " + std::to_string(i) + ": " + lgm_kmc_last_error(nullptr));
         b->reps.push_back(k);
     }
+    if (cudaDeviceSynchronize() != cudaSuccess) return bail(LGM_ERR_CUDA, "replica set-up");
     // one interaction kind and one cutoff-table layout per batch
     b->gauss = b->reps[0]->D.gauss;
     b->coulomb = b->reps[0]->D.coulomb;
@@ -1507,9 +1568,6 @@ lgm_status lgm_kmc_batch_create(const lgm_params* params, int32_t count, int32_t
         if (k->D.gauss != b->gauss || k->D.coulomb != b->coulomb)
             return bail(LGM_ERR_UNSUPPORTED,
                         "a batch mixes point and Gaussian charges or Coulomb on and off");
-    if (cudaSetDevice(b->device) != cudaSuccess ||
-        cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess)
-        return bail(LGM_ERR_CUDA, "stream");
     for (lgm_kmc* k : b->reps) b->hD.push_back(k->D);
     // block maps: {replica, local block, blocks of the replica, index bound}
     std::vector<int4> car, pack, fin, guard;
@@ -1568,8 +1626,9 @@ lgm_status lgm_kmc_batch_destroy(lgm_kmc_batch* b) {
                     b->map_guard};
     for (void* p : ptrs)
         if (p) cudaFree(p);
+    for (lgm_kmc* k : b->reps) lgm_kmc_destroy(k);  // they do not own the stream or pool
     if (b->stream) cudaStreamDestroy(b->stream);
-    for (lgm_kmc* k : b->reps) lgm_kmc_destroy(k);
+    b->pool.release();
     delete b;
     return LGM_OK;
 }
@@ -1588,7 +1647,7 @@ lgm_kmc* lgm_kmc_batch_replica(lgm_kmc_batch* b, int32_t i) {
 lgm_status lgm_kmc_batch_run(lgm_kmc_batch* b, int32_t steps) {
     if (!b || steps < 0) return LGM_ERR_INVALID_ARGUMENT;
     BCUDA(b, cudaSetDevice(b->device));
-    for (lgm_kmc* k : b->reps) BCUDA(b, cudaStreamSynchronize(k->stream));
+    BCUDA(b, cudaStreamSynchronize(b->stream));  // every replica's work is on the batch stream
     if (!b->exec && steps > 0) {
         lgm_status s = tune_batch(b);
         if (s != LGM_OK) return s;
