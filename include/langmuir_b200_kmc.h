@@ -93,6 +93,17 @@ lgm_status lgm_params_parse(const char* text, lgm_params* p, char* err, int32_t 
  * with the reference's message on failure. */
 lgm_status lgm_params_check(lgm_params* p, char* err, int32_t err_len);
 
+/* The [Parameters] section of a checkpoint as the reference writes it
+ * (CheckPointer::saveParameters, checkpointer.cpp; KeyValueParser stream
+ * operator, keyvalueparser.cpp:217-228; TypedVariable::keyValue,
+ * variable.h:196-238): every non-constant key in registration order, the key
+ * left-aligned in 30 columns, then "=", then the value (doubles in scientific
+ * notation with 15 digits, booleans True/False).  Extension keys are written
+ * only when set, so that the reference reads the text.  Unlike the reference
+ * the text ends with a newline, so its last key is not lost on reading.
+ * Returns the size needed including the terminating zero (out may be NULL). */
+int32_t lgm_params_format(const lgm_params* p, char* out, int32_t cap);
+
 /* ---- one replica on the GPU ------------------------------------------------ */
 typedef struct lgm_kmc lgm_kmc;
 
@@ -104,6 +115,38 @@ typedef struct lgm_kmc lgm_kmc;
  * supported (LGM_ERR_UNSUPPORTED). */
 lgm_status lgm_kmc_create(const lgm_params* p, int32_t device, uint32_t replica, lgm_kmc** out);
 lgm_status lgm_kmc_destroy(lgm_kmc* k);
+/* A world restored from a checkpoint (ConfigurationInfo filled by
+ * CheckPointer::load, checkpointer.cpp:22-163): site lists in the reference's
+ * section order.  Every count may be 0 (section absent).  As World::initialize
+ * does (world.cpp:619-657), the listed defects, carriers and traps are placed
+ * first and the rest are drawn as without a checkpoint: defects up to
+ * defect.percentage, carriers up to (electron|hole).percentage * seed.charges,
+ * traps up to trap.percentage (placeDefects world.cpp:659-757, placeElectrons
+ * world.cpp:759-859, setPotentialTraps potential.cpp:74-244).  trap_potentials
+ * is empty (trap.potential applies) or one per listed trap.  flux holds the
+ * [FluxState] values in one of World::setFluxInfo's layouts (world.cpp:1189-1318):
+ * 4 (transistor legacy), 10 or 12 (solar-cell legacy) or 20 (current). */
+typedef struct lgm_world_config {
+    const int32_t* electrons;
+    int32_t n_electrons;
+    const int32_t* holes;
+    int32_t n_holes;
+    const int32_t* defects;
+    int32_t n_defects;
+    const int32_t* traps;
+    int32_t n_traps;
+    const double* trap_potentials;
+    int32_t n_trap_potentials;
+    const uint64_t* flux;
+    int32_t n_flux;
+} lgm_world_config;
+
+/* lgm_kmc_create with the world taken from `w`.  The step counter starts at
+ * p->current_step; with the same random.seed and replica the counter-based
+ * stream continues where the checkpointed run left off. */
+lgm_status lgm_kmc_create_from(const lgm_params* p, const lgm_world_config* w, int32_t device,
+                               uint32_t replica, lgm_kmc** out);
+
 /* Text of the last error on `k`; k == NULL: why lgm_kmc_create failed on this thread. */
 const char* lgm_kmc_last_error(const lgm_kmc* k);
 

@@ -763,6 +763,8 @@ struct lgm_kmc {
     lgm_params p{};
     DevicePool* pool = nullptr;  // a batch's pool, or null: own allocations
     bool own_stream = true;
+    const lgm_world_config* wcfg = nullptr;  // checkpointed world (creation only)
+    std::vector<unsigned long long> flux0;   // restored flux counters (our layout)
     int device = 0;
     uint32_t replica = 0;
     int V = 0, max_e = 0, max_h = 0;
@@ -846,8 +848,19 @@ lgm_status build_world(lgm_kmc* k) {
     const int max_d = (int)(p.defect_percentage * (double)V);
     const int max_t = (int)(p.trap_percentage * (double)V);
     std::vector<uint8_t> is_def(V, 0), is_trap(V, 0);
-    // placeDefects (world.cpp:659-757)
+    const lgm_world_config* w = k->wcfg;
+    // placeDefects (world.cpp:659-757): listed defects first, the rest drawn
     {
+        const int given = w ? w->n_defects : 0;
+        if (given < 0 || given > max_d || (given && !w->defects))
+            return kfail(k, LGM_ERR_INVALID_ARGUMENT, "langmuir: invalid number of defects in checkpoint");
+        for (int i = 0; i < given; ++i) {
+            const int s = w->defects[i];
+            if (s < 0 || s >= V) return kfail(k, LGM_ERR_OUT_OF_RANGE, "defect site out of range");
+            if (is_def[s]) return kfail(k, LGM_ERR_INVALID_ARGUMENT, "langmuir: defect already exists");
+            is_def[s] = 1;
+            k->defects.push_back(s);
+        }
         Stream r{seed, k->replica, RNG_SETUP + 0};
         long tries = 0;
         while ((int)k->defects.size() < max_d) {
@@ -856,15 +869,32 @@ lgm_status build_world(lgm_kmc* k) {
             if (!is_def[s]) { is_def[s] = 1; k->defects.push_back(s); }
         }
     }
-    // setPotentialTraps (potential.cpp:74-244): seeds, then growth onto neighbours
+    // setPotentialTraps (potential.cpp:74-244): listed traps first (with their
+    // potentials or trap.potential), then random seeds and growth onto
+    // neighbours of the random ones; the Gaussian spread applies to those only
     {
+        const int forced = w ? w->n_traps : 0;
+        if (forced < 0 || forced > max_t || (forced && !w->traps))
+            return kfail(k, LGM_ERR_INVALID_ARGUMENT, "langmuir: invalid trap parameters");
+        if (forced > 0 && w->n_trap_potentials != 0 &&
+            (w->n_trap_potentials != forced || !w->trap_potentials))
+            return kfail(k, LGM_ERR_INVALID_ARGUMENT,
+                         "langmuir: trapPotential and trap arrays different sizes in checkpoint file");
+        for (int i = 0; i < forced; ++i) {
+            const int s = w->traps[i];
+            if (s < 0 || s >= V) return kfail(k, LGM_ERR_OUT_OF_RANGE, "trap site out of range");
+            is_trap[s] = 1;
+            k->traps.push_back(s);
+            k->trap_pots.push_back(w->n_trap_potentials ? w->trap_potentials[i] : p.trap_potential);
+        }
         Stream r{seed, k->replica, RNG_SETUP + 1};
-        int seeds = (int)(max_t * p.seed_percentage);
-        int grown = max_t - seeds;
-        if (max_t <= 0) { seeds = 0; grown = 0; }
+        const int random = max_t - forced;
+        int seeds = (int)(random * p.seed_percentage);
+        int grown = random - seeds;
+        if (random <= 0) { seeds = 0; grown = 0; }
         if (seeds == 0 && grown > 0) { seeds = grown; grown = 0; }
         long tries = 0;
-        while ((int)k->traps.size() < seeds) {
+        while ((int)k->traps.size() < forced + seeds) {
             if (++tries > 100L * V + 1000) return kfail(k, LGM_ERR_INVALID_ARGUMENT, "can not seed traps");
             const int s = (int)r.below((uint32_t)V);
             if (!is_trap[s]) { is_trap[s] = 1; k->traps.push_back(s); }
@@ -873,14 +903,16 @@ lgm_status build_world(lgm_kmc* k) {
         int progress = 0;
         while (progress < grown) {
             if (++tries > 100L * V + 1000) return kfail(k, LGM_ERR_INVALID_ARGUMENT, "can not grow traps");
-            const int seed_site = k->traps[r.below((uint32_t)k->traps.size())];
+            const int n_random = (int)k->traps.size() - forced;
+            const int seed_site = k->traps[forced + (int)r.below((uint32_t)n_random)];
             host_neighbors1(X, Y, Z, seed_site, nb);
             const int s = nb[r.below((uint32_t)nb.size())];
             if (s < V && !is_trap[s]) { is_trap[s] = 1; k->traps.push_back(s); ++progress; }
         }
-        k->trap_pots.assign(k->traps.size(), p.trap_potential);
+        k->trap_pots.resize(k->traps.size(), p.trap_potential);
         if (std::fabs(p.gaussian_stdev) > 0)
-            for (double& v : k->trap_pots) v += r.normal(0.0, p.gaussian_stdev);
+            for (size_t i = forced; i < k->trap_pots.size(); ++i)
+                k->trap_pots[i] += r.normal(0.0, p.gaussian_stdev);
     }
     // setPotentialZero / Linear / Gate (potential.cpp:17-72), traps, disorder
     k->pot.assign(V, 0.0);
@@ -897,12 +929,14 @@ lgm_status build_world(lgm_kmc* k) {
         Stream r{seed, k->replica, RNG_SETUP + 2};
         for (int s = 0; s < V; ++s) k->pot[s] += r.normal(0.0, p.site_disorder);
     }
-    // placeElectrons / placeHoles (world.cpp:759-959): tryToSeed at uniform sites
+    // placeElectrons / placeHoles (world.cpp:759-959): listed sites first, then
+    // tryToSeed at uniform sites up to max * seed.charges
     auto seed_carriers = [&](int max, uint32_t purpose, std::vector<int32_t>& out) -> bool {
         Stream r{seed, k->replica, purpose};
         std::vector<uint8_t> occ(V, 0);
+        for (int s : out) occ[s] = 1;
         long tries = 0;
-        for (int i = 0; i < max * p.seed_charges;) {
+        for (int i = (int)out.size(); i < max * p.seed_charges;) {
             if (++tries > 10L * V) return false;
             const int s = (int)r.below((uint32_t)V);
             if (!occ[s] && !is_def[s] && (int)out.size() < max) {
@@ -913,6 +947,49 @@ lgm_status build_world(lgm_kmc* k) {
         }
         return true;
     };
+    auto given = [&](const int32_t* ids, int n, int max, std::vector<int32_t>& out,
+                     const char* what) -> lgm_status {
+        if (n < 0 || n > max || (n && !ids))
+            return kfail(k, LGM_ERR_INVALID_ARGUMENT,
+                         std::string("langmuir: invalid number of ") + what + " in checkpoint");
+        std::vector<uint8_t> occ(V, 0);
+        for (int i = 0; i < n; ++i) {
+            const int s = ids[i];
+            if (s < 0 || s >= V || occ[s] || is_def[s])
+                return kfail(k, LGM_ERR_INVALID_ARGUMENT, std::string("langmuir: can not inject ") +
+                                                              what + " at site " + std::to_string(s));
+            occ[s] = 1;
+            out.push_back(s);
+        }
+        return LGM_OK;
+    };
+    if (w) {
+        lgm_status st;
+        if ((st = given(w->electrons, w->n_electrons, k->max_e, k->e0, "electron")) != LGM_OK) return st;
+        if ((st = given(w->holes, w->n_holes, k->max_h, k->h0, "hole")) != LGM_OK) return st;
+        // World::setFluxInfo (world.cpp:1189-1318) into this library's counter layout:
+        // eSL eSR hSL hSR (0-7), eDL eDR hDL hDR (8-15), exciton source (16-17),
+        // recombination (18-19), each (attempts, successes)
+        if (w->n_flux) {
+            if (!w->flux) return kfail(k, LGM_ERR_INVALID_ARGUMENT, "flux state without values");
+            const uint64_t* f = w->flux;
+            k->flux0.assign(20, 0ull);
+            auto put = [&](int agent, int at) { k->flux0[2 * agent] = f[at]; k->flux0[2 * agent + 1] = f[at + 1]; };
+            const bool solar = std::string(p.simulation_type) == "solarcell";
+            if (w->n_flux == 4 && !solar) {
+                put(0, 0); put(5, 2);
+            } else if ((w->n_flux == 10 || w->n_flux == 12) && solar) {
+                put(8, 0); put(4, 2); put(6, 4); put(5, 6); put(7, 8);
+                if (w->n_flux == 12) put(9, 10);
+            } else if (w->n_flux == 20) {
+                put(0, 0); put(1, 2); put(2, 4); put(3, 6); put(8, 8);
+                put(4, 10); put(5, 12); put(6, 14); put(7, 16); put(9, 18);
+            } else {
+                return kfail(k, LGM_ERR_PARSE, "langmuir: do not recognize [FluxInfo] format (of size " +
+                                                   std::to_string(w->n_flux) + ")");
+            }
+        }
+    }
     if (!seed_carriers(k->max_e, RNG_SETUP + 3, k->e0))
         return kfail(k, LGM_ERR_INVALID_ARGUMENT, "can not seed electrons");
     if (!seed_carriers(k->max_h, RNG_SETUP + 4, k->h0))
@@ -995,13 +1072,15 @@ extern "C" {
 // One replica.  pool / shared: a batch's device pool and stream (the batch
 // synchronises once after creating all replicas), or null for a standalone one.
 static lgm_status kmc_create_impl(const lgm_params* pin, int32_t device, uint32_t replica,
-                                  lgm_kmc** out, DevicePool* pool, cudaStream_t shared) {
+                                  lgm_kmc** out, DevicePool* pool, cudaStream_t shared,
+                                  const lgm_world_config* wcfg = nullptr) {
     if (!pin || !out) return LGM_ERR_INVALID_ARGUMENT;
     *out = nullptr;
     lgm_kmc* k = new (std::nothrow) lgm_kmc();
     if (!k) return LGM_ERR_INVALID_ARGUMENT;
     k->p = *pin;
     k->pool = pool;
+    k->wcfg = wcfg;
     k->replica = replica;
     char msg[256] = {0};
     lgm_status s = lgm_params_check(&k->p, msg, sizeof msg);
@@ -1198,6 +1277,9 @@ static lgm_status kmc_create_impl(const lgm_params* pin, int32_t device, uint32_
     cudaMemset(D.h_rm, 0, std::max(D.cap_h, 1));
     cudaMemset(D.cnt, 0, sizeof(int32_t) * I_NUM);
     cudaMemset(D.ctr, 0, sizeof(unsigned long long) * C_NUM);
+    if (!k->flux0.empty())
+        cudaMemcpy(D.ctr, k->flux0.data(), sizeof(unsigned long long) * k->flux0.size(),
+                   cudaMemcpyHostToDevice);
     cudaMemset(D.err, 0, sizeof(unsigned));
     int32_t step0 = (int32_t)p.current_step;
     cudaMemcpy(D.cnt + I_STEP, &step0, sizeof step0, cudaMemcpyHostToDevice);
@@ -1205,12 +1287,19 @@ static lgm_status kmc_create_impl(const lgm_params* pin, int32_t device, uint32_
                               (int)k->h0.size())) != LGM_OK)
         return bail(st, k->err);
     if (!pool && cudaDeviceSynchronize() != cudaSuccess) return bail(LGM_ERR_CUDA, "set-up");
+    k->wcfg = nullptr;  // the caller's arrays are not kept
     *out = k;
     return LGM_OK;
 }
 
 lgm_status lgm_kmc_create(const lgm_params* pin, int32_t device, uint32_t replica, lgm_kmc** out) {
     return kmc_create_impl(pin, device, replica, out, nullptr, nullptr);
+}
+
+lgm_status lgm_kmc_create_from(const lgm_params* pin, const lgm_world_config* w, int32_t device,
+                               uint32_t replica, lgm_kmc** out) {
+    if (!w) return LGM_ERR_INVALID_ARGUMENT;
+    return kmc_create_impl(pin, device, replica, out, nullptr, nullptr, w);
 }
 
 lgm_status lgm_kmc_destroy(lgm_kmc* k) {

@@ -366,4 +366,61 @@ lgm_status lgm_params_check(lgm_params* p, char* err, int32_t err_len) {
     return LGM_OK;
 }
 
+int32_t lgm_params_format(const lgm_params* p, char* out, int32_t cap) {
+    if (!p) return -1;
+    std::string text = "[Parameters]";
+    const size_t n_reference = sizeof(kKeys) / sizeof(kKeys[0]) - 4;  // the extension keys last
+    for (size_t i = 0; i < sizeof(kKeys) / sizeof(kKeys[0]); ++i) {
+        const Key& k = kKeys[i];
+        if (k.constant) continue;
+        const char* base = reinterpret_cast<const char*>(p) + k.offset;
+        std::string value;
+        char buf[64];
+        switch (k.kind) {
+        case K_STR16:
+            value.assign(base, strnlen(base, 16));
+            break;
+        case K_STR64:
+            value.assign(base, strnlen(base, 64));
+            break;
+        case K_U32:
+            std::snprintf(buf, sizeof buf, "%u", *reinterpret_cast<const uint32_t*>(base));
+            value = buf;
+            break;
+        case K_U64:
+            std::snprintf(buf, sizeof buf, "%llu",
+                          (unsigned long long)*reinterpret_cast<const uint64_t*>(base));
+            value = buf;
+            break;
+        case K_I32:
+            std::snprintf(buf, sizeof buf, "%d", *reinterpret_cast<const int32_t*>(base));
+            value = buf;
+            break;
+        case K_BOOL:
+            value = *reinterpret_cast<const int32_t*>(base) ? "True" : "False";
+            break;
+        case K_F64:
+            // TypedVariable<qreal>::value: scientific, digits10 = 15 digits
+            std::snprintf(buf, sizeof buf, "%.15e", *reinterpret_cast<const double*>(base));
+            value = buf;
+            break;
+        }
+        // extension keys only when set, so that the reference can read the text
+        if (i >= n_reference && (value == "0" || value == "False" ||
+                                 (k.kind == K_F64 && *reinterpret_cast<const double*>(base) == 0.0)))
+            continue;
+        // TypedVariable::keyValue (variable.h:196-238): key left in 30 columns,
+        // '=' in 3 columns (2 before a minus sign), then the value
+        std::string line = k.name;
+        if (line.size() < 30) line.append(30 - line.size(), ' ');
+        if (value.empty()) line += "=";
+        else line += (value[0] == '-' ? "= " : "=  ") + value;
+        text += "\n" + line;
+    }
+    text += "\n";
+    const int32_t need = (int32_t)text.size() + 1;
+    if (out && cap > 0) std::snprintf(out, (size_t)cap, "%s", text.c_str());
+    return need;
+}
+
 }  // extern "C"

@@ -83,6 +83,13 @@ class Params(ctypes.Structure):
     def from_text(cls, text: str) -> "Params":
         return cls.default().parse(text)
 
+    def format(self) -> str:
+        """The [Parameters] section of a checkpoint (lgm_params_format)."""
+        need = N.lib().lgm_params_format(ctypes.byref(self), None, 0)
+        buf = ctypes.create_string_buffer(need)
+        N.lib().lgm_params_format(ctypes.byref(self), buf, need)
+        return buf.value.decode()
+
     def check(self) -> "Params":
         err = ctypes.create_string_buffer(512)
         st = N.lib().lgm_params_check(ctypes.byref(self), err, len(err))
@@ -102,8 +109,21 @@ _vp = ctypes.c_void_p
 _i32p = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
 _f64p = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
 
+class WorldConfig(ctypes.Structure):
+    """lgm_world_config: a world restored from a checkpoint."""
+    _fields_ = [("electrons", ctypes.c_void_p), ("n_electrons", _i32),
+                ("holes", ctypes.c_void_p), ("n_holes", _i32),
+                ("defects", ctypes.c_void_p), ("n_defects", _i32),
+                ("traps", ctypes.c_void_p), ("n_traps", _i32),
+                ("trap_potentials", ctypes.c_void_p), ("n_trap_potentials", _i32),
+                ("flux", ctypes.c_void_p), ("n_flux", _i32)]
+
+
 N.SIGNATURES.update({
     "lgm_params_default": (None, [ctypes.POINTER(Params)]),
+    "lgm_params_format": (_i32, [ctypes.POINTER(Params), ctypes.c_char_p, _i32]),
+    "lgm_kmc_create_from": (_i32, [ctypes.POINTER(Params), ctypes.POINTER(WorldConfig), _i32,
+                                   ctypes.c_uint32, ctypes.POINTER(ctypes.c_void_p)]),
     "lgm_params_size": (_i32, []),
     "lgm_params_parse": (_i32, [ctypes.c_char_p, ctypes.POINTER(Params), ctypes.c_char_p, _i32]),
     "lgm_params_check": (_i32, [ctypes.POINTER(Params), ctypes.c_char_p, _i32]),
@@ -121,7 +141,8 @@ N.SIGNATURES.update({
                                                                   flags="C_CONTIGUOUS")]),
 })
 if N._lib is not None:  # bind the new symbols if the library was already loaded
-    for _name in ("lgm_params_default", "lgm_params_size", "lgm_params_parse",
+    for _name in ("lgm_params_default", "lgm_params_format", "lgm_kmc_create_from",
+                  "lgm_params_size", "lgm_params_parse",
                   "lgm_params_check", "lgm_kmc_create", "lgm_kmc_destroy", "lgm_kmc_last_error",
                   "lgm_kmc_run", "lgm_kmc_stats_get", "lgm_kmc_get_carriers",
                   "lgm_kmc_set_carriers", "lgm_kmc_get_world", "lgm_kmc_last_outcomes",
@@ -134,14 +155,35 @@ class KMC:
     """One replica on the GPU: the world is built from ``params`` and the
     (random.seed, replica) Philox stream."""
 
-    def __init__(self, params: Params, device: int = 0, replica: int = 0):
+    def __init__(self, params: Params, device: int = 0, replica: int = 0, world=None):
+        """world: optional dict of site lists restored from a checkpoint --
+        electrons, holes, defects, traps, trap_potentials, flux (see
+        lgm_world_config) -- placed before the rest is drawn."""
         h = ctypes.c_void_p()
-        st = N.lib().lgm_kmc_create(ctypes.byref(params), int(device), int(replica),
-                                    ctypes.byref(h))
+        if world is None:
+            st = N.lib().lgm_kmc_create(ctypes.byref(params), int(device), int(replica),
+                                        ctypes.byref(h))
+        else:
+            keep = []
+
+            def arr(key, dtype):
+                a = np.ascontiguousarray(world.get(key, []), dtype=dtype)
+                keep.append(a)
+                return (a.ctypes.data if a.size else None), int(a.size)
+            w = WorldConfig()
+            for key, dt in (("electrons", np.int32), ("holes", np.int32), ("defects", np.int32),
+                            ("traps", np.int32), ("trap_potentials", np.float64),
+                            ("flux", np.uint64)):
+                ptr, n = arr(key, dt)
+                setattr(w, key, ptr)
+                setattr(w, "n_" + key, n)
+            st = N.lib().lgm_kmc_create_from(ctypes.byref(params), ctypes.byref(w), int(device),
+                                             int(replica), ctypes.byref(h))
         if st != N.OK:
             raise N.LgmError(st, N.lib().lgm_kmc_last_error(None).decode())
         self._h = h
         self.params = params
+        self.replica = int(replica)
         self.volume = params.grid_x * params.grid_y * params.grid_z
 
     def _check(self, st):
