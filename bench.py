@@ -385,7 +385,8 @@ def cnn_layers(S, peaks):
             "conv2_pool": {"ms": t2, "achieved": f2 / (t2 * 1e-3) / 1e12, "peak": bf16,
                            "unit": "TFLOP/s", "frac": f2 / (t2 * 1e-3) / 1e12 / bf16,
                            "bound": "tensor",
-                           "note": "mma.sync m16n8k16 bf16; peak = measured cuBLAS bf16 GEMM"}}
+                           "note": "tcgen05.mma M128 N32 K16 bf16, TMA-loaded patches; peak = "
+                                   "measured cuBLAS bf16 GEMM"}}
 
 
 def surrogate_run(args, rank):

@@ -33,6 +33,20 @@ lgm_status lgm_cnn_conv3x3_fwd(int32_t cin, const void* x, const void* w, const 
                                void* act, void* pooled, int32_t B, int32_t H, int32_t W,
                                int32_t relu, void* stream);
 
+/* lgm_cnn_conv3x3_fwd for cin = LGM_CNN_CHANNELS on the 5th-generation
+ * tensor cores: tcgen05.mma (M128 N32 K16, BF16 in, FP32 accumulators in
+ * tensor memory), the input patch staged three times shifted by one column so
+ * that every tap's operand is a contiguous shared-memory block.  Same
+ * arguments and results as lgm_cnn_conv3x3_fwd; all pointers 16-byte aligned.
+ * A bounded wait that runs out sets a flag read by lgm_cnn_error. */
+lgm_status lgm_cnn_conv3x3_fwd_tc(const void* x, const void* w, const float* bias, void* act,
+                                  void* pooled, int32_t B, int32_t H, int32_t W, int32_t relu,
+                                  void* stream);
+
+/* Error bits raised on the device by the tensor-core kernels since the last
+ * call (LGM_ERR_TIMEOUT if any), then cleared.  Synchronises the device. */
+lgm_status lgm_cnn_error(uint32_t* flags);
+
 /* dW[cout][k] += sum over pixels of dA[p][cout] * im2col(x)[p][k] and
  * db[cout] += sum_p dA[p][cout] (db may be NULL).  dW and db are FP32 and are
  * added to, not overwritten. */

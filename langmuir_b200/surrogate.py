@@ -52,6 +52,8 @@ N.SIGNATURES.update({
     "lgm_cnn_gap_fwd": (_i32, [_vp, _vp, _vp, _i32, _i32, _vp]),
     "lgm_cnn_gap_relu_bwd": (_i32, [_vp, _vp, _vp, _i32, _i32, _vp]),
     "lgm_cnn_to_bf16": (_i32, [_vp, _vp, _i32, _vp, _vp]),
+    "lgm_cnn_conv3x3_fwd_tc": (_i32, [_vp, _vp, _vp, _vp, _vp, _i32, _i32, _i32, _i32, _vp]),
+    "lgm_cnn_error": (_i32, [ctypes.POINTER(ctypes.c_uint32)]),
 })
 _CNN_SYMBOLS = [k for k in N.SIGNATURES if k.startswith("lgm_cnn_")]
 if N._lib is not None:
@@ -75,7 +77,16 @@ def _stream():
 
 # ---- kernel wrappers -----------------------------------------------------------------------
 def conv3x3(x, w16, bias, H, W, relu=True, keep_act=True, pool=True):
-    """x: [B,H,W,cin] bf16, w16: [CH, 16 or 9*CH] bf16 -> (act or None, pooled or None)."""
+    """x: [B,H,W,cin] bf16, w16: [CH, 16 or 9*CH] bf16 -> (act or None, pooled or None).
+    32 input channels run on the tcgen05 kernel, 1 input channel on mma.sync."""
+    B, cin = x.shape[0], x.shape[-1]
+    if cin == CH:
+        return conv3x3_tc(x, w16, bias, H, W, relu, keep_act, pool)
+    return conv3x3_mma(x, w16, bias, H, W, relu, keep_act, pool)
+
+
+def conv3x3_mma(x, w16, bias, H, W, relu=True, keep_act=True, pool=True):
+    """The mma.sync kernel (lgm_cnn_conv3x3_fwd), for 1 or 32 input channels."""
     B, cin = x.shape[0], x.shape[-1]
     act = torch.empty(B, H, W, CH, dtype=torch.bfloat16, device=x.device) if keep_act else None
     pooled = (torch.empty(B, H // 2, W // 2, CH, dtype=torch.bfloat16, device=x.device)
@@ -83,6 +94,24 @@ def conv3x3(x, w16, bias, H, W, relu=True, keep_act=True, pool=True):
     _ok(N.lib().lgm_cnn_conv3x3_fwd(cin, _p(x), _p(w16), _p(bias), _p(act), _p(pooled), B, H, W,
                                     int(relu), _stream()))
     return act, pooled
+
+
+def conv3x3_tc(x, w16, bias, H, W, relu=True, keep_act=True, pool=True):
+    """conv3x3 for 32 input channels on the tcgen05 tensor cores."""
+    B = x.shape[0]
+    act = torch.empty(B, H, W, CH, dtype=torch.bfloat16, device=x.device) if keep_act else None
+    pooled = (torch.empty(B, H // 2, W // 2, CH, dtype=torch.bfloat16, device=x.device)
+              if pool else None)
+    _ok(N.lib().lgm_cnn_conv3x3_fwd_tc(_p(x), _p(w16), _p(bias), _p(act), _p(pooled), B, H, W,
+                                       int(relu), _stream()))
+    return act, pooled
+
+
+def device_errors() -> int:
+    """Error bits the tensor-core kernels raised since the last call (0 = none)."""
+    v = ctypes.c_uint32()
+    N.lib().lgm_cnn_error(ctypes.byref(v))
+    return v.value
 
 
 def conv3x3_wgrad(x, dA, dW, db, H, W):

@@ -111,8 +111,8 @@ def test_conv_forward_matches_oracle(cin, H, W, B):
     pre = C.conv3x3(x, w, b)
     relu = np.maximum(pre, 0)
     w16 = S.conv_weights_bf16(torch.as_tensor(w, dtype=torch.float32).cuda(), cin)
-    act, pooled = S.conv3x3(_bf16(torch, x), w16, torch.as_tensor(b, dtype=torch.float32).cuda(),
-                            H, W)
+    act, pooled = S.conv3x3_mma(_bf16(torch, x), w16,
+                                torch.as_tensor(b, dtype=torch.float32).cuda(), H, W)
     torch.cuda.synchronize()
     # one BF16 rounding of an FP32 sum: within 2^-8 relative, plus FP32 order
     scale = np.abs(relu).max()
@@ -120,10 +120,44 @@ def test_conv_forward_matches_oracle(cin, H, W, B):
     ref_pool = C.avgpool2(relu)
     assert np.all(np.abs(_f64(pooled) - ref_pool) <= 2 ** -8 * np.abs(ref_pool) + 1e-5 * scale)
     # no ReLU, no bias
-    act2, _ = S.conv3x3(_bf16(torch, x), w16, None, H, W, relu=False, pool=False)
+    act2, _ = S.conv3x3_mma(_bf16(torch, x), w16, None, H, W, relu=False, pool=False)
     torch.cuda.synchronize()
     pre0 = C.conv3x3(x, w)
     assert np.all(np.abs(_f64(act2) - pre0) <= 2 ** -8 * np.abs(pre0) + 1e-5 * np.abs(pre0).max())
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("H,W,B", [(8, 16, 1), (16, 16, 5), (32, 64, 3), (64, 64, 9)])
+def test_tcgen05_conv_matches_oracle_and_mma_sync(H, W, B):
+    """The tcgen05 kernel against the FP64 oracle (one BF16 rounding) and
+    against the mma.sync kernel, in every output mode, with no device error."""
+    import torch
+    from langmuir_b200 import surrogate as S
+    rng = rng_for(f"tc{H}{W}{B}")
+    x = C.round_bf16(rng.standard_normal((B, H, W, 32)))
+    w = C.round_bf16(rng.standard_normal((32, 288)) * np.sqrt(2.0 / 288))
+    b = rng.standard_normal(32) * 0.1
+    relu = np.maximum(C.conv3x3(x, w, b), 0)
+    scale = np.abs(relu).max()
+    x16, w16 = _bf16(torch, x), _bf16(torch, w)
+    bt = torch.as_tensor(b, dtype=torch.float32).cuda()
+    act, pooled = S.conv3x3_tc(x16, w16, bt, H, W)
+    act_m, pooled_m = S.conv3x3_mma(x16, w16, bt, H, W)
+    torch.cuda.synchronize()
+    assert S.device_errors() == 0
+    assert np.all(np.abs(_f64(act) - relu) <= 2 ** -8 * np.abs(relu) + 1e-5 * scale)
+    ref_pool = C.avgpool2(relu)
+    assert np.all(np.abs(_f64(pooled) - ref_pool) <= 2 ** -8 * np.abs(ref_pool) + 1e-5 * scale)
+    # the two tensor-core paths differ at most by one BF16 rounding
+    assert np.all(np.abs(_f64(act) - _f64(act_m)) <= 2 ** -7 * np.abs(_f64(act_m)) + 1e-5 * scale)
+    # pooled only; then no bias, no ReLU, activation only (the input-gradient use)
+    _, pooled2 = S.conv3x3_tc(x16, w16, bt, H, W, keep_act=False)
+    act3, _ = S.conv3x3_tc(x16, w16, None, H, W, relu=False, pool=False)
+    torch.cuda.synchronize()
+    assert torch.equal(pooled2, pooled)
+    pre0 = C.conv3x3(x, w)
+    assert np.all(np.abs(_f64(act3) - pre0) <= 2 ** -8 * np.abs(pre0) + 1e-5 * np.abs(pre0).max())
+    assert S.device_errors() == 0
 
 
 @pytest.mark.gpu
