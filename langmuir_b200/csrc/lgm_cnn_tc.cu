@@ -21,10 +21,15 @@
 // staged once per CTA as ws[tap][c8][out channel][8 channels] (8 x 16-byte
 // core matrices, SBO 128 bytes, LBO one 8-channel plane).
 //
-// Pipeline (two stages of patch buffers and of 32 TMEM columns): while the
-// four warps run the epilogue of tile k (tcgen05.ld of the accumulators, bias,
-// ReLU, stores, 2x2 pooling with warp shuffles), the tensor core computes tile
-// k+1 and TMA loads tile k+2.  One thread issues the copies and the MMAs.
+// Pipeline (two stages of patch buffers and of 32 TMEM columns), warp
+// specialised: one thread of warp 4 issues the TMA loads and the MMAs; warps
+// 0-3 run the epilogue (tcgen05.ld of the accumulators, bias, ReLU, stores,
+// 2x2 pooling with warp shuffles).  Three pairs of mbarriers hand the stages
+// over: "full" (the patch has landed), "done" (the MMAs have finished: the
+// accumulators are ready and the patch buffer is free) and "empty" (the
+// epilogue has read the accumulators: the TMEM stage is free).  While the
+// epilogue warps finish tile k, the tensor core computes tile k+1 and TMA
+// loads tile k+2.
 //
 // Every wait is bounded: a timeout sets a flag that lgm_cnn_error reports;
 // the CTA then waits (bounded) for its own copies and MMAs, frees its TMEM and
@@ -47,7 +52,8 @@ using bf16 = __nv_bfloat16;
 using lgm::smem_addr;
 
 constexpr int TY = 8, TX = 16;                 // output tile
-constexpr int THREADS = 128;                   // one pixel (TMEM lane) per thread
+constexpr int EPI_THREADS = 128;               // epilogue warps 0-3: one pixel (TMEM lane) each
+constexpr int THREADS = EPI_THREADS + 32;      // + warp 4: issues the copies and the MMAs
 constexpr int COUT = LGM_CNN_CHANNELS;         // 32
 constexpr int CIN = LGM_CNN_CHANNELS;          // 32
 constexpr int C8 = CIN / 8;                    // 16-byte channel groups
@@ -136,6 +142,15 @@ __device__ __forceinline__ uint32_t pack2(float lo, float hi) {
 
 __device__ unsigned g_tc_error = 0;  // DEVERR_* bits of the tensor-core conv
 
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
+}
+
+// Bounded wait that returns false after a timeout (and records it).
+__device__ __forceinline__ bool wait(uint64_t* bar, int use) {
+    return lgm::mbar_wait_bounded(bar, (uint32_t)(use & 1), &g_tc_error);
+}
+
 // x (through the tensor map): [B,H,W,32] bf16; w: [32][288] bf16
 // (k = (ky*3 + kx)*32 + c); act [B,H,W,32] and/or pooled [B,H/2,W/2,32].
 // H % 8 == 0, W % 16 == 0.
@@ -145,8 +160,9 @@ conv3x3_fwd_tc(const __grid_constant__ CUtensorMap xmap, const bf16* __restrict_
                int B, int H, int W, int relu) {
     extern __shared__ __align__(1024) unsigned char smem[];
     unsigned char* ws = smem + XS_BYTES;            // [9][C8][COUT][16 B]
-    uint64_t* tbar = reinterpret_cast<uint64_t*>(smem + XS_BYTES + WS_BYTES);  // [2] patch loaded
-    uint64_t* mbar = tbar + 2;                                                  // [2] MMAs done
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem + XS_BYTES + WS_BYTES);  // [2]
+    uint64_t* done = full + 2;                                                  // [2]
+    uint64_t* empty = full + 4;                                                 // [2]
     uint32_t* tslot = reinterpret_cast<uint32_t*>(smem + XS_BYTES + WS_BYTES + 64);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int tiles_x = W / TX, tiles_y = H / TY;
@@ -161,7 +177,8 @@ conv3x3_fwd_tc(const __grid_constant__ CUtensorMap xmap, const bf16* __restrict_
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
     if (tid == 0) {
-        for (int i = 0; i < 4; ++i) lgm::mbar_init(&tbar[i], 1);
+        for (int i = 0; i < 4; ++i) lgm::mbar_init(&full[i], 1);          // full, done
+        for (int i = 4; i < 6; ++i) lgm::mbar_init(&full[i], EPI_THREADS / 32);  // empty: a lane per warp
         lgm::fence_mbar_init();
         asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&xmap)) : "memory");
     }
@@ -177,9 +194,6 @@ conv3x3_fwd_tc(const __grid_constant__ CUtensorMap xmap, const bf16* __restrict_
     fence_after_sync();
     const uint32_t tmem = *tslot;
     const uint32_t xs_a = smem_addr(smem), ws_a = smem_addr(ws);
-    float bv[32];
-#pragma unroll
-    for (int c = 0; c < 32; ++c) bv[c] = bias ? bias[c] : 0.f;
 
     auto origin = [&](int k, int& b, int& y0, int& x0) {
         const int tile = (int)blockIdx.x + k * (int)gridDim.x;
@@ -188,105 +202,114 @@ conv3x3_fwd_tc(const __grid_constant__ CUtensorMap xmap, const bf16* __restrict_
         y0 = (rem / tiles_x) * TY;
         x0 = (rem % tiles_x) * TX;
     };
-    // thread 0 only: copies and MMAs in flight, for the clean-up after a timeout
-    int tma_issued = 0, mma_issued = 0;
-    auto issue_tma = [&](int k) {
-        const int st = k & 1;
-        int b, y0, x0;
-        origin(k, b, y0, x0);
-        lgm::mbar_arrive_expect_tx(&tbar[st], STAGE_BYTES);
-#pragma unroll 1
-        for (int kx = 0; kx < 3; ++kx)
-            tma_load_4d(xs_a + st * STAGE_BYTES + kx * COPY_BYTES, &xmap, 0, x0 + kx - 1, y0 - 1, b,
-                        &tbar[st]);
-        ++tma_issued;
-    };
-    auto issue_mma = [&](int k) -> bool {
-        const int st = k & 1;
-        if (!lgm::mbar_wait_bounded(&tbar[st], (uint32_t)((k >> 1) & 1), &g_tc_error)) return false;
-        fence_after_sync();
-        const uint32_t xa = xs_a + st * STAGE_BYTES, d = tmem + (uint32_t)(st * 32);
-#pragma unroll 1
-        for (int t = 0; t < 9; ++t) {
-            const int ky = t / 3, kx = t % 3;
-#pragma unroll
-            for (int j = 0; j < 2; ++j) {
-                // A: rows 16 ky .. 16 ky + 127 of copy kx, channels 16j .. 16j+15
-                const uint64_t da = smem_desc(xa + kx * COPY_BYTES + ky * TX * 64 + j * 32, 16, 512, 4);
-                // B: 32 output channels of tap t, the same 16 channels
-                const uint64_t db =
-                    smem_desc(ws_a + (uint32_t)(((t * C8 + 2 * j) * COUT) * 16), COUT * 16, 128);
-                umma(d, da, db, (t | j) ? 1u : 0u);
-            }
-        }
-        umma_commit(&mbar[st]);
-        ++mma_issued;
-        return true;
-    };
 
-    bool ok = true;  // thread 0's view of its own waits
-    if (tid == 0 && n > 0) {
-        issue_tma(0);
-        if (n > 1) issue_tma(1);
-        ok = issue_mma(0);
-    }
-    int consumed = 0;
-    for (int k = 0; k < n; ++k) {
-        const int st = k & 1;
-        if (tid == 0 && ok && k + 1 < n) ok = issue_mma(k + 1);
-        const bool mine = lgm::mbar_wait_bounded(&mbar[st], (uint32_t)((k >> 1) & 1), &g_tc_error);
-        if (!__syncthreads_and(mine && (tid != 0 || ok))) break;
-        consumed = k + 1;
-        // tile k's MMAs are done: its patch buffer takes tile k+2
-        if (tid == 0 && k + 2 < n) issue_tma(k + 2);
-        fence_after_sync();
-        float v[32];
-        tmem_ld32(tmem + (uint32_t)(st * 32) + ((uint32_t)(warp * 32) << 16), v);
-        int b, y0, x0;
-        origin(k, b, y0, x0);
-        // this thread's pixel: tile row 2*warp + lane/16, column lane%16
-        const int r = 2 * warp + (lane >> 4), c = lane & 15;
+    if (warp == EPI_THREADS / 32) {
+        // ---- producer: TMA loads and MMAs, one thread ----
+        if (lane == 0 && n > 0) {
+            int tma_issued = 0, mma_issued = 0, mma_waited = 0;
+            bool ok = true;
+            auto issue_tma = [&](int k) {
+                const int st = k & 1;
+                int b, y0, x0;
+                origin(k, b, y0, x0);
+                lgm::mbar_arrive_expect_tx(&full[st], STAGE_BYTES);
+#pragma unroll 1
+                for (int kx = 0; kx < 3; ++kx)
+                    tma_load_4d(xs_a + st * STAGE_BYTES + kx * COPY_BYTES, &xmap, 0, x0 + kx - 1,
+                                y0 - 1, b, &full[st]);
+                ++tma_issued;
+            };
+            issue_tma(0);
+            if (n > 1) issue_tma(1);
+            for (int k = 0; k < n && ok; ++k) {
+                const int st = k & 1;
+                // the patch has landed; the epilogue has released the TMEM stage (tile k-2)
+                ok = wait(&full[st], k >> 1) && (k < 2 || wait(&empty[st], (k - 2) >> 1));
+                if (!ok) break;
+                fence_after_sync();
+                const uint32_t xa = xs_a + st * STAGE_BYTES, d = tmem + (uint32_t)(st * 32);
+#pragma unroll 1
+                for (int t = 0; t < 9; ++t) {
+                    const int ky = t / 3, kx = t % 3;
 #pragma unroll
-        for (int ch = 0; ch < 32; ++ch) {
-            v[ch] += bv[ch];
-            if (relu) v[ch] = fmaxf(v[ch], 0.f);
+                    for (int j = 0; j < 2; ++j) {
+                        // A: rows 16 ky .. 16 ky + 127 of copy kx, channels 16j .. 16j+15
+                        const uint64_t da =
+                            smem_desc(xa + kx * COPY_BYTES + ky * TX * 64 + j * 32, 16, 512, 4);
+                        // B: 32 output channels of tap t, the same 16 channels
+                        const uint64_t db =
+                            smem_desc(ws_a + (uint32_t)(((t * C8 + 2 * j) * COUT) * 16), COUT * 16, 128);
+                        umma(d, da, db, (t | j) ? 1u : 0u);
+                    }
+                }
+                umma_commit(&done[st]);
+                ++mma_issued;
+                // tile k-1's MMAs finished -> its patch buffer takes tile k+1
+                if (k >= 1 && k + 1 < n) {
+                    ok = wait(&done[(k - 1) & 1], (k - 1) >> 1);
+                    mma_waited = k;
+                    if (ok) issue_tma(k + 1);
+                }
+            }
+            // after a timeout: wait (bounded) for the MMAs and copies still in flight
+            for (int k = mma_waited; k < mma_issued; ++k)
+                for (int it = 0; it < lgm::kWaitLimit; ++it)
+                    if (lgm::mbar_try_wait(&done[k & 1], (uint32_t)((k >> 1) & 1))) break;
+            for (int k = mma_issued; k < tma_issued; ++k)
+                for (int it = 0; it < lgm::kWaitLimit; ++it)
+                    if (lgm::mbar_try_wait(&full[k & 1], (uint32_t)((k >> 1) & 1))) break;
         }
-        if (act) {
-            uint4* dst = reinterpret_cast<uint4*>(act + (((size_t)b * H + y0 + r) * W + x0 + c) * COUT);
+    } else {
+        // ---- epilogue: warps 0-3, thread = pixel = TMEM lane ----
+        float bv[32];
 #pragma unroll
-            for (int q = 0; q < 4; ++q)
-                dst[q] = make_uint4(pack2(v[8 * q], v[8 * q + 1]), pack2(v[8 * q + 2], v[8 * q + 3]),
-                                    pack2(v[8 * q + 4], v[8 * q + 5]), pack2(v[8 * q + 6], v[8 * q + 7]));
-        }
-        if (pooled) {
-            // (row 2w + row 2w+1) first, then the column pair: lanes 16 apart, then 1 apart
+        for (int c = 0; c < 32; ++c) bv[c] = bias ? bias[c] : 0.f;
+        for (int k = 0; k < n; ++k) {
+            const int st = k & 1;
+            if (!wait(&done[st], k >> 1)) break;
+            fence_after_sync();
+            float v[32];
+            tmem_ld32(tmem + (uint32_t)(st * 32) + ((uint32_t)(warp * 32) << 16), v);
+            fence_before_sync();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&empty[st]);  // this warp's TMEM lanes are read
+            int b, y0, x0;
+            origin(k, b, y0, x0);
+            // this thread's pixel: tile row 2*warp + lane/16, column lane%16
+            const int r = 2 * warp + (lane >> 4), c = lane & 15;
 #pragma unroll
-            for (int ch = 0; ch < 32; ++ch) v[ch] += __shfl_down_sync(0xffffffffu, v[ch], 16);
-#pragma unroll
-            for (int ch = 0; ch < 32; ++ch) v[ch] += __shfl_down_sync(0xffffffffu, v[ch], 1);
-            if (lane < 16 && (lane & 1) == 0) {
-                const int H2 = H / 2, W2 = W / 2;
-                uint4* dst = reinterpret_cast<uint4*>(
-                    pooled + (((size_t)b * H2 + y0 / 2 + warp) * W2 + x0 / 2 + lane / 2) * COUT);
+            for (int ch = 0; ch < 32; ++ch) {
+                v[ch] += bv[ch];
+                if (relu) v[ch] = fmaxf(v[ch], 0.f);
+            }
+            if (act) {
+                uint4* dst =
+                    reinterpret_cast<uint4*>(act + (((size_t)b * H + y0 + r) * W + x0 + c) * COUT);
 #pragma unroll
                 for (int q = 0; q < 4; ++q)
-                    dst[q] = make_uint4(pack2(0.25f * v[8 * q], 0.25f * v[8 * q + 1]),
-                                        pack2(0.25f * v[8 * q + 2], 0.25f * v[8 * q + 3]),
-                                        pack2(0.25f * v[8 * q + 4], 0.25f * v[8 * q + 5]),
-                                        pack2(0.25f * v[8 * q + 6], 0.25f * v[8 * q + 7]));
+                    dst[q] = make_uint4(pack2(v[8 * q], v[8 * q + 1]), pack2(v[8 * q + 2], v[8 * q + 3]),
+                                        pack2(v[8 * q + 4], v[8 * q + 5]),
+                                        pack2(v[8 * q + 6], v[8 * q + 7]));
+            }
+            if (pooled) {
+                // (row 2w + row 2w+1) first, then the column pair: lanes 16 apart, then 1 apart
+#pragma unroll
+                for (int ch = 0; ch < 32; ++ch) v[ch] += __shfl_down_sync(0xffffffffu, v[ch], 16);
+#pragma unroll
+                for (int ch = 0; ch < 32; ++ch) v[ch] += __shfl_down_sync(0xffffffffu, v[ch], 1);
+                if (lane < 16 && (lane & 1) == 0) {
+                    const int H2 = H / 2, W2 = W / 2;
+                    uint4* dst = reinterpret_cast<uint4*>(
+                        pooled + (((size_t)b * H2 + y0 / 2 + warp) * W2 + x0 / 2 + lane / 2) * COUT);
+#pragma unroll
+                    for (int q = 0; q < 4; ++q)
+                        dst[q] = make_uint4(pack2(0.25f * v[8 * q], 0.25f * v[8 * q + 1]),
+                                            pack2(0.25f * v[8 * q + 2], 0.25f * v[8 * q + 3]),
+                                            pack2(0.25f * v[8 * q + 4], 0.25f * v[8 * q + 5]),
+                                            pack2(0.25f * v[8 * q + 6], 0.25f * v[8 * q + 7]));
+                }
             }
         }
-        fence_before_sync();
-        __syncthreads();  // TMEM stage st is free for tile k+2
-    }
-    if (tid == 0) {
-        // after a timeout: wait (bounded) for the MMAs and copies still in flight
-        for (int k = consumed; k < mma_issued; ++k)
-            for (int it = 0; it < lgm::kWaitLimit; ++it)
-                if (lgm::mbar_try_wait(&mbar[k & 1], (uint32_t)((k >> 1) & 1))) break;
-        for (int k = mma_issued; k < tma_issued; ++k)
-            for (int it = 0; it < lgm::kWaitLimit; ++it)
-                if (lgm::mbar_try_wait(&tbar[k & 1], (uint32_t)((k >> 1) & 1))) break;
     }
     fence_before_sync();
     __syncthreads();
