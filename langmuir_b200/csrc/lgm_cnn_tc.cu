@@ -21,15 +21,17 @@
 // staged once per CTA as ws[tap][c8][out channel][8 channels] (8 x 16-byte
 // core matrices, SBO 128 bytes, LBO one 8-channel plane).
 //
-// Pipeline (two stages of patch buffers and of 32 TMEM columns), warp
-// specialised: one thread of warp 4 issues the TMA loads and the MMAs; warps
-// 0-3 run the epilogue (tcgen05.ld of the accumulators, bias, ReLU, stores,
-// 2x2 pooling with warp shuffles).  Three pairs of mbarriers hand the stages
+// Pipeline (three stages of patch buffers and of 32 TMEM columns), warp
+// specialised: one thread of warp 8 issues the TMA loads and the MMAs; two
+// groups of four warps run the epilogue of alternate tiles (warps 0-3 the
+// even, 4-7 the odd ones; warp w reads TMEM lanes 32 (w % 4) ..): tcgen05.ld
+// of the accumulators, bias, ReLU, stores, 2x2 pooling with warp shuffles.  Three pairs of mbarriers hand the stages
 // over: "full" (the patch has landed), "done" (the MMAs have finished: the
 // accumulators are ready and the patch buffer is free) and "empty" (the
 // epilogue has read the accumulators: the TMEM stage is free).  While the
 // epilogue warps finish tile k, the tensor core computes tile k+1 and TMA
-// loads tile k+2.
+// loads tiles k+2 and k+3; three stages cover the copy latency, which is
+// longer than one tile's MMAs.
 //
 // Every wait is bounded: a timeout sets a flag that lgm_cnn_error reports;
 // the CTA then waits (bounded) for its own copies and MMAs, frees its TMEM and
@@ -52,8 +54,9 @@ using bf16 = __nv_bfloat16;
 using lgm::smem_addr;
 
 constexpr int TY = 8, TX = 16;                 // output tile
-constexpr int EPI_THREADS = 128;               // epilogue warps 0-3: one pixel (TMEM lane) each
-constexpr int THREADS = EPI_THREADS + 32;      // + warp 4: issues the copies and the MMAs
+constexpr int EPI_THREADS = 256;               // epilogue warps 0-7: two groups of four, a
+                                               // group per stage, one pixel (TMEM lane) per thread
+constexpr int THREADS = EPI_THREADS + 32;      // + warp 8: issues the copies and the MMAs
 constexpr int COUT = LGM_CNN_CHANNELS;         // 32
 constexpr int CIN = LGM_CNN_CHANNELS;          // 32
 constexpr int C8 = CIN / 8;                    // 16-byte channel groups
@@ -61,10 +64,11 @@ constexpr int PROWS = TY + 2;                  // patch rows
 constexpr int XPIX = PROWS * TX;               // rows of one shifted copy (160)
 constexpr uint32_t COPY_BYTES = XPIX * CIN * 2u;           // 10240: one TMA box
 constexpr uint32_t STAGE_BYTES = 3u * COPY_BYTES;          // 30720: one tile's patch copies
-constexpr uint32_t XS_BYTES = 2u * STAGE_BYTES;            // two stages
+constexpr int NST = 3;                                     // pipeline stages
+constexpr uint32_t XS_BYTES = NST * STAGE_BYTES;
 constexpr uint32_t WS_BYTES = 9u * C8 * COUT * 16u;        // 18432
 constexpr uint32_t SMEM_BYTES = XS_BYTES + WS_BYTES + 128; // + mbarriers and TMEM slot
-constexpr uint32_t TMEM_COLS = 64;                         // two stages of 32 columns
+constexpr uint32_t TMEM_COLS = 128;                        // NST stages of 32 columns (power of 2)
 
 // Instruction descriptor of tcgen05.mma kind::f16: D FP32 (bits 4-5 = 1),
 // A and B BF16 (bits 7-9, 10-12 = 1), both K-major, N >> 3 at bit 17,
@@ -160,10 +164,12 @@ conv3x3_fwd_tc(const __grid_constant__ CUtensorMap xmap, const bf16* __restrict_
                int B, int H, int W, int relu) {
     extern __shared__ __align__(1024) unsigned char smem[];
     unsigned char* ws = smem + XS_BYTES;            // [9][C8][COUT][16 B]
-    uint64_t* full = reinterpret_cast<uint64_t*>(smem + XS_BYTES + WS_BYTES);  // [2]
-    uint64_t* done = full + 2;                                                  // [2]
-    uint64_t* empty = full + 4;                                                 // [2]
-    uint32_t* tslot = reinterpret_cast<uint32_t*>(smem + XS_BYTES + WS_BYTES + 64);
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem + XS_BYTES + WS_BYTES);  // [NST]
+    uint64_t* done = full + NST;                                                // [NST]
+    uint64_t* empty = full + 2 * NST;                                           // [NST]
+    // 3 * NST mbarriers (72 bytes), then the TMEM address
+    static_assert(3 * NST * 8 <= 96, "mbarriers overlap the TMEM slot");
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(smem + XS_BYTES + WS_BYTES + 96);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int tiles_x = W / TX, tiles_y = H / TY;
     const int ntiles = B * tiles_x * tiles_y;
@@ -177,8 +183,9 @@ conv3x3_fwd_tc(const __grid_constant__ CUtensorMap xmap, const bf16* __restrict_
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
     if (tid == 0) {
-        for (int i = 0; i < 4; ++i) lgm::mbar_init(&full[i], 1);          // full, done
-        for (int i = 4; i < 6; ++i) lgm::mbar_init(&full[i], EPI_THREADS / 32);  // empty: a lane per warp
+        for (int i = 0; i < 2 * NST; ++i) lgm::mbar_init(&full[i], 1);       // full, done
+        for (int i = 2 * NST; i < 3 * NST; ++i) lgm::mbar_init(&full[i], 4);  // empty: a lane per
+                                                                              // warp of a group
         lgm::fence_mbar_init();
         asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&xmap)) : "memory");
     }
@@ -209,7 +216,7 @@ conv3x3_fwd_tc(const __grid_constant__ CUtensorMap xmap, const bf16* __restrict_
             int tma_issued = 0, mma_issued = 0, mma_waited = 0;
             bool ok = true;
             auto issue_tma = [&](int k) {
-                const int st = k & 1;
+                const int st = k % NST;
                 int b, y0, x0;
                 origin(k, b, y0, x0);
                 lgm::mbar_arrive_expect_tx(&full[st], STAGE_BYTES);
@@ -219,12 +226,11 @@ conv3x3_fwd_tc(const __grid_constant__ CUtensorMap xmap, const bf16* __restrict_
                                 y0 - 1, b, &full[st]);
                 ++tma_issued;
             };
-            issue_tma(0);
-            if (n > 1) issue_tma(1);
+            for (int k = 0; k < NST && k < n; ++k) issue_tma(k);
             for (int k = 0; k < n && ok; ++k) {
-                const int st = k & 1;
-                // the patch has landed; the epilogue has released the TMEM stage (tile k-2)
-                ok = wait(&full[st], k >> 1) && (k < 2 || wait(&empty[st], (k - 2) >> 1));
+                const int st = k % NST;
+                // the patch has landed; the epilogue has released the TMEM stage (tile k-NST)
+                ok = wait(&full[st], k / NST) && (k < NST || wait(&empty[st], (k - NST) / NST));
                 if (!ok) break;
                 fence_after_sync();
                 const uint32_t xa = xs_a + st * STAGE_BYTES, d = tmem + (uint32_t)(st * 32);
@@ -244,39 +250,41 @@ conv3x3_fwd_tc(const __grid_constant__ CUtensorMap xmap, const bf16* __restrict_
                 }
                 umma_commit(&done[st]);
                 ++mma_issued;
-                // tile k-1's MMAs finished -> its patch buffer takes tile k+1
-                if (k >= 1 && k + 1 < n) {
-                    ok = wait(&done[(k - 1) & 1], (k - 1) >> 1);
+                // tile k-1's MMAs finished -> its patch buffer takes tile k-1+NST
+                if (k >= 1 && k - 1 + NST < n) {
+                    ok = wait(&done[(k - 1) % NST], (k - 1) / NST);
                     mma_waited = k;
-                    if (ok) issue_tma(k + 1);
+                    if (ok) issue_tma(k - 1 + NST);
                 }
             }
             // after a timeout: wait (bounded) for the MMAs and copies still in flight
             for (int k = mma_waited; k < mma_issued; ++k)
                 for (int it = 0; it < lgm::kWaitLimit; ++it)
-                    if (lgm::mbar_try_wait(&done[k & 1], (uint32_t)((k >> 1) & 1))) break;
+                    if (lgm::mbar_try_wait(&done[k % NST], (uint32_t)((k / NST) & 1))) break;
             for (int k = mma_issued; k < tma_issued; ++k)
                 for (int it = 0; it < lgm::kWaitLimit; ++it)
-                    if (lgm::mbar_try_wait(&full[k & 1], (uint32_t)((k >> 1) & 1))) break;
+                    if (lgm::mbar_try_wait(&full[k % NST], (uint32_t)((k / NST) & 1))) break;
         }
     } else {
-        // ---- epilogue: warps 0-3, thread = pixel = TMEM lane ----
+        // ---- epilogue: group g = warp / 4 takes the tiles k = g, g + 2, ...
+        // (stage k % NST); thread = pixel = TMEM lane 32 (warp % 4) + lane ----
+        const int g = warp >> 2, wq = warp & 3;
         float bv[32];
 #pragma unroll
         for (int c = 0; c < 32; ++c) bv[c] = bias ? bias[c] : 0.f;
-        for (int k = 0; k < n; ++k) {
-            const int st = k & 1;
-            if (!wait(&done[st], k >> 1)) break;
+        for (int k = g; k < n; k += 2) {
+            const int st = k % NST;
+            if (!wait(&done[st], k / NST)) break;
             fence_after_sync();
             float v[32];
-            tmem_ld32(tmem + (uint32_t)(st * 32) + ((uint32_t)(warp * 32) << 16), v);
+            tmem_ld32(tmem + (uint32_t)(st * 32) + ((uint32_t)(wq * 32) << 16), v);
             fence_before_sync();
             __syncwarp();
             if (lane == 0) mbar_arrive(&empty[st]);  // this warp's TMEM lanes are read
             int b, y0, x0;
             origin(k, b, y0, x0);
-            // this thread's pixel: tile row 2*warp + lane/16, column lane%16
-            const int r = 2 * warp + (lane >> 4), c = lane & 15;
+            // this thread's pixel: tile row 2*wq + lane/16, column lane%16
+            const int r = 2 * wq + (lane >> 4), c = lane & 15;
 #pragma unroll
             for (int ch = 0; ch < 32; ++ch) {
                 v[ch] += bv[ch];
@@ -300,7 +308,7 @@ conv3x3_fwd_tc(const __grid_constant__ CUtensorMap xmap, const bf16* __restrict_
                 if (lane < 16 && (lane & 1) == 0) {
                     const int H2 = H / 2, W2 = W / 2;
                     uint4* dst = reinterpret_cast<uint4*>(
-                        pooled + (((size_t)b * H2 + y0 / 2 + warp) * W2 + x0 / 2 + lane / 2) * COUT);
+                        pooled + (((size_t)b * H2 + y0 / 2 + wq) * W2 + x0 / 2 + lane / 2) * COUT);
 #pragma unroll
                     for (int q = 0; q < 4; ++q)
                         dst[q] = make_uint4(pack2(0.25f * v[8 * q], 0.25f * v[8 * q + 1]),
