@@ -379,7 +379,15 @@ def cnn_layers(S, peaks):
     b1 = B * 128 * 128 * 2 + B * 64 * 64 * 32 * 2            # image in, pooled map out
     f2 = 2 * B * 64 * 64 * 32 * 288                            # layer-2 MACs x 2
     hbm, bf16 = float(peaks.get("hbm_gbs", 6650.0)), float(peaks.get("bf16_tflops", 1590.0))
-    return {"images": B,
+    # the 32-channel layers on both tensor-core kernels (tcgen05 is the product path)
+    compare = {}
+    for size, pool in ((64, True), (32, True), (16, False)):
+        xin = torch.randn(B, size, size, 32, device="cuda").to(torch.bfloat16)
+        fl = 2 * B * size * size * 32 * 288
+        ms = {name: timeit(lambda f=f: f(xin, w2, prm[3], size, size, keep_act=not pool, pool=pool))
+              for name, f in (("tcgen05", S.conv3x3_tc), ("mma_sync", S.conv3x3_mma))}
+        compare[f"{size}x{size}"] = {k + "_tflops": fl / (v * 1e-3) / 1e12 for k, v in ms.items()}
+    return {"images": B, "conv32_tcgen05_vs_mma_sync": compare,
             "conv1_pool": {"ms": t1, "achieved": b1 / (t1 * 1e-3) / 1e9, "peak": hbm,
                            "unit": "GB/s", "frac": b1 / (t1 * 1e-3) / 1e9 / hbm, "bound": "hbm"},
             "conv2_pool": {"ms": t2, "achieved": f2 / (t2 * 1e-3) / 1e12, "peak": bf16,
