@@ -71,6 +71,23 @@ def make_inputs(w, seed):
     return s_all, q_all, ne + nh
 
 
+def job_totals(dist, units, seconds):
+    """Whole-job figures of one bench leg run as independent replicas: the
+    units every rank processed, summed, and the longest rank's time (max over
+    ranks).  Every rank calls this in the same order, leg by leg.  With no
+    process group the rank's own figures come back unchanged."""
+    if dist is None:
+        return float(units), float(seconds)
+    import torch
+    dev = (torch.device("cuda", torch.cuda.current_device())
+           if dist.get_backend() == "nccl" else torch.device("cpu"))
+    u = torch.tensor([float(units)], dtype=torch.float64, device=dev)
+    s = torch.tensor([float(seconds)], dtype=torch.float64, device=dev)
+    dist.all_reduce(u, op=dist.ReduceOp.SUM)
+    dist.all_reduce(s, op=dist.ReduceOp.MAX)
+    return float(u.item()), float(s.item())
+
+
 def measured_peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -222,7 +239,7 @@ def kmc_run(L, w, args, seed, replica):
     hops = s1["proposals"] - s0["proposals"]
     return {"workload": w["desc"] + ", traps 2% at 0.2 eV, site disorder 0.05 eV, 1 V",
             "steps": args.kmc_steps, "ms_per_step": 1e3 * dt / args.kmc_steps,
-            "hops_per_s": hops / dt, "accepted_per_s": (s1["accepted"] - s0["accepted"]) / dt,
+            "hops": hops, "timed_s": dt, "hops_per_s": hops / dt, "accepted_per_s": (s1["accepted"] - s0["accepted"]) / dt,
             "guard_fp64_per_step": (s1["guard_evaluations"] - s0["guard_evaluations"])
             / args.kmc_steps,
             "carriers": s1["electrons"] + s1["holes"],
@@ -284,7 +301,8 @@ def batch_run(L, args, rank):
                         "occupancy U(0.5%,3%) e/h, V U(0.1,2), traps U(0,10%) at U(0.05,0.3) eV, "
                         "cutoff 50",
             "steps": args.batch_steps, "charges": charges,
-            "ms_per_step": 1e3 * dt / args.batch_steps, "hops_per_s": hops / dt,
+            "ms_per_step": 1e3 * dt / args.batch_steps, "hops": hops, "timed_s": dt,
+            "hops_per_s": hops / dt,
             "single_replica_hops_per_s": single,
             "single_replica_sample": f"{len(sample)} of {len(params)} replicas stepped one by one",
             "speedup_vs_single": (hops / dt) / single, "tuning": tuning,
@@ -554,15 +572,12 @@ def main():
         torch.cuda.synchronize(dev)
     ctx.sync(sp)
     step_ms = [a.elapsed_time(b) for a, b in ev]
-    span_ms = float(sum(step_ms))
+    job_pairs, span_s = job_totals(dist, pairs_per_step * args.steps, 1e-3 * sum(step_ms))
     if dist:
-        t = torch.tensor([span_ms], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        span_ms = float(t.item())
         dist.barrier()
     clocks = clk.summary()
-    ms_per_step = span_ms / args.steps
-    value = pairs_per_step * world / (ms_per_step * 1e-3)
+    ms_per_step = 1e3 * span_s / args.steps
+    value = job_pairs / span_s
 
     # accuracy on a sample of targets against the FP64 oracle (the checker)
     o = d_out.cpu().numpy()
@@ -601,14 +616,23 @@ def main():
     kmc = None
     if not args.no_kmc and w["e"] + w["h"] > 0:
         kmc = kmc_run(L, w, args, seed=2 + rank, replica=rank)
+        if dist:
+            h, t = job_totals(dist, kmc["hops"], kmc["timed_s"])
+            kmc["job_hops_per_s"] = h / t
 
     batch = None
     if not args.no_batch:
         batch = batch_run(L, args, rank)
+        if dist:
+            h, t = job_totals(dist, batch["hops"], batch["timed_s"])
+            batch["job_hops_per_s"] = h / t
 
     surrogate = None
     if not args.no_surrogate:
         surrogate = surrogate_run(args, rank)
+        if dist:
+            m, t = job_totals(dist, args.surrogate_candidates, 1e-3 * surrogate["screen_ms"])
+            surrogate["job_morphs_per_s"] = m / t
 
     peaks = measured_peaks()
     props = torch.cuda.get_device_properties(dev)
