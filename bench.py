@@ -88,6 +88,42 @@ def job_totals(dist, units, seconds):
     return float(u.item()), float(s.item())
 
 
+def accuracy_vs_oracle(w, src, q, tgt, got, terms):
+    """FP32 sums against the FP64 oracle (the checker) on a sample of targets:
+    max |V32 - V64| / N with N = sum_j |q_j| w(r_j) (the error scale of a
+    target's potential), and the error relative to |V|."""
+    from oracle import oracle as O
+    orc = O.Oracle(w["X"], w["Y"], w["Z"], cutoff=w["cutoff"], sigma=w["sigma"])
+    g = w["sigma"] > 0
+    want = orc.potentials(src, q, tgt, g, terms)
+    aq = np.abs(q).astype(np.int32)
+    nrm = orc.potentials(src, aq, tgt, g, 1)
+    for t in (2, 4):
+        if terms & t:
+            nrm -= orc.potentials(src, aq, tgt, g, t)  # image terms carry -|q|
+    err = np.abs(np.asarray(got) - want)
+    nrm = np.maximum(nrm, 1e-300)  # a target with no charge inside the cutoff has V = N = 0
+    return {"targets_checked": len(tgt), "max_err_over_norm": float((err / nrm).max()),
+            "max_rel_err": float((err / np.maximum(np.abs(want), 1e-3 * nrm)).max()),
+            "tolerance_over_norm": 1e-6}
+
+
+def grf_phase_3d(X, Y, Z, ell, seed):
+    """Binary bulk-heterojunction morphology: white noise blurred by a
+    Gaussian of standard deviation ``ell`` sites (in Fourier space, on a
+    padded box so the blur does not wrap), thresholded at its median.
+    phase[site] 0 donor, 1 acceptor, x fastest."""
+    rng = np.random.default_rng(seed)
+    pad = int(3 * ell)
+    P = (Z + 2 * pad, Y + 2 * pad, X + 2 * pad)
+    k2 = sum(np.fft.fftfreq(n)[tuple(slice(None) if a == i else None for a in range(3))] ** 2
+             for i, n in enumerate(P))
+    f = np.fft.irfftn(np.fft.rfftn(rng.standard_normal(P))
+                      * np.exp(-2.0 * np.pi ** 2 * k2[:, :, : P[2] // 2 + 1] * ell ** 2), P)
+    f = f[pad:pad + Z, pad:pad + Y, pad:pad + X]
+    return (f > np.median(f)).astype(np.uint8).reshape(-1)
+
+
 def measured_peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -246,6 +282,109 @@ def kmc_run(L, w, args, seed, replica):
             "timing": "host wall clock around graph replays of the whole step"}
 
 
+def _timed_kmc(k, warmup, steps):
+    k.run(warmup)
+    s0 = k.stats()
+    t0 = time.perf_counter()
+    k.run(steps)
+    dt = time.perf_counter() - t0
+    s1 = k.stats()
+    return s0, s1, dt
+
+
+def cfg1_params(L, seed):
+    """Hole transport on 128x128x1: 1% holes seeded uniformly, traps on 5% of
+    sites at 0.1 eV, cutoff 50, no image charges, 1 V across x with the hole
+    source at x = 0 and the drain at x = 127."""
+    p = L.Params.default()
+    for k, v in dict(grid_x=128, grid_y=128, grid_z=1, hole_percentage=0.01,
+                     electron_percentage=0.0, seed_charges=1.0, coulomb_carriers=1,
+                     electrostatic_cutoff=50, trap_percentage=0.05, trap_potential=0.1,
+                     voltage_left=1.0, e_source_l_rate=0.0, h_source_l_rate=0.9,
+                     h_drain_r_rate=0.9, random_seed=seed).items():
+        p.set(k, v)
+    return p
+
+
+def cfg3_params(L, seed):
+    """Solar cell on 128x128x64 with Gaussian-smeared charges (sigma 1, cutoff
+    30): holes confined to donor and electrons to acceptor sites, excitons
+    split at donor-acceptor bonds with probability 1e-3 per step,
+    recombination of interface pairs with probability 1e-3, 0.5 V across x
+    (the engine's field axis), room for 1.25% electrons and holes."""
+    p = L.Params.default()
+    for k, v in dict(simulation_type="solarcell", grid_x=128, grid_y=128, grid_z=64,
+                     electron_percentage=0.0125, hole_percentage=0.0125, seed_charges=0.0,
+                     coulomb_carriers=1, coulomb_gaussian_sigma=1.0, electrostatic_cutoff=30,
+                     voltage_right=0.5, generation_rate=1e-3, source_scale_area=0.0,
+                     recombination_rate=1e-3, recombination_range=1, morphology_confine=1,
+                     generation_interface=1, random_seed=seed).items():
+        p.set(k, v)
+    return p
+
+
+def kmc_configs_run(L, args, rank, world):
+    """The kMC step on config 1 (128x128 holes, with the oracle's FP64 step
+    timed beside it on the host) and config 3 (3-D Gaussian solar cell on a
+    GRF morphology, 1% electrons on acceptor and 1% holes on donor sites)."""
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    out = {}
+    p = cfg1_params(L, seed=11 + rank)
+    with L.KMC(p, device=dev, replica=rank) as k:
+        s0, s1, dt = _timed_kmc(k, args.warmup, args.cfg1_steps)
+        hops = s1["proposals"] - s0["proposals"]
+        out["cfg1"] = {"workload": "128x128x1, 1% holes, traps 5% at 0.1 eV, cutoff 50, "
+                                   "1 V across x",
+                       "steps": args.cfg1_steps, "carriers": s1["holes"],
+                       "ms_per_step": 1e3 * dt / args.cfg1_steps, "hops": hops, "timed_s": dt,
+                       "hops_per_s": hops / dt,
+                       "timing": "host wall clock around graph replays of the whole step"}
+        if rank == 0 and world == 1 and not args.no_cpu_baseline:
+            # the oracle's FP64 kMC step (one host thread) from the same world
+            from oracle import oracle as O
+            from oracle.kmc_setup import oracle_for
+            st = k.stats()
+            e, h = k.carriers()
+            orc = oracle_for(O, p, k.world(), e, h, st["max_electrons"], st["max_holes"],
+                             replica=rank, step=st["step"])
+            n_cpu, h0 = 0, orc.counters.copy()
+            props = 0
+            t0 = time.perf_counter()
+            while time.perf_counter() - t0 < args.cfg1_cpu_seconds:
+                ne, nh = (len(a) for a in orc.carriers())
+                orc.step(threads=1)
+                props += ne + nh
+                n_cpu += 1
+            cdt = time.perf_counter() - t0
+            out["cfg1"]["cpu_baseline"] = {
+                "value": props / cdt, "unit": "hops/s", "cores": 1, "kind": "port",
+                "sample": f"{n_cpu} steps of the oracle's FP64 kMC step (one proposal per "
+                          f"carrier per step) from the GPU replica's world ({cdt:.1f} s)"}
+    p = cfg3_params(L, seed=13 + rank)
+    X, Y, Z = p.grid_x, p.grid_y, p.grid_z
+    phase = grf_phase_3d(X, Y, Z, ell=8.0, seed=17 + rank)
+    rng = np.random.default_rng(19 + rank)
+    n1 = int(0.01 * X * Y * Z)
+    e = rng.choice(np.flatnonzero(phase == 1), n1, replace=False).astype(np.int32)
+    h = rng.choice(np.flatnonzero(phase == 0), n1, replace=False).astype(np.int32)
+    with L.KMC(p, device=dev, replica=rank) as k:
+        k.set_morphology(phase)
+        k.set_carriers(e, h)
+        s0, s1, dt = _timed_kmc(k, args.warmup, args.cfg3_steps)
+        hops = s1["proposals"] - s0["proposals"]
+        out["cfg3"] = {"workload": "128x128x64 solar cell, GRF morphology (blur 8 sites, median "
+                                   "threshold), Gaussian charges sigma 1, cutoff 30, generation "
+                                   "and recombination 1e-3 per step, 0.5 V across x, 1% e + 1% h",
+                       "steps": args.cfg3_steps,
+                       "carriers": s1["electrons"] + s1["holes"],
+                       "ms_per_step": 1e3 * dt / args.cfg3_steps, "hops": hops, "timed_s": dt,
+                       "hops_per_s": hops / dt,
+                       "guard_fp64_per_step": (s1["guard_evaluations"] - s0["guard_evaluations"])
+                       / args.cfg3_steps,
+                       "timing": "host wall clock around graph replays of the whole step"}
+    return out
+
+
 def batch_params(L, n, seed=4):
     """Replicas drawn as the batched configuration draws them: square lattices
     of side {32,64,128,256} x depth {1,2,4,8}, occupancy U(0.5%, 3%) split
@@ -337,6 +476,8 @@ def other_kernels_run(L, args, fp32_peak):
                 ms.append(ctx.last_launch()["pair_kernel_ms"])
         pk = float(np.median(ms))
         pairs = n * T
+        idx = np.linspace(0, T - 1, 512).astype(int)
+        acc = accuracy_vs_oracle(w, s_all[:n], q_all[:n], s_all[idx], d_o.cpu().numpy()[idx], 1)
         achieved = FLOP_PER_PAIR * pairs / (pk * 1e-3) / 1e12
         out["gauss2_cfg3"] = {
             "workload": w["desc"], "pairs_per_launch": pairs, "pair_kernel_ms": pk,
@@ -345,7 +486,7 @@ def other_kernels_run(L, args, fp32_peak):
                          "unit": "TFLOP/s", "frac": achieved / fp32_peak,
                          "note": "11 FLOP per pair as for point charges; erf(f r)/r is a "
                                  "shared-memory table gather on top"},
-            "tile_variant": dict(ctx.variants()[v], id=v)}
+            "tile_variant": dict(ctx.variants()[v], id=v), "accuracy": acc}
     # kernel 1, every site of config 1's lattice
     w = WORKLOADS["cfg1_2d_holes"]
     s_all, q_all, n = make_inputs(w, 6)
@@ -363,7 +504,10 @@ def other_kernels_run(L, args, fp32_peak):
             if i >= args.warmup:
                 ms.append(ctx.last_launch()["pair_kernel_ms"])
         pk = float(np.median(ms))
+        idx = np.linspace(0, vol - 1, 512).astype(np.int32)
+        acc = accuracy_vs_oracle(w, s_all[:n], q_all[:n], idx, d_o.cpu().numpy()[idx], 1)
         out["kernel1_cfg1"] = {"workload": f"every site of {w['desc']}", "charges": n,
+                               "accuracy": acc,
                                "sites": vol, "pair_kernel_ms": pk,
                                "site_charge_evals_per_s": vol * n / (pk * 1e-3),
                                "note": "163 charges: launch- and latency-bound; the "
@@ -492,6 +636,10 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-kmc", action="store_true")
     ap.add_argument("--kmc-steps", type=int, default=50)
+    ap.add_argument("--no-configs", action="store_true", help="skip the config 1 and 3 kMC legs")
+    ap.add_argument("--cfg1-steps", type=int, default=2000)
+    ap.add_argument("--cfg1-cpu-seconds", type=float, default=5.0)
+    ap.add_argument("--cfg3-steps", type=int, default=50)
     ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--batch-replicas", type=int, default=512)
     ap.add_argument("--batch-steps", type=int, default=20)
@@ -583,19 +731,8 @@ def main():
     o = d_out.cpu().numpy()
     acc = None
     if rank == 0:
-        from oracle import oracle as O
-        orc = O.Oracle(w["X"], w["Y"], w["Z"], cutoff=w["cutoff"], sigma=w["sigma"])
         idx = np.linspace(0, T - 1, 512).astype(int)
-        want = orc.potentials(s_all[:n], q_all[:n], s_all[idx], w["sigma"] > 0, w["terms"])
-        nrm = orc.potentials(s_all[:n], np.abs(q_all[:n]), s_all[idx], w["sigma"] > 0, 1)
-        if w["terms"] & 2:
-            nrm -= orc.potentials(s_all[:n], np.abs(q_all[:n]), s_all[idx], w["sigma"] > 0, 2)
-        if w["terms"] & 4:
-            nrm -= orc.potentials(s_all[:n], np.abs(q_all[:n]), s_all[idx], w["sigma"] > 0, 4)
-        err = np.abs(o[idx] - want)
-        acc = {"targets_checked": len(idx), "max_err_over_norm": float((err / nrm).max()),
-               "max_rel_err": float((err / np.maximum(np.abs(want), 1e-3 * nrm)).max()),
-               "tolerance_over_norm": 1e-6}
+        acc = accuracy_vs_oracle(w, s_all[:n], q_all[:n], s_all[idx], o[idx], w["terms"])
 
     # end to end through the host-buffer ABI: H2D inputs, kernels, D2H result
     e2e = None
@@ -619,6 +756,14 @@ def main():
         if dist:
             h, t = job_totals(dist, kmc["hops"], kmc["timed_s"])
             kmc["job_hops_per_s"] = h / t
+
+    configs = None
+    if not args.no_configs:
+        configs = kmc_configs_run(L, args, rank, world)
+        if dist:
+            for key in ("cfg1", "cfg3"):
+                h, t = job_totals(dist, configs[key]["hops"], configs[key]["timed_s"])
+                configs[key]["job_hops_per_s"] = h / t
 
     batch = None
     if not args.no_batch:
@@ -681,7 +826,8 @@ def main():
                        "tile_variant": dict(ctx.variants()[variant], id=variant),
                        "parallelism": "replicas" if world > 1 else "single"},
             "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks, "kmc": kmc,
-            "kmc_batched": batch, "surrogate": surrogate, "other_kernels": others,
+            "kmc_configs": configs, "kmc_batched": batch, "surrogate": surrogate,
+            "other_kernels": others,
             "gpu_launches": launches, "accuracy": acc,
         }
         print(json.dumps(line), flush=True)

@@ -12,6 +12,7 @@ import numpy as np
 import pytest
 
 import langmuir_b200 as L
+from oracle.kmc_setup import interface_bonds, oracle_for, rates  # noqa: F401
 
 
 def make_params(**keys):
@@ -24,50 +25,6 @@ def make_params(**keys):
     return p
 
 
-def rates(p):
-    """World::createSources / createDrains (world.cpp:982-1030, 1110-1150)."""
-    smart = lambda r, d: d if r < 0 else r
-    if p.simulation_type == b"solarcell":
-        gen = smart(p.generation_rate, p.source_rate)
-        area = p.grid_x * p.grid_y
-        if p.source_scale_area > 0 and p.source_scale_area != area:
-            gen *= area / p.source_scale_area
-        return dict(rate_e_source_l=smart(p.e_source_l_rate, 0.0),
-                    rate_e_source_r=smart(p.e_source_r_rate, 0.0),
-                    rate_h_source_l=smart(p.h_source_l_rate, 0.0),
-                    rate_h_source_r=smart(p.h_source_r_rate, 0.0),
-                    rate_e_drain_l=smart(p.e_drain_l_rate, p.drain_rate),
-                    rate_e_drain_r=smart(p.e_drain_r_rate, p.drain_rate),
-                    rate_h_drain_l=smart(p.h_drain_l_rate, p.drain_rate),
-                    rate_h_drain_r=smart(p.h_drain_r_rate, p.drain_rate),
-                    solar=1, generation_rate=gen, recombination_rate=p.recombination_rate,
-                    recombination_range=p.recombination_range)
-    return dict(rate_e_source_l=smart(p.e_source_l_rate, p.source_rate),
-                rate_e_source_r=smart(p.e_source_r_rate, 0.0),
-                rate_h_source_l=smart(p.h_source_l_rate, 0.0),
-                rate_h_source_r=smart(p.h_source_r_rate, 0.0),
-                rate_e_drain_l=smart(p.e_drain_l_rate, 0.0),
-                rate_e_drain_r=smart(p.e_drain_r_rate, p.drain_rate),
-                rate_h_drain_l=smart(p.h_drain_l_rate, 0.0),
-                rate_h_drain_r=smart(p.h_drain_r_rate, 0.0))
-
-
-def interface_bonds(phase, X, Y, Z):
-    """Donor-acceptor bonds in the order lgm_kmc_set_morphology lists them."""
-    bonds = []
-    for s in range(X * Y * Z):
-        if phase[s] != 0:
-            continue
-        z, y, x = s // (X * Y), (s // X) % Y, s % X
-        for (a, b, c) in ((x - 1, y, z), (x + 1, y, z), (x, y - 1, z), (x, y + 1, z),
-                          (x, y, z - 1), (x, y, z + 1)):
-            if 0 <= a < X and 0 <= b < Y and 0 <= c < Z:
-                t = X * (b + c * Y) + a
-                if phase[t] == 1:
-                    bonds += [s, t]
-    return np.array(bonds, dtype=np.int32)
-
-
 def blob_phase(X, Y, Z, seed):
     """A seeded two-phase morphology: smoothed noise thresholded at its median."""
     rng = np.random.default_rng(seed)
@@ -77,28 +34,6 @@ def blob_phase(X, Y, Z, seed):
             if f.shape[ax] > 1:
                 f = (f + np.roll(f, 1, ax) + np.roll(f, -1, ax)) / 3
     return (f > np.median(f)).astype(np.uint8).reshape(-1)
-
-
-def oracle_for(O, p, world, e, h, max_e, max_h, replica=0, step=0, phase=None):
-    q = L.Params.from_text("[Parameters]\n")  # fresh copy for the derived constants
-    for name, _ in L.Params._fields_:
-        setattr(q, name, getattr(p, name))
-    q.check()
-    orc = O.Oracle(q.grid_x, q.grid_y, q.grid_z, cutoff=q.electrostatic_cutoff,
-                   hopping_range=q.hopping_range, sigma=q.coulomb_gaussian_sigma,
-                   prefactor=q.electrostatic_prefactor)
-    cfg = O.KmcConfig(inverse_kt=q.inverse_kt, exciton_binding=q.exciton_binding,
-                      coulomb_carriers=q.coulomb_carriers, defects_charge=q.defects_charge,
-                      image_terms=(2 if q.image_charges & 1 else 0) | (4 if q.image_charges & 2 else 0),
-                      max_electrons=max_e, max_holes=max_h,
-                      seed=q.random_seed & 0xFFFFFFFF, replica=replica, **rates(q))
-    bonds = None
-    if phase is not None:
-        cfg.confine = q.morphology_confine
-        if q.generation_interface:
-            bonds = interface_bonds(phase, q.grid_x, q.grid_y, q.grid_z)
-    return O.KmcOracle(orc, world["site_energy"], world["defects"], e, h, cfg, step,
-                       phase=phase, bonds=bonds)
 
 
 # ---- CPU: the oracle step's invariants ------------------------------------------------
@@ -184,6 +119,14 @@ CASES = {
                                      source_scale_area=0, recombination_rate=0.1,
                                      recombination_range=1, morphology_confine=1,
                                      generation_interface=1, steps=120, morphology=3),
+    "solar_3d_gauss_confined": dict(simulation_type="solarcell", grid_x=24, grid_y=24,
+                                    grid_z=12, electron_percentage=0.02, hole_percentage=0.02,
+                                    seed_charges=0.0, coulomb_gaussian_sigma=1.0,
+                                    electrostatic_cutoff=30, voltage_right=0.5,
+                                    generation_rate=0.8, source_scale_area=0,
+                                    recombination_rate=0.05, recombination_range=1,
+                                    morphology_confine=1, generation_interface=1, steps=150,
+                                    morphology=5),
     "2d_128_holes_1pct": dict(grid_x=128, grid_y=128, grid_z=1, hole_percentage=0.01,
                               electron_percentage=0.0, trap_percentage=0.05,
                               trap_potential=0.1, voltage_left=1.0, e_source_l_rate=0.0,
