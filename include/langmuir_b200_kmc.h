@@ -191,11 +191,19 @@ lgm_status lgm_kmc_last_outcomes(lgm_kmc* k, int32_t* outcome, double* de, int32
 /* ---- batched replicas --------------------------------------------------------
  * `count` independent replicas, params[i] for replica i (sizes, occupancies,
  * voltages and traps may all differ; the interaction kind must not), advanced
- * together: each phase of the step is one launch over all replicas and a
- * batched step is one CUDA graph.  Replica i uses the random stream of a
- * single replica with id replica0 + i, so its trajectory equals that of
- * lgm_kmc_create(&params[i], device, replica0 + i).  Before the first step the
- * pair-sum tile shape and work split are tuned on the batch itself. */
+ * together.  Replica i uses the random stream of a single replica with id
+ * replica0 + i, so its trajectory equals that of
+ * lgm_kmc_create(&params[i], device, replica0 + i).
+ * Two step forms share the batch:
+ *  - fused: each replica runs the whole step inside one block, many steps
+ *    per launch;
+ *  - per phase: each phase of the step is one launch over the replicas, with
+ *    the pair-sum tile shape and work split tuned on the batch before the
+ *    first step; a batched step is one CUDA graph.
+ * By default a batch whose replicas all have room for at most 2048 charges
+ * (electron plus hole capacity) takes the fused form, any other the per-phase
+ * form.  lgm_kmc_batch_set_fused splits a batch by capacity: both forms then
+ * run in one graph, the fused kernel on a parallel branch. */
 typedef struct lgm_kmc_batch lgm_kmc_batch;
 lgm_status lgm_kmc_batch_create(const lgm_params* params, int32_t count, int32_t device,
                                 uint32_t replica0, lgm_kmc_batch** out);
@@ -207,6 +215,12 @@ int32_t lgm_kmc_batch_size(const lgm_kmc_batch* b);
 /* Replica i, owned by the batch: use the lgm_kmc_* accessors on it (stats,
  * carriers, world, outcomes); do not destroy or run it. */
 lgm_kmc* lgm_kmc_batch_replica(lgm_kmc_batch* b, int32_t i);
+/* Replicas with room for at most `max_charges` charges take the fused step,
+ * the others the per-phase kernels (0: none fused).  Only before the first
+ * lgm_kmc_batch_run. */
+lgm_status lgm_kmc_batch_set_fused(lgm_kmc_batch* b, int32_t max_charges);
+/* How many replicas take the fused step. */
+int32_t lgm_kmc_batch_fused_count(const lgm_kmc_batch* b);
 /* The tuned pair-sum shape: threads per CTA, target pairs per thread, source
  * chunks per work item, and the number of work items. */
 lgm_status lgm_kmc_batch_tuning(const lgm_kmc_batch* b, int32_t* threads, int32_t* target_pairs,

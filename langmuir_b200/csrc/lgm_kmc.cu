@@ -90,6 +90,8 @@ struct Dev {
     float* part_norm;
     double *Vt, *Nt;
     double* w64;          // FP64 w(k) for integer r^2 = k < cutoff^2 (w(0) = 0), the guard's table
+    const float* gtab;    // Gaussian charges: the pair kernel's FP32 erf(f r)/r table
+    int gtab_k;           // its last index (NaN there: past it the term is 1/r)
     int splits;
     int src_cap;   // source records capacity (multiple of CH)
     int tpad_cap;  // per-term target block capacity
@@ -688,11 +690,148 @@ __global__ void kb_recomb_reset(const Dev* R, const int4* map) {
 __global__ void kb_claim(const Dev* R, const int4* map) { LGM_BATCH_LOOP(claim_body(D, i)) }
 __global__ void kb_move(const Dev* R, const int4* map) { LGM_BATCH_LOOP(move_body(D, i)) }
 __global__ void kb_unclaim(const Dev* R, const int4* map) { LGM_BATCH_LOOP(unclaim_body(D, i)) }
-// one block per replica
-__global__ void __launch_bounds__(kCompactThreads) kb_compact_inject(const Dev* R) {
+// one block per replica of the list
+__global__ void __launch_bounds__(kCompactThreads) kb_compact_inject(const Dev* R, const int* list) {
     __shared__ int warp_sums[32];
-    compact_inject_body(R[blockIdx.x], warp_sums);
+    compact_inject_body(R[list[blockIdx.x]], warp_sums);
 }
+
+// ---- the fused step: one block per replica, every phase inside the block ----------
+//
+// For replicas small enough that one block carries their whole step, the
+// phases above run back to back inside one kernel with __syncthreads between
+// them, for many steps per launch.  The phase bodies are the ones the
+// separate kernels call, over the same index ranges, with a block-uniform
+// loop (every thread runs the same iterations, so the warp-level sums in
+// move_body see full warps); __syncthreads orders their global-memory writes
+// as the kernel boundaries do.  Only the pair sum differs in form.
+
+
+// The replica's pair sum inside the block: for every target the arithmetic of
+// pair_tile with a single source split -- runs of kSUB sources in FP32 (r^2 - 1/2
+// exact, MUFU rsqrt, predicated FFMA), each run folded into FP64 in source
+// order, |run sum| added to the FP32 norm -- so the partials equal those of the
+// pair kernel with one split bit for bit.  One target per thread at a time:
+// every thread reads the same source record at a time (one broadcast load per
+// warp, an L1 hit after the first warp).  Carrying 2-4 targets per thread
+// through the source loop measured slower here (fewer threads busy, more
+// registers).  A charge class is padded to whole chunks with records of
+// charge 0; its runs past the class's live charges add exact zeros and are
+// skipped.
+__device__ void fused_pair_body(const Dev& D) {
+    const int ne = D.cnt[I_NE], nh = D.cnt[I_NH];
+    const int nd = D.dq != 0 ? D.nd : 0;
+    const int pe = (ne + CH - 1) / CH * CH, ph = (nh + CH - 1) / CH * CH;
+    const int start[3] = {0, pe, pe + ph}, count[3] = {ne, nh, nd};
+    const int t = 2 * (ne + nh);
+    const int tpad = D.cnt[I_TPAD];
+    const float4* geo = D.geo;
+    const float2* qq = D.qq;
+    const float* gtab = D.gtab;
+    const int gtab_k = D.gtab_k, gauss = D.gauss;
+    const unsigned ulim = __float_as_uint((float)D.cutoff2 - 0.5f);
+    for (int g = threadIdx.x; g < D.nterms * t; g += blockDim.x) {
+        const int slot = g / t;
+        const int p = slot * tpad + (g - slot * t);
+        const float4 tg = D.tgt[p];
+        double acc64 = 0.0;
+        float nrm = 0.f;
+        for (int c = 0; c < 3; ++c) {
+            const int s1 = start[c] + count[c];
+            for (int r0 = start[c]; r0 < s1; r0 += kSUB) {
+                const int r1 = min(r0 + kSUB, s1);
+                float acc = 0.f;
+                for (int j = r0; j < r1; ++j) {
+                    const float4 g0 = geo[2 * j], g1 = geo[2 * j + 1];
+                    float u = __fadd_rn(g1.z, tg.w);  // d + |t|^2
+                    u = __fmaf_rn(tg.x, g0.x, u);
+                    u = __fmaf_rn(tg.y, g0.z, u);
+                    u = __fmaf_rn(tg.z, g1.x, u);     // r^2 - 1/2, exact
+                    const float r2 = __fadd_rn(u, 0.5f);
+                    float w = rsqrt_mufu(r2);
+                    if (gauss) {
+                        const int ix = min(__float_as_int(r2 + 8388608.f) & 0x7fffff, gtab_k);
+                        w = fminf(gtab[ix], w);
+                    }
+                    fma_if_below(acc, qq[j].x, w, __float_as_uint(u), ulim);
+                }
+                acc64 += (double)acc;
+                nrm += fabsf(acc);
+            }
+        }
+        D.part[p] = acc64;
+        D.part_norm[p] = nrm;
+    }
+}
+
+#define LGM_BLOCK_LOOP(BOUND, CALL)                                                     \
+    for (int base_ = 0; base_ < (BOUND); base_ += (int)blockDim.x) {                  \
+        const int i = base_ + (int)threadIdx.x;                                       \
+        CALL;                                                                         \
+    }
+
+// Block b advances replica list[b] by `steps` steps.  `recomb` is the batch's
+// flag (the recombination phases run for every replica of a batch in which any
+// replica recombines, as the separate kernels do).  The replica's descriptor
+// is copied to shared memory once; each phase loops over the live charges
+// counted at the phase's start, not over the capacity.
+template <int NT>
+__global__ void __launch_bounds__(NT) kb_fused(const Dev* R, const int* list, int steps, int recomb) {
+    __shared__ double2 red[NT];
+    __shared__ int warp_sums[32];
+    __shared__ Dev sD;
+    {
+        static_assert(sizeof(Dev) % 4 == 0, "word copy");
+        const uint32_t* src = reinterpret_cast<const uint32_t*>(&R[list[blockIdx.x]]);
+        uint32_t* dst = reinterpret_cast<uint32_t*>(&sD);
+        for (int w = threadIdx.x; w < (int)(sizeof(Dev) / 4); w += NT) dst[w] = src[w];
+    }
+    __syncthreads();
+    const Dev& D = sD;
+    const int nd = D.dq != 0 ? D.nd : 0;
+    for (int s = 0; s < steps; ++s) {
+        int ne = D.cnt[I_NE], nh = D.cnt[I_NH];
+        LGM_BLOCK_LOOP(max(1, ne + nh), choose_body(D, i))
+        __syncthreads();
+        if (D.coulomb) {
+            const int nsrc = (ne + CH - 1) / CH * CH + (nh + CH - 1) / CH * CH +
+                             (nd + CH - 1) / CH * CH;
+            const int tpad = (2 * (ne + nh) + 63) / 64 * 64;
+            LGM_BLOCK_LOOP(max(nsrc, tpad), pack_body(D, i))
+            __syncthreads();
+            fused_pair_body(D);
+            __syncthreads();
+            LGM_BLOCK_LOOP(2 * (ne + nh), finalize_body(D, i))
+            __syncthreads();
+        }
+        LGM_BLOCK_LOOP(ne + nh, decide_body(D, i))
+        __syncthreads();
+        if (D.coulomb) {
+            guard_body(D, 0, 1, red);
+            __syncthreads();
+        }
+        if (recomb) {
+            LGM_BLOCK_LOOP(nh, hmap_body(D, i, true))
+            __syncthreads();
+            LGM_BLOCK_LOOP(ne, recomb_propose_body(D, i))
+            __syncthreads();
+            LGM_BLOCK_LOOP(ne, recomb_resolve_body(D, i))
+            __syncthreads();
+            LGM_BLOCK_LOOP(max(ne, nh), recomb_reset_body(D, i))
+            __syncthreads();
+        }
+        LGM_BLOCK_LOOP(ne + nh, claim_body(D, i))
+        __syncthreads();
+        LGM_BLOCK_LOOP(ne + nh, move_body(D, i))
+        __syncthreads();
+        LGM_BLOCK_LOOP(ne + nh, unclaim_body(D, i))
+        __syncthreads();
+        compact_inject_body(D, warp_sums);
+        __syncthreads();
+    }
+}
+// Block sizes of the fused step: small replicas fill 128 threads, larger 256.
+constexpr int kFusedSmallCharges = 512;
 
 // ---- host side -------------------------------------------------------------------
 
@@ -1254,6 +1393,8 @@ static lgm_status kmc_create_impl(const lgm_params* pin, int32_t device, uint32_
         if ((st = dalloc(k, &k->gtab, gt.size())) != LGM_OK) return bail(st, k->err);
         if (cudaMemcpy(k->gtab, gt.data(), gt.size() * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess)
             return bail(LGM_ERR_CUDA, "table upload");
+        D.gtab = k->gtab;
+        D.gtab_k = kmax;
         cudaFuncSetAttribute(kmc_pair(1), cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)pair_smem_bytes(kmax));
     }
@@ -1472,6 +1613,12 @@ const BatchVariant kBatchVariants[] = {LGM_BV(128, 4), LGM_BV(128, 2), LGM_BV(64
 constexpr int kNumBatchVariants = 4;
 // Source chunks per pair work item tried by the tuner.
 const int kChunksPerItem[] = {16, 48};
+// A batch whose replicas all have room for at most this many charges takes
+// the fused step by default (one block per replica).
+constexpr int kFusedMaxCharges = 2048;
+// Steps per launch of the fused kernel when no replica needs the per-phase
+// kernels (bounds the length of one launch).
+constexpr int kFusedStepsPerLaunch = 1000;
 
 }  // namespace
 
@@ -1491,6 +1638,15 @@ struct lgm_kmc_batch {
     int4 *map_car = nullptr, *map_pack = nullptr, *map_fin = nullptr, *map_guard = nullptr;
     int nb_car = 0, nb_pack = 0, nb_fin = 0, nb_guard = 0;
     int compact_threads = kCompactThreads;  // block size of the per-replica list compaction
+    // replicas on the fused step and on the per-phase kernels
+    int fused_max = kFusedMaxCharges;
+    bool started = false;  // a step has run: the partition is fixed
+    bool fused_small = false;  // every fused replica fits the 128-thread block
+    bool fused_set = false;    // the caller set the bound: capacity alone decides
+    std::vector<int> fused, classic;
+    int *d_fused = nullptr, *d_classic = nullptr;
+    cudaStream_t aux = nullptr;            // the fused branch of the graph
+    cudaEvent_t fork = nullptr, join = nullptr;
     DevicePool pool;                         // every replica's buffers
     int variant = 0, cpi = 16;
     std::vector<Dev> hD;
@@ -1519,7 +1675,8 @@ lgm_status build_items(lgm_kmc_batch* b, int v, int cpi) {
     const int tile = BV.nt * 2 * BV.rp;
     std::vector<int4> items;
     std::vector<PairArgs> pargs(b->reps.size());
-    for (size_t r = 0; r < b->reps.size(); ++r) {
+    for (int r : b->fused) b->hD[r].splits = 1;  // the fused pair sum is one split
+    for (int r : b->classic) {
         Dev& D = b->hD[r];
         const lgm_kmc* k = b->reps[r];
         const int chunks = D.src_cap / CH;
@@ -1527,7 +1684,7 @@ lgm_status build_items(lgm_kmc_batch* b, int v, int cpi) {
         D.splits = splits;
         const int tiles = (D.nterms * D.tpad_cap + tile - 1) / tile;
         for (int t = 0; t < tiles; ++t)
-            for (int sp = 0; sp < splits; ++sp) items.push_back(make_int4((int)r, t, sp, splits));
+            for (int sp = 0; sp < splits; ++sp) items.push_back(make_int4(r, t, sp, splits));
         PairArgs& A = pargs[r];
         A.geo = D.geo; A.qq = D.qq; A.splits = splits; A.tgt = D.tgt; A.part = D.part;
         A.part_norm = D.part_norm; A.c2 = (float)D.cutoff2;
@@ -1537,7 +1694,8 @@ lgm_status build_items(lgm_kmc_batch* b, int v, int cpi) {
     if (b->d_items) cudaFree(b->d_items);
     b->d_items = nullptr;
     BCUDA(b, cudaMalloc(&b->d_items, sizeof(int4) * std::max<size_t>(items.size(), 1)));
-    BCUDA(b, cudaMemcpy(b->d_items, items.data(), sizeof(int4) * items.size(), cudaMemcpyHostToDevice));
+    if (!items.empty())
+        BCUDA(b, cudaMemcpy(b->d_items, items.data(), sizeof(int4) * items.size(), cudaMemcpyHostToDevice));
     BCUDA(b, cudaMemcpy(b->d_pargs, pargs.data(), sizeof(PairArgs) * pargs.size(), cudaMemcpyHostToDevice));
     BCUDA(b, cudaMemcpy(b->d_reps, b->hD.data(), sizeof(Dev) * b->hD.size(), cudaMemcpyHostToDevice));
     b->n_items = (int)items.size();
@@ -1557,9 +1715,44 @@ lgm_status enqueue_batch_pair(lgm_kmc_batch* b, cudaStream_t st) {
     return LGM_OK;
 }
 
+void launch_fused(const lgm_kmc_batch* b, cudaStream_t st, int steps) {
+    const int n = (int)b->fused.size();
+    if (b->fused_small)
+        kb_fused<128><<<n, 128, 0, st>>>(b->d_reps, b->d_fused, steps, b->recomb);
+    else
+        kb_fused<256><<<n, 256, 0, st>>>(b->d_reps, b->d_fused, steps, b->recomb);
+}
+
+// The fused replicas' step on the aux stream, forked from and joined back to
+// the batch stream (inside a capture: a parallel branch of the graph).
+lgm_status enqueue_fused(lgm_kmc_batch* b, int steps, bool branch) {
+    if (b->fused.empty()) return LGM_OK;
+    cudaStream_t st = b->stream;
+    if (branch) {
+        BCUDA(b, cudaEventRecord(b->fork, b->stream));
+        BCUDA(b, cudaStreamWaitEvent(b->aux, b->fork, 0));
+        st = b->aux;
+    }
+    launch_fused(b, st, steps);
+    BCUDA(b, cudaGetLastError());
+    if (branch) {
+        BCUDA(b, cudaEventRecord(b->join, b->aux));
+        BCUDA(b, cudaStreamWaitEvent(b->stream, b->join, 0));
+    }
+    return LGM_OK;
+}
+
 lgm_status enqueue_batch_step(lgm_kmc_batch* b) {
     cudaStream_t st = b->stream;
-    const int R = (int)b->reps.size();
+    if (b->classic.empty()) return enqueue_fused(b, 1, false);
+    const bool fork = !b->fused.empty();
+    if (fork) {
+        BCUDA(b, cudaEventRecord(b->fork, b->stream));
+        BCUDA(b, cudaStreamWaitEvent(b->aux, b->fork, 0));
+        launch_fused(b, b->aux, 1);
+        BCUDA(b, cudaGetLastError());
+    }
+    const int R = (int)b->classic.size();
     kb_choose<<<b->nb_car, 256, 0, st>>>(b->d_reps, b->map_car);
     if (b->coulomb) {
         kb_pack<<<b->nb_pack, 256, 0, st>>>(b->d_reps, b->map_pack);
@@ -1578,15 +1771,19 @@ lgm_status enqueue_batch_step(lgm_kmc_batch* b) {
     kb_claim<<<b->nb_car, 256, 0, st>>>(b->d_reps, b->map_car);
     kb_move<<<b->nb_car, 256, 0, st>>>(b->d_reps, b->map_car);
     kb_unclaim<<<b->nb_car, 256, 0, st>>>(b->d_reps, b->map_car);
-    kb_compact_inject<<<R, b->compact_threads, 0, st>>>(b->d_reps);
+    kb_compact_inject<<<R, b->compact_threads, 0, st>>>(b->d_reps, b->d_classic);
     BCUDA(b, cudaGetLastError());
+    if (fork) {
+        BCUDA(b, cudaEventRecord(b->join, b->aux));
+        BCUDA(b, cudaStreamWaitEvent(b->stream, b->join, 0));
+    }
     return LGM_OK;
 }
 
 // The project's tile tuner for the batch: times every (variant, chunks per
 // item) pair on the batch's current charges with CUDA events, keeps the best.
 lgm_status tune_batch(lgm_kmc_batch* b) {
-    if (!b->coulomb) return LGM_OK;
+    if (!b->coulomb || b->classic.empty()) return LGM_OK;
     cudaStream_t st = b->stream;
     kb_choose<<<b->nb_car, 256, 0, st>>>(b->d_reps, b->map_car);
     kb_pack<<<b->nb_pack, 256, 0, st>>>(b->d_reps, b->map_pack);
@@ -1618,6 +1815,65 @@ lgm_status tune_batch(lgm_kmc_batch* b) {
     b->cpi = bc;
     // the step counters advanced by nothing: choose/pack only snapshot counts
     return build_items(b, bv, bc);
+}
+
+// Splits the replicas between the fused step (room for at most b->fused_max
+// charges) and the per-phase kernels, and builds the per-phase kernels' block
+// maps -- {replica, local block, blocks of the replica, index bound} -- and
+// pair work items over the latter.
+lgm_status partition_batch(lgm_kmc_batch* b) {
+    b->fused.clear();
+    b->classic.clear();
+    // By default a batch takes one form: the fused step when every replica fits
+    // one block, else the per-phase kernels for all (beside a graph of large
+    // replicas the fused blocks measured slower than the per-phase kernels on
+    // the same small replicas).  A bound set by the caller splits the batch.
+    bool all_fit = true;
+    for (const Dev& D : b->hD) all_fit &= D.cap_e + D.cap_h <= b->fused_max;
+    for (int r = 0; r < (int)b->hD.size(); ++r) {
+        const Dev& D = b->hD[r];
+        const bool fits = D.cap_e + D.cap_h <= b->fused_max && (b->fused_set || all_fit);
+        (fits ? b->fused : b->classic).push_back(r);
+    }
+    b->fused_small = true;
+    for (int r : b->fused)
+        b->fused_small &= b->hD[r].cap_e + b->hD[r].cap_h <= kFusedSmallCharges;
+    std::vector<int4> car, pack, fin, guard;
+    auto add = [](std::vector<int4>& v, int r, int bound) {
+        const int nb = std::max(1, (bound + kItemsPerThread * 256 - 1) / (kItemsPerThread * 256));
+        for (int i = 0; i < nb; ++i) v.push_back(make_int4(r, i, nb, bound));
+    };
+    int max_cap = 1;
+    for (int r : b->classic) {
+        const Dev& D = b->hD[r];
+        const int ncap = std::max(1, D.cap_e + D.cap_h);
+        add(car, r, ncap);
+        add(pack, r, std::max(D.src_cap, D.tpad_cap));
+        add(fin, r, 2 * ncap);
+        // flagged decisions grow with the charge count: one block per 2048 of capacity
+        const int ng = std::min(kGuardBlocksPerReplica, std::max(1, (ncap + 2047) / 2048));
+        for (int i = 0; i < ng; ++i) guard.push_back(make_int4(r, i, ng, 0));
+        max_cap = std::max(max_cap, std::max(D.cap_e, D.cap_h));
+    }
+    auto upload = [&](auto** dst, const auto& v) -> bool {
+        if (*dst) cudaFree(*dst);
+        *dst = nullptr;
+        const size_t bytes = sizeof(v[0]) * std::max<size_t>(v.size(), 1);
+        return cudaMalloc(dst, bytes) == cudaSuccess &&
+               (v.empty() || cudaMemcpy(*dst, v.data(), sizeof(v[0]) * v.size(),
+                                        cudaMemcpyHostToDevice) == cudaSuccess);
+    };
+    if (!upload(&b->map_car, car) || !upload(&b->map_pack, pack) || !upload(&b->map_fin, fin) ||
+        !upload(&b->map_guard, guard) || !upload(&b->d_fused, b->fused) ||
+        !upload(&b->d_classic, b->classic))
+        return bfail(b, LGM_ERR_CUDA, "block maps");
+    b->nb_guard = (int)guard.size();
+    // the compaction loops over its list in blocks: small replicas need no 1024-thread block
+    b->compact_threads = max_cap > 4096 ? kCompactThreads : 256;
+    b->nb_car = (int)car.size();
+    b->nb_pack = (int)pack.size();
+    b->nb_fin = (int)fin.size();
+    return build_items(b, 0, kChunksPerItem[0]);
 }
 
 }  // namespace
@@ -1658,37 +1914,6 @@ lgm_status lgm_kmc_batch_create(const lgm_params* params, int32_t count, int32_t
             return bail(LGM_ERR_UNSUPPORTED,
                         "a batch mixes point and Gaussian charges or Coulomb on and off");
     for (lgm_kmc* k : b->reps) b->hD.push_back(k->D);
-    // block maps: {replica, local block, blocks of the replica, index bound}
-    std::vector<int4> car, pack, fin, guard;
-    auto add = [](std::vector<int4>& v, int r, int bound) {
-        const int nb = std::max(1, (bound + kItemsPerThread * 256 - 1) / (kItemsPerThread * 256));
-        for (int i = 0; i < nb; ++i) v.push_back(make_int4(r, i, nb, bound));
-    };
-    for (int r = 0; r < count; ++r) {
-        const Dev& D = b->hD[r];
-        const int ncap = std::max(1, D.cap_e + D.cap_h);
-        add(car, r, ncap);
-        add(pack, r, std::max(D.src_cap, D.tpad_cap));
-        add(fin, r, 2 * ncap);
-        // flagged decisions grow with the charge count: one block per 2048 of capacity
-        const int ng = std::min(kGuardBlocksPerReplica, std::max(1, (ncap + 2047) / 2048));
-        for (int i = 0; i < ng; ++i) guard.push_back(make_int4(r, i, ng, 0));
-    }
-    auto upload = [&](int4** dst, const std::vector<int4>& v) -> bool {
-        return cudaMalloc(dst, sizeof(int4) * v.size()) == cudaSuccess &&
-               cudaMemcpy(*dst, v.data(), sizeof(int4) * v.size(), cudaMemcpyHostToDevice) == cudaSuccess;
-    };
-    if (!upload(&b->map_car, car) || !upload(&b->map_pack, pack) || !upload(&b->map_fin, fin) ||
-        !upload(&b->map_guard, guard))
-        return bail(LGM_ERR_CUDA, "block maps");
-    b->nb_guard = (int)guard.size();
-    // the compaction loops over its list in blocks: small replicas need no 1024-thread block
-    int max_cap = 1;
-    for (const Dev& D : b->hD) max_cap = std::max(max_cap, std::max(D.cap_e, D.cap_h));
-    b->compact_threads = max_cap > 4096 ? kCompactThreads : 256;
-    b->nb_car = (int)car.size();
-    b->nb_pack = (int)pack.size();
-    b->nb_fin = (int)fin.size();
     if (cudaMalloc(&b->d_reps, sizeof(Dev) * count) != cudaSuccess ||
         cudaMalloc(&b->d_pargs, sizeof(PairArgs) * count) != cudaSuccess)
         return bail(LGM_ERR_CUDA, "descriptors");
@@ -1699,7 +1924,11 @@ lgm_status lgm_kmc_batch_create(const lgm_params* params, int32_t count, int32_t
             cudaFuncSetAttribute(BV.fn[1], cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)batch_smem(b));
     }
-    lgm_status s = build_items(b, 0, kChunksPerItem[0]);
+    if (cudaStreamCreateWithFlags(&b->aux, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&b->join, cudaEventDisableTiming) != cudaSuccess)
+        return bail(LGM_ERR_CUDA, "fused branch stream");
+    lgm_status s = partition_batch(b);
     if (s != LGM_OK) return bail(s, b->err);
     *out = b;
     return LGM_OK;
@@ -1712,9 +1941,12 @@ lgm_status lgm_kmc_batch_destroy(lgm_kmc_batch* b) {
     if (b->exec) cudaGraphExecDestroy(b->exec);
     if (b->graph) cudaGraphDestroy(b->graph);
     void* ptrs[] = {b->d_reps, b->d_pargs, b->d_items, b->map_car, b->map_pack, b->map_fin,
-                    b->map_guard};
+                    b->map_guard, b->d_fused, b->d_classic};
     for (void* p : ptrs)
         if (p) cudaFree(p);
+    if (b->fork) cudaEventDestroy(b->fork);
+    if (b->join) cudaEventDestroy(b->join);
+    if (b->aux) cudaStreamDestroy(b->aux);
     for (lgm_kmc* k : b->reps) lgm_kmc_destroy(k);  // they do not own the stream or pool
     if (b->stream) cudaStreamDestroy(b->stream);
     b->pool.release();
@@ -1737,6 +1969,16 @@ lgm_status lgm_kmc_batch_run(lgm_kmc_batch* b, int32_t steps) {
     if (!b || steps < 0) return LGM_ERR_INVALID_ARGUMENT;
     BCUDA(b, cudaSetDevice(b->device));
     BCUDA(b, cudaStreamSynchronize(b->stream));  // every replica's work is on the batch stream
+    b->started = true;
+    if (b->classic.empty()) {
+        // every replica on the fused step: many steps per launch, no graph needed
+        for (int done = 0; done < steps; done += kFusedStepsPerLaunch) {
+            lgm_status s = enqueue_fused(b, std::min(kFusedStepsPerLaunch, steps - done), false);
+            if (s != LGM_OK) return s;
+        }
+        BCUDA(b, cudaStreamSynchronize(b->stream));
+        return LGM_OK;
+    }
     if (!b->exec && steps > 0) {
         lgm_status s = tune_batch(b);
         if (s != LGM_OK) return s;
@@ -1753,6 +1995,19 @@ lgm_status lgm_kmc_batch_run(lgm_kmc_batch* b, int32_t steps) {
     for (int i = 0; i < steps; ++i) BCUDA(b, cudaGraphLaunch(b->exec, b->stream));
     BCUDA(b, cudaStreamSynchronize(b->stream));
     return LGM_OK;
+}
+
+lgm_status lgm_kmc_batch_set_fused(lgm_kmc_batch* b, int32_t max_charges) {
+    if (!b || max_charges < 0) return LGM_ERR_INVALID_ARGUMENT;
+    if (b->started) return bfail(b, LGM_ERR_INVALID_ARGUMENT, "set before the first step");
+    BCUDA(b, cudaSetDevice(b->device));
+    b->fused_max = max_charges;
+    b->fused_set = true;
+    return partition_batch(b);
+}
+
+int32_t lgm_kmc_batch_fused_count(const lgm_kmc_batch* b) {
+    return b ? (int32_t)b->fused.size() : 0;
 }
 
 lgm_status lgm_kmc_batch_tuning(const lgm_kmc_batch* b, int32_t* threads, int32_t* target_pairs,

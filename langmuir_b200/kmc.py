@@ -261,11 +261,13 @@ N.SIGNATURES.update({
     "lgm_kmc_batch_replica": (_vp, [_vp, _i32]),
     "lgm_kmc_batch_tuning": (_i32, [_vp, ctypes.POINTER(_i32), ctypes.POINTER(_i32),
                                     ctypes.POINTER(_i32), ctypes.POINTER(_i32)]),
+    "lgm_kmc_batch_set_fused": (_i32, [_vp, _i32]),
+    "lgm_kmc_batch_fused_count": (_i32, [_vp]),
 })
 if N._lib is not None:
     for _name in ("lgm_kmc_batch_create", "lgm_kmc_batch_destroy", "lgm_kmc_batch_last_error",
                   "lgm_kmc_batch_run", "lgm_kmc_batch_size", "lgm_kmc_batch_replica",
-                  "lgm_kmc_batch_tuning"):
+                  "lgm_kmc_batch_tuning", "lgm_kmc_batch_set_fused", "lgm_kmc_batch_fused_count"):
         _fn = getattr(N._lib, _name)
         _fn.restype, _fn.argtypes = N.SIGNATURES[_name]
 
@@ -289,7 +291,10 @@ class KMCBatch:
     """Replicas of uneven size advanced together on one GPU; replica i has the
     random stream of a single replica with id replica0 + i."""
 
-    def __init__(self, params_list, device=0, replica0=0):
+    def __init__(self, params_list, device=0, replica0=0, fused_max_charges=None):
+        """``fused_max_charges``: replicas with room for at most this many
+        charges advance by the fused one-block step (None: the library's
+        default bound, 0: none)."""
         arr = (Params * len(params_list))(*params_list)
         h = ctypes.c_void_p()
         st = N.lib().lgm_kmc_batch_create(arr, len(params_list), int(device), int(replica0),
@@ -298,6 +303,15 @@ class KMCBatch:
             raise N.LgmError(st, N.lib().lgm_kmc_batch_last_error(None).decode())
         self._h = h
         self._params = list(params_list)
+        if fused_max_charges is not None:
+            st = N.lib().lgm_kmc_batch_set_fused(self._h, int(fused_max_charges))
+            if st != N.OK:
+                raise N.LgmError(st, N.lib().lgm_kmc_batch_last_error(self._h).decode())
+
+    @property
+    def fused_count(self) -> int:
+        """Replicas on the fused step."""
+        return N.lib().lgm_kmc_batch_fused_count(self._h)
 
     def close(self):
         if getattr(self, "_h", None) and self._h.value and N._lib is not None:

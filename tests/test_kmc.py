@@ -224,15 +224,33 @@ def uneven_params(n, seed=1):
     return out
 
 
+def _capacities(params):
+    out = []
+    for p in params:
+        with L.KMC(p) as k:
+            st = k.stats()
+            out.append(st["max_electrons"] + st["max_holes"])
+    return out
+
+
 @pytest.mark.gpu
-def test_batch_matches_single_replicas():
+@pytest.mark.parametrize("form", ["fused", "per_phase", "mixed"])
+def test_batch_matches_single_replicas(form):
+    """Both step forms of the batch, alone and together in one graph, give
+    every replica the trajectory of a single replica with its id."""
     params = uneven_params(9)
     steps = 40
-    with L.KMCBatch(params, replica0=100) as b:
+    caps = _capacities(params)
+    bound = {"fused": max(caps), "per_phase": 0, "mixed": int(np.median(caps))}[form]
+    with L.KMCBatch(params, replica0=100, fused_max_charges=bound) as b:
+        n_fused = b.fused_count
+        assert n_fused == sum(c <= bound for c in caps)
         b.run(steps)
         got = [b.replica(i).carriers() for i in range(len(params))]
         stats = [b.replica(i).stats() for i in range(len(params))]
-        assert b.tuning()["items"] > 0
+        assert (b.tuning()["items"] > 0) == (n_fused < len(params))
+    if form == "mixed":
+        assert 0 < n_fused < len(params)
     for i, p in enumerate(params):
         with L.KMC(p, replica=100 + i) as g:
             g.run(steps)
@@ -244,10 +262,42 @@ def test_batch_matches_single_replicas():
 
 
 @pytest.mark.gpu
-def test_batch_replica_matches_oracle(oracle_mod):
+@pytest.mark.parametrize("case", ["solar_confined_interface", "solar_3d_gauss_confined"])
+def test_fused_batch_solar_matches_single_replicas(case):
+    """Solar-cell replicas (exciton source, recombination, confinement) with a
+    morphology each: the fused step against single replicas."""
+    keys = dict(CASES[case])
+    steps = keys.pop("steps")
+    morph = keys.pop("morphology")
+    params = []
+    for i in range(4):
+        kk = dict(keys, random_seed=20 + i)
+        params.append(make_params(**kk))
+    phases = [blob_phase(p.grid_x, p.grid_y, p.grid_z, morph + i) for i, p in enumerate(params)]
+    with L.KMCBatch(params, replica0=50) as b:
+        assert b.fused_count == len(params)
+        for i in range(len(params)):
+            b.replica(i).set_morphology(phases[i])
+        b.run(steps)
+        got = [(b.replica(i).carriers(), b.replica(i).stats()) for i in range(len(params))]
+    for i, p in enumerate(params):
+        with L.KMC(p, replica=50 + i) as g:
+            g.set_morphology(phases[i])
+            g.run(steps)
+            (e, h), s = g.carriers(), g.stats()
+        np.testing.assert_array_equal(got[i][0][0], e, err_msg=f"{case} replica {i} electrons")
+        np.testing.assert_array_equal(got[i][0][1], h, err_msg=f"{case} replica {i} holes")
+        assert got[i][1]["counters"] == s["counters"]
+        assert s["counters"][17] > 0  # excitons were generated
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("fused", [True, False])
+def test_batch_replica_matches_oracle(oracle_mod, fused):
     params = uneven_params(3, seed=5)
     steps = 25
-    with L.KMCBatch(params, replica0=7) as b:
+    with L.KMCBatch(params, replica0=7, fused_max_charges=None if fused else 0) as b:
+        assert (b.fused_count == 3) == fused
         reps = [b.replica(i) for i in range(3)]
         orcs = []
         for i, r in enumerate(reps):
