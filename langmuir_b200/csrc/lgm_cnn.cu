@@ -321,6 +321,189 @@ conv3x3_fwd(const bf16* __restrict__ x, const bf16* __restrict__ w, const float*
     }
 }
 
+// The first layer (one input channel) on a wide tile.  With 9 taps the GEMM
+// is one k16 step per 16 pixels, so the 8x16 tile of conv3x3_fwd spends its
+// time in barriers and staging; here a CTA takes 8 rows x 64 pixels per
+// iteration (4 sub-tiles of 16 per warp row pair), with one patch, one set of
+// barriers and one vectorised store of the tile.  Same arithmetic and layouts
+// as conv3x3_fwd<1>: x [B,H,W] bf16, w [COUT][16] (taps 0..8, zero padding),
+// act [B,H,W,COUT] and pooled [B,H/2,W/2,COUT], each optional.
+constexpr int C1_TX = 64;                               // tile width of the first layer
+constexpr int C1_CPAD = 2;                              // patch pixel stride (bf16)
+constexpr int C1_PATCH = (TY + 2) * (C1_TX + 2);        // patch pixels
+constexpr int C1_WSTRIDE = 16 + 8;
+constexpr int C1_OSTR = COUT + 8;
+constexpr int C1_PER = (C1_PATCH + CONV_THREADS - 1) / CONV_THREADS;
+constexpr size_t C1_SMEM_BASE =
+    ((size_t)C1_PATCH * C1_CPAD + (size_t)COUT * C1_WSTRIDE + (size_t)(TY / 2) * (C1_TX / 2) * C1_OSTR) *
+    sizeof(bf16);
+constexpr size_t C1_SMEM_ACT = (size_t)TY * C1_TX * C1_OSTR * sizeof(bf16);
+
+__global__ void __launch_bounds__(CONV_THREADS)
+conv1_fwd(const bf16* __restrict__ x, const bf16* __restrict__ w, const float* __restrict__ bias,
+          bf16* __restrict__ act, bf16* __restrict__ pooled, int B, int H, int W, int relu) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    bf16* patch = reinterpret_cast<bf16*>(smem_raw);
+    bf16* ws = patch + C1_PATCH * C1_CPAD;
+    bf16* pst = ws + COUT * C1_WSTRIDE;                   // [(TY/2)*(C1_TX/2)][C1_OSTR]
+    bf16* ost = pst + (TY / 2) * (C1_TX / 2) * C1_OSTR;   // [TY*C1_TX][C1_OSTR], if act
+    const int tiles_x = W / C1_TX, tiles_y = H / TY;
+    const int ntiles = B * tiles_x * tiles_y;
+    const int tid = threadIdx.x;
+    const int warp = tid >> 5, lane = tid & 31, g = lane >> 2, t = lane & 3;
+    const bf16 zero = __float2bfloat16(0.f);
+
+    for (int i = tid; i < COUT * 16; i += CONV_THREADS) ws[(i / 16) * C1_WSTRIDE + (i % 16)] = w[i];
+    float bv[4][2];
+#pragma unroll
+    for (int n = 0; n < 4; ++n) {
+        bv[n][0] = bias ? bias[n * 8 + 2 * t] : 0.f;
+        bv[n][1] = bias ? bias[n * 8 + 2 * t + 1] : 0.f;
+    }
+    __syncthreads();
+    // the thread's B fragments and tap offsets: columns k = 2t, 2t+1, 2t+8, 2t+9
+    // are taps (ky, kx) = (k / 3, k % 3) for k < 9, zero padding above
+    uint32_t bb[4][2];
+#pragma unroll
+    for (int n = 0; n < 4; ++n) {
+        const bf16* wr = ws + (n * 8 + g) * C1_WSTRIDE;
+        bb[n][0] = pack2(wr[2 * t], wr[2 * t + 1]);
+        bb[n][1] = pack2(wr[2 * t + 8], wr[2 * t + 9]);
+    }
+    int toff[4];
+    bool tok[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const int k = 2 * t + (j & 1) + (j >> 1) * 8;
+        tok[j] = k < 9;
+        toff[j] = tok[j] ? ((k / 3) * (C1_TX + 2) + k % 3) * C1_CPAD : 0;
+    }
+
+    unsigned short pre[C1_PER];
+    auto origin = [&](int tile, int& b, int& y0, int& x0) {
+        b = tile / (tiles_x * tiles_y);
+        const int rem = tile % (tiles_x * tiles_y);
+        y0 = (rem / tiles_x) * TY;
+        x0 = (rem % tiles_x) * C1_TX;
+    };
+    auto prefetch = [&](int tile) {
+        int b, y0, x0;
+        origin(tile, b, y0, x0);
+#pragma unroll
+        for (int k = 0; k < C1_PER; ++k) {
+            const int i = tid + k * CONV_THREADS;
+            const int px = i % (C1_TX + 2), py = i / (C1_TX + 2);
+            const int yy = y0 + py - 1, xx = x0 + px - 1;
+            const bool in = i < C1_PATCH && yy >= 0 && yy < H && xx >= 0 && xx < W;
+            pre[k] = in ? reinterpret_cast<const unsigned short*>(x)[((size_t)b * H + yy) * W + xx]
+                        : (unsigned short)0;
+        }
+    };
+    if ((int)blockIdx.x < ntiles) prefetch(blockIdx.x);
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        int b, y0, x0;
+        origin(tile, b, y0, x0);
+        __syncthreads();  // the previous tile is done with patch, ost and pst
+#pragma unroll
+        for (int k = 0; k < C1_PER; ++k) {
+            const int i = tid + k * CONV_THREADS;
+            if (i < C1_PATCH) reinterpret_cast<unsigned short*>(patch)[i * C1_CPAD] = pre[k];
+        }
+        __syncthreads();
+        if (tile + (int)gridDim.x < ntiles) prefetch(tile + gridDim.x);  // overlaps the math
+
+#pragma unroll
+        for (int sx = 0; sx < C1_TX / TX; ++sx) {
+            float acc[2][4][4];
+#pragma unroll
+            for (int i = 0; i < 2; ++i)
+#pragma unroll
+                for (int n = 0; n < 4; ++n)
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) acc[i][n][j] = 0.f;
+#pragma unroll
+            for (int i = 0; i < 2; ++i) {
+                const int row = 2 * warp + i;
+                const bf16* p0 = patch + (row * (C1_TX + 2) + sx * TX + g) * C1_CPAD;
+                const bf16* p1 = p0 + 8 * C1_CPAD;
+                bf16 v0[4], v1[4];
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    v0[j] = tok[j] ? p0[toff[j]] : zero;
+                    v1[j] = tok[j] ? p1[toff[j]] : zero;
+                }
+                uint32_t a[4];
+                a[0] = pack2(v0[0], v0[1]);
+                a[1] = pack2(v1[0], v1[1]);
+                a[2] = pack2(v0[2], v0[3]);
+                a[3] = pack2(v1[2], v1[3]);
+#pragma unroll
+                for (int n = 0; n < 4; ++n) mma16816(acc[i][n], a, bb[n]);
+            }
+            // epilogue of the sub-tile: rows g / g+8 of a fragment are pixels
+            // sx*16 + g / + 8 of tile row 2*warp + i; columns 2t, 2t+1 of n-tile
+            // n are channels n*8 + 2t, + 1
+#pragma unroll
+            for (int n = 0; n < 4; ++n) {
+                const int ch = n * 8 + 2 * t;
+                float v[2][4];
+#pragma unroll
+                for (int i = 0; i < 2; ++i) {
+                    v[i][0] = acc[i][n][0] + bv[n][0];
+                    v[i][1] = acc[i][n][1] + bv[n][1];
+                    v[i][2] = acc[i][n][2] + bv[n][0];
+                    v[i][3] = acc[i][n][3] + bv[n][1];
+                    if (relu)
+#pragma unroll
+                        for (int j = 0; j < 4; ++j) v[i][j] = fmaxf(v[i][j], 0.f);
+                    if (act) {
+                        const int r = 2 * warp + i, c = sx * TX + g;
+                        *reinterpret_cast<uint32_t*>(ost + (r * C1_TX + c) * C1_OSTR + ch) =
+                            pack2(__float2bfloat16(v[i][0]), __float2bfloat16(v[i][1]));
+                        *reinterpret_cast<uint32_t*>(ost + (r * C1_TX + c + 8) * C1_OSTR + ch) =
+                            pack2(__float2bfloat16(v[i][2]), __float2bfloat16(v[i][3]));
+                    }
+                }
+                if (pooled) {
+                    float sm[4];
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) sm[j] = v[0][j] + v[1][j];
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) sm[j] += __shfl_xor_sync(0xffffffffu, sm[j], 4);
+                    if ((g & 1) == 0) {
+                        // pooled row warp, columns sx*8 + g/2 and sx*8 + g/2 + 4
+                        const int pc = sx * (TX / 2) + g / 2;
+                        *reinterpret_cast<uint32_t*>(pst + (warp * (C1_TX / 2) + pc) * C1_OSTR + ch) =
+                            pack2(__float2bfloat16(0.25f * sm[0]), __float2bfloat16(0.25f * sm[1]));
+                        *reinterpret_cast<uint32_t*>(pst + (warp * (C1_TX / 2) + pc + 4) * C1_OSTR + ch) =
+                            pack2(__float2bfloat16(0.25f * sm[2]), __float2bfloat16(0.25f * sm[3]));
+                    }
+                }
+            }
+        }
+        __syncthreads();
+        constexpr int VO = COUT / 8;  // 16-byte vectors per output pixel
+        if (act) {
+            for (int i = tid; i < TY * C1_TX * VO; i += CONV_THREADS) {
+                const int c8 = i % VO, pix = i / VO;
+                const int r = pix / C1_TX, c = pix % C1_TX;
+                *reinterpret_cast<uint4*>(act + (((size_t)b * H + y0 + r) * W + x0 + c) * COUT + c8 * 8) =
+                    *reinterpret_cast<const uint4*>(ost + pix * C1_OSTR + c8 * 8);
+            }
+        }
+        if (pooled) {
+            const int H2 = H / 2, W2 = W / 2;
+            for (int i = tid; i < (TY / 2) * (C1_TX / 2) * VO; i += CONV_THREADS) {
+                const int c8 = i % VO, pix = i / VO;
+                const int r = pix / (C1_TX / 2), c = pix % (C1_TX / 2);
+                *reinterpret_cast<uint4*>(
+                    pooled + (((size_t)b * H2 + y0 / 2 + r) * W2 + x0 / 2 + c) * COUT + c8 * 8) =
+                    *reinterpret_cast<const uint4*>(pst + pix * C1_OSTR + c8 * 8);
+            }
+        }
+    }
+}
+
 // Weight/bias gradients.  GEMM with M = COUT (2 m16 tiles), N = KPAD,
 // K = pixels: A(n, p) = dA[p][n], B(p, k) = x_col[p][k].  A CTA walks pixel
 // tiles of 8x16 with a grid stride, keeps its partial dW in registers and
@@ -527,6 +710,25 @@ lgm_status lgm_cnn_conv3x3_fwd(int32_t cin, const void* x, const void* w, const 
         (pooled && (H % 2 || W % 2)) || (!act && !pooled))
         return LGM_ERR_INVALID_ARGUMENT;
     cudaStream_t st = (cudaStream_t)stream;
+    if (cin == 1 && W % C1_TX == 0) {
+        // the wide-tile first layer; persistent: at most the CTAs resident at once
+        const size_t smem = C1_SMEM_BASE + (act ? C1_SMEM_ACT : 0);
+        static int cap1[2] = {0, 0};
+        const int ai = act ? 1 : 0;
+        if (!cap1[ai]) {
+            int dev = 0, sms = 0, per_sm = 0;
+            cudaGetDevice(&dev);
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+            cudaFuncSetAttribute(conv1_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)(C1_SMEM_BASE + C1_SMEM_ACT));
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, conv1_fwd, CONV_THREADS, smem);
+            cap1[ai] = std::max(1, sms * std::max(1, per_sm));
+        }
+        const int ntiles1 = B * (H / TY) * (W / C1_TX);
+        conv1_fwd<<<std::min(ntiles1, cap1[ai]), CONV_THREADS, smem, st>>>(
+            (const bf16*)x, (const bf16*)w, bias, (bf16*)act, (bf16*)pooled, B, H, W, relu);
+        return launch_check();
+    }
     const int ntiles = B * (H / TY) * (W / TX);
     // persistent: at most the CTAs that fit on the device at once
     static int cap[2] = {0, 0};

@@ -271,10 +271,19 @@ def init_params(seed, device="cuda"):
     return out
 
 
-def phases_to_input(phases, device="cuda"):
-    """uint8 phases [B,H,W] (0 donor, 1 acceptor) -> bf16 [B,H,W,1] in {-1, +1}."""
+def phases_to_input(phases, device="cuda", ramp=0.0):
+    """uint8 phases [B,H,W] (0 donor, 1 acceptor) -> bf16 [B,H,W,1]: -1 donor,
+    +1 acceptor, plus ``ramp`` * (2x/(W-1) - 1) along x (the axis between the
+    electrodes).  The global pool of the network makes it blind to where a
+    feature sits; the ramp tells it how far a site is from either electrode.
+    Mirroring x and exchanging the phases maps the input to minus its mirror
+    image, ramp included, so the device symmetries stay a sign flip."""
     t = torch.as_tensor(phases, device=device)
-    return (t.to(torch.float32) * 2.0 - 1.0).to(torch.bfloat16).unsqueeze(-1).contiguous()
+    x = t.to(torch.float32) * 2.0 - 1.0
+    if ramp:
+        W = x.shape[-1]
+        x = x + ramp * torch.linspace(-1.0, 1.0, W, device=x.device)
+    return x.to(torch.bfloat16).unsqueeze(-1).contiguous()
 
 
 # ---- morphologies --------------------------------------------------------------------------
@@ -412,19 +421,21 @@ class Surrogate:
     not, such as the donor fraction (augment=False there); ``tta`` > 1
     averages predictions over that many symmetries."""
 
-    def __init__(self, members=4, seed=0, device="cuda", log_targets=True, augment=True, tta=1):
+    def __init__(self, members=4, seed=0, device="cuda", log_targets=True, augment=True, tta=1,
+                 ramp=0.0):
         self.device = device
         self.members = [init_params(seed * 1000 + m, device) for m in range(members)]
         self.mean = torch.zeros(OUTPUTS, device=device)
         self.std = torch.ones(OUTPUTS, device=device)
         self.log_targets, self.augment, self.tta = log_targets, augment, tta
+        self.ramp = float(ramp)
 
     def _encode(self, y):
         return torch.log(y.clamp_min(1e-6)) if self.log_targets else y
 
     def fit(self, phases, targets, epochs=30, batch=64, lr=2e-3, seed=0, log=None):
         """phases uint8 [n,H,W], targets float [n,2] (current, efficiency)."""
-        x = phases_to_input(phases, self.device)
+        x = phases_to_input(phases, self.device, self.ramp)
         y = self._encode(torch.as_tensor(np.asarray(targets, np.float32), device=self.device))
         self.mean = y.mean(0)
         self.std = y.std(0).clamp_min(1e-6)
@@ -461,7 +472,7 @@ class Surrogate:
         log targets the mean is the geometric mean over members and the spread
         is mean * (std of the log predictions)."""
         if x16 is None:
-            x16 = phases_to_input(phases, self.device)
+            x16 = phases_to_input(phases, self.device, self.ramp)
         n = x16.shape[0]
         views = max(1, self.tta)
         preds = torch.zeros(len(self.members), n, OUTPUTS, device=self.device)
@@ -482,12 +493,13 @@ class Surrogate:
     def state_dict(self):
         return {"members": [[p.detach().cpu() for p in ps] for ps in self.members],
                 "mean": self.mean.cpu(), "std": self.std.cpu(), "log_targets": self.log_targets,
-                "tta": self.tta}
+                "tta": self.tta, "ramp": self.ramp}
 
     def load_state_dict(self, sd):
         self.members = [[p.to(self.device).requires_grad_(True) for p in ps] for ps in sd["members"]]
         self.mean, self.std = sd["mean"].to(self.device), sd["std"].to(self.device)
         self.log_targets, self.tta = sd.get("log_targets", False), sd.get("tta", 1)
+        self.ramp = float(sd.get("ramp", 0.0))
 
 
 def screen(model, candidates, top=256, uncertainty_quantile=0.9975, batch=1024):
@@ -629,11 +641,13 @@ def main(argv=None):
     ap.add_argument("--lr", type=float, default=4e-3)
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--tta", type=int, default=1, help="symmetry views averaged per prediction")
+    ap.add_argument("--ramp", type=float, default=0.5, help="x-position ramp added to the input")
     ap.add_argument("--labels-cache", default="", help="prefix of cached training/holdout labels")
     ap.add_argument("--out", default="")
     a = ap.parse_args(argv)
     rep = run_pipeline(a.train, a.holdout, a.candidates, a.steps, a.burn_in, a.members, a.epochs,
-                       seed=a.seed, labels_cache=a.labels_cache, lr=a.lr, tta=a.tta)
+                       seed=a.seed, labels_cache=a.labels_cache, lr=a.lr, tta=a.tta,
+                       ramp=a.ramp)
     arrays = rep.pop("_arrays")
     model = rep.pop("_model")
     text = json.dumps(rep, indent=1)
