@@ -364,24 +364,24 @@ def _label_from_counters(c0, c1, steps):
     return current, eff, int(gen), int(d[_RECOMB])
 
 
-def kmc_labels(phases, steps=50000, burn_in=10000, seed=1, replica0=0, device=0, chunk=4096,
-               **setup):
-    """Current and efficiency of every morphology from the batched GPU kMC.
+LABEL_KEYS = ("current", "efficiency", "generated", "recombined")
 
-    phases: uint8 [n,H,W] (numpy or torch).  The window [burn_in, steps)
-    defines the labels (the first burn_in steps fill the device).  Returns a
-    dict of numpy arrays plus the wall time."""
-    ph = phases.cpu().numpy() if torch.is_tensor(phases) else np.asarray(phases)
-    ph = np.ascontiguousarray(ph, dtype=np.uint8)
-    n, H, W = ph.shape
-    if H != W:
-        raise ValueError("square morphologies only")
-    out = {k: np.zeros(n) for k in ("current", "efficiency", "generated", "recombined")}
-    t0 = time.perf_counter()
-    for i0 in range(0, n, chunk):
-        i1 = min(n, i0 + chunk)
+
+def shard_range(n, world, rank):
+    """Rank ``rank``'s contiguous share [lo, hi) of n morphologies (the shares
+    of a world differ in size by at most one)."""
+    return rank * n // world, (rank + 1) * n // world
+
+
+def _label_slice(ph, replica_start, steps, burn_in, seed, device, chunk, setup):
+    """Labels of the morphologies ph [m,H,W]; morphology i is replica
+    replica_start + i, so its label does not depend on how the set is split."""
+    m, H, _ = ph.shape
+    out = {k: np.zeros(m) for k in LABEL_KEYS}
+    for i0 in range(0, m, chunk):
+        i1 = min(m, i0 + chunk)
         params = [solar_label_params(size=H, seed=seed, **setup) for _ in range(i0, i1)]
-        with KMCBatch(params, device=device, replica0=replica0 + i0) as b:
+        with KMCBatch(params, device=device, replica0=replica_start + i0) as b:
             reps = [b.replica(i) for i in range(i1 - i0)]
             for i, r in enumerate(reps):
                 # the site order is x fastest: site = x + X*y, image[y][x]
@@ -391,13 +391,66 @@ def kmc_labels(phases, steps=50000, burn_in=10000, seed=1, replica0=0, device=0,
             b.run(steps - burn_in)
             c1 = [r.stats()["counters"] for r in reps]
         for i in range(i1 - i0):
-            cur, eff, gen, rec = _label_from_counters(c0[i], c1[i], steps - burn_in)
-            out["current"][i0 + i] = cur
-            out["efficiency"][i0 + i] = eff
-            out["generated"][i0 + i] = gen
-            out["recombined"][i0 + i] = rec
-    out["seconds"] = time.perf_counter() - t0
+            lab = _label_from_counters(c0[i], c1[i], steps - burn_in)
+            for k, v in zip(LABEL_KEYS, lab):
+                out[k][i0 + i] = v
     return out
+
+
+def gather_labels(local, n, group=None):
+    """Every rank's share of the labels (``local``, the arrays of its
+    shard_range) assembled into n-long arrays on every rank: one all_gather of
+    a padded [keys, ceil(n/world)] FP64 tensor (on the GPU for NCCL, on the
+    host for gloo).  The wall time is the longest rank's."""
+    import torch.distributed as dist
+    world, rank = dist.get_world_size(group), dist.get_rank(group)
+    dev = (torch.device("cuda", torch.cuda.current_device())
+           if dist.get_backend(group) == "nccl" else torch.device("cpu"))
+    cap = -(-n // world)
+    lo, hi = shard_range(n, world, rank)
+    buf = torch.zeros(len(LABEL_KEYS), cap, dtype=torch.float64, device=dev)
+    for j, k in enumerate(LABEL_KEYS):
+        buf[j, : hi - lo] = torch.as_tensor(np.asarray(local[k], np.float64))
+    parts = [torch.empty_like(buf) for _ in range(world)]
+    dist.all_gather(parts, buf, group=group)
+    t = torch.tensor([float(local.get("seconds", 0.0))], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX, group=group)
+    out = {k: np.zeros(n) for k in LABEL_KEYS}
+    for r, part in enumerate(parts):
+        a, b = shard_range(n, world, r)
+        arr = part.cpu().numpy()
+        for j, k in enumerate(LABEL_KEYS):
+            out[k][a:b] = arr[j, : b - a]
+    out["seconds"] = float(t.item())
+    return out
+
+
+def kmc_labels(phases, steps=50000, burn_in=10000, seed=1, replica0=0, device=0, chunk=4096,
+               group=None, **setup):
+    """Current and efficiency of every morphology from the batched GPU kMC.
+
+    phases: uint8 [n,H,W] (numpy or torch).  The window [burn_in, steps)
+    defines the labels (the first burn_in steps fill the device).  Returns a
+    dict of numpy arrays plus the wall time.  With a process group ``group``
+    (torch.distributed, one GPU per rank) each rank labels its shard_range of
+    the morphologies on its own GPU and the labels are gathered to every
+    rank; morphology i is replica replica0 + i either way, so the labels equal
+    the single-GPU ones."""
+    ph = phases.cpu().numpy() if torch.is_tensor(phases) else np.asarray(phases)
+    ph = np.ascontiguousarray(ph, dtype=np.uint8)
+    n, H, W = ph.shape
+    if H != W:
+        raise ValueError("square morphologies only")
+    t0 = time.perf_counter()
+    if group is None:
+        out = _label_slice(ph, replica0, steps, burn_in, seed, device, chunk, setup)
+        out["seconds"] = time.perf_counter() - t0
+        return out
+    import torch.distributed as dist
+    lo, hi = shard_range(n, dist.get_world_size(group), dist.get_rank(group))
+    local = _label_slice(ph[lo:hi], replica0 + lo, steps, burn_in, seed, device, chunk, setup)
+    local["seconds"] = time.perf_counter() - t0
+    return gather_labels(local, n, group)
 
 
 # ---- ensemble ------------------------------------------------------------------------------

@@ -39,6 +39,30 @@ def _rank(rank, world, port, legs, out):
         dist.destroy_process_group()
 
 
+def _fake_label_slice(ph, replica_start, steps, burn_in, seed, device, chunk, setup):
+    # a stand-in for the GPU labeller: each label a function of the replica id
+    ids = replica_start + np.arange(len(ph), dtype=np.float64)
+    return {"current": ids, "efficiency": 0.5 * ids, "generated": ids + 7.0,
+            "recombined": ids % 3}
+
+
+def _label_rank(rank, world, port, n, out):
+    import datetime
+    import torch.distributed as dist
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    sys.path.insert(0, ROOT)
+    from langmuir_b200 import surrogate as S
+    S._label_slice = _fake_label_slice
+    dist.init_process_group("gloo", rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=60))
+    try:
+        ph = np.zeros((n, 4, 4), np.uint8)
+        got = S.kmc_labels(ph, steps=10, burn_in=2, replica0=100, group=dist.group.WORLD)
+        out.put((rank, {k: got[k].tolist() for k in S.LABEL_KEYS}))
+    finally:
+        dist.destroy_process_group()
+
+
 def _run(world, legs):
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
@@ -95,3 +119,26 @@ def test_reference_arm_under_torchrun_prints_one_line_from_rank_0(oracle_mod):
     assert line["impl"] == "reference" and line["n_gpus"] == 2
     assert line["value"] > 0 and line["e2e"]["value"] == line["value"]
     assert line["cpu_baseline"]["kind"] in ("port", "reference")
+
+
+@pytest.mark.parametrize("n", [7, 1])
+def test_sharded_labels_equal_unsharded(n):
+    """Replica sharding of the label batch (surrogate.kmc_labels with a
+    process group): each rank labels its slice, morphology i stays replica
+    replica0 + i, and the gathered labels equal the one-GPU ones on every rank."""
+    sys.path.insert(0, ROOT)
+    from langmuir_b200 import surrogate as S
+    want = _fake_label_slice(np.zeros((n, 4, 4)), 100, 10, 2, 1, 0, 4096, {})
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_label_rank, args=(r, 2, port, n, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    got = dict(q.get(timeout=120) for _ in range(2))
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    for r in (0, 1):
+        for k in S.LABEL_KEYS:
+            np.testing.assert_array_equal(got[r][k], want[k])

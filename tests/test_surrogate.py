@@ -311,6 +311,31 @@ def test_batched_labels_equal_single_replica():
 
 
 @pytest.mark.gpu
+def test_labels_through_a_process_group_equal_plain():
+    """The sharded path of kmc_labels (labels of the rank's slice, then an
+    all_gather) on a one-rank gloo group gives the plain labels."""
+    import os
+    import socket
+    import torch.distributed as dist
+    from langmuir_b200 import surrogate as S
+    ph, _, _ = S.grf_morphologies(5, size=64, seed=8, device="cuda")
+    ph = ph.cpu().numpy()
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=0, world_size=1)
+    try:
+        got = S.kmc_labels(ph, steps=500, burn_in=100, seed=3, replica0=60, chunk=2,
+                           group=dist.group.WORLD)
+    finally:
+        dist.destroy_process_group()
+    want = S.kmc_labels(ph, steps=500, burn_in=100, seed=3, replica0=60)
+    for k in S.LABEL_KEYS:
+        np.testing.assert_array_equal(got[k], want[k])
+
+
+@pytest.mark.gpu
 def test_surrogate_gain_over_descriptor_regression():
     """What the trained network gains over the method without it: on held-out
     morphologies labelled by kMC, the CNN trained on batched-kMC labels ranks
