@@ -65,6 +65,26 @@ def test_create_validates_before_touching_a_device():
     assert N.lib().lgm_create(ctypes.byref(cfg), 0, ctypes.byref(h)) == N.ERR_UNSUPPORTED
 
 
+@pytest.mark.parametrize("dims,ok", [((418, 8, 1), True), ((419, 8, 1), False),
+                                     ((8, 836, 1), True), ((8, 837, 1), False),
+                                     ((8, 8, 835), True), ((8, 8, 836), False)])
+def test_lattice_bound_for_exact_fp32_r2(dims, ok):
+    """6 max(2X, Y, Z+1)^2 < 2^22 keeps every intermediate of the expanded r^2
+    exact in FP32 (right-image targets reach x' = 2X - 1): the largest lattices
+    pass validation (and then report the missing device here), one more site
+    along any axis is refused as unsupported."""
+    X, Y, Z = dims
+    cfg = N.default_config(grid_x=X, grid_y=Y, grid_z=Z)
+    h = ctypes.c_void_p()
+    st = N.lib().lgm_create(ctypes.byref(cfg), 0, ctypes.byref(h))
+    if ok:
+        assert st != N.ERR_UNSUPPORTED
+        if st == N.OK:
+            N.lib().lgm_destroy(h)
+    else:
+        assert st == N.ERR_UNSUPPORTED
+
+
 def test_create_without_gpu_reports_no_device():
     from tests.conftest import HAS_GPU
     if HAS_GPU:

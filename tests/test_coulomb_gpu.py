@@ -180,6 +180,31 @@ def test_colocated_and_shell(lgm, oracle_mod):
     assert o[0] == pytest.approx(orc.prefactor * (2 / 9 - 1.0), rel=1e-6)
 
 
+def test_largest_lattice_with_both_images(lgm, oracle_mod):
+    """At the largest accepted lattice (2X = Y = 836) the expanded r^2 of a pair
+    at opposite corners, and of right-image targets at x' = 2X - 1 - x, stays
+    exact: potentials at the corners match the FP64 oracle to the FP32 bound."""
+    X, Y, Z, c = 418, 836, 1, 40
+    orc = oracle_mod.Oracle(X, Y, Z, cutoff=c)
+    rng = np.random.default_rng(17)
+    corner = []
+    for x0 in (0, X - 12):
+        for y0 in (0, Y - 12):
+            for _ in range(40):
+                corner.append(orc.site(x0 + int(rng.integers(12)), y0 + int(rng.integers(12)), 0))
+    src = np.unique(np.array(corner, np.int32))
+    q = np.where(rng.random(len(src)) < 0.5, -1, 1).astype(np.int32)
+    tgt = src.copy()
+    with lgm.Coulomb(X, Y, Z, cutoff=c) as ctx:
+        got = ctx.potentials(src, q, tgt, lgm.POINT, 7)
+    want = orc.potentials(src, q, tgt, False, 7)
+    aq = np.abs(q).astype(np.int32)
+    nrm = (orc.potentials(src, aq, tgt, False, 1) - orc.potentials(src, aq, tgt, False, 2)
+           - orc.potentials(src, aq, tgt, False, 4))
+    assert np.all(np.abs(got - want) <= TOL32 * np.maximum(nrm, 1e-12) + 1e-13)
+    assert np.abs(want).max() > 0
+
+
 def test_full_lattice_of_charges(lgm, oracle_mod):
     X, Y, Z, c = 12, 10, 6, 7
     orc = oracle_mod.Oracle(X, Y, Z, cutoff=c)
