@@ -201,6 +201,13 @@ lgm_status lgm_set_variant(lgm_ctx* ctx, int32_t variant);
 int32_t lgm_variant_count(void);
 lgm_status lgm_variant_info(int32_t variant, int32_t* threads, int32_t* target_pairs,
                             int32_t* run);
+/* Variant flags.  LGM_VARIANT_WARP_SKIP: a warp owns 64 * target_pairs
+ * consecutive targets of the spatially sorted order (every call sorts its
+ * targets by lattice cell) and skips the 1/r and accumulation of a source
+ * that no pair of its targets has inside the cutoff; r^2 is still tested for
+ * every pair and the sums are unchanged. */
+#define LGM_VARIANT_WARP_SKIP 1
+lgm_status lgm_variant_flags(int32_t variant, int32_t* flags);
 
 #ifdef __cplusplus
 }

@@ -100,6 +100,7 @@ SIGNATURES = {
                                                      ctypes.c_double, _vp, _vp, ctypes.c_int32,
                                                      ctypes.c_int32, _vp, _vp]),
     "lgm_variant_count": (ctypes.c_int32, []),
+    "lgm_variant_flags": (ctypes.c_int32, [ctypes.c_int32, ctypes.POINTER(ctypes.c_int32)]),
     "lgm_variant_info": (ctypes.c_int32, [ctypes.c_int32, ctypes.POINTER(ctypes.c_int32),
                                           ctypes.POINTER(ctypes.c_int32),
                                           ctypes.POINTER(ctypes.c_int32)]),

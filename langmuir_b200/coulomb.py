@@ -116,7 +116,10 @@ class Coulomb:
         for v in range(N.lib().lgm_variant_count()):
             a, b, c = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32()
             N.lib().lgm_variant_info(v, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c))
-            out.append({"threads": a.value, "target_pairs": b.value, "run": c.value})
+            f = ctypes.c_int32()
+            N.lib().lgm_variant_flags(v, ctypes.byref(f))
+            out.append({"threads": a.value, "target_pairs": b.value, "run": c.value,
+                        "warp_skip": bool(f.value & 1)})
         return out
 
     def set_timing(self, on: bool = True):

@@ -102,12 +102,14 @@ __global__ void prep_sources(const int32_t* __restrict__ s, const int32_t* __res
 // at x' = 2X - 1 - x.  all_sites != 0: target g is lattice site g (kernel 1).
 __global__ void prep_targets(const int32_t* __restrict__ ts, int t, int t_pad, int all_sites,
                              unsigned terms, int X, int Y, int XY, int volume,
-                             float4* __restrict__ tgt, unsigned* err) {
-    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+                             const int32_t* __restrict__ perm, float4* __restrict__ tgt,
+                             unsigned* err) {
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;  // physical slot
     if (g >= t_pad) return;
     int x = 0, y = 0, z = 0;
     if (g < t) {
-        const int sg = all_sites ? g : ts[g];
+        const int tg = perm[g];                           // the target in this slot
+        const int sg = all_sites ? tg : ts[tg];
         if (sg < 0 || sg >= volume + kDrainIds) {
             atomicOr(err, DEVERR_TARGET_RANGE);
         } else {
@@ -127,9 +129,11 @@ __global__ void prep_targets(const int32_t* __restrict__ ts, int t, int t_pad, i
     }
 }
 
-// out[g] = prefactor * (sum over splits of the direct block - image blocks).
+// out[perm[g]] = prefactor * (sum over splits of the direct block - image
+// blocks) of physical slot g.
 __global__ void finalize(const double* __restrict__ part, int splits, int t_phys, int t,
-                         int t_pad, int nterms, double prefactor, double* __restrict__ out) {
+                         int t_pad, int nterms, double prefactor,
+                         const int32_t* __restrict__ perm, double* __restrict__ out) {
     const int g = blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= t) return;
     double total = 0.0;
@@ -139,7 +143,68 @@ __global__ void finalize(const double* __restrict__ part, int splits, int t_phys
         for (int sp = 0; sp < splits; ++sp) s += p[(size_t)sp * t_phys];
         total = (slot == 0) ? s : total - s;
     }
-    out[g] = prefactor * total;
+    out[perm[g]] = prefactor * total;
+}
+
+// Counting sort of the targets by lattice cell (the spatial order the SKIP
+// pair tiles run in).  target_bins: the bin of every target -- the Morton
+// rank of its cell, sites beyond the lattice (drains, or ids the prep flags
+// as out of range) in the last bin -- and the bin counts.
+__global__ void target_bins(const int32_t* __restrict__ ts, int t, int all_sites, int X, int Y,
+                            int XY, int volume, int shift, int cells_x, int cells_y,
+                            const int32_t* __restrict__ cell_rank, int ncells,
+                            int32_t* __restrict__ key, int32_t* __restrict__ bins) {
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= t) return;
+    const int sg = all_sites ? g : ts[g];
+    int b = ncells;
+    if (sg >= 0 && sg < volume) {
+        const int z = sg / XY, y = sg / X - z * Y, x = sg % X;
+        b = cell_rank[(x >> shift) + cells_x * ((y >> shift) + cells_y * (z >> shift))];
+    }
+    key[g] = b;
+    atomicAdd(&bins[b], 1);
+}
+
+// Exclusive scan of nb bin counts in place, one block of kScanThreads.
+constexpr int kScanThreads = 1024;
+__global__ void __launch_bounds__(kScanThreads) bins_scan(int32_t* __restrict__ bins, int nb) {
+    __shared__ int32_t warp_tot[kScanThreads / 32];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int per = (nb + kScanThreads - 1) / kScanThreads;
+    const int lo = min(nb, tid * per), hi = min(nb, lo + per);
+    int32_t sum = 0;
+    for (int i = lo; i < hi; ++i) sum += bins[i];
+    int32_t incl = sum;  // inclusive scan of the thread sums: warps, then warp totals
+    for (int o = 1; o < 32; o <<= 1) {
+        const int32_t v = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += v;
+    }
+    if (lane == 31) warp_tot[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+        int32_t w = lane < kScanThreads / 32 ? warp_tot[lane] : 0;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int32_t v = __shfl_up_sync(0xffffffffu, w, o);
+            if (lane >= o) w += v;
+        }
+        if (lane < kScanThreads / 32) warp_tot[lane] = w;
+    }
+    __syncthreads();
+    int32_t run = incl - sum + (warp > 0 ? warp_tot[warp - 1] : 0);
+    for (int i = lo; i < hi; ++i) {
+        const int32_t c = bins[i];
+        bins[i] = run;
+        run += c;
+    }
+}
+
+// perm[slot] = target: each target takes the next slot of its bin.
+__global__ void target_scatter(const int32_t* __restrict__ key, int t, int32_t* __restrict__ bins,
+                               int32_t* __restrict__ perm) {
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= t) return;
+    perm[atomicAdd(&bins[key[g]], 1)] = g;
 }
 
 __global__ void fill_zero(double* out, int t) {
@@ -199,24 +264,29 @@ using PairFn = void (*)(PairArgs);
 
 // Compiled tile variants of the pair kernel: threads per CTA, target pairs per
 // thread, FP32 run length.  fn[0] point/rsqrt, fn[1] gauss/rsqrt, fn[2] table.
+// skip: warp-owned spatially sorted targets with the per-source warp vote
+// (the rsqrt paths; the table path runs the plain tile).
 struct Variant {
-    int nt, rp, sub;
+    int nt, rp, sub, skip;
     PairFn fn[3];
 };
-#define LGM_VARIANT(NT, RP, SUB)                                                  \
-    Variant {                                                                     \
-        NT, RP, SUB, {                                                            \
-            &pair_kernel<0, 0, NT, RP, SUB>, &pair_kernel<1, 0, NT, RP, SUB>,     \
-                &pair_kernel<0, 1, NT, RP, SUB>                                   \
-        }                                                                         \
+#define LGM_VARIANT_S(NT, RP, SUB, SK)                                                    \
+    Variant {                                                                             \
+        NT, RP, SUB, SK, {                                                                \
+            &pair_kernel<0, 0, NT, RP, SUB, false, SK>,                                   \
+                &pair_kernel<1, 0, NT, RP, SUB, false, SK>, &pair_kernel<0, 1, NT, RP, SUB> \
+        }                                                                                 \
     }
+#define LGM_VARIANT(NT, RP, SUB) LGM_VARIANT_S(NT, RP, SUB, false)
+#define LGM_VARIANT_SKIP(NT, RP, SUB) LGM_VARIANT_S(NT, RP, SUB, true)
 const Variant kVariants[] = {
-    LGM_VARIANT(128, 4, 16), LGM_VARIANT(128, 4, 8),  LGM_VARIANT(128, 2, 16),
-    LGM_VARIANT(128, 8, 16), LGM_VARIANT(256, 4, 16), LGM_VARIANT(64, 4, 16),
-    LGM_VARIANT(128, 4, 32), LGM_VARIANT(256, 2, 16),
+    LGM_VARIANT(128, 4, 16),       LGM_VARIANT(128, 4, 8),        LGM_VARIANT(128, 2, 16),
+    LGM_VARIANT(128, 8, 16),       LGM_VARIANT(256, 4, 16),       LGM_VARIANT(64, 4, 16),
+    LGM_VARIANT(128, 4, 32),       LGM_VARIANT(256, 2, 16),       LGM_VARIANT_SKIP(128, 4, 32),
+    LGM_VARIANT_SKIP(128, 4, 16),  LGM_VARIANT_SKIP(128, 2, 32),  LGM_VARIANT_SKIP(64, 4, 32),
 };
 constexpr int kNumVariants = (int)(sizeof(kVariants) / sizeof(kVariants[0]));
-constexpr int kDefaultVariant = 0;
+constexpr int kDefaultVariant = 8;  // skip, 128 threads, 4 target pairs, runs of 32
 
 int fn_index(int kind, int path) {
     if (path == LGM_PATH_TABLE) return 2;
@@ -261,9 +331,20 @@ lgm_status prep(lgm_ctx* c, unsigned terms, const int32_t* d_src, const int32_t*
                                                           cf.grid_y, c->xy, c->volume, c->d_geo,
                                                           c->d_qq, c->d_err);
     LGM_CUDA(c, cudaGetLastError());
+    // targets in spatial order: bins, scan, scatter
+    if ((s = grow_device(c, &c->d_key, &c->key_cap, (size_t)t)) != LGM_OK) return s;
+    if ((s = grow_device(c, &c->d_perm, &c->perm_cap, (size_t)t)) != LGM_OK) return s;
+    LGM_CUDA(c, cudaMemsetAsync(c->d_bins, 0, sizeof(int32_t) * (c->ncells + 1), st));
+    const int tb = (t + 255) / 256;
+    target_bins<<<tb, 256, 0, st>>>(d_tgt_site, t, all_sites, cf.grid_x, cf.grid_y, c->xy,
+                                    c->volume, c->cell_shift, c->cells_x, c->cells_y,
+                                    c->d_cell_rank, c->ncells, c->d_key, c->d_bins);
+    bins_scan<<<1, kScanThreads, 0, st>>>(c->d_bins, c->ncells + 1);
+    target_scatter<<<tb, 256, 0, st>>>(c->d_key, t, c->d_bins, c->d_perm);
+    LGM_CUDA(c, cudaGetLastError());
     prep_targets<<<(sh.t_pad + 255) / 256, 256, 0, st>>>(d_tgt_site, t, sh.t_pad, all_sites, terms,
                                                           cf.grid_x, cf.grid_y, c->xy, c->volume,
-                                                          c->d_tgt, c->d_err);
+                                                          c->d_perm, c->d_tgt, c->d_err);
     LGM_CUDA(c, cudaGetLastError());
     return LGM_OK;
 }
@@ -365,11 +446,11 @@ lgm_status launch_potentials(lgm_ctx* c, int kind, unsigned terms, const int32_t
         c->timed_pending = true;
     }
     finalize<<<(t + 255) / 256, 256, 0, st>>>(c->d_part, splits, sh.t_phys, t, sh.t_pad, sh.nterms,
-                                               cf.electrostatic_prefactor, d_out);
+                                               cf.electrostatic_prefactor, c->d_perm, d_out);
     LGM_CUDA(c, cudaGetLastError());
     c->last.pairs_tested = (int64_t)sh.nterms * t * (int64_t)n;
     c->last.splits = splits;
-    c->last.kernel_launches = 4;
+    c->last.kernel_launches = 7;  // bins, scan, scatter, two preps, pair, finalize
     return LGM_OK;
 }
 
@@ -593,6 +674,39 @@ lgm_status lgm_create(const lgm_config* cfg, int32_t device, lgm_ctx** out) {
                             cudaMemcpyHostToDevice)) != cudaSuccess)
             return bail("cudaMemcpy", e);
     }
+    // Lattice cells for the spatial target order: cubes of 2^shift sites,
+    // at most 65536 cells, ranked in Morton (Z-order) of their coordinates.
+    {
+        int sh = 2;
+        auto cells = [&](int d) { return (d + (1 << sh) - 1) >> sh; };
+        while ((long long)cells(cf.grid_x) * cells(cf.grid_y) * cells(cf.grid_z) > 65536) ++sh;
+        c->cell_shift = sh;
+        c->cells_x = cells(cf.grid_x);
+        c->cells_y = cells(cf.grid_y);
+        const int cz = cells(cf.grid_z);
+        c->ncells = c->cells_x * c->cells_y * cz;
+        auto spread = [](uint64_t v) {  // bit i of v to bit 3i
+            uint64_t r = 0;
+            for (int i = 0; i < 21; ++i) r |= ((v >> i) & 1ull) << (3 * i);
+            return r;
+        };
+        std::vector<std::pair<uint64_t, int>> code(c->ncells);
+        for (int z = 0; z < cz; ++z)
+            for (int y = 0; y < c->cells_y; ++y)
+                for (int x = 0; x < c->cells_x; ++x) {
+                    const int cell = x + c->cells_x * (y + c->cells_y * z);
+                    code[cell] = {spread(x) | (spread(y) << 1) | (spread(z) << 2), cell};
+                }
+        std::sort(code.begin(), code.end());
+        std::vector<int32_t> rank(c->ncells);
+        for (int r = 0; r < c->ncells; ++r) rank[code[r].second] = r;
+        if ((e = cudaMalloc(&c->d_cell_rank, sizeof(int32_t) * rank.size())) != cudaSuccess ||
+            (e = cudaMalloc(&c->d_bins, sizeof(int32_t) * (rank.size() + 2))) != cudaSuccess)
+            return bail("cudaMalloc", e);
+        if ((e = cudaMemcpy(c->d_cell_rank, rank.data(), sizeof(int32_t) * rank.size(),
+                            cudaMemcpyHostToDevice)) != cudaSuccess)
+            return bail("cudaMemcpy", e);
+    }
     // Shared memory above the 48 KB default for large cutoffs, and the
     // resident CTAs per SM of every variant (the split count fills one wave).
     {
@@ -628,7 +742,8 @@ lgm_status lgm_destroy(lgm_ctx* c) {
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
     void* dev_ptrs[] = {c->d_geo, c->d_qq, c->d_tgt, c->d_part, c->d_s, c->d_q,
-                        c->d_t, c->d_o, c->d_gtab, c->d_rtab, c->d_err};
+                        c->d_t, c->d_o, c->d_gtab, c->d_rtab, c->d_err, c->d_cell_rank,
+                        c->d_bins, c->d_key, c->d_perm};
     for (void* p : dev_ptrs)
         if (p) cudaFree(p);
     void* host_ptrs[] = {c->h_s, c->h_q, c->h_t, c->h_o, c->h_err};
@@ -678,6 +793,12 @@ lgm_status lgm_variant_info(int32_t v, int32_t* threads, int32_t* target_pairs, 
     if (threads) *threads = kVariants[v].nt;
     if (target_pairs) *target_pairs = kVariants[v].rp;
     if (run) *run = kVariants[v].sub;
+    return LGM_OK;
+}
+
+lgm_status lgm_variant_flags(int32_t v, int32_t* flags) {
+    if (v < 0 || v >= kNumVariants || !flags) return LGM_ERR_INVALID_ARGUMENT;
+    *flags = kVariants[v].skip ? LGM_VARIANT_WARP_SKIP : 0;
     return LGM_OK;
 }
 

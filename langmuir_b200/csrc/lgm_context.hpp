@@ -30,6 +30,15 @@ struct lgm_ctx {
     float* d_rtab = nullptr;  int rtab_k = 0;       // 1/sqrt(k) table
     unsigned* d_err = nullptr;                       // device error word
 
+    // Spatial order of the targets: a target's bin is the Morton rank of its
+    // lattice cell (cubes of 2^cell_shift sites); a counting sort by bin gives
+    // the permutation the pair tiles run in (perm[physical] = target).
+    int cell_shift = 2, cells_x = 0, cells_y = 0, ncells = 0;
+    int32_t* d_cell_rank = nullptr;                  // [ncells]
+    int32_t* d_bins = nullptr;                       // [ncells + 2] counts, then offsets
+    int32_t* d_key = nullptr;  size_t key_cap = 0;   // bin per target
+    int32_t* d_perm = nullptr; size_t perm_cap = 0;  // target of each physical slot
+
     // Pinned host staging for the host-buffer entry points.
     int32_t* h_s = nullptr;   size_t hs_cap = 0;
     int32_t* h_q = nullptr;   size_t hq_cap = 0;
@@ -37,7 +46,7 @@ struct lgm_ctx {
     double* h_o = nullptr;    size_t ho_cap = 0;
     unsigned* h_err = nullptr;
 
-    int bps[16][3] = {};                 // resident CTAs per SM, per variant and kernel
+    int bps[24][3] = {};                 // resident CTAs per SM, per variant and kernel
     int forced_variant = -1;             // -1: autotuned / default
     std::map<uint64_t, int> tune_cache;  // size bucket -> fastest variant
 

@@ -24,6 +24,13 @@
 // Sources are staged through shared memory in chunks of CH by bulk TMA copies
 // (cp.async.bulk, no multicast) on two mbarrier-tracked stages; all threads
 // read each source by broadcast.
+//
+// SKIP tiles run on targets in spatial order (the host sorts them by lattice
+// cell): a warp owns 64*RP consecutive targets, which lie close together.
+// Every pair's r^2 is still computed and tested; when no pair of the warp's
+// targets with a source is inside the cutoff, the warp skips that source's
+// rsqrt and accumulation (a warp vote).  Skipped pairs would have added
+// nothing, so the sums are bit for bit those of the plain tile.
 #pragma once
 
 #include "lgm_device.cuh"
@@ -66,8 +73,9 @@ inline size_t pair_smem_bytes(int tab_k) {
 // for every integer r^2 = k (entries 0 and c^2 are 0).  NT threads, RP target
 // pairs per thread, SUB sources per FP32 run (SUB divides CH).
 // One CTA's work: target tile `tile`, source split `split` of A.splits.
-template <int KIND, int PATH, int NT, int RP, int SUB, bool NORM>
+template <int KIND, int PATH, int NT, int RP, int SUB, bool NORM, bool SKIP = false>
 __device__ __forceinline__ void pair_tile(PairArgs A, const int tile, const int split) {
+    static_assert(!SKIP || PATH == 0, "the warp skip serves the rsqrt path");
     static_assert(CH % SUB == 0, "SUB must divide CH");
     if (A.dyn) {
         A.n_chunks = A.dyn[0];
@@ -108,14 +116,17 @@ __device__ __forceinline__ void pair_tile(PairArgs A, const int tile, const int 
         if (nck > 1) issue(1);
     }
 
-    // Targets of this thread: p = base + tid + k*NT, k = 0 .. 2*RP-1; pair k
-    // packs targets 2k and 2k+1.
+    // Targets of this thread: p = base + tid + k*NT, k = 0 .. 2*RP-1 (SKIP:
+    // p = base + warp*64*RP + k*32 + lane); pair k packs targets 2k and 2k+1.
     const int base = tile * (NT * 2 * RP);
+    auto target_of = [&](int k) {
+        return SKIP ? base + (tid >> 5) * (64 * RP) + k * 32 + (tid & 31) : base + tid + k * NT;
+    };
     float2 tx[RP], ty[RP], tz[RP], tt[RP];
 #pragma unroll
     for (int k = 0; k < RP; ++k) {
-        const int p0 = base + tid + (2 * k) * NT;
-        const int p1 = p0 + NT;
+        const int p0 = target_of(2 * k);
+        const int p1 = target_of(2 * k + 1);
         const float4 a = p0 < A.t_phys ? A.tgt[p0] : make_float4(0.f, 0.f, 0.f, 0.f);
         const float4 b = p1 < A.t_phys ? A.tgt[p1] : make_float4(0.f, 0.f, 0.f, 0.f);
         tx[k] = f2(a.x, b.x); ty[k] = f2(a.y, b.y); tz[k] = f2(a.z, b.z); tt[k] = f2(a.w, b.w);
@@ -149,9 +160,41 @@ __device__ __forceinline__ void pair_tile(PairArgs A, const int tile, const int 
                 const int j = j0 + jj;
                 const float4 g0 = sg[2 * j];
                 const float4 g1 = sg[2 * j + 1];
-                const float qs = sq[j].x;
                 const float2 av = f2(g0.x, g0.y), bv = f2(g0.z, g0.w);
                 const float2 cv = f2(g1.x, g1.y), dv = f2(g1.z, g1.w);
+                if constexpr (SKIP) {
+                    float2 uu[RP];
+                    unsigned m = 0xffffffffu;
+#pragma unroll
+                    for (int k = 0; k < RP; ++k) {
+                        uu[k] = __fadd2_rn(dv, tt[k]);
+                        uu[k] = __ffma2_rn(tx[k], av, uu[k]);
+                        uu[k] = __ffma2_rn(ty[k], bv, uu[k]);
+                        uu[k] = __ffma2_rn(tz[k], cv, uu[k]);  // r^2 - 1/2, exact
+                        m = min(m, min(__float_as_uint(uu[k].x), __float_as_uint(uu[k].y)));
+                    }
+                    if (__any_sync(0xffffffffu, m < ulim)) {
+                        const float qs = sq[j].x;
+#pragma unroll
+                        for (int k = 0; k < RP; ++k) {
+                            const float2 r2 = __fadd2_rn(uu[k], half2);
+                            float wx = rsqrt_mufu(r2.x);
+                            float wy = rsqrt_mufu(r2.y);
+                            if (KIND == 1) {
+                                const int ix =
+                                    min(__float_as_int(r2.x + 8388608.f) & 0x7fffff, A.tab_k);
+                                const int iy =
+                                    min(__float_as_int(r2.y + 8388608.f) & 0x7fffff, A.tab_k);
+                                wx = fminf(s_tab[ix], wx);
+                                wy = fminf(s_tab[iy], wy);
+                            }
+                            fma_if_below(acc[2 * k], qs, wx, __float_as_uint(uu[k].x), ulim);
+                            fma_if_below(acc[2 * k + 1], qs, wy, __float_as_uint(uu[k].y), ulim);
+                        }
+                    }
+                    continue;
+                }
+                const float qs = sq[j].x;
 #pragma unroll
                 for (int k = 0; k < RP; ++k) {
                     float2 u = __fadd2_rn(dv, tt[k]);
@@ -216,7 +259,7 @@ __device__ __forceinline__ void pair_tile(PairArgs A, const int tile, const int 
     double* out = A.part + (size_t)split * A.t_phys;
 #pragma unroll
     for (int k = 0; k < 2 * RP; ++k) {
-        const int p = base + tid + k * NT;
+        const int p = target_of(k);
         if (p < A.t_phys) {
             out[p] = acc64[k];
             if (NORM) A.part_norm[(size_t)split * A.t_phys + p] = nrm[NORM ? k : 0];
@@ -225,9 +268,9 @@ __device__ __forceinline__ void pair_tile(PairArgs A, const int tile, const int 
 }
 
 // Grid form: blockIdx.x = target tile, blockIdx.y = source split.
-template <int KIND, int PATH, int NT, int RP, int SUB, bool NORM = false>
+template <int KIND, int PATH, int NT, int RP, int SUB, bool NORM = false, bool SKIP = false>
 __global__ void __launch_bounds__(NT) pair_kernel(PairArgs A) {
-    pair_tile<KIND, PATH, NT, RP, SUB, NORM>(A, blockIdx.x, blockIdx.y);
+    pair_tile<KIND, PATH, NT, RP, SUB, NORM, SKIP>(A, blockIdx.x, blockIdx.y);
 }
 
 // Work-item form for many independent problems in one launch (batched

@@ -110,3 +110,10 @@ def test_variant_table():
         assert N.lib().lgm_variant_info(v, C.byref(a), C.byref(b), C.byref(c)) == N.OK
         assert a.value % 32 == 0 and b.value >= 1 and 128 % c.value == 0
     assert N.lib().lgm_variant_info(n, None, None, None) == N.ERR_INVALID_ARGUMENT
+    f = C.c_int32()
+    flags = []
+    for v in range(n):
+        assert N.lib().lgm_variant_flags(v, C.byref(f)) == N.OK
+        flags.append(f.value)
+    assert 0 in flags and 1 in flags  # plain and warp-skip tiles both present
+    assert N.lib().lgm_variant_flags(n, C.byref(f)) == N.ERR_INVALID_ARGUMENT
