@@ -169,34 +169,7 @@ __global__ void target_bins(const int32_t* __restrict__ ts, int t, int all_sites
 // Exclusive scan of nb bin counts in place, one block of kScanThreads.
 constexpr int kScanThreads = 1024;
 __global__ void __launch_bounds__(kScanThreads) bins_scan(int32_t* __restrict__ bins, int nb) {
-    __shared__ int32_t warp_tot[kScanThreads / 32];
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int per = (nb + kScanThreads - 1) / kScanThreads;
-    const int lo = min(nb, tid * per), hi = min(nb, lo + per);
-    int32_t sum = 0;
-    for (int i = lo; i < hi; ++i) sum += bins[i];
-    int32_t incl = sum;  // inclusive scan of the thread sums: warps, then warp totals
-    for (int o = 1; o < 32; o <<= 1) {
-        const int32_t v = __shfl_up_sync(0xffffffffu, incl, o);
-        if (lane >= o) incl += v;
-    }
-    if (lane == 31) warp_tot[warp] = incl;
-    __syncthreads();
-    if (warp == 0) {
-        int32_t w = lane < kScanThreads / 32 ? warp_tot[lane] : 0;
-        for (int o = 1; o < 32; o <<= 1) {
-            const int32_t v = __shfl_up_sync(0xffffffffu, w, o);
-            if (lane >= o) w += v;
-        }
-        if (lane < kScanThreads / 32) warp_tot[lane] = w;
-    }
-    __syncthreads();
-    int32_t run = incl - sum + (warp > 0 ? warp_tot[warp - 1] : 0);
-    for (int i = lo; i < hi; ++i) {
-        const int32_t c = bins[i];
-        bins[i] = run;
-        run += c;
-    }
+    block_exclusive_scan(bins, nb);
 }
 
 // perm[slot] = target: each target takes the next slot of its bin.
@@ -674,32 +647,11 @@ lgm_status lgm_create(const lgm_config* cfg, int32_t device, lgm_ctx** out) {
                             cudaMemcpyHostToDevice)) != cudaSuccess)
             return bail("cudaMemcpy", e);
     }
-    // Lattice cells for the spatial target order: cubes of 2^shift sites,
-    // at most 65536 cells, ranked in Morton (Z-order) of their coordinates.
+    // Lattice cells for the spatial target order (Morton rank per cell).
     {
-        int sh = 2;
-        auto cells = [&](int d) { return (d + (1 << sh) - 1) >> sh; };
-        while ((long long)cells(cf.grid_x) * cells(cf.grid_y) * cells(cf.grid_z) > 65536) ++sh;
-        c->cell_shift = sh;
-        c->cells_x = cells(cf.grid_x);
-        c->cells_y = cells(cf.grid_y);
-        const int cz = cells(cf.grid_z);
-        c->ncells = c->cells_x * c->cells_y * cz;
-        auto spread = [](uint64_t v) {  // bit i of v to bit 3i
-            uint64_t r = 0;
-            for (int i = 0; i < 21; ++i) r |= ((v >> i) & 1ull) << (3 * i);
-            return r;
-        };
-        std::vector<std::pair<uint64_t, int>> code(c->ncells);
-        for (int z = 0; z < cz; ++z)
-            for (int y = 0; y < c->cells_y; ++y)
-                for (int x = 0; x < c->cells_x; ++x) {
-                    const int cell = x + c->cells_x * (y + c->cells_y * z);
-                    code[cell] = {spread(x) | (spread(y) << 1) | (spread(z) << 2), cell};
-                }
-        std::sort(code.begin(), code.end());
-        std::vector<int32_t> rank(c->ncells);
-        for (int r = 0; r < c->ncells; ++r) rank[code[r].second] = r;
+        const std::vector<int32_t> rank =
+            cell_ranks(cf.grid_x, cf.grid_y, cf.grid_z, &c->cell_shift, &c->cells_x, &c->cells_y);
+        c->ncells = (int)rank.size();
         if ((e = cudaMalloc(&c->d_cell_rank, sizeof(int32_t) * rank.size())) != cudaSuccess ||
             (e = cudaMalloc(&c->d_bins, sizeof(int32_t) * (rank.size() + 2))) != cudaSuccess)
             return bail("cudaMalloc", e);

@@ -92,6 +92,13 @@ struct Dev {
     double* w64;          // FP64 w(k) for integer r^2 = k < cutoff^2 (w(0) = 0), the guard's table
     const float* gtab;    // Gaussian charges: the pair kernel's FP32 erf(f r)/r table
     int gtab_k;           // its last index (NaN there: past it the term is 1/r)
+    // Targets in lattice-cell order for the skip pair tiles (sorted != 0): a
+    // counting sort by the Morton rank of each target's cell; tperm[slot] is
+    // the target in physical slot `slot`.
+    int sorted, cell_shift, cells_x, cells_y, ncells;
+    const int32_t* cell_rank;  // [ncells]
+    int32_t* bins;             // [ncells + 2]
+    int32_t *tkey, *tperm;     // [2 ncap]
     int splits;
     int src_cap;   // source records capacity (multiple of CH)
     int tpad_cap;  // per-term target block capacity
@@ -226,10 +233,11 @@ __device__ __forceinline__ void pack_body(const Dev& D, const int j) {
     }
     if (j < tpad) {
         int s = -1;
-        if (j < ne) s = D.e_site[j];
-        else if (j < ne + nh) s = D.h_site[j - ne];
-        else if (j < 2 * ne + nh) s = D.e_f[j - ne - nh];
-        else if (j < t) s = D.h_f[j - 2 * ne - nh];
+        const int g = (D.sorted && j < t) ? D.tperm[j] : j;  // the target in slot j
+        if (g < ne) s = D.e_site[g];
+        else if (g < ne + nh) s = D.h_site[g - ne];
+        else if (g < 2 * ne + nh) s = D.e_f[g - ne - nh];
+        else if (g < t) s = D.h_f[g - 2 * ne - nh];
         int x = 0, y = 0, z = 0;
         if (s >= 0) xyz(D, s, x, y, z);  // drain ids decode beyond the lattice: unused
         int slot = 0;
@@ -258,8 +266,39 @@ __device__ __forceinline__ void finalize_body(const Dev& D, const int g) {
         v = slot == 0 ? s : v - s;
         n += m;
     }
-    D.Vt[g] = D.prefactor * v;
-    D.Nt[g] = D.prefactor * n;
+    const int target = D.sorted ? D.tperm[g] : g;  // g is a physical slot
+    D.Vt[target] = D.prefactor * v;
+    D.Nt[target] = D.prefactor * n;
+}
+
+// The counting sort of the step's targets (current sites of electrons and
+// holes, then their proposed sites, as pack_body lists them) by the Morton
+// rank of their lattice cell; proposed drains go to the last bin.
+__device__ __forceinline__ void tbins_zero_body(const Dev& D, const int i) {
+    if (i <= D.ncells) D.bins[i] = 0;
+}
+__device__ __forceinline__ void tbins_body(const Dev& D, const int g) {
+    const int ne = D.cnt[I_NE], nh = D.cnt[I_NH];
+    if (g >= 2 * (ne + nh)) return;
+    int s;
+    if (g < ne) s = D.e_site[g];
+    else if (g < ne + nh) s = D.h_site[g - ne];
+    else if (g < 2 * ne + nh) s = D.e_f[g - ne - nh];
+    else s = D.h_f[g - 2 * ne - nh];
+    int b = D.ncells;
+    if (s >= 0 && s < D.V) {
+        int x, y, z;
+        xyz(D, s, x, y, z);
+        const int sh = D.cell_shift;
+        b = D.cell_rank[(x >> sh) + D.cells_x * ((y >> sh) + D.cells_y * (z >> sh))];
+    }
+    D.tkey[g] = b;
+    atomicAdd(&D.bins[b], 1);
+}
+__device__ __forceinline__ void tscatter_body(const Dev& D, const int g) {
+    const int ne = D.cnt[I_NE], nh = D.cnt[I_NH];
+    if (g >= 2 * (ne + nh)) return;
+    D.tperm[atomicAdd(&D.bins[D.tkey[g]], 1)] = g;
 }
 
 // ChargeAgent::bindingPotential (chargeagent.cpp:463-481)
@@ -639,6 +678,10 @@ __global__ void k_choose(Dev D) { choose_body(D, LGM_THREAD_INDEX); }
 __global__ void k_pack(Dev D) { pack_body(D, LGM_THREAD_INDEX); }
 __global__ void k_finalize(Dev D) { finalize_body(D, LGM_THREAD_INDEX); }
 __global__ void k_decide(Dev D) { decide_body(D, LGM_THREAD_INDEX); }
+__global__ void k_tbins_zero(Dev D) { tbins_zero_body(D, LGM_THREAD_INDEX); }
+__global__ void k_tbins(Dev D) { tbins_body(D, LGM_THREAD_INDEX); }
+__global__ void __launch_bounds__(1024) k_tbins_scan(Dev D) { block_exclusive_scan(D.bins, D.ncells + 1); }
+__global__ void k_tscatter(Dev D) { tscatter_body(D, LGM_THREAD_INDEX); }
 __global__ void __launch_bounds__(kGuardThreads) k_guard(Dev D) {
     __shared__ double2 red[kGuardThreads];
     guard_body(D, blockIdx.x, gridDim.x, red);
@@ -672,6 +715,14 @@ __global__ void kb_choose(const Dev* R, const int4* map) { LGM_BATCH_LOOP(choose
 __global__ void kb_pack(const Dev* R, const int4* map) { LGM_BATCH_LOOP(pack_body(D, i)) }
 __global__ void kb_finalize(const Dev* R, const int4* map) { LGM_BATCH_LOOP(finalize_body(D, i)) }
 __global__ void kb_decide(const Dev* R, const int4* map) { LGM_BATCH_LOOP(decide_body(D, i)) }
+__global__ void kb_tbins_zero(const Dev* R, const int4* map) { LGM_BATCH_LOOP(tbins_zero_body(D, i)) }
+__global__ void kb_tbins(const Dev* R, const int4* map) { LGM_BATCH_LOOP(tbins_body(D, i)) }
+__global__ void kb_tscatter(const Dev* R, const int4* map) { LGM_BATCH_LOOP(tscatter_body(D, i)) }
+// one block per replica of the list
+__global__ void __launch_bounds__(1024) kb_tbins_scan(const Dev* R, const int* list) {
+    const Dev& D = R[list[blockIdx.x]];
+    block_exclusive_scan(D.bins, D.ncells + 1);
+}
 __global__ void __launch_bounds__(kGuardThreads) kb_guard(const Dev* R, const int4* map) {
     __shared__ double2 red[kGuardThreads];
     const int4 m = map[blockIdx.x];
@@ -1166,7 +1217,10 @@ lgm_status upload_carriers(lgm_kmc* k, const int32_t* e, int ne, const int32_t* 
 
 using KPairFn = void (*)(PairArgs);
 
-KPairFn kmc_pair(int gauss) {
+KPairFn kmc_pair(int gauss, int sorted = 1) {
+    if (sorted)
+        return gauss ? &pair_kernel<1, 0, kNT, kRP, kSUB, true, true>
+                     : &pair_kernel<0, 0, kNT, kRP, kSUB, true, true>;
     return gauss ? &pair_kernel<1, 0, kNT, kRP, kSUB, true> : &pair_kernel<0, 0, kNT, kRP, kSUB, true>;
 }
 
@@ -1178,6 +1232,12 @@ lgm_status enqueue_step(lgm_kmc* k) {
     const int blk = 256;
     k_choose<<<(nc + blk - 1) / blk, blk, 0, st>>>(D);
     if (D.coulomb) {
+        if (D.sorted) {
+            k_tbins_zero<<<(D.ncells + 1 + blk - 1) / blk, blk, 0, st>>>(D);
+            k_tbins<<<(2 * nc + blk - 1) / blk, blk, 0, st>>>(D);
+            k_tbins_scan<<<1, 1024, 0, st>>>(D);
+            k_tscatter<<<(2 * nc + blk - 1) / blk, blk, 0, st>>>(D);
+        }
         const int npack = std::max(D.src_cap, D.tpad_cap);
         k_pack<<<(npack + blk - 1) / blk, blk, 0, st>>>(D);
         PairArgs A;
@@ -1185,7 +1245,8 @@ lgm_status enqueue_step(lgm_kmc* k) {
         A.part_norm = D.part_norm;
         A.c2 = (float)D.cutoff2; A.tab = k->gtab; A.tab_k = D.gauss ? k->gtab_k : 0;
         A.err = D.err; A.dyn = D.cnt + I_NCHUNK;  // dyn[0] = n_chunks, dyn[1] = t_phys
-        kmc_pair(D.gauss)<<<dim3(k->pair_tiles, D.splits), kNT, pair_smem_bytes(A.tab_k), st>>>(A);
+        kmc_pair(D.gauss, D.sorted)<<<dim3(k->pair_tiles, D.splits), kNT, pair_smem_bytes(A.tab_k),
+                                      st>>>(A);
         k_finalize<<<(2 * nc + blk - 1) / blk, blk, 0, st>>>(D);
     }
     k_decide<<<(nc + blk - 1) / blk, blk, 0, st>>>(D);
@@ -1376,6 +1437,15 @@ static lgm_status kmc_create_impl(const lgm_params* pin, int32_t device, uint32_
     DA(D.e_rm, std::max(D.cap_e, 1));
     DA(D.h_rm, std::max(D.cap_h, 1));
     DA(D.w64, std::max(D.cutoff2, 1));
+    const std::vector<int32_t> crank =
+        cell_ranks(p.grid_x, p.grid_y, p.grid_z, &D.cell_shift, &D.cells_x, &D.cells_y);
+    D.ncells = (int)crank.size();
+    D.sorted = D.coulomb ? 1 : 0;
+    int32_t* crank_d = nullptr;
+    DA(crank_d, D.ncells);
+    DA(D.bins, D.ncells + 2);
+    DA(D.tkey, 2 * ncap);
+    DA(D.tperm, 2 * ncap);
 #undef DA
     if ((st = arena.commit(k)) != LGM_OK) return bail(st, k->err);
     if (D.gauss) {
@@ -1395,9 +1465,12 @@ static lgm_status kmc_create_impl(const lgm_params* pin, int32_t device, uint32_
             return bail(LGM_ERR_CUDA, "table upload");
         D.gtab = k->gtab;
         D.gtab_k = kmax;
-        cudaFuncSetAttribute(kmc_pair(1), cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)pair_smem_bytes(kmax));
+        for (int sorted = 0; sorted < 2; ++sorted)
+            cudaFuncSetAttribute(kmc_pair(1, sorted), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)pair_smem_bytes(kmax));
     }
+    cudaMemcpy(crank_d, crank.data(), sizeof(int32_t) * crank.size(), cudaMemcpyHostToDevice);
+    D.cell_rank = crank_d;
     {
         std::vector<double> w(std::max(D.cutoff2, 1), 0.0);
         for (int r2 = 1; r2 < D.cutoff2; ++r2) {
@@ -1604,8 +1677,8 @@ struct BatchVariant {
 #define LGM_BV(NT, RP)                                                                 \
     BatchVariant {                                                                     \
         NT, RP, {                                                                      \
-            &pair_kernel_items<0, 0, NT, RP, kSUB, true>,                              \
-                &pair_kernel_items<1, 0, NT, RP, kSUB, true>                           \
+            &pair_kernel_items<0, 0, NT, RP, kSUB, true, true>,                        \
+                &pair_kernel_items<1, 0, NT, RP, kSUB, true, true>                     \
         }                                                                              \
     }
 const BatchVariant kBatchVariants[] = {LGM_BV(128, 4), LGM_BV(128, 2), LGM_BV(64, 4),
@@ -1636,7 +1709,8 @@ struct lgm_kmc_batch {
     int4* d_items = nullptr;
     int n_items = 0;
     int4 *map_car = nullptr, *map_pack = nullptr, *map_fin = nullptr, *map_guard = nullptr;
-    int nb_car = 0, nb_pack = 0, nb_fin = 0, nb_guard = 0;
+    int4* map_bins = nullptr;  // the target sort's bin counters
+    int nb_car = 0, nb_pack = 0, nb_fin = 0, nb_guard = 0, nb_bins = 0;
     int compact_threads = kCompactThreads;  // block size of the per-replica list compaction
     // replicas on the fused step and on the per-phase kernels
     int fused_max = kFusedMaxCharges;
@@ -1742,6 +1816,14 @@ lgm_status enqueue_fused(lgm_kmc_batch* b, int steps, bool branch) {
     return LGM_OK;
 }
 
+// The per-phase replicas' targets in lattice-cell order (before pack).
+void enqueue_batch_sort(lgm_kmc_batch* b, cudaStream_t st) {
+    kb_tbins_zero<<<b->nb_bins, 256, 0, st>>>(b->d_reps, b->map_bins);
+    kb_tbins<<<b->nb_fin, 256, 0, st>>>(b->d_reps, b->map_fin);
+    kb_tbins_scan<<<(int)b->classic.size(), 1024, 0, st>>>(b->d_reps, b->d_classic);
+    kb_tscatter<<<b->nb_fin, 256, 0, st>>>(b->d_reps, b->map_fin);
+}
+
 lgm_status enqueue_batch_step(lgm_kmc_batch* b) {
     cudaStream_t st = b->stream;
     if (b->classic.empty()) return enqueue_fused(b, 1, false);
@@ -1755,6 +1837,7 @@ lgm_status enqueue_batch_step(lgm_kmc_batch* b) {
     const int R = (int)b->classic.size();
     kb_choose<<<b->nb_car, 256, 0, st>>>(b->d_reps, b->map_car);
     if (b->coulomb) {
+        enqueue_batch_sort(b, st);
         kb_pack<<<b->nb_pack, 256, 0, st>>>(b->d_reps, b->map_pack);
         lgm_status s = enqueue_batch_pair(b, st);
         if (s != LGM_OK) return s;
@@ -1786,6 +1869,7 @@ lgm_status tune_batch(lgm_kmc_batch* b) {
     if (!b->coulomb || b->classic.empty()) return LGM_OK;
     cudaStream_t st = b->stream;
     kb_choose<<<b->nb_car, 256, 0, st>>>(b->d_reps, b->map_car);
+    enqueue_batch_sort(b, st);
     kb_pack<<<b->nb_pack, 256, 0, st>>>(b->d_reps, b->map_pack);
     BCUDA(b, cudaGetLastError());
     cudaEvent_t e0, e1;
@@ -1838,7 +1922,9 @@ lgm_status partition_batch(lgm_kmc_batch* b) {
     b->fused_small = true;
     for (int r : b->fused)
         b->fused_small &= b->hD[r].cap_e + b->hD[r].cap_h <= kFusedSmallCharges;
-    std::vector<int4> car, pack, fin, guard;
+    for (int r : b->fused) b->hD[r].sorted = 0;  // the fused step keeps the list order
+    for (int r : b->classic) b->hD[r].sorted = b->hD[r].coulomb;
+    std::vector<int4> car, pack, fin, guard, bins;
     auto add = [](std::vector<int4>& v, int r, int bound) {
         const int nb = std::max(1, (bound + kItemsPerThread * 256 - 1) / (kItemsPerThread * 256));
         for (int i = 0; i < nb; ++i) v.push_back(make_int4(r, i, nb, bound));
@@ -1850,6 +1936,7 @@ lgm_status partition_batch(lgm_kmc_batch* b) {
         add(car, r, ncap);
         add(pack, r, std::max(D.src_cap, D.tpad_cap));
         add(fin, r, 2 * ncap);
+        add(bins, r, D.ncells + 1);
         // flagged decisions grow with the charge count: one block per 2048 of capacity
         const int ng = std::min(kGuardBlocksPerReplica, std::max(1, (ncap + 2047) / 2048));
         for (int i = 0; i < ng; ++i) guard.push_back(make_int4(r, i, ng, 0));
@@ -1864,10 +1951,11 @@ lgm_status partition_batch(lgm_kmc_batch* b) {
                                         cudaMemcpyHostToDevice) == cudaSuccess);
     };
     if (!upload(&b->map_car, car) || !upload(&b->map_pack, pack) || !upload(&b->map_fin, fin) ||
-        !upload(&b->map_guard, guard) || !upload(&b->d_fused, b->fused) ||
-        !upload(&b->d_classic, b->classic))
+        !upload(&b->map_guard, guard) || !upload(&b->map_bins, bins) ||
+        !upload(&b->d_fused, b->fused) || !upload(&b->d_classic, b->classic))
         return bfail(b, LGM_ERR_CUDA, "block maps");
     b->nb_guard = (int)guard.size();
+    b->nb_bins = (int)bins.size();
     // the compaction loops over its list in blocks: small replicas need no 1024-thread block
     b->compact_threads = max_cap > 4096 ? kCompactThreads : 256;
     b->nb_car = (int)car.size();
@@ -1941,7 +2029,7 @@ lgm_status lgm_kmc_batch_destroy(lgm_kmc_batch* b) {
     if (b->exec) cudaGraphExecDestroy(b->exec);
     if (b->graph) cudaGraphDestroy(b->graph);
     void* ptrs[] = {b->d_reps, b->d_pargs, b->d_items, b->map_car, b->map_pack, b->map_fin,
-                    b->map_guard, b->d_fused, b->d_classic};
+                    b->map_guard, b->map_bins, b->d_fused, b->d_classic};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (b->fork) cudaEventDestroy(b->fork);

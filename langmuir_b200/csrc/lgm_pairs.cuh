@@ -33,6 +33,10 @@
 // nothing, so the sums are bit for bit those of the plain tile.
 #pragma once
 
+#include <algorithm>
+#include <utility>
+#include <vector>
+
 #include "lgm_device.cuh"
 
 namespace lgm {
@@ -276,13 +280,77 @@ __global__ void __launch_bounds__(NT) pair_kernel(PairArgs A) {
 // Work-item form for many independent problems in one launch (batched
 // replicas): item = {problem, tile, split, splits}; problem p's arguments are
 // args[p].  Items of uneven problems share the grid.
-template <int KIND, int PATH, int NT, int RP, int SUB, bool NORM = false>
+template <int KIND, int PATH, int NT, int RP, int SUB, bool NORM = false, bool SKIP = false>
 __global__ void __launch_bounds__(NT) pair_kernel_items(const PairArgs* __restrict__ args,
                                                         const int4* __restrict__ items) {
     const int4 it = items[blockIdx.x];
     PairArgs A = args[it.x];
     A.splits = it.w;
-    pair_tile<KIND, PATH, NT, RP, SUB, NORM>(A, it.y, it.z);
+    pair_tile<KIND, PATH, NT, RP, SUB, NORM, SKIP>(A, it.y, it.z);
+}
+
+// Exclusive prefix sum of a[0..n) in place by one block (blockDim a multiple
+// of 32, at most 1024; every thread of the block calls it).
+__device__ __forceinline__ void block_exclusive_scan(int32_t* a, int n) {
+    __shared__ int32_t warp_tot[32];
+    const int nt = (int)blockDim.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int per = (n + nt - 1) / nt;
+    const int lo = min(n, tid * per), hi = min(n, lo + per);
+    int32_t sum = 0;
+    for (int i = lo; i < hi; ++i) sum += a[i];
+    int32_t incl = sum;
+    for (int o = 1; o < 32; o <<= 1) {
+        const int32_t v = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += v;
+    }
+    if (lane == 31) warp_tot[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+        int32_t w = lane < nt / 32 ? warp_tot[lane] : 0;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int32_t v = __shfl_up_sync(0xffffffffu, w, o);
+            if (lane >= o) w += v;
+        }
+        if (lane < nt / 32) warp_tot[lane] = w;
+    }
+    __syncthreads();
+    int32_t run = incl - sum + (warp > 0 ? warp_tot[warp - 1] : 0);
+    for (int i = lo; i < hi; ++i) {
+        const int32_t c = a[i];
+        a[i] = run;
+        run += c;
+    }
+    __syncthreads();
+}
+
+// Morton (Z-order) rank of every lattice cell -- cubes of 2^shift sites,
+// the shift the smallest that keeps the cells at most 65536 -- for sorting
+// targets in spatial order.  Host side; returns the rank table.
+inline std::vector<int32_t> cell_ranks(int X, int Y, int Z, int* shift, int* cx, int* cy) {
+    int sh = 2;
+    auto cells = [&](int d) { return (d + (1 << sh) - 1) >> sh; };
+    while ((long long)cells(X) * cells(Y) * cells(Z) > 65536) ++sh;
+    *shift = sh;
+    *cx = cells(X);
+    *cy = cells(Y);
+    const int cz = cells(Z);
+    const int n = *cx * *cy * cz;
+    auto spread = [](uint64_t v) {  // bit i of v to bit 3i
+        uint64_t r = 0;
+        for (int i = 0; i < 21; ++i) r |= ((v >> i) & 1ull) << (3 * i);
+        return r;
+    };
+    std::vector<std::pair<uint64_t, int>> code(n);
+    for (int z = 0; z < cz; ++z)
+        for (int y = 0; y < *cy; ++y)
+            for (int x = 0; x < *cx; ++x) {
+                const int cell = x + *cx * (y + *cy * z);
+                code[cell] = {spread(x) | (spread(y) << 1) | (spread(z) << 2), cell};
+            }
+    std::sort(code.begin(), code.end());
+    std::vector<int32_t> rank(n);
+    for (int r = 0; r < n; ++r) rank[code[r].second] = r;
+    return rank;
 }
 
 }  // namespace lgm
