@@ -322,6 +322,28 @@ def test_full_size_3d_config_parity_and_symmetry(lgm, oracle_mod):
     assert_close(o64, want, nrm, TOL64)
 
 
+def test_skip_tile_equals_plain_tile(lgm, oracle_mod):
+    """The warp-skip tile (spatially sorted targets, a warp vote per source)
+    gives bit for bit the plain tile's potentials: skipped pairs lie outside
+    the cutoff and each target keeps its order over the sources."""
+    X, Y, Z, c = 128, 96, 8, 20
+    rng = np.random.default_rng(12)
+    orc = oracle_mod.Oracle(X, Y, Z, cutoff=c)
+    s, q, n = packed_case(orc, rng, 2500, 2300, 0, 0, drains=2)
+    with lgm.Coulomb(X, Y, Z, cutoff=c) as ctx:
+        vs = ctx.variants()
+        plain = next(i for i, v in enumerate(vs) if not v["warp_skip"] and v["threads"] == 128
+                     and v["target_pairs"] == 4 and v["run"] == 32)
+        skip = next(i for i, v in enumerate(vs) if v["warp_skip"] and v["threads"] == 128
+                    and v["target_pairs"] == 4 and v["run"] == 32)
+        out = {}
+        for v in (plain, skip):
+            ctx.set_variant(v)
+            out[v] = (ctx.potentials(s[:n], q[:n], s, lgm.POINT, 7), ctx.last_launch()["splits"])
+    assert out[plain][1] == out[skip][1]
+    np.testing.assert_array_equal(out[plain][0], out[skip][0])
+
+
 # ---- every compiled tile variant is exact to the same bound --------------------------
 def test_every_variant_and_autotune(lgm, oracle_mod):
     X, Y, Z, c = 96, 80, 12, 30
