@@ -159,7 +159,9 @@ __device__ __forceinline__ void pair_tile(PairArgs A, const int tile, const int 
             float acc[2 * RP];
 #pragma unroll
             for (int k = 0; k < 2 * RP; ++k) acc[k] = 0.f;
-#pragma unroll
+            // the skip tile branches per source: a partial unroll keeps its code small
+            constexpr int kUnrollJ = SKIP ? 4 : SUB;
+#pragma unroll kUnrollJ
             for (int jj = 0; jj < SUB; ++jj) {
                 const int j = j0 + jj;
                 const float4 g0 = sg[2 * j];
