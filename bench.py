@@ -49,7 +49,7 @@ FLOP_PER_TEST = 8
 FLOP_PER_CONTRIB = 3
 # DRAM bytes per launch of the pair kernel from one ncu capture of this
 # workload (profiles/pair_kernel_cfg2.md): dram__bytes_read + dram__bytes_write.
-PAIR_KERNEL_DRAM_BYTES = 2891264
+PAIR_KERNEL_DRAM_BYTES = 2872832
 
 
 def make_inputs(w, seed):
@@ -532,6 +532,53 @@ def other_kernels_run(L, args, fp32_peak):
                          "note": "8 FLOP per pair tested + 3 per pair inside the cutoff, as for "
                                  "point charges; erf(f r)/r is a "
                                  "shared-memory table gather on top"},
+            "tile_variant": dict(ctx.variants()[v], id=v), "accuracy": acc}
+    # the precomputed 1/sqrt(k) table path on the cfg2 workload: every pair
+    # gathers one 4-byte table entry from shared memory, and every target tile
+    # streams all 40-byte source records from L2
+    w = WORKLOADS["cfg2_3d_eh_images"]
+    s_all, q_all, n = make_inputs(w, 7)
+    T = len(s_all)
+    with L.Coulomb(w["X"], w["Y"], w["Z"], cutoff=w["cutoff"], device=dev.index,
+                   path=L.PATH_TABLE) as ctx:
+        d_s, d_q = torch.from_numpy(s_all).to(dev), torch.from_numpy(q_all).to(dev)
+        d_o = torch.empty(T, dtype=torch.float64, device=dev)
+        v = ctx.autotune(n, T, L.POINT, w["terms"])
+        ctx.set_variant(v)
+        ctx.set_timing(True)
+        ms = []
+        for i in range(args.warmup + args.steps):
+            ctx.potentials_async(d_s.data_ptr(), d_q.data_ptr(), n, d_s.data_ptr(), T,
+                                 d_o.data_ptr(), L.POINT, w["terms"], st.cuda_stream)
+            ctx.sync(st.cuda_stream)
+            if i >= args.warmup:
+                ms.append(ctx.last_launch()["pair_kernel_ms"])
+        last = ctx.last_launch()
+        pk = float(np.median(ms))
+        nterms = bin(w["terms"]).count("1")
+        pairs = nterms * n * T
+        idx = np.linspace(0, T - 1, 512).astype(int)
+        acc = accuracy_vs_oracle(w, s_all[:n], q_all[:n], s_all[idx], d_o.cpu().numpy()[idx],
+                                 w["terms"])
+        peaks = measured_peaks()
+        props = torch.cuda.get_device_properties(dev)
+        clk = float(peaks.get("sm_max_mhz", 1965.0)) * 1e6
+        smem_peak = props.multi_processor_count * 128 * clk / 1e9  # 32 banks x 4 B per clock
+        tiles = last["ctas"] // max(1, last["splits"])
+        n_pad = (n + 127) // 128 * 128
+        l2_bytes = tiles * n_pad * 40
+        gather = 4.0 * pairs / (pk * 1e-3) / 1e9
+        out["table_cfg2"] = {
+            "workload": w["desc"] + ", 1/sqrt(k) table path", "pairs_per_launch": pairs,
+            "pair_kernel_ms": pk, "pair_evals_per_s": pairs / (pk * 1e-3),
+            "roofline": {"bound": "shared-memory gather", "achieved": gather,
+                         "peak": smem_peak, "unit": "GB/s", "frac": gather / smem_peak,
+                         "basis": "4 B table entry per pair tested",
+                         "peak_source": "derived: SMs x 128 B per clock x sm_max_mhz",
+                         "l2_source_bytes": l2_bytes,
+                         "l2_source_gbs": l2_bytes / (pk * 1e-3) / 1e9,
+                         "frac_of_fp32_peak_at_11_flop_per_pair":
+                             FLOP_PER_PAIR * pairs / (pk * 1e-3) / 1e12 / fp32_peak},
             "tile_variant": dict(ctx.variants()[v], id=v), "accuracy": acc}
     # kernel 1, every site of config 1's lattice
     w = WORKLOADS["cfg1_2d_holes"]
