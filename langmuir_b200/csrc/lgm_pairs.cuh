@@ -169,16 +169,26 @@ __device__ __forceinline__ void pair_tile(PairArgs A, const int tile, const int 
                 const float2 av = f2(g0.x, g0.y), bv = f2(g0.z, g0.w);
                 const float2 cv = f2(g1.x, g1.y), dv = f2(g1.z, g1.w);
                 if constexpr (SKIP) {
+                    // r^2 - 1/2 as (tt + x a) + y b + (d + z c): three
+                    // dependent steps instead of four.  Every partial sum is
+                    // an integer or half-integer no larger in magnitude than
+                    // |t|^2 + |s|^2, so each step is exact and u has the bits
+                    // of the plain tile's order.  The per-thread minimum is a
+                    // tree for the same reason.
                     float2 uu[RP];
-                    unsigned m = 0xffffffffu;
+                    unsigned mk[RP];
 #pragma unroll
                     for (int k = 0; k < RP; ++k) {
-                        uu[k] = __fadd2_rn(dv, tt[k]);
-                        uu[k] = __ffma2_rn(tx[k], av, uu[k]);
-                        uu[k] = __ffma2_rn(ty[k], bv, uu[k]);
-                        uu[k] = __ffma2_rn(tz[k], cv, uu[k]);  // r^2 - 1/2, exact
-                        m = min(m, min(__float_as_uint(uu[k].x), __float_as_uint(uu[k].y)));
+                        const float2 pa = __ffma2_rn(tx[k], av, tt[k]);
+                        const float2 pc = __ffma2_rn(tz[k], cv, dv);
+                        uu[k] = __fadd2_rn(__ffma2_rn(ty[k], bv, pa), pc);
+                        mk[k] = min(__float_as_uint(uu[k].x), __float_as_uint(uu[k].y));
                     }
+#pragma unroll
+                    for (int w = 1; w < RP; w *= 2)
+#pragma unroll
+                        for (int k = 0; k + w < RP; k += 2 * w) mk[k] = min(mk[k], mk[k + w]);
+                    const unsigned m = mk[0];
                     if (__any_sync(0xffffffffu, m < ulim)) {
                         const float qs = sq[j].x;
 #pragma unroll
