@@ -445,12 +445,19 @@ def batch_run(L, args, rank):
         build_s = time.perf_counter() - t0
         b.run(max(1, args.warmup))  # tunes the tile shape, records the graph
         reps = [b.replica(i) for i in range(len(params))]
-        h0 = sum(r.stats()["proposals"] for r in reps)
+        st0 = [r.stats() for r in reps]
+        h0 = sum(st["proposals"] for st in st0)
         t0 = time.perf_counter()
         b.run(args.batch_steps)
         dt = time.perf_counter() - t0
-        hops = sum(r.stats()["proposals"] for r in reps) - h0
-        charges = sum(r.stats()["electrons"] + r.stats()["holes"] for r in reps)
+        st1 = [r.stats() for r in reps]
+        hops = sum(st["proposals"] for st in st1) - h0
+        charges = sum(st["electrons"] + st["holes"] for st in st1)
+        # pairs the step's Coulomb sums test: 2M targets x M sources per
+        # replica, averaged over the carrier counts before and after
+        m0 = np.array([st["electrons"] + st["holes"] for st in st0], dtype=np.float64)
+        m1 = np.array([st["electrons"] + st["holes"] for st in st1], dtype=np.float64)
+        pairs_per_step = float(np.sum(m0 * m0 + m1 * m1))
         tuning = b.tuning()
         fused = b.fused_count
     # the same replicas with every one on the per-phase kernels
@@ -483,6 +490,8 @@ def batch_run(L, args, rank):
             "single_replica_hops_per_s": single,
             "single_replica_sample": f"{len(sample)} of {len(params)} replicas stepped one by one",
             "speedup_vs_single": (hops / dt) / single, "tuning": tuning,
+            "pairs_per_step": pairs_per_step,
+            "pair_evals_per_s_in_step": pairs_per_step / (dt / args.batch_steps),
             "fused_replicas": fused,
             "per_phase_only": {"ms_per_step": 1e3 * pp_dt / args.batch_steps,
                                "hops_per_s": pp_hops / pp_dt},
@@ -915,6 +924,9 @@ def main():
         kmc["pair_evals_per_s_in_step"] = kp / (kmc["ms_per_step"] * 1e-3)
         kmc["pair_frac_of_fp32_peak_in_step"] = (FLOP_PER_PAIR * kmc["pair_evals_per_s_in_step"]
                                                  / 1e12 / fp32_peak)
+    if batch is not None:
+        batch["pair_frac_of_fp32_peak_in_step"] = (FLOP_PER_PAIR * batch["pair_evals_per_s_in_step"]
+                                                   / 1e12 / fp32_peak)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -85,6 +85,37 @@ def test_lattice_bound_for_exact_fp32_r2(dims, ok):
         assert st == N.ERR_UNSUPPORTED
 
 
+@pytest.mark.parametrize("dims", [(418, 8, 1), (8, 836, 1), (8, 8, 835), (418, 836, 835)])
+def test_both_r2_orders_are_exact_at_the_lattice_bound(dims):
+    """The plain tile forms r^2 - 1/2 as ((d + tt) + x a) + y b) + z c; the
+    skip tile's vote forms it as (tt + x a) + y b + (d + z c).  Emulating the
+    FP32 FMAs and adds step by step (each rounded once to FP32) at extreme
+    coordinates of the largest accepted lattices -- targets at x' in [-X, 2X)
+    for the image terms -- both orders give the exact r^2 - 1/2, so the vote
+    sees the plain tile's bits."""
+    import itertools
+    import numpy as np
+    X, Y, Z = dims
+    f32 = np.float32
+
+    def fma(a, b, c):  # one rounding, as FFMA: a*b + c is exact in float64 here
+        return f32(np.float64(a) * np.float64(b) + np.float64(c))
+
+    def add(a, b):
+        return f32(np.float64(a) + np.float64(b))
+
+    sx, sy, sz = {0, X - 1, X // 2}, {0, Y - 1, Y // 2}, {0, Z - 1, Z // 2}
+    tx = {-X, -1, 0, X // 2, X - 1, 2 * X - 1}
+    for xs, ys, zs, xt, yt, zt in itertools.product(sx, sy, sz, tx, sy, sz):
+        a, b, c = f32(-2 * xs), f32(-2 * ys), f32(-2 * zs)
+        d = f32(xs * xs + ys * ys + zs * zs - 0.5)
+        tt = f32(xt * xt + yt * yt + zt * zt)
+        want = (xt - xs) ** 2 + (yt - ys) ** 2 + (zt - zs) ** 2 - 0.5
+        plain = fma(zt, c, fma(yt, b, fma(xt, a, add(d, tt))))
+        vote = add(fma(yt, b, fma(xt, a, tt)), fma(zt, c, d))
+        assert float(plain) == want and float(vote) == want, (xs, ys, zs, xt, yt, zt)
+
+
 def test_create_without_gpu_reports_no_device():
     from tests.conftest import HAS_GPU
     if HAS_GPU:
