@@ -367,7 +367,28 @@ def kmc_configs_run(L, args, rank, world):
                        "ms_per_step": 1e3 * dt / args.cfg1_steps, "hops": hops, "timed_s": dt,
                        "hops_per_s": hops / dt,
                        "timing": "host wall clock around graph replays of the whole step"}
-        if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        e_single, h_single = k.carriers()
+    # the same replica as a batch of one: 163 carriers fit the fused
+    # one-block step, which runs many steps per launch instead of one graph
+    # replay per step; same Philox key, so the same trajectory
+    with L.KMCBatch([p], device=dev, replica0=rank) as b:
+        r = b.replica(0)
+        b.run(args.warmup)
+        f0 = r.stats()
+        t0 = time.perf_counter()
+        b.run(args.cfg1_steps)
+        fdt = time.perf_counter() - t0
+        f1 = r.stats()
+        e_f, h_f = r.carriers()
+        out["cfg1"]["fused_batch_of_one"] = {
+            "fused_replicas": b.fused_count, "ms_per_step": 1e3 * fdt / args.cfg1_steps,
+            "hops_per_s": (f1["proposals"] - f0["proposals"]) / fdt,
+            "same_carriers_as_single": bool(np.array_equal(e_f, e_single)
+                                            and np.array_equal(h_f, h_single)),
+            "timing": "host wall clock around the batch run (fused kernel launches)"}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        with L.KMC(p, device=dev, replica=rank) as k:
+            k.run(args.warmup + args.cfg1_steps)  # the state the timed leg ended in
             # the oracle's FP64 kMC step (one host thread) from the same world
             from oracle import oracle as O
             from oracle.kmc_setup import oracle_for
@@ -458,6 +479,10 @@ def batch_run(L, args, rank):
         m0 = np.array([st["electrons"] + st["holes"] for st in st0], dtype=np.float64)
         m1 = np.array([st["electrons"] + st["holes"] for st in st1], dtype=np.float64)
         pairs_per_step = float(np.sum(m0 * m0 + m1 * m1))
+        # the pair sum alone (CUDA events), after one more step from these counts
+        b.run(1)
+        pair_ms = b.time_pair(7)
+        pairs_timed = float(np.sum(2.0 * m1 * m1))
         tuning = b.tuning()
         fused = b.fused_count
     # the same replicas with every one on the per-phase kernels
@@ -492,6 +517,10 @@ def batch_run(L, args, rank):
             "speedup_vs_single": (hops / dt) / single, "tuning": tuning,
             "pairs_per_step": pairs_per_step,
             "pair_evals_per_s_in_step": pairs_per_step / (dt / args.batch_steps),
+            "pair_kernel": {"ms": pair_ms, "pairs": pairs_timed,
+                            "pair_evals_per_s": pairs_timed / (pair_ms * 1e-3),
+                            "timing": "CUDA events around the batched work-item pair kernel "
+                                      "alone, median of 7, over the charges of one step"},
             "fused_replicas": fused,
             "per_phase_only": {"ms_per_step": 1e3 * pp_dt / args.batch_steps,
                                "hops_per_s": pp_hops / pp_dt},
@@ -927,6 +956,8 @@ def main():
     if batch is not None:
         batch["pair_frac_of_fp32_peak_in_step"] = (FLOP_PER_PAIR * batch["pair_evals_per_s_in_step"]
                                                    / 1e12 / fp32_peak)
+        batch["pair_kernel"]["frac_of_fp32_peak_at_11_flop_per_pair"] = (
+            FLOP_PER_PAIR * batch["pair_kernel"]["pair_evals_per_s"] / 1e12 / fp32_peak)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -225,6 +225,13 @@ int32_t lgm_kmc_batch_fused_count(const lgm_kmc_batch* b);
  * chunks per work item, and the number of work items. */
 lgm_status lgm_kmc_batch_tuning(const lgm_kmc_batch* b, int32_t* threads, int32_t* target_pairs,
                                 int32_t* chunks_per_item, int32_t* items);
+/* Times the batched pair sum on its own: `reps` launches of the tuned
+ * work-item kernel over the charges the last step packed, each bracketed by
+ * CUDA events on the batch stream; *ms is the median launch time.  The sums
+ * it writes are the last step's sums again, so the simulation is unchanged.
+ * Needs at least one step run on the per-phase kernels (LGM_ERR_STATE
+ * otherwise).  Measurement aid with no counterpart in the reference. */
+lgm_status lgm_kmc_batch_time_pair(lgm_kmc_batch* b, int32_t reps, float* ms);
 
 #ifdef __cplusplus
 }

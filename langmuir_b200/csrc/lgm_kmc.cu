@@ -1748,6 +1748,7 @@ lgm_status build_items(lgm_kmc_batch* b, int v, int cpi) {
     const BatchVariant& BV = kBatchVariants[v];
     const int tile = BV.nt * 2 * BV.rp;
     std::vector<int4> items;
+    std::vector<float> cost;  // source chunks an item streams (capacity estimate)
     std::vector<PairArgs> pargs(b->reps.size());
     for (int r : b->fused) b->hD[r].splits = 1;  // the fused pair sum is one split
     for (int r : b->classic) {
@@ -1759,11 +1760,24 @@ lgm_status build_items(lgm_kmc_batch* b, int v, int cpi) {
         const int tiles = (D.nterms * D.tpad_cap + tile - 1) / tile;
         for (int t = 0; t < tiles; ++t)
             for (int sp = 0; sp < splits; ++sp) items.push_back(make_int4(r, t, sp, splits));
+        cost.resize(items.size(), (float)chunks / splits);
         PairArgs& A = pargs[r];
         A.geo = D.geo; A.qq = D.qq; A.splits = splits; A.tgt = D.tgt; A.part = D.part;
         A.part_norm = D.part_norm; A.c2 = (float)D.cutoff2;
         A.tab = k->gtab; A.tab_k = D.gauss ? k->gtab_k : 0;
         A.err = D.err; A.dyn = D.cnt + I_NCHUNK;
+    }
+    // Longest items first: the block scheduler hands out blocks in index
+    // order, so the long items of the large replicas start in the first wave
+    // and the short ones fill in behind them.  The order does not change any
+    // sum (each item writes its own partials).
+    {
+        std::vector<int> ord(items.size());
+        for (size_t i = 0; i < ord.size(); ++i) ord[i] = (int)i;
+        std::stable_sort(ord.begin(), ord.end(), [&](int x, int y) { return cost[x] > cost[y]; });
+        std::vector<int4> sorted(items.size());
+        for (size_t i = 0; i < ord.size(); ++i) sorted[i] = items[ord[i]];
+        items.swap(sorted);
     }
     if (b->d_items) cudaFree(b->d_items);
     b->d_items = nullptr;
@@ -2096,6 +2110,36 @@ lgm_status lgm_kmc_batch_set_fused(lgm_kmc_batch* b, int32_t max_charges) {
 
 int32_t lgm_kmc_batch_fused_count(const lgm_kmc_batch* b) {
     return b ? (int32_t)b->fused.size() : 0;
+}
+
+lgm_status lgm_kmc_batch_time_pair(lgm_kmc_batch* b, int32_t reps, float* ms) {
+    if (!b || reps < 1 || !ms) return LGM_ERR_INVALID_ARGUMENT;
+    if (!b->exec || !b->coulomb || b->classic.empty())
+        return bfail(b, LGM_ERR_STATE, "no per-phase Coulomb step has run");
+    BCUDA(b, cudaSetDevice(b->device));
+    cudaStream_t st = b->stream;
+    BCUDA(b, cudaStreamSynchronize(st));
+    cudaEvent_t e0, e1;
+    BCUDA(b, cudaEventCreate(&e0));
+    if (cudaEventCreate(&e1) != cudaSuccess) {
+        cudaEventDestroy(e0);
+        return bfail(b, LGM_ERR_CUDA, "cudaEventCreate");
+    }
+    std::vector<float> t(reps);
+    lgm_status s = LGM_OK;
+    for (int r = 0; r < reps && s == LGM_OK; ++r) {
+        cudaEventRecord(e0, st);
+        s = enqueue_batch_pair(b, st);
+        cudaEventRecord(e1, st);
+        if (cudaEventSynchronize(e1) != cudaSuccess) s = bfail(b, LGM_ERR_CUDA, "pair launch");
+        cudaEventElapsedTime(&t[r], e0, e1);
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (s != LGM_OK) return s;
+    std::sort(t.begin(), t.end());
+    *ms = t[reps / 2];
+    return LGM_OK;
 }
 
 lgm_status lgm_kmc_batch_tuning(const lgm_kmc_batch* b, int32_t* threads, int32_t* target_pairs,

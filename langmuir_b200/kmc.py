@@ -263,11 +263,13 @@ N.SIGNATURES.update({
                                     ctypes.POINTER(_i32), ctypes.POINTER(_i32)]),
     "lgm_kmc_batch_set_fused": (_i32, [_vp, _i32]),
     "lgm_kmc_batch_fused_count": (_i32, [_vp]),
+    "lgm_kmc_batch_time_pair": (_i32, [_vp, _i32, ctypes.POINTER(ctypes.c_float)]),
 })
 if N._lib is not None:
     for _name in ("lgm_kmc_batch_create", "lgm_kmc_batch_destroy", "lgm_kmc_batch_last_error",
                   "lgm_kmc_batch_run", "lgm_kmc_batch_size", "lgm_kmc_batch_replica",
-                  "lgm_kmc_batch_tuning", "lgm_kmc_batch_set_fused", "lgm_kmc_batch_fused_count"):
+                  "lgm_kmc_batch_tuning", "lgm_kmc_batch_set_fused", "lgm_kmc_batch_fused_count",
+                  "lgm_kmc_batch_time_pair"):
         _fn = getattr(N._lib, _name)
         _fn.restype, _fn.argtypes = N.SIGNATURES[_name]
 
@@ -347,3 +349,12 @@ class KMCBatch:
                                      ctypes.byref(d))
         return {"threads": a.value, "target_pairs": b.value, "chunks_per_item": c.value,
                 "items": d.value}
+
+    def time_pair(self, reps: int = 5) -> float:
+        """Median CUDA-event time (ms) of the batched pair sum alone, over
+        the charges the last step packed."""
+        ms = ctypes.c_float()
+        st = N.lib().lgm_kmc_batch_time_pair(self._h, int(reps), ctypes.byref(ms))
+        if st != N.OK:
+            raise N.LgmError(st, N.lib().lgm_kmc_batch_last_error(self._h).decode())
+        return ms.value
