@@ -322,14 +322,20 @@ lgm_status prep(lgm_ctx* c, unsigned terms, const int32_t* d_src, const int32_t*
     return LGM_OK;
 }
 
-// Splits of the source range for variant v: as many as fill one wave of
-// resident CTAs, never more than the chunks.
+// Splits of the source range for variant v: as many as fill kSplitWaves
+// waves of resident CTAs, never more than the chunks.  With the warp skip the
+// CTAs of one launch do uneven work (tiles near few charges, image tiles far
+// from the electrode skip most sources), and three waves of smaller CTAs let
+// the block scheduler even it out; more waves cost more in the FP64 partials
+// that finalize sums than they save (cfg2 step: 1 wave 0.647 ms, 3 waves
+// 0.607 ms, 8 waves 0.614 ms).
+constexpr int kSplitWaves = 3;
 int splits_for(const lgm_ctx* c, int v, int fi, const Shape& sh, int* tiles_out) {
     const Variant& V = kVariants[v];
     const int tiles = (sh.t_phys + V.nt * 2 * V.rp - 1) / (V.nt * 2 * V.rp);
     const int capacity = c->sm_count * std::max(1, c->bps[v][fi]);
     *tiles_out = tiles;
-    return std::max(1, std::min({kMaxSplits, capacity / tiles, sh.n_chunks}));
+    return std::max(1, std::min({kMaxSplits, kSplitWaves * capacity / tiles, sh.n_chunks}));
 }
 
 lgm_status launch_pair(lgm_ctx* c, int kind, int v, const Shape& sh, cudaStream_t st,

@@ -1409,7 +1409,8 @@ static lgm_status kmc_create_impl(const lgm_params* pin, int32_t device, uint32_
     k->pair_tiles = (tphys_cap + kTile - 1) / kTile;
     int bps = 1;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, kmc_pair(D.gauss), kNT, pair_smem_bytes(64));
-    D.splits = std::max(1, std::min({64, n_sms * std::max(1, bps) / k->pair_tiles,
+    // three waves of resident CTAs, as for the single pair sums (lgm_api.cu)
+    D.splits = std::max(1, std::min({64, 3 * n_sms * std::max(1, bps) / k->pair_tiles,
                                      D.src_cap / CH}));
     lgm_status st;
     // every buffer of the replica in one allocation (256-byte aligned slices)
