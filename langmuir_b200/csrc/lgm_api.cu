@@ -140,7 +140,16 @@ __global__ void finalize(const double* __restrict__ part, int splits, int t_phys
     for (int slot = 0; slot < nterms; ++slot) {
         double s = 0.0;
         const double* p = part + (size_t)slot * t_pad + g;
-        for (int sp = 0; sp < splits; ++sp) s += p[(size_t)sp * t_phys];
+        // eight loads in flight, then the adds in split order (same bits)
+        int sp = 0;
+        for (; sp + 8 <= splits; sp += 8) {
+            double v[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) v[u] = p[(size_t)(sp + u) * t_phys];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) s += v[u];
+        }
+        for (; sp < splits; ++sp) s += p[(size_t)sp * t_phys];
         total = (slot == 0) ? s : total - s;
     }
     out[perm[g]] = prefactor * total;

@@ -258,7 +258,24 @@ __device__ __forceinline__ void finalize_body(const Dev& D, const int g) {
     double v = 0.0, n = 0.0;
     for (int slot = 0; slot < D.nterms; ++slot) {
         double s = 0.0, m = 0.0;
-        for (int sp = 0; sp < D.splits; ++sp) {
+        // four splits' loads in flight, then the adds in split order (same bits)
+        int sp = 0;
+        for (; sp + 4 <= D.splits; sp += 4) {
+            double pv[4];
+            float nv[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const size_t o = (size_t)(sp + u) * tphys + (size_t)slot * tpad + g;
+                pv[u] = D.part[o];
+                nv[u] = D.part_norm[o];
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                s += pv[u];
+                m += (double)nv[u];
+            }
+        }
+        for (; sp < D.splits; ++sp) {
             const size_t o = (size_t)sp * tphys + (size_t)slot * tpad + g;
             s += D.part[o];
             m += (double)D.part_norm[o];
