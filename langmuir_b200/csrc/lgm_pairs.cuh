@@ -302,55 +302,53 @@ __global__ void __launch_bounds__(NT) pair_kernel_items(const PairArgs* __restri
 }
 
 // Exclusive prefix sum of a[0..n) in place by one block (blockDim a multiple
-// of 32, at most 1024; every thread of the block calls it).  The array goes
-// through shared memory in tiles of 4 entries per thread, loaded and stored
-// coalesced; each thread scans 4 consecutive entries of the tile, and a carry
-// runs from tile to tile.
+// of 32, at most 1024; every thread of the block calls it; a 16-byte
+// aligned).  Each thread owns a run of consecutive entries, a multiple of 4
+// long, read and written as int4 so that its loads are in flight together.
 __device__ __forceinline__ void block_exclusive_scan(int32_t* a, int n) {
-    constexpr int kPer = 4;
-    __shared__ __align__(16) int32_t tile[1024 * kPer];
     __shared__ int32_t warp_tot[32];
     const int nt = (int)blockDim.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int nw = nt / 32, tn = nt * kPer;
-    int32_t carry = 0;
-    for (int base = 0; base < n; base += tn) {
-        const int m = min(tn, n - base);
-        for (int i = tid; i < m; i += nt) tile[i] = a[base + i];
-        __syncthreads();
-        const int4 q = reinterpret_cast<const int4*>(tile)[tid];
-        int32_t v[kPer] = {q.x, q.y, q.z, q.w};
-        int32_t sum = 0;
-#pragma unroll
-        for (int k = 0; k < kPer; ++k) {
-            if (tid * kPer + k >= m) v[k] = 0;
-            sum += v[k];
-        }
-        int32_t incl = sum;
+    const int per = ((n + nt - 1) / nt + 3) & ~3;
+    const int lo = min(n, tid * per), hi = min(n, lo + per);
+    const int hi4 = lo + ((hi - lo) & ~3);
+    int32_t sum = 0;
+#pragma unroll 4
+    for (int i = lo; i < hi4; i += 4) {
+        const int4 q = *reinterpret_cast<const int4*>(a + i);
+        sum += q.x + q.y + q.z + q.w;
+    }
+    for (int i = hi4; i < hi; ++i) sum += a[i];
+    int32_t incl = sum;
+    for (int o = 1; o < 32; o <<= 1) {
+        const int32_t v = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += v;
+    }
+    if (lane == 31) warp_tot[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+        int32_t w = lane < nt / 32 ? warp_tot[lane] : 0;
         for (int o = 1; o < 32; o <<= 1) {
-            const int32_t w = __shfl_up_sync(0xffffffffu, incl, o);
-            if (lane >= o) incl += w;
+            const int32_t v = __shfl_up_sync(0xffffffffu, w, o);
+            if (lane >= o) w += v;
         }
-        if (lane == 31) warp_tot[warp] = incl;
-        __syncthreads();
-        if (warp == 0) {
-            int32_t w = lane < nw ? warp_tot[lane] : 0;
-            for (int o = 1; o < 32; o <<= 1) {
-                const int32_t u = __shfl_up_sync(0xffffffffu, w, o);
-                if (lane >= o) w += u;
-            }
-            if (lane < nw) warp_tot[lane] = w;
-        }
-        __syncthreads();
-        int32_t run = carry + incl - sum + (warp > 0 ? warp_tot[warp - 1] : 0);
-#pragma unroll
-        for (int k = 0; k < kPer; ++k) {
-            if (tid * kPer + k < m) tile[tid * kPer + k] = run;
-            run += v[k];
-        }
-        carry += warp_tot[nw - 1];
-        __syncthreads();
-        for (int i = tid; i < m; i += nt) a[base + i] = tile[i];
-        __syncthreads();  // tile and warp_tot are reused by the next tile
+        if (lane < nt / 32) warp_tot[lane] = w;
+    }
+    __syncthreads();
+    int32_t run = incl - sum + (warp > 0 ? warp_tot[warp - 1] : 0);
+#pragma unroll 4
+    for (int i = lo; i < hi4; i += 4) {
+        int4 q = *reinterpret_cast<int4*>(a + i);
+        const int4 c = q;
+        q.x = run; run += c.x;
+        q.y = run; run += c.y;
+        q.z = run; run += c.z;
+        q.w = run; run += c.w;
+        *reinterpret_cast<int4*>(a + i) = q;
+    }
+    for (int i = hi4; i < hi; ++i) {
+        const int32_t c = a[i];
+        a[i] = run;
+        run += c;
     }
     __syncthreads();
 }
