@@ -617,7 +617,8 @@ def other_kernels_run(L, args, fp32_peak):
                          "l2_source_gbs": l2_bytes / (pk * 1e-3) / 1e9,
                          "frac_of_fp32_peak_at_11_flop_per_pair":
                              FLOP_PER_PAIR * pairs / (pk * 1e-3) / 1e12 / fp32_peak},
-            "tile_variant": dict(ctx.variants()[v], id=v), "accuracy": acc}
+            # the table path runs the plain tile whatever the variant's flag
+            "tile_variant": dict(ctx.variants()[v], id=v, warp_skip=False), "accuracy": acc}
     # kernel 1, every site of config 1's lattice
     w = WORKLOADS["cfg1_2d_holes"]
     s_all, q_all, n = make_inputs(w, 6)
