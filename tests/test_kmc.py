@@ -12,6 +12,7 @@ import numpy as np
 import pytest
 
 import langmuir_b200 as L
+from langmuir_b200 import _native as N
 from oracle.kmc_setup import interface_bonds, oracle_for, rates  # noqa: F401
 
 
@@ -259,6 +260,29 @@ def test_batch_matches_single_replicas(form):
         np.testing.assert_array_equal(got[i][0], e, err_msg=f"replica {i} electrons")
         np.testing.assert_array_equal(got[i][1], h, err_msg=f"replica {i} holes")
         assert stats[i]["counters"] == s["counters"] and stats[i]["step"] == steps
+
+
+@pytest.mark.gpu
+def test_batch_time_pair_leaves_the_run_unchanged():
+    """lgm_kmc_batch_time_pair times the per-phase batch's pair sum on its
+    own: it refuses before a step has run, returns a positive time after, and
+    the replicas then follow the same trajectories as a batch never timed."""
+    params = uneven_params(4, seed=3)
+    got = []
+    for timed in (False, True):
+        with L.KMCBatch(params, replica0=30, fused_max_charges=0) as b:
+            if timed:
+                with pytest.raises(N.LgmError) as e:
+                    b.time_pair(3)
+                assert e.value.status == N.ERR_STATE
+            b.run(10)
+            if timed:
+                assert b.time_pair(3) > 0.0
+            b.run(10)
+            got.append([b.replica(i).carriers() for i in range(len(params))])
+    for (e0, h0), (e1, h1) in zip(*got):
+        np.testing.assert_array_equal(e0, e1)
+        np.testing.assert_array_equal(h0, h1)
 
 
 @pytest.mark.gpu
