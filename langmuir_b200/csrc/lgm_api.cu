@@ -477,6 +477,29 @@ lgm_status check_common(lgm_ctx* c, int kind, unsigned terms, int n, int t) {
 
 // Host-side range checks for the host-buffer entry points (the reference
 // would index garbage; here the call fails before any work).
+// Copies site ids into a pinned staging buffer and checks each one against
+// [0, lim) in the same pass; the first bad id gives the error that
+// check_sites would give.  `what` names the role in the message, and `base`
+// is the index of src[0] in the caller's array.
+lgm_status stage_sites(lgm_ctx* c, const int32_t* src, int n, int32_t lim, const char* what,
+                       int32_t* dst, int base = 0) {
+    bool bad = false;
+    for (int j = 0; j < n; ++j) {
+        const int32_t v = src[j];
+        bad |= (v < 0) | (v >= lim);
+        dst[j] = v;
+    }
+    if (!bad) return LGM_OK;
+    for (int j = 0; j < n; ++j)
+        if (src[j] < 0 || src[j] >= lim) {
+            char b[128];
+            std::snprintf(b, sizeof b, "%s %d: site %d outside [0, %d)", what, base + j, src[j],
+                          lim);
+            return fail(c, LGM_ERR_OUT_OF_RANGE, b);
+        }
+    return LGM_OK;
+}
+
 lgm_status check_sites(lgm_ctx* c, const int32_t* src, int n, const int32_t* tgt, int t) {
     for (int j = 0; j < n; ++j)
         if (src[j] < 0 || src[j] >= c->volume) {
@@ -853,7 +876,6 @@ lgm_status lgm_potentials(lgm_ctx* c, lgm_kind kind, uint32_t terms, const int32
     if (s != LGM_OK) return s;
     if ((n > 0 && (!src_site || !src_q)) || (t > 0 && (!tgt_site || !out)))
         return fail(c, LGM_ERR_INVALID_ARGUMENT, "null buffer");
-    if ((s = check_sites(c, src_site, n, tgt_site, t)) != LGM_OK) return s;
     LGM_CUDA(c, cudaSetDevice(c->device));
     cudaStream_t st = c->stream;
     const size_t nn = std::max(n, 1), tt = std::max(t, 1);
@@ -865,14 +887,27 @@ lgm_status lgm_potentials(lgm_ctx* c, lgm_kind kind, uint32_t terms, const int32
     if ((s = grow_device(c, &c->d_q, &c->q_cap, nn)) != LGM_OK) return s;
     if ((s = grow_device(c, &c->d_t, &c->t_cap, tt)) != LGM_OK) return s;
     if ((s = grow_device(c, &c->d_o, &c->o_cap, tt)) != LGM_OK) return s;
-    std::memcpy(c->h_s, src_site, sizeof(int32_t) * n);
+    // Sites are checked while they are staged (sources first, then targets,
+    // as check_sites orders its errors).  When the sources are the first n
+    // targets (kernel 2: w aliases s, openclhelper.cpp:154) they are staged
+    // and copied once, as part of the targets.
+    const bool alias = tgt_site == src_site && n <= t;
+    if (alias) {
+        if ((s = stage_sites(c, src_site, n, c->volume, "source", c->h_t)) != LGM_OK) return s;
+    } else {
+        if ((s = stage_sites(c, src_site, n, c->volume, "source", c->h_s)) != LGM_OK) return s;
+        LGM_CUDA(c, cudaMemcpyAsync(c->d_s, c->h_s, sizeof(int32_t) * n, cudaMemcpyHostToDevice,
+                                    st));
+    }
     std::memcpy(c->h_q, src_q, sizeof(int32_t) * n);
-    std::memcpy(c->h_t, tgt_site, sizeof(int32_t) * t);
-    LGM_CUDA(c, cudaMemcpyAsync(c->d_s, c->h_s, sizeof(int32_t) * n, cudaMemcpyHostToDevice, st));
     LGM_CUDA(c, cudaMemcpyAsync(c->d_q, c->h_q, sizeof(int32_t) * n, cudaMemcpyHostToDevice, st));
+    const int t0 = alias ? n : 0;  // aliased: the first n are staged and in range already
+    if ((s = stage_sites(c, tgt_site + t0, t - t0, c->volume + kDrainIds, "target", c->h_t + t0,
+                         t0)) != LGM_OK)
+        return s;
     LGM_CUDA(c, cudaMemcpyAsync(c->d_t, c->h_t, sizeof(int32_t) * t, cudaMemcpyHostToDevice, st));
-    if ((s = launch_potentials(c, kind, terms, c->d_s, c->d_q, n, c->d_t, t, 0, c->d_o, st)) !=
-        LGM_OK)
+    if ((s = launch_potentials(c, kind, terms, alias ? c->d_t : c->d_s, c->d_q, n, c->d_t, t, 0,
+                               c->d_o, st)) != LGM_OK)
         return s;
     LGM_CUDA(c, cudaMemcpyAsync(c->h_o, c->d_o, sizeof(double) * t, cudaMemcpyDeviceToHost, st));
     if ((s = check_device_error(c, st)) != LGM_OK) return s;

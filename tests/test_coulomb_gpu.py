@@ -228,6 +228,20 @@ def test_range_errors(lgm):
         ctx.potentials([0], [1], [8 * 8 * 2 + 34])
         with pytest.raises(lgm.LgmError):
             ctx.kernel2([1, 2], [1, 1], 3)
+        # the messages name the role and the index in the caller's array, for
+        # separate source and target arrays and for kernel 2's shared one
+        with pytest.raises(lgm.LgmError) as e:
+            ctx.potentials([0, 5], [1, 1], [0, 8 * 8 * 2 + 35])
+        assert "target 1:" in str(e.value)
+        with pytest.raises(lgm.LgmError) as e:
+            ctx.kernel2(np.array([1, 2, 3, 8 * 8 * 2 + 35], np.int32), np.ones(4, np.int32), 2)
+        assert "target 3:" in str(e.value)
+        with pytest.raises(lgm.LgmError) as e:  # a drain id is a target, never a source
+            ctx.kernel2(np.array([1, 8 * 8 * 2, 3], np.int32), np.ones(3, np.int32), 2)
+        assert "source 1:" in str(e.value)
+        # the context stays usable, and kernel 2 still sums correctly after the errors
+        o = ctx.kernel2(np.array([0, 1, 8 * 8 * 2], np.int32), np.array([1, 1, 1], np.int32), 2)
+        assert o[0] == o[1] and o[0] > 0
 
 
 def test_async_range_error_reported_by_sync(lgm):
