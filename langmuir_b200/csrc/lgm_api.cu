@@ -698,7 +698,8 @@ lgm_status lgm_create(const lgm_config* cfg, int32_t device, lgm_ctx** out) {
             return bail("cudaMemcpy", e);
     }
     // Shared memory above the 48 KB default for large cutoffs, and the
-    // resident CTAs per SM of every variant (the split count fills one wave).
+    // resident CTAs per SM of every variant (the split count fills
+    // kSplitWaves waves of them).
     {
         const size_t smem_tab[3] = {pair_smem_bytes(0), pair_smem_bytes(c->gtab_k),
                                     pair_smem_bytes(std::max(c->rtab_k, c->gtab_k))};
