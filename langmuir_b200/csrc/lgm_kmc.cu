@@ -49,8 +49,10 @@ enum : int32_t { O_OCCUPIED = 0, O_MET_ACCEPT = 1, O_MET_REJECT = 2, O_DRAIN_ACC
 // Device counters: 20 flux (attempts, successes) + proposals + accepted + guard.
 enum { C_XSRC = 16, C_RECOMB = 18, C_PROPOSALS = 20, C_ACCEPTED = 21, C_GUARD = 22, C_NUM = 23 };
 // Device ints.
+// I_FIRST_E/H: the lowest list index a step removes (INT_MAX: none), where
+// the stable compaction of that list starts.
 enum { I_NE = 0, I_NH, I_STEP, I_NFLAG, I_REMOVED, I_NE0, I_NH0, I_NCHUNK, I_TPHYS, I_TPAD,
-       I_NBONDS, I_NUM };
+       I_NBONDS, I_FIRST_E, I_FIRST_H, I_NUM };
 // Recombination and exciton-source purposes of the random stream.
 constexpr uint32_t RNG_RECOMB = 5, RNG_EXCITON = RNG_SOURCE + 4;
 
@@ -186,6 +188,8 @@ __device__ __forceinline__ void choose_body(const Dev& D, const int i) {
         D.cnt[I_NH0] = nh;
         D.cnt[I_NFLAG] = 0;
         D.cnt[I_REMOVED] = 0;
+        D.cnt[I_FIRST_E] = INT_MAX;
+        D.cnt[I_FIRST_H] = INT_MAX;
     }
     if (i >= ne + nh) return;
     const bool e = i < ne;
@@ -527,6 +531,7 @@ __device__ __forceinline__ void move_body(const Dev& D, const int i) {
             (e0 ? D.et : D.ht)[sites[k0]] = T_EMPTY;
             sites[k0] = -1;
             D.cnt[I_REMOVED] = 1;
+            atomicMin(&D.cnt[e0 ? I_FIRST_E : I_FIRST_H], k0);
         } else if (D.accept[i]) {
             const bool e = i < ne;
             const int k = e ? i : i - ne;
@@ -538,6 +543,7 @@ __device__ __forceinline__ void move_body(const Dev& D, const int i) {
                 own[s] = T_EMPTY;
                 sites[k] = -1;
                 D.cnt[I_REMOVED] = 1;
+                atomicMin(&D.cnt[e ? I_FIRST_E : I_FIRST_H], k);
                 moved = 1;
             } else if ((e ? D.claim_e : D.claim_h)[f] == k) {
                 own[s] = T_EMPTY;
@@ -620,10 +626,12 @@ __device__ __forceinline__ void recomb_reset_body(const Dev& D, const int i) {
 // electrode sources (simulation.cpp:246-249) and currentStep += 1.  One block.
 constexpr int kCompactThreads = 1024;
 
-__device__ int compact(int32_t* a, int n, int* warp_sums) {
-    int base = 0;
+// Entries before `start` are all kept (no removal below it) and stay put.
+__device__ int compact(int32_t* a, int n, int* warp_sums, int start) {
+    start = min(max(start, 0), n);
+    int base = start;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for (int t0 = 0; t0 < n; t0 += blockDim.x) {
+    for (int t0 = start; t0 < n; t0 += blockDim.x) {
         const int i = t0 + threadIdx.x;
         const int v = i < n ? a[i] : -1;
         const bool keep = v >= 0;
@@ -647,8 +655,8 @@ __device__ int compact(int32_t* a, int n, int* warp_sums) {
 __device__ __forceinline__ void compact_inject_body(const Dev& D, int* warp_sums) {
     int ne = D.cnt[I_NE0], nh = D.cnt[I_NH0];
     if (D.cnt[I_REMOVED]) {
-        ne = compact(D.e_site, ne, warp_sums);
-        nh = compact(D.h_site, nh, warp_sums);
+        ne = compact(D.e_site, ne, warp_sums, D.cnt[I_FIRST_E]);
+        nh = compact(D.h_site, nh, warp_sums, D.cnt[I_FIRST_H]);
     }
     if (threadIdx.x != 0) return;
     const uint32_t step = (uint32_t)D.cnt[I_STEP];
