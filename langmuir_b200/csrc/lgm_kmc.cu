@@ -415,7 +415,7 @@ __device__ __forceinline__ void decide_body(const Dev& D, const int i) {
 constexpr int kGuardThreads = 1024;
 // Blocks per replica of the batched guard: flagged decisions of one replica
 // are spread over them (a replica with M charges flags ~1e-3 M per step).
-constexpr int kGuardBlocksPerReplica = 4;
+constexpr int kGuardBlocksPerReplica = 12;
 // Indices per thread of the batched element-wise kernels (see LGM_BATCH_LOOP).
 constexpr int kItemsPerThread = 4;
 
