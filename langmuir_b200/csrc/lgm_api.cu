@@ -266,8 +266,11 @@ const Variant kVariants[] = {
     LGM_VARIANT(128, 8, 16),       LGM_VARIANT(256, 4, 16),       LGM_VARIANT(64, 4, 16),
     LGM_VARIANT(128, 4, 32),       LGM_VARIANT(256, 2, 16),       LGM_VARIANT_SKIP(128, 4, 32),
     LGM_VARIANT_SKIP(128, 4, 16),  LGM_VARIANT_SKIP(128, 2, 32),  LGM_VARIANT_SKIP(64, 4, 32),
+    LGM_VARIANT_SKIP(64, 3, 32),   LGM_VARIANT_SKIP(128, 3, 32),
 };
 constexpr int kNumVariants = (int)(sizeof(kVariants) / sizeof(kVariants[0]));
+static_assert(kNumVariants <= (int)(sizeof(lgm_ctx::bps) / sizeof(lgm_ctx::bps[0])),
+              "lgm_ctx::bps holds every variant");
 constexpr int kDefaultVariant = 8;  // skip, 128 threads, 4 target pairs, runs of 32
 
 int fn_index(int kind, int path) {
