@@ -23,6 +23,7 @@
 #ifndef LANGMUIR_B200_HELPER_HPP
 #define LANGMUIR_B200_HELPER_HPP
 
+#include <cmath>
 #include <cstdint>
 #include <string>
 #include <vector>
@@ -35,7 +36,10 @@ template <class WorldT>
 class OpenClHelper {
 public:
     explicit OpenClHelper(WorldT& world) : m_world(world) {}
-    ~OpenClHelper() { lgm_destroy(m_ctx); }
+    ~OpenClHelper() {
+        lgm_destroy(m_ctx);
+        lgm_destroy(m_ctx64);
+    }
     OpenClHelper(const OpenClHelper&) = delete;
     OpenClHelper& operator=(const OpenClHelper&) = delete;
 
@@ -58,7 +62,10 @@ public:
         cfg.work_size = p.workSize;
         cfg.opencl_threshold = p.openclThreshold;
         lgm_destroy(m_ctx);
-        m_ctx = nullptr;
+        lgm_destroy(m_ctx64);
+        m_ctx = m_ctx64 = nullptr;
+        m_cfg = cfg;
+        m_device = gpuID;
         m_status = lgm_create(&cfg, gpuID, &m_ctx);
         if (m_status != LGM_OK) {
             m_error = lgm_last_error(nullptr);
@@ -91,6 +98,72 @@ public:
     // openclhelper.cpp:567-583
     double getOutputHost(int index) const { return m_o[index]; }
     double getOutputHostFuture(int index) const { return m_o[index + m_offset]; }
+
+    // One carrier's check by compareHostAndDeviceForAllCarriers.
+    struct CoulombComparison {
+        int openclID;
+        double gpu1, gpu2;  // last launch: current site, future site minus the carrier's own term
+        double cpu1, cpu2;  // the same from FP64 sums over the same charges
+        double gpu, cpu;    // energy change q * (V2 - V1) of each
+        bool failed;        // the reference's acceptance test
+    };
+
+    // openclhelper.cpp:546-558 and ChargeAgent::compareCoulomb
+    // (chargeagent.cpp:298-370): every electron's and hole's potentials from
+    // the last kernel-2 launch against FP64 sums over the same sources (a
+    // second context in LGM_PREC_FP64, made on the first call).  A carrier
+    // fails when the energy change differs by more than 1e-4 (signed, as the
+    // reference tests it) or either potential by more than 1e-4 percent of
+    // the mean of the two magnitudes.  The reference prints each comparison;
+    // this returns them in `out` (if given) and returns the number that fail,
+    // or -1 with lastStatus() set if the FP64 sums could not be made.
+    int compareHostAndDeviceForAllCarriers(std::vector<CoulombComparison>* out = nullptr) {
+        if (out) out->clear();
+        const int nc = (int)(m_world.electrons().size() + m_world.holes().size());
+        if (nc == 0 || m_o.size() < (size_t)(m_offset + nc)) return 0;
+        if (!m_ctx64) {
+            lgm_config cfg = m_cfg;
+            cfg.precision = LGM_PREC_FP64;
+            m_status = lgm_create(&cfg, m_device, &m_ctx64);
+            if (m_status != LGM_OK) {
+                m_error = lgm_last_error(nullptr);
+                return -1;
+            }
+        }
+        std::vector<int32_t> tgt(2 * (size_t)nc);
+        for (int i = 0; i < nc; ++i) {
+            tgt[i] = m_s[i];
+            tgt[nc + i] = m_s[m_offset + i];
+        }
+        std::vector<double> cpu(tgt.size());
+        m_status = lgm_potentials(m_ctx64, m_kind, LGM_TERM_DIRECT, m_s.data(), m_q.data(),
+                                  m_offset, tgt.data(), (int32_t)tgt.size(), cpu.data());
+        if (m_status != LGM_OK) {
+            m_error = lgm_last_error(m_ctx64);
+            return -1;
+        }
+        auto pdiff = [](double gpu, double cpu) {
+            return std::fabs(gpu - cpu) / (0.5 * (std::fabs(cpu) + std::fabs(gpu))) * 100.0;
+        };
+        int failed = 0;
+        for (int i = 0; i < nc; ++i) {
+            const double q = m_q[i];
+            const double self = m_cfg.electrostatic_prefactor * q;  // iR[1][0][0] = 1
+            CoulombComparison c;
+            c.openclID = i;
+            c.gpu1 = m_o[i];
+            c.gpu2 = m_o[m_offset + i] - self;
+            c.cpu1 = cpu[i];
+            c.cpu2 = cpu[nc + i] - self;
+            c.gpu = q * (c.gpu2 - c.gpu1);
+            c.cpu = q * (c.cpu2 - c.cpu1);
+            c.failed = (c.gpu - c.cpu) > 1e-4 || pdiff(c.gpu1, c.cpu1) > 1e-4 ||
+                       pdiff(c.gpu2, c.cpu2) > 1e-4;
+            failed += c.failed;
+            if (out) out->push_back(c);
+        }
+        return failed;
+    }
 
     lgm_status lastStatus() const { return m_status; }
     const std::string& lastError() const { return m_error; }
@@ -134,6 +207,7 @@ private:
     }
 
     void launch2(lgm_kind kind) {
+        m_kind = kind;
         const int n = pack(true);
         m_o.assign(m_s.size(), 0.0);
         m_status = lgm_coulomb_kernel2(m_ctx, kind, m_s.data(), m_q.data(), n, (int32_t)m_s.size(),
@@ -151,6 +225,10 @@ private:
 
     WorldT& m_world;
     lgm_ctx* m_ctx = nullptr;
+    lgm_ctx* m_ctx64 = nullptr;  // FP64 sums for compareHostAndDeviceForAllCarriers
+    lgm_config m_cfg{};
+    int m_device = -1;
+    lgm_kind m_kind = LGM_POINT;
     std::vector<int32_t> m_s, m_q;
     std::vector<double> m_o;
     int m_offset = 0;

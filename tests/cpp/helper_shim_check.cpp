@@ -3,8 +3,11 @@
 // kernel-2 launch, and the getOutputHost / getOutputHostFuture accessors.
 // Input on stdin: X Y Z cutoff ne nh nd defects_charge, then ne+nh lines
 // "site future_site", then nd defect sites.  Output: okCL, status, then one
-// line per carrier: opencl_id p_current p_future.
+// line per carrier: opencl_id p_current p_future.  With --compare, instead
+// compareHostAndDeviceForAllCarriers: "failed N", then per carrier
+// "opencl_id gpu1 gpu2 cpu1 cpu2 gpu cpu failed".
 #include <cstdio>
+#include <string>
 #include <vector>
 
 #include "langmuir_b200_helper.hpp"
@@ -34,7 +37,8 @@ struct World {
     std::vector<int>& defectSiteIDs() { return d; }
 };
 
-int main() {
+int main(int argc, char** argv) {
+    const bool compare = argc > 1 && std::string(argv[1]) == "--compare";
     World w{};
     int ne, nh, nd;
     if (std::scanf("%d %d %d %d %d %d %d %d", &w.p.gridX, &w.p.gridY, &w.p.gridZ,
@@ -67,6 +71,19 @@ int main() {
     if (helper.lastStatus() != LGM_OK) {
         std::printf("error %s\n", helper.lastError().c_str());
         return 1;
+    }
+    if (compare) {
+        std::vector<langmuir_b200::OpenClHelper<World>::CoulombComparison> cmp;
+        const int failed = helper.compareHostAndDeviceForAllCarriers(&cmp);
+        std::printf("failed %d\n", failed);
+        if (failed < 0) {
+            std::printf("error %s\n", helper.lastError().c_str());
+            return 1;
+        }
+        for (const auto& c : cmp)
+            std::printf("%d %.17g %.17g %.17g %.17g %.17g %.17g %d\n", c.openclID, c.gpu1, c.gpu2,
+                        c.cpu1, c.cpu2, c.gpu, c.cpu, (int)c.failed);
+        return 0;
     }
     for (Charge& c : store)
         std::printf("%d %.17g %.17g\n", c.id, helper.getOutputHost(c.id),

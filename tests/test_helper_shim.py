@@ -22,11 +22,12 @@ def shim_exe(tmp_path_factory):
     return out
 
 
-def run_shim(exe, X, Y, Z, c, e, ef, h, hf, d, dq):
+def run_shim(exe, X, Y, Z, c, e, ef, h, hf, d, dq, *args):
     lines = [f"{X} {Y} {Z} {c} {len(e)} {len(h)} {len(d)} {dq}"]
     lines += [f"{s} {f}" for s, f in zip(list(e) + list(h), list(ef) + list(hf))]
     lines += [str(s) for s in d]
-    p = subprocess.run([exe], input="\n".join(lines) + "\n", capture_output=True, text=True)
+    p = subprocess.run([exe, *args], input="\n".join(lines) + "\n", capture_output=True,
+                       text=True)
     return p.returncode, p.stdout
 
 
@@ -63,3 +64,46 @@ def test_shim_kernel2_matches_oracle(shim_exe, oracle_mod):
         assert int(oid) == i
         assert abs(float(p1) - want1[i]) <= 1e-6 * n1[i] + 1e-13
         assert abs(float(p2) - want2[i]) <= 1e-6 * n2[i] + 1e-13
+
+
+@pytest.mark.gpu
+def test_shim_compare_host_and_device(shim_exe, oracle_mod):
+    """compareHostAndDeviceForAllCarriers (openclhelper.cpp:546-558 with
+    chargeagent.cpp:298-370): the FP64 side equals the oracle, the GPU side is
+    the kernel-2 output, and each carrier's flag is the reference's rule."""
+    X, Y, Z, c = 40, 36, 6, 25
+    rng = np.random.default_rng(9)
+    orc = oracle_mod.Oracle(X, Y, Z, cutoff=c)
+    sites = rng.choice(X * Y * Z, 300, replace=False)
+    e, h, d = sites[:140], sites[140:290], sites[290:]
+    ef = [int(rng.choice(orc.neighbors(int(s)))) for s in e]
+    hf = [int(rng.choice(orc.neighbors(int(s)))) for s in h]
+    rc, out = run_shim(shim_exe, X, Y, Z, c, e, ef, h, hf, d, -1, "--compare")
+    assert rc == 0, out
+    rows = out.strip().splitlines()
+    assert rows[0] == "okCL 1 use 1 status 0"
+    failed = int(rows[1].split()[1])
+    src = np.concatenate([e, h, d]).astype(np.int32)
+    q = np.concatenate([-np.ones(140), np.ones(150), -np.ones(10)]).astype(np.int32)
+    cur = np.concatenate([e, h]).astype(np.int32)
+    fut = np.array(ef + hf, dtype=np.int32)
+    pref = N.default_config().electrostatic_prefactor
+    self_term = pref * q[:290]
+    want1 = orc.potentials(src, q, cur)
+    want2 = orc.potentials(src, q, fut) - self_term
+    n1, n2 = orc.potentials(src, np.abs(q), cur), orc.potentials(src, np.abs(q), fut)
+    vals = np.array([[float(x) for x in r.split()] for r in rows[2:]])
+    assert len(vals) == 290 and np.array_equal(vals[:, 0], np.arange(290))
+    gpu1, gpu2, cpu1, cpu2, gpu, cpu, flag = vals[:, 1:].T
+    np.testing.assert_allclose(cpu1, want1, rtol=0, atol=1e-12 * n1.max())
+    np.testing.assert_allclose(cpu2, want2, rtol=0, atol=1e-12 * n2.max())
+    assert np.all(np.abs(gpu1 - want1) <= 1e-6 * n1 + 1e-13)
+    assert np.all(np.abs(gpu2 - want2) <= 1e-6 * n2 + 1e-13)
+    np.testing.assert_allclose(gpu, q[:290] * (gpu2 - gpu1), rtol=1e-15, atol=1e-15)
+
+    def pdiff(a, b):
+        with np.errstate(invalid="ignore", divide="ignore"):
+            return np.abs(a - b) / (0.5 * (np.abs(b) + np.abs(a))) * 100.0
+    rule = ((gpu - cpu) > 1e-4) | (pdiff(gpu1, cpu1) > 1e-4) | (pdiff(gpu2, cpu2) > 1e-4)
+    assert np.array_equal(flag.astype(bool), rule)
+    assert failed == int(rule.sum())
