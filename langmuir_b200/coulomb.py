@@ -158,24 +158,36 @@ class OpenClHelper:
         self.ok_cl = False
         self.use_opencl = False
         self._ctx = None
+        self._ctx64 = None
         self._o = np.zeros(0, dtype=np.float64)
+        self._s = np.zeros(0, dtype=np.int32)
+        self._q = np.zeros(0, dtype=np.int32)
+        self._kind = N.POINT
         self._offset = 0
 
     # openclhelper.cpp:17-187
     def initializeOpenCL(self, gpuID=-1):
         p = self.world.parameters
         self.ok_cl = False
+        for ctx in (self._ctx, self._ctx64):
+            if ctx is not None:
+                ctx.close()
+        self._ctx = self._ctx64 = None
+        self._device = max(int(gpuID), 0)
         try:
-            self._ctx = Coulomb(p["grid.x"], p["grid.y"], p["grid.z"],
-                                cutoff=p.get("electrostatic.cutoff", 50),
-                                prefactor=p.get("electrostatic.prefactor"),
-                                sigma=p.get("coulomb.gaussian.sigma", 0.0),
-                                device=max(int(gpuID), 0))
+            self._ctx = Coulomb(**self._context_args(), device=self._device)
         except (N.LgmError, ImportError):
             if p.get("use.opencl", False):
                 raise
             return
         self.ok_cl = True
+
+    def _context_args(self):
+        p = self.world.parameters
+        return dict(grid_x=p["grid.x"], grid_y=p["grid.y"], grid_z=p["grid.z"],
+                    cutoff=p.get("electrostatic.cutoff", 50),
+                    prefactor=p.get("electrostatic.prefactor"),
+                    sigma=p.get("coulomb.gaussian.sigma", 0.0))
 
     # openclhelper.cpp:190-218
     def toggleOpenCL(self, on: bool) -> bool:
@@ -205,7 +217,8 @@ class OpenClHelper:
                 s.append(c.future_site); q.append(c.charge)
             for c in w.holes:
                 s.append(c.future_site); q.append(c.charge)
-        return _i32(s), _i32(q)
+        self._s, self._q = _i32(s), _i32(q)
+        return self._s, self._q
 
     def _require(self):
         if self._ctx is None:
@@ -214,11 +227,13 @@ class OpenClHelper:
     def launchCoulombKernel2(self):
         self._require()
         s, q = self._pack(True)
+        self._kind = N.POINT
         self._o = self._ctx.kernel2(s, q, self._offset, N.POINT)
 
     def launchGaussKernel2(self):
         self._require()
         s, q = self._pack(True)
+        self._kind = N.GAUSS
         self._o = self._ctx.kernel2(s, q, self._offset, N.GAUSS)
 
     def launchCoulombKernel1(self):
@@ -236,3 +251,46 @@ class OpenClHelper:
 
     def getOutputHostFuture(self, index: int) -> float:
         return float(self._o[index + self._offset])
+
+    # openclhelper.cpp:560-565: one entry of the host site and charge mirrors
+    # (the next launch packs them from the world again, as the reference does)
+    def copySiteAndChargeToHostVector(self, index: int, site: int, charge: int = -1):
+        if index >= len(self._s):
+            self._s = np.resize(self._s, index + 1)
+            self._q = np.resize(self._q, index + 1)
+        self._s[index] = site
+        self._q[index] = charge
+
+    # openclhelper.cpp:546-558 and ChargeAgent::compareCoulomb
+    # (chargeagent.cpp:298-370)
+    def compareHostAndDeviceForAllCarriers(self):
+        """Every carrier's potentials from the last kernel-2 launch against
+        FP64 sums over the same sources (a second context in FP64, made on the
+        first call).  A carrier fails when its energy change differs by more
+        than 1e-4 (signed, as the reference tests it) or either potential by
+        more than 1e-4 percent.  Returns (number failed, per-carrier rows
+        (gpu1, gpu2, cpu1, cpu2, gpu, cpu, failed) in opencl_id order), where
+        the reference prints each comparison."""
+        self._require()
+        nc = len(self.world.electrons) + len(self.world.holes)
+        if nc == 0 or len(self._o) < self._offset + nc:
+            return 0, []
+        if self._ctx64 is None:
+            self._ctx64 = Coulomb(**self._context_args(), device=self._device,
+                                  precision=N.PREC_FP64)
+        src, q = self._s[: self._offset], self._q[: self._offset]
+        tgt = np.concatenate([self._s[:nc], self._s[self._offset: self._offset + nc]])
+        cpu = self._ctx64.potentials(src, q, tgt, self._kind)
+        selfterm = self._ctx.prefactor * self._q[:nc].astype(np.float64)  # iR[1][0][0] = 1
+        gpu1 = self._o[:nc]
+        gpu2 = self._o[self._offset: self._offset + nc] - selfterm
+        cpu1, cpu2 = cpu[:nc], cpu[nc:] - selfterm
+        qd = self._q[:nc].astype(np.float64)
+        gpu, cpuv = qd * (gpu2 - gpu1), qd * (cpu2 - cpu1)
+
+        def pdiff(a, b):
+            with np.errstate(invalid="ignore", divide="ignore"):
+                return np.abs(a - b) / (0.5 * (np.abs(b) + np.abs(a))) * 100.0
+        failed = ((gpu - cpuv) > 1e-4) | (pdiff(gpu1, cpu1) > 1e-4) | (pdiff(gpu2, cpu2) > 1e-4)
+        rows = list(zip(gpu1, gpu2, cpu1, cpu2, gpu, cpuv, failed))
+        return int(failed.sum()), rows

@@ -310,6 +310,25 @@ def test_openclhelper_mirror_matches_coulomb_cpu(lgm, oracle_mod):
         assert abs(de_gpu - de_cpu[i]) <= 1e-4
         assert abs(g1 - p1[i]) <= TOL32 * n1[i] + 1e-13
         assert abs(g2 - p2[i]) <= TOL32 * n2[i] + 1e-13
+    # compareHostAndDeviceForAllCarriers: its FP64 side is the oracle's sum, its
+    # GPU side the launch's output, its flags the reference's rule
+    nfail, rows = helper.compareHostAndDeviceForAllCarriers()
+    gpu1, gpu2, cpu1, cpu2, gpu, cpu, flag = (np.array(c) for c in zip(*rows))
+    q_src = np.concatenate([-np.ones(300), np.ones(380), np.ones(20)]).astype(np.int32)
+    qc = q_src[:680].astype(np.float64)
+    pref = helper._ctx.prefactor
+    want1 = orc.potentials(s_src, q_src, np.concatenate([e_site, h_site]))
+    want2 = orc.potentials(s_src, q_src, np.concatenate([e_f, h_f])) - pref * qc
+    np.testing.assert_allclose(cpu1, want1, rtol=0, atol=1e-12 * n1.max())
+    np.testing.assert_allclose(cpu2, want2, rtol=0, atol=1e-12 * n2.max())
+    ids = [ch.opencl_id for ch in w.electrons + w.holes]
+    assert np.array_equal(gpu1, [helper.getOutputHost(i) for i in ids])
+    assert np.array_equal(gpu2, [helper.getOutputHostFuture(i) - pref * qc[i] for i in ids])
+    with np.errstate(invalid="ignore", divide="ignore"):
+        rule = (((gpu - cpu) > 1e-4) | (np.abs(gpu1 - cpu1) / (0.5 * (np.abs(cpu1) + np.abs(gpu1)))
+                                        * 100.0 > 1e-4)
+                | (np.abs(gpu2 - cpu2) / (0.5 * (np.abs(cpu2) + np.abs(gpu2))) * 100.0 > 1e-4))
+    assert np.array_equal(flag.astype(bool), rule) and nfail == int(rule.sum())
 
 
 # ---- full-size configuration: parity and size-independent properties --------------------
