@@ -339,8 +339,9 @@ lgm_status prep(lgm_ctx* c, unsigned terms, const int32_t* d_src, const int32_t*
 // CTAs of one launch do uneven work (tiles near few charges, image tiles far
 // from the electrode skip most sources), and three waves of smaller CTAs let
 // the block scheduler even it out; more waves cost more in the FP64 partials
-// that finalize sums than they save (cfg2 step: 1 wave 0.647 ms, 3 waves
-// 0.607 ms, 8 waves 0.614 ms).
+// that finalize sums than they save (256x256x16 lattice, 20,970 charges,
+// images at both electrodes: 1 wave 0.647 ms, 3 waves 0.607 ms, 8 waves
+// 0.614 ms per call).
 constexpr int kSplitWaves = 3;
 int splits_for(const lgm_ctx* c, int v, int fi, const Shape& sh, int* tiles_out) {
     const Variant& V = kVariants[v];
