@@ -48,7 +48,7 @@ FLOP_PER_PAIR = 11
 FLOP_PER_TEST = 8
 FLOP_PER_CONTRIB = 3
 # DRAM bytes per launch of the pair kernel from one ncu capture of this
-# workload (profiles/pair_kernel_cfg2.md): dram__bytes_read + dram__bytes_write.
+# workload: dram__bytes_read.sum + dram__bytes_write.sum.
 PAIR_KERNEL_DRAM_BYTES = 2878976
 
 

@@ -158,9 +158,16 @@ lgm_status lgm_coulomb_kernel1_async(lgm_ctx* ctx, lgm_kind kind, const int32_t*
  * device and returns when the result is in d_o, with LGM_ERR_OUT_OF_RANGE
  * for a site outside the lattice.
  *
- * The first call on a device looks up the array's device address and caches
- * it; make that first call before any stream capture.  All calls share the
- * array, so calls that overlap on the GPU race: serialize them. */
+ * Each call waits for its own work before it returns: it reads the device
+ * error word back on `stream`.  A leftover error of the caller's earlier CUDA
+ * work is neither reported as this call's nor cleared.
+ *
+ * Set-up: the first call in a CUDA context (the primary context of the
+ * current device, or a driver context the caller made current) looks up the
+ * array's device address in that context and caches it under the context's
+ * unique id; make that first call before any stream capture begins.  After
+ * cudaDeviceReset the new primary context gets its own set-up.  All calls
+ * share the array, so calls that overlap on the GPU race: serialize them. */
 #define LGM_NOALLOC_MAX_SOURCES 32768
 #define LGM_NOALLOC_MAX_TARGETS 65536
 #define LGM_NOALLOC_SCRATCH_BYTES 4456704

@@ -73,7 +73,17 @@ typedef struct lgm_params {
      *   generation.interface: excitons split across a random donor-acceptor bond */
     int32_t morphology_confine;
     int32_t generation_interface;
+    /* Not an input key: the width of the FP64 guard band of the Metropolis
+     * decisions, relative to the error scale N of the decision's two
+     * potentials.  A decision whose FP32C energy lies within
+     * guard_band * (N_current + N_future) of its acceptance threshold is taken
+     * again from FP64 sums.  Default LGM_GUARD_BAND_MIN, the smallest width
+     * that covers the FP32C error bound (lgm_params_check rejects less); a
+     * wider band sends more decisions through the FP64 re-evaluation, which
+     * tests use to exercise it. */
+    double guard_band;
 } lgm_params;
+#define LGM_GUARD_BAND_MIN 8e-6
 
 void lgm_params_default(lgm_params* p);
 /* sizeof(lgm_params), for bindings that declare the struct themselves. */

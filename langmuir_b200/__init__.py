@@ -8,8 +8,8 @@ missing: there is no CPU fallback.
 from ._native import (GAUSS, PATH_RSQRT, PATH_TABLE, POINT, PREC_FP32C, PREC_FP64,
                       TERM_DIRECT, TERM_IMAGE_LEFT, TERM_IMAGE_RIGHT, LgmError)
 from .coulomb import Carrier, Coulomb, OpenClHelper
-from .kmc import KMC, KMCBatch, Params
+from .kmc import GUARD_BAND_MIN, KMC, KMCBatch, Params
 
-__all__ = ["Coulomb", "OpenClHelper", "Carrier", "KMC", "KMCBatch", "Params", "LgmError", "POINT", "GAUSS", "PREC_FP32C",
+__all__ = ["GUARD_BAND_MIN", "Coulomb", "OpenClHelper", "Carrier", "KMC", "KMCBatch", "Params", "LgmError", "POINT", "GAUSS", "PREC_FP32C",
            "PREC_FP64", "PATH_RSQRT", "PATH_TABLE", "TERM_DIRECT", "TERM_IMAGE_LEFT",
            "TERM_IMAGE_RIGHT"]

@@ -6,6 +6,7 @@ with the source tree.  nvcc cross-compiles without a GPU.
 """
 from __future__ import annotations
 
+import concurrent.futures
 import glob
 import os
 import subprocess
@@ -40,13 +41,18 @@ def build(force: bool = False, verbose_ptxas: bool = False) -> str:
         return LIB
     os.makedirs(OUT_DIR, exist_ok=True)
     objs = []
+    cmds = []
     for src in sources():
         obj = os.path.join(OUT_DIR, os.path.basename(src) + ".o")
         cmd = ["nvcc", *ARCH, *NVCC_FLAGS, "-c", src, "-o", obj]
         if verbose_ptxas and src.endswith(".cu"):
             cmd.insert(1, "-Xptxas=-v")
-        subprocess.run(cmd, check=True)
+        cmds.append(cmd)
         objs.append(obj)
+    # one nvcc per source file, side by side
+    with concurrent.futures.ThreadPoolExecutor(max_workers=max(1, os.cpu_count() or 1)) as ex:
+        for f in [ex.submit(subprocess.run, c, check=True) for c in cmds]:
+            f.result()
     tmp = LIB + ".tmp"
     subprocess.run(["nvcc", *ARCH, "-shared", "-o", tmp, *objs, "-lcudart"], check=True)
     os.replace(tmp, LIB)

@@ -57,9 +57,9 @@ enum { I_NE = 0, I_NH, I_STEP, I_NFLAG, I_REMOVED, I_NE0, I_NH0, I_NCHUNK, I_TPH
 constexpr uint32_t RNG_RECOMB = 5, RNG_EXCITON = RNG_SOURCE + 4;
 
 // Guard band: FP32C potentials carry at most (2 ulp rsqrt + 31 u run sums)
-// ~ 2.1e-6 N of error each; a decision whose energy lies within kGuard*(N_c +
-// N_f) of the threshold is redone in FP64.
-constexpr double kGuard = 8e-6;
+// ~ 2.1e-6 N of error each; a decision whose energy lies within
+// guard*(N_c + N_f) of the threshold is redone in FP64, with guard =
+// lgm_params::guard_band >= LGM_GUARD_BAND_MIN (8e-6).
 
 constexpr int kNT = 128, kRP = 4, kSUB = 32;
 constexpr int kTile = kNT * 2 * kRP;
@@ -69,6 +69,7 @@ struct Dev {
     int cap_e, cap_h, nd, dq;
     uint32_t seed, replica;
     double beta, exciton_binding, sI100, prefactor, erffactor;
+    double guard;  // guard band width relative to N (lgm_params::guard_band)
     double coupling[27];
     double rate_src[4], rate_drain[4];  // eL eR hL hR
     int coulomb, gauss;
@@ -372,7 +373,7 @@ __device__ __forceinline__ void decide_body(const Dev& D, const int i) {
             pd += de;
             if (u < c) {
                 const double tau = log(c / u) / D.beta;
-                const double g = kGuard * (D.Nt[i] + D.Nt[t + i]) + 1e-12 * (1.0 + fabs(pd));
+                const double g = D.guard * (D.Nt[i] + D.Nt[t + i]) + 1e-12 * (1.0 + fabs(pd));
                 if (fabs(pd - tau) <= g) flag = true;
                 else acc = pd < tau;
             }
@@ -1007,6 +1008,7 @@ struct lgm_kmc {
     float* gtab = nullptr;
     int gtab_k = 0;
     int pair_blocks = 0, pair_tiles = 0;
+    int sm_count = 0;   // SMs of the device (the guard's grid)
     std::string err;
 };
 
@@ -1288,7 +1290,7 @@ lgm_status enqueue_step(lgm_kmc* k) {
         k_finalize<<<(2 * nc + blk - 1) / blk, blk, 0, st>>>(D);
     }
     k_decide<<<(nc + blk - 1) / blk, blk, 0, st>>>(D);
-    if (D.coulomb) k_guard<<<2 * 148, kGuardThreads, 0, st>>>(D);
+    if (D.coulomb) k_guard<<<2 * k->sm_count, kGuardThreads, 0, st>>>(D);
     if (D.solar && D.rec_rate > 0) {
         k_hmap<<<(nc + blk - 1) / blk, blk, 0, st>>>(D);
         k_recomb_propose<<<(nc + blk - 1) / blk, blk, 0, st>>>(D);
@@ -1362,6 +1364,7 @@ static lgm_status kmc_create_impl(const lgm_params* pin, int32_t device, uint32_
     D.seed = (uint32_t)(p.random_seed & 0xffffffffu); D.replica = replica;
     D.beta = p.inverse_kt; D.exciton_binding = p.exciton_binding;
     D.prefactor = p.electrostatic_prefactor;
+    D.guard = p.guard_band;
     D.erffactor = p.coulomb_gaussian_sigma > 0 ? 1.0 / (std::sqrt(2.0) * p.coulomb_gaussian_sigma) : 0.0;
     D.gauss = p.coulomb_gaussian_sigma > 0;
     // sI[1][0][0] = prefactor * iR * eR at r = 1 (potential.cpp:311-323)
@@ -1448,6 +1451,7 @@ static lgm_status kmc_create_impl(const lgm_params* pin, int32_t device, uint32_
     int bps = 1;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, kmc_pair(D.gauss), kNT, pair_smem_bytes(64));
     // three waves of resident CTAs, as for the single pair sums (lgm_api.cu)
+    k->sm_count = n_sms;
     D.splits = std::max(1, std::min({64, 3 * n_sms * std::max(1, bps) / k->pair_tiles,
                                      D.src_cap / CH}));
     lgm_status st;

@@ -9,16 +9,21 @@
 // file-scope device array of fixed size, loaded with the library and held
 // by every GPU that loads it until the process exits.
 //
-// Set-up: the first call on a device looks up the array's device address
-// with cudaGetSymbolAddress (the array's name is only a host-side stand-in;
-// a kernel given that name from host code would read the wrong memory) and
-// caches it per device.  Make that first call before any stream capture.
+// Set-up: the array's name is only a host-side stand-in (a kernel given that
+// name from host code would read the wrong memory), so the first call in a
+// CUDA context looks up the array's device address in that context with
+// cudaGetSymbolAddress and caches it under the context's unique id
+// (cuCtxGetId).  A call in another context -- a driver context the caller
+// made current, or the primary context created anew after cudaDeviceReset --
+// does its own set-up.  Make the first call in a context before any stream
+// capture begins.
 //
 // Every call shares the array and leaves the previous call's contents in
 // it; the error word is cleared at the start of each call, everything else
 // is fully written before it is read.  Calls that overlap on the GPU (two
 // streams, two host threads, two devices' worth of work aimed at one device)
 // race on the array: serialize them.
+#include <cuda.h>  // CUcontext and the driver entry points' types (no link to libcuda)
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -54,42 +59,106 @@ static_assert(kScratchBytes == LGM_NOALLOC_SCRATCH_BYTES, "header states the scr
 // the address obtained from cudaGetSymbolAddress.
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 
-struct DeviceSetup {
-    bool ready = false;
-    unsigned char* base = nullptr;   // device address of g_noalloc_scratch
+struct ContextSetup {
+    unsigned long long ctx_id = 0;   // cuCtxGetId of the context the entry was set up in
+    unsigned char* base = nullptr;   // device address of g_noalloc_scratch in that context
     int sm_count = 0;
     int blocks_per_sm = 0;
 };
-constexpr int kMaxDevices = 64;
-DeviceSetup g_setup[kMaxDevices];
+constexpr int kMaxContexts = 64;
+ContextSetup g_setup[kMaxContexts];
+int g_setup_count = 0;
+int g_setup_next = 0;                // slot replaced when every slot is taken
 std::mutex g_setup_mutex;
 
 using NalPairFn = void (*)(PairArgs);
 constexpr NalPairFn kNalPair = &pair_kernel<0, 0, kNalThreads, kNalRP, kNalSub>;
 
-// Once per device, with that device current.
-lgm_status setup_device(int dev, DeviceSetup** out) {
-    std::lock_guard<std::mutex> lock(g_setup_mutex);
-    DeviceSetup& s = g_setup[dev];
-    if (!s.ready) {
-        int major = 0;
-        if (cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev) != cudaSuccess ||
-            major != 10)
-            return LGM_ERR_NO_DEVICE;
+// The driver's cuCtxGetCurrent and cuCtxGetId, found through the runtime so
+// that the library does not link libcuda itself.
+typedef CUresult(CUDAAPI* CtxGetCurrentFn)(CUcontext*);
+typedef CUresult(CUDAAPI* CtxGetIdFn)(CUcontext, unsigned long long*);
+struct DriverFns {
+    CtxGetCurrentFn get_current = nullptr;
+    CtxGetIdFn get_id = nullptr;
+};
+const DriverFns& driver_fns() {
+    static const DriverFns fns = [] {
+        DriverFns f;
         void* p = nullptr;
-        if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || p == nullptr)
-            return LGM_ERR_CUDA;
-        if (cudaDeviceGetAttribute(&s.sm_count, cudaDevAttrMultiProcessorCount, dev) !=
-            cudaSuccess)
-            return LGM_ERR_CUDA;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&s.blocks_per_sm, kNalPair, kNalThreads,
-                                                          pair_smem_bytes(0)) != cudaSuccess)
-            return LGM_ERR_CUDA;
-        s.base = static_cast<unsigned char*>(p);
-        s.ready = true;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            f.get_current = reinterpret_cast<CtxGetCurrentFn>(p);
+        p = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetId", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            f.get_id = reinterpret_cast<CtxGetIdFn>(p);
+        return f;
+    }();
+    return fns;
+}
+
+// The unique id of the calling thread's current context on `dev`.  With no
+// context current yet, the device's primary context is made current first
+// (cudaSetDevice initialises it); a context the caller made current is kept.
+lgm_status current_context_id(int dev, unsigned long long* id) {
+    const DriverFns& f = driver_fns();
+    if (!f.get_current || !f.get_id) return LGM_ERR_NO_DEVICE;
+    CUcontext ctx = nullptr;
+    if (f.get_current(&ctx) != CUDA_SUCCESS) return LGM_ERR_CUDA;
+    if (!ctx) {
+        if (cudaSetDevice(dev) != cudaSuccess) return LGM_ERR_CUDA;
+        if (f.get_current(&ctx) != CUDA_SUCCESS || !ctx) return LGM_ERR_CUDA;
     }
-    *out = &s;
+    return f.get_id(ctx, id) == CUDA_SUCCESS ? LGM_OK : LGM_ERR_CUDA;
+}
+
+// Once per context, with that context current on `dev`.
+lgm_status setup_context(int dev, ContextSetup* out) {
+    unsigned long long id = 0;
+    lgm_status st = current_context_id(dev, &id);
+    if (st != LGM_OK) return st;
+    std::lock_guard<std::mutex> lock(g_setup_mutex);
+    for (int i = 0; i < g_setup_count; ++i)
+        if (g_setup[i].ctx_id == id) {
+            *out = g_setup[i];
+            return LGM_OK;
+        }
+    int major = 0;
+    if (cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev) != cudaSuccess ||
+        major != 10)
+        return LGM_ERR_NO_DEVICE;
+    ContextSetup s;
+    s.ctx_id = id;
+    void* p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || p == nullptr)
+        return LGM_ERR_CUDA;
+    s.base = static_cast<unsigned char*>(p);
+    if (cudaDeviceGetAttribute(&s.sm_count, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+        return LGM_ERR_CUDA;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&s.blocks_per_sm, kNalPair, kNalThreads,
+                                                      pair_smem_bytes(0)) != cudaSuccess)
+        return LGM_ERR_CUDA;
+    int slot = g_setup_count;
+    if (slot < kMaxContexts) {
+        ++g_setup_count;
+    } else {
+        slot = g_setup_next;
+        g_setup_next = (g_setup_next + 1) % kMaxContexts;
+    }
+    g_setup[slot] = s;
+    *out = s;
     return LGM_OK;
+}
+
+// A launch whose own status is returned (a leftover error of the caller's
+// earlier work is neither reported as this entry's nor cleared).
+template <class... Args>
+cudaError_t launch(void (*kern)(Args...), dim3 grid, dim3 block, size_t smem, cudaStream_t st,
+                   Args... args) {
+    void* argv[] = {static_cast<void*>(&args)...};
+    return cudaLaunchKernel(reinterpret_cast<const void*>(kern), grid, block, argv, smem, st);
 }
 
 __global__ void nal_prep_sources(const int32_t* __restrict__ s, const int32_t* __restrict__ q,
@@ -157,46 +226,55 @@ extern "C" lgm_status lgm_coulomb_kernel2_noalloc(int32_t grid_x, int32_t grid_y
     if (total == 0) return LGM_OK;
     if (!d_s || !d_q || !d_o) return LGM_ERR_INVALID_ARGUMENT;
     int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices)
-        return LGM_ERR_NO_DEVICE;
-    DeviceSetup* S = nullptr;
-    lgm_status st = setup_device(dev, &S);
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0) return LGM_ERR_NO_DEVICE;
+    ContextSetup S;
+    lgm_status st = setup_context(dev, &S);
     if (st != LGM_OK) return st;
 
     cudaStream_t cs = static_cast<cudaStream_t>(stream);
-    float4* geo = reinterpret_cast<float4*>(S->base + kGeoOff);
-    float2* qq = reinterpret_cast<float2*>(S->base + kQqOff);
-    float4* tgt = reinterpret_cast<float4*>(S->base + kTgtOff);
-    double* part = reinterpret_cast<double*>(S->base + kPartOff);
-    unsigned* err = reinterpret_cast<unsigned*>(S->base + kErrOff);
+    float4* geo = reinterpret_cast<float4*>(S.base + kGeoOff);
+    float2* qq = reinterpret_cast<float2*>(S.base + kQqOff);
+    float4* tgt = reinterpret_cast<float4*>(S.base + kTgtOff);
+    double* part = reinterpret_cast<double*>(S.base + kPartOff);
+    unsigned* err = reinterpret_cast<unsigned*>(S.base + kErrOff);
     const int XY = grid_x * grid_y, volume = XY * grid_z;
+    const int t_phys = (total + 63) / 64 * 64;
 
     if (cudaMemsetAsync(err, 0, sizeof(unsigned), cs) != cudaSuccess) return LGM_ERR_CUDA;
+    // The target records, with the range check of every target, also when
+    // there are no sources (the potentials are then all zero).
+    if (launch(nal_prep_targets, dim3((t_phys + 255) / 256), dim3(256), 0, cs,
+               d_s, (int)total, t_phys, (int)grid_x, (int)grid_y, XY, volume, tgt, err) !=
+        cudaSuccess)
+        return LGM_ERR_CUDA;
     if (n == 0) {
         if (cudaMemsetAsync(d_o, 0, sizeof(double) * total, cs) != cudaSuccess) return LGM_ERR_CUDA;
-        return cudaStreamSynchronize(cs) == cudaSuccess ? LGM_OK : LGM_ERR_CUDA;
+    } else {
+        const int n_pad = (n + CH - 1) / CH * CH;
+        const int n_chunks = n_pad / CH;
+        const int tiles = (t_phys + kNalTile - 1) / kNalTile;
+        const int splits = std::max(
+            1, std::min({kNalMaxSplits, S.sm_count * std::max(1, S.blocks_per_sm) / tiles,
+                         n_chunks}));
+        if (launch(nal_prep_sources, dim3((n_pad + 255) / 256), dim3(256), 0, cs, d_s, d_q,
+                   (int)n, n_pad, (int)grid_x, (int)grid_y, XY, volume, geo, qq, err) !=
+            cudaSuccess)
+            return LGM_ERR_CUDA;
+        PairArgs A;
+        A.geo = geo; A.qq = qq; A.n_chunks = n_chunks; A.splits = splits;
+        A.tgt = tgt; A.t_phys = t_phys; A.part = part;
+        A.c2 = (float)(cutoff * cutoff);
+        A.tab = nullptr; A.tab_k = 0;  // point charges, MUFU path: no table
+        A.err = err;
+        if (launch(kNalPair, dim3(tiles, splits), dim3(kNalThreads), pair_smem_bytes(0), cs, A) !=
+                cudaSuccess ||
+            launch(nal_finalize, dim3((total + 255) / 256), dim3(256), 0, cs,
+                   (const double*)part, splits, t_phys, (int)total, prefactor, d_o) != cudaSuccess)
+            return LGM_ERR_CUDA;
     }
-    const int n_pad = (n + CH - 1) / CH * CH;
-    const int n_chunks = n_pad / CH;
-    const int t_phys = (total + 63) / 64 * 64;
-    const int tiles = (t_phys + kNalTile - 1) / kNalTile;
-    const int splits = std::max(
-        1, std::min({kNalMaxSplits, S->sm_count * std::max(1, S->blocks_per_sm) / tiles, n_chunks}));
 
-    nal_prep_sources<<<(n_pad + 255) / 256, 256, 0, cs>>>(d_s, d_q, n, n_pad, grid_x, grid_y, XY,
-                                                           volume, geo, qq, err);
-    nal_prep_targets<<<(t_phys + 255) / 256, 256, 0, cs>>>(d_s, total, t_phys, grid_x, grid_y, XY,
-                                                            volume, tgt, err);
-    PairArgs A;
-    A.geo = geo; A.qq = qq; A.n_chunks = n_chunks; A.splits = splits;
-    A.tgt = tgt; A.t_phys = t_phys; A.part = part;
-    A.c2 = (float)(cutoff * cutoff);
-    A.tab = nullptr; A.tab_k = 0;  // point charges, MUFU path: no table
-    A.err = err;
-    kNalPair<<<dim3(tiles, splits), kNalThreads, pair_smem_bytes(0), cs>>>(A);
-    nal_finalize<<<(total + 255) / 256, 256, 0, cs>>>(part, splits, t_phys, total, prefactor, d_o);
-    if (cudaGetLastError() != cudaSuccess) return LGM_ERR_CUDA;
-
+    // The call returns once its work is done: the device error word is read
+    // back on `stream`.
     unsigned h_err = 0;
     if (cudaMemcpyAsync(&h_err, err, sizeof(unsigned), cudaMemcpyDeviceToHost, cs) != cudaSuccess ||
         cudaStreamSynchronize(cs) != cudaSuccess)

@@ -224,6 +224,7 @@ void lgm_params_default(lgm_params* p) {
     p->recombination_rate = 0.0; p->recombination_range = 0;
     p->output_ids_on_encounter = 0; p->source_scale_area = 65536; p->max_threads = -1;
     p->image_charges = 0; p->site_disorder = 0.0;
+    p->guard_band = LGM_GUARD_BAND_MIN;
 }
 
 lgm_status lgm_params_parse(const char* text, lgm_params* p, char* err, int32_t err_len) {
@@ -361,6 +362,9 @@ lgm_status lgm_params_check(lgm_params* p, char* err, int32_t err_len) {
     if (p->output_ids_on_encounter) return bad("output.ids.on.encouter is deprecated");
     if (p->image_charges < 0 || p->image_charges > 3) return bad("image.charges must be 0..3");
     if (p->site_disorder < 0) return bad("site.disorder < 0");
+    if (!(p->guard_band >= LGM_GUARD_BAND_MIN) || !std::isfinite(p->guard_band))
+        return bad("guard band %g below the FP32C error bound %g", p->guard_band,
+                   LGM_GUARD_BAND_MIN);
     if (p->generation_interface && st != "solarcell")
         return bad("generation.interface == true, yet simulation.type != solarcell");
     return LGM_OK;

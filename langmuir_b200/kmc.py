@@ -19,6 +19,10 @@ from . import _native as N
 _i32 = ctypes.c_int32
 _f64 = ctypes.c_double
 
+# LGM_GUARD_BAND_MIN (langmuir_b200_kmc.h): the narrowest FP64 guard band, the
+# FP32C error bound of a decision's potentials relative to their scale N.
+GUARD_BAND_MIN = 8e-6
+
 
 class Params(ctypes.Structure):
     _fields_ = [
@@ -54,6 +58,7 @@ class Params(ctypes.Structure):
         ("electrostatic_cutoff", _i32), ("electrostatic_prefactor", _f64), ("inverse_kt", _f64),
         ("image_charges", _i32), ("site_disorder", _f64),
         ("morphology_confine", _i32), ("generation_interface", _i32),
+        ("guard_band", _f64),
     ]
 
     @classmethod

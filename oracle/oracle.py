@@ -27,11 +27,20 @@ _u32p = np.ctypeslib.ndpointer(dtype=np.uint32, flags="C_CONTIGUOUS")
 EMPTY, ELECTRON, HOLE, DEFECT, SOURCE, DRAIN = range(6)
 
 
+def reference_tree():
+    """The reference source tree the compiled-reference recipes read: the
+    REFERENCE environment variable, else the tree's usual mount point; None
+    where neither holds it (a GPU box has no copy)."""
+    path = os.environ.get("REFERENCE", "/root/reference")
+    return path if os.path.isdir(path) else None
+
+
 def build(ref: bool = False) -> None:
     """Compile the oracle (and the compiled-reference checker when ``ref``)."""
     subprocess.run(["make", "-s", "-C", HERE], check=True)
-    if ref:
-        subprocess.run(["make", "-s", "-C", HERE, "ref"], check=True)
+    tree = reference_tree()
+    if ref and tree:
+        subprocess.run(["make", "-s", "-C", HERE, "ref", f"REFERENCE={tree}"], check=True)
 
 
 _lib = None

@@ -35,5 +35,5 @@ def pytest_collection_modifyitems(config, items):
 @pytest.fixture(scope="session")
 def oracle_mod():
     from oracle import oracle as O
-    O.build(ref=os.path.isdir("/root/reference"))
+    O.build(ref=O.reference_tree() is not None)
     return O

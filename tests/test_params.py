@@ -99,7 +99,9 @@ def test_validation_messages(key, value, needle):
 
 
 def test_reference_example_inputs_parse():
-    files = sorted(glob.glob("/root/reference/examples/*.inp"))
+    from oracle import oracle as O
+    tree = O.reference_tree()
+    files = sorted(glob.glob(os.path.join(tree, "examples", "*.inp"))) if tree else []
     if not files:
         pytest.skip("reference examples not present")
     for f in files:
