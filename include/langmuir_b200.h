@@ -176,6 +176,22 @@ lgm_status lgm_coulomb_kernel2_noalloc(int32_t grid_x, int32_t grid_y, int32_t g
                                        const int32_t* d_q, int32_t n, int32_t total,
                                        double* d_o, void* stream);
 
+/* Measured arithmetic peaks of one device (no reference counterpart): the
+ * pair sums are bounded by FP32 FMA issue and by the MUFU pipe (rsqrt).  Each
+ * probe runs 8 independent chains per thread on 8 blocks of 256 threads per
+ * SM and reports the best of five launches (CUDA events): scalar FFMA and
+ * packed FFMA2 in FP32 FLOP/s (2 per FMA lane), MUFU rsqrt per second.
+ * clock_mhz_attribute is the device's clock-rate attribute (its maximum),
+ * not the clock the probe ran at. */
+typedef struct lgm_peaks {
+    double ffma_tflops;
+    double ffma2_tflops;
+    double rsqrt_per_s;
+    int32_t sm_count;
+    double clock_mhz_attribute;
+} lgm_peaks;
+lgm_status lgm_probe_peaks(int32_t device, lgm_peaks* out);
+
 /* Launch statistics of the last pair-sum launch on the context. */
 typedef struct lgm_launch_info {
     int64_t pairs_tested;      /* (physical targets) x (sources), padding excluded */
@@ -186,6 +202,8 @@ typedef struct lgm_launch_info {
     int32_t kernel_launches;   /* kernels launched by the call                      */
     float pair_kernel_ms;      /* device time of the pair kernel (timing on), else -1 */
     int32_t variant;           /* tile variant of the pair kernel, -1 if none ran   */
+    int64_t pairs_examined;    /* culled variants with counting on (lgm_set_counting):
+                                  the pairs whose r^2 the kernel computed; else -1    */
 } lgm_launch_info;
 /* Waits for the last launch when timing is on. */
 lgm_status lgm_last_launch(lgm_ctx* ctx, lgm_launch_info* info);
@@ -193,6 +211,10 @@ lgm_status lgm_last_launch(lgm_ctx* ctx, lgm_launch_info* info);
 /* Timing on: CUDA events on the launch stream bracket the pair kernel of
  * every call, read back by lgm_last_launch. */
 lgm_status lgm_set_timing(lgm_ctx* ctx, int32_t enable);
+/* Counting on: culled pair sums count the pairs they examine (one atomic add
+ * per warp and live source chunk), read back by lgm_last_launch as
+ * pairs_examined.  A measurement aid: leave it off in timed runs. */
+lgm_status lgm_set_counting(lgm_ctx* ctx, int32_t enable);
 
 /* ---- tile autotuner --------------------------------------------------------
  * The pair kernel is compiled in several tile shapes (threads per CTA, target
@@ -214,6 +236,14 @@ lgm_status lgm_variant_info(int32_t variant, int32_t* threads, int32_t* target_p
  * that no pair of its targets has inside the cutoff; r^2 is still tested for
  * every pair and the sums are unchanged. */
 #define LGM_VARIANT_WARP_SKIP 1
+/* LGM_VARIANT_CULLED: the sources are sorted by lattice cell as well; each
+ * source chunk (128 sources) and each group of 32 gets a bounding box, a cull
+ * pass lists per tile of targets the chunks whose box comes within the cutoff,
+ * and a persistent kernel sums over those work items only, a warp skipping any
+ * group whose box lies beyond the cutoff of its own targets.  Skipped pairs
+ * all have r >= cutoff, so the sums are those of the full tile over the same
+ * source order. */
+#define LGM_VARIANT_CULLED 2
 lgm_status lgm_variant_flags(int32_t variant, int32_t* flags);
 
 #ifdef __cplusplus

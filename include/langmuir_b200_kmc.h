@@ -121,9 +121,20 @@ typedef struct lgm_kmc lgm_kmc;
  * potential.cpp:74-244), site energies (linear field, gate, traps,
  * potential.cpp:17-72), seeded carriers (world.cpp:759-959) -- from a
  * Philox stream keyed by (random.seed, replica), then uploads it.  Transistor
- * and solar-cell set-ups; source.metropolis and balance.charges are not
- * supported (LGM_ERR_UNSUPPORTED). */
+ * and solar-cell set-ups. */
 lgm_status lgm_kmc_create(const lgm_params* p, int32_t device, uint32_t replica, lgm_kmc** out);
+/* The world lgm_kmc_create builds, on the host alone (no device is touched):
+ * site energies [volume], defect sites, trap sites and potentials, and the
+ * seeded electron and hole lists in list order.  counts receives the numbers
+ * of defects, traps, electrons and holes; LGM_ERR_CAPACITY when a list does
+ * not fit its capacity (counts are still set).  Every set-up draw comes from
+ * one Philox stream in the order World::initialize consumes its generator
+ * (world.cpp:589-650): placeDefects, placeElectrons, placeHoles,
+ * setPotentialTraps. */
+lgm_status lgm_kmc_world_host(const lgm_params* p, uint32_t replica, double* site_energy,
+                              int32_t* defects, int32_t d_cap, int32_t* traps, double* trap_pots,
+                              int32_t t_cap, int32_t* electrons, int32_t e_cap, int32_t* holes,
+                              int32_t h_cap, int32_t* counts);
 lgm_status lgm_kmc_destroy(lgm_kmc* k);
 /* A world restored from a checkpoint (ConfigurationInfo filled by
  * CheckPointer::load, checkpointer.cpp:22-163): site lists in the reference's

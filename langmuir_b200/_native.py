@@ -64,7 +64,24 @@ class LaunchInfo(ctypes.Structure):
         ("kernel_launches", ctypes.c_int32),
         ("pair_kernel_ms", ctypes.c_float),
         ("variant", ctypes.c_int32),
+        ("pairs_examined", ctypes.c_int64),
     ]
+
+
+class Peaks(ctypes.Structure):
+    """lgm_peaks: measured FP32 FMA and MUFU rsqrt throughput."""
+    _fields_ = [("ffma_tflops", ctypes.c_double), ("ffma2_tflops", ctypes.c_double),
+                ("rsqrt_per_s", ctypes.c_double), ("sm_count", ctypes.c_int32),
+                ("clock_mhz_attribute", ctypes.c_double)]
+
+
+def probe_peaks(device=0) -> dict:
+    """lgm_probe_peaks: FFMA, FFMA2 and MUFU rsqrt rates measured on `device`."""
+    p = Peaks()
+    st = lib().lgm_probe_peaks(int(device), ctypes.byref(p))
+    if st != OK:
+        raise LgmError(st, "lgm_probe_peaks")
+    return {k: getattr(p, k) for k, _ in Peaks._fields_}
 
 
 _i32p = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
@@ -92,6 +109,8 @@ SIGNATURES = {
                                                    ctypes.c_int32, _vp, _vp]),
     "lgm_last_launch": (ctypes.c_int32, [_vp, ctypes.POINTER(LaunchInfo)]),
     "lgm_set_timing": (ctypes.c_int32, [_vp, ctypes.c_int32]),
+    "lgm_set_counting": (ctypes.c_int32, [_vp, ctypes.c_int32]),
+    "lgm_probe_peaks": (ctypes.c_int32, [ctypes.c_int32, _vp]),
     "lgm_autotune": (ctypes.c_int32, [_vp, ctypes.c_int32, ctypes.c_uint32, ctypes.c_int32,
                                       ctypes.c_int32, ctypes.POINTER(ctypes.c_int32)]),
     "lgm_set_variant": (ctypes.c_int32, [_vp, ctypes.c_int32]),

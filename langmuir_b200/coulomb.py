@@ -119,11 +119,15 @@ class Coulomb:
             f = ctypes.c_int32()
             N.lib().lgm_variant_flags(v, ctypes.byref(f))
             out.append({"threads": a.value, "target_pairs": b.value, "run": c.value,
-                        "warp_skip": bool(f.value & 1)})
+                        "warp_skip": bool(f.value & 1), "culled": bool(f.value & 2)})
         return out
 
     def set_timing(self, on: bool = True):
         self._check(N.lib().lgm_set_timing(self._h, int(bool(on))))
+
+    def set_counting(self, on: bool = True):
+        """Culled pair sums count the pairs they examine (lgm_set_counting)."""
+        self._check(N.lib().lgm_set_counting(self._h, int(bool(on))))
 
     def last_launch(self) -> dict:
         info = N.LaunchInfo()

@@ -15,7 +15,7 @@
 
 #include "langmuir_b200.h"
 #include "lgm_context.hpp"
-#include "lgm_pairs.cuh"
+#include "lgm_cull.cuh"
 
 using namespace lgm;
 
@@ -70,29 +70,57 @@ lgm_status grow_host(lgm_ctx* c, T** p, size_t* cap, size_t need) {
 
 // ---- prep kernels ---------------------------------------------------------
 
-// Source records (see lgm_pairs.cuh).  Entries n .. n_pad-1 are zero-charge
-// padding at the origin; their weight is (q*m) * y = 0 * finite = 0.
-__global__ void prep_sources(const int32_t* __restrict__ s, const int32_t* __restrict__ q, int n,
-                             int n_pad, int X, int Y, int XY, int volume, float4* __restrict__ geo,
-                             float2* __restrict__ qq, unsigned* err) {
+// Source records (see lgm_pairs.cuh) in spatial order.  The sources were
+// counted into bins by lattice cell (bins_both) and scattered by bin
+// (scatter_both, in no particular order inside a bin); slot j of that scatter
+// takes its final place here: the bin's start plus its rank inside the bin by
+// (site, index), so the order depends on the sources alone and the sums are
+// deterministic.  bins_end[b] is the end of bin b after the scatter.  Entries
+// n .. n_pad-1 are zero-charge padding at the origin; their weight is
+// (q*m) * y = 0 * finite = 0.
+__device__ __forceinline__ void source_record(int sj, int qj, int X, int XY, int Y, int volume,
+                                              float4* __restrict__ geo, float2* __restrict__ qq,
+                                              int dst, unsigned* err) {
+    float a = 0.f, b = 0.f, cc = 0.f, d = -0.5f, qf = 0.f;
+    if (sj < 0 || sj >= volume) {
+        atomicOr(err, DEVERR_SOURCE_RANGE);
+    } else {
+        // Grid::getIndexX/Y/Z (cubicgrid.cpp:132-145), as kernel.cl:266-268.
+        const int z = sj / XY, y = sj / X - z * Y, x = sj % X;
+        a = -2.f * x; b = -2.f * y; cc = -2.f * z;
+        d = (float)(x * x + y * y + z * z) - 0.5f;
+        qf = (float)qj;
+    }
+    geo[2 * dst] = make_float4(a, a, b, b);
+    geo[2 * dst + 1] = make_float4(cc, cc, d, d);
+    qq[dst] = make_float2(qf, qf);
+}
+
+__global__ void prep_sources_sorted(const int32_t* __restrict__ s, const int32_t* __restrict__ q,
+                                    int n, int n_pad, const int32_t* __restrict__ key,
+                                    const int32_t* __restrict__ tmp,
+                                    const int32_t* __restrict__ bins_end, int X, int Y, int XY,
+                                    int volume, float4* __restrict__ geo,
+                                    float2* __restrict__ qq, unsigned* err) {
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= n_pad) return;
-    float a = 0.f, b = 0.f, cc = 0.f, d = -0.5f, qf = 0.f;
-    if (j < n) {
-        const int sj = s[j];
-        if (sj < 0 || sj >= volume) {
-            atomicOr(err, DEVERR_SOURCE_RANGE);
-        } else {
-            // Grid::getIndexX/Y/Z (cubicgrid.cpp:132-145), as kernel.cl:266-268.
-            const int z = sj / XY, y = sj / X - z * Y, x = sj % X;
-            a = -2.f * x; b = -2.f * y; cc = -2.f * z;
-            d = (float)(x * x + y * y + z * z) - 0.5f;
-            qf = (float)q[j];
-        }
+    if (j >= n) {
+        geo[2 * j] = make_float4(0.f, 0.f, 0.f, 0.f);
+        geo[2 * j + 1] = make_float4(0.f, 0.f, -0.5f, -0.5f);
+        qq[j] = make_float2(0.f, 0.f);
+        return;
     }
-    geo[2 * j] = make_float4(a, a, b, b);
-    geo[2 * j + 1] = make_float4(cc, cc, d, d);
-    qq[j] = make_float2(qf, qf);
+    const int i = tmp[j];
+    const int b = key[i];
+    const int lo = b > 0 ? bins_end[b - 1] : 0, hi = bins_end[b];
+    const int si = s[i];
+    int rank = 0;
+    for (int k = lo; k < hi; ++k) {
+        const int o = tmp[k];
+        const int so = s[o];
+        rank += (so < si) | ((so == si) & (o < i));
+    }
+    source_record(si, q[i], X, XY, Y, volume, geo, qq, lo + rank, err);
 }
 
 // Physical targets: for each requested term the (possibly mirrored) target
@@ -123,8 +151,10 @@ __global__ void prep_targets(const int32_t* __restrict__ ts, int t, int t_pad, i
         if (term == 1) xp = -1 - x;
         if (term == 2) xp = 2 * X - 1 - x;
         const float fx = (float)xp, fy = (float)y, fz = (float)z;
+        // padding slots (g >= t) carry w = -1: the cull leaves them out of the
+        // tiles' boxes, and their sums are never read
         tgt[(size_t)slot * t_pad + g] =
-            make_float4(fx, fy, fz, (float)(xp * xp + y * y + z * z));
+            make_float4(fx, fy, fz, g < t ? (float)(xp * xp + y * y + z * z) : -1.f);
         ++slot;
     }
 }
@@ -155,38 +185,74 @@ __global__ void finalize(const double* __restrict__ part, int splits, int t_phys
     out[perm[g]] = prefactor * total;
 }
 
-// Counting sort of the targets by lattice cell (the spatial order the SKIP
-// pair tiles run in).  target_bins: the bin of every target -- the Morton
-// rank of its cell, sites beyond the lattice (drains, or ids the prep flags
-// as out of range) in the last bin -- and the bin counts.
-__global__ void target_bins(const int32_t* __restrict__ ts, int t, int all_sites, int X, int Y,
-                            int XY, int volume, int shift, int cells_x, int cells_y,
-                            const int32_t* __restrict__ cell_rank, int ncells,
-                            int32_t* __restrict__ key, int32_t* __restrict__ bins) {
+// Counting sort of the targets and of the sources by lattice cell (the
+// spatial order the SKIP and culled pair tiles run in).  bins_both: the bin of
+// every target and every source -- the Morton rank of its cell, sites beyond
+// the lattice (drains, or ids the prep flags as out of range) in the last bin
+// -- and the bin counts (target bins tbins, source bins sbins).
+__device__ __forceinline__ int cell_bin(int sg, int X, int Y, int XY, int volume, int shift,
+                                        int cells_x, int cells_y,
+                                        const int32_t* __restrict__ cell_rank, int ncells) {
+    if (sg < 0 || sg >= volume) return ncells;
+    const int z = sg / XY, y = sg / X - z * Y, x = sg % X;
+    return cell_rank[(x >> shift) + cells_x * ((y >> shift) + cells_y * (z >> shift))];
+}
+
+__global__ void bins_both(const int32_t* __restrict__ ts, int t, int all_sites,
+                          const int32_t* __restrict__ ss, int n, int X, int Y, int XY, int volume,
+                          int shift, int cells_x, int cells_y,
+                          const int32_t* __restrict__ cell_rank, int ncells,
+                          int32_t* __restrict__ tkey, int32_t* __restrict__ tbins,
+                          int32_t* __restrict__ skey, int32_t* __restrict__ sbins) {
     const int g = blockIdx.x * blockDim.x + threadIdx.x;
-    if (g >= t) return;
-    const int sg = all_sites ? g : ts[g];
-    int b = ncells;
-    if (sg >= 0 && sg < volume) {
-        const int z = sg / XY, y = sg / X - z * Y, x = sg % X;
-        b = cell_rank[(x >> shift) + cells_x * ((y >> shift) + cells_y * (z >> shift))];
+    if (g < t) {
+        const int b = cell_bin(all_sites ? g : ts[g], X, Y, XY, volume, shift, cells_x, cells_y,
+                               cell_rank, ncells);
+        tkey[g] = b;
+        atomicAdd(&tbins[b], 1);
     }
-    key[g] = b;
-    atomicAdd(&bins[b], 1);
+    if (g < n) {
+        const int b =
+            cell_bin(ss[g], X, Y, XY, volume, shift, cells_x, cells_y, cell_rank, ncells);
+        skey[g] = b;
+        atomicAdd(&sbins[b], 1);
+    }
 }
 
-// Exclusive scan of nb bin counts in place, one block of kScanThreads.
+// Exclusive scans of the target bins (block 0) and the source bins (block 1)
+// in place, nb entries each.
 constexpr int kScanThreads = 1024;
-__global__ void __launch_bounds__(kScanThreads) bins_scan(int32_t* __restrict__ bins, int nb) {
-    block_exclusive_scan(bins, nb);
+__global__ void __launch_bounds__(kScanThreads) bins_scan2(int32_t* __restrict__ tbins,
+                                                           int32_t* __restrict__ sbins, int nb) {
+    block_exclusive_scan(blockIdx.x == 0 ? tbins : sbins, nb);
 }
 
-// perm[slot] = target: each target takes the next slot of its bin.
-__global__ void target_scatter(const int32_t* __restrict__ key, int t, int32_t* __restrict__ bins,
-                               int32_t* __restrict__ perm) {
+// perm[slot] = target: each target takes the next slot of its bin (the order
+// inside a bin does not change a target's sum); stmp likewise for the
+// sources, whose final order prep_sources_sorted fixes.
+__global__ void scatter_both(const int32_t* __restrict__ tkey, int t, int32_t* __restrict__ tbins,
+                             int32_t* __restrict__ perm, const int32_t* __restrict__ skey, int n,
+                             int32_t* __restrict__ sbins, int32_t* __restrict__ stmp) {
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g < t) perm[atomicAdd(&tbins[tkey[g]], 1)] = g;
+    if (g < n) stmp[atomicAdd(&sbins[skey[g]], 1)] = g;
+}
+
+// out[perm[g]] = prefactor * (sum of the item partials of the direct slot -
+// those of the image slots) of target g, for the culled pair sums.
+__global__ void finalize_items(const double* __restrict__ part,
+                               const int* __restrict__ tile_first,
+                               const int* __restrict__ tile_items, int tile_size, int t,
+                               int t_pad, int nterms, double prefactor,
+                               const int32_t* __restrict__ perm, double* __restrict__ out) {
     const int g = blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= t) return;
-    perm[atomicAdd(&bins[key[g]], 1)] = g;
+    double total = 0.0;
+    for (int slot = 0; slot < nterms; ++slot) {
+        const double s = item_sum(part, tile_first, tile_items, tile_size, slot * t_pad + g);
+        total = (slot == 0) ? s : total - s;
+    }
+    out[perm[g]] = prefactor * total;
 }
 
 __global__ void fill_zero(double* out, int t) {
@@ -243,35 +309,57 @@ pair_kernel_f64(const float4* __restrict__ geo, const float2* __restrict__ qq, i
 // ---- launch plumbing --------------------------------------------------------
 
 using PairFn = void (*)(PairArgs);
+using CulledFn = void (*)(PairArgs, CullArgs);
 
 // Compiled tile variants of the pair kernel: threads per CTA, target pairs per
 // thread, FP32 run length.  fn[0] point/rsqrt, fn[1] gauss/rsqrt, fn[2] table.
 // skip: warp-owned spatially sorted targets with the per-source warp vote
-// (the rsqrt paths; the table path runs the plain tile).
+// (the rsqrt paths; the table path runs the plain tile).  cull: the work-list
+// kernel of lgm_cull.cuh over the live source chunks of each tile, per_item
+// chunks per work item (cfn[] instead of fn[]).
 struct Variant {
-    int nt, rp, sub, skip;
+    int nt, rp, sub, skip, cull, per_item;
     PairFn fn[3];
+    CulledFn cfn[3];
 };
 #define LGM_VARIANT_S(NT, RP, SUB, SK)                                                    \
     Variant {                                                                             \
-        NT, RP, SUB, SK, {                                                                \
-            &pair_kernel<0, 0, NT, RP, SUB, false, SK>,                                   \
-                &pair_kernel<1, 0, NT, RP, SUB, false, SK>, &pair_kernel<0, 1, NT, RP, SUB> \
+        NT, RP, SUB, SK, 0, 0,                                                            \
+            {&pair_kernel<0, 0, NT, RP, SUB, false, SK>,                                  \
+             &pair_kernel<1, 0, NT, RP, SUB, false, SK>, &pair_kernel<0, 1, NT, RP, SUB>}, \
+        {                                                                                 \
+            nullptr, nullptr, nullptr                                                     \
         }                                                                                 \
     }
 #define LGM_VARIANT(NT, RP, SUB) LGM_VARIANT_S(NT, RP, SUB, false)
 #define LGM_VARIANT_SKIP(NT, RP, SUB) LGM_VARIANT_S(NT, RP, SUB, true)
+#define LGM_VARIANT_CULL(NT, RP, SUB, K)                                                      \
+    Variant {                                                                                 \
+        NT, RP, SUB, 1, 1, K, {nullptr, nullptr, nullptr}, {                                  \
+            &pair_kernel_culled<0, 0, NT, RP, SUB>, &pair_kernel_culled<1, 0, NT, RP, SUB>,   \
+                &pair_kernel_culled<0, 1, NT, RP, SUB>                                        \
+        }                                                                                     \
+    }
 const Variant kVariants[] = {
     LGM_VARIANT(128, 4, 16),       LGM_VARIANT(128, 4, 8),        LGM_VARIANT(128, 2, 16),
     LGM_VARIANT(128, 8, 16),       LGM_VARIANT(256, 4, 16),       LGM_VARIANT(64, 4, 16),
     LGM_VARIANT(128, 4, 32),       LGM_VARIANT(256, 2, 16),       LGM_VARIANT_SKIP(128, 4, 32),
     LGM_VARIANT_SKIP(128, 4, 16),  LGM_VARIANT_SKIP(128, 2, 32),  LGM_VARIANT_SKIP(64, 4, 32),
     LGM_VARIANT_SKIP(64, 3, 32),   LGM_VARIANT_SKIP(128, 3, 32),
+    LGM_VARIANT_CULL(128, 4, 32, 2), LGM_VARIANT_CULL(128, 4, 32, 1),
+    LGM_VARIANT_CULL(128, 4, 32, 4), LGM_VARIANT_CULL(128, 2, 32, 2),
+    LGM_VARIANT_CULL(64, 4, 32, 2),  LGM_VARIANT_CULL(128, 4, 16, 2),
+    LGM_VARIANT_CULL(64, 2, 32, 2),
 };
 constexpr int kNumVariants = (int)(sizeof(kVariants) / sizeof(kVariants[0]));
 static_assert(kNumVariants <= (int)(sizeof(lgm_ctx::bps) / sizeof(lgm_ctx::bps[0])),
               "lgm_ctx::bps holds every variant");
-constexpr int kDefaultVariant = 8;  // skip, 128 threads, 4 target pairs, runs of 32
+constexpr int kDefaultVariant = 14;  // culled, 128 threads, 4 target pairs, runs of 32, 2 chunks per item
+
+const void* kernel_of(const Variant& V, int fi) {
+    return V.cull ? reinterpret_cast<const void*>(V.cfn[fi])
+                  : reinterpret_cast<const void*>(V.fn[fi]);
+}
 
 int fn_index(int kind, int path) {
     if (path == LGM_PATH_TABLE) return 2;
@@ -312,24 +400,27 @@ lgm_status prep(lgm_ctx* c, unsigned terms, const int32_t* d_src, const int32_t*
     if ((s = grow_device(c, &c->d_qq, &c->qq_cap, (size_t)sh.n_pad)) != LGM_OK) return s;
     // room for the widest target tile of any variant
     if ((s = grow_device(c, &c->d_tgt, &c->tgt_cap, (size_t)sh.t_phys + 4096)) != LGM_OK) return s;
-    prep_sources<<<(sh.n_pad + 255) / 256, 256, 0, st>>>(d_src, d_q, n, sh.n_pad, cf.grid_x,
-                                                          cf.grid_y, c->xy, c->volume, c->d_geo,
-                                                          c->d_qq, c->d_err);
-    LGM_CUDA(c, cudaGetLastError());
-    // targets in spatial order: bins, scan, scatter
     if ((s = grow_device(c, &c->d_key, &c->key_cap, (size_t)t)) != LGM_OK) return s;
     if ((s = grow_device(c, &c->d_perm, &c->perm_cap, (size_t)t)) != LGM_OK) return s;
-    LGM_CUDA(c, cudaMemsetAsync(c->d_bins, 0, sizeof(int32_t) * (c->ncells + 1), st));
-    const int tb = (t + 255) / 256;
-    target_bins<<<tb, 256, 0, st>>>(d_tgt_site, t, all_sites, cf.grid_x, cf.grid_y, c->xy,
-                                    c->volume, c->cell_shift, c->cells_x, c->cells_y,
-                                    c->d_cell_rank, c->ncells, c->d_key, c->d_bins);
-    bins_scan<<<1, kScanThreads, 0, st>>>(c->d_bins, c->ncells + 1);
-    target_scatter<<<tb, 256, 0, st>>>(c->d_key, t, c->d_bins, c->d_perm);
+    if ((s = grow_device(c, &c->d_skey, &c->skey_cap, (size_t)n)) != LGM_OK) return s;
+    if ((s = grow_device(c, &c->d_stmp, &c->stmp_cap, (size_t)n)) != LGM_OK) return s;
+    // targets and sources in spatial order: bins, scans, scatters
+    LGM_CUDA(c, cudaMemsetAsync(c->d_bins, 0, sizeof(int32_t) * 2 * c->bins_stride, st));
+    const int tb = (std::max(t, n) + 255) / 256;
+    bins_both<<<tb, 256, 0, st>>>(d_tgt_site, t, all_sites, d_src, n, cf.grid_x, cf.grid_y, c->xy,
+                                  c->volume, c->cell_shift, c->cells_x, c->cells_y,
+                                  c->d_cell_rank, c->ncells, c->d_key, c->d_bins, c->d_skey,
+                                  c->d_sbins);
+    bins_scan2<<<2, kScanThreads, 0, st>>>(c->d_bins, c->d_sbins, c->ncells + 1);
+    scatter_both<<<tb, 256, 0, st>>>(c->d_key, t, c->d_bins, c->d_perm, c->d_skey, n, c->d_sbins,
+                                     c->d_stmp);
     LGM_CUDA(c, cudaGetLastError());
     prep_targets<<<(sh.t_pad + 255) / 256, 256, 0, st>>>(d_tgt_site, t, sh.t_pad, all_sites, terms,
                                                           cf.grid_x, cf.grid_y, c->xy, c->volume,
                                                           c->d_perm, c->d_tgt, c->d_err);
+    prep_sources_sorted<<<(sh.n_pad + 255) / 256, 256, 0, st>>>(
+        d_src, d_q, n, sh.n_pad, c->d_skey, c->d_stmp, c->d_sbins, cf.grid_x, cf.grid_y, c->xy,
+        c->volume, c->d_geo, c->d_qq, c->d_err);
     LGM_CUDA(c, cudaGetLastError());
     return LGM_OK;
 }
@@ -351,10 +442,86 @@ int splits_for(const lgm_ctx* c, int v, int fi, const Shape& sh, int* tiles_out)
     return std::max(1, std::min({kMaxSplits, kSplitWaves * capacity / tiles, sh.n_chunks}));
 }
 
+// Culled variant v: chunk boxes, the cull, the persistent pair kernel (one
+// wave of resident CTAs).  *splits_out = 0 tells the caller to finalize from
+// the item partials.
+lgm_status launch_culled(lgm_ctx* c, int kind, int v, const Shape& sh, const PairArgs& A,
+                         cudaStream_t st, int* splits_out) {
+    const Variant& V = kVariants[v];
+    const int fi = fn_index(kind, c->cfg.path);
+    const int TS = V.nt * 2 * V.rp;
+    const int tiles = (sh.t_phys + TS - 1) / TS;
+    const int max_items = std::min(kMaxItemsPerTile, (sh.n_chunks + V.per_item - 1) / V.per_item);
+    const size_t item_cap = (size_t)tiles * std::max(1, max_items);
+    lgm_status s;
+    if ((s = grow_device(c, &c->d_cbox, &c->cbox_cap, (size_t)sh.n_chunks)) != LGM_OK) return s;
+    if ((s = grow_device(c, &c->d_gbox, &c->gbox_cap, (size_t)sh.n_chunks * kGroupsPerChunk)) !=
+        LGM_OK)
+        return s;
+    if ((s = grow_device(c, &c->d_live, &c->live_cap, (size_t)tiles * sh.n_chunks)) != LGM_OK)
+        return s;
+    if ((s = grow_device(c, &c->d_items, &c->items_cap, item_cap)) != LGM_OK) return s;
+    if ((s = grow_device(c, &c->d_tile_first, &c->tfirst_cap, (size_t)tiles)) != LGM_OK) return s;
+    if ((s = grow_device(c, &c->d_tile_items, &c->titems_cap, (size_t)tiles)) != LGM_OK) return s;
+    if ((s = grow_device(c, &c->d_part, &c->part_cap, item_cap * TS)) != LGM_OK) return s;
+    PairArgs P = A;
+    P.part = c->d_part;
+    CullArgs C;
+    C.n_chunks = sh.n_chunks;
+    C.cbox = reinterpret_cast<Box*>(c->d_cbox);
+    C.gbox = reinterpret_cast<Box*>(c->d_gbox);
+    C.tgt = c->d_tgt;
+    C.t_phys = sh.t_phys;
+    C.c2 = c->cfg.electrostatic_cutoff * c->cfg.electrostatic_cutoff;
+    C.tile_size = TS;
+    C.per_item = V.per_item;
+    C.max_items = std::max(1, max_items);
+    C.live = c->d_live;
+    C.live_stride = sh.n_chunks;
+    C.items = c->d_items;
+    C.item_count = c->d_item_count;
+    C.tile_first = c->d_tile_first;
+    C.tile_items = c->d_tile_items;
+    if (c->counting) {
+        LGM_CUDA(c, cudaMemsetAsync(c->d_examined, 0, sizeof(unsigned long long), st));
+        C.examined = c->d_examined;
+        c->count_pending = true;
+    }
+    chunk_boxes_kernel<<<sh.n_chunks, CH, 0, st>>>(P, C);
+    cull_kernel<<<tiles, kCullThreads, 0, st>>>(C);
+    // timing on: the events bracket the pair kernel alone (recorded again here)
+    if (c->timing) LGM_CUDA(c, cudaEventRecord(c->ev_pair0, st));
+    const int grid = c->sm_count * std::max(1, c->bps[v][fi]);
+    V.cfn[fi]<<<grid, V.nt, pair_smem_bytes(P.tab_k), st>>>(P, C);
+    LGM_CUDA(c, cudaGetLastError());
+    c->last.ctas = grid;
+    c->last.threads = V.nt;
+    c->last.targets_per_thread = 2 * V.rp;
+    c->last.variant = v;
+    c->last.splits = 0;
+    *splits_out = 0;
+    return LGM_OK;
+}
+
 lgm_status launch_pair(lgm_ctx* c, int kind, int v, const Shape& sh, cudaStream_t st,
                        int* splits_out) {
     const lgm_config& cf = c->cfg;
     const int fi = fn_index(kind, cf.path);
+    if (kVariants[v].cull) {
+        PairArgs A;
+        A.geo = c->d_geo; A.qq = c->d_qq; A.n_chunks = sh.n_chunks; A.splits = 1;
+        A.tgt = c->d_tgt; A.t_phys = sh.t_phys;
+        A.c2 = (float)(cf.electrostatic_cutoff * cf.electrostatic_cutoff);
+        A.err = c->d_err;
+        if (cf.path == LGM_PATH_TABLE) {
+            A.tab = kind == LGM_GAUSS ? c->d_gtab : c->d_rtab;
+            A.tab_k = kind == LGM_GAUSS ? c->gtab_k : c->rtab_k;
+        } else {
+            A.tab = c->d_gtab;
+            A.tab_k = kind == LGM_GAUSS ? c->gtab_k : 0;
+        }
+        return launch_culled(c, kind, v, sh, A, st, splits_out);
+    }
     int tiles;
     const int splits = splits_for(c, v, fi, sh, &tiles);
     lgm_status s;
@@ -399,7 +566,9 @@ lgm_status launch_potentials(lgm_ctx* c, int kind, unsigned terms, const int32_t
     c->last = lgm_launch_info{};
     c->last.pair_kernel_ms = -1.f;
     c->last.variant = -1;
+    c->last.pairs_examined = -1;
     c->timed_pending = false;
+    c->count_pending = false;
     if (t == 0) return LGM_OK;
     if (n == 0) {
         fill_zero<<<(t + 255) / 256, 256, 0, st>>>(d_out, t);
@@ -437,12 +606,21 @@ lgm_status launch_potentials(lgm_ctx* c, int kind, unsigned terms, const int32_t
         LGM_CUDA(c, cudaEventRecord(c->ev_pair1, st));
         c->timed_pending = true;
     }
-    finalize<<<(t + 255) / 256, 256, 0, st>>>(c->d_part, splits, sh.t_phys, t, sh.t_pad, sh.nterms,
-                                               cf.electrostatic_prefactor, c->d_perm, d_out);
+    if (splits > 0) {
+        finalize<<<(t + 255) / 256, 256, 0, st>>>(c->d_part, splits, sh.t_phys, t, sh.t_pad,
+                                                   sh.nterms, cf.electrostatic_prefactor,
+                                                   c->d_perm, d_out);
+        c->last.kernel_launches = 7;  // bins, scan, scatter, two preps, pair, finalize
+    } else {
+        const Variant& V = kVariants[c->last.variant];
+        finalize_items<<<(t + 255) / 256, 256, 0, st>>>(
+            c->d_part, c->d_tile_first, c->d_tile_items, V.nt * 2 * V.rp, t, sh.t_pad, sh.nterms,
+            cf.electrostatic_prefactor, c->d_perm, d_out);
+        c->last.kernel_launches = 9;  // bins, scan, scatter, two preps, boxes, cull, pair, finalize
+    }
     LGM_CUDA(c, cudaGetLastError());
     c->last.pairs_tested = (int64_t)sh.nterms * t * (int64_t)n;
     c->last.splits = splits;
-    c->last.kernel_launches = 7;  // bins, scan, scatter, two preps, pair, finalize
     return LGM_OK;
 }
 
@@ -694,9 +872,13 @@ lgm_status lgm_create(const lgm_config* cfg, int32_t device, lgm_ctx** out) {
         const std::vector<int32_t> rank =
             cell_ranks(cf.grid_x, cf.grid_y, cf.grid_z, &c->cell_shift, &c->cells_x, &c->cells_y);
         c->ncells = (int)rank.size();
+        c->bins_stride = (c->ncells + 2 + 3) / 4 * 4;
         if ((e = cudaMalloc(&c->d_cell_rank, sizeof(int32_t) * rank.size())) != cudaSuccess ||
-            (e = cudaMalloc(&c->d_bins, sizeof(int32_t) * (rank.size() + 2))) != cudaSuccess)
+            (e = cudaMalloc(&c->d_bins, sizeof(int32_t) * 2 * c->bins_stride)) != cudaSuccess ||
+            (e = cudaMalloc(&c->d_item_count, sizeof(int32_t))) != cudaSuccess)
             return bail("cudaMalloc", e);
+        // the source bins follow the target bins, 16-byte aligned (the scan reads int4)
+        c->d_sbins = c->d_bins + c->bins_stride;
         if ((e = cudaMemcpy(c->d_cell_rank, rank.data(), sizeof(int32_t) * rank.size(),
                             cudaMemcpyHostToDevice)) != cudaSuccess)
             return bail("cudaMemcpy", e);
@@ -716,14 +898,14 @@ lgm_status lgm_create(const lgm_config* cfg, int32_t device, lgm_ctx** out) {
                         lgm_destroy(c);
                         return LGM_ERR_UNSUPPORTED;
                     }
-                    if ((e = cudaFuncSetAttribute(kVariants[v].fn[fi],
+                    if ((e = cudaFuncSetAttribute(kernel_of(kVariants[v], fi),
                                                   cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                   (int)smem)) != cudaSuccess)
                         return bail("cudaFuncSetAttribute", e);
                 }
                 int bps = 0;
                 if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-                         &bps, kVariants[v].fn[fi], kVariants[v].nt, smem)) != cudaSuccess)
+                         &bps, kernel_of(kVariants[v], fi), kVariants[v].nt, smem)) != cudaSuccess)
                     return bail("cudaOccupancyMaxActiveBlocksPerMultiprocessor", e);
                 c->bps[v][fi] = bps;
             }
@@ -736,9 +918,12 @@ lgm_status lgm_destroy(lgm_ctx* c) {
     if (!c) return LGM_OK;
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
-    void* dev_ptrs[] = {c->d_geo, c->d_qq, c->d_tgt, c->d_part, c->d_s, c->d_q,
-                        c->d_t, c->d_o, c->d_gtab, c->d_rtab, c->d_err, c->d_cell_rank,
-                        c->d_bins, c->d_key, c->d_perm};
+    void* dev_ptrs[] = {c->d_geo,  c->d_qq,        c->d_tgt,       c->d_part,      c->d_s,
+                        c->d_q,    c->d_t,         c->d_o,         c->d_gtab,      c->d_rtab,
+                        c->d_err,  c->d_cell_rank, c->d_bins,      c->d_key,       c->d_perm,
+                        c->d_skey, c->d_stmp,      c->d_cbox,      c->d_gbox,      c->d_live,
+                        c->d_items, c->d_tile_first, c->d_tile_items, c->d_item_count,
+                        c->d_examined};
     for (void* p : dev_ptrs)
         if (p) cudaFree(p);
     void* host_ptrs[] = {c->h_s, c->h_q, c->h_t, c->h_o, c->h_err};
@@ -765,7 +950,23 @@ lgm_status lgm_last_launch(lgm_ctx* c, lgm_launch_info* info) {
         c->last.pair_kernel_ms = ms;
         c->timed_pending = false;
     }
+    if (c->count_pending) {
+        unsigned long long n = 0;
+        LGM_CUDA(c, cudaMemcpy(&n, c->d_examined, sizeof n, cudaMemcpyDeviceToHost));
+        c->last.pairs_examined = (int64_t)n;
+        c->count_pending = false;
+    }
     *info = c->last;
+    return LGM_OK;
+}
+
+lgm_status lgm_set_counting(lgm_ctx* c, int32_t enable) {
+    if (!c) return LGM_ERR_INVALID_ARGUMENT;
+    LGM_CUDA(c, cudaSetDevice(c->device));
+    if (enable && !c->d_examined)
+        LGM_CUDA(c, cudaMalloc(&c->d_examined, sizeof(unsigned long long)));
+    c->counting = enable != 0;
+    c->count_pending = false;
     return LGM_OK;
 }
 
@@ -793,7 +994,8 @@ lgm_status lgm_variant_info(int32_t v, int32_t* threads, int32_t* target_pairs, 
 
 lgm_status lgm_variant_flags(int32_t v, int32_t* flags) {
     if (v < 0 || v >= kNumVariants || !flags) return LGM_ERR_INVALID_ARGUMENT;
-    *flags = kVariants[v].skip ? LGM_VARIANT_WARP_SKIP : 0;
+    *flags = (kVariants[v].skip ? LGM_VARIANT_WARP_SKIP : 0) |
+             (kVariants[v].cull ? LGM_VARIANT_CULLED : 0);
     return LGM_OK;
 }
 

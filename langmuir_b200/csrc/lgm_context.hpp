@@ -38,6 +38,23 @@ struct lgm_ctx {
     int32_t* d_bins = nullptr;                       // [ncells + 2] counts, then offsets
     int32_t* d_key = nullptr;  size_t key_cap = 0;   // bin per target
     int32_t* d_perm = nullptr; size_t perm_cap = 0;  // target of each physical slot
+    // The sources in the same spatial order: bin per source (d_sbins follows
+    // the target bins in the d_bins allocation), the sources scattered by bin,
+    // then ranked inside their bin by (site, index), so that the order is a
+    // function of the sources alone.
+    int32_t* d_sbins = nullptr;                       // [ncells + 2], inside d_bins
+    int bins_stride = 0;                              // ncells + 2 rounded up to 4
+    int32_t* d_skey = nullptr; size_t skey_cap = 0;   // bin per source
+    int32_t* d_stmp = nullptr; size_t stmp_cap = 0;   // sources scattered by bin
+    // Culled pair sums (lgm_cull.cuh): chunk and group boxes, live chunk
+    // lists per tile, work items, and where each tile's items start.
+    int4* d_cbox = nullptr;  size_t cbox_cap = 0;     // lgm::Box per chunk
+    int4* d_gbox = nullptr;  size_t gbox_cap = 0;     // lgm::Box per 32-source group
+    int32_t* d_live = nullptr; size_t live_cap = 0;
+    int4* d_items = nullptr; size_t items_cap = 0;
+    int32_t* d_tile_first = nullptr; size_t tfirst_cap = 0;
+    int32_t* d_tile_items = nullptr; size_t titems_cap = 0;
+    int32_t* d_item_count = nullptr;                  // one int
 
     // Pinned host staging for the host-buffer entry points.
     int32_t* h_s = nullptr;   size_t hs_cap = 0;
@@ -46,10 +63,13 @@ struct lgm_ctx {
     double* h_o = nullptr;    size_t ho_cap = 0;
     unsigned* h_err = nullptr;
 
-    int bps[24][3] = {};                 // resident CTAs per SM, per variant and kernel
+    int bps[40][3] = {};                 // resident CTAs per SM, per variant and kernel
     int forced_variant = -1;             // -1: autotuned / default
     std::map<uint64_t, int> tune_cache;  // size bucket -> fastest variant
 
+    bool counting = false;
+    unsigned long long* d_examined = nullptr;  // pairs examined by the last culled launch
+    bool count_pending = false;
     bool timing = false;
     cudaEvent_t ev_pair0 = nullptr, ev_pair1 = nullptr;  // bracket the pair kernel
     bool timed_pending = false;

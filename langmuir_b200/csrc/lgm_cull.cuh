@@ -1,0 +1,466 @@
+// lgm_cull.cuh -- the pair sum over spatially culled source chunks.
+//
+// The reference's coulomb2/gauss2 (src/langmuirCore/kernel.cl:222-369) test
+// every (target, source) pair against the cutoff.  With the sources in
+// spatial order (sorted by lattice cell) and the targets too, whole blocks of
+// pairs lie beyond the cutoff and add exactly nothing, so they need not be
+// visited at all:
+//
+//   chunk_boxes  the bounding box of every source chunk (CH = 128 sources)
+//                and of each of its four groups of 32;
+//   cull         per target tile (the targets of one CTA), the ordered list
+//                of source chunks whose box comes within the cutoff of the
+//                tile's box, cut into work items of at most `per_item` chunks;
+//   pair         a persistent kernel: CTA b takes items b, b + G, b + 2G, ...
+//                and streams their chunks through shared memory (bulk TMA, two
+//                stages, the next item's chunks prefetched across the item
+//                boundary).  Each warp skips a 32-source group whose box lies
+//                beyond the cutoff of its own targets' box, and inside a live
+//                group the warp still votes per source (the SKIP tile of
+//                lgm_pairs.cuh);
+//   finalize     per target, the partials of its tile's items summed in item
+//                (= chunk) order.
+//
+// A skipped chunk or group holds only pairs with r^2 >= c^2 (box distance
+// tested exactly in integers), whose terms are zero; an FP32 run over a
+// skipped group would have summed to +0 and been folded as a no-op.  The sums
+// are therefore those of the unculled tile over the same source order, and
+// they are deterministic: items of a tile are numbered in chunk order, and a
+// tile's partials are added in that order whatever CTA computed them.
+#pragma once
+
+#include "lgm_pairs.cuh"
+
+namespace lgm {
+
+constexpr int kGroup = 32;                    // sources per group box
+constexpr int kGroupsPerChunk = CH / kGroup;  // 4
+constexpr int kCullThreads = 256;             // threads of the cull kernel
+constexpr int kMaxItemsPerTile = 32;          // items a tile's chunk list is cut into, at most
+
+// A box of lattice coordinates [lo, hi] per axis (inclusive).  Empty: lo > hi.
+struct __align__(16) Box {
+    short xl, yl, zl, pad0;
+    short xh, yh, zh, pad1;
+};
+
+__host__ __device__ inline Box empty_box() {
+    Box b;
+    b.xl = b.yl = b.zl = 32767;
+    b.xh = b.yh = b.zh = -32768;
+    b.pad0 = b.pad1 = 0;
+    return b;
+}
+
+// Squared distance between two boxes (0 when they overlap); each axis gap is
+// clamped at 4096 so that empty boxes give a large value without overflow.
+__device__ __forceinline__ int box_gap2(const Box& a, const Box& b) {
+    const int gx = min(4096, max(0, max(a.xl - b.xh, b.xl - a.xh)));
+    const int gy = min(4096, max(0, max(a.yl - b.yh, b.yl - a.yh)));
+    const int gz = min(4096, max(0, max(a.zl - b.zh, b.zl - a.zh)));
+    return gx * gx + gy * gy + gz * gz;
+}
+
+// Min and max of six coordinates over a full warp.
+__device__ __forceinline__ void warp_box(int& xl, int& yl, int& zl, int& xh, int& yh, int& zh) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        xl = min(xl, __shfl_xor_sync(0xffffffffu, xl, o));
+        yl = min(yl, __shfl_xor_sync(0xffffffffu, yl, o));
+        zl = min(zl, __shfl_xor_sync(0xffffffffu, zl, o));
+        xh = max(xh, __shfl_xor_sync(0xffffffffu, xh, o));
+        yh = max(yh, __shfl_xor_sync(0xffffffffu, yh, o));
+        zh = max(zh, __shfl_xor_sync(0xffffffffu, zh, o));
+    }
+}
+
+__device__ __forceinline__ Box make_box(int xl, int yl, int zl, int xh, int yh, int zh) {
+    Box b;
+    b.xl = (short)max(xl, -32768); b.yl = (short)max(yl, -32768); b.zl = (short)max(zl, -32768);
+    b.xh = (short)min(xh, 32767);  b.yh = (short)min(yh, 32767);  b.zh = (short)min(zh, 32767);
+    b.pad0 = b.pad1 = 0;
+    return b;
+}
+
+struct CullArgs {
+    // sources (records as PairArgs) and their boxes
+    int n_chunks = 0;                 // source chunks (dyn[0] overrides)
+    Box* cbox = nullptr;              // [chunks]
+    Box* gbox = nullptr;              // [chunks * kGroupsPerChunk]
+    // targets
+    const float4* tgt = nullptr;      // physical target records (w < 0: padding)
+    int t_phys = 0;                   // physical targets (dyn[1] overrides)
+    const int* dyn = nullptr;         // as PairArgs::dyn
+    int c2 = 0;                       // cutoff^2
+    int tile_size = 0;                // targets per tile = NT * 2 * RP of the pair kernel
+    // the work list
+    int per_item = 2;                 // chunks per item (fewer items are never cut)
+    int max_items = kMaxItemsPerTile; // items per tile, at most
+    int32_t* live = nullptr;          // [tiles][live_stride] live chunk ids in order
+    int live_stride = 0;
+    int4* items = nullptr;            // {tile, first live index, chunk count, 0}
+    int* item_count = nullptr;        // items written (zeroed by chunk_boxes block 0)
+    int* tile_first = nullptr;        // [tiles] first item of the tile
+    int* tile_items = nullptr;        // [tiles] items of the tile
+    // Optional (null: off): pairs whose r^2 the pair kernel computed, i.e.
+    // 32 sources x 64 RP targets per live group of a warp, summed over warps.
+    unsigned long long* examined = nullptr;
+};
+
+// One block of CH threads per source chunk: group and chunk boxes of the
+// records with a nonzero charge.  Block 0 also zeroes the item counter for
+// the cull that follows.
+__device__ __forceinline__ void chunk_boxes_body(const PairArgs& A, const CullArgs& C,
+                                                 const int chunk) {
+    __shared__ Box s_g[kGroupsPerChunk];
+    const int n_chunks = A.dyn ? A.dyn[0] : A.n_chunks;
+    if (chunk == 0 && threadIdx.x == 0 && C.item_count) *C.item_count = 0;
+    if (chunk >= n_chunks) return;
+    const int j = chunk * CH + (int)threadIdx.x;
+    const float4 g0 = A.geo[2 * j], g1 = A.geo[2 * j + 1];
+    const bool valid = A.qq[j].x != 0.f;
+    const int x = (int)(-0.5f * g0.x), y = (int)(-0.5f * g0.z), z = (int)(-0.5f * g1.x);
+    int xl = valid ? x : 32767, yl = valid ? y : 32767, zl = valid ? z : 32767;
+    int xh = valid ? x : -32768, yh = valid ? y : -32768, zh = valid ? z : -32768;
+    warp_box(xl, yl, zl, xh, yh, zh);
+    const int warp = (int)threadIdx.x >> 5;
+    if ((threadIdx.x & 31) == 0) {
+        const Box b = make_box(xl, yl, zl, xh, yh, zh);
+        C.gbox[chunk * kGroupsPerChunk + warp] = b;
+        s_g[warp] = b;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        Box u = s_g[0];
+        for (int g = 1; g < kGroupsPerChunk; ++g) {
+            u.xl = min(u.xl, s_g[g].xl); u.yl = min(u.yl, s_g[g].yl); u.zl = min(u.zl, s_g[g].zl);
+            u.xh = max(u.xh, s_g[g].xh); u.yh = max(u.yh, s_g[g].yh); u.zh = max(u.zh, s_g[g].zh);
+        }
+        C.cbox[chunk] = u;
+    }
+}
+
+// One block of kCullThreads per target tile: the tile's box, its live chunks
+// in source order, and its work items.
+__device__ __forceinline__ void cull_body(const CullArgs& C, const int tile) {
+    __shared__ int s_red[6][kCullThreads / 32];
+    __shared__ int s_wcount[kCullThreads / 32];
+    __shared__ int s_base;
+    const int n_chunks = C.dyn ? C.dyn[0] : C.n_chunks;
+    const int t_phys = C.dyn ? C.dyn[1] : C.t_phys;
+    const int tid = (int)threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    constexpr int nw = kCullThreads / 32;
+    if (tile * C.tile_size >= t_phys) {
+        if (tid == 0) C.tile_items[tile] = 0;
+        return;
+    }
+    int xl = 32767, yl = 32767, zl = 32767, xh = -32768, yh = -32768, zh = -32768;
+    const int p1 = min((tile + 1) * C.tile_size, t_phys);
+    for (int p = tile * C.tile_size + tid; p < p1; p += kCullThreads) {
+        const float4 t = C.tgt[p];
+        if (t.w >= 0.f) {
+            const int x = (int)t.x, y = (int)t.y, z = (int)t.z;
+            xl = min(xl, x); yl = min(yl, y); zl = min(zl, z);
+            xh = max(xh, x); yh = max(yh, y); zh = max(zh, z);
+        }
+    }
+    warp_box(xl, yl, zl, xh, yh, zh);
+    if (lane == 0) {
+        s_red[0][warp] = xl; s_red[1][warp] = yl; s_red[2][warp] = zl;
+        s_red[3][warp] = xh; s_red[4][warp] = yh; s_red[5][warp] = zh;
+    }
+    __syncthreads();
+    for (int w = 0; w < nw; ++w) {
+        xl = min(xl, s_red[0][w]); yl = min(yl, s_red[1][w]); zl = min(zl, s_red[2][w]);
+        xh = max(xh, s_red[3][w]); yh = max(yh, s_red[4][w]); zh = max(zh, s_red[5][w]);
+    }
+    const Box tb = make_box(xl, yl, zl, xh, yh, zh);
+    int32_t* live = C.live + (size_t)tile * C.live_stride;
+    int L = 0;
+    for (int c0 = 0; c0 < n_chunks; c0 += kCullThreads) {
+        const int c = c0 + tid;
+        const bool on = c < n_chunks && box_gap2(tb, C.cbox[c]) < C.c2;
+        const unsigned m = __ballot_sync(0xffffffffu, on);
+        __syncthreads();  // s_wcount of the previous round is read
+        if (lane == 0) s_wcount[warp] = __popc(m);
+        __syncthreads();
+        int before = 0, total = 0;
+        for (int w = 0; w < nw; ++w) {
+            before += w < warp ? s_wcount[w] : 0;
+            total += s_wcount[w];
+        }
+        if (on) live[L + before + __popc(m & ((1u << lane) - 1u))] = c;
+        L += total;
+    }
+    const int per = max(C.per_item, (L + C.max_items - 1) / C.max_items);
+    const int nit = L == 0 ? 0 : (L + per - 1) / per;
+    if (tid == 0) {
+        const int base = nit ? atomicAdd(C.item_count, nit) : 0;
+        C.tile_first[tile] = base;
+        C.tile_items[tile] = nit;
+        s_base = base;
+    }
+    __syncthreads();
+    for (int i = tid; i < nit; i += kCullThreads)
+        C.items[s_base + i] = make_int4(tile, i * per, min(per, L - i * per), 0);
+}
+
+// The pair sum over the work items (see the file comment).  KIND 0 point, 1
+// gauss; PATH 0 MUFU rsqrt with the per-source warp vote, 1 the shared-memory
+// table of w(k); NT threads, RP target pairs per thread (a warp owns 64 RP
+// consecutive targets), SUB sources per FP32 run (SUB divides kGroup).
+// Partials go to A.part[item * tile_size + local target] (and A.part_norm).
+// Launched with a persistent grid and dynamic shared memory
+// pair_smem_bytes(tab_k).
+template <int KIND, int PATH, int NT, int RP, int SUB, bool NORM>
+__device__ __forceinline__ void pair_items_culled(const PairArgs& A, const CullArgs& C) {
+    static_assert(kGroup % SUB == 0, "an FP32 run lies inside one group");
+    constexpr int TS = NT * 2 * RP;
+    const int nit = *C.item_count;
+    if ((int)blockIdx.x >= nit) return;
+    extern __shared__ __align__(128) unsigned char smem[];
+    float4* s_geo = reinterpret_cast<float4*>(smem);                               // [2][CH*2]
+    float2* s_qq = reinterpret_cast<float2*>(smem + 2 * CH * 2 * sizeof(float4));  // [2][CH]
+    uint64_t* s_bar = reinterpret_cast<uint64_t*>(smem + 2 * pair_stage_bytes());
+    float* s_tab = reinterpret_cast<float*>(smem + 2 * pair_stage_bytes() + 16);
+
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int t_phys = A.dyn ? A.dyn[1] : A.t_phys;
+    if (tid == 0) {
+        mbar_init(&s_bar[0], 1);
+        mbar_init(&s_bar[1], 1);
+        fence_mbar_init();
+    }
+    if (KIND == 1 || PATH == 1)
+        for (int k = tid; k <= A.tab_k; k += NT) s_tab[k] = A.tab[k];
+    __syncthreads();
+
+    // Producer (thread 0): walks this CTA's chunk sequence -- the live chunks
+    // of items blockIdx.x, blockIdx.x + G, ... -- two chunks ahead.  Its
+    // cursor lives in shared memory, out of the other threads' registers.
+    __shared__ int s_prod[6];  // item, position, tile, first, count, chunks issued
+    __shared__ Box s_wbox[NT / 32];
+    auto issue_next = [&]() {
+        int* P = s_prod;
+        if (P[0] >= nit) return;
+        const int chunk = C.live[(size_t)P[2] * C.live_stride + P[3] + P[1]];
+        const int st = P[5] & 1;
+        mbar_arrive_expect_tx(&s_bar[st], (uint32_t)pair_stage_bytes());
+        bulk_g2s(s_geo + st * CH * 2, A.geo + (size_t)chunk * CH * 2,
+                 (uint32_t)(CH * 2 * sizeof(float4)), &s_bar[st]);
+        bulk_g2s(s_qq + st * CH, A.qq + (size_t)chunk * CH, (uint32_t)(CH * sizeof(float2)),
+                 &s_bar[st]);
+        ++P[5];
+        if (++P[1] == P[4]) {
+            P[0] += (int)gridDim.x;
+            P[1] = 0;
+            if (P[0] < nit) {
+                const int4 r = C.items[P[0]];
+                P[2] = r.x; P[3] = r.y; P[4] = r.z;
+            }
+        }
+    };
+    if (tid == 0) {
+        const int4 r = C.items[blockIdx.x];
+        s_prod[0] = (int)blockIdx.x; s_prod[1] = 0;
+        s_prod[2] = r.x; s_prod[3] = r.y; s_prod[4] = r.z; s_prod[5] = 0;
+        issue_next();
+        issue_next();
+    }
+
+    const unsigned ulim = __float_as_uint(A.c2 - 0.5f);
+    const float2 half2 = f2(0.5f, 0.5f);
+    uint32_t consumed = 0;
+    bool failed = false;
+
+    for (int it = (int)blockIdx.x; it < nit; it += (int)gridDim.x) {
+        const int4 rec = C.items[it];
+        const int tile = rec.x, first = rec.y, count = rec.z;
+        const int base = tile * TS;
+        auto target_of = [&](int k) { return base + warp * (64 * RP) + k * 32 + lane; };
+        float2 tx[RP], ty[RP], tz[RP], tt[RP];
+        int xl = 32767, yl = 32767, zl = 32767, xh = -32768, yh = -32768, zh = -32768;
+#pragma unroll
+        for (int k = 0; k < RP; ++k) {
+            const int p0 = target_of(2 * k), p1 = target_of(2 * k + 1);
+            const float4 a = p0 < t_phys ? A.tgt[p0] : make_float4(0.f, 0.f, 0.f, -1.f);
+            const float4 b = p1 < t_phys ? A.tgt[p1] : make_float4(0.f, 0.f, 0.f, -1.f);
+            tx[k] = f2(a.x, b.x); ty[k] = f2(a.y, b.y); tz[k] = f2(a.z, b.z); tt[k] = f2(a.w, b.w);
+            if (a.w >= 0.f) {
+                xl = min(xl, (int)a.x); yl = min(yl, (int)a.y); zl = min(zl, (int)a.z);
+                xh = max(xh, (int)a.x); yh = max(yh, (int)a.y); zh = max(zh, (int)a.z);
+            }
+            if (b.w >= 0.f) {
+                xl = min(xl, (int)b.x); yl = min(yl, (int)b.y); zl = min(zl, (int)b.z);
+                xh = max(xh, (int)b.x); yh = max(yh, (int)b.y); zh = max(zh, (int)b.z);
+            }
+        }
+        warp_box(xl, yl, zl, xh, yh, zh);
+        if (lane == 0) s_wbox[warp] = make_box(xl, yl, zl, xh, yh, zh);
+        __syncwarp();
+
+        double acc64[2 * RP];
+        float nrm[NORM ? 2 * RP : 1];
+#pragma unroll
+        for (int k = 0; k < 2 * RP; ++k) acc64[k] = 0.0;
+#pragma unroll
+        for (int k = 0; k < (NORM ? 2 * RP : 1); ++k) nrm[k] = 0.f;
+
+        for (int c = 0; c < count; ++c) {
+            const int st = (int)(consumed & 1u);
+            const uint32_t parity = (consumed >> 1) & 1u;
+            const bool mine = mbar_wait_bounded(&s_bar[st], parity, A.err);
+            if (!__syncthreads_and(mine)) { failed = true; break; }
+            const int chunk = C.live[(size_t)tile * C.live_stride + first + c];
+            bool gon = false;
+            if (lane < kGroupsPerChunk)
+                gon = box_gap2(s_wbox[warp], C.gbox[chunk * kGroupsPerChunk + lane]) < C.c2;
+            const unsigned gmask = __ballot_sync(0xffffffffu, gon);
+            if (C.examined && lane == 0 && gmask)
+                atomicAdd(C.examined, (unsigned long long)__popc(gmask) * kGroup * 64 * RP);
+            const float4* sg = s_geo + st * CH * 2;
+            const float2* sq = s_qq + st * CH;
+#pragma unroll 1
+            for (int j0 = 0; j0 < CH; j0 += SUB) {
+                if (!((gmask >> (j0 / kGroup)) & 1u)) continue;  // warp-uniform
+                float acc[2 * RP];
+#pragma unroll
+                for (int k = 0; k < 2 * RP; ++k) acc[k] = 0.f;
+                constexpr int kUnrollJ = PATH == 0 ? 4 : SUB;
+#pragma unroll kUnrollJ
+                for (int jj = 0; jj < SUB; ++jj) {
+                    const int j = j0 + jj;
+                    const float4 g0 = sg[2 * j];
+                    const float4 g1 = sg[2 * j + 1];
+                    const float2 av = f2(g0.x, g0.y), bv = f2(g0.z, g0.w);
+                    const float2 cv = f2(g1.x, g1.y), dv = f2(g1.z, g1.w);
+                    if constexpr (PATH == 0) {
+                        // r^2 - 1/2 in three exact steps and the warp vote, as
+                        // the SKIP tile of lgm_pairs.cuh
+                        float2 uu[RP];
+                        unsigned mk[RP];
+#pragma unroll
+                        for (int k = 0; k < RP; ++k) {
+                            const float2 pa = __ffma2_rn(tx[k], av, tt[k]);
+                            const float2 pc = __ffma2_rn(tz[k], cv, dv);
+                            uu[k] = __fadd2_rn(__ffma2_rn(ty[k], bv, pa), pc);
+                            mk[k] = min(__float_as_uint(uu[k].x), __float_as_uint(uu[k].y));
+                        }
+#pragma unroll
+                        for (int w = 1; w < RP; w *= 2)
+#pragma unroll
+                            for (int k = 0; k + w < RP; k += 2 * w) mk[k] = min(mk[k], mk[k + w]);
+                        if (__any_sync(0xffffffffu, mk[0] < ulim)) {
+                            const float qs = sq[j].x;
+#pragma unroll
+                            for (int k = 0; k < RP; ++k) {
+                                const float2 r2 = __fadd2_rn(uu[k], half2);
+                                float wx = rsqrt_mufu(r2.x);
+                                float wy = rsqrt_mufu(r2.y);
+                                if (KIND == 1) {
+                                    const int ix =
+                                        min(__float_as_int(r2.x + 8388608.f) & 0x7fffff, A.tab_k);
+                                    const int iy =
+                                        min(__float_as_int(r2.y + 8388608.f) & 0x7fffff, A.tab_k);
+                                    wx = fminf(s_tab[ix], wx);
+                                    wy = fminf(s_tab[iy], wy);
+                                }
+                                fma_if_below(acc[2 * k], qs, wx, __float_as_uint(uu[k].x), ulim);
+                                fma_if_below(acc[2 * k + 1], qs, wy, __float_as_uint(uu[k].y),
+                                             ulim);
+                            }
+                        }
+                    } else {
+                        const float qs = sq[j].x;
+#pragma unroll
+                        for (int k = 0; k < RP; ++k) {
+                            float2 u = __fadd2_rn(dv, tt[k]);
+                            u = __ffma2_rn(tx[k], av, u);
+                            u = __ffma2_rn(ty[k], bv, u);
+                            u = __ffma2_rn(tz[k], cv, u);  // r^2 - 1/2, exact
+                            const float2 r2 = __fadd2_rn(u, half2);
+                            // w(k) from the table; entries 0 and c^2 are 0
+                            const int ix =
+                                min(__float_as_int(r2.x + 8388608.f) & 0x7fffff, A.tab_k);
+                            const int iy =
+                                min(__float_as_int(r2.y + 8388608.f) & 0x7fffff, A.tab_k);
+                            fma_if_below(acc[2 * k], qs, s_tab[ix], __float_as_uint(u.x), ulim);
+                            fma_if_below(acc[2 * k + 1], qs, s_tab[iy], __float_as_uint(u.y),
+                                         ulim);
+                        }
+                    }
+                }
+#pragma unroll
+                for (int k = 0; k < 2 * RP; ++k) acc64[k] += (double)acc[k];
+                if (NORM) {
+#pragma unroll
+                    for (int k = 0; k < 2 * RP; ++k) nrm[NORM ? k : 0] += fabsf(acc[k]);
+                }
+            }
+            __syncthreads();  // every thread is done with stage st
+            ++consumed;
+            if (tid == 0) {
+                fence_proxy_async_smem();
+                issue_next();
+            }
+        }
+        if (failed) break;
+        double* out = A.part + (size_t)it * TS;
+#pragma unroll
+        for (int k = 0; k < 2 * RP; ++k) {
+            const int p = target_of(k);
+            if (p < t_phys) {
+                out[p - base] = acc64[k];
+                if (NORM) A.part_norm[(size_t)it * TS + (p - base)] = nrm[NORM ? k : 0];
+            }
+        }
+    }
+
+    if (failed && tid == 0) {
+        // A stage never completed: wait (bounded) for the copies still in
+        // flight, then leave without results; the host sees DEVERR_TIMEOUT.
+        const uint32_t issued = (uint32_t)s_prod[5];
+        for (uint32_t g = consumed; g < issued; ++g) {
+            const uint32_t parity = (g >> 1) & 1u;
+            for (int i = 0; i < kWaitLimit; ++i)
+                if (mbar_try_wait(&s_bar[g & 1u], parity)) break;
+        }
+    }
+}
+
+template <int KIND, int PATH, int NT, int RP, int SUB, bool NORM = false>
+__global__ void __launch_bounds__(NT) pair_kernel_culled(PairArgs A, CullArgs C) {
+    pair_items_culled<KIND, PATH, NT, RP, SUB, NORM>(A, C);
+}
+
+// (static: each translation unit that launches them has its own copy)
+static __global__ void __launch_bounds__(CH) chunk_boxes_kernel(PairArgs A, CullArgs C) {
+    chunk_boxes_body(A, C, (int)blockIdx.x);
+}
+
+static __global__ void __launch_bounds__(kCullThreads) cull_kernel(CullArgs C) {
+    cull_body(C, (int)blockIdx.x);
+}
+
+// Sum of one physical target's item partials (its tile's items, in order).
+__device__ __forceinline__ double item_sum(const double* __restrict__ part,
+                                           const int* __restrict__ tile_first,
+                                           const int* __restrict__ tile_items, int tile_size,
+                                           int p) {
+    const int tile = p / tile_size, loc = p - tile * tile_size;
+    const int n = tile_items[tile];
+    const double* q = part + (size_t)tile_first[tile] * tile_size + loc;
+    double s = 0.0;
+    int i = 0;
+    for (; i + 4 <= n; i += 4) {  // four loads in flight, then the adds in order
+        double v[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) v[u] = q[(size_t)(i + u) * tile_size];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) s += v[u];
+    }
+    for (; i < n; ++i) s += q[(size_t)i * tile_size];
+    return s;
+}
+
+}  // namespace lgm

@@ -30,7 +30,7 @@
 #include <vector>
 
 #include "langmuir_b200_kmc.h"
-#include "lgm_pairs.cuh"
+#include "lgm_cull.cuh"
 #include "lgm_rng.cuh"
 
 using namespace lgm;
@@ -63,6 +63,7 @@ constexpr uint32_t RNG_RECOMB = 5, RNG_EXCITON = RNG_SOURCE + 4;
 
 constexpr int kNT = 128, kRP = 4, kSUB = 32;
 constexpr int kTile = kNT * 2 * kRP;
+constexpr int kCullPerItem = 2;  // source chunks per work item of the culled pair sum
 
 struct Dev {
     int X, Y, Z, XY, V, hr;
@@ -103,6 +104,17 @@ struct Dev {
     int32_t* bins;             // [ncells + 2]
     int32_t *tkey, *tperm;     // [2 ncap]
     int splits;
+    // Culled pair sums (standalone replicas, lgm_cull.cuh): the sources
+    // sorted by (charge class, lattice cell) and by site inside a bin (skey:
+    // bin per source, stmp: sources scattered by bin, sbins: 3 (ncells + 1)
+    // bin counters), chunk and group boxes, each tile's live chunks and the
+    // work items.  A charge class stays padded to whole chunks.
+    int culled, max_items;
+    int32_t *skey, *stmp, *sbins;
+    Box *cbox, *gbox;
+    int32_t* live;
+    int4* items;
+    int32_t *item_count, *tile_first, *tile_items;
     int src_cap;   // source records capacity (multiple of CH)
     int tpad_cap;  // per-term target block capacity
     unsigned* err;
@@ -204,6 +216,14 @@ __device__ __forceinline__ void choose_body(const Dev& D, const int i) {
     (e ? D.e_f : D.h_f)[k] = f;
 }
 
+// Site of source i in list order: electrons, holes, then defects.
+__device__ __forceinline__ int src_site(const Dev& D, const int i) {
+    const int ne = D.cnt[I_NE], nh = D.cnt[I_NH];
+    if (i < ne) return D.e_site[i];
+    if (i < ne + nh) return D.h_site[i - ne];
+    return D.defects[i - ne - nh];
+}
+
 // Source records (electrons, holes, defects, each padded to whole chunks so
 // that every FP32 run holds one charge sign) and target records (current sites
 // then future sites, one block per term).
@@ -220,21 +240,45 @@ __device__ __forceinline__ void pack_body(const Dev& D, const int j) {
         D.cnt[I_TPHYS] = D.nterms * tpad;
         D.cnt[I_TPAD] = tpad;
     }
-    if (j < nsrc) {  // records past the live chunks are never read
-        float a = 0.f, b = 0.f, c = 0.f, d = -0.5f, q = 0.f;
-        int s = -1;
-        if (j < pe) { if (j < ne) { s = D.e_site[j]; q = -1.f; } }
-        else if (j < pe + ph) { const int k = j - pe; if (k < nh) { s = D.h_site[k]; q = 1.f; } }
-        else if (j < nsrc) { const int k = j - pe - ph; if (k < nd) { s = D.defects[k]; q = (float)D.dq; } }
+    auto record = [&](int dst, int s, float q) {
+        float a = 0.f, b = 0.f, c = 0.f, d = -0.5f;
         if (s >= 0) {
             int x, y, z;
             xyz(D, s, x, y, z);
             a = -2.f * x; b = -2.f * y; c = -2.f * z;
             d = (float)(x * x + y * y + z * z) - 0.5f;
+        } else {
+            q = 0.f;
         }
-        D.geo[2 * j] = make_float4(a, a, b, b);
-        D.geo[2 * j + 1] = make_float4(c, c, d, d);
-        D.qq[j] = make_float2(q, q);
+        D.geo[2 * dst] = make_float4(a, a, b, b);
+        D.geo[2 * dst + 1] = make_float4(c, c, d, d);
+        D.qq[dst] = make_float2(q, q);
+    };
+    if (j < nsrc && !D.culled) {  // records past the live chunks are never read
+        float q = 0.f;
+        int s = -1;
+        if (j < pe) { if (j < ne) { s = D.e_site[j]; q = -1.f; } }
+        else if (j < pe + ph) { const int k = j - pe; if (k < nh) { s = D.h_site[k]; q = 1.f; } }
+        else if (j < nsrc) { const int k = j - pe - ph; if (k < nd) { s = D.defects[k]; q = (float)D.dq; } }
+        record(j, s, q);
+    } else if (j < nsrc) {
+        // Sorted sources: slot j of the scatter by (class, cell) takes its
+        // place at the bin's start plus its rank inside the bin by site (sites
+        // are distinct inside a class), shifted to the class's padded start.
+        const bool pad = (j >= ne && j < pe) || (j >= pe + nh && j < pe + ph) || j >= pe + ph + nd;
+        if (pad) record(j, -1, 0.f);
+        if (j < ne + nh + nd) {
+            const int i = D.stmp[j];
+            const int key = D.skey[i];
+            const int lo = key > 0 ? D.sbins[key - 1] : 0, hi = D.sbins[key];
+            const int si = src_site(D, i);
+            int rank = 0;
+            for (int k = lo; k < hi; ++k) rank += src_site(D, D.stmp[k]) < si;
+            const int cls = key / (D.ncells + 1);
+            const int from = cls == 0 ? 0 : (cls == 1 ? ne : ne + nh);
+            const int to = cls == 0 ? 0 : (cls == 1 ? pe : pe + ph);
+            record(lo + rank - from + to, si, cls == 0 ? -1.f : (cls == 1 ? 1.f : (float)D.dq));
+        }
     }
     if (j < tpad) {
         int s = -1;
@@ -249,8 +293,9 @@ __device__ __forceinline__ void pack_body(const Dev& D, const int j) {
         for (int term = 0; term < 3; ++term) {
             if (!(D.terms & (1u << term))) continue;
             const int xp = term == 0 ? x : (term == 1 ? -1 - x : 2 * D.X - 1 - x);
-            D.tgt[(size_t)slot * tpad + j] =
-                make_float4((float)xp, (float)y, (float)z, (float)(xp * xp + y * y + z * z));
+            // padding slots carry w = -1: left out of the cull's boxes, never read
+            D.tgt[(size_t)slot * tpad + j] = make_float4(
+                (float)xp, (float)y, (float)z, j < t ? (float)(xp * xp + y * y + z * z) : -1.f);
             ++slot;
         }
     }
@@ -261,6 +306,26 @@ __device__ __forceinline__ void finalize_body(const Dev& D, const int g) {
     const int tpad = D.cnt[I_TPAD], tphys = D.cnt[I_TPHYS];
     if (g >= t) return;
     double v = 0.0, n = 0.0;
+    if (D.culled) {
+        // the partials of the tile's work items, in item (= chunk) order
+        for (int slot = 0; slot < D.nterms; ++slot) {
+            const int p = slot * tpad + g;
+            const int tile = p / kTile, loc = p - tile * kTile;
+            const int ni = D.tile_items[tile];
+            const size_t f = (size_t)D.tile_first[tile] * kTile + loc;
+            double s = 0.0, m = 0.0;
+            for (int i = 0; i < ni; ++i) {
+                s += D.part[f + (size_t)i * kTile];
+                m += (double)D.part_norm[f + (size_t)i * kTile];
+            }
+            v = slot == 0 ? s : v - s;
+            n += m;
+        }
+        const int target = D.tperm[g];
+        D.Vt[target] = D.prefactor * v;
+        D.Nt[target] = D.prefactor * n;
+        return;
+    }
     for (int slot = 0; slot < D.nterms; ++slot) {
         double s = 0.0, m = 0.0;
         // four splits' loads in flight, then the adds in split order (same bits)
@@ -296,31 +361,43 @@ __device__ __forceinline__ void finalize_body(const Dev& D, const int g) {
 // The counting sort of the step's targets (current sites of electrons and
 // holes, then their proposed sites, as pack_body lists them) by the Morton
 // rank of their lattice cell; proposed drains go to the last bin.
+// Culled replicas sort their sources the same way, keyed by (charge class,
+// cell): key = class * (ncells + 1) + cell rank.
 __device__ __forceinline__ void tbins_zero_body(const Dev& D, const int i) {
     if (i <= D.ncells) D.bins[i] = 0;
+    if (D.culled && i < 3 * (D.ncells + 1)) D.sbins[i] = 0;
+}
+__device__ __forceinline__ int site_bin(const Dev& D, const int s) {
+    if (s < 0 || s >= D.V) return D.ncells;
+    int x, y, z;
+    xyz(D, s, x, y, z);
+    const int sh = D.cell_shift;
+    return D.cell_rank[(x >> sh) + D.cells_x * ((y >> sh) + D.cells_y * (z >> sh))];
 }
 __device__ __forceinline__ void tbins_body(const Dev& D, const int g) {
     const int ne = D.cnt[I_NE], nh = D.cnt[I_NH];
-    if (g >= 2 * (ne + nh)) return;
-    int s;
-    if (g < ne) s = D.e_site[g];
-    else if (g < ne + nh) s = D.h_site[g - ne];
-    else if (g < 2 * ne + nh) s = D.e_f[g - ne - nh];
-    else s = D.h_f[g - 2 * ne - nh];
-    int b = D.ncells;
-    if (s >= 0 && s < D.V) {
-        int x, y, z;
-        xyz(D, s, x, y, z);
-        const int sh = D.cell_shift;
-        b = D.cell_rank[(x >> sh) + D.cells_x * ((y >> sh) + D.cells_y * (z >> sh))];
+    if (g < 2 * (ne + nh)) {
+        int s;
+        if (g < ne) s = D.e_site[g];
+        else if (g < ne + nh) s = D.h_site[g - ne];
+        else if (g < 2 * ne + nh) s = D.e_f[g - ne - nh];
+        else s = D.h_f[g - 2 * ne - nh];
+        const int b = site_bin(D, s);
+        D.tkey[g] = b;
+        atomicAdd(&D.bins[b], 1);
     }
-    D.tkey[g] = b;
-    atomicAdd(&D.bins[b], 1);
+    if (D.culled && g < ne + nh + (D.dq != 0 ? D.nd : 0)) {
+        const int cls = g < ne ? 0 : (g < ne + nh ? 1 : 2);
+        const int key = cls * (D.ncells + 1) + site_bin(D, src_site(D, g));
+        D.skey[g] = key;
+        atomicAdd(&D.sbins[key], 1);
+    }
 }
 __device__ __forceinline__ void tscatter_body(const Dev& D, const int g) {
     const int ne = D.cnt[I_NE], nh = D.cnt[I_NH];
-    if (g >= 2 * (ne + nh)) return;
-    D.tperm[atomicAdd(&D.bins[D.tkey[g]], 1)] = g;
+    if (g < 2 * (ne + nh)) D.tperm[atomicAdd(&D.bins[D.tkey[g]], 1)] = g;
+    if (D.culled && g < ne + nh + (D.dq != 0 ? D.nd : 0))
+        D.stmp[atomicAdd(&D.sbins[D.skey[g]], 1)] = g;
 }
 
 // ChargeAgent::bindingPotential (chargeagent.cpp:463-481)
@@ -719,7 +796,34 @@ __global__ void k_finalize(Dev D) { finalize_body(D, LGM_THREAD_INDEX); }
 __global__ void k_decide(Dev D) { decide_body(D, LGM_THREAD_INDEX); }
 __global__ void k_tbins_zero(Dev D) { tbins_zero_body(D, LGM_THREAD_INDEX); }
 __global__ void k_tbins(Dev D) { tbins_body(D, LGM_THREAD_INDEX); }
-__global__ void __launch_bounds__(1024) k_tbins_scan(Dev D) { block_exclusive_scan(D.bins, D.ncells + 1); }
+__global__ void __launch_bounds__(1024) k_tbins_scan(Dev D) {
+    if (blockIdx.x == 0) block_exclusive_scan(D.bins, D.ncells + 1);
+    else block_exclusive_scan(D.sbins, 3 * (D.ncells + 1));
+}
+// Source records and work list of the culled pair sum (lgm_cull.cuh).
+__host__ __device__ __forceinline__ PairArgs pair_args(const Dev& D) {
+    PairArgs A;
+    A.geo = D.geo; A.qq = D.qq; A.splits = D.splits; A.tgt = D.tgt; A.part = D.part;
+    A.part_norm = D.part_norm;
+    A.c2 = (float)D.cutoff2; A.tab = D.gtab; A.tab_k = D.gauss ? D.gtab_k : 0;
+    A.err = D.err; A.dyn = D.cnt + I_NCHUNK;  // dyn[0] = n_chunks, dyn[1] = t_phys
+    return A;
+}
+__host__ __device__ __forceinline__ CullArgs cull_args(const Dev& D) {
+    CullArgs C;
+    C.cbox = D.cbox; C.gbox = D.gbox;
+    C.tgt = D.tgt; C.dyn = D.cnt + I_NCHUNK;
+    C.c2 = D.cutoff2; C.tile_size = kTile;
+    C.per_item = kCullPerItem; C.max_items = D.max_items;
+    C.live = D.live; C.live_stride = D.src_cap / CH;
+    C.items = D.items; C.item_count = D.item_count;
+    C.tile_first = D.tile_first; C.tile_items = D.tile_items;
+    return C;
+}
+__global__ void __launch_bounds__(CH) k_chunk_boxes(Dev D) {
+    chunk_boxes_body(pair_args(D), cull_args(D), (int)blockIdx.x);
+}
+__global__ void __launch_bounds__(kCullThreads) k_cull(Dev D) { cull_body(cull_args(D), (int)blockIdx.x); }
 __global__ void k_tscatter(Dev D) { tscatter_body(D, LGM_THREAD_INDEX); }
 __global__ void __launch_bounds__(kGuardThreads) k_guard(Dev D) {
     __shared__ double2 red[32];
@@ -1008,6 +1112,7 @@ struct lgm_kmc {
     float* gtab = nullptr;
     int gtab_k = 0;
     int pair_blocks = 0, pair_tiles = 0;
+    int cull_grid = 0;  // persistent grid of the culled pair kernel (one wave)
     int sm_count = 0;   // SMs of the device (the guard's grid)
     std::string err;
 };
@@ -1067,7 +1172,12 @@ struct Arena {
     }
 };
 
-// World::initialize order (world.cpp:625-643) on a Philox stream.
+// World::initialize (world.cpp:589-650) on one Philox stream: every set-up
+// draw comes from the sequential counter {n, 0, RNG_SETUP, 0} in the order the
+// reference consumes its generator -- placeDefects, placeElectrons,
+// placeHoles, then setPotentialTraps (seeds, growth, the Gaussian spread) --
+// so the reference's own set-up code, given the same draws, builds the same
+// world.  The site.disorder extension draws from its own stream afterwards.
 lgm_status build_world(lgm_kmc* k) {
     const lgm_params& p = k->p;
     const int X = p.grid_x, Y = p.grid_y, Z = p.grid_z, V = X * Y * Z;
@@ -1079,6 +1189,7 @@ lgm_status build_world(lgm_kmc* k) {
     const int max_t = (int)(p.trap_percentage * (double)V);
     std::vector<uint8_t> is_def(V, 0), is_trap(V, 0);
     const lgm_world_config* w = k->wcfg;
+    Stream r{seed, k->replica, RNG_SETUP + 0};
     // placeDefects (world.cpp:659-757): listed defects first, the rest drawn
     {
         const int given = w ? w->n_defects : 0;
@@ -1091,7 +1202,6 @@ lgm_status build_world(lgm_kmc* k) {
             is_def[s] = 1;
             k->defects.push_back(s);
         }
-        Stream r{seed, k->replica, RNG_SETUP + 0};
         long tries = 0;
         while ((int)k->defects.size() < max_d) {
             if (++tries > 10L * V) return kfail(k, LGM_ERR_INVALID_ARGUMENT, "can not seed defects");
@@ -1099,70 +1209,10 @@ lgm_status build_world(lgm_kmc* k) {
             if (!is_def[s]) { is_def[s] = 1; k->defects.push_back(s); }
         }
     }
-    // setPotentialTraps (potential.cpp:74-244): listed traps first (with their
-    // potentials or trap.potential), then random seeds and growth onto
-    // neighbours of the random ones; the Gaussian spread applies to those only
-    {
-        const int forced = w ? w->n_traps : 0;
-        if (forced < 0 || forced > max_t || (forced && !w->traps))
-            return kfail(k, LGM_ERR_INVALID_ARGUMENT, "langmuir: invalid trap parameters");
-        if (forced > 0 && w->n_trap_potentials != 0 &&
-            (w->n_trap_potentials != forced || !w->trap_potentials))
-            return kfail(k, LGM_ERR_INVALID_ARGUMENT,
-                         "langmuir: trapPotential and trap arrays different sizes in checkpoint file");
-        for (int i = 0; i < forced; ++i) {
-            const int s = w->traps[i];
-            if (s < 0 || s >= V) return kfail(k, LGM_ERR_OUT_OF_RANGE, "trap site out of range");
-            is_trap[s] = 1;
-            k->traps.push_back(s);
-            k->trap_pots.push_back(w->n_trap_potentials ? w->trap_potentials[i] : p.trap_potential);
-        }
-        Stream r{seed, k->replica, RNG_SETUP + 1};
-        const int random = max_t - forced;
-        int seeds = (int)(random * p.seed_percentage);
-        int grown = random - seeds;
-        if (random <= 0) { seeds = 0; grown = 0; }
-        if (seeds == 0 && grown > 0) { seeds = grown; grown = 0; }
-        long tries = 0;
-        while ((int)k->traps.size() < forced + seeds) {
-            if (++tries > 100L * V + 1000) return kfail(k, LGM_ERR_INVALID_ARGUMENT, "can not seed traps");
-            const int s = (int)r.below((uint32_t)V);
-            if (!is_trap[s]) { is_trap[s] = 1; k->traps.push_back(s); }
-        }
-        std::vector<int> nb;
-        int progress = 0;
-        while (progress < grown) {
-            if (++tries > 100L * V + 1000) return kfail(k, LGM_ERR_INVALID_ARGUMENT, "can not grow traps");
-            const int n_random = (int)k->traps.size() - forced;
-            const int seed_site = k->traps[forced + (int)r.below((uint32_t)n_random)];
-            host_neighbors1(X, Y, Z, seed_site, nb);
-            const int s = nb[r.below((uint32_t)nb.size())];
-            if (s < V && !is_trap[s]) { is_trap[s] = 1; k->traps.push_back(s); ++progress; }
-        }
-        k->trap_pots.resize(k->traps.size(), p.trap_potential);
-        if (std::fabs(p.gaussian_stdev) > 0)
-            for (size_t i = forced; i < k->trap_pots.size(); ++i)
-                k->trap_pots[i] += r.normal(0.0, p.gaussian_stdev);
-    }
-    // setPotentialZero / Linear / Gate (potential.cpp:17-72), traps, disorder
-    k->pot.assign(V, 0.0);
-    const double m = (p.voltage_right - p.voltage_left) / (double)X, b = p.voltage_left;
-    for (int i = 0; i < X; ++i)
-        for (int j = 0; j < Y; ++j)
-            for (int z = 0; z < Z; ++z) k->pot[X * (j + z * Y) + i] += m * (i + 0.5) + b;
-    if (!(Z == 1 || p.slope_z == 0))
-        for (int i = 0; i < X; ++i)
-            for (int j = 0; j < Y; ++j)
-                for (int z = 0; z < Z; ++z) k->pot[X * (j + z * Y) + i] += p.slope_z * (z + 0.5);
-    for (size_t i = 0; i < k->traps.size(); ++i) k->pot[k->traps[i]] += k->trap_pots[i];
-    if (p.site_disorder > 0) {
-        Stream r{seed, k->replica, RNG_SETUP + 2};
-        for (int s = 0; s < V; ++s) k->pot[s] += r.normal(0.0, p.site_disorder);
-    }
     // placeElectrons / placeHoles (world.cpp:759-959): listed sites first, then
-    // tryToSeed at uniform sites up to max * seed.charges
-    auto seed_carriers = [&](int max, uint32_t purpose, std::vector<int32_t>& out) -> bool {
-        Stream r{seed, k->replica, purpose};
+    // SourceAgent::tryToSeed at uniform sites (sourceagent.cpp:71-80,
+    // validToInject 192-232) up to max * seed.charges
+    auto seed_carriers = [&](int max, std::vector<int32_t>& out) -> bool {
         std::vector<uint8_t> occ(V, 0);
         for (int s : out) occ[s] = 1;
         long tries = 0;
@@ -1220,10 +1270,69 @@ lgm_status build_world(lgm_kmc* k) {
             }
         }
     }
-    if (!seed_carriers(k->max_e, RNG_SETUP + 3, k->e0))
+    if (!seed_carriers(k->max_e, k->e0))
         return kfail(k, LGM_ERR_INVALID_ARGUMENT, "can not seed electrons");
-    if (!seed_carriers(k->max_h, RNG_SETUP + 4, k->h0))
+    if (!seed_carriers(k->max_h, k->h0))
         return kfail(k, LGM_ERR_INVALID_ARGUMENT, "can not seed holes");
+    // setPotentialTraps (potential.cpp:74-244): listed traps first (with their
+    // potentials or trap.potential), then random seeds and growth onto
+    // neighbours of the random ones; the Gaussian spread applies to those only
+    {
+        const int forced = w ? w->n_traps : 0;
+        if (forced < 0 || forced > max_t || (forced && !w->traps))
+            return kfail(k, LGM_ERR_INVALID_ARGUMENT, "langmuir: invalid trap parameters");
+        if (forced > 0 && w->n_trap_potentials != 0 &&
+            (w->n_trap_potentials != forced || !w->trap_potentials))
+            return kfail(k, LGM_ERR_INVALID_ARGUMENT,
+                         "langmuir: trapPotential and trap arrays different sizes in checkpoint file");
+        for (int i = 0; i < forced; ++i) {
+            const int s = w->traps[i];
+            if (s < 0 || s >= V) return kfail(k, LGM_ERR_OUT_OF_RANGE, "trap site out of range");
+            is_trap[s] = 1;
+            k->traps.push_back(s);
+            k->trap_pots.push_back(w->n_trap_potentials ? w->trap_potentials[i] : p.trap_potential);
+        }
+        const int random = max_t - forced;
+        int seeds = (int)(random * p.seed_percentage);
+        int grown = random - seeds;
+        if (random <= 0) { seeds = 0; grown = 0; }
+        if (seeds == 0 && grown > 0) { seeds = grown; grown = 0; }
+        long tries = 0;
+        while ((int)k->traps.size() < forced + seeds) {
+            if (++tries > 100L * V + 1000) return kfail(k, LGM_ERR_INVALID_ARGUMENT, "can not seed traps");
+            const int s = (int)r.below((uint32_t)V);
+            if (!is_trap[s]) { is_trap[s] = 1; k->traps.push_back(s); }
+        }
+        std::vector<int> nb;
+        int progress = 0;
+        while (progress < grown) {
+            if (++tries > 100L * V + 1000) return kfail(k, LGM_ERR_INVALID_ARGUMENT, "can not grow traps");
+            const int n_random = (int)k->traps.size() - forced;
+            const int seed_site = k->traps[forced + (int)r.below((uint32_t)n_random)];
+            host_neighbors1(X, Y, Z, seed_site, nb);
+            const int s = nb[r.below((uint32_t)nb.size())];
+            if (s < V && !is_trap[s]) { is_trap[s] = 1; k->traps.push_back(s); ++progress; }
+        }
+        k->trap_pots.resize(k->traps.size(), p.trap_potential);
+        if (std::fabs(p.gaussian_stdev) > 0)
+            for (size_t i = forced; i < k->trap_pots.size(); ++i)
+                k->trap_pots[i] += r.normal(0.0, p.gaussian_stdev);
+    }
+    // setPotentialZero / Linear / Gate (potential.cpp:17-72), traps, disorder
+    k->pot.assign(V, 0.0);
+    const double m = (p.voltage_right - p.voltage_left) / (double)X, b = p.voltage_left;
+    for (int i = 0; i < X; ++i)
+        for (int j = 0; j < Y; ++j)
+            for (int z = 0; z < Z; ++z) k->pot[X * (j + z * Y) + i] += m * (i + 0.5) + b;
+    if (!(Z == 1 || p.slope_z == 0))
+        for (int i = 0; i < X; ++i)
+            for (int j = 0; j < Y; ++j)
+                for (int z = 0; z < Z; ++z) k->pot[X * (j + z * Y) + i] += p.slope_z * (z + 0.5);
+    for (size_t i = 0; i < k->traps.size(); ++i) k->pot[k->traps[i]] += k->trap_pots[i];
+    if (p.site_disorder > 0) {
+        Stream rd{seed, k->replica, RNG_SETUP + 2};
+        for (int s = 0; s < V; ++s) k->pot[s] += rd.normal(0.0, p.site_disorder);
+    }
     return LGM_OK;
 }
 
@@ -1257,6 +1366,12 @@ lgm_status upload_carriers(lgm_kmc* k, const int32_t* e, int ne, const int32_t* 
 
 using KPairFn = void (*)(PairArgs);
 
+using KCulledFn = void (*)(PairArgs, CullArgs);
+KCulledFn kmc_pair_culled(int gauss) {
+    return gauss ? &pair_kernel_culled<1, 0, kNT, kRP, kSUB, true>
+                 : &pair_kernel_culled<0, 0, kNT, kRP, kSUB, true>;
+}
+
 KPairFn kmc_pair(int gauss, int sorted = 1) {
     if (sorted)
         return gauss ? &pair_kernel<1, 0, kNT, kRP, kSUB, true, true>
@@ -1273,20 +1388,25 @@ lgm_status enqueue_step(lgm_kmc* k) {
     k_choose<<<(nc + blk - 1) / blk, blk, 0, st>>>(D);
     if (D.coulomb) {
         if (D.sorted) {
-            k_tbins_zero<<<(D.ncells + 1 + blk - 1) / blk, blk, 0, st>>>(D);
-            k_tbins<<<(2 * nc + blk - 1) / blk, blk, 0, st>>>(D);
-            k_tbins_scan<<<1, 1024, 0, st>>>(D);
-            k_tscatter<<<(2 * nc + blk - 1) / blk, blk, 0, st>>>(D);
+            const int nz = D.culled ? 3 * (D.ncells + 1) : D.ncells + 1;
+            const int nb = std::max(2 * nc, nc + (D.dq != 0 ? D.nd : 0));
+            k_tbins_zero<<<(nz + blk - 1) / blk, blk, 0, st>>>(D);
+            k_tbins<<<(nb + blk - 1) / blk, blk, 0, st>>>(D);
+            k_tbins_scan<<<D.culled ? 2 : 1, 1024, 0, st>>>(D);
+            k_tscatter<<<(nb + blk - 1) / blk, blk, 0, st>>>(D);
         }
         const int npack = std::max(D.src_cap, D.tpad_cap);
         k_pack<<<(npack + blk - 1) / blk, blk, 0, st>>>(D);
-        PairArgs A;
-        A.geo = D.geo; A.qq = D.qq; A.splits = D.splits; A.tgt = D.tgt; A.part = D.part;
-        A.part_norm = D.part_norm;
-        A.c2 = (float)D.cutoff2; A.tab = k->gtab; A.tab_k = D.gauss ? k->gtab_k : 0;
-        A.err = D.err; A.dyn = D.cnt + I_NCHUNK;  // dyn[0] = n_chunks, dyn[1] = t_phys
-        kmc_pair(D.gauss, D.sorted)<<<dim3(k->pair_tiles, D.splits), kNT, pair_smem_bytes(A.tab_k),
-                                      st>>>(A);
+        const PairArgs A = pair_args(D);
+        if (D.culled) {
+            k_chunk_boxes<<<D.src_cap / CH, CH, 0, st>>>(D);
+            k_cull<<<k->pair_tiles, kCullThreads, 0, st>>>(D);
+            kmc_pair_culled(D.gauss)<<<k->cull_grid, kNT, pair_smem_bytes(A.tab_k), st>>>(
+                A, cull_args(D));
+        } else {
+            kmc_pair(D.gauss, D.sorted)<<<dim3(k->pair_tiles, D.splits), kNT,
+                                          pair_smem_bytes(A.tab_k), st>>>(A);
+        }
         k_finalize<<<(2 * nc + blk - 1) / blk, blk, 0, st>>>(D);
     }
     k_decide<<<(nc + blk - 1) / blk, blk, 0, st>>>(D);
@@ -1469,7 +1589,21 @@ static lgm_status kmc_create_impl(const lgm_params* pin, int32_t device, uint32_
     DA(D.cnt, I_NUM); DA(D.ctr, C_NUM);
     DA(D.geo, 2 * D.src_cap); DA(D.qq, D.src_cap);
     DA(D.tgt, tphys_cap + kTile);
-    DA(D.part, (size_t)D.splits * tphys_cap); DA(D.part_norm, (size_t)D.splits * tphys_cap);
+    // A standalone replica's pair sum culls source chunks beyond the cutoff;
+    // a batch's replicas keep the batch's work-item kernels.
+    D.culled = (!pool && D.coulomb) ? 1 : 0;
+    const int src_chunks = D.src_cap / CH;
+    D.max_items = std::min(kMaxItemsPerTile, (src_chunks + kCullPerItem - 1) / kCullPerItem);
+    const size_t part_n = D.culled ? (size_t)k->pair_tiles * D.max_items * kTile
+                                   : (size_t)D.splits * tphys_cap;
+    DA(D.part, part_n); DA(D.part_norm, part_n);
+    if (D.culled) {
+        DA(D.skey, D.cap_e + D.cap_h + nd_src); DA(D.stmp, D.cap_e + D.cap_h + nd_src);
+        DA(D.cbox, src_chunks); DA(D.gbox, (size_t)src_chunks * kGroupsPerChunk);
+        DA(D.live, (size_t)k->pair_tiles * src_chunks);
+        DA(D.items, (size_t)k->pair_tiles * D.max_items);
+        DA(D.item_count, 1); DA(D.tile_first, k->pair_tiles); DA(D.tile_items, k->pair_tiles);
+    }
     DA(D.Vt, 2 * ncap); DA(D.Nt, 2 * ncap);
     DA(D.err, 1);
     DA(D.phase, k->V);
@@ -1487,6 +1621,7 @@ static lgm_status kmc_create_impl(const lgm_params* pin, int32_t device, uint32_
     int32_t* crank_d = nullptr;
     DA(crank_d, D.ncells);
     DA(D.bins, D.ncells + 2);
+    if (D.culled) DA(D.sbins, 3 * (D.ncells + 1) + 1);
     DA(D.tkey, 2 * ncap);
     DA(D.tperm, 2 * ncap);
 #undef DA
@@ -1511,9 +1646,17 @@ static lgm_status kmc_create_impl(const lgm_params* pin, int32_t device, uint32_
         for (int sorted = 0; sorted < 2; ++sorted)
             cudaFuncSetAttribute(kmc_pair(1, sorted), cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)pair_smem_bytes(kmax));
+        cudaFuncSetAttribute(kmc_pair_culled(1), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)pair_smem_bytes(kmax));
     }
     cudaMemcpy(crank_d, crank.data(), sizeof(int32_t) * crank.size(), cudaMemcpyHostToDevice);
     D.cell_rank = crank_d;
+    if (D.culled) {
+        int cbps = 1;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&cbps, kmc_pair_culled(D.gauss), kNT,
+                                                      pair_smem_bytes(D.gauss ? D.gtab_k : 0));
+        k->cull_grid = n_sms * std::max(1, cbps);
+    }
     {
         std::vector<double> w(std::max(D.cutoff2, 1), 0.0);
         for (int r2 = 1; r2 < D.cutoff2; ++r2) {
@@ -1557,6 +1700,39 @@ lgm_status lgm_kmc_create_from(const lgm_params* pin, const lgm_world_config* w,
                                uint32_t replica, lgm_kmc** out) {
     if (!w) return LGM_ERR_INVALID_ARGUMENT;
     return kmc_create_impl(pin, device, replica, out, nullptr, nullptr, w);
+}
+
+lgm_status lgm_kmc_world_host(const lgm_params* pin, uint32_t replica, double* site_energy,
+                              int32_t* defects, int32_t d_cap, int32_t* traps, double* trap_pots,
+                              int32_t t_cap, int32_t* electrons, int32_t e_cap, int32_t* holes,
+                              int32_t h_cap, int32_t* counts) {
+    if (!pin || !counts) return LGM_ERR_INVALID_ARGUMENT;
+    lgm_kmc k;
+    k.p = *pin;
+    k.replica = replica;
+    char msg[256] = {0};
+    lgm_status st = lgm_params_check(&k.p, msg, sizeof msg);
+    if (st != LGM_OK) {
+        g_kmc_create_error = msg;
+        return st;
+    }
+    if ((st = build_world(&k)) != LGM_OK) {
+        g_kmc_create_error = k.err;
+        return st;
+    }
+    counts[0] = (int32_t)k.defects.size();
+    counts[1] = (int32_t)k.traps.size();
+    counts[2] = (int32_t)k.e0.size();
+    counts[3] = (int32_t)k.h0.size();
+    if (counts[0] > d_cap || counts[1] > t_cap || counts[2] > e_cap || counts[3] > h_cap)
+        return LGM_ERR_CAPACITY;
+    if (site_energy) std::memcpy(site_energy, k.pot.data(), sizeof(double) * k.pot.size());
+    if (defects) std::memcpy(defects, k.defects.data(), sizeof(int32_t) * k.defects.size());
+    if (traps) std::memcpy(traps, k.traps.data(), sizeof(int32_t) * k.traps.size());
+    if (trap_pots) std::memcpy(trap_pots, k.trap_pots.data(), sizeof(double) * k.trap_pots.size());
+    if (electrons) std::memcpy(electrons, k.e0.data(), sizeof(int32_t) * k.e0.size());
+    if (holes) std::memcpy(holes, k.h0.data(), sizeof(int32_t) * k.h0.size());
+    return LGM_OK;
 }
 
 lgm_status lgm_kmc_destroy(lgm_kmc* k) {

@@ -144,6 +144,8 @@ N.SIGNATURES.update({
     "lgm_kmc_last_outcomes": (_i32, [_vp, _vp, _vp, _i32]),
     "lgm_kmc_set_morphology": (_i32, [_vp, np.ctypeslib.ndpointer(dtype=np.uint8,
                                                                   flags="C_CONTIGUOUS")]),
+    "lgm_kmc_world_host": (_i32, [ctypes.POINTER(Params), ctypes.c_uint32, _vp, _vp, _i32, _vp,
+                                  _vp, _i32, _vp, _i32, _vp, _i32, _vp]),
 })
 if N._lib is not None:  # bind the new symbols if the library was already loaded
     for _name in ("lgm_params_default", "lgm_params_format", "lgm_kmc_create_from",
@@ -151,9 +153,32 @@ if N._lib is not None:  # bind the new symbols if the library was already loaded
                   "lgm_params_check", "lgm_kmc_create", "lgm_kmc_destroy", "lgm_kmc_last_error",
                   "lgm_kmc_run", "lgm_kmc_stats_get", "lgm_kmc_get_carriers",
                   "lgm_kmc_set_carriers", "lgm_kmc_get_world", "lgm_kmc_last_outcomes",
-                  "lgm_kmc_set_morphology"):
+                  "lgm_kmc_set_morphology", "lgm_kmc_world_host"):
         _fn = getattr(N._lib, _name)
         _fn.restype, _fn.argtypes = N.SIGNATURES[_name]
+
+
+def world_host(params: Params, replica: int = 0) -> dict:
+    """The world a replica starts from, built on the host alone
+    (lgm_kmc_world_host): site energies, defects, traps with their
+    potentials, and the seeded electron and hole lists."""
+    V = params.grid_x * params.grid_y * params.grid_z
+    cap = V
+    pot = np.zeros(V, np.float64)
+    d = np.zeros(cap, np.int32)
+    t = np.zeros(cap, np.int32)
+    tp = np.zeros(cap, np.float64)
+    e = np.zeros(cap, np.int32)
+    h = np.zeros(cap, np.int32)
+    cnt = np.zeros(4, np.int32)
+    st = N.lib().lgm_kmc_world_host(ctypes.byref(params), int(replica), pot.ctypes.data,
+                                    d.ctypes.data, cap, t.ctypes.data, tp.ctypes.data, cap,
+                                    e.ctypes.data, cap, h.ctypes.data, cap, cnt.ctypes.data)
+    if st != N.OK:
+        raise N.LgmError(st, (N.lib().lgm_kmc_last_error(None) or b"").decode())
+    nd, nt, ne, nh = (int(x) for x in cnt)
+    return dict(site_energy=pot, defects=d[:nd].copy(), traps=t[:nt].copy(),
+                trap_potentials=tp[:nt].copy(), electrons=e[:ne].copy(), holes=h[:nh].copy())
 
 
 class KMC:
