@@ -37,9 +37,18 @@ def lib():
         _lib.ref_kmc_create.restype = _vp
         _lib.ref_kmc_create.argtypes = [_vp, ctypes.c_uint32] + [_vp, ctypes.c_int] * 5 + [
             ctypes.c_char_p, ctypes.c_int]
-        for name in ("ref_kmc_sizes", "ref_kmc_world", "ref_kmc_carriers", "ref_kmc_step",
-                     "ref_kmc_counters", "ref_kmc_neighbors", "ref_kmc_coupling"):
-            getattr(_lib, name).restype = ctypes.c_int
+        sig = {"ref_kmc_sizes": [_vp, _vp],
+               "ref_kmc_world": [_vp, _vp, _vp, _vp, _vp, _vp],
+               "ref_kmc_carriers": [_vp, _vp, _vp],
+               "ref_kmc_step": [_vp, _vp, _vp, ctypes.c_char_p, ctypes.c_int],
+               "ref_kmc_counters": [_vp, _vp],
+               "ref_kmc_neighbors": [_vp, ctypes.c_int, ctypes.c_int, _vp, ctypes.c_int],
+               "ref_kmc_coupling": [_vp, _vp]}
+        for name, args in sig.items():
+            fn = getattr(_lib, name)
+            fn.restype = ctypes.c_int
+            fn.argtypes = args
+        _lib.ref_kmc_destroy.restype = None
         _lib.ref_kmc_destroy.argtypes = [_vp]
     return _lib
 
