@@ -6,8 +6,12 @@ baseline only).
   createDrains derive from the input keys (world.cpp:982-1030, 1110-1150).
 * ``interface_bonds`` -- donor-acceptor bonds in the order
   lgm_kmc_set_morphology lists them.
-* ``oracle_for`` -- a KmcOracle over the replica's site energies, defects and
+* ``oracle_for`` -- a KmcOracle over a world's site energies, defects and
   carriers, with the same seed and replica key.
+* ``independent_world`` -- the world a replica starts from, taken from the
+  parameters alone: the library's host set-up (lgm_kmc_world_host), which
+  tests/test_reference_pin.py pins bit for bit to the reference's own
+  World::initialize; never read back from a GPU replica.
 """
 import numpy as np
 
@@ -80,3 +84,18 @@ def oracle_for(O, p, world, e, h, max_e, max_h, replica=0, step=0, phase=None):
             bonds = interface_bonds(phase, q.grid_x, q.grid_y, q.grid_z)
     return O.KmcOracle(orc, world["site_energy"], world["defects"], e, h, cfg, step,
                        phase=phase, bonds=bonds)
+
+
+def independent_world(p, replica=0):
+    """Site energies, defects and seeded carriers of replica ``replica`` of
+    parameters ``p`` (lgm_kmc_world_host, no device involved)."""
+    from langmuir_b200.kmc import world_host
+    return world_host(p, replica)
+
+
+def assert_same_world(gpu_world, world):
+    """The world a GPU replica holds equals the independent one."""
+    np.testing.assert_array_equal(gpu_world["site_energy"], world["site_energy"])
+    np.testing.assert_array_equal(gpu_world["defects"], world["defects"])
+    np.testing.assert_array_equal(gpu_world["traps"], world["traps"])
+    np.testing.assert_array_equal(gpu_world["trap_potentials"], world["trap_potentials"])

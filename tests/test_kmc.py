@@ -13,7 +13,9 @@ import pytest
 
 import langmuir_b200 as L
 from langmuir_b200 import _native as N
-from oracle.kmc_setup import interface_bonds, oracle_for, rates  # noqa: F401
+from oracle import refkmc
+from oracle.kmc_setup import (assert_same_world, independent_world, interface_bonds,  # noqa: F401
+                              oracle_for, rates)
 
 
 def make_params(**keys):
@@ -147,7 +149,11 @@ def run_parity(O, name, keys, replica=0):
             g.set_morphology(phase)
         st = g.stats()
         e0, h0 = g.carriers()
-        k = oracle_for(O, p, g.world(), e0, h0, st["max_electrons"], st["max_holes"], replica,
+        world = independent_world(p, replica)
+        assert_same_world(g.world(), world)
+        np.testing.assert_array_equal(e0, world["electrons"])
+        np.testing.assert_array_equal(h0, world["holes"])
+        k = oracle_for(O, p, world, e0, h0, st["max_electrons"], st["max_holes"], replica,
                        phase=phase)
         worst = 0.0
         for s in range(steps):
@@ -327,7 +333,9 @@ def test_batch_replica_matches_oracle(oracle_mod, fused):
         for i, r in enumerate(reps):
             st = r.stats()
             e0, h0 = r.carriers()
-            orcs.append(oracle_for(oracle_mod, params[i], r.world(), e0, h0, st["max_electrons"],
+            world = independent_world(params[i], 7 + i)
+            assert_same_world(r.world(), world)
+            orcs.append(oracle_for(oracle_mod, params[i], world, e0, h0, st["max_electrons"],
                                    st["max_holes"], replica=7 + i))
         for _ in range(steps):
             for k in orcs:
@@ -339,3 +347,43 @@ def test_batch_replica_matches_oracle(oracle_mod, fused):
             np.testing.assert_array_equal(e, e_o)
             np.testing.assert_array_equal(h, h_o)
             np.testing.assert_array_equal(np.array(r.stats()["counters"], np.uint64), k.counters)
+
+
+# ---- GPU: the step against the reference's own compiled code ---------------------------
+REFERENCE_CASES = [n for n, k in CASES.items()
+                   if not any(k.get(x) for x in ("image_charges", "site_disorder",
+                                                  "morphology_confine", "generation_interface"))
+                   and "morphology" not in k]
+
+
+@pytest.mark.gpu
+@pytest.mark.skipif(not refkmc.available(), reason="the compiled reference is not built")
+@pytest.mark.parametrize("name", REFERENCE_CASES)
+def test_gpu_step_matches_the_reference_engine(name):
+    """The GPU replica and the reference's World + agents (oracle/_ref,
+    compiled from its sources) from the same parameters: the same world, then
+    the same outcomes and carrier lists after every step and the same flux
+    counters -- no restatement in between."""
+    keys = dict(CASES[name])
+    steps = keys.pop("steps")
+    p = make_params(**keys)
+    ref = refkmc.RefKMC(p, 2)
+    with L.KMC(p, device=0, replica=2) as g:
+        w = ref.world()
+        gw = g.world()
+        np.testing.assert_array_equal(gw["site_energy"], w["site_energy"])
+        np.testing.assert_array_equal(gw["defects"], w["defects"])
+        for a, b in zip(g.carriers(), ref.carriers()):
+            np.testing.assert_array_equal(a, b)
+        for s in range(steps):
+            n0 = sum(len(a) for a in ref.carriers())
+            out_r, de_r = ref.step()
+            g.run(1)
+            out_g, de_g = g.last_outcomes(n0)
+            np.testing.assert_array_equal(out_g, out_r, err_msg=f"{name}: outcomes, step {s}")
+            for a, b in zip(g.carriers(), ref.carriers()):
+                np.testing.assert_array_equal(a, b, err_msg=f"{name}: carriers, step {s}")
+            met = (out_r == 1) | (out_r == 2)
+            if met.any():
+                assert np.abs(de_g[met] - de_r[met]).max() <= 1e-4
+        np.testing.assert_array_equal(np.array(g.stats()["counters"], np.uint64), ref.counters)

@@ -23,7 +23,7 @@ import pytest
 
 import bench
 import langmuir_b200 as L
-from oracle.kmc_setup import oracle_for
+from oracle.kmc_setup import assert_same_world, independent_world, oracle_for
 from tests.test_kmc import CASES, blob_phase, make_params
 
 pytestmark = pytest.mark.gpu
@@ -34,7 +34,9 @@ def step_against_oracle(O, g, p, steps, replica=0, phase=None, threads=0):
     (metropolis decisions, guard evaluations, worst |dE| difference)."""
     st = g.stats()
     e0, h0 = g.carriers()
-    k = oracle_for(O, p, g.world(), e0, h0, st["max_electrons"], st["max_holes"], replica,
+    world = independent_world(p, replica)
+    assert_same_world(g.world(), world)
+    k = oracle_for(O, p, world, e0, h0, st["max_electrons"], st["max_holes"], replica,
                    step=st["step"], phase=phase)
     guard0 = st["guard_evaluations"]
     worst, metropolis = 0.0, 0
@@ -137,7 +139,9 @@ def test_largest_batched_replicas_match_oracle(oracle_mod):
             st = r.stats()
             e0, h0 = r.carriers()
             assert st["max_electrons"] + st["max_holes"] > 10000
-            orcs.append(oracle_for(oracle_mod, chosen[i], r.world(), e0, h0, st["max_electrons"],
+            world = independent_world(chosen[i], i)
+            assert_same_world(r.world(), world)
+            orcs.append(oracle_for(oracle_mod, chosen[i], world, e0, h0, st["max_electrons"],
                                    st["max_holes"], replica=i))
         for s in range(steps):
             outs = [k.step()[0] for k in orcs]
