@@ -53,8 +53,14 @@ enum { C_XSRC = 16, C_RECOMB = 18, C_PROPOSALS = 20, C_ACCEPTED = 21, C_GUARD = 
 // the stable compaction of that list starts.
 enum { I_NE = 0, I_NH, I_STEP, I_NFLAG, I_REMOVED, I_NE0, I_NH0, I_NCHUNK, I_TPHYS, I_TPAD,
        I_NBONDS, I_FIRST_E, I_FIRST_H, I_NUM };
-// Recombination and exciton-source purposes of the random stream.
+// Recombination, exciton-source and charge-balancing purposes of the random
+// stream (balancing try t of electrons draws at {step, t, RNG_BALANCE_E}, its
+// side at {step, t, RNG_BALANCE_E + 1}; holes at RNG_BALANCE_H, + 1).
 constexpr uint32_t RNG_RECOMB = 5, RNG_EXCITON = RNG_SOURCE + 4;
+constexpr uint32_t RNG_BALANCE_E = RNG_SOURCE + 8, RNG_BALANCE_H = RNG_SOURCE + 10;
+// Tries of one species' balancing per step before the reference gives up
+// (Simulation::balanceCharges, simulation.cpp:272-276).
+constexpr int kBalanceTries = 1024;
 
 // Guard band: FP32C potentials carry at most (2 ulp rsqrt + 31 u run sums)
 // ~ 2.1e-6 N of error each; a decision whose energy lies within
@@ -118,6 +124,11 @@ struct Dev {
     int src_cap;   // source records capacity (multiple of CH)
     int tpad_cap;  // per-term target block capacity
     unsigned* err;
+    // injection energetics (sourceagent.cpp:125-181) and charge balancing
+    // (simulation.cpp:253-353): source.metropolis, source.coulomb,
+    // balance.charges, and the electrode voltages that pick the balancing side
+    int src_metro, src_coulomb, balance;
+    double volt_l, volt_r;
     // solar-cell set-up
     int solar, rec_range, confine, gen_iface;
     double gen_rate, rec_rate;
@@ -730,62 +741,173 @@ __device__ int compact(int32_t* a, int n, int* warp_sums, int start) {
     return base;
 }
 
-__device__ __forceinline__ void compact_inject_body(const Dev& D, int* warp_sums) {
+// Potential::coulombE/H/D or coulombImageE/H/D (potential.cpp:351-415,
+// 483-547, 615-683) at one site: point charges q at `sites`, direct or the
+// image in the left electrode (x distance x_i + x_j + 1), 1/r in FP64 as the
+// reference's iR table holds it (1.0 / sqrt(r^2)), times the prefactor.  The
+// whole block takes part; the partial sums are added in a fixed order.
+__device__ double block_species_potential(const Dev& D, int site, const int32_t* sites, int n,
+                                          double q, bool image, double* red) {
+    int xi, yi, zi;
+    xyz(D, site, xi, yi, zi);
+    double acc = 0.0;
+    for (int j = threadIdx.x; j < n; j += blockDim.x) {
+        int xj, yj, zj;
+        xyz(D, sites[j], xj, yj, zj);
+        const int dx = image ? xi + xj + 1 : xi - xj, dy = yi - yj, dz = zi - zj;
+        const int r2 = dx * dx + dy * dy + dz * dz;
+        if (r2 > 0 && r2 < D.cutoff2) {
+            const double w = 1.0 / sqrt((double)r2);
+            acc = image ? acc - w * q : acc + w * q;
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    __syncthreads();
+    if (lane == 0) red[warp] = acc;
+    __syncthreads();
+    double total = 0.0;
+    for (int w = 0; w < nw; ++w) total += red[w];
+    __syncthreads();
+    return total * D.prefactor;
+}
+
+// Block-shared state of the injection phase.
+struct InjectState {
+    int ne, nh, site, valid;
+    double u;
+};
+
+// SourceAgent::tryToInject (sourceagent.cpp:92-103) for electrode source s
+// (0 eL, 1 eR, 2 hL, 3 hR) on the draw at {step, index, purpose}: the site
+// from the face, validToInject (sourceagent.cpp:192-232), then shouldTransport
+// (sourceagent.cpp:168-181): chooseYes on the rate, or with source.metropolis
+// metropolisWithCoupling on energyChange (sourceagent.cpp:125-161), which with
+// source.coulomb adds the Coulomb and left-image sums at the site (the
+// source's own potential is 0).  Every thread of the block calls it.
+__device__ void block_try_inject(const Dev& D, InjectState& S, int s, uint32_t step,
+                                 uint32_t index, uint32_t purpose, double* red) {
+    const bool e = s < 2, left = (s % 2) == 0;
+    if (threadIdx.x == 0) {
+        D.ctr[2 * s] += 1;  // attempts (sourceagent.cpp:94)
+        const Philox4 r = draw(D, step, index, purpose);
+        const int idx = (int)uint_below(r.w[0], (uint32_t)(D.Y * D.Z));
+        const int site = D.X * idx + (left ? 0 : D.X - 1);
+        const uint8_t* own = e ? D.et : D.ht;
+        const int count = e ? S.ne : S.nh;
+        const int cap = e ? D.cap_e : D.cap_h;
+        S.site = site;
+        S.valid = count < cap && D.rate_src[s] > 0 && own[site] == T_EMPTY;
+        S.u = unit_double(r.w[1], r.w[2]);
+    }
+    __syncthreads();
+    if (!S.valid) return;
+    const int site = S.site;
+    double de = 0.0;
+    if (D.src_metro) {
+        double p2 = D.pot[site];
+        if (D.src_coulomb) {
+            // p2 += coulombH + coulombImageH + coulombE + coulombImageE (+ D)
+            p2 += block_species_potential(D, site, D.h_site, S.nh, 1.0, false, red);
+            p2 += block_species_potential(D, site, D.h_site, S.nh, 1.0, true, red);
+            p2 += block_species_potential(D, site, D.e_site, S.ne, -1.0, false, red);
+            p2 += block_species_potential(D, site, D.e_site, S.ne, -1.0, true, red);
+            if (D.dq != 0) {
+                p2 += block_species_potential(D, site, D.defects, D.nd, (double)D.dq, false, red);
+                p2 += block_species_potential(D, site, D.defects, D.nd, (double)D.dq, true, red);
+            }
+        }
+        de = e ? 0.0 - p2 : p2 - 0.0;
+    }
+    if (threadIdx.x == 0) {
+        const double rate = D.rate_src[s];
+        const bool accept = D.src_metro ? metropolis(de, D.beta, rate, S.u) : rate > S.u;
+        if (accept) {
+            D.ctr[2 * s + 1] += 1;
+            (e ? D.et : D.ht)[site] = e ? T_ELECTRON : T_HOLE;
+            if (e) D.e_site[S.ne++] = site;
+            else D.h_site[S.nh++] = site;
+        }
+    }
+    __syncthreads();
+}
+
+__device__ __forceinline__ void compact_inject_body(const Dev& D, int* warp_sums, double* red) {
+    __shared__ InjectState S;
     int ne = D.cnt[I_NE0], nh = D.cnt[I_NH0];
     if (D.cnt[I_REMOVED]) {
         ne = compact(D.e_site, ne, warp_sums, D.cnt[I_FIRST_E]);
         nh = compact(D.h_site, nh, warp_sums, D.cnt[I_FIRST_H]);
     }
-    if (threadIdx.x != 0) return;
     const uint32_t step = (uint32_t)D.cnt[I_STEP];
+    if (threadIdx.x == 0) {
+        S.ne = ne;
+        S.nh = nh;
+    }
+    __syncthreads();
     if (D.solar) {
-        // ExcitonSourceAgent::tryToInject (sourceagent.cpp:92-103, 120-123, 234-250)
-        D.ctr[C_XSRC] += 1;
-        const Philox4 r = draw(D, step, 0u, RNG_EXCITON);
-        const int nb = D.cnt[I_NBONDS];
-        int es, hs;
-        if (D.gen_iface && nb > 0) {
-            const uint32_t b = uint_below(r.w[0], (uint32_t)nb);
-            hs = D.bonds[2 * b];
-            es = D.bonds[2 * b + 1];
-        } else {
-            es = hs = (int)uint_below(r.w[0], (uint32_t)D.V);
+        if (threadIdx.x == 0) {
+            // ExcitonSourceAgent::tryToInject (sourceagent.cpp:92-103, 120-123, 234-250)
+            D.ctr[C_XSRC] += 1;
+            const Philox4 r = draw(D, step, 0u, RNG_EXCITON);
+            const int nb = D.cnt[I_NBONDS];
+            int es, hs;
+            if (D.gen_iface && nb > 0) {
+                const uint32_t b = uint_below(r.w[0], (uint32_t)nb);
+                hs = D.bonds[2 * b];
+                es = D.bonds[2 * b + 1];
+            } else {
+                es = hs = (int)uint_below(r.w[0], (uint32_t)D.V);
+            }
+            const bool valid = S.ne < D.cap_e && S.nh < D.cap_h && D.gen_rate > 0 &&
+                               D.et[es] == T_EMPTY && D.ht[hs] == T_EMPTY;
+            if (valid && D.gen_rate > unit_double(r.w[1], r.w[2])) {
+                D.ctr[C_XSRC + 1] += 1;
+                D.et[es] = T_ELECTRON;
+                D.ht[hs] = T_HOLE;
+                D.e_site[S.ne++] = es;
+                D.h_site[S.nh++] = hs;
+            }
         }
-        const bool valid = ne < D.cap_e && nh < D.cap_h && D.gen_rate > 0 &&
-                           D.et[es] == T_EMPTY && D.ht[hs] == T_EMPTY;
-        if (valid && D.gen_rate > unit_double(r.w[1], r.w[2])) {
-            D.ctr[C_XSRC + 1] += 1;
-            D.et[es] = T_ELECTRON;
-            D.ht[hs] = T_HOLE;
-            D.e_site[ne++] = es;
-            D.h_site[nh++] = hs;
+        __syncthreads();
+        if (D.balance) {
+            // Simulation::balanceCharges (simulation.cpp:253-353): electrons
+            // from the electrode on the low-potential side until they are no
+            // fewer than the holes, then holes alike; a uniform draw picks
+            // the side when the voltages are equal
+            for (int species = 0; species < 2; ++species) {
+                const bool e = species == 0;
+                const uint32_t purpose = e ? RNG_BALANCE_E : RNG_BALANCE_H;
+                for (int t = 0;; ++t) {
+                    const int more = e ? S.nh - S.ne : S.ne - S.nh;
+                    const bool at_max = e ? S.ne >= D.cap_e : S.nh >= D.cap_h;
+                    if (more <= 0 || at_max) break;
+                    if (t >= kBalanceTries) {  // the reference stops with a fatal error
+                        if (threadIdx.x == 0) atomicOr(D.err, DEVERR_STATE);
+                        break;
+                    }
+                    bool left;
+                    if (D.volt_r > D.volt_l) left = e;
+                    else if (D.volt_l > D.volt_r) left = !e;
+                    else {
+                        const Philox4 r = draw(D, step, (uint32_t)t, purpose + 1);
+                        const bool above = unit_double(r.w[0], r.w[1]) > 0.5;
+                        left = e ? above : !above;
+                    }
+                    block_try_inject(D, S, (e ? 0 : 2) + (left ? 0 : 1), step, (uint32_t)t,
+                                     purpose, red);
+                }
+            }
         }
-        D.cnt[I_NE] = ne;
-        D.cnt[I_NH] = nh;
+    } else {
+        // the electrode sources in the reference's order (simulation.cpp:246-249)
+        for (int s = 0; s < 4; ++s) block_try_inject(D, S, s, step, 0u, RNG_SOURCE + (uint32_t)s, red);
+    }
+    if (threadIdx.x == 0) {
+        D.cnt[I_NE] = S.ne;
+        D.cnt[I_NH] = S.nh;
         D.cnt[I_STEP] = (int32_t)(step + 1);
-        return;
     }
-    for (int s = 0; s < 4; ++s) {
-        const bool e = s < 2, left = (s % 2) == 0;
-        D.ctr[2 * s] += 1;  // attempts (sourceagent.cpp:94)
-        const Philox4 r = draw(D, step, 0u, RNG_SOURCE + (uint32_t)s);
-        const int idx = (int)uint_below(r.w[0], (uint32_t)(D.Y * D.Z));
-        const int site = D.X * idx + (left ? 0 : D.X - 1);
-        uint8_t* own = e ? D.et : D.ht;
-        const int count = e ? ne : nh;
-        const int cap = e ? D.cap_e : D.cap_h;
-        if (!(count < cap && D.rate_src[s] > 0 && own[site] == T_EMPTY)) continue;
-        const double u = unit_double(r.w[1], r.w[2]);
-        if (D.rate_src[s] > u) {
-            D.ctr[2 * s + 1] += 1;
-            own[site] = e ? T_ELECTRON : T_HOLE;
-            if (e) D.e_site[ne++] = site;
-            else D.h_site[nh++] = site;
-        }
-    }
-    D.cnt[I_NE] = ne;
-    D.cnt[I_NH] = nh;
-    D.cnt[I_STEP] = (int32_t)(step + 1);
 }
 
 // Single-replica kernels: the Dev travels by value.
@@ -838,7 +960,8 @@ __global__ void k_move(Dev D) { move_body(D, LGM_THREAD_INDEX); }
 __global__ void k_unclaim(Dev D) { unclaim_body(D, LGM_THREAD_INDEX); }
 __global__ void __launch_bounds__(kCompactThreads) k_compact_inject(Dev D) {
     __shared__ int warp_sums[32];
-    compact_inject_body(D, warp_sums);
+    __shared__ double red[32];
+    compact_inject_body(D, warp_sums, red);
 }
 
 // Batched kernels: block b works for replica map[b].x as its local block
@@ -887,7 +1010,8 @@ __global__ void kb_unclaim(const Dev* R, const int4* map) { LGM_BATCH_LOOP(uncla
 // one block per replica of the list
 __global__ void __launch_bounds__(kCompactThreads) kb_compact_inject(const Dev* R, const int* list) {
     __shared__ int warp_sums[32];
-    compact_inject_body(R[list[blockIdx.x]], warp_sums);
+    __shared__ double red[32];
+    compact_inject_body(R[list[blockIdx.x]], warp_sums, red);
 }
 
 // ---- the fused step: one block per replica, every phase inside the block ----------
@@ -1020,7 +1144,7 @@ __global__ void __launch_bounds__(NT) kb_fused(const Dev* R, const int* list, in
         __syncthreads();
         LGM_BLOCK_LOOP(ne + nh, unclaim_body(D, i))
         __syncthreads();
-        compact_inject_body(D, warp_sums);
+        compact_inject_body(D, warp_sums, reinterpret_cast<double*>(red));
         __syncthreads();
     }
 }
@@ -1452,8 +1576,6 @@ static lgm_status kmc_create_impl(const lgm_params* pin, int32_t device, uint32_
     g_kmc_create_error.clear();
     if (s != LGM_OK) return bail(s, msg);
     const lgm_params& p = k->p;
-    if (p.source_metropolis || p.balance_charges)
-        return bail(LGM_ERR_UNSUPPORTED, "source.metropolis and balance.charges are not supported");
     if (p.recombination_range < 0 || p.recombination_range > 2)
         return bail(LGM_ERR_INVALID_ARGUMENT, "langmuir: recombination.range must be 0, 1 or 2");
     const bool solar = std::string(p.simulation_type) == "solarcell";
@@ -1485,6 +1607,11 @@ static lgm_status kmc_create_impl(const lgm_params* pin, int32_t device, uint32_
     D.beta = p.inverse_kt; D.exciton_binding = p.exciton_binding;
     D.prefactor = p.electrostatic_prefactor;
     D.guard = p.guard_band;
+    D.src_metro = p.source_metropolis ? 1 : 0;
+    D.src_coulomb = p.source_coulomb ? 1 : 0;
+    D.balance = p.balance_charges ? 1 : 0;
+    D.volt_l = p.voltage_left;
+    D.volt_r = p.voltage_right;
     D.erffactor = p.coulomb_gaussian_sigma > 0 ? 1.0 / (std::sqrt(2.0) * p.coulomb_gaussian_sigma) : 0.0;
     D.gauss = p.coulomb_gaussian_sigma > 0;
     // sI[1][0][0] = prefactor * iR * eR at r = 1 (potential.cpp:311-323)
@@ -1768,7 +1895,11 @@ lgm_status lgm_kmc_run(lgm_kmc* k, int32_t steps) {
     KCUDA(k, cudaStreamSynchronize(k->stream));
     unsigned e = 0;
     KCUDA(k, cudaMemcpy(&e, k->D.err, sizeof e, cudaMemcpyDeviceToHost));
-    if (e) return kfail(k, LGM_ERR_TIMEOUT, "device reported an error during the step");
+    if (e & DEVERR_TIMEOUT) return kfail(k, LGM_ERR_TIMEOUT, "a bounded device wait ran out");
+    if (e & DEVERR_STATE)
+        return kfail(k, LGM_ERR_STATE,
+                     "langmuir: can not balance the charges (balance.charges, 1024 tries)");
+    if (e) return kfail(k, LGM_ERR_STATE, "device reported an error during the step");
     return LGM_OK;
 }
 

@@ -76,7 +76,10 @@ def oracle_for(O, p, world, e, h, max_e, max_h, replica=0, step=0, phase=None):
                       coulomb_carriers=q.coulomb_carriers, defects_charge=q.defects_charge,
                       image_terms=(2 if q.image_charges & 1 else 0) | (4 if q.image_charges & 2 else 0),
                       max_electrons=max_e, max_holes=max_h,
-                      seed=q.random_seed & 0xFFFFFFFF, replica=replica, **rates(q))
+                      seed=q.random_seed & 0xFFFFFFFF, replica=replica,
+                      source_metropolis=q.source_metropolis, source_coulomb=q.source_coulomb,
+                      balance_charges=q.balance_charges, voltage_left=q.voltage_left,
+                      voltage_right=q.voltage_right, **rates(q))
     bonds = None
     if phase is not None:
         cfg.confine = q.morphology_confine

@@ -153,6 +153,14 @@ typedef struct orc_kmc_config {
     int32_t confine;
     const int32_t* bonds;
     int32_t nbonds;
+    /* injection energetics (sourceagent.cpp:125-181): source.metropolis takes
+     * the Metropolis test on the injection energy instead of chooseYes;
+     * source.coulomb adds the Coulomb and left-image sums of every charge at
+     * the injection site; balance.charges (solar cell) injects from the
+     * electrodes until electrons and holes balance (simulation.cpp:253-353),
+     * the side set by voltage.left / voltage.right */
+    int32_t source_metropolis, source_coulomb, balance_charges;
+    double voltage_left, voltage_right;
 } orc_kmc_config;
 
 /* decideFuture outcomes per carrier */

@@ -242,6 +242,61 @@ extern "C" int orc_kmc_step(const orc_ctx* ctx, const orc_kmc_config* k, const d
     ne = tick(e_site, ef.data(), ne, et, ORC_ELECTRON, e_rm);
     nh = tick(h_site, hf.data(), nh, ht, ORC_HOLE, h_rm);
 
+    // SourceAgent::tryToInject for electrode source s (0 eL, 1 eR, 2 hL, 3 hR)
+    // on the draw at {step, index, purpose} (sourceagent.cpp:92-103): the site
+    // from the face (randomNeighborSiteID over the sorted face slice,
+    // cubicgrid.cpp:167-205, 473-487), validToInject (sourceagent.cpp:192-232),
+    // then shouldTransport (sourceagent.cpp:168-181): chooseYes on the rate,
+    // or with source.metropolis the Metropolis test on energyChange
+    // (sourceagent.cpp:125-161; the source's own potential is 0, never set).
+    const double src_rate[4] = {k->rate_e_source_l, k->rate_e_source_r, k->rate_h_source_l,
+                                k->rate_h_source_r};
+    std::vector<uint8_t> is_defect(V, 0);
+    for (int i = 0; i < nd; ++i) is_defect[defects[i]] = 1;
+    auto try_inject = [&](int s, uint32_t index, uint32_t purpose) {
+        const bool electron = s < 2;
+        const bool left = (s % 2) == 0;
+        counters[2 * s] += 1;  // attempts (sourceagent.cpp:94)
+        const Draw d = draw(k, step, index, purpose);
+        const uint32_t idx = uint_below(d.w[0], (uint32_t)(GY * GZ));
+        const int site = GX * (int)idx + (left ? 0 : GX - 1);
+        std::vector<uint8_t>& own = electron ? et : ht;
+        const int count = electron ? ne : nh;
+        const int cap = electron ? k->max_electrons : k->max_holes;
+        const bool valid =
+            count < cap && src_rate[s] > 0 && own[site] == ORC_EMPTY && !is_defect[site];
+        if (!valid) return;
+        const double u = unit_double(d.w[1], d.w[2]);
+        bool accept;
+        if (k->source_metropolis) {
+            double p2 = pot[site];
+            if (k->source_coulomb) {
+                // p2 += coulombH + coulombImageH + coulombE + coulombImageE
+                // (+ coulombD + coulombImageD), point charges, in that order
+                std::vector<int32_t> qh(nh, 1), qe(ne, -1), qd(nd, k->defects_charge);
+                p2 += orc_species_potential(ctx, site, h_site, qh.data(), nh, 0, 0);
+                p2 += orc_species_potential(ctx, site, h_site, qh.data(), nh, 0, 1);
+                p2 += orc_species_potential(ctx, site, e_site, qe.data(), ne, 0, 0);
+                p2 += orc_species_potential(ctx, site, e_site, qe.data(), ne, 0, 1);
+                if (k->defects_charge != 0) {
+                    p2 += orc_species_potential(ctx, site, defects, qd.data(), nd, 0, 0);
+                    p2 += orc_species_potential(ctx, site, defects, qd.data(), nd, 0, 1);
+                }
+            }
+            const double de = electron ? 0.0 - p2 : p2 - 0.0;
+            // Random::metropolisWithCoupling (rand.cpp:91-106), coupling = rate
+            accept = de > 0.0 ? src_rate[s] * std::exp(-de * k->inverse_kt) > u : src_rate[s] > u;
+        } else {
+            accept = src_rate[s] > u;  // chooseYes (rand.cpp:117-124)
+        }
+        if (accept) {
+            counters[2 * s + 1] += 1;
+            own[site] = electron ? ORC_ELECTRON : ORC_HOLE;
+            if (electron) e_site[ne++] = site;
+            else h_site[nh++] = site;
+        }
+    };
+
     if (k->solar) {
         // performInjections, solar (simulation.cpp:235-243): the exciton source,
         // ExcitonSourceAgent::tryToInject (sourceagent.cpp:92-103, 120-123, 234-250).
@@ -265,35 +320,38 @@ extern "C" int orc_kmc_step(const orc_ctx* ctx, const orc_kmc_config* k, const d
             e_site[ne++] = es;
             h_site[nh++] = hs;
         }
+        // Simulation::balanceCharges (simulation.cpp:253-353): electrons from
+        // the electrode on the low-potential side (a uniform draw picks it when
+        // the voltages are equal) until electrons >= holes, then holes alike;
+        // try t of a species draws at {step, t, 24 / 26} (25 / 27: the side)
+        if (k->balance_charges) {
+            for (int species = 0; species < 2; ++species) {
+                const bool electron = species == 0;
+                for (int t = 0;; ++t) {
+                    const int more = electron ? nh - ne : ne - nh;
+                    const bool at_max = electron ? ne >= k->max_electrons : nh >= k->max_holes;
+                    if (more <= 0 || at_max) break;
+                    if (t >= 1024) return -1;  // qFatal "can not balance ..."
+                    bool left;
+                    if (k->voltage_right > k->voltage_left) left = electron;
+                    else if (k->voltage_left > k->voltage_right) left = !electron;
+                    else {
+                        const Draw d = draw(k, step, (uint32_t)t, electron ? 25u : 27u);
+                        const bool above = unit_double(d.w[0], d.w[1]) > 0.5;
+                        left = electron ? above : !above;
+                    }
+                    try_inject((electron ? 0 : 2) + (left ? 0 : 1), (uint32_t)t,
+                               electron ? 24u : 26u);
+                }
+            }
+        }
         *ne_io = ne;
         *nh_io = nh;
         return 0;
     }
 
     // performInjections, transistor (simulation.cpp:246-249): eL, eR, hL, hR.
-    const double src_rate[4] = {k->rate_e_source_l, k->rate_e_source_r, k->rate_h_source_l,
-                                k->rate_h_source_r};
-    for (int s = 0; s < 4; ++s) {
-        const bool electron = s < 2;
-        const bool left = (s % 2) == 0;
-        counters[2 * s] += 1;  // attempts (sourceagent.cpp:94)
-        const Draw d = draw(k, step, 0u, 16u + (uint32_t)s);
-        // randomNeighborSiteID over the sorted face slice (cubicgrid.cpp:167-205, 473-487)
-        const uint32_t idx = uint_below(d.w[0], (uint32_t)(GY * GZ));
-        const int site = GX * (int)idx + (left ? 0 : GX - 1);
-        std::vector<uint8_t>& own = electron ? et : ht;
-        const int count = electron ? ne : nh;
-        const int cap = electron ? k->max_electrons : k->max_holes;
-        const bool valid = count < cap && src_rate[s] > 0 && own[site] == ORC_EMPTY;
-        if (!valid) continue;
-        const double u = unit_double(d.w[1], d.w[2]);
-        if (src_rate[s] > u) {
-            counters[2 * s + 1] += 1;
-            own[site] = electron ? ORC_ELECTRON : ORC_HOLE;
-            if (electron) e_site[ne++] = site;
-            else h_site[nh++] = site;
-        }
-    }
+    for (int s = 0; s < 4; ++s) try_inject(s, 0u, 16u + (uint32_t)s);
     *ne_io = ne;
     *nh_io = nh;
     return 0;

@@ -62,7 +62,10 @@ class KmcConfig(ctypes.Structure):
                 ("recombination_rate", ctypes.c_double), ("recombination_range", ctypes.c_int32),
                 ("hopping_range_neighbors", ctypes.c_int32),
                 ("phase", ctypes.c_void_p), ("confine", ctypes.c_int32),
-                ("bonds", ctypes.c_void_p), ("nbonds", ctypes.c_int32)]
+                ("bonds", ctypes.c_void_p), ("nbonds", ctypes.c_int32),
+                ("source_metropolis", ctypes.c_int32), ("source_coulomb", ctypes.c_int32),
+                ("balance_charges", ctypes.c_int32), ("voltage_left", ctypes.c_double),
+                ("voltage_right", ctypes.c_double)]
 
 
 def lib():

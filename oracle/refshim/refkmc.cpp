@@ -81,7 +81,8 @@ namespace {
 // the same numbers).
 enum : uint32_t {
     P_CHOOSE_E = 1, P_DECIDE_E = 2, P_CHOOSE_H = 3, P_DECIDE_H = 4, P_RECOMB = 5,
-    P_SOURCE = 16, P_EXCITON = 20, P_SETUP = 64
+    P_SOURCE = 16, P_EXCITON = 20, P_BALANCE_E = 24, P_BALANCE_SIDE_E = 25, P_BALANCE_H = 26,
+    P_BALANCE_SIDE_H = 27, P_SETUP = 64
 };
 
 void set_err(char* err, int len, const std::string& m) {
@@ -298,8 +299,44 @@ int ref_kmc_step(ref_kmc* k, int32_t* outcome, double* de, char* err, int errlen
         if (w.parameters().simulationType == "solarcell") {
             dr.set_keyed(step, 0u, P_EXCITON);
             w.excitonSourceAgent().tryToInject();
-            if (w.parameters().balanceCharges)
-                throw std::runtime_error("balance.charges: not restated in the harness");
+            // Simulation::balanceCharges (simulation.cpp:253-353), restated
+            // for its draws: try t of a species injects on {step, t, 24 / 26},
+            // the side draw of equal voltages is on {step, t, 25 / 27}
+            if (w.parameters().balanceCharges) {
+                const double VL = w.parameters().voltageLeft, VR = w.parameters().voltageRight;
+                int tries = 0;
+                while (w.electronsMinusHoles() < 0 && !w.atMaxElectrons()) {
+                    SourceAgent* src;
+                    if (VR > VL) src = &w.electronSourceAgentLeft();
+                    else if (VL > VR) src = &w.electronSourceAgentRight();
+                    else {
+                        dr.set_keyed(step, (uint32_t)tries, P_BALANCE_SIDE_E);
+                        src = w.randomNumberGenerator().random() > 0.5
+                                  ? static_cast<SourceAgent*>(&w.electronSourceAgentLeft())
+                                  : static_cast<SourceAgent*>(&w.electronSourceAgentRight());
+                    }
+                    dr.set_keyed(step, (uint32_t)tries, P_BALANCE_E);
+                    src->tryToInject();
+                    tries += 1;
+                    if (tries > 1024) qFatal("langmuir: can not balance electrons");
+                }
+                tries = 0;
+                while (w.holesMinusElectrons() < 0 && !w.atMaxHoles()) {
+                    SourceAgent* src;
+                    if (VR > VL) src = &w.holeSourceAgentRight();
+                    else if (VL > VR) src = &w.holeSourceAgentLeft();
+                    else {
+                        dr.set_keyed(step, (uint32_t)tries, P_BALANCE_SIDE_H);
+                        src = w.randomNumberGenerator().random() > 0.5
+                                  ? static_cast<SourceAgent*>(&w.holeSourceAgentRight())
+                                  : static_cast<SourceAgent*>(&w.holeSourceAgentLeft());
+                    }
+                    dr.set_keyed(step, (uint32_t)tries, P_BALANCE_H);
+                    src->tryToInject();
+                    tries += 1;
+                    if (tries > 1024) qFatal("langmuir: can not balance holes");
+                }
+            }
         } else {
             dr.set_keyed(step, 0u, P_SOURCE + 0);
             w.electronSourceAgentLeft().tryToInject();

@@ -130,6 +130,30 @@ CASES = {
                                     recombination_rate=0.05, recombination_range=1,
                                     morphology_confine=1, generation_interface=1, steps=150,
                                     morphology=5),
+    "source_metropolis_coulomb": dict(grid_x=32, grid_y=24, grid_z=4, electron_percentage=0.03,
+                                      hole_percentage=0.03, defect_percentage=0.02,
+                                      defects_charge=1, voltage_right=1.0, e_source_l_rate=0.6,
+                                      e_source_r_rate=0.3, h_source_l_rate=0.4,
+                                      h_source_r_rate=0.7, e_drain_r_rate=0.9,
+                                      h_drain_l_rate=0.9, source_metropolis=1, source_coulomb=1,
+                                      steps=80),
+    "source_metropolis": dict(grid_x=32, grid_y=24, grid_z=1, electron_percentage=0.03,
+                              hole_percentage=0.02, voltage_right=0.5, e_source_l_rate=0.6,
+                              h_source_r_rate=0.7, e_drain_r_rate=0.9, h_drain_l_rate=0.9,
+                              source_metropolis=1, steps=80),
+    "solar_balance_charges": dict(simulation_type="solarcell", grid_x=24, grid_y=24, grid_z=4,
+                                  electron_percentage=0.05, hole_percentage=0.05,
+                                  seed_charges=0.3, voltage_right=0.5, generation_rate=0.4,
+                                  source_scale_area=0, recombination_rate=0.3,
+                                  recombination_range=1, balance_charges=1,
+                                  e_source_l_rate=0.5, e_source_r_rate=0.5,
+                                  h_source_l_rate=0.5, h_source_r_rate=0.5, steps=100),
+    "solar_balance_equal_voltages_coulomb": dict(
+        simulation_type="solarcell", grid_x=24, grid_y=24, grid_z=4, electron_percentage=0.05,
+        hole_percentage=0.05, seed_charges=0.3, voltage_right=0.0, generation_rate=0.4,
+        source_scale_area=0, recombination_rate=0.3, recombination_range=1, balance_charges=1,
+        e_source_l_rate=0.5, e_source_r_rate=0.5, h_source_l_rate=0.5, h_source_r_rate=0.5,
+        source_metropolis=1, source_coulomb=1, steps=100),
     "2d_128_holes_1pct": dict(grid_x=128, grid_y=128, grid_z=1, hole_percentage=0.01,
                               electron_percentage=0.0, trap_percentage=0.05,
                               trap_potential=0.1, voltage_left=1.0, e_source_l_rate=0.0,
