@@ -111,6 +111,7 @@ SIGNATURES = {
     "lgm_set_timing": (ctypes.c_int32, [_vp, ctypes.c_int32]),
     "lgm_set_counting": (ctypes.c_int32, [_vp, ctypes.c_int32]),
     "lgm_probe_peaks": (ctypes.c_int32, [ctypes.c_int32, _vp]),
+    "lgm_selftest_timeout": (ctypes.c_int32, [ctypes.c_int32, ctypes.c_int32]),
     "lgm_autotune": (ctypes.c_int32, [_vp, ctypes.c_int32, ctypes.c_uint32, ctypes.c_int32,
                                       ctypes.c_int32, ctypes.POINTER(ctypes.c_int32)]),
     "lgm_set_variant": (ctypes.c_int32, [_vp, ctypes.c_int32]),

@@ -419,12 +419,7 @@ __device__ __forceinline__ void pair_items_culled(const PairArgs& A, const CullA
     if (failed && tid == 0) {
         // A stage never completed: wait (bounded) for the copies still in
         // flight, then leave without results; the host sees DEVERR_TIMEOUT.
-        const uint32_t issued = (uint32_t)s_prod[5];
-        for (uint32_t g = consumed; g < issued; ++g) {
-            const uint32_t parity = (g >> 1) & 1u;
-            for (int i = 0; i < kWaitLimit; ++i)
-                if (mbar_try_wait(&s_bar[g & 1u], parity)) break;
-        }
+        mbar_drain_stages(s_bar, consumed, (uint32_t)s_prod[5]);
     }
 }
 

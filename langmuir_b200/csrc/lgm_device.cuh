@@ -73,12 +73,26 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
 }
 
 // Bounded wait for phase `parity` of `bar`.  Returns false (and raises
-// DEVERR_TIMEOUT) when the limit runs out.
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, unsigned* err) {
-    for (int it = 0; it < kWaitLimit; ++it)
+// DEVERR_TIMEOUT) when `limit` tries run out.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, unsigned* err,
+                                                  int limit = kWaitLimit) {
+    for (int it = 0; it < limit; ++it)
         if (mbar_try_wait(bar, parity)) return true;
     atomicOr(err, DEVERR_TIMEOUT);
     return false;
+}
+
+// After a wait ran out: wait (bounded, no error raised) for the phases of
+// the bulk copies a CTA still has in flight -- sequence numbers first .. last-1
+// of a two-stage pipeline, stage g & 1, phase (g >> 1) & 1 -- so that no copy
+// lands in shared memory after the CTA has left.  One thread calls it.
+__device__ __forceinline__ void mbar_drain_stages(uint64_t* bars, uint32_t first, uint32_t last,
+                                                  int limit = kWaitLimit) {
+    for (uint32_t g = first; g < last; ++g) {
+        const uint32_t parity = (g >> 1) & 1u;
+        for (int it = 0; it < limit; ++it)
+            if (mbar_try_wait(&bars[g & 1u], parity)) break;
+    }
 }
 
 // MUFU reciprocal square root (PTX rsqrt.approx.ftz.f32).  rsqrt(+0) = +inf,

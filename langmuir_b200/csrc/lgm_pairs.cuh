@@ -262,13 +262,8 @@ __device__ __forceinline__ void pair_tile(PairArgs A, const int tile, const int 
         // A stage never completed: wait (bounded) for the copies this CTA
         // still has in flight -- chunks failed_at and failed_at + 1 -- then
         // leave without writing results; the host sees DEVERR_TIMEOUT.
-        if (tid == 0) {
-            for (int i = failed_at; i < failed_at + 2 && i < nck; ++i) {
-                const uint32_t parity = (uint32_t)((i >> 1) & 1);
-                for (int it = 0; it < kWaitLimit; ++it)
-                    if (mbar_try_wait(&s_bar[i & 1], parity)) break;
-            }
-        }
+        if (tid == 0)
+            mbar_drain_stages(s_bar, (uint32_t)failed_at, (uint32_t)min(failed_at + 2, nck));
         return;
     }
 

@@ -129,3 +129,52 @@ extern "C" lgm_status lgm_probe_peaks(int32_t device, lgm_peaks* out) {
     cudaFree(sink);
     return st;
 }
+
+namespace {
+
+// The failure path of the pair kernels, made to run: both stages of a
+// two-stage bulk-copy pipeline are armed for a chunk's bytes, but no copy is
+// issued, so the bounded wait runs out (limit tries), raises DEVERR_TIMEOUT
+// and the CTA drains its (absent) copies before leaving -- the same device
+// functions the pair kernels call.  Nothing waits without a bound.
+__global__ void __launch_bounds__(128) selftest_wait_timeout(unsigned* err, int limit) {
+    __shared__ __align__(8) uint64_t bars[2];
+    if (threadIdx.x == 0) {
+        lgm::mbar_init(&bars[0], 1);
+        lgm::mbar_init(&bars[1], 1);
+        lgm::fence_mbar_init();
+        lgm::mbar_arrive_expect_tx(&bars[0], 5120u);
+        lgm::mbar_arrive_expect_tx(&bars[1], 5120u);
+    }
+    __syncthreads();
+    const bool mine = lgm::mbar_wait_bounded(&bars[0], 0u, err, limit);
+    if (!__syncthreads_and(mine) && threadIdx.x == 0) lgm::mbar_drain_stages(bars, 0u, 2u, limit);
+}
+
+}  // namespace
+
+extern "C" lgm_status lgm_selftest_timeout(int32_t device, int32_t wait_limit) {
+    if (wait_limit < 1 || wait_limit > (1 << 20)) return LGM_ERR_INVALID_ARGUMENT;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev)
+        return LGM_ERR_NO_DEVICE;
+    if (cudaSetDevice(device) != cudaSuccess) return LGM_ERR_CUDA;
+    unsigned* d_err = nullptr;
+    if (cudaMalloc(&d_err, sizeof(unsigned)) != cudaSuccess) return LGM_ERR_CUDA;
+    lgm_status st = LGM_OK;
+    unsigned h_err = 0;
+    if (cudaMemset(d_err, 0, sizeof(unsigned)) != cudaSuccess) {
+        st = LGM_ERR_CUDA;
+    } else {
+        selftest_wait_timeout<<<2, 128>>>(d_err, wait_limit);
+        if (cudaGetLastError() != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess ||
+            cudaMemcpy(&h_err, d_err, sizeof h_err, cudaMemcpyDeviceToHost) != cudaSuccess)
+            st = LGM_ERR_CUDA;
+        else if (h_err & lgm::DEVERR_TIMEOUT)
+            st = LGM_ERR_TIMEOUT;
+        else if (h_err)
+            st = LGM_ERR_STATE;
+    }
+    cudaFree(d_err);
+    return st;
+}

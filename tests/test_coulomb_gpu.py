@@ -475,3 +475,19 @@ def test_probe_peaks_measure_plausible_rates():
     for key in ("ffma_tflops", "ffma2_tflops"):
         assert derived / 3 < p[key] <= derived * 1.02, (key, p[key], derived)
     assert 0 < p["rsqrt_per_s"] <= 16.5 * p["sm_count"] * p["clock_mhz_attribute"] * 1e6
+
+
+def test_bounded_wait_runs_out_and_the_context_stays_usable(lgm, oracle_mod):
+    """Failure detection without a fault: a pipeline stage that no copy fills
+    makes the pair kernels' bounded wait run out (a small limit), the device
+    error word reports LGM_ERR_TIMEOUT, and a kernel-2 call afterwards on the
+    same device is still correct."""
+    from langmuir_b200 import _native as N
+    assert N.lib().lgm_selftest_timeout(0, 1 << 10) == N.ERR_TIMEOUT
+    assert N.lib().lgm_selftest_timeout(0, 0) == N.ERR_INVALID_ARGUMENT
+    X, Y, Z, c = 40, 30, 6, 20
+    rng = np.random.default_rng(4)
+    orc = oracle_mod.Oracle(X, Y, Z, cutoff=c)
+    s, q, n = packed_case(orc, rng, 300, 280, 0, 0)
+    with lgm.Coulomb(X, Y, Z, cutoff=c) as ctx:
+        assert_close(ctx.kernel2(s, q, n), orc.kernel2(s, q, n), norm_of(orc, s, q, n), TOL32)
