@@ -50,8 +50,14 @@ typedef enum lgm_kind { LGM_POINT = 0, LGM_GAUSS = 1 } lgm_kind;
 typedef enum lgm_precision { LGM_PREC_FP32C = 0, LGM_PREC_FP64 = 1 } lgm_precision;
 
 /* How 1/r is formed in FP32C: MUFU reciprocal square root, or a per-r^2
- * shared-memory table of correctly rounded values (r^2 is an integer). */
-typedef enum lgm_path { LGM_PATH_RSQRT = 0, LGM_PATH_TABLE = 1 } lgm_path;
+ * shared-memory table of correctly rounded values (r^2 is an integer).
+ * TABLE64: r^2 exact in FP32 as in the other paths, each term w(r^2) read
+ * from a per-r^2 table of FP64 values (1/sqrt(k), or erf(f sqrt(k))/sqrt(k)
+ * for Gaussian charges, both correctly rounded) and accumulated in FP64: the
+ * sums are as accurate as the FP64 path's.  Served by the culled tile
+ * variants (LGM_VARIANT_CULLED); needs 8 (cutoff^2 + 1) bytes of shared
+ * memory per CTA. */
+typedef enum lgm_path { LGM_PATH_RSQRT = 0, LGM_PATH_TABLE = 1, LGM_PATH_TABLE64 = 2 } lgm_path;
 
 /* Terms of lgm_potentials: direct sum, and the images of the sources in the
  * x = -1/2 electrode (Potential::coulombImage*, potential.cpp:384-753) and,

@@ -28,7 +28,7 @@ ERR_STATE = 9
 
 POINT, GAUSS = 0, 1
 PREC_FP32C, PREC_FP64 = 0, 1
-PATH_RSQRT, PATH_TABLE = 0, 1
+PATH_RSQRT, PATH_TABLE, PATH_TABLE64 = 0, 1, 2
 TERM_DIRECT, TERM_IMAGE_LEFT, TERM_IMAGE_RIGHT = 1, 2, 4
 
 

@@ -319,25 +319,26 @@ using CulledFn = void (*)(PairArgs, CullArgs);
 // chunks per work item (cfn[] instead of fn[]).
 struct Variant {
     int nt, rp, sub, skip, cull, per_item;
-    PairFn fn[3];
-    CulledFn cfn[3];
+    PairFn fn[4];
+    CulledFn cfn[4];  // [3]: the FP64-table path (culled variants only)
 };
 #define LGM_VARIANT_S(NT, RP, SUB, SK)                                                    \
     Variant {                                                                             \
         NT, RP, SUB, SK, 0, 0,                                                            \
             {&pair_kernel<0, 0, NT, RP, SUB, false, SK>,                                  \
-             &pair_kernel<1, 0, NT, RP, SUB, false, SK>, &pair_kernel<0, 1, NT, RP, SUB>}, \
+             &pair_kernel<1, 0, NT, RP, SUB, false, SK>, &pair_kernel<0, 1, NT, RP, SUB>,  \
+             nullptr},                                                                    \
         {                                                                                 \
-            nullptr, nullptr, nullptr                                                     \
+            nullptr, nullptr, nullptr, nullptr                                            \
         }                                                                                 \
     }
 #define LGM_VARIANT(NT, RP, SUB) LGM_VARIANT_S(NT, RP, SUB, false)
 #define LGM_VARIANT_SKIP(NT, RP, SUB) LGM_VARIANT_S(NT, RP, SUB, true)
 #define LGM_VARIANT_CULL(NT, RP, SUB, K)                                                      \
     Variant {                                                                                 \
-        NT, RP, SUB, 1, 1, K, {nullptr, nullptr, nullptr}, {                                  \
+        NT, RP, SUB, 1, 1, K, {nullptr, nullptr, nullptr, nullptr}, {                         \
             &pair_kernel_culled<0, 0, NT, RP, SUB>, &pair_kernel_culled<1, 0, NT, RP, SUB>,   \
-                &pair_kernel_culled<0, 1, NT, RP, SUB>                                        \
+                &pair_kernel_culled<0, 1, NT, RP, SUB>, &pair_kernel_culled<0, 2, NT, RP, SUB> \
         }                                                                                     \
     }
 const Variant kVariants[] = {
@@ -362,6 +363,7 @@ const void* kernel_of(const Variant& V, int fi) {
 }
 
 int fn_index(int kind, int path) {
+    if (path == LGM_PATH_TABLE64) return 3;  // one kernel: the table holds w for the kind
     if (path == LGM_PATH_TABLE) return 2;
     return kind == LGM_GAUSS ? 1 : 0;
 }
@@ -492,7 +494,8 @@ lgm_status launch_culled(lgm_ctx* c, int kind, int v, const Shape& sh, const Pai
     // timing on: the events bracket the pair kernel alone (recorded again here)
     if (c->timing) LGM_CUDA(c, cudaEventRecord(c->ev_pair0, st));
     const int grid = c->sm_count * std::max(1, c->bps[v][fi]);
-    V.cfn[fi]<<<grid, V.nt, pair_smem_bytes(P.tab_k), st>>>(P, C);
+    const size_t smem = fi == 3 ? pair_smem_bytes64(P.tab_k) : pair_smem_bytes(P.tab_k);
+    V.cfn[fi]<<<grid, V.nt, smem, st>>>(P, C);
     LGM_CUDA(c, cudaGetLastError());
     c->last.ctas = grid;
     c->last.threads = V.nt;
@@ -513,7 +516,10 @@ lgm_status launch_pair(lgm_ctx* c, int kind, int v, const Shape& sh, cudaStream_
         A.tgt = c->d_tgt; A.t_phys = sh.t_phys;
         A.c2 = (float)(cf.electrostatic_cutoff * cf.electrostatic_cutoff);
         A.err = c->d_err;
-        if (cf.path == LGM_PATH_TABLE) {
+        if (cf.path == LGM_PATH_TABLE64) {
+            A.tab64 = kind == LGM_GAUSS ? c->d_gtab64 : c->d_rtab64;
+            A.tab_k = c->rtab_k;  // both hold every r^2 <= c^2 (entries 0 and c^2 are 0)
+        } else if (cf.path == LGM_PATH_TABLE) {
             A.tab = kind == LGM_GAUSS ? c->d_gtab : c->d_rtab;
             A.tab_k = kind == LGM_GAUSS ? c->gtab_k : c->rtab_k;
         } else {
@@ -552,9 +558,16 @@ lgm_status launch_pair(lgm_ctx* c, int kind, int v, const Shape& sh, cudaStream_
 }
 
 int choose_variant(const lgm_ctx* c, int kind, const Shape& sh) {
-    if (c->forced_variant >= 0) return c->forced_variant;
-    auto it = c->tune_cache.find(tune_key(kind, c->cfg.path, sh.t_phys, sh.n_chunks));
-    return it == c->tune_cache.end() ? kDefaultVariant : it->second;
+    int v = kDefaultVariant;
+    if (c->forced_variant >= 0) {
+        v = c->forced_variant;
+    } else {
+        auto it = c->tune_cache.find(tune_key(kind, c->cfg.path, sh.t_phys, sh.n_chunks));
+        if (it != c->tune_cache.end()) v = it->second;
+    }
+    // the FP64-table path is served by the culled variants only
+    if (c->cfg.path == LGM_PATH_TABLE64 && !kVariants[v].cull) v = kDefaultVariant;
+    return v;
 }
 
 // Shared launch sequence.  d_src/d_q: n sources; d_tgt_site: t targets (or
@@ -767,7 +780,7 @@ lgm_status lgm_create(const lgm_config* cfg, int32_t device, lgm_ctx** out) {
         g_create_error = "unknown precision";
         return LGM_ERR_INVALID_ARGUMENT;
     }
-    if (cf.path != LGM_PATH_RSQRT && cf.path != LGM_PATH_TABLE) {
+    if (cf.path != LGM_PATH_RSQRT && cf.path != LGM_PATH_TABLE && cf.path != LGM_PATH_TABLE64) {
         g_create_error = "unknown path";
         return LGM_ERR_INVALID_ARGUMENT;
     }
@@ -867,6 +880,26 @@ lgm_status lgm_create(const lgm_config* cfg, int32_t device, lgm_ctx** out) {
                             cudaMemcpyHostToDevice)) != cudaSuccess)
             return bail("cudaMemcpy", e);
     }
+    // FP64 tables of the TABLE64 path: w(k) for every integer r^2 = k <= c^2,
+    // correctly rounded in IEEE double, 0 at k = 0 and k = c^2.
+    if (cf.path == LGM_PATH_TABLE64) {
+        std::vector<double> rt(c2 + 1, 0.0), gt(c2 + 1, 0.0);
+        const double sig = cf.coulomb_gaussian_sigma;
+        const double f = sig > 0 ? 1.0 / (std::sqrt(2.0) * sig) : 0.0;
+        for (int k = 1; k < c2; ++k) {
+            const double r = std::sqrt((double)k);
+            rt[k] = 1.0 / r;
+            gt[k] = sig > 0 ? std::erf(f * r) / r : rt[k];
+        }
+        if ((e = cudaMalloc(&c->d_rtab64, rt.size() * sizeof(double))) != cudaSuccess ||
+            (e = cudaMalloc(&c->d_gtab64, gt.size() * sizeof(double))) != cudaSuccess)
+            return bail("cudaMalloc", e);
+        if ((e = cudaMemcpy(c->d_rtab64, rt.data(), rt.size() * sizeof(double),
+                            cudaMemcpyHostToDevice)) != cudaSuccess ||
+            (e = cudaMemcpy(c->d_gtab64, gt.data(), gt.size() * sizeof(double),
+                            cudaMemcpyHostToDevice)) != cudaSuccess)
+            return bail("cudaMemcpy", e);
+    }
     // Lattice cells for the spatial target order (Morton rank per cell).
     {
         const std::vector<int32_t> rank =
@@ -887,10 +920,15 @@ lgm_status lgm_create(const lgm_config* cfg, int32_t device, lgm_ctx** out) {
     // resident CTAs per SM of every variant (the split count fills
     // kSplitWaves waves of them).
     {
-        const size_t smem_tab[3] = {pair_smem_bytes(0), pair_smem_bytes(c->gtab_k),
-                                    pair_smem_bytes(std::max(c->rtab_k, c->gtab_k))};
+        const size_t smem_tab[4] = {pair_smem_bytes(0), pair_smem_bytes(c->gtab_k),
+                                    pair_smem_bytes(std::max(c->rtab_k, c->gtab_k)),
+                                    pair_smem_bytes64(c->rtab_k)};
         for (int v = 0; v < kNumVariants; ++v)
-            for (int fi = 0; fi < 3; ++fi) {
+            for (int fi = 0; fi < 4; ++fi) {
+                if (!kernel_of(kVariants[v], fi)) continue;
+                // the table kernels serve only their own path
+                if (fi == 2 && cf.path != LGM_PATH_TABLE) continue;
+                if (fi == 3 && cf.path != LGM_PATH_TABLE64) continue;
                 const size_t smem = smem_tab[fi];
                 if (smem > 48 * 1024) {
                     if (smem > (size_t)prop.sharedMemPerBlockOptin) {
@@ -923,7 +961,7 @@ lgm_status lgm_destroy(lgm_ctx* c) {
                         c->d_err,  c->d_cell_rank, c->d_bins,      c->d_key,       c->d_perm,
                         c->d_skey, c->d_stmp,      c->d_cbox,      c->d_gbox,      c->d_live,
                         c->d_items, c->d_tile_first, c->d_tile_items, c->d_item_count,
-                        c->d_examined};
+                        c->d_examined, c->d_rtab64, c->d_gtab64};
     for (void* p : dev_ptrs)
         if (p) cudaFree(p);
     void* host_ptrs[] = {c->h_s, c->h_q, c->h_t, c->h_o, c->h_err};
@@ -1033,6 +1071,7 @@ lgm_status lgm_autotune(lgm_ctx* c, lgm_kind kind, uint32_t terms, int32_t n, in
     int best = kDefaultVariant;
     float best_ms = 1e30f;
     for (int v = 0; v < kNumVariants; ++v) {
+        if (c->cfg.path == LGM_PATH_TABLE64 && !kVariants[v].cull) continue;
         int splits;
         if ((s = launch_pair(c, kind, v, sh, st, &splits)) != LGM_OK) break;  // warm
         float ms[3];

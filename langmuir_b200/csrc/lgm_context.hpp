@@ -28,6 +28,8 @@ struct lgm_ctx {
     double* d_o = nullptr;    size_t o_cap = 0;
     float* d_gtab = nullptr;  int gtab_k = 0;       // gauss correction table
     float* d_rtab = nullptr;  int rtab_k = 0;       // 1/sqrt(k) table
+    double* d_rtab64 = nullptr;                      // FP64 1/sqrt(k) (TABLE64 path)
+    double* d_gtab64 = nullptr;                      // FP64 erf(f sqrt(k))/sqrt(k) (TABLE64)
     unsigned* d_err = nullptr;                       // device error word
 
     // Spatial order of the targets: a target's bin is the Morton rank of its
@@ -63,7 +65,7 @@ struct lgm_ctx {
     double* h_o = nullptr;    size_t ho_cap = 0;
     unsigned* h_err = nullptr;
 
-    int bps[40][3] = {};                 // resident CTAs per SM, per variant and kernel
+    int bps[40][4] = {};                 // resident CTAs per SM, per variant and kernel
     int forced_variant = -1;             // -1: autotuned / default
     std::map<uint64_t, int> tune_cache;  // size bucket -> fastest variant
 

@@ -207,14 +207,17 @@ __device__ __forceinline__ void cull_body(const CullArgs& C, const int tile) {
 
 // The pair sum over the work items (see the file comment).  KIND 0 point, 1
 // gauss; PATH 0 MUFU rsqrt with the per-source warp vote, 1 the shared-memory
-// table of w(k); NT threads, RP target pairs per thread (a warp owns 64 RP
-// consecutive targets), SUB sources per FP32 run (SUB divides kGroup).
-// Partials go to A.part[item * tile_size + local target] (and A.part_norm).
-// Launched with a persistent grid and dynamic shared memory
-// pair_smem_bytes(tab_k).
+// table of w(k), 2 the shared-memory FP64 table of w(k) (1/sqrt(k) or the
+// Gaussian term, whatever KIND) with the warp vote, every term added in FP64;
+// NT threads, RP target pairs per thread (a warp owns 64 RP consecutive
+// targets), SUB sources per FP32 run (SUB divides kGroup).  Partials go to
+// A.part[item * tile_size + local target] (and A.part_norm).  Launched with a
+// persistent grid and dynamic shared memory pair_smem_bytes(tab_k)
+// (pair_smem_bytes64 for PATH 2).
 template <int KIND, int PATH, int NT, int RP, int SUB, bool NORM>
 __device__ __forceinline__ void pair_items_culled(const PairArgs& A, const CullArgs& C) {
     static_assert(kGroup % SUB == 0, "an FP32 run lies inside one group");
+    static_assert(PATH != 2 || !NORM, "the FP64-table path carries no FP32 run norms");
     constexpr int TS = NT * 2 * RP;
     const int nit = *C.item_count;
     if ((int)blockIdx.x >= nit) return;
@@ -223,6 +226,7 @@ __device__ __forceinline__ void pair_items_culled(const PairArgs& A, const CullA
     float2* s_qq = reinterpret_cast<float2*>(smem + 2 * CH * 2 * sizeof(float4));  // [2][CH]
     uint64_t* s_bar = reinterpret_cast<uint64_t*>(smem + 2 * pair_stage_bytes());
     float* s_tab = reinterpret_cast<float*>(smem + 2 * pair_stage_bytes() + 16);
+    double* s_tab64 = reinterpret_cast<double*>(smem + 2 * pair_stage_bytes() + 16);
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int t_phys = A.dyn ? A.dyn[1] : A.t_phys;
@@ -231,8 +235,11 @@ __device__ __forceinline__ void pair_items_culled(const PairArgs& A, const CullA
         mbar_init(&s_bar[1], 1);
         fence_mbar_init();
     }
-    if (KIND == 1 || PATH == 1)
+    if (PATH == 2) {
+        for (int k = tid; k <= A.tab_k; k += NT) s_tab64[k] = A.tab64[k];
+    } else if (KIND == 1 || PATH == 1) {
         for (int k = tid; k <= A.tab_k; k += NT) s_tab[k] = A.tab[k];
+    }
     __syncthreads();
 
     // Producer (thread 0): walks this CTA's chunk sequence -- the live chunks
@@ -326,7 +333,7 @@ __device__ __forceinline__ void pair_items_culled(const PairArgs& A, const CullA
                 float acc[2 * RP];
 #pragma unroll
                 for (int k = 0; k < 2 * RP; ++k) acc[k] = 0.f;
-                constexpr int kUnrollJ = PATH == 0 ? 4 : SUB;
+                constexpr int kUnrollJ = PATH != 1 ? 4 : SUB;
 #pragma unroll kUnrollJ
                 for (int jj = 0; jj < SUB; ++jj) {
                     const int j = j0 + jj;
@@ -334,7 +341,37 @@ __device__ __forceinline__ void pair_items_culled(const PairArgs& A, const CullA
                     const float4 g1 = sg[2 * j + 1];
                     const float2 av = f2(g0.x, g0.y), bv = f2(g0.z, g0.w);
                     const float2 cv = f2(g1.x, g1.y), dv = f2(g1.z, g1.w);
-                    if constexpr (PATH == 0) {
+                    if constexpr (PATH == 2) {
+                        // r^2 - 1/2 exactly, the warp vote, then w(r^2) from the
+                        // FP64 table: u + 2^23 + 1/2 holds r^2 in its low mantissa
+                        // bits; entries 0 and past the cutoff are 0, so the
+                        // clamped index also applies the cutoff and the r = 0 skip
+                        float2 uu[RP];
+                        unsigned mk[RP];
+#pragma unroll
+                        for (int k = 0; k < RP; ++k) {
+                            const float2 pa = __ffma2_rn(tx[k], av, tt[k]);
+                            const float2 pc = __ffma2_rn(tz[k], cv, dv);
+                            uu[k] = __fadd2_rn(__ffma2_rn(ty[k], bv, pa), pc);
+                            mk[k] = min(__float_as_uint(uu[k].x), __float_as_uint(uu[k].y));
+                        }
+#pragma unroll
+                        for (int w = 1; w < RP; w *= 2)
+#pragma unroll
+                            for (int k = 0; k + w < RP; k += 2 * w) mk[k] = min(mk[k], mk[k + w]);
+                        if (__any_sync(0xffffffffu, mk[0] < ulim)) {
+                            const double qd = (double)sq[j].x;
+                            const float2 magic = f2(8388608.5f, 8388608.5f);
+#pragma unroll
+                            for (int k = 0; k < RP; ++k) {
+                                const float2 m2 = __fadd2_rn(uu[k], magic);
+                                const int ix = min(__float_as_int(m2.x) & 0x7fffff, A.tab_k);
+                                const int iy = min(__float_as_int(m2.y) & 0x7fffff, A.tab_k);
+                                acc64[2 * k] = fma(qd, s_tab64[ix], acc64[2 * k]);
+                                acc64[2 * k + 1] = fma(qd, s_tab64[iy], acc64[2 * k + 1]);
+                            }
+                        }
+                    } else if constexpr (PATH == 0) {
                         // r^2 - 1/2 in three exact steps and the warp vote, as
                         // the SKIP tile of lgm_pairs.cuh
                         float2 uu[RP];
@@ -390,8 +427,10 @@ __device__ __forceinline__ void pair_items_culled(const PairArgs& A, const CullA
                         }
                     }
                 }
+                if constexpr (PATH != 2) {  // PATH 2 adds every term in FP64 already
 #pragma unroll
-                for (int k = 0; k < 2 * RP; ++k) acc64[k] += (double)acc[k];
+                    for (int k = 0; k < 2 * RP; ++k) acc64[k] += (double)acc[k];
+                }
                 if (NORM) {
 #pragma unroll
                     for (int k = 0; k < 2 * RP; ++k) nrm[NORM ? k : 0] += fabsf(acc[k]);

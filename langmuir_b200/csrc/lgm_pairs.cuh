@@ -53,6 +53,7 @@ struct PairArgs {
     double* part = nullptr;           // [splits][t_phys]
     float c2 = 0.f;                   // cutoff^2
     const float* tab = nullptr;       // gauss correction table or 1/sqrt(k) table
+    const double* tab64 = nullptr;    // FP64 w(k) for every integer r^2 = k (TABLE64 path)
     int tab_k = 0;                    // last valid table index (clamp)
     unsigned* err = nullptr;
     // Optional: counts read on the device (dyn[0] = n_chunks, dyn[1] = t_phys)
@@ -71,6 +72,10 @@ __host__ __device__ constexpr size_t pair_stage_bytes() {
 }
 inline size_t pair_smem_bytes(int tab_k) {
     return 2 * pair_stage_bytes() + 16 + (size_t)(tab_k + 1) * sizeof(float) + 16;
+}
+// The same with the FP64 table of the TABLE64 path (PATH 2).
+inline size_t pair_smem_bytes64(int tab_k) {
+    return 2 * pair_stage_bytes() + 16 + (size_t)(tab_k + 1) * sizeof(double) + 16;
 }
 
 // KIND 0 point, 1 gauss.  PATH 0 MUFU rsqrt, 1 shared-memory table of w(k)
