@@ -533,10 +533,65 @@ def batch_run(L, args, rank):
             "build_s": build_s}
 
 
+def _kernel_leg(L, ctx, args, w, s_all, q_all, n, kind, terms, dev, st, fp32_peak,
+                all_sites=False):
+    """One timed pair-sum workload on a context: the autotuned tile variant,
+    the pair kernel's own CUDA events (median over args.steps after
+    args.warmup), one untimed call counting the pairs the culled kernel
+    examines, the FP64 oracle's accuracy on 512 targets, and the roofline on
+    the work done (8 FLOP per pair examined + 3 per pair inside the cutoff)."""
+    import torch
+    T = w["X"] * w["Y"] * w["Z"] if all_sites else len(s_all)
+    d_s = torch.from_numpy(s_all[: (n if all_sites else T)].copy()).to(dev)
+    d_q = torch.from_numpy(q_all[: (n if all_sites else T)].copy()).to(dev)
+    d_o = torch.empty(T, dtype=torch.float64, device=dev)
+
+    def call():
+        if all_sites:
+            ctx.kernel1_async(d_s.data_ptr(), d_q.data_ptr(), n, d_o.data_ptr(), kind,
+                              st.cuda_stream)
+        else:
+            ctx.potentials_async(d_s.data_ptr(), d_q.data_ptr(), n, d_s.data_ptr(), T,
+                                 d_o.data_ptr(), kind, terms, st.cuda_stream)
+        ctx.sync(st.cuda_stream)
+    v = ctx.autotune(n, T, kind, terms)
+    ctx.set_variant(v)
+    ctx.set_timing(True)
+    ms = []
+    for i in range(args.warmup + args.steps):
+        call()
+        if i >= args.warmup:
+            ms.append(ctx.last_launch()["pair_kernel_ms"])
+    ctx.set_timing(False)
+    ctx.set_counting(True)
+    call()
+    examined = ctx.last_launch()["pairs_examined"]
+    ctx.set_counting(False)
+    pk = float(np.median(ms))
+    nterms = bin(terms).count("1")
+    pairs = nterms * n * T
+    tgt = np.arange(T, dtype=np.int32) if all_sites else s_all
+    idx = np.linspace(0, T - 1, 512).astype(int)
+    acc = accuracy_vs_oracle(w, s_all[:n], q_all[:n], tgt[idx], d_o.cpu().numpy()[idx], terms)
+    p_in = pairs_in_cutoff(w, tgt, s_all[:n], terms, dev)
+    done = examined if examined >= 0 else pairs
+    achieved = (FLOP_PER_TEST * done + FLOP_PER_CONTRIB * p_in) / (pk * 1e-3) / 1e12
+    return {"pairs_reference": pairs, "pairs_examined": done, "pairs_inside_cutoff": p_in,
+            "pair_kernel_ms": pk, "pair_evals_per_s": pairs / (pk * 1e-3),
+            "roofline": {"bound": "fp32", "achieved": achieved, "peak": fp32_peak,
+                         "unit": "TFLOP/s", "frac": achieved / fp32_peak,
+                         "basis": f"{FLOP_PER_TEST} FLOP per pair examined + "
+                                  f"{FLOP_PER_CONTRIB} per pair inside the cutoff"},
+            "tile_variant": dict(ctx.variants()[v], id=v), "accuracy": acc}
+
+
 def other_kernels_run(L, args, fp32_peak):
-    """Rows a2 and a3: the Gaussian kernel-2 sum on config 3 (128x128x64,
-    sigma 1, cutoff 30) and the whole-grid kernel 1 (every site of config 1's
-    128x128 lattice) -- pair kernel time from the library's own CUDA events."""
+    """Rows a2 and a3 and the other accumulation paths: the Gaussian kernel-2
+    sum on config 3 (128x128x64, sigma 1, cutoff 30), the cfg2 kernel-2 sum
+    through the FP32 1/sqrt(k) table and through the FP64 table (TABLE64,
+    FP64-accurate sums), and the whole-grid kernel 1 on config 1's lattice and
+    on the 1,048,576 sites of the 256x256x16 lattice -- pair kernel time from
+    the library's own CUDA events."""
     import torch
     dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
     st = torch.cuda.Stream(dev)
@@ -544,112 +599,46 @@ def other_kernels_run(L, args, fp32_peak):
     # gauss2, config 3
     w = WORKLOADS["cfg3_gauss"]
     s_all, q_all, n = make_inputs(w, 5)
-    T = len(s_all)
     with L.Coulomb(w["X"], w["Y"], w["Z"], cutoff=w["cutoff"], sigma=w["sigma"],
                    device=dev.index) as ctx:
-        d_s, d_q = torch.from_numpy(s_all).to(dev), torch.from_numpy(q_all).to(dev)
-        d_o = torch.empty(T, dtype=torch.float64, device=dev)
-        v = ctx.autotune(n, T, L.GAUSS, 1)
-        ctx.set_variant(v)
-        ctx.set_timing(True)
-        ms = []
-        for i in range(args.warmup + args.steps):
-            ctx.potentials_async(d_s.data_ptr(), d_q.data_ptr(), n, d_s.data_ptr(), T,
-                                 d_o.data_ptr(), L.GAUSS, 1, st.cuda_stream)
-            ctx.sync(st.cuda_stream)
-            if i >= args.warmup:
-                ms.append(ctx.last_launch()["pair_kernel_ms"])
-        pk = float(np.median(ms))
-        pairs = n * T
-        idx = np.linspace(0, T - 1, 512).astype(int)
-        acc = accuracy_vs_oracle(w, s_all[:n], q_all[:n], s_all[idx], d_o.cpu().numpy()[idx], 1)
-        p_in = pairs_in_cutoff(w, s_all, s_all[:n], 1, dev)
-        achieved = (FLOP_PER_TEST * pairs + FLOP_PER_CONTRIB * p_in) / (pk * 1e-3) / 1e12
-        out["gauss2_cfg3"] = {
-            "workload": w["desc"], "pairs_per_launch": pairs, "pair_kernel_ms": pk,
-            "pair_evals_per_s": pairs / (pk * 1e-3),
-            "roofline": {"bound": "fp32", "achieved": achieved, "peak": fp32_peak,
-                         "unit": "TFLOP/s", "frac": achieved / fp32_peak,
-                         "pairs_inside_cutoff": p_in,
-                         "frac_at_11_flop_per_pair": FLOP_PER_PAIR * pairs / (pk * 1e-3) / 1e12
-                         / fp32_peak,
-                         "note": "8 FLOP per pair tested + 3 per pair inside the cutoff, as for "
-                                 "point charges; erf(f r)/r is a "
-                                 "shared-memory table gather on top"},
-            "tile_variant": dict(ctx.variants()[v], id=v), "accuracy": acc}
-    # the precomputed 1/sqrt(k) table path on the cfg2 workload: every pair
-    # gathers one 4-byte table entry from shared memory, and every target tile
-    # streams all 40-byte source records from L2
+        out["gauss2_cfg3"] = dict(workload=w["desc"], **_kernel_leg(
+            L, ctx, args, w, s_all, q_all, n, L.GAUSS, 1, dev, st, fp32_peak))
+    # cfg2 through the FP32 1/sqrt(k) table and through the FP64 table
     w = WORKLOADS["cfg2_3d_eh_images"]
     s_all, q_all, n = make_inputs(w, 7)
-    T = len(s_all)
-    with L.Coulomb(w["X"], w["Y"], w["Z"], cutoff=w["cutoff"], device=dev.index,
-                   path=L.PATH_TABLE) as ctx:
-        d_s, d_q = torch.from_numpy(s_all).to(dev), torch.from_numpy(q_all).to(dev)
-        d_o = torch.empty(T, dtype=torch.float64, device=dev)
-        v = ctx.autotune(n, T, L.POINT, w["terms"])
-        ctx.set_variant(v)
-        ctx.set_timing(True)
-        ms = []
-        for i in range(args.warmup + args.steps):
-            ctx.potentials_async(d_s.data_ptr(), d_q.data_ptr(), n, d_s.data_ptr(), T,
-                                 d_o.data_ptr(), L.POINT, w["terms"], st.cuda_stream)
-            ctx.sync(st.cuda_stream)
-            if i >= args.warmup:
-                ms.append(ctx.last_launch()["pair_kernel_ms"])
-        last = ctx.last_launch()
-        pk = float(np.median(ms))
-        nterms = bin(w["terms"]).count("1")
-        pairs = nterms * n * T
-        idx = np.linspace(0, T - 1, 512).astype(int)
-        acc = accuracy_vs_oracle(w, s_all[:n], q_all[:n], s_all[idx], d_o.cpu().numpy()[idx],
-                                 w["terms"])
-        peaks = measured_peaks()
-        props = torch.cuda.get_device_properties(dev)
-        clk = float(peaks.get("sm_max_mhz", 1965.0)) * 1e6
-        smem_peak = props.multi_processor_count * 128 * clk / 1e9  # 32 banks x 4 B per clock
-        tiles = last["ctas"] // max(1, last["splits"])
-        n_pad = (n + 127) // 128 * 128
-        l2_bytes = tiles * n_pad * 40
-        gather = 4.0 * pairs / (pk * 1e-3) / 1e9
-        out["table_cfg2"] = {
-            "workload": w["desc"] + ", 1/sqrt(k) table path", "pairs_per_launch": pairs,
-            "pair_kernel_ms": pk, "pair_evals_per_s": pairs / (pk * 1e-3),
-            "roofline": {"bound": "shared-memory gather", "achieved": gather,
-                         "peak": smem_peak, "unit": "GB/s", "frac": gather / smem_peak,
-                         "basis": "4 B table entry per pair tested",
-                         "peak_source": "derived: SMs x 128 B per clock x sm_max_mhz",
-                         "l2_source_bytes": l2_bytes,
-                         "l2_source_gbs": l2_bytes / (pk * 1e-3) / 1e9,
-                         "frac_of_fp32_peak_at_11_flop_per_pair":
-                             FLOP_PER_PAIR * pairs / (pk * 1e-3) / 1e12 / fp32_peak},
-            # the table path runs the plain tile whatever the variant's flag
-            "tile_variant": dict(ctx.variants()[v], id=v, warp_skip=False), "accuracy": acc}
-    # kernel 1, every site of config 1's lattice
+    for key, path, what in (("table_cfg2", L.PATH_TABLE, "FP32 1/sqrt(k) table path"),
+                            ("table64_cfg2", L.PATH_TABLE64,
+                             "FP64 w(k) table, every term added in FP64")):
+        with L.Coulomb(w["X"], w["Y"], w["Z"], cutoff=w["cutoff"], device=dev.index,
+                       path=path) as ctx:
+            leg = _kernel_leg(L, ctx, args, w, s_all, q_all, n, L.POINT, w["terms"], dev, st,
+                              fp32_peak)
+            # one table entry gathered from shared memory per pair examined
+            # (4 B FP32, 8 B FP64)
+            nb = 8 if path == L.PATH_TABLE64 else 4
+            leg["shared_memory_gather_gbs"] = nb * leg["pairs_examined"] / (
+                leg["pair_kernel_ms"] * 1e-3) / 1e9
+            out[key] = dict(workload=w["desc"] + ", " + what, **leg)
+    # kernel 1: every site of config 1's lattice (163 charges) and of the
+    # 256x256x16 lattice (20,970 charges), point charges, cutoff 50
     w = WORKLOADS["cfg1_2d_holes"]
     s_all, q_all, n = make_inputs(w, 6)
-    vol = w["X"] * w["Y"] * w["Z"]
     with L.Coulomb(w["X"], w["Y"], w["Z"], cutoff=w["cutoff"], device=dev.index) as ctx:
-        d_s = torch.from_numpy(s_all[:n].copy()).to(dev)
-        d_q = torch.from_numpy(q_all[:n].copy()).to(dev)
-        d_o = torch.empty(vol, dtype=torch.float64, device=dev)
-        ctx.set_timing(True)
-        ms = []
-        for i in range(args.warmup + args.steps):
-            ctx.kernel1_async(d_s.data_ptr(), d_q.data_ptr(), n, d_o.data_ptr(), L.POINT,
-                              st.cuda_stream)
-            ctx.sync(st.cuda_stream)
-            if i >= args.warmup:
-                ms.append(ctx.last_launch()["pair_kernel_ms"])
-        pk = float(np.median(ms))
-        idx = np.linspace(0, vol - 1, 512).astype(np.int32)
-        acc = accuracy_vs_oracle(w, s_all[:n], q_all[:n], idx, d_o.cpu().numpy()[idx], 1)
-        out["kernel1_cfg1"] = {"workload": f"every site of {w['desc']}", "charges": n,
-                               "accuracy": acc,
-                               "sites": vol, "pair_kernel_ms": pk,
-                               "site_charge_evals_per_s": vol * n / (pk * 1e-3),
-                               "note": "163 charges: launch- and latency-bound; the "
-                                       "reference runs this only for output.coulomb"}
+        leg = _kernel_leg(L, ctx, args, w, s_all, q_all, n, L.POINT, 1, dev, st, fp32_peak,
+                          all_sites=True)
+        out["kernel1_cfg1"] = dict(workload=f"every site of {w['desc']}", charges=n,
+                                   note="163 charges: launch- and latency-bound; the "
+                                        "reference runs this only for output.coulomb", **leg)
+    w = dict(WORKLOADS["cfg2_3d_eh_images"], terms=1)
+    s_all, q_all, n = make_inputs(w, 8)
+    with L.Coulomb(w["X"], w["Y"], w["Z"], cutoff=w["cutoff"], device=dev.index) as ctx:
+        leg = _kernel_leg(L, ctx, args, w, s_all, q_all, n, L.POINT, 1, dev, st, fp32_peak,
+                          all_sites=True)
+        out["kernel1_1M_sites"] = dict(
+            workload="every site of 256x256x16 (1,048,576 sites), 1% electrons + 1% holes, "
+                     "cutoff 50", charges=n,
+            note="the output.coulomb dump (writer.cpp:545-581) at a size where it matters",
+            **leg)
     return out
 
 

@@ -70,6 +70,13 @@ constexpr int kBalanceTries = 1024;
 constexpr int kNT = 128, kRP = 4, kSUB = 32;
 constexpr int kTile = kNT * 2 * kRP;
 constexpr int kCullPerItem = 2;  // source chunks per work item of the culled pair sum
+// Tile of the culled pair sum: 64 threads, 2 target pairs each (the shape the
+// API's autotuner picks for the 256x256x16 and 128x128x64 workloads).
+constexpr int kCNT = 64, kCRP = 2;
+constexpr int kCTile = kCNT * 2 * kCRP;
+// Replicas with room for fewer source chunks than this keep the unculled
+// skip tile: with a handful of chunks the boxes and the cull only add launches.
+constexpr int kCullMinChunks = 8;
 
 struct Dev {
     int X, Y, Z, XY, V, hr;
@@ -321,13 +328,13 @@ __device__ __forceinline__ void finalize_body(const Dev& D, const int g) {
         // the partials of the tile's work items, in item (= chunk) order
         for (int slot = 0; slot < D.nterms; ++slot) {
             const int p = slot * tpad + g;
-            const int tile = p / kTile, loc = p - tile * kTile;
+            const int tile = p / kCTile, loc = p - tile * kCTile;
             const int ni = D.tile_items[tile];
-            const size_t f = (size_t)D.tile_first[tile] * kTile + loc;
+            const size_t f = (size_t)D.tile_first[tile] * kCTile + loc;
             double s = 0.0, m = 0.0;
             for (int i = 0; i < ni; ++i) {
-                s += D.part[f + (size_t)i * kTile];
-                m += (double)D.part_norm[f + (size_t)i * kTile];
+                s += D.part[f + (size_t)i * kCTile];
+                m += (double)D.part_norm[f + (size_t)i * kCTile];
             }
             v = slot == 0 ? s : v - s;
             n += m;
@@ -935,7 +942,7 @@ __host__ __device__ __forceinline__ CullArgs cull_args(const Dev& D) {
     CullArgs C;
     C.cbox = D.cbox; C.gbox = D.gbox;
     C.tgt = D.tgt; C.dyn = D.cnt + I_NCHUNK;
-    C.c2 = D.cutoff2; C.tile_size = kTile;
+    C.c2 = D.cutoff2; C.tile_size = kCTile;
     C.per_item = kCullPerItem; C.max_items = D.max_items;
     C.live = D.live; C.live_stride = D.src_cap / CH;
     C.items = D.items; C.item_count = D.item_count;
@@ -1237,6 +1244,7 @@ struct lgm_kmc {
     int gtab_k = 0;
     int pair_blocks = 0, pair_tiles = 0;
     int cull_grid = 0;  // persistent grid of the culled pair kernel (one wave)
+    int cull_tiles = 0; // target tiles of the culled pair sum (kCTile targets each)
     int sm_count = 0;   // SMs of the device (the guard's grid)
     std::string err;
 };
@@ -1492,8 +1500,8 @@ using KPairFn = void (*)(PairArgs);
 
 using KCulledFn = void (*)(PairArgs, CullArgs);
 KCulledFn kmc_pair_culled(int gauss) {
-    return gauss ? &pair_kernel_culled<1, 0, kNT, kRP, kSUB, true>
-                 : &pair_kernel_culled<0, 0, kNT, kRP, kSUB, true>;
+    return gauss ? &pair_kernel_culled<1, 0, kCNT, kCRP, kSUB, true>
+                 : &pair_kernel_culled<0, 0, kCNT, kCRP, kSUB, true>;
 }
 
 KPairFn kmc_pair(int gauss, int sorted = 1) {
@@ -1524,8 +1532,8 @@ lgm_status enqueue_step(lgm_kmc* k) {
         const PairArgs A = pair_args(D);
         if (D.culled) {
             k_chunk_boxes<<<D.src_cap / CH, CH, 0, st>>>(D);
-            k_cull<<<k->pair_tiles, kCullThreads, 0, st>>>(D);
-            kmc_pair_culled(D.gauss)<<<k->cull_grid, kNT, pair_smem_bytes(A.tab_k), st>>>(
+            k_cull<<<k->cull_tiles, kCullThreads, 0, st>>>(D);
+            kmc_pair_culled(D.gauss)<<<k->cull_grid, kCNT, pair_smem_bytes(A.tab_k), st>>>(
                 A, cull_args(D));
         } else {
             kmc_pair(D.gauss, D.sorted)<<<dim3(k->pair_tiles, D.splits), kNT,
@@ -1718,18 +1726,19 @@ static lgm_status kmc_create_impl(const lgm_params* pin, int32_t device, uint32_
     DA(D.tgt, tphys_cap + kTile);
     // A standalone replica's pair sum culls source chunks beyond the cutoff;
     // a batch's replicas keep the batch's work-item kernels.
-    D.culled = (!pool && D.coulomb) ? 1 : 0;
     const int src_chunks = D.src_cap / CH;
+    D.culled = (!pool && D.coulomb && src_chunks >= kCullMinChunks) ? 1 : 0;
+    k->cull_tiles = (tphys_cap + kCTile - 1) / kCTile;
     D.max_items = std::min(kMaxItemsPerTile, (src_chunks + kCullPerItem - 1) / kCullPerItem);
-    const size_t part_n = D.culled ? (size_t)k->pair_tiles * D.max_items * kTile
+    const size_t part_n = D.culled ? (size_t)k->cull_tiles * D.max_items * kCTile
                                    : (size_t)D.splits * tphys_cap;
     DA(D.part, part_n); DA(D.part_norm, part_n);
     if (D.culled) {
         DA(D.skey, D.cap_e + D.cap_h + nd_src); DA(D.stmp, D.cap_e + D.cap_h + nd_src);
         DA(D.cbox, src_chunks); DA(D.gbox, (size_t)src_chunks * kGroupsPerChunk);
-        DA(D.live, (size_t)k->pair_tiles * src_chunks);
-        DA(D.items, (size_t)k->pair_tiles * D.max_items);
-        DA(D.item_count, 1); DA(D.tile_first, k->pair_tiles); DA(D.tile_items, k->pair_tiles);
+        DA(D.live, (size_t)k->cull_tiles * src_chunks);
+        DA(D.items, (size_t)k->cull_tiles * D.max_items);
+        DA(D.item_count, 1); DA(D.tile_first, k->cull_tiles); DA(D.tile_items, k->cull_tiles);
     }
     DA(D.Vt, 2 * ncap); DA(D.Nt, 2 * ncap);
     DA(D.err, 1);
@@ -1780,7 +1789,7 @@ static lgm_status kmc_create_impl(const lgm_params* pin, int32_t device, uint32_
     D.cell_rank = crank_d;
     if (D.culled) {
         int cbps = 1;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&cbps, kmc_pair_culled(D.gauss), kNT,
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&cbps, kmc_pair_culled(D.gauss), kCNT,
                                                       pair_smem_bytes(D.gauss ? D.gtab_k : 0));
         k->cull_grid = n_sms * std::max(1, cbps);
     }
