@@ -247,16 +247,21 @@ __device__ __forceinline__ void pair_items_culled(const PairArgs& A, const CullA
     // cursor lives in shared memory, out of the other threads' registers.
     __shared__ int s_prod[6];  // item, position, tile, first, count, chunks issued
     __shared__ Box s_wbox[NT / 32];
+    // each stage also holds its chunk's four group boxes, copied with it
+    __shared__ Box s_gbox[2][kGroupsPerChunk];
     auto issue_next = [&]() {
         int* P = s_prod;
         if (P[0] >= nit) return;
         const int chunk = C.live[(size_t)P[2] * C.live_stride + P[3] + P[1]];
         const int st = P[5] & 1;
-        mbar_arrive_expect_tx(&s_bar[st], (uint32_t)pair_stage_bytes());
+        mbar_arrive_expect_tx(&s_bar[st],
+                              (uint32_t)(pair_stage_bytes() + kGroupsPerChunk * sizeof(Box)));
         bulk_g2s(s_geo + st * CH * 2, A.geo + (size_t)chunk * CH * 2,
                  (uint32_t)(CH * 2 * sizeof(float4)), &s_bar[st]);
         bulk_g2s(s_qq + st * CH, A.qq + (size_t)chunk * CH, (uint32_t)(CH * sizeof(float2)),
                  &s_bar[st]);
+        bulk_g2s(&s_gbox[st][0], C.gbox + (size_t)chunk * kGroupsPerChunk,
+                 (uint32_t)(kGroupsPerChunk * sizeof(Box)), &s_bar[st]);
         ++P[5];
         if (++P[1] == P[4]) {
             P[0] += (int)gridDim.x;
@@ -318,10 +323,8 @@ __device__ __forceinline__ void pair_items_culled(const PairArgs& A, const CullA
             const uint32_t parity = (consumed >> 1) & 1u;
             const bool mine = mbar_wait_bounded(&s_bar[st], parity, A.err);
             if (!__syncthreads_and(mine)) { failed = true; break; }
-            const int chunk = C.live[(size_t)tile * C.live_stride + first + c];
             bool gon = false;
-            if (lane < kGroupsPerChunk)
-                gon = box_gap2(s_wbox[warp], C.gbox[chunk * kGroupsPerChunk + lane]) < C.c2;
+            if (lane < kGroupsPerChunk) gon = box_gap2(s_wbox[warp], s_gbox[st][lane]) < C.c2;
             const unsigned gmask = __ballot_sync(0xffffffffu, gon);
             if (C.examined && lane == 0 && gmask)
                 atomicAdd(C.examined, (unsigned long long)__popc(gmask) * kGroup * 64 * RP);
@@ -343,9 +346,11 @@ __device__ __forceinline__ void pair_items_culled(const PairArgs& A, const CullA
                     const float2 cv = f2(g1.x, g1.y), dv = f2(g1.z, g1.w);
                     if constexpr (PATH == 2) {
                         // r^2 - 1/2 exactly, the warp vote, then w(r^2) from the
-                        // FP64 table: u + 2^23 + 1/2 holds r^2 in its low mantissa
-                        // bits; entries 0 and past the cutoff are 0, so the
-                        // clamped index also applies the cutoff and the r = 0 skip
+                        // FP64 table: r^2 = u + 1/2 and r^2 + 2^23 are exact in
+                        // FP32 (r^2 < 2^22), and the latter holds r^2 in its low
+                        // 23 mantissa bits; entries 0 and past the cutoff are 0,
+                        // so the clamped index also applies the cutoff and the
+                        // r = 0 skip
                         float2 uu[RP];
                         unsigned mk[RP];
 #pragma unroll
@@ -361,10 +366,10 @@ __device__ __forceinline__ void pair_items_culled(const PairArgs& A, const CullA
                             for (int k = 0; k + w < RP; k += 2 * w) mk[k] = min(mk[k], mk[k + w]);
                         if (__any_sync(0xffffffffu, mk[0] < ulim)) {
                             const double qd = (double)sq[j].x;
-                            const float2 magic = f2(8388608.5f, 8388608.5f);
+                            const float2 two23 = f2(8388608.f, 8388608.f);
 #pragma unroll
                             for (int k = 0; k < RP; ++k) {
-                                const float2 m2 = __fadd2_rn(uu[k], magic);
+                                const float2 m2 = __fadd2_rn(__fadd2_rn(uu[k], half2), two23);
                                 const int ix = min(__float_as_int(m2.x) & 0x7fffff, A.tab_k);
                                 const int iy = min(__float_as_int(m2.y) & 0x7fffff, A.tab_k);
                                 acc64[2 * k] = fma(qd, s_tab64[ix], acc64[2 * k]);
