@@ -246,13 +246,23 @@ int32_t lgm_kmc_batch_fused_count(const lgm_kmc_batch* b);
  * chunks per work item, and the number of work items. */
 lgm_status lgm_kmc_batch_tuning(const lgm_kmc_batch* b, int32_t* threads, int32_t* target_pairs,
                                 int32_t* chunks_per_item, int32_t* items);
-/* Times the batched pair sum on its own: `reps` launches of the tuned
- * work-item kernel over the charges the last step packed, each bracketed by
- * CUDA events on the batch stream; *ms is the median launch time.  The sums
- * it writes are the last step's sums again, so the simulation is unchanged.
- * Needs at least one step run on the per-phase kernels (LGM_ERR_STATE
- * otherwise).  Measurement aid with no counterpart in the reference. */
+/* Times the batched pair sum on its own over the charges the last step
+ * packed, `reps` times, each bracketed by CUDA events on the batch stream;
+ * *ms is the median.  The pair sum is the culled replicas' chunk boxes, tile
+ * culls and culled launch (per-phase replicas of point charges with room for
+ * at least 1024 charges) followed by the tuned work-item kernel over the
+ * other per-phase replicas.  The sums it writes are the last step's sums
+ * again, so the simulation is unchanged.  Needs at least one step run on the
+ * per-phase kernels (LGM_ERR_STATE otherwise).  Measurement aid with no
+ * counterpart in the reference. */
 lgm_status lgm_kmc_batch_time_pair(lgm_kmc_batch* b, int32_t reps, float* ms);
+/* Runs the batched pair sum once more (as lgm_kmc_batch_time_pair) and counts
+ * the source-target pairs it examined: for culled replicas, the pairs of the
+ * 32-source groups whose boxes lie within the cutoff of a warp's targets; for
+ * the others, every target against every packed source.  Measurement aid. */
+lgm_status lgm_kmc_batch_count_pairs(lgm_kmc_batch* b, uint64_t* pairs);
+/* How many replicas of the batch take the culled pair sum. */
+int32_t lgm_kmc_batch_culled_count(const lgm_kmc_batch* b);
 
 #ifdef __cplusplus
 }

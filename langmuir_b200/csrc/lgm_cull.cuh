@@ -214,13 +214,58 @@ __device__ __forceinline__ void cull_body(const CullArgs& C, const int tile) {
 // A.part[item * tile_size + local target] (and A.part_norm).  Launched with a
 // persistent grid and dynamic shared memory pair_smem_bytes(tab_k)
 // (pair_smem_bytes64 for PATH 2).
-template <int KIND, int PATH, int NT, int RP, int SUB, bool NORM>
-__device__ __forceinline__ void pair_items_culled(const PairArgs& A, const CullArgs& C) {
+//
+// The items come from a problem set PS: one problem (a call of the API, one
+// replica), or the culled replicas of a batch, whose items are numbered one
+// after the other (ProblemList).  PS::count() is the number of items,
+// PS::resolve(g, prob, local) the problem and local item of item g,
+// PS::A(prob) / PS::C(prob) that problem's arguments, and PS::first() the
+// arguments whose tables go to shared memory.
+struct OneProblem {
+    const PairArgs& a;
+    const CullArgs& c;
+    __device__ __forceinline__ int count() const { return *c.item_count; }
+    __device__ __forceinline__ void resolve(int g, int& prob, int& local) const {
+        prob = 0;
+        local = g;
+    }
+    __device__ __forceinline__ const PairArgs& A(int) const { return a; }
+    __device__ __forceinline__ const CullArgs& C(int) const { return c; }
+    __device__ __forceinline__ const PairArgs& first() const { return a; }
+};
+// The culled replicas list[0 .. n-1] of a batch, their arguments pa[r] and
+// ca[r], and offs[i] the number of items of list[0 .. i-1] (offs[n] = all).
+struct ProblemList {
+    const PairArgs* pa;
+    const CullArgs* ca;
+    const int* list;
+    const int* offs;
+    int n;
+    __device__ __forceinline__ int count() const { return n > 0 ? offs[n] : 0; }
+    __device__ __forceinline__ void resolve(int g, int& prob, int& local) const {
+        int lo = 0, hi = n;  // the last i with offs[i] <= g
+        while (hi - lo > 1) {
+            const int mid = (lo + hi) >> 1;
+            if (offs[mid] <= g) lo = mid;
+            else hi = mid;
+        }
+        prob = list[lo];
+        local = g - offs[lo];
+    }
+    __device__ __forceinline__ const PairArgs& A(int p) const { return pa[p]; }
+    __device__ __forceinline__ const CullArgs& C(int p) const { return ca[p]; }
+    __device__ __forceinline__ const PairArgs& first() const { return pa[list[0]]; }
+};
+
+template <int KIND, int PATH, int NT, int RP, int SUB, bool NORM, class PS>
+__device__ __forceinline__ void pair_items_culled(const PS& P) {
     static_assert(kGroup % SUB == 0, "an FP32 run lies inside one group");
     static_assert(PATH != 2 || !NORM, "the FP64-table path carries no FP32 run norms");
     constexpr int TS = NT * 2 * RP;
-    const int nit = *C.item_count;
+    const int nit = P.count();
     if ((int)blockIdx.x >= nit) return;
+    // the shared-memory tables are the first problem's (a problem set shares them)
+    const PairArgs& A0 = P.first();
     extern __shared__ __align__(128) unsigned char smem[];
     float4* s_geo = reinterpret_cast<float4*>(smem);                               // [2][CH*2]
     float2* s_qq = reinterpret_cast<float2*>(smem + 2 * CH * 2 * sizeof(float4));  // [2][CH]
@@ -229,65 +274,74 @@ __device__ __forceinline__ void pair_items_culled(const PairArgs& A, const CullA
     double* s_tab64 = reinterpret_cast<double*>(smem + 2 * pair_stage_bytes() + 16);
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int t_phys = A.dyn ? A.dyn[1] : A.t_phys;
     if (tid == 0) {
         mbar_init(&s_bar[0], 1);
         mbar_init(&s_bar[1], 1);
         fence_mbar_init();
     }
     if (PATH == 2) {
-        for (int k = tid; k <= A.tab_k; k += NT) s_tab64[k] = A.tab64[k];
+        for (int k = tid; k <= A0.tab_k; k += NT) s_tab64[k] = A0.tab64[k];
     } else if (KIND == 1 || PATH == 1) {
-        for (int k = tid; k <= A.tab_k; k += NT) s_tab[k] = A.tab[k];
+        for (int k = tid; k <= A0.tab_k; k += NT) s_tab[k] = A0.tab[k];
     }
     __syncthreads();
 
     // Producer (thread 0): walks this CTA's chunk sequence -- the live chunks
     // of items blockIdx.x, blockIdx.x + G, ... -- two chunks ahead.  Its
     // cursor lives in shared memory, out of the other threads' registers.
-    __shared__ int s_prod[6];  // item, position, tile, first, count, chunks issued
+    // item, position, tile, first, count, chunks issued, problem
+    __shared__ int s_prod[7];
     __shared__ Box s_wbox[NT / 32];
     // each stage also holds its chunk's four group boxes, copied with it
     __shared__ Box s_gbox[2][kGroupsPerChunk];
+    auto load_item = [&](int g) {  // the producer's cursor onto item g
+        int prob, local;
+        P.resolve(g, prob, local);
+        const int4 r = P.C(prob).items[local];
+        s_prod[2] = r.x; s_prod[3] = r.y; s_prod[4] = r.z; s_prod[6] = prob;
+    };
     auto issue_next = [&]() {
-        int* P = s_prod;
-        if (P[0] >= nit) return;
-        const int chunk = C.live[(size_t)P[2] * C.live_stride + P[3] + P[1]];
-        const int st = P[5] & 1;
+        int* Q = s_prod;
+        if (Q[0] >= nit) return;
+        const PairArgs& Ap = P.A(Q[6]);
+        const CullArgs& Cp = P.C(Q[6]);
+        const int chunk = Cp.live[(size_t)Q[2] * Cp.live_stride + Q[3] + Q[1]];
+        const int st = Q[5] & 1;
         mbar_arrive_expect_tx(&s_bar[st],
                               (uint32_t)(pair_stage_bytes() + kGroupsPerChunk * sizeof(Box)));
-        bulk_g2s(s_geo + st * CH * 2, A.geo + (size_t)chunk * CH * 2,
+        bulk_g2s(s_geo + st * CH * 2, Ap.geo + (size_t)chunk * CH * 2,
                  (uint32_t)(CH * 2 * sizeof(float4)), &s_bar[st]);
-        bulk_g2s(s_qq + st * CH, A.qq + (size_t)chunk * CH, (uint32_t)(CH * sizeof(float2)),
+        bulk_g2s(s_qq + st * CH, Ap.qq + (size_t)chunk * CH, (uint32_t)(CH * sizeof(float2)),
                  &s_bar[st]);
-        bulk_g2s(&s_gbox[st][0], C.gbox + (size_t)chunk * kGroupsPerChunk,
+        bulk_g2s(&s_gbox[st][0], Cp.gbox + (size_t)chunk * kGroupsPerChunk,
                  (uint32_t)(kGroupsPerChunk * sizeof(Box)), &s_bar[st]);
-        ++P[5];
-        if (++P[1] == P[4]) {
-            P[0] += (int)gridDim.x;
-            P[1] = 0;
-            if (P[0] < nit) {
-                const int4 r = C.items[P[0]];
-                P[2] = r.x; P[3] = r.y; P[4] = r.z;
-            }
+        ++Q[5];
+        if (++Q[1] == Q[4]) {
+            Q[0] += (int)gridDim.x;
+            Q[1] = 0;
+            if (Q[0] < nit) load_item(Q[0]);
         }
     };
     if (tid == 0) {
-        const int4 r = C.items[blockIdx.x];
-        s_prod[0] = (int)blockIdx.x; s_prod[1] = 0;
-        s_prod[2] = r.x; s_prod[3] = r.y; s_prod[4] = r.z; s_prod[5] = 0;
+        s_prod[0] = (int)blockIdx.x; s_prod[1] = 0; s_prod[5] = 0;
+        load_item((int)blockIdx.x);
         issue_next();
         issue_next();
     }
 
-    const unsigned ulim = __float_as_uint(A.c2 - 0.5f);
     const float2 half2 = f2(0.5f, 0.5f);
     uint32_t consumed = 0;
     bool failed = false;
 
     for (int it = (int)blockIdx.x; it < nit; it += (int)gridDim.x) {
-        const int4 rec = C.items[it];
-        const int tile = rec.x, first = rec.y, count = rec.z;
+        int prob, local;
+        P.resolve(it, prob, local);
+        const PairArgs& A = P.A(prob);
+        const CullArgs& C = P.C(prob);
+        const int t_phys = A.dyn ? A.dyn[1] : A.t_phys;
+        const unsigned ulim = __float_as_uint(A.c2 - 0.5f);
+        const int4 rec = C.items[local];
+        const int tile = rec.x, count = rec.z;
         const int base = tile * TS;
         auto target_of = [&](int k) { return base + warp * (64 * RP) + k * 32 + lane; };
         float2 tx[RP], ty[RP], tz[RP], tt[RP];
@@ -449,13 +503,13 @@ __device__ __forceinline__ void pair_items_culled(const PairArgs& A, const CullA
             }
         }
         if (failed) break;
-        double* out = A.part + (size_t)it * TS;
+        double* out = A.part + (size_t)local * TS;
 #pragma unroll
         for (int k = 0; k < 2 * RP; ++k) {
             const int p = target_of(k);
             if (p < t_phys) {
                 out[p - base] = acc64[k];
-                if (NORM) A.part_norm[(size_t)it * TS + (p - base)] = nrm[NORM ? k : 0];
+                if (NORM) A.part_norm[(size_t)local * TS + (p - base)] = nrm[NORM ? k : 0];
             }
         }
     }
@@ -469,7 +523,14 @@ __device__ __forceinline__ void pair_items_culled(const PairArgs& A, const CullA
 
 template <int KIND, int PATH, int NT, int RP, int SUB, bool NORM = false>
 __global__ void __launch_bounds__(NT) pair_kernel_culled(PairArgs A, CullArgs C) {
-    pair_items_culled<KIND, PATH, NT, RP, SUB, NORM>(A, C);
+    pair_items_culled<KIND, PATH, NT, RP, SUB, NORM>(OneProblem{A, C});
+}
+
+// The culled replicas of a batch in one persistent launch (point charges,
+// MUFU path): their items are numbered one after the other (ProblemList).
+template <int NT, int RP, int SUB, bool NORM>
+__global__ void __launch_bounds__(NT) pair_kernel_culled_list(ProblemList L) {
+    pair_items_culled<0, 0, NT, RP, SUB, NORM>(L);
 }
 
 // (static: each translation unit that launches them has its own copy)

@@ -991,10 +991,38 @@ __global__ void kb_decide(const Dev* R, const int4* map) { LGM_BATCH_LOOP(decide
 __global__ void kb_tbins_zero(const Dev* R, const int4* map) { LGM_BATCH_LOOP(tbins_zero_body(D, i)) }
 __global__ void kb_tbins(const Dev* R, const int4* map) { LGM_BATCH_LOOP(tbins_body(D, i)) }
 __global__ void kb_tscatter(const Dev* R, const int4* map) { LGM_BATCH_LOOP(tscatter_body(D, i)) }
-// one block per replica of the list
+// one block per replica of the list; a second row scans culled replicas' source bins
 __global__ void __launch_bounds__(1024) kb_tbins_scan(const Dev* R, const int* list) {
     const Dev& D = R[list[blockIdx.x]];
-    block_exclusive_scan(D.bins, D.ncells + 1);
+    if (blockIdx.y == 0) block_exclusive_scan(D.bins, D.ncells + 1);
+    else if (D.culled) block_exclusive_scan(D.sbins, 3 * (D.ncells + 1));
+}
+// The culled replicas' chunk boxes and tile culls: block b works for replica
+// map[b].x as its chunk or tile map[b].y.
+__global__ void __launch_bounds__(CH) kb_chunk_boxes(const Dev* R, const int2* map) {
+    const Dev& D = R[map[blockIdx.x].x];
+    chunk_boxes_body(pair_args(D), cull_args(D), map[blockIdx.x].y);
+}
+__global__ void __launch_bounds__(kCullThreads) kb_cull(const Dev* R, const int2* map) {
+    cull_body(cull_args(R[map[blockIdx.x].x]), map[blockIdx.x].y);
+}
+// Pairs the work-item kernel tests for the per-phase replicas that do not
+// cull: every physical target against every packed source (one block).
+__global__ void kb_tested_pairs(const Dev* R, const int* list, int n, unsigned long long* out) {
+    for (int i = (int)threadIdx.x; i < n; i += (int)blockDim.x) {
+        const Dev& D = R[list[i]];
+        if (D.culled) continue;
+        const int32_t* dyn = D.cnt + I_NCHUNK;
+        atomicAdd(out, (unsigned long long)dyn[0] * CH * (unsigned long long)dyn[1]);
+    }
+}
+// offs[i] = work items of culled replicas list[0 .. i-1], i <= n (one block)
+__global__ void __launch_bounds__(1024) kb_item_offsets(const Dev* R, const int* list, int n,
+                                                        int32_t* offs) {
+    for (int i = (int)threadIdx.x; i <= n; i += (int)blockDim.x)
+        offs[i] = i < n ? *R[list[i]].item_count : 0;
+    __syncthreads();
+    block_exclusive_scan(offs, n + 1);
 }
 __global__ void __launch_bounds__(kGuardThreads) kb_guard(const Dev* R, const int4* map) {
     __shared__ double2 red[32];
@@ -1245,6 +1273,7 @@ struct lgm_kmc {
     int pair_blocks = 0, pair_tiles = 0;
     int cull_grid = 0;  // persistent grid of the culled pair kernel (one wave)
     int cull_tiles = 0; // target tiles of the culled pair sum (kCTile targets each)
+    bool cull_ok = false;  // the culled pair sum's buffers exist
     int sm_count = 0;   // SMs of the device (the guard's grid)
     std::string err;
 };
@@ -1504,6 +1533,9 @@ KCulledFn kmc_pair_culled(int gauss) {
                  : &pair_kernel_culled<0, 0, kCNT, kCRP, kSUB, true>;
 }
 
+// the culled replicas of a batch (point charges), one persistent launch
+constexpr auto kBatchCulled = &pair_kernel_culled_list<kCNT, kCRP, kSUB, true>;
+
 KPairFn kmc_pair(int gauss, int sorted = 1) {
     if (sorted)
         return gauss ? &pair_kernel<1, 0, kNT, kRP, kSUB, true, true>
@@ -1724,16 +1756,21 @@ static lgm_status kmc_create_impl(const lgm_params* pin, int32_t device, uint32_
     DA(D.cnt, I_NUM); DA(D.ctr, C_NUM);
     DA(D.geo, 2 * D.src_cap); DA(D.qq, D.src_cap);
     DA(D.tgt, tphys_cap + kTile);
-    // A standalone replica's pair sum culls source chunks beyond the cutoff;
-    // a batch's replicas keep the batch's work-item kernels.
+    // The pair sum culls source chunks beyond the cutoff when the replica has
+    // room for kCullMinChunks of them: a standalone replica always, a batch's
+    // replica when the batch puts it on the per-phase kernels (partition_batch
+    // sets D.culled; its partials then take either layout).
     const int src_chunks = D.src_cap / CH;
-    D.culled = (!pool && D.coulomb && src_chunks >= kCullMinChunks) ? 1 : 0;
+    k->cull_ok = D.coulomb && src_chunks >= kCullMinChunks;
+    D.culled = (k->cull_ok && !pool) ? 1 : 0;
     k->cull_tiles = (tphys_cap + kCTile - 1) / kCTile;
     D.max_items = std::min(kMaxItemsPerTile, (src_chunks + kCullPerItem - 1) / kCullPerItem);
-    const size_t part_n = D.culled ? (size_t)k->cull_tiles * D.max_items * kCTile
-                                   : (size_t)D.splits * tphys_cap;
+    const size_t part_cull = (size_t)k->cull_tiles * D.max_items * kCTile;
+    const size_t part_n = D.culled ? part_cull
+                          : k->cull_ok ? std::max(part_cull, (size_t)D.splits * tphys_cap)
+                                       : (size_t)D.splits * tphys_cap;
     DA(D.part, part_n); DA(D.part_norm, part_n);
-    if (D.culled) {
+    if (k->cull_ok) {
         DA(D.skey, D.cap_e + D.cap_h + nd_src); DA(D.stmp, D.cap_e + D.cap_h + nd_src);
         DA(D.cbox, src_chunks); DA(D.gbox, (size_t)src_chunks * kGroupsPerChunk);
         DA(D.live, (size_t)k->cull_tiles * src_chunks);
@@ -1757,7 +1794,7 @@ static lgm_status kmc_create_impl(const lgm_params* pin, int32_t device, uint32_
     int32_t* crank_d = nullptr;
     DA(crank_d, D.ncells);
     DA(D.bins, D.ncells + 2);
-    if (D.culled) DA(D.sbins, 3 * (D.ncells + 1) + 1);
+    if (k->cull_ok) DA(D.sbins, 3 * (D.ncells + 1) + 1);
     DA(D.tkey, 2 * ncap);
     DA(D.tperm, 2 * ncap);
 #undef DA
@@ -2078,6 +2115,16 @@ struct lgm_kmc_batch {
     bool fused_set = false;    // the caller set the bound: capacity alone decides
     std::vector<int> fused, classic;
     int *d_fused = nullptr, *d_classic = nullptr;
+    // per-phase replicas whose pair sum culls source chunks (point charges):
+    // their chunk boxes, tile culls and one persistent launch over all their
+    // work items (lgm_cull.cuh, ProblemList); the others take the items kernel
+    std::vector<int> culled;
+    int* d_culled = nullptr;
+    int32_t* d_coffs = nullptr;      // [culled + 1] work-item offsets
+    PairArgs* d_cpargs = nullptr;    // [count], filled for the culled replicas
+    CullArgs* d_cargs = nullptr;     // [count]
+    int2 *map_box = nullptr, *map_cull = nullptr;
+    int nb_box = 0, nb_cull = 0, cull_grid = 0;
     cudaStream_t aux = nullptr;            // the fused branch of the graph
     cudaEvent_t fork = nullptr, join = nullptr;
     DevicePool pool;                         // every replica's buffers
@@ -2112,6 +2159,7 @@ lgm_status build_items(lgm_kmc_batch* b, int v, int cpi) {
     for (int r : b->fused) b->hD[r].splits = 1;  // the fused pair sum is one split
     for (int r : b->classic) {
         Dev& D = b->hD[r];
+        if (D.culled) continue;  // the culled launch covers it
         const lgm_kmc* k = b->reps[r];
         const int chunks = D.src_cap / CH;
         const int splits = std::max(1, std::min(k->D.splits, (chunks + cpi - 1) / cpi));
@@ -2155,11 +2203,29 @@ size_t batch_smem(const lgm_kmc_batch* b) {
     return pair_smem_bytes(tk);
 }
 
-lgm_status enqueue_batch_pair(lgm_kmc_batch* b, cudaStream_t st) {
-    const BatchVariant& BV = kBatchVariants[b->variant];
-    BV.fn[b->gauss]<<<b->n_items, BV.nt, batch_smem(b), st>>>(b->d_pargs, b->d_items);
+// The work-item kernel over the per-phase replicas that do not cull.
+lgm_status enqueue_batch_items(lgm_kmc_batch* b, cudaStream_t st) {
+    if (b->n_items > 0) {
+        const BatchVariant& BV = kBatchVariants[b->variant];
+        BV.fn[b->gauss]<<<b->n_items, BV.nt, batch_smem(b), st>>>(b->d_pargs, b->d_items);
+    }
     BCUDA(b, cudaGetLastError());
     return LGM_OK;
+}
+
+// The batched pair sum: the culled replicas' chunk boxes, tile culls, item
+// offsets and one persistent launch over all their items, then the work-item
+// kernel over the rest.
+lgm_status enqueue_batch_pair(lgm_kmc_batch* b, cudaStream_t st) {
+    if (!b->culled.empty()) {
+        const int n = (int)b->culled.size();
+        kb_chunk_boxes<<<b->nb_box, CH, 0, st>>>(b->d_reps, b->map_box);
+        kb_cull<<<b->nb_cull, kCullThreads, 0, st>>>(b->d_reps, b->map_cull);
+        kb_item_offsets<<<1, 1024, 0, st>>>(b->d_reps, b->d_culled, n, b->d_coffs);
+        kBatchCulled<<<b->cull_grid, kCNT, pair_smem_bytes(0), st>>>(
+            ProblemList{b->d_cpargs, b->d_cargs, b->d_culled, b->d_coffs, n});
+    }
+    return enqueue_batch_items(b, st);
 }
 
 void launch_fused(const lgm_kmc_batch* b, cudaStream_t st, int steps) {
@@ -2193,7 +2259,8 @@ lgm_status enqueue_fused(lgm_kmc_batch* b, int steps, bool branch) {
 void enqueue_batch_sort(lgm_kmc_batch* b, cudaStream_t st) {
     kb_tbins_zero<<<b->nb_bins, 256, 0, st>>>(b->d_reps, b->map_bins);
     kb_tbins<<<b->nb_fin, 256, 0, st>>>(b->d_reps, b->map_fin);
-    kb_tbins_scan<<<(int)b->classic.size(), 1024, 0, st>>>(b->d_reps, b->d_classic);
+    kb_tbins_scan<<<dim3((unsigned)b->classic.size(), b->culled.empty() ? 1u : 2u), 1024, 0, st>>>(
+        b->d_reps, b->d_classic);
     kb_tscatter<<<b->nb_fin, 256, 0, st>>>(b->d_reps, b->map_fin);
 }
 
@@ -2239,7 +2306,7 @@ lgm_status enqueue_batch_step(lgm_kmc_batch* b) {
 // The project's tile tuner for the batch: times every (variant, chunks per
 // item) pair on the batch's current charges with CUDA events, keeps the best.
 lgm_status tune_batch(lgm_kmc_batch* b) {
-    if (!b->coulomb || b->classic.empty()) return LGM_OK;
+    if (!b->coulomb || b->classic.size() == b->culled.size()) return LGM_OK;
     cudaStream_t st = b->stream;
     kb_choose<<<b->nb_car, 256, 0, st>>>(b->d_reps, b->map_car);
     enqueue_batch_sort(b, st);
@@ -2258,7 +2325,7 @@ lgm_status tune_batch(lgm_kmc_batch* b) {
             float ms[3];
             for (int r = 0; r < 3; ++r) {
                 cudaEventRecord(e0, st);
-                if ((s = enqueue_batch_pair(b, st)) != LGM_OK) return s;
+                if ((s = enqueue_batch_items(b, st)) != LGM_OK) return s;
                 cudaEventRecord(e1, st);
                 cudaEventSynchronize(e1);
                 cudaEventElapsedTime(&ms[r], e0, e1);
@@ -2297,6 +2364,25 @@ lgm_status partition_batch(lgm_kmc_batch* b) {
         b->fused_small &= b->hD[r].cap_e + b->hD[r].cap_h <= kFusedSmallCharges;
     for (int r : b->fused) b->hD[r].sorted = 0;  // the fused step keeps the list order
     for (int r : b->classic) b->hD[r].sorted = b->hD[r].coulomb;
+    // culled pair sums for the per-phase replicas with room for enough chunks
+    // (point charges: the Gaussian tables differ between replicas)
+    b->culled.clear();
+    for (int r = 0; r < (int)b->hD.size(); ++r) b->hD[r].culled = 0;
+    for (int r : b->classic)
+        if (b->reps[r]->cull_ok && !b->gauss) {
+            b->hD[r].culled = 1;
+            b->culled.push_back(r);
+        }
+    std::vector<int2> box, cull;
+    std::vector<PairArgs> cpargs(b->hD.size());
+    std::vector<CullArgs> cargs(b->hD.size());
+    for (int r : b->culled) {
+        const Dev& D = b->hD[r];
+        for (int c = 0; c < D.src_cap / CH; ++c) box.push_back(make_int2(r, c));
+        for (int t = 0; t < b->reps[r]->cull_tiles; ++t) cull.push_back(make_int2(r, t));
+        cpargs[r] = pair_args(D);
+        cargs[r] = cull_args(D);
+    }
     std::vector<int4> car, pack, fin, guard, bins;
     auto add = [](std::vector<int4>& v, int r, int bound) {
         const int nb = std::max(1, (bound + kItemsPerThread * 256 - 1) / (kItemsPerThread * 256));
@@ -2308,8 +2394,9 @@ lgm_status partition_batch(lgm_kmc_batch* b) {
         const int ncap = std::max(1, D.cap_e + D.cap_h);
         add(car, r, ncap);
         add(pack, r, std::max(D.src_cap, D.tpad_cap));
-        add(fin, r, 2 * ncap);
-        add(bins, r, D.ncells + 1);
+        // a culled replica's source sort also walks the defects
+        add(fin, r, D.culled ? std::max(2 * ncap, ncap + (D.dq != 0 ? D.nd : 0)) : 2 * ncap);
+        add(bins, r, D.culled ? 3 * (D.ncells + 1) : D.ncells + 1);
         // flagged decisions grow with the charge count: one block per 2048 of capacity
         const int ng = std::min(kGuardBlocksPerReplica, std::max(1, (ncap + 2047) / 2048));
         for (int i = 0; i < ng; ++i) guard.push_back(make_int4(r, i, ng, 0));
@@ -2325,8 +2412,23 @@ lgm_status partition_batch(lgm_kmc_batch* b) {
     };
     if (!upload(&b->map_car, car) || !upload(&b->map_pack, pack) || !upload(&b->map_fin, fin) ||
         !upload(&b->map_guard, guard) || !upload(&b->map_bins, bins) ||
-        !upload(&b->d_fused, b->fused) || !upload(&b->d_classic, b->classic))
+        !upload(&b->d_fused, b->fused) || !upload(&b->d_classic, b->classic) ||
+        !upload(&b->d_culled, b->culled) || !upload(&b->map_box, box) ||
+        !upload(&b->map_cull, cull) || !upload(&b->d_cpargs, cpargs) ||
+        !upload(&b->d_cargs, cargs))
         return bfail(b, LGM_ERR_CUDA, "block maps");
+    if (b->d_coffs) cudaFree(b->d_coffs);
+    b->d_coffs = nullptr;
+    if (cudaMalloc(&b->d_coffs, sizeof(int32_t) * (b->culled.size() + 1)) != cudaSuccess)
+        return bfail(b, LGM_ERR_CUDA, "work-item offsets");
+    b->nb_box = (int)box.size();
+    b->nb_cull = (int)cull.size();
+    if (!b->culled.empty()) {
+        int dev_sms = 0, cbps = 1;
+        cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, b->device);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&cbps, kBatchCulled, kCNT, pair_smem_bytes(0));
+        b->cull_grid = std::max(1, dev_sms) * std::max(1, cbps);
+    }
     b->nb_guard = (int)guard.size();
     b->nb_bins = (int)bins.size();
     // the compaction loops over its list in blocks: small replicas need no 1024-thread block
@@ -2402,7 +2504,8 @@ lgm_status lgm_kmc_batch_destroy(lgm_kmc_batch* b) {
     if (b->exec) cudaGraphExecDestroy(b->exec);
     if (b->graph) cudaGraphDestroy(b->graph);
     void* ptrs[] = {b->d_reps, b->d_pargs, b->d_items, b->map_car, b->map_pack, b->map_fin,
-                    b->map_guard, b->map_bins, b->d_fused, b->d_classic};
+                    b->map_guard, b->map_bins, b->d_fused, b->d_classic, b->d_culled,
+                    b->d_coffs, b->d_cpargs, b->d_cargs, b->map_box, b->map_cull};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (b->fork) cudaEventDestroy(b->fork);
@@ -2420,6 +2523,10 @@ const char* lgm_kmc_batch_last_error(const lgm_kmc_batch* b) {
 }
 
 int32_t lgm_kmc_batch_size(const lgm_kmc_batch* b) { return b ? (int32_t)b->reps.size() : 0; }
+
+int32_t lgm_kmc_batch_culled_count(const lgm_kmc_batch* b) {
+    return b ? (int32_t)b->culled.size() : 0;
+}
 
 lgm_kmc* lgm_kmc_batch_replica(lgm_kmc_batch* b, int32_t i) {
     if (!b || i < 0 || i >= (int)b->reps.size()) return nullptr;
@@ -2499,6 +2606,45 @@ lgm_status lgm_kmc_batch_time_pair(lgm_kmc_batch* b, int32_t reps, float* ms) {
     std::sort(t.begin(), t.end());
     *ms = t[reps / 2];
     return LGM_OK;
+}
+
+lgm_status lgm_kmc_batch_count_pairs(lgm_kmc_batch* b, uint64_t* pairs) {
+    if (!b || !pairs) return LGM_ERR_INVALID_ARGUMENT;
+    if (!b->exec || !b->coulomb || b->classic.empty())
+        return bfail(b, LGM_ERR_STATE, "no per-phase Coulomb step has run");
+    BCUDA(b, cudaSetDevice(b->device));
+    cudaStream_t st = b->stream;
+    BCUDA(b, cudaStreamSynchronize(st));
+    unsigned long long* d_n = nullptr;
+    BCUDA(b, cudaMalloc(&d_n, sizeof *d_n));
+    std::vector<CullArgs> cargs(b->hD.size());
+    for (int r : b->culled) {
+        cargs[r] = cull_args(b->hD[r]);
+        cargs[r].examined = d_n;
+    }
+    lgm_status s = LGM_OK;
+    unsigned long long h = 0;
+    auto put = [&](bool on) {
+        if (!on)
+            for (int r : b->culled) cargs[r].examined = nullptr;
+        return cudaMemcpy(b->d_cargs, cargs.data(), sizeof(CullArgs) * cargs.size(),
+                          cudaMemcpyHostToDevice) == cudaSuccess;
+    };
+    if (cudaMemset(d_n, 0, sizeof *d_n) != cudaSuccess || !put(true)) {
+        s = bfail(b, LGM_ERR_CUDA, "pair counter");
+    } else {
+        s = enqueue_batch_pair(b, st);
+        if (s == LGM_OK) {
+            kb_tested_pairs<<<1, 256, 0, st>>>(b->d_reps, b->d_classic, (int)b->classic.size(), d_n);
+            if (cudaStreamSynchronize(st) != cudaSuccess ||
+                cudaMemcpy(&h, d_n, sizeof h, cudaMemcpyDeviceToHost) != cudaSuccess)
+                s = bfail(b, LGM_ERR_CUDA, "pair count");
+        }
+        if (!put(false) && s == LGM_OK) s = bfail(b, LGM_ERR_CUDA, "pair counter");
+    }
+    cudaFree(d_n);
+    if (s == LGM_OK) *pairs = h;
+    return s;
 }
 
 lgm_status lgm_kmc_batch_tuning(const lgm_kmc_batch* b, int32_t* threads, int32_t* target_pairs,

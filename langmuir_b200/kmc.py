@@ -294,12 +294,15 @@ N.SIGNATURES.update({
     "lgm_kmc_batch_set_fused": (_i32, [_vp, _i32]),
     "lgm_kmc_batch_fused_count": (_i32, [_vp]),
     "lgm_kmc_batch_time_pair": (_i32, [_vp, _i32, ctypes.POINTER(ctypes.c_float)]),
+    "lgm_kmc_batch_count_pairs": (_i32, [_vp, ctypes.POINTER(ctypes.c_uint64)]),
+    "lgm_kmc_batch_culled_count": (_i32, [_vp]),
 })
 if N._lib is not None:
     for _name in ("lgm_kmc_batch_create", "lgm_kmc_batch_destroy", "lgm_kmc_batch_last_error",
                   "lgm_kmc_batch_run", "lgm_kmc_batch_size", "lgm_kmc_batch_replica",
                   "lgm_kmc_batch_tuning", "lgm_kmc_batch_set_fused", "lgm_kmc_batch_fused_count",
-                  "lgm_kmc_batch_time_pair"):
+                  "lgm_kmc_batch_time_pair", "lgm_kmc_batch_count_pairs",
+                  "lgm_kmc_batch_culled_count"):
         _fn = getattr(N._lib, _name)
         _fn.restype, _fn.argtypes = N.SIGNATURES[_name]
 
@@ -345,6 +348,11 @@ class KMCBatch:
         """Replicas on the fused step."""
         return N.lib().lgm_kmc_batch_fused_count(self._h)
 
+    @property
+    def culled_count(self) -> int:
+        """Replicas whose pair sum culls source chunks beyond the cutoff."""
+        return N.lib().lgm_kmc_batch_culled_count(self._h)
+
     def close(self):
         if getattr(self, "_h", None) and self._h.value and N._lib is not None:
             N._lib.lgm_kmc_batch_destroy(self._h)
@@ -388,3 +396,13 @@ class KMCBatch:
         if st != N.OK:
             raise N.LgmError(st, N.lib().lgm_kmc_batch_last_error(self._h).decode())
         return ms.value
+
+    def count_pairs(self) -> int:
+        """Source-target pairs the batched pair sum examines over the charges
+        the last step packed (culled replicas: the pairs of source groups
+        within the cutoff of a warp's targets; the others: all pairs)."""
+        n = ctypes.c_uint64()
+        st = N.lib().lgm_kmc_batch_count_pairs(self._h, ctypes.byref(n))
+        if st != N.OK:
+            raise N.LgmError(st, N.lib().lgm_kmc_batch_last_error(self._h).decode())
+        return n.value

@@ -316,6 +316,45 @@ def test_batch_time_pair_leaves_the_run_unchanged():
 
 
 @pytest.mark.gpu
+def test_batch_culled_replicas_match_single_replicas():
+    """Per-phase replicas with room for 8 or more source chunks take the
+    culled pair sum (one persistent launch over every such replica's work
+    items), the smaller ones the work-item kernel, in one batch: each replica
+    follows the trajectory of the standalone replica with its id, also after
+    the pair sum was timed and counted in between."""
+    rng = np.random.default_rng(8)
+    params = []
+    for i in range(6):
+        xy = [48, 64, 96, 128, 128, 112][i]
+        z = [1, 1, 2, 2, 1, 2][i]
+        occ = float(rng.uniform(0.02, 0.04))
+        params.append(make_params(grid_x=xy, grid_y=xy, grid_z=z, electron_percentage=occ,
+                                  hole_percentage=occ / 2,
+                                  electrostatic_cutoff=[20, 50, 30, 50, 40, 50][i],
+                                  voltage_right=float(rng.uniform(0.1, 2.0)),
+                                  trap_percentage=0.05, trap_potential=0.1,
+                                  h_source_r_rate=0.5, h_drain_l_rate=0.9))
+    steps = 24
+    with L.KMCBatch(params, replica0=60, fused_max_charges=0) as b:
+        assert 0 < b.culled_count < len(params)
+        b.run(steps // 2)
+        assert b.time_pair(3) > 0.0
+        examined = b.count_pairs()
+        full = sum(2 * (r.stats()["electrons"] + r.stats()["holes"]) ** 2
+                   for r in (b.replica(i) for i in range(len(params))))
+        assert 0 < examined < full
+        b.run(steps - steps // 2)
+        got = [(b.replica(i).carriers(), b.replica(i).stats()) for i in range(len(params))]
+    for i, p in enumerate(params):
+        with L.KMC(p, replica=60 + i) as g:
+            g.run(steps)
+            (e, h), s = g.carriers(), g.stats()
+        np.testing.assert_array_equal(got[i][0][0], e, err_msg=f"replica {i} electrons")
+        np.testing.assert_array_equal(got[i][0][1], h, err_msg=f"replica {i} holes")
+        assert got[i][1]["counters"] == s["counters"]
+
+
+@pytest.mark.gpu
 @pytest.mark.parametrize("case", ["solar_confined_interface", "solar_3d_gauss_confined"])
 def test_fused_batch_solar_matches_single_replicas(case):
     """Solar-cell replicas (exciton source, recombination, confinement) with a
