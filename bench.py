@@ -463,8 +463,17 @@ def batch_params(L, n, seed=4):
     return out
 
 
+def fp32_peak_derived(dev):
+    """FP32 FMA peak from the SM count and the maximum SM clock: 128 lanes x
+    2 FLOP per SM per cycle (TFLOP/s)."""
+    import torch
+    sms = torch.cuda.get_device_properties(dev).multi_processor_count
+    return sms * 128 * 2 * float(measured_peaks().get("sm_max_mhz", 1965.0)) * 1e6 / 1e12
+
+
 def batch_run(L, args, rank):
     """Batched replicas in one graph vs the same replicas stepped one by one."""
+    import torch
     params = batch_params(L, args.batch_replicas, seed=4 + rank)
     dev = int(os.environ.get("LOCAL_RANK", "0"))
     t0 = time.perf_counter()
@@ -488,9 +497,22 @@ def batch_run(L, args, rank):
         # the pair sum alone (CUDA events), after one more step from these counts
         b.run(1)
         pair_ms = b.time_pair(7)
-        pairs_timed = float(np.sum(2.0 * m1 * m1))
+        m2 = np.array([r.stats()["electrons"] + r.stats()["holes"] for r in reps], np.float64)
+        pairs_timed = float(np.sum(2.0 * m2 * m2))
+        examined = b.count_pairs()
+        # pairs inside the cutoff, estimated from the current sites: each
+        # replica's 2M targets are its M current sites and M proposed sites
+        # one hop away, so about twice the current-current pairs
+        p_in = 0
+        for i, r in enumerate(reps):
+            e, h = r.carriers()
+            sites = np.concatenate([e, h])
+            p = params[i]
+            w = {"X": p.grid_x, "Y": p.grid_y, "cutoff": p.electrostatic_cutoff}
+            p_in += 2 * pairs_in_cutoff(w, sites, sites, 1, torch.device("cuda", dev))
         tuning = b.tuning()
         fused = b.fused_count
+        culled = b.culled_count
     # the same replicas with every one on the per-phase kernels
     with L.KMCBatch(params, device=dev, replica0=1000 * rank, fused_max_charges=0) as b:
         b.run(max(1, args.warmup))
@@ -512,6 +534,8 @@ def batch_run(L, args, rank):
             s_time += time.perf_counter() - t1
             s_hops += k.stats()["proposals"] - h
     single = s_hops / s_time
+    fp32_peak = fp32_peak_derived(torch.device("cuda", dev))
+    ach = (FLOP_PER_TEST * examined + FLOP_PER_CONTRIB * p_in) / (pair_ms * 1e-3) / 1e12
     return {"workload": f"{len(params)} replicas, side {{32,64,128,256}} x depth {{1,2,4,8}}, "
                         "occupancy U(0.5%,3%) e/h, V U(0.1,2), traps U(0,10%) at U(0.05,0.3) eV, "
                         "cutoff 50",
@@ -523,11 +547,21 @@ def batch_run(L, args, rank):
             "speedup_vs_single": (hops / dt) / single, "tuning": tuning,
             "pairs_per_step": pairs_per_step,
             "pair_evals_per_s_in_step": pairs_per_step / (dt / args.batch_steps),
-            "pair_kernel": {"ms": pair_ms, "pairs": pairs_timed,
+            "pair_kernel": {"ms": pair_ms, "pairs_reference": pairs_timed,
+                            "pairs_examined": examined,
+                            "pairs_inside_cutoff_estimate": p_in,
                             "pair_evals_per_s": pairs_timed / (pair_ms * 1e-3),
-                            "timing": "CUDA events around the batched work-item pair kernel "
-                                      "alone, median of 7, over the charges of one step"},
-            "fused_replicas": fused,
+                            "examined_per_s": examined / (pair_ms * 1e-3),
+                            "roofline": {"bound": "fp32", "achieved": ach,
+                                         "peak": fp32_peak, "unit": "TFLOP/s",
+                                         "frac": ach / fp32_peak,
+                                         "basis": f"{FLOP_PER_TEST} FLOP per pair examined + "
+                                                  f"{FLOP_PER_CONTRIB} per pair inside the "
+                                                  "cutoff (estimated)"},
+                            "timing": "CUDA events around the batched pair sum alone (culled "
+                                      "replicas' boxes, culls and culled launch, then the "
+                                      "work-item kernel), median of 7, over one step's charges"},
+            "fused_replicas": fused, "culled_replicas": culled,
             "per_phase_only": {"ms_per_step": 1e3 * pp_dt / args.batch_steps,
                                "hops_per_s": pp_hops / pp_dt},
             "build_s": build_s}
@@ -929,7 +963,7 @@ def main():
     props = torch.cuda.get_device_properties(dev)
     sms = props.multi_processor_count
     clk_max = float(peaks.get("sm_max_mhz", 1965.0))
-    fp32_peak = sms * 128 * 2 * clk_max * 1e6 / 1e12          # TFLOP/s, derived
+    fp32_peak = fp32_peak_derived(dev)                         # TFLOP/s, derived
     sfu_peak = sms * 16 * clk_max * 1e6                        # rsqrt/s, derived
     pk = float(np.median(pair_ms))
     p_in = pairs_in_cutoff(w, s_all, s_all[:n], w["terms"], dev)

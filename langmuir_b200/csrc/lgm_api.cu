@@ -227,15 +227,34 @@ __global__ void __launch_bounds__(kScanThreads) bins_scan2(int32_t* __restrict__
     block_exclusive_scan(blockIdx.x == 0 ? tbins : sbins, nb);
 }
 
-// perm[slot] = target: each target takes the next slot of its bin (the order
-// inside a bin does not change a target's sum); stmp likewise for the
-// sources, whose final order prep_sources_sorted fixes.
+// ttmp[slot] = target and stmp[slot] = source: each takes the next slot of
+// its bin, in no particular order inside the bin; rank_targets and
+// prep_sources_sorted fix the final order.
 __global__ void scatter_both(const int32_t* __restrict__ tkey, int t, int32_t* __restrict__ tbins,
-                             int32_t* __restrict__ perm, const int32_t* __restrict__ skey, int n,
+                             int32_t* __restrict__ ttmp, const int32_t* __restrict__ skey, int n,
                              int32_t* __restrict__ sbins, int32_t* __restrict__ stmp) {
     const int g = blockIdx.x * blockDim.x + threadIdx.x;
-    if (g < t) perm[atomicAdd(&tbins[tkey[g]], 1)] = g;
+    if (g < t) ttmp[atomicAdd(&tbins[tkey[g]], 1)] = g;
     if (g < n) stmp[atomicAdd(&sbins[skey[g]], 1)] = g;
+}
+
+// perm[slot] = target in spatial order: the target scattered to slot j goes
+// to its bin's start plus its rank inside the bin by index.  A target's sum
+// is split into the work items of its tile (the culled tiles), so its tile,
+// and with it the rounding of the item partials' sum, must not depend on the
+// scatter's order: with this rank the sums are a function of the target list
+// and the source set.  bins_end[b] is the end of bin b after the scatter.
+__global__ void rank_targets(const int32_t* __restrict__ tkey, const int32_t* __restrict__ ttmp,
+                             const int32_t* __restrict__ bins_end, int t,
+                             int32_t* __restrict__ perm) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= t) return;
+    const int i = ttmp[j];
+    const int b = tkey[i];
+    const int lo = b > 0 ? bins_end[b - 1] : 0, hi = bins_end[b];
+    int rank = 0;
+    for (int k = lo; k < hi; ++k) rank += ttmp[k] < i;
+    perm[lo + rank] = i;
 }
 
 // out[perm[g]] = prefactor * (sum of the item partials of the direct slot -
@@ -404,6 +423,7 @@ lgm_status prep(lgm_ctx* c, unsigned terms, const int32_t* d_src, const int32_t*
     if ((s = grow_device(c, &c->d_tgt, &c->tgt_cap, (size_t)sh.t_phys + 4096)) != LGM_OK) return s;
     if ((s = grow_device(c, &c->d_key, &c->key_cap, (size_t)t)) != LGM_OK) return s;
     if ((s = grow_device(c, &c->d_perm, &c->perm_cap, (size_t)t)) != LGM_OK) return s;
+    if ((s = grow_device(c, &c->d_ttmp, &c->ttmp_cap, (size_t)t)) != LGM_OK) return s;
     if ((s = grow_device(c, &c->d_skey, &c->skey_cap, (size_t)n)) != LGM_OK) return s;
     if ((s = grow_device(c, &c->d_stmp, &c->stmp_cap, (size_t)n)) != LGM_OK) return s;
     // targets and sources in spatial order: bins, scans, scatters
@@ -414,8 +434,9 @@ lgm_status prep(lgm_ctx* c, unsigned terms, const int32_t* d_src, const int32_t*
                                   c->d_cell_rank, c->ncells, c->d_key, c->d_bins, c->d_skey,
                                   c->d_sbins);
     bins_scan2<<<2, kScanThreads, 0, st>>>(c->d_bins, c->d_sbins, c->ncells + 1);
-    scatter_both<<<tb, 256, 0, st>>>(c->d_key, t, c->d_bins, c->d_perm, c->d_skey, n, c->d_sbins,
+    scatter_both<<<tb, 256, 0, st>>>(c->d_key, t, c->d_bins, c->d_ttmp, c->d_skey, n, c->d_sbins,
                                      c->d_stmp);
+    rank_targets<<<(t + 255) / 256, 256, 0, st>>>(c->d_key, c->d_ttmp, c->d_bins, t, c->d_perm);
     LGM_CUDA(c, cudaGetLastError());
     prep_targets<<<(sh.t_pad + 255) / 256, 256, 0, st>>>(d_tgt_site, t, sh.t_pad, all_sites, terms,
                                                           cf.grid_x, cf.grid_y, c->xy, c->volume,
@@ -956,12 +977,13 @@ lgm_status lgm_destroy(lgm_ctx* c) {
     if (!c) return LGM_OK;
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
-    void* dev_ptrs[] = {c->d_geo,  c->d_qq,        c->d_tgt,       c->d_part,      c->d_s,
-                        c->d_q,    c->d_t,         c->d_o,         c->d_gtab,      c->d_rtab,
-                        c->d_err,  c->d_cell_rank, c->d_bins,      c->d_key,       c->d_perm,
-                        c->d_skey, c->d_stmp,      c->d_cbox,      c->d_gbox,      c->d_live,
-                        c->d_items, c->d_tile_first, c->d_tile_items, c->d_item_count,
-                        c->d_examined, c->d_rtab64, c->d_gtab64};
+    void* dev_ptrs[] = {c->d_geo,   c->d_qq,         c->d_tgt,        c->d_part,
+                        c->d_s,     c->d_q,          c->d_t,          c->d_o,
+                        c->d_gtab,  c->d_rtab,       c->d_err,        c->d_cell_rank,
+                        c->d_bins,  c->d_key,        c->d_perm,       c->d_ttmp,
+                        c->d_skey,  c->d_stmp,       c->d_cbox,       c->d_gbox,
+                        c->d_live,  c->d_items,      c->d_tile_first, c->d_tile_items,
+                        c->d_item_count, c->d_examined, c->d_rtab64,  c->d_gtab64};
     for (void* p : dev_ptrs)
         if (p) cudaFree(p);
     void* host_ptrs[] = {c->h_s, c->h_q, c->h_t, c->h_o, c->h_err};

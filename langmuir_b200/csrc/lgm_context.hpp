@@ -40,6 +40,7 @@ struct lgm_ctx {
     int32_t* d_bins = nullptr;                       // [ncells + 2] counts, then offsets
     int32_t* d_key = nullptr;  size_t key_cap = 0;   // bin per target
     int32_t* d_perm = nullptr; size_t perm_cap = 0;  // target of each physical slot
+    int32_t* d_ttmp = nullptr; size_t ttmp_cap = 0;  // targets scattered by bin
     // The sources in the same spatial order: bin per source (d_sbins follows
     // the target bins in the d_bins allocation), the sources scattered by bin,
     // then ranked inside their bin by (site, index), so that the order is a

@@ -117,13 +117,15 @@ struct Dev {
     int32_t* bins;             // [ncells + 2]
     int32_t *tkey, *tperm;     // [2 ncap]
     int splits;
-    // Culled pair sums (standalone replicas, lgm_cull.cuh): the sources
-    // sorted by (charge class, lattice cell) and by site inside a bin (skey:
-    // bin per source, stmp: sources scattered by bin, sbins: 3 (ncells + 1)
-    // bin counters), chunk and group boxes, each tile's live chunks and the
-    // work items.  A charge class stays padded to whole chunks.
+    // Culled pair sums (lgm_cull.cuh; standalone replicas and a batch's
+    // per-phase replicas of point charges): the sources sorted by (charge
+    // class, lattice cell) and by site inside a bin (skey: bin per source,
+    // stmp: sources scattered by bin, sbins: 3 (ncells + 1) bin counters), the
+    // targets scattered by bin before their rank inside it (ttmp, [2 ncap]),
+    // chunk and group boxes, each tile's live chunks and the work items.  A
+    // charge class stays padded to whole chunks.
     int culled, max_items;
-    int32_t *skey, *stmp, *sbins;
+    int32_t *skey, *stmp, *sbins, *ttmp;
     Box *cbox, *gbox;
     int32_t* live;
     int4* items;
@@ -413,9 +415,23 @@ __device__ __forceinline__ void tbins_body(const Dev& D, const int g) {
 }
 __device__ __forceinline__ void tscatter_body(const Dev& D, const int g) {
     const int ne = D.cnt[I_NE], nh = D.cnt[I_NH];
-    if (g < 2 * (ne + nh)) D.tperm[atomicAdd(&D.bins[D.tkey[g]], 1)] = g;
+    if (g < 2 * (ne + nh)) (D.culled ? D.ttmp : D.tperm)[atomicAdd(&D.bins[D.tkey[g]], 1)] = g;
     if (D.culled && g < ne + nh + (D.dq != 0 ? D.nd : 0))
         D.stmp[atomicAdd(&D.sbins[D.skey[g]], 1)] = g;
+}
+// Culled replicas: the target scattered to slot j goes to its bin's start
+// plus its rank inside the bin by index.  A target's sum is split into the
+// work items of its tile, so its tile -- and the rounding of the item
+// partials' sum -- must not depend on the scatter's order.  D.bins holds the
+// bin ends after the scatter.
+__device__ __forceinline__ void trank_body(const Dev& D, const int j) {
+    if (!D.culled || j >= 2 * (D.cnt[I_NE] + D.cnt[I_NH])) return;
+    const int i = D.ttmp[j];
+    const int b = D.tkey[i];
+    const int lo = b > 0 ? D.bins[b - 1] : 0, hi = D.bins[b];
+    int rank = 0;
+    for (int k = lo; k < hi; ++k) rank += D.ttmp[k] < i;
+    D.tperm[lo + rank] = i;
 }
 
 // ChargeAgent::bindingPotential (chargeagent.cpp:463-481)
@@ -954,6 +970,7 @@ __global__ void __launch_bounds__(CH) k_chunk_boxes(Dev D) {
 }
 __global__ void __launch_bounds__(kCullThreads) k_cull(Dev D) { cull_body(cull_args(D), (int)blockIdx.x); }
 __global__ void k_tscatter(Dev D) { tscatter_body(D, LGM_THREAD_INDEX); }
+__global__ void k_trank(Dev D) { trank_body(D, LGM_THREAD_INDEX); }
 __global__ void __launch_bounds__(kGuardThreads) k_guard(Dev D) {
     __shared__ double2 red[32];
     guard_body(D, blockIdx.x, gridDim.x, red);
@@ -991,6 +1008,7 @@ __global__ void kb_decide(const Dev* R, const int4* map) { LGM_BATCH_LOOP(decide
 __global__ void kb_tbins_zero(const Dev* R, const int4* map) { LGM_BATCH_LOOP(tbins_zero_body(D, i)) }
 __global__ void kb_tbins(const Dev* R, const int4* map) { LGM_BATCH_LOOP(tbins_body(D, i)) }
 __global__ void kb_tscatter(const Dev* R, const int4* map) { LGM_BATCH_LOOP(tscatter_body(D, i)) }
+__global__ void kb_trank(const Dev* R, const int4* map) { LGM_BATCH_LOOP(trank_body(D, i)) }
 // one block per replica of the list; a second row scans culled replicas' source bins
 __global__ void __launch_bounds__(1024) kb_tbins_scan(const Dev* R, const int* list) {
     const Dev& D = R[list[blockIdx.x]];
@@ -1558,6 +1576,7 @@ lgm_status enqueue_step(lgm_kmc* k) {
             k_tbins<<<(nb + blk - 1) / blk, blk, 0, st>>>(D);
             k_tbins_scan<<<D.culled ? 2 : 1, 1024, 0, st>>>(D);
             k_tscatter<<<(nb + blk - 1) / blk, blk, 0, st>>>(D);
+            if (D.culled) k_trank<<<(2 * nc + blk - 1) / blk, blk, 0, st>>>(D);
         }
         const int npack = std::max(D.src_cap, D.tpad_cap);
         k_pack<<<(npack + blk - 1) / blk, blk, 0, st>>>(D);
@@ -1772,6 +1791,7 @@ static lgm_status kmc_create_impl(const lgm_params* pin, int32_t device, uint32_
     DA(D.part, part_n); DA(D.part_norm, part_n);
     if (k->cull_ok) {
         DA(D.skey, D.cap_e + D.cap_h + nd_src); DA(D.stmp, D.cap_e + D.cap_h + nd_src);
+        DA(D.ttmp, 2 * ncap);
         DA(D.cbox, src_chunks); DA(D.gbox, (size_t)src_chunks * kGroupsPerChunk);
         DA(D.live, (size_t)k->cull_tiles * src_chunks);
         DA(D.items, (size_t)k->cull_tiles * D.max_items);
@@ -2262,6 +2282,7 @@ void enqueue_batch_sort(lgm_kmc_batch* b, cudaStream_t st) {
     kb_tbins_scan<<<dim3((unsigned)b->classic.size(), b->culled.empty() ? 1u : 2u), 1024, 0, st>>>(
         b->d_reps, b->d_classic);
     kb_tscatter<<<b->nb_fin, 256, 0, st>>>(b->d_reps, b->map_fin);
+    if (!b->culled.empty()) kb_trank<<<b->nb_fin, 256, 0, st>>>(b->d_reps, b->map_fin);
 }
 
 lgm_status enqueue_batch_step(lgm_kmc_batch* b) {
