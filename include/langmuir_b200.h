@@ -257,7 +257,17 @@ lgm_status lgm_variant_info(int32_t variant, int32_t* threads, int32_t* target_p
  * all have r >= cutoff, so the sums are those of the full tile over the same
  * source order. */
 #define LGM_VARIANT_CULLED 2
+/* LGM_VARIANT_WARP_SPECIALISED (with LGM_VARIANT_CULLED): one producer warp
+ * per CTA streams the chunks through a ring of stages and the CTAs take work
+ * items from a shared counter; the target warps do not wait for one another.
+ * The sums equal those of the other culled variants bit for bit.  `threads`
+ * of lgm_variant_info counts the target warps' threads only. */
+#define LGM_VARIANT_WARP_SPECIALISED 4
 lgm_status lgm_variant_flags(int32_t variant, int32_t* flags);
+/* Culled variants: source chunks per work item (at least; more when a
+ * tile's live chunks exceed 32 items) and, warp-specialised, the stages of
+ * the copy ring (0 otherwise); both 0 for the other variants. */
+lgm_status lgm_variant_items(int32_t variant, int32_t* chunks_per_item, int32_t* stages);
 
 #ifdef __cplusplus
 }

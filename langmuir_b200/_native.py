@@ -121,6 +121,8 @@ SIGNATURES = {
                                                      ctypes.c_int32, _vp, _vp]),
     "lgm_variant_count": (ctypes.c_int32, []),
     "lgm_variant_flags": (ctypes.c_int32, [ctypes.c_int32, ctypes.POINTER(ctypes.c_int32)]),
+    "lgm_variant_items": (ctypes.c_int32, [ctypes.c_int32, ctypes.POINTER(ctypes.c_int32),
+                                           ctypes.POINTER(ctypes.c_int32)]),
     "lgm_variant_info": (ctypes.c_int32, [ctypes.c_int32, ctypes.POINTER(ctypes.c_int32),
                                           ctypes.POINTER(ctypes.c_int32),
                                           ctypes.POINTER(ctypes.c_int32)]),

@@ -118,8 +118,12 @@ class Coulomb:
             N.lib().lgm_variant_info(v, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c))
             f = ctypes.c_int32()
             N.lib().lgm_variant_flags(v, ctypes.byref(f))
+            k, st = ctypes.c_int32(), ctypes.c_int32()
+            N.lib().lgm_variant_items(v, ctypes.byref(k), ctypes.byref(st))
             out.append({"threads": a.value, "target_pairs": b.value, "run": c.value,
-                        "warp_skip": bool(f.value & 1), "culled": bool(f.value & 2)})
+                        "warp_skip": bool(f.value & 1), "culled": bool(f.value & 2),
+                        "warp_specialised": bool(f.value & 4), "chunks_per_item": k.value,
+                        "stages": st.value})
         return out
 
     def set_timing(self, on: bool = True):

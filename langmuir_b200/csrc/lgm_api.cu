@@ -340,6 +340,7 @@ struct Variant {
     int nt, rp, sub, skip, cull, per_item;
     PairFn fn[4];
     CulledFn cfn[4];  // [3]: the FP64-table path (culled variants only)
+    int ws = 0;       // warp-specialised culled kernel: its stages (0: not)
 };
 #define LGM_VARIANT_S(NT, RP, SUB, SK)                                                    \
     Variant {                                                                             \
@@ -360,6 +361,15 @@ struct Variant {
                 &pair_kernel_culled<0, 1, NT, RP, SUB>, &pair_kernel_culled<0, 2, NT, RP, SUB> \
         }                                                                                     \
     }
+#define LGM_VARIANT_CULL_WS(NW, RP, SUB, K, S, MINB)                                        \
+    Variant {                                                                                 \
+        NW * 32, RP, SUB, 1, 1, K, {nullptr, nullptr, nullptr, nullptr},                      \
+            {&pair_kernel_culled_ws<0, 0, NW, RP, SUB, S, MINB>,                              \
+             &pair_kernel_culled_ws<1, 0, NW, RP, SUB, S, MINB>,                              \
+             &pair_kernel_culled_ws<0, 1, NW, RP, SUB, S, MINB>,                              \
+             &pair_kernel_culled_ws<0, 2, NW, RP, SUB, S, MINB>},                             \
+            S                                                                                 \
+    }
 const Variant kVariants[] = {
     LGM_VARIANT(128, 4, 16),       LGM_VARIANT(128, 4, 8),        LGM_VARIANT(128, 2, 16),
     LGM_VARIANT(128, 8, 16),       LGM_VARIANT(256, 4, 16),       LGM_VARIANT(64, 4, 16),
@@ -370,6 +380,11 @@ const Variant kVariants[] = {
     LGM_VARIANT_CULL(128, 4, 32, 4), LGM_VARIANT_CULL(128, 2, 32, 2),
     LGM_VARIANT_CULL(64, 4, 32, 2),  LGM_VARIANT_CULL(128, 4, 16, 2),
     LGM_VARIANT_CULL(64, 2, 32, 2),
+    // warp-specialised: (target warps, target pairs, run, chunks per item,
+    // stages, CTAs per SM); the register bound counts the producer warp
+    LGM_VARIANT_CULL_WS(4, 4, 32, 2, 4, 4), LGM_VARIANT_CULL_WS(8, 2, 32, 2, 4, 3),
+    LGM_VARIANT_CULL_WS(4, 2, 32, 2, 4, 5), LGM_VARIANT_CULL_WS(3, 4, 32, 2, 4, 5),
+    LGM_VARIANT_CULL_WS(7, 2, 32, 2, 4, 3), LGM_VARIANT_CULL_WS(4, 4, 32, 4, 4, 4),
 };
 constexpr int kNumVariants = (int)(sizeof(kVariants) / sizeof(kVariants[0]));
 static_assert(kNumVariants <= (int)(sizeof(lgm_ctx::bps) / sizeof(lgm_ctx::bps[0])),
@@ -379,6 +394,14 @@ constexpr int kDefaultVariant = 14;  // culled, 128 threads, 4 target pairs, run
 const void* kernel_of(const Variant& V, int fi) {
     return V.cull ? reinterpret_cast<const void*>(V.cfn[fi])
                   : reinterpret_cast<const void*>(V.fn[fi]);
+}
+
+// Threads of a CTA (a warp-specialised variant adds its producer warp) and
+// dynamic shared memory for path index fi with table entries 0 .. tab_k.
+int variant_threads(const Variant& V) { return V.nt + (V.ws ? 32 : 0); }
+size_t variant_smem(const Variant& V, int fi, int tab_k) {
+    if (V.ws) return ws_smem_bytes(V.ws, tab_k, fi == 3 ? 8 : 4);
+    return fi == 3 ? pair_smem_bytes64(tab_k) : pair_smem_bytes(tab_k);
 }
 
 int fn_index(int kind, int path) {
@@ -503,6 +526,7 @@ lgm_status launch_culled(lgm_ctx* c, int kind, int v, const Shape& sh, const Pai
     C.live_stride = sh.n_chunks;
     C.items = c->d_items;
     C.item_count = c->d_item_count;
+    C.work = c->d_item_count + 1;
     C.tile_first = c->d_tile_first;
     C.tile_items = c->d_tile_items;
     if (c->counting) {
@@ -515,11 +539,10 @@ lgm_status launch_culled(lgm_ctx* c, int kind, int v, const Shape& sh, const Pai
     // timing on: the events bracket the pair kernel alone (recorded again here)
     if (c->timing) LGM_CUDA(c, cudaEventRecord(c->ev_pair0, st));
     const int grid = c->sm_count * std::max(1, c->bps[v][fi]);
-    const size_t smem = fi == 3 ? pair_smem_bytes64(P.tab_k) : pair_smem_bytes(P.tab_k);
-    V.cfn[fi]<<<grid, V.nt, smem, st>>>(P, C);
+    V.cfn[fi]<<<grid, variant_threads(V), variant_smem(V, fi, P.tab_k), st>>>(P, C);
     LGM_CUDA(c, cudaGetLastError());
     c->last.ctas = grid;
-    c->last.threads = V.nt;
+    c->last.threads = variant_threads(V);
     c->last.targets_per_thread = 2 * V.rp;
     c->last.variant = v;
     c->last.splits = 0;
@@ -929,7 +952,7 @@ lgm_status lgm_create(const lgm_config* cfg, int32_t device, lgm_ctx** out) {
         c->bins_stride = (c->ncells + 2 + 3) / 4 * 4;
         if ((e = cudaMalloc(&c->d_cell_rank, sizeof(int32_t) * rank.size())) != cudaSuccess ||
             (e = cudaMalloc(&c->d_bins, sizeof(int32_t) * 2 * c->bins_stride)) != cudaSuccess ||
-            (e = cudaMalloc(&c->d_item_count, sizeof(int32_t))) != cudaSuccess)
+            (e = cudaMalloc(&c->d_item_count, 2 * sizeof(int32_t))) != cudaSuccess)
             return bail("cudaMalloc", e);
         // the source bins follow the target bins, 16-byte aligned (the scan reads int4)
         c->d_sbins = c->d_bins + c->bins_stride;
@@ -941,16 +964,14 @@ lgm_status lgm_create(const lgm_config* cfg, int32_t device, lgm_ctx** out) {
     // resident CTAs per SM of every variant (the split count fills
     // kSplitWaves waves of them).
     {
-        const size_t smem_tab[4] = {pair_smem_bytes(0), pair_smem_bytes(c->gtab_k),
-                                    pair_smem_bytes(std::max(c->rtab_k, c->gtab_k)),
-                                    pair_smem_bytes64(c->rtab_k)};
+        const int tab_of[4] = {0, c->gtab_k, std::max(c->rtab_k, c->gtab_k), c->rtab_k};
         for (int v = 0; v < kNumVariants; ++v)
             for (int fi = 0; fi < 4; ++fi) {
                 if (!kernel_of(kVariants[v], fi)) continue;
                 // the table kernels serve only their own path
                 if (fi == 2 && cf.path != LGM_PATH_TABLE) continue;
                 if (fi == 3 && cf.path != LGM_PATH_TABLE64) continue;
-                const size_t smem = smem_tab[fi];
+                const size_t smem = variant_smem(kVariants[v], fi, tab_of[fi]);
                 if (smem > 48 * 1024) {
                     if (smem > (size_t)prop.sharedMemPerBlockOptin) {
                         g_create_error = "cutoff too large for the shared-memory tables";
@@ -964,7 +985,8 @@ lgm_status lgm_create(const lgm_config* cfg, int32_t device, lgm_ctx** out) {
                 }
                 int bps = 0;
                 if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-                         &bps, kernel_of(kVariants[v], fi), kVariants[v].nt, smem)) != cudaSuccess)
+                         &bps, kernel_of(kVariants[v], fi), variant_threads(kVariants[v]),
+                         smem)) != cudaSuccess)
                     return bail("cudaOccupancyMaxActiveBlocksPerMultiprocessor", e);
                 c->bps[v][fi] = bps;
             }
@@ -1055,7 +1077,15 @@ lgm_status lgm_variant_info(int32_t v, int32_t* threads, int32_t* target_pairs, 
 lgm_status lgm_variant_flags(int32_t v, int32_t* flags) {
     if (v < 0 || v >= kNumVariants || !flags) return LGM_ERR_INVALID_ARGUMENT;
     *flags = (kVariants[v].skip ? LGM_VARIANT_WARP_SKIP : 0) |
-             (kVariants[v].cull ? LGM_VARIANT_CULLED : 0);
+             (kVariants[v].cull ? LGM_VARIANT_CULLED : 0) |
+             (kVariants[v].ws ? LGM_VARIANT_WARP_SPECIALISED : 0);
+    return LGM_OK;
+}
+
+lgm_status lgm_variant_items(int32_t v, int32_t* chunks_per_item, int32_t* stages) {
+    if (v < 0 || v >= kNumVariants) return LGM_ERR_INVALID_ARGUMENT;
+    if (chunks_per_item) *chunks_per_item = kVariants[v].cull ? kVariants[v].per_item : 0;
+    if (stages) *stages = kVariants[v].ws;
     return LGM_OK;
 }
 

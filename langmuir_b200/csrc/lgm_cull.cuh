@@ -100,6 +100,8 @@ struct CullArgs {
     int live_stride = 0;
     int4* items = nullptr;            // {tile, first live index, chunk count, 0}
     int* item_count = nullptr;        // items written (zeroed by chunk_boxes block 0)
+    int* work = nullptr;              // next item to take, warp-specialised kernel (zeroed
+                                      // by chunk_boxes block 0; may be null otherwise)
     int* tile_first = nullptr;        // [tiles] first item of the tile
     int* tile_items = nullptr;        // [tiles] items of the tile
     // Optional (null: off): pairs whose r^2 the pair kernel computed, i.e.
@@ -114,7 +116,10 @@ __device__ __forceinline__ void chunk_boxes_body(const PairArgs& A, const CullAr
                                                  const int chunk) {
     __shared__ Box s_g[kGroupsPerChunk];
     const int n_chunks = A.dyn ? A.dyn[0] : A.n_chunks;
-    if (chunk == 0 && threadIdx.x == 0 && C.item_count) *C.item_count = 0;
+    if (chunk == 0 && threadIdx.x == 0) {
+        if (C.item_count) *C.item_count = 0;
+        if (C.work) *C.work = 0;
+    }
     if (chunk >= n_chunks) return;
     const int j = chunk * CH + (int)threadIdx.x;
     const float4 g0 = A.geo[2 * j], g1 = A.geo[2 * j + 1];
@@ -232,6 +237,7 @@ struct OneProblem {
     __device__ __forceinline__ const PairArgs& A(int) const { return a; }
     __device__ __forceinline__ const CullArgs& C(int) const { return c; }
     __device__ __forceinline__ const PairArgs& first() const { return a; }
+    __device__ __forceinline__ int* work() const { return c.work; }
 };
 // The culled replicas list[0 .. n-1] of a batch, their arguments pa[r] and
 // ca[r], and offs[i] the number of items of list[0 .. i-1] (offs[n] = all).
@@ -239,7 +245,7 @@ struct ProblemList {
     const PairArgs* pa;
     const CullArgs* ca;
     const int* list;
-    const int* offs;
+    const int* offs;   // [n + 2]: offs[n + 1] is the next item to take (zeroed with offs)
     int n;
     __device__ __forceinline__ int count() const { return n > 0 ? offs[n] : 0; }
     __device__ __forceinline__ void resolve(int g, int& prob, int& local) const {
@@ -255,7 +261,135 @@ struct ProblemList {
     __device__ __forceinline__ const PairArgs& A(int p) const { return pa[p]; }
     __device__ __forceinline__ const CullArgs& C(int p) const { return ca[p]; }
     __device__ __forceinline__ const PairArgs& first() const { return pa[list[0]]; }
+    __device__ __forceinline__ int* work() const { return const_cast<int*>(offs) + n + 1; }
 };
+
+// The pairs of one staged chunk for one warp: the sources of its live groups
+// (bit g of gmask: group g), in FP32 runs of SUB sources folded into acc64
+// (PATH 0, 1), or term by term in FP64 (PATH 2).  sg/sq: the stage's source
+// records; tx..tt: the warp's target pairs; nrm: the runs' |sums| (NORM).
+template <int KIND, int PATH, int RP, int SUB, bool NORM>
+__device__ __forceinline__ void chunk_pairs(const float4* __restrict__ sg,
+                                            const float2* __restrict__ sq, const unsigned gmask,
+                                            const float2 (&tx)[RP], const float2 (&ty)[RP],
+                                            const float2 (&tz)[RP], const float2 (&tt)[RP],
+                                            double (&acc64)[2 * RP],
+                                            float (&nrm)[NORM ? 2 * RP : 1], const unsigned ulim,
+                                            const int tab_k, const float* s_tab,
+                                            const double* s_tab64) {
+    const float2 half2 = f2(0.5f, 0.5f);
+#pragma unroll 1
+    for (int j0 = 0; j0 < CH; j0 += SUB) {
+        if (!((gmask >> (j0 / kGroup)) & 1u)) continue;  // warp-uniform
+        float acc[2 * RP];
+#pragma unroll
+        for (int k = 0; k < 2 * RP; ++k) acc[k] = 0.f;
+        constexpr int kUnrollJ = PATH != 1 ? 4 : SUB;
+#pragma unroll kUnrollJ
+        for (int jj = 0; jj < SUB; ++jj) {
+            const int j = j0 + jj;
+            const float4 g0 = sg[2 * j];
+            const float4 g1 = sg[2 * j + 1];
+            const float2 av = f2(g0.x, g0.y), bv = f2(g0.z, g0.w);
+            const float2 cv = f2(g1.x, g1.y), dv = f2(g1.z, g1.w);
+            if constexpr (PATH == 2) {
+                // r^2 - 1/2 exactly, the warp vote, then w(r^2) from the
+                // FP64 table: r^2 = u + 1/2 and r^2 + 2^23 are exact in
+                // FP32 (r^2 < 2^22), and the latter holds r^2 in its low
+                // 23 mantissa bits; entries 0 and past the cutoff are 0,
+                // so the clamped index also applies the cutoff and the
+                // r = 0 skip
+                float2 uu[RP];
+                unsigned mk[RP];
+#pragma unroll
+                for (int k = 0; k < RP; ++k) {
+                    const float2 pa = __ffma2_rn(tx[k], av, tt[k]);
+                    const float2 pc = __ffma2_rn(tz[k], cv, dv);
+                    uu[k] = __fadd2_rn(__ffma2_rn(ty[k], bv, pa), pc);
+                    mk[k] = min(__float_as_uint(uu[k].x), __float_as_uint(uu[k].y));
+                }
+#pragma unroll
+                for (int w = 1; w < RP; w *= 2)
+#pragma unroll
+                    for (int k = 0; k + w < RP; k += 2 * w) mk[k] = min(mk[k], mk[k + w]);
+                if (__any_sync(0xffffffffu, mk[0] < ulim)) {
+                    const double qd = (double)sq[j].x;
+                    const float2 two23 = f2(8388608.f, 8388608.f);
+#pragma unroll
+                    for (int k = 0; k < RP; ++k) {
+                        const float2 m2 = __fadd2_rn(__fadd2_rn(uu[k], half2), two23);
+                        const int ix = min(__float_as_int(m2.x) & 0x7fffff, tab_k);
+                        const int iy = min(__float_as_int(m2.y) & 0x7fffff, tab_k);
+                        acc64[2 * k] = fma(qd, s_tab64[ix], acc64[2 * k]);
+                        acc64[2 * k + 1] = fma(qd, s_tab64[iy], acc64[2 * k + 1]);
+                    }
+                }
+            } else if constexpr (PATH == 0) {
+                // r^2 - 1/2 in three exact steps and the warp vote, as
+                // the SKIP tile of lgm_pairs.cuh
+                float2 uu[RP];
+                unsigned mk[RP];
+#pragma unroll
+                for (int k = 0; k < RP; ++k) {
+                    const float2 pa = __ffma2_rn(tx[k], av, tt[k]);
+                    const float2 pc = __ffma2_rn(tz[k], cv, dv);
+                    uu[k] = __fadd2_rn(__ffma2_rn(ty[k], bv, pa), pc);
+                    mk[k] = min(__float_as_uint(uu[k].x), __float_as_uint(uu[k].y));
+                }
+#pragma unroll
+                for (int w = 1; w < RP; w *= 2)
+#pragma unroll
+                    for (int k = 0; k + w < RP; k += 2 * w) mk[k] = min(mk[k], mk[k + w]);
+                if (__any_sync(0xffffffffu, mk[0] < ulim)) {
+                    const float qs = sq[j].x;
+#pragma unroll
+                    for (int k = 0; k < RP; ++k) {
+                        const float2 r2 = __fadd2_rn(uu[k], half2);
+                        float wx = rsqrt_mufu(r2.x);
+                        float wy = rsqrt_mufu(r2.y);
+                        if (KIND == 1) {
+                            const int ix =
+                                min(__float_as_int(r2.x + 8388608.f) & 0x7fffff, tab_k);
+                            const int iy =
+                                min(__float_as_int(r2.y + 8388608.f) & 0x7fffff, tab_k);
+                            wx = fminf(s_tab[ix], wx);
+                            wy = fminf(s_tab[iy], wy);
+                        }
+                        fma_if_below(acc[2 * k], qs, wx, __float_as_uint(uu[k].x), ulim);
+                        fma_if_below(acc[2 * k + 1], qs, wy, __float_as_uint(uu[k].y),
+                                     ulim);
+                    }
+                }
+            } else {
+                const float qs = sq[j].x;
+#pragma unroll
+                for (int k = 0; k < RP; ++k) {
+                    float2 u = __fadd2_rn(dv, tt[k]);
+                    u = __ffma2_rn(tx[k], av, u);
+                    u = __ffma2_rn(ty[k], bv, u);
+                    u = __ffma2_rn(tz[k], cv, u);  // r^2 - 1/2, exact
+                    const float2 r2 = __fadd2_rn(u, half2);
+                    // w(k) from the table; entries 0 and c^2 are 0
+                    const int ix =
+                        min(__float_as_int(r2.x + 8388608.f) & 0x7fffff, tab_k);
+                    const int iy =
+                        min(__float_as_int(r2.y + 8388608.f) & 0x7fffff, tab_k);
+                    fma_if_below(acc[2 * k], qs, s_tab[ix], __float_as_uint(u.x), ulim);
+                    fma_if_below(acc[2 * k + 1], qs, s_tab[iy], __float_as_uint(u.y),
+                                 ulim);
+                }
+            }
+        }
+        if constexpr (PATH != 2) {  // PATH 2 adds every term in FP64 already
+#pragma unroll
+            for (int k = 0; k < 2 * RP; ++k) acc64[k] += (double)acc[k];
+        }
+        if (NORM) {
+#pragma unroll
+            for (int k = 0; k < 2 * RP; ++k) nrm[NORM ? k : 0] += fabsf(acc[k]);
+        }
+    }
+}
 
 template <int KIND, int PATH, int NT, int RP, int SUB, bool NORM, class PS>
 __device__ __forceinline__ void pair_items_culled(const PS& P) {
@@ -329,7 +463,6 @@ __device__ __forceinline__ void pair_items_culled(const PS& P) {
         issue_next();
     }
 
-    const float2 half2 = f2(0.5f, 0.5f);
     uint32_t consumed = 0;
     bool failed = false;
 
@@ -382,119 +515,9 @@ __device__ __forceinline__ void pair_items_culled(const PS& P) {
             const unsigned gmask = __ballot_sync(0xffffffffu, gon);
             if (C.examined && lane == 0 && gmask)
                 atomicAdd(C.examined, (unsigned long long)__popc(gmask) * kGroup * 64 * RP);
-            const float4* sg = s_geo + st * CH * 2;
-            const float2* sq = s_qq + st * CH;
-#pragma unroll 1
-            for (int j0 = 0; j0 < CH; j0 += SUB) {
-                if (!((gmask >> (j0 / kGroup)) & 1u)) continue;  // warp-uniform
-                float acc[2 * RP];
-#pragma unroll
-                for (int k = 0; k < 2 * RP; ++k) acc[k] = 0.f;
-                constexpr int kUnrollJ = PATH != 1 ? 4 : SUB;
-#pragma unroll kUnrollJ
-                for (int jj = 0; jj < SUB; ++jj) {
-                    const int j = j0 + jj;
-                    const float4 g0 = sg[2 * j];
-                    const float4 g1 = sg[2 * j + 1];
-                    const float2 av = f2(g0.x, g0.y), bv = f2(g0.z, g0.w);
-                    const float2 cv = f2(g1.x, g1.y), dv = f2(g1.z, g1.w);
-                    if constexpr (PATH == 2) {
-                        // r^2 - 1/2 exactly, the warp vote, then w(r^2) from the
-                        // FP64 table: r^2 = u + 1/2 and r^2 + 2^23 are exact in
-                        // FP32 (r^2 < 2^22), and the latter holds r^2 in its low
-                        // 23 mantissa bits; entries 0 and past the cutoff are 0,
-                        // so the clamped index also applies the cutoff and the
-                        // r = 0 skip
-                        float2 uu[RP];
-                        unsigned mk[RP];
-#pragma unroll
-                        for (int k = 0; k < RP; ++k) {
-                            const float2 pa = __ffma2_rn(tx[k], av, tt[k]);
-                            const float2 pc = __ffma2_rn(tz[k], cv, dv);
-                            uu[k] = __fadd2_rn(__ffma2_rn(ty[k], bv, pa), pc);
-                            mk[k] = min(__float_as_uint(uu[k].x), __float_as_uint(uu[k].y));
-                        }
-#pragma unroll
-                        for (int w = 1; w < RP; w *= 2)
-#pragma unroll
-                            for (int k = 0; k + w < RP; k += 2 * w) mk[k] = min(mk[k], mk[k + w]);
-                        if (__any_sync(0xffffffffu, mk[0] < ulim)) {
-                            const double qd = (double)sq[j].x;
-                            const float2 two23 = f2(8388608.f, 8388608.f);
-#pragma unroll
-                            for (int k = 0; k < RP; ++k) {
-                                const float2 m2 = __fadd2_rn(__fadd2_rn(uu[k], half2), two23);
-                                const int ix = min(__float_as_int(m2.x) & 0x7fffff, A.tab_k);
-                                const int iy = min(__float_as_int(m2.y) & 0x7fffff, A.tab_k);
-                                acc64[2 * k] = fma(qd, s_tab64[ix], acc64[2 * k]);
-                                acc64[2 * k + 1] = fma(qd, s_tab64[iy], acc64[2 * k + 1]);
-                            }
-                        }
-                    } else if constexpr (PATH == 0) {
-                        // r^2 - 1/2 in three exact steps and the warp vote, as
-                        // the SKIP tile of lgm_pairs.cuh
-                        float2 uu[RP];
-                        unsigned mk[RP];
-#pragma unroll
-                        for (int k = 0; k < RP; ++k) {
-                            const float2 pa = __ffma2_rn(tx[k], av, tt[k]);
-                            const float2 pc = __ffma2_rn(tz[k], cv, dv);
-                            uu[k] = __fadd2_rn(__ffma2_rn(ty[k], bv, pa), pc);
-                            mk[k] = min(__float_as_uint(uu[k].x), __float_as_uint(uu[k].y));
-                        }
-#pragma unroll
-                        for (int w = 1; w < RP; w *= 2)
-#pragma unroll
-                            for (int k = 0; k + w < RP; k += 2 * w) mk[k] = min(mk[k], mk[k + w]);
-                        if (__any_sync(0xffffffffu, mk[0] < ulim)) {
-                            const float qs = sq[j].x;
-#pragma unroll
-                            for (int k = 0; k < RP; ++k) {
-                                const float2 r2 = __fadd2_rn(uu[k], half2);
-                                float wx = rsqrt_mufu(r2.x);
-                                float wy = rsqrt_mufu(r2.y);
-                                if (KIND == 1) {
-                                    const int ix =
-                                        min(__float_as_int(r2.x + 8388608.f) & 0x7fffff, A.tab_k);
-                                    const int iy =
-                                        min(__float_as_int(r2.y + 8388608.f) & 0x7fffff, A.tab_k);
-                                    wx = fminf(s_tab[ix], wx);
-                                    wy = fminf(s_tab[iy], wy);
-                                }
-                                fma_if_below(acc[2 * k], qs, wx, __float_as_uint(uu[k].x), ulim);
-                                fma_if_below(acc[2 * k + 1], qs, wy, __float_as_uint(uu[k].y),
-                                             ulim);
-                            }
-                        }
-                    } else {
-                        const float qs = sq[j].x;
-#pragma unroll
-                        for (int k = 0; k < RP; ++k) {
-                            float2 u = __fadd2_rn(dv, tt[k]);
-                            u = __ffma2_rn(tx[k], av, u);
-                            u = __ffma2_rn(ty[k], bv, u);
-                            u = __ffma2_rn(tz[k], cv, u);  // r^2 - 1/2, exact
-                            const float2 r2 = __fadd2_rn(u, half2);
-                            // w(k) from the table; entries 0 and c^2 are 0
-                            const int ix =
-                                min(__float_as_int(r2.x + 8388608.f) & 0x7fffff, A.tab_k);
-                            const int iy =
-                                min(__float_as_int(r2.y + 8388608.f) & 0x7fffff, A.tab_k);
-                            fma_if_below(acc[2 * k], qs, s_tab[ix], __float_as_uint(u.x), ulim);
-                            fma_if_below(acc[2 * k + 1], qs, s_tab[iy], __float_as_uint(u.y),
-                                         ulim);
-                        }
-                    }
-                }
-                if constexpr (PATH != 2) {  // PATH 2 adds every term in FP64 already
-#pragma unroll
-                    for (int k = 0; k < 2 * RP; ++k) acc64[k] += (double)acc[k];
-                }
-                if (NORM) {
-#pragma unroll
-                    for (int k = 0; k < 2 * RP; ++k) nrm[NORM ? k : 0] += fabsf(acc[k]);
-                }
-            }
+            chunk_pairs<KIND, PATH, RP, SUB, NORM>(s_geo + st * CH * 2, s_qq + st * CH, gmask, tx, ty,
+                                                   tz, tt, acc64, nrm, ulim, A.tab_k, s_tab,
+                                                   s_tab64);
             __syncthreads();  // every thread is done with stage st
             ++consumed;
             if (tid == 0) {
@@ -521,6 +544,183 @@ __device__ __forceinline__ void pair_items_culled(const PS& P) {
     }
 }
 
+// Dynamic shared memory of the warp-specialised kernel: S stages of source
+// records and group boxes, their item records and full/empty barriers, then
+// the table (elem bytes per entry; tab_k = 0 and elem = 0: none).
+__host__ __device__ constexpr size_t ws_stage_bytes() {
+    return pair_stage_bytes() + kGroupsPerChunk * sizeof(Box) + sizeof(int4) + 2 * sizeof(uint64_t);
+}
+inline size_t ws_smem_bytes(int S, int tab_k, int elem) {
+    return (size_t)S * ws_stage_bytes() + (size_t)(tab_k + 1) * elem + 16;
+}
+
+// The pair sum over the work items, warp-specialised.  NW consumer warps own
+// the tile's targets as in pair_items_culled (TS = NW * 64 RP); one producer
+// warp (its lane 0) takes items from an atomic counter -- whichever CTA is
+// free takes the next item -- and streams their chunks through an S-stage
+// ring: stage records {local item, chunk position, chunks, problem}, full
+// barriers (the bulk copies) and empty barriers (one arrival per consumer
+// warp).  Consumer warps never wait for one another: a warp whose groups are
+// all beyond the cutoff of its targets passes a chunk at once, and may run up
+// to S chunks ahead of the slowest warp.  After the last item the producer
+// posts a record with item -1 (no copy) that ends the consumers.  Every wait
+// is bounded: on a timeout the warp raises DEVERR_TIMEOUT and leaves, the
+// producer's own waits then run out, and it waits (bounded) for the copies it
+// has in flight before leaving.  Per target, chunks and FP32 runs are added
+// in the order of pair_items_culled: the sums are bit for bit the same.
+template <int KIND, int PATH, int NW, int RP, int SUB, bool NORM, int S, class PS>
+__device__ __forceinline__ void pair_items_culled_ws(const PS& P) {
+    static_assert(kGroup % SUB == 0, "an FP32 run lies inside one group");
+    static_assert(PATH != 2 || !NORM, "the FP64-table path carries no FP32 run norms");
+    constexpr int NT = NW * 32;
+    constexpr int TS = NT * 2 * RP;
+    const int nit = P.count();
+    if ((int)blockIdx.x >= nit) return;
+    const PairArgs& A0 = P.first();
+    extern __shared__ __align__(128) unsigned char smem[];
+    float4* s_geo = reinterpret_cast<float4*>(smem);                               // [S][CH*2]
+    float2* s_qq = reinterpret_cast<float2*>(smem + S * CH * 2 * sizeof(float4));  // [S][CH]
+    Box* s_gbox = reinterpret_cast<Box*>(smem + S * pair_stage_bytes());  // [S][groups]
+    int4* s_rec = reinterpret_cast<int4*>(smem + S * (pair_stage_bytes() +
+                                                      kGroupsPerChunk * sizeof(Box)));
+    uint64_t* s_full = reinterpret_cast<uint64_t*>(s_rec + S);
+    uint64_t* s_empty = s_full + S;
+    float* s_tab = reinterpret_cast<float*>(smem + S * ws_stage_bytes());
+    double* s_tab64 = reinterpret_cast<double*>(smem + S * ws_stage_bytes());
+    __shared__ Box s_wbox[NW];
+
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (tid == 0) {
+        for (int i = 0; i < S; ++i) {
+            mbar_init(&s_full[i], 1);
+            mbar_init(&s_empty[i], NW);
+        }
+        fence_mbar_init();
+    }
+    if (PATH == 2) {
+        for (int k = tid; k <= A0.tab_k; k += NT + 32) s_tab64[k] = A0.tab64[k];
+    } else if (KIND == 1 || PATH == 1) {
+        for (int k = tid; k <= A0.tab_k; k += NT + 32) s_tab[k] = A0.tab[k];
+    }
+    __syncthreads();
+
+    if (warp == NW) {  // the producer warp
+        if (lane != 0) return;
+        unsigned* err = A0.err;
+        uint32_t k = 0;  // stages issued
+        bool ok = true;
+        for (;;) {
+            const int g = atomicAdd(P.work(), 1);
+            const bool done = g >= nit;
+            int prob = 0, local = -1;
+            int4 r = make_int4(0, 0, 1, 0);
+            if (!done) {
+                P.resolve(g, prob, local);
+                r = P.C(prob).items[local];
+            }
+            for (int c = 0; c < r.z; ++c, ++k) {
+                const int st = (int)(k % S);
+                if (k >= (uint32_t)S && !mbar_wait_bounded(&s_empty[st], (k / S - 1) & 1u, err)) {
+                    ok = false;
+                    break;
+                }
+                s_rec[st] = make_int4(local, c, r.z, prob);
+                if (done) {
+                    mbar_arrive(&s_full[st]);  // the end record: no copy
+                } else {
+                    const PairArgs& Ap = P.A(prob);
+                    const CullArgs& Cp = P.C(prob);
+                    const int chunk = Cp.live[(size_t)r.x * Cp.live_stride + r.y + c];
+                    fence_proxy_async_smem();
+                    mbar_arrive_expect_tx(&s_full[st], (uint32_t)(pair_stage_bytes() +
+                                                                  kGroupsPerChunk * sizeof(Box)));
+                    bulk_g2s(s_geo + st * CH * 2, Ap.geo + (size_t)chunk * CH * 2,
+                             (uint32_t)(CH * 2 * sizeof(float4)), &s_full[st]);
+                    bulk_g2s(s_qq + st * CH, Ap.qq + (size_t)chunk * CH,
+                             (uint32_t)(CH * sizeof(float2)), &s_full[st]);
+                    bulk_g2s(s_gbox + st * kGroupsPerChunk,
+                             Cp.gbox + (size_t)chunk * kGroupsPerChunk,
+                             (uint32_t)(kGroupsPerChunk * sizeof(Box)), &s_full[st]);
+                }
+            }
+            if (!ok || done) break;
+        }
+        // a consumer that gave up leaves copies unconsumed: let them land first
+        if (!ok) mbar_drain_ring(s_full, S, k > (uint32_t)S ? k - S : 0u, k);
+        return;
+    }
+
+    // consumer warps
+    float2 tx[RP], ty[RP], tz[RP], tt[RP];
+    double acc64[2 * RP];
+    float nrm[NORM ? 2 * RP : 1];
+    int base = 0, t_phys = 0, c2 = 0, tab_k = 0;
+    unsigned ulim = 0;
+    auto target_of = [&](int q) { return base + warp * (64 * RP) + q * 32 + lane; };
+    for (uint32_t k = 0;; ++k) {
+        const int st = (int)(k % S);
+        // every lane waits (acquiring the copy), and the warp leaves as one
+        if (!__all_sync(0xffffffffu, mbar_wait_bounded(&s_full[st], (k / S) & 1u, A0.err)))
+            break;
+        const int4 m = s_rec[st];
+        if (m.x < 0) break;  // the end record
+        const PairArgs& A = P.A(m.w);
+        const CullArgs& C = P.C(m.w);
+        if (m.y == 0) {  // the item's first chunk: its tile's targets of this warp
+            base = C.items[m.x].x * TS;
+            t_phys = A.dyn ? A.dyn[1] : A.t_phys;
+            c2 = C.c2;
+            tab_k = A.tab_k;
+            ulim = __float_as_uint(A.c2 - 0.5f);
+            int xl = 32767, yl = 32767, zl = 32767, xh = -32768, yh = -32768, zh = -32768;
+#pragma unroll
+            for (int q = 0; q < RP; ++q) {
+                const int p0 = target_of(2 * q), p1 = target_of(2 * q + 1);
+                const float4 a = p0 < t_phys ? A.tgt[p0] : make_float4(0.f, 0.f, 0.f, -1.f);
+                const float4 b = p1 < t_phys ? A.tgt[p1] : make_float4(0.f, 0.f, 0.f, -1.f);
+                tx[q] = f2(a.x, b.x); ty[q] = f2(a.y, b.y); tz[q] = f2(a.z, b.z);
+                tt[q] = f2(a.w, b.w);
+                if (a.w >= 0.f) {
+                    xl = min(xl, (int)a.x); yl = min(yl, (int)a.y); zl = min(zl, (int)a.z);
+                    xh = max(xh, (int)a.x); yh = max(yh, (int)a.y); zh = max(zh, (int)a.z);
+                }
+                if (b.w >= 0.f) {
+                    xl = min(xl, (int)b.x); yl = min(yl, (int)b.y); zl = min(zl, (int)b.z);
+                    xh = max(xh, (int)b.x); yh = max(yh, (int)b.y); zh = max(zh, (int)b.z);
+                }
+            }
+            warp_box(xl, yl, zl, xh, yh, zh);
+            if (lane == 0) s_wbox[warp] = make_box(xl, yl, zl, xh, yh, zh);
+            __syncwarp();
+#pragma unroll
+            for (int q = 0; q < 2 * RP; ++q) acc64[q] = 0.0;
+#pragma unroll
+            for (int q = 0; q < (NORM ? 2 * RP : 1); ++q) nrm[q] = 0.f;
+        }
+        bool gon = false;
+        if (lane < kGroupsPerChunk)
+            gon = box_gap2(s_wbox[warp], s_gbox[st * kGroupsPerChunk + lane]) < c2;
+        const unsigned gmask = __ballot_sync(0xffffffffu, gon);
+        if (C.examined && lane == 0 && gmask)
+            atomicAdd(C.examined, (unsigned long long)__popc(gmask) * kGroup * 64 * RP);
+        chunk_pairs<KIND, PATH, RP, SUB, NORM>(s_geo + st * CH * 2, s_qq + st * CH, gmask, tx, ty,
+                                               tz, tt, acc64, nrm, ulim, tab_k, s_tab, s_tab64);
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&s_empty[st]);  // this warp is done with stage st
+        if (m.y == m.z - 1) {  // the item's last chunk: its partials
+            double* out = A.part + (size_t)m.x * TS;
+#pragma unroll
+            for (int q = 0; q < 2 * RP; ++q) {
+                const int p = target_of(q);
+                if (p < t_phys) {
+                    out[p - base] = acc64[q];
+                    if (NORM) A.part_norm[(size_t)m.x * TS + (p - base)] = nrm[NORM ? q : 0];
+                }
+            }
+        }
+    }
+}
+
 template <int KIND, int PATH, int NT, int RP, int SUB, bool NORM = false>
 __global__ void __launch_bounds__(NT) pair_kernel_culled(PairArgs A, CullArgs C) {
     pair_items_culled<KIND, PATH, NT, RP, SUB, NORM>(OneProblem{A, C});
@@ -531,6 +731,18 @@ __global__ void __launch_bounds__(NT) pair_kernel_culled(PairArgs A, CullArgs C)
 template <int NT, int RP, int SUB, bool NORM>
 __global__ void __launch_bounds__(NT) pair_kernel_culled_list(ProblemList L) {
     pair_items_culled<0, 0, NT, RP, SUB, NORM>(L);
+}
+
+// Warp-specialised: NW consumer warps and one producer warp, S stages, at
+// least MINB resident CTAs per SM (a register bound).
+template <int KIND, int PATH, int NW, int RP, int SUB, int S, int MINB, bool NORM = false>
+__global__ void __launch_bounds__(NW * 32 + 32, MINB)
+    pair_kernel_culled_ws(PairArgs A, CullArgs C) {
+    pair_items_culled_ws<KIND, PATH, NW, RP, SUB, NORM, S>(OneProblem{A, C});
+}
+template <int NW, int RP, int SUB, int S, int MINB, bool NORM>
+__global__ void __launch_bounds__(NW * 32 + 32, MINB) pair_kernel_culled_ws_list(ProblemList L) {
+    pair_items_culled_ws<0, 0, NW, RP, SUB, NORM, S>(L);
 }
 
 // (static: each translation unit that launches them has its own copy)

@@ -60,6 +60,11 @@ __device__ __forceinline__ void bulk_g2s(void* smem_dst, const void* gmem_src, u
         : "memory");
 }
 
+// Plain arrival (no transaction count), release semantics at CTA scope.
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
+}
+
 __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
     uint32_t done;
     asm volatile(
@@ -92,6 +97,17 @@ __device__ __forceinline__ void mbar_drain_stages(uint64_t* bars, uint32_t first
         const uint32_t parity = (g >> 1) & 1u;
         for (int it = 0; it < limit; ++it)
             if (mbar_try_wait(&bars[g & 1u], parity)) break;
+    }
+}
+
+// The same for an S-stage ring: sequence number g uses stage g % S and
+// phase (g / S) & 1.
+__device__ __forceinline__ void mbar_drain_ring(uint64_t* bars, int S, uint32_t first,
+                                                uint32_t last, int limit = kWaitLimit) {
+    for (uint32_t g = first; g < last; ++g) {
+        const uint32_t parity = (g / (uint32_t)S) & 1u;
+        for (int it = 0; it < limit; ++it)
+            if (mbar_try_wait(&bars[g % (uint32_t)S], parity)) break;
     }
 }
 

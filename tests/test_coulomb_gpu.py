@@ -448,6 +448,45 @@ def test_culled_sums_examine_fewer_pairs(lgm, oracle_mod):
     assert 0 < info["pairs_examined"] < 0.5 * info["pairs_tested"]
 
 
+def test_warp_specialised_culled_sums_equal_the_culled_sums(lgm, oracle_mod):
+    """A warp-specialised culled variant (producer warp, ring of stages, items
+    taken from a counter) adds every target's terms in the order of a culled
+    variant with the same tile, FP32 run and chunks per item: the sums are
+    equal bit for bit, for every path and kind, with images at both
+    electrodes (a group one warp shape skips adds +0 in the other), and with
+    the same warp shape so are the pairs examined."""
+    X, Y, Z, c = 128, 128, 16, 40
+    rng = np.random.default_rng(12)
+    orc = oracle_mod.Oracle(X, Y, Z, cutoff=c, sigma=1.0)
+    ne = nh = int(0.008 * X * Y * Z)
+    s, q, n = packed_case(orc, rng, ne, nh, drains=6)
+    terms = lgm.TERM_DIRECT | lgm.TERM_IMAGE_LEFT | lgm.TERM_IMAGE_RIGHT
+    pairs = 0
+    for kind, path in [(lgm.POINT, 0), (lgm.GAUSS, 0), (lgm.POINT, 1), (lgm.POINT, 2),
+                       (lgm.GAUSS, 2)]:
+        with lgm.Coulomb(X, Y, Z, cutoff=c, sigma=1.0, path=path) as ctx:
+            vs = ctx.variants()
+            shape = lambda v: (vs[v]["threads"] * vs[v]["target_pairs"], vs[v]["run"],
+                               vs[v]["chunks_per_item"])
+            for w in [i for i, v in enumerate(vs) if v["warp_specialised"]]:
+                twins = [i for i, v in enumerate(vs) if v["culled"] and
+                         not v["warp_specialised"] and shape(i) == shape(w)]
+                for t in twins:
+                    got = []
+                    for v in (t, w):
+                        ctx.set_variant(v)
+                        ctx.set_counting(True)
+                        got.append((ctx.potentials(s[:n], q[:n], s, kind, terms),
+                                    ctx.last_launch()["pairs_examined"]))
+                        ctx.set_counting(False)
+                    np.testing.assert_array_equal(got[0][0], got[1][0])
+                    assert got[0][1] > 0 and got[1][1] > 0
+                    if vs[t]["target_pairs"] == vs[w]["target_pairs"]:
+                        assert got[0][1] == got[1][1]
+                    pairs += 1
+    assert pairs >= 10
+
+
 # ---- every compiled tile variant is exact to the same bound --------------------------
 def test_every_variant_and_autotune(lgm, oracle_mod):
     X, Y, Z, c = 96, 80, 12, 30
