@@ -498,6 +498,7 @@ lgm_status launch_culled(lgm_ctx* c, int kind, int v, const Shape& sh, const Pai
     const int TS = V.nt * 2 * V.rp;
     const int tiles = (sh.t_phys + TS - 1) / TS;
     const int max_items = std::min(kMaxItemsPerTile, (sh.n_chunks + V.per_item - 1) / V.per_item);
+    if (V.nt / 32 > kMaxSegments) return fail(c, LGM_ERR_STATE, "culled variant wider than the cull");
     const size_t item_cap = (size_t)tiles * std::max(1, max_items);
     lgm_status s;
     if ((s = grow_device(c, &c->d_cbox, &c->cbox_cap, (size_t)sh.n_chunks)) != LGM_OK) return s;
@@ -510,6 +511,7 @@ lgm_status launch_culled(lgm_ctx* c, int kind, int v, const Shape& sh, const Pai
     if ((s = grow_device(c, &c->d_tile_first, &c->tfirst_cap, (size_t)tiles)) != LGM_OK) return s;
     if ((s = grow_device(c, &c->d_tile_items, &c->titems_cap, (size_t)tiles)) != LGM_OK) return s;
     if ((s = grow_device(c, &c->d_part, &c->part_cap, item_cap * TS)) != LGM_OK) return s;
+    if ((s = grow_device(c, &c->d_order, &c->order_cap, item_cap)) != LGM_OK) return s;
     PairArgs P = A;
     P.part = c->d_part;
     CullArgs C;
@@ -529,6 +531,10 @@ lgm_status launch_culled(lgm_ctx* c, int kind, int v, const Shape& sh, const Pai
     C.work = c->d_item_count + 1;
     C.tile_first = c->d_tile_first;
     C.tile_items = c->d_tile_items;
+    // the items largest first (costs from the pair kernel's warp segments)
+    C.warp_targets = 64 * V.rp;
+    C.hist = c->d_cost_hist;
+    C.order = c->d_order;
     if (c->counting) {
         LGM_CUDA(c, cudaMemsetAsync(c->d_examined, 0, sizeof(unsigned long long), st));
         C.examined = c->d_examined;
@@ -536,6 +542,7 @@ lgm_status launch_culled(lgm_ctx* c, int kind, int v, const Shape& sh, const Pai
     }
     chunk_boxes_kernel<<<sh.n_chunks, CH, 0, st>>>(P, C);
     cull_kernel<<<tiles, kCullThreads, 0, st>>>(C);
+    order_items_kernel<<<1, 1024, 0, st>>>(C);
     // timing on: the events bracket the pair kernel alone (recorded again here)
     if (c->timing) LGM_CUDA(c, cudaEventRecord(c->ev_pair0, st));
     const int grid = c->sm_count * std::max(1, c->bps[v][fi]);
@@ -952,7 +959,8 @@ lgm_status lgm_create(const lgm_config* cfg, int32_t device, lgm_ctx** out) {
         c->bins_stride = (c->ncells + 2 + 3) / 4 * 4;
         if ((e = cudaMalloc(&c->d_cell_rank, sizeof(int32_t) * rank.size())) != cudaSuccess ||
             (e = cudaMalloc(&c->d_bins, sizeof(int32_t) * 2 * c->bins_stride)) != cudaSuccess ||
-            (e = cudaMalloc(&c->d_item_count, 2 * sizeof(int32_t))) != cudaSuccess)
+            (e = cudaMalloc(&c->d_item_count, 2 * sizeof(int32_t))) != cudaSuccess ||
+            (e = cudaMalloc(&c->d_cost_hist, kCostBuckets * sizeof(int32_t))) != cudaSuccess)
             return bail("cudaMalloc", e);
         // the source bins follow the target bins, 16-byte aligned (the scan reads int4)
         c->d_sbins = c->d_bins + c->bins_stride;
@@ -1005,7 +1013,8 @@ lgm_status lgm_destroy(lgm_ctx* c) {
                         c->d_bins,  c->d_key,        c->d_perm,       c->d_ttmp,
                         c->d_skey,  c->d_stmp,       c->d_cbox,       c->d_gbox,
                         c->d_live,  c->d_items,      c->d_tile_first, c->d_tile_items,
-                        c->d_item_count, c->d_examined, c->d_rtab64,  c->d_gtab64};
+                        c->d_item_count, c->d_examined, c->d_rtab64,  c->d_gtab64,
+                        c->d_cost_hist,  c->d_order};
     for (void* p : dev_ptrs)
         if (p) cudaFree(p);
     void* host_ptrs[] = {c->h_s, c->h_q, c->h_t, c->h_o, c->h_err};

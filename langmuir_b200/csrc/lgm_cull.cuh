@@ -37,6 +37,8 @@ constexpr int kGroup = 32;                    // sources per group box
 constexpr int kGroupsPerChunk = CH / kGroup;  // 4
 constexpr int kCullThreads = 256;             // threads of the cull kernel
 constexpr int kMaxItemsPerTile = 32;          // items a tile's chunk list is cut into, at most
+constexpr int kMaxSegments = 16;              // warp target segments of a tile, at most
+constexpr int kCostBuckets = 256;             // item cost classes of the largest-first order
 
 // A box of lattice coordinates [lo, hi] per axis (inclusive).  Empty: lo > hi.
 struct __align__(16) Box {
@@ -107,6 +109,15 @@ struct CullArgs {
     // Optional (null: off): pairs whose r^2 the pair kernel computed, i.e.
     // 32 sources x 64 RP targets per live group of a warp, summed over warps.
     unsigned long long* examined = nullptr;
+    // Optional largest-first order (hist null: off).  warp_targets: targets
+    // of one warp of the pair kernel (64 RP); an item's cost is the number of
+    // (warp, group) pairs whose boxes lie within the cutoff, i.e. the groups
+    // the pair kernel's warps will visit; hist[kCostBuckets] counts items per
+    // cost (zeroed by chunk_boxes block 0), and order_items writes order[]:
+    // the items by decreasing cost, which the pair kernels take in turn.
+    int warp_targets = 0;
+    int* hist = nullptr;
+    int* order = nullptr;
 };
 
 // One block of CH threads per source chunk: group and chunk boxes of the
@@ -116,9 +127,13 @@ __device__ __forceinline__ void chunk_boxes_body(const PairArgs& A, const CullAr
                                                  const int chunk) {
     __shared__ Box s_g[kGroupsPerChunk];
     const int n_chunks = A.dyn ? A.dyn[0] : A.n_chunks;
-    if (chunk == 0 && threadIdx.x == 0) {
-        if (C.item_count) *C.item_count = 0;
-        if (C.work) *C.work = 0;
+    if (chunk == 0) {
+        if (threadIdx.x == 0) {
+            if (C.item_count) *C.item_count = 0;
+            if (C.work) *C.work = 0;
+        }
+        if (C.hist)
+            for (int b = (int)threadIdx.x; b < kCostBuckets; b += (int)blockDim.x) C.hist[b] = 0;
     }
     if (chunk >= n_chunks) return;
     const int j = chunk * CH + (int)threadIdx.x;
@@ -148,8 +163,9 @@ __device__ __forceinline__ void chunk_boxes_body(const PairArgs& A, const CullAr
 // One block of kCullThreads per target tile: the tile's box, its live chunks
 // in source order, and its work items.
 __device__ __forceinline__ void cull_body(const CullArgs& C, const int tile) {
-    __shared__ int s_red[6][kCullThreads / 32];
+    __shared__ Box s_seg[kMaxSegments];
     __shared__ int s_wcount[kCullThreads / 32];
+    __shared__ int s_cost[kMaxItemsPerTile];
     __shared__ int s_base;
     const int n_chunks = C.dyn ? C.dyn[0] : C.n_chunks;
     const int t_phys = C.dyn ? C.dyn[1] : C.t_phys;
@@ -159,27 +175,33 @@ __device__ __forceinline__ void cull_body(const CullArgs& C, const int tile) {
         if (tid == 0) C.tile_items[tile] = 0;
         return;
     }
-    int xl = 32767, yl = 32767, zl = 32767, xh = -32768, yh = -32768, zh = -32768;
-    const int p1 = min((tile + 1) * C.tile_size, t_phys);
-    for (int p = tile * C.tile_size + tid; p < p1; p += kCullThreads) {
-        const float4 t = C.tgt[p];
-        if (t.w >= 0.f) {
-            const int x = (int)t.x, y = (int)t.y, z = (int)t.z;
-            xl = min(xl, x); yl = min(yl, y); zl = min(zl, z);
-            xh = max(xh, x); yh = max(yh, y); zh = max(zh, z);
+    // The boxes of the tile's warp segments (one segment: the whole tile),
+    // one warp of this block per segment; the tile box is their union.
+    const int seg_len = C.warp_targets > 0 ? C.warp_targets : C.tile_size;
+    const int nseg = C.tile_size / seg_len;
+    for (int sg = warp; sg < nseg; sg += nw) {
+        int xl = 32767, yl = 32767, zl = 32767, xh = -32768, yh = -32768, zh = -32768;
+        const int p0 = tile * C.tile_size + sg * seg_len;
+        const int p1 = min(p0 + seg_len, t_phys);
+        for (int p = p0 + lane; p < p1; p += 32) {
+            const float4 t = C.tgt[p];
+            if (t.w >= 0.f) {
+                const int x = (int)t.x, y = (int)t.y, z = (int)t.z;
+                xl = min(xl, x); yl = min(yl, y); zl = min(zl, z);
+                xh = max(xh, x); yh = max(yh, y); zh = max(zh, z);
+            }
         }
+        warp_box(xl, yl, zl, xh, yh, zh);
+        if (lane == 0) s_seg[sg] = make_box(xl, yl, zl, xh, yh, zh);
     }
-    warp_box(xl, yl, zl, xh, yh, zh);
-    if (lane == 0) {
-        s_red[0][warp] = xl; s_red[1][warp] = yl; s_red[2][warp] = zl;
-        s_red[3][warp] = xh; s_red[4][warp] = yh; s_red[5][warp] = zh;
-    }
+    if (tid < kMaxItemsPerTile) s_cost[tid] = 0;
     __syncthreads();
-    for (int w = 0; w < nw; ++w) {
-        xl = min(xl, s_red[0][w]); yl = min(yl, s_red[1][w]); zl = min(zl, s_red[2][w]);
-        xh = max(xh, s_red[3][w]); yh = max(yh, s_red[4][w]); zh = max(zh, s_red[5][w]);
+    Box tb = s_seg[0];
+    for (int sg = 1; sg < nseg; ++sg) {
+        tb.xl = min(tb.xl, s_seg[sg].xl); tb.yl = min(tb.yl, s_seg[sg].yl);
+        tb.zl = min(tb.zl, s_seg[sg].zl); tb.xh = max(tb.xh, s_seg[sg].xh);
+        tb.yh = max(tb.yh, s_seg[sg].yh); tb.zh = max(tb.zh, s_seg[sg].zh);
     }
-    const Box tb = make_box(xl, yl, zl, xh, yh, zh);
     int32_t* live = C.live + (size_t)tile * C.live_stride;
     int L = 0;
     for (int c0 = 0; c0 < n_chunks; c0 += kCullThreads) {
@@ -199,6 +221,20 @@ __device__ __forceinline__ void cull_body(const CullArgs& C, const int tile) {
     }
     const int per = max(C.per_item, (L + C.max_items - 1) / C.max_items);
     const int nit = L == 0 ? 0 : (L + per - 1) / per;
+    __syncthreads();  // the last round's live entries are visible to the block
+    if (C.hist) {
+        // item cost: the (segment, group) pairs within the cutoff; the live
+        // list was written by this block (visible after the barriers above)
+        const int work = L * kGroupsPerChunk * nseg;
+        for (int w = tid; w < work; w += kCullThreads) {
+            const int li = w / (kGroupsPerChunk * nseg);
+            const int r = w - li * (kGroupsPerChunk * nseg);
+            const int g = r / nseg, sg = r - g * nseg;
+            const int chunk = live[li];
+            if (box_gap2(s_seg[sg], C.gbox[(size_t)chunk * kGroupsPerChunk + g]) < C.c2)
+                atomicAdd(&s_cost[li / per], 1);
+        }
+    }
     if (tid == 0) {
         const int base = nit ? atomicAdd(C.item_count, nit) : 0;
         C.tile_first[tile] = base;
@@ -206,8 +242,33 @@ __device__ __forceinline__ void cull_body(const CullArgs& C, const int tile) {
         s_base = base;
     }
     __syncthreads();
-    for (int i = tid; i < nit; i += kCullThreads)
-        C.items[s_base + i] = make_int4(tile, i * per, min(per, L - i * per), 0);
+    for (int i = tid; i < nit; i += kCullThreads) {
+        C.items[s_base + i] = make_int4(tile, i * per, min(per, L - i * per), s_cost[i]);
+        if (C.hist) atomicAdd(&C.hist[min(s_cost[i], kCostBuckets - 1)], 1);
+    }
+}
+
+// order[] = the items by decreasing cost (a counting sort over the cost
+// classes; the order inside a class is arbitrary and changes no sum: an
+// item's partials go to its own slot whichever CTA computes it).  One block.
+__device__ __forceinline__ void order_items_body(const CullArgs& C) {
+    __shared__ int s_off[kCostBuckets];
+    const int nit = *C.item_count;
+    for (int b = (int)threadIdx.x; b < kCostBuckets; b += (int)blockDim.x) s_off[b] = C.hist[b];
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int run = 0;
+        for (int b = kCostBuckets - 1; b >= 0; --b) {
+            const int h = s_off[b];
+            s_off[b] = run;
+            run += h;
+        }
+    }
+    __syncthreads();
+    for (int g = (int)threadIdx.x; g < nit; g += (int)blockDim.x) {
+        const int c = min(C.items[g].w, kCostBuckets - 1);
+        C.order[atomicAdd(&s_off[c], 1)] = g;
+    }
 }
 
 // The pair sum over the work items (see the file comment).  KIND 0 point, 1
@@ -232,7 +293,7 @@ struct OneProblem {
     __device__ __forceinline__ int count() const { return *c.item_count; }
     __device__ __forceinline__ void resolve(int g, int& prob, int& local) const {
         prob = 0;
-        local = g;
+        local = c.order ? c.order[g] : g;
     }
     __device__ __forceinline__ const PairArgs& A(int) const { return a; }
     __device__ __forceinline__ const CullArgs& C(int) const { return c; }
@@ -752,6 +813,10 @@ static __global__ void __launch_bounds__(CH) chunk_boxes_kernel(PairArgs A, Cull
 
 static __global__ void __launch_bounds__(kCullThreads) cull_kernel(CullArgs C) {
     cull_body(C, (int)blockIdx.x);
+}
+
+static __global__ void __launch_bounds__(1024) order_items_kernel(CullArgs C) {
+    order_items_body(C);
 }
 
 // Sum of one physical target's item partials (its tile's items, in order).

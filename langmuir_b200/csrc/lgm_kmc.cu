@@ -98,6 +98,10 @@ struct Dev {
     double* de;
     uint8_t* accept;
     int32_t* flagged;
+    // the guard's per-split FP64 partials [ncap][kGuardSplits] and, per queued
+    // decision, the splits done (the last one sums them; zero between steps)
+    double2* gpart;
+    int32_t* gdone;
     int32_t* cnt;
     unsigned long long* ctr;
     float4* geo;
@@ -334,7 +338,22 @@ __device__ __forceinline__ void finalize_body(const Dev& D, const int g) {
             const int ni = D.tile_items[tile];
             const size_t f = (size_t)D.tile_first[tile] * kCTile + loc;
             double s = 0.0, m = 0.0;
-            for (int i = 0; i < ni; ++i) {
+            int i = 0;
+            for (; i + 4 <= ni; i += 4) {  // four items' loads in flight, adds in order
+                double pv[4];
+                float nv[4];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    pv[u] = D.part[f + (size_t)(i + u) * kCTile];
+                    nv[u] = D.part_norm[f + (size_t)(i + u) * kCTile];
+                }
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    s += pv[u];
+                    m += (double)nv[u];
+                }
+            }
+            for (; i < ni; ++i) {
                 s += D.part[f + (size_t)i * kCTile];
                 m += (double)D.part_norm[f + (size_t)i * kCTile];
             }
@@ -525,6 +544,10 @@ __device__ __forceinline__ void decide_body(const Dev& D, const int i) {
 // faster than 256 for a single replica (256x256x16, 20,922 carriers: step
 // 0.646 -> 0.620 ms) and for a batch of 512 uneven replicas (2.27 -> 2.20 ms).
 constexpr int kGuardThreads = 1024;
+// Each queued decision's source range is cut into this many splits, one
+// block each; the block that completes a decision last adds the splits'
+// partials in split order (a fixed order) and decides.
+constexpr int kGuardSplits = 16;
 // Blocks per replica of the batched guard: flagged decisions of one replica
 // are spread over them (a replica with M charges flags ~1e-3 M per step).
 constexpr int kGuardBlocksPerReplica = 12;
@@ -535,15 +558,13 @@ constexpr int kItemsPerThread = 4;
 // re-evaluation): the same cutoff and image rules as the pair kernel, terms
 // w(r^2) from the FP64 table (1/sqrt(k) or erf(f sqrt(k))/sqrt(k), computed on
 // the host in IEEE double), summed per thread and then across the block.
-__device__ double2 fp64_potential2(const Dev& D, int ne, int nh, int site_a, int site_b,
-                                   double2* red) {
+__device__ double2 fp64_potential2(const Dev& D, int ne, int nh, int site_a, int site_b, int j0,
+                                   int j1, double2* red) {
     int xa, ya, za, xb, yb, zb;
     xyz(D, site_a, xa, ya, za);
     xyz(D, site_b, xb, yb, zb);
-    const int nd = D.dq != 0 ? D.nd : 0;
-    const int n = ne + nh + nd;
     double acc_a = 0.0, acc_b = 0.0;
-    for (int j = threadIdx.x; j < n; j += blockDim.x) {
+    for (int j = j0 + (int)threadIdx.x; j < j1; j += blockDim.x) {
         int s;
         double q;
         if (j < ne) { s = D.e_site[j]; q = -1.0; }
@@ -584,24 +605,43 @@ __device__ double2 fp64_potential2(const Dev& D, int ne, int nh, int site_a, int
     __syncthreads();
     const double2 v = red[0];
     __syncthreads();
-    return make_double2(D.prefactor * v.x, D.prefactor * v.y);
+    return v;
 }
 
 __device__ __forceinline__ void guard_body(const Dev& D, const int block, const int nblocks,
                                            double2* red) {
+    __shared__ int s_last;
     const int ne = D.cnt[I_NE0], nh = D.cnt[I_NH0];
     const int nflag = D.cnt[I_NFLAG];
     const uint32_t step = (uint32_t)D.cnt[I_STEP];
-    for (int q_i = block; q_i < nflag; q_i += nblocks) {
+    const int n = ne + nh + (D.dq != 0 ? D.nd : 0);
+    for (int w = block; w < nflag * kGuardSplits; w += nblocks) {
+        const int q_i = w / kGuardSplits, sp = w - q_i * kGuardSplits;
         const int i = D.flagged[q_i];
         const bool e = i < ne;
         const int k = e ? i : i - ne;
         const int site = e ? D.e_site[k] : D.h_site[k];
         const int f = e ? D.e_f[k] : D.h_f[k];
         const double q = e ? -1.0 : 1.0;
-        const double2 v = fp64_potential2(D, ne, nh, site, f, red);
-        const double v1 = v.x, v2 = v.y;
+        const int j0 = (int)((long long)sp * n / kGuardSplits);
+        const int j1 = (int)((long long)(sp + 1) * n / kGuardSplits);
+        const double2 part = fp64_potential2(D, ne, nh, site, f, j0, j1, red);
         if (threadIdx.x == 0) {
+            D.gpart[(size_t)q_i * kGuardSplits + sp] = part;
+            __threadfence();
+            s_last = atomicAdd(&D.gdone[q_i], 1) == kGuardSplits - 1;
+        }
+        __syncthreads();
+        if (s_last && threadIdx.x == 0) {
+            __threadfence();
+            double2 t = make_double2(0.0, 0.0);
+            for (int u = 0; u < kGuardSplits; ++u) {  // split order
+                const double2 p = __ldcg(&D.gpart[(size_t)q_i * kGuardSplits + u]);
+                t.x += p.x;
+                t.y += p.y;
+            }
+            D.gdone[q_i] = 0;
+            const double v1 = D.prefactor * t.x, v2 = D.prefactor * t.y;
             const double p1 = v1 + binding(D, e, site);
             const double p2 = v2 - D.sI100 * q + binding(D, e, f);
             const double de = q * (p2 - p1);
@@ -615,6 +655,7 @@ __device__ __forceinline__ void guard_body(const Dev& D, const int block, const 
             D.de[i] = de;
             atomicAdd(&D.ctr[C_GUARD], 1ull);
         }
+        __syncthreads();  // s_last is read before the next decision writes it
     }
 }
 
@@ -739,27 +780,49 @@ __device__ __forceinline__ void recomb_reset_body(const Dev& D, const int i) {
 constexpr int kCompactThreads = 1024;
 
 // Entries before `start` are all kept (no removal below it) and stay put.
+constexpr int kCompactPer = 8;  // consecutive list entries per thread and round
 __device__ int compact(int32_t* a, int n, int* warp_sums, int start) {
     start = min(max(start, 0), n);
     int base = start;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for (int t0 = start; t0 < n; t0 += blockDim.x) {
-        const int i = t0 + threadIdx.x;
-        const int v = i < n ? a[i] : -1;
-        const bool keep = v >= 0;
-        const unsigned m = __ballot_sync(0xffffffffu, keep);
-        if (lane == 0) warp_sums[warp] = __popc(m);
-        __syncthreads();
-        int before = 0, total = 0;
-        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
-            if (w < warp) before += warp_sums[w];
-            total += warp_sums[w];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = (int)(blockDim.x >> 5);
+    const int span = (int)blockDim.x * kCompactPer;
+    for (int t0 = start; t0 < n; t0 += span) {
+        // Every read of the round precedes every write (two barriers apart),
+        // and an entry only moves to a lower index inside the rounds read so
+        // far, so the compaction runs in place.
+        const int i0 = t0 + (int)threadIdx.x * kCompactPer;
+        int v[kCompactPer];
+        int cnt = 0;
+#pragma unroll
+        for (int u = 0; u < kCompactPer; ++u) {
+            v[u] = i0 + u < n ? a[i0 + u] : -1;
+            cnt += v[u] >= 0;
         }
-        before += __popc(m & ((1u << lane) - 1u));
+        int inc = cnt;  // inclusive scan over the warp, then over the warps
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, inc, o);
+            if (lane >= o) inc += y;
+        }
+        if (lane == 31) warp_sums[warp] = inc;
         __syncthreads();
-        if (keep) a[base + before] = v;
+        if (warp == 0) {
+            int w = lane < nw ? warp_sums[lane] : 0;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, w, o);
+                if (lane >= o) w += y;
+            }
+            if (lane < nw) warp_sums[lane] = w;
+        }
+        __syncthreads();
+        int pos = base + (warp > 0 ? warp_sums[warp - 1] : 0) + inc - cnt;
+        const int total = warp_sums[nw - 1];
+#pragma unroll
+        for (int u = 0; u < kCompactPer; ++u)
+            if (v[u] >= 0) a[pos++] = v[u];
         base += total;
-        __syncthreads();
+        __syncthreads();  // warp_sums is read before the next round writes it
     }
     return base;
 }
@@ -1772,6 +1835,7 @@ static lgm_status kmc_create_impl(const lgm_params* pin, int32_t device, uint32_
     DA(D.defects, std::max(D.nd, 1));
     DA(D.claim_e, k->V); DA(D.claim_h, k->V);
     DA(D.outcome, ncap); DA(D.de, ncap); DA(D.accept, ncap); DA(D.flagged, ncap);
+    DA(D.gpart, (size_t)ncap * kGuardSplits); DA(D.gdone, ncap);
     DA(D.cnt, I_NUM); DA(D.ctr, C_NUM);
     DA(D.geo, 2 * D.src_cap); DA(D.qq, D.src_cap);
     DA(D.tgt, tphys_cap + kTile);
@@ -1869,6 +1933,7 @@ static lgm_status kmc_create_impl(const lgm_params* pin, int32_t device, uint32_
     cudaMemset(D.e_rm, 0, std::max(D.cap_e, 1));
     cudaMemset(D.h_rm, 0, std::max(D.cap_h, 1));
     cudaMemset(D.cnt, 0, sizeof(int32_t) * I_NUM);
+    cudaMemset(D.gdone, 0, sizeof(int32_t) * ncap);
     cudaMemset(D.ctr, 0, sizeof(unsigned long long) * C_NUM);
     if (!k->flux0.empty())
         cudaMemcpy(D.ctr, k->flux0.data(), sizeof(unsigned long long) * k->flux0.size(),
