@@ -361,11 +361,11 @@ struct Variant {
                 &pair_kernel_culled<0, 1, NT, RP, SUB>, &pair_kernel_culled<0, 2, NT, RP, SUB> \
         }                                                                                     \
     }
-#define LGM_VARIANT_CULL_WS(NW, RP, SUB, K, S, MINB)                                        \
+#define LGM_VARIANT_CULL_WS(NW, RP, SUB, K, S, MINB, PIPE)                                  \
     Variant {                                                                                 \
         NW * 32, RP, SUB, 1, 1, K, {nullptr, nullptr, nullptr, nullptr},                      \
-            {&pair_kernel_culled_ws<0, 0, NW, RP, SUB, S, MINB>,                              \
-             &pair_kernel_culled_ws<1, 0, NW, RP, SUB, S, MINB>,                              \
+            {&pair_kernel_culled_ws<0, 0, NW, RP, SUB, S, MINB, false, PIPE>,                 \
+             &pair_kernel_culled_ws<1, 0, NW, RP, SUB, S, MINB, false, PIPE>,                 \
              &pair_kernel_culled_ws<0, 1, NW, RP, SUB, S, MINB>,                              \
              &pair_kernel_culled_ws<0, 2, NW, RP, SUB, S, MINB>},                             \
             S                                                                                 \
@@ -382,9 +382,12 @@ const Variant kVariants[] = {
     LGM_VARIANT_CULL(64, 2, 32, 2),
     // warp-specialised: (target warps, target pairs, run, chunks per item,
     // stages, CTAs per SM); the register bound counts the producer warp
-    LGM_VARIANT_CULL_WS(4, 4, 32, 2, 4, 4), LGM_VARIANT_CULL_WS(8, 2, 32, 2, 4, 3),
-    LGM_VARIANT_CULL_WS(4, 2, 32, 2, 4, 5), LGM_VARIANT_CULL_WS(3, 4, 32, 2, 4, 5),
-    LGM_VARIANT_CULL_WS(7, 2, 32, 2, 4, 3), LGM_VARIANT_CULL_WS(4, 4, 32, 4, 4, 4),
+    LGM_VARIANT_CULL_WS(4, 4, 32, 2, 4, 4, false), LGM_VARIANT_CULL_WS(8, 2, 32, 2, 4, 3, false),
+    LGM_VARIANT_CULL_WS(4, 2, 32, 2, 4, 5, false), LGM_VARIANT_CULL_WS(3, 4, 32, 2, 4, 5, false),
+    LGM_VARIANT_CULL_WS(7, 2, 32, 2, 4, 3, false), LGM_VARIANT_CULL_WS(4, 4, 32, 4, 4, 4, false),
+    // the same with the next source's r^2 ahead of each vote
+    LGM_VARIANT_CULL_WS(4, 2, 32, 2, 4, 5, true), LGM_VARIANT_CULL_WS(7, 2, 32, 2, 4, 3, true),
+    LGM_VARIANT_CULL_WS(4, 2, 32, 2, 4, 4, true), LGM_VARIANT_CULL_WS(2, 2, 32, 2, 4, 8, true),
 };
 constexpr int kNumVariants = (int)(sizeof(kVariants) / sizeof(kVariants[0]));
 static_assert(kNumVariants <= (int)(sizeof(lgm_ctx::bps) / sizeof(lgm_ctx::bps[0])),

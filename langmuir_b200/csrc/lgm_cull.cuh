@@ -308,8 +308,10 @@ struct ProblemList {
     const int* list;
     const int* offs;   // [n + 2]: offs[n + 1] is the next item to take (zeroed with offs)
     int n;
+    const int* order;  // the items largest first (null: in number order)
     __device__ __forceinline__ int count() const { return n > 0 ? offs[n] : 0; }
     __device__ __forceinline__ void resolve(int g, int& prob, int& local) const {
+        if (order) g = order[g];
         int lo = 0, hi = n;  // the last i with offs[i] <= g
         while (hi - lo > 1) {
             const int mid = (lo + hi) >> 1;
@@ -329,7 +331,11 @@ struct ProblemList {
 // (bit g of gmask: group g), in FP32 runs of SUB sources folded into acc64
 // (PATH 0, 1), or term by term in FP64 (PATH 2).  sg/sq: the stage's source
 // records; tx..tt: the warp's target pairs; nrm: the runs' |sums| (NORM).
-template <int KIND, int PATH, int RP, int SUB, bool NORM>
+//
+// PIPE (PATH 0): the next source's r^2 is computed before the vote on this
+// one, so that two independent chains are in flight across the branch; the
+// arithmetic and the order of the additions are the same, and so are the bits.
+template <int KIND, int PATH, int RP, int SUB, bool NORM, bool PIPE = false>
 __device__ __forceinline__ void chunk_pairs(const float4* __restrict__ sg,
                                             const float2* __restrict__ sq, const unsigned gmask,
                                             const float2 (&tx)[RP], const float2 (&ty)[RP],
@@ -345,6 +351,66 @@ __device__ __forceinline__ void chunk_pairs(const float4* __restrict__ sg,
         float acc[2 * RP];
 #pragma unroll
         for (int k = 0; k < 2 * RP; ++k) acc[k] = 0.f;
+        if constexpr (PATH == 0 && PIPE) {
+            // r^2 - 1/2 of source j (three exact steps, as below)
+            auto r2_of = [&](const int j, float2 (&u)[RP]) {
+                const float4 g0 = sg[2 * j];
+                const float4 g1 = sg[2 * j + 1];
+                const float2 av = f2(g0.x, g0.y), bv = f2(g0.z, g0.w);
+                const float2 cv = f2(g1.x, g1.y), dv = f2(g1.z, g1.w);
+#pragma unroll
+                for (int k = 0; k < RP; ++k) {
+                    const float2 pa = __ffma2_rn(tx[k], av, tt[k]);
+                    const float2 pc = __ffma2_rn(tz[k], cv, dv);
+                    u[k] = __fadd2_rn(__ffma2_rn(ty[k], bv, pa), pc);
+                }
+            };
+            float2 un[RP];
+            r2_of(j0, un);
+#pragma unroll 4
+            for (int jj = 0; jj < SUB; ++jj) {
+                float2 uu[RP];
+                unsigned mk[RP];
+#pragma unroll
+                for (int k = 0; k < RP; ++k) {
+                    uu[k] = un[k];
+                    mk[k] = min(__float_as_uint(uu[k].x), __float_as_uint(uu[k].y));
+                }
+                // the next source (clamped inside the stage; unused past the run)
+                r2_of(min(j0 + jj + 1, CH - 1), un);
+#pragma unroll
+                for (int w = 1; w < RP; w *= 2)
+#pragma unroll
+                    for (int k = 0; k + w < RP; k += 2 * w) mk[k] = min(mk[k], mk[k + w]);
+                if (__any_sync(0xffffffffu, mk[0] < ulim)) {
+                    const float qs = sq[j0 + jj].x;
+#pragma unroll
+                    for (int k = 0; k < RP; ++k) {
+                        const float2 r2 = __fadd2_rn(uu[k], half2);
+                        float wx = rsqrt_mufu(r2.x);
+                        float wy = rsqrt_mufu(r2.y);
+                        if (KIND == 1) {
+                            const int ix =
+                                min(__float_as_int(r2.x + 8388608.f) & 0x7fffff, tab_k);
+                            const int iy =
+                                min(__float_as_int(r2.y + 8388608.f) & 0x7fffff, tab_k);
+                            wx = fminf(s_tab[ix], wx);
+                            wy = fminf(s_tab[iy], wy);
+                        }
+                        fma_if_below(acc[2 * k], qs, wx, __float_as_uint(uu[k].x), ulim);
+                        fma_if_below(acc[2 * k + 1], qs, wy, __float_as_uint(uu[k].y),
+                                     ulim);
+                    }
+                }
+            }
+#pragma unroll
+            for (int k = 0; k < 2 * RP; ++k) acc64[k] += (double)acc[k];
+            if (NORM) {
+#pragma unroll
+                for (int k = 0; k < 2 * RP; ++k) nrm[NORM ? k : 0] += fabsf(acc[k]);
+            }
+            continue;
+        }
         constexpr int kUnrollJ = PATH != 1 ? 4 : SUB;
 #pragma unroll kUnrollJ
         for (int jj = 0; jj < SUB; ++jj) {
@@ -629,7 +695,7 @@ inline size_t ws_smem_bytes(int S, int tab_k, int elem) {
 // producer's own waits then run out, and it waits (bounded) for the copies it
 // has in flight before leaving.  Per target, chunks and FP32 runs are added
 // in the order of pair_items_culled: the sums are bit for bit the same.
-template <int KIND, int PATH, int NW, int RP, int SUB, bool NORM, int S, class PS>
+template <int KIND, int PATH, int NW, int RP, int SUB, bool NORM, int S, bool PIPE, class PS>
 __device__ __forceinline__ void pair_items_culled_ws(const PS& P) {
     static_assert(kGroup % SUB == 0, "an FP32 run lies inside one group");
     static_assert(PATH != 2 || !NORM, "the FP64-table path carries no FP32 run norms");
@@ -764,8 +830,9 @@ __device__ __forceinline__ void pair_items_culled_ws(const PS& P) {
         const unsigned gmask = __ballot_sync(0xffffffffu, gon);
         if (C.examined && lane == 0 && gmask)
             atomicAdd(C.examined, (unsigned long long)__popc(gmask) * kGroup * 64 * RP);
-        chunk_pairs<KIND, PATH, RP, SUB, NORM>(s_geo + st * CH * 2, s_qq + st * CH, gmask, tx, ty,
-                                               tz, tt, acc64, nrm, ulim, tab_k, s_tab, s_tab64);
+        chunk_pairs<KIND, PATH, RP, SUB, NORM, PIPE>(s_geo + st * CH * 2, s_qq + st * CH, gmask,
+                                                     tx, ty, tz, tt, acc64, nrm, ulim, tab_k,
+                                                     s_tab, s_tab64);
         __syncwarp();
         if (lane == 0) mbar_arrive(&s_empty[st]);  // this warp is done with stage st
         if (m.y == m.z - 1) {  // the item's last chunk: its partials
@@ -796,14 +863,15 @@ __global__ void __launch_bounds__(NT) pair_kernel_culled_list(ProblemList L) {
 
 // Warp-specialised: NW consumer warps and one producer warp, S stages, at
 // least MINB resident CTAs per SM (a register bound).
-template <int KIND, int PATH, int NW, int RP, int SUB, int S, int MINB, bool NORM = false>
+template <int KIND, int PATH, int NW, int RP, int SUB, int S, int MINB, bool NORM = false,
+          bool PIPE = false>
 __global__ void __launch_bounds__(NW * 32 + 32, MINB)
     pair_kernel_culled_ws(PairArgs A, CullArgs C) {
-    pair_items_culled_ws<KIND, PATH, NW, RP, SUB, NORM, S>(OneProblem{A, C});
+    pair_items_culled_ws<KIND, PATH, NW, RP, SUB, NORM, S, PIPE>(OneProblem{A, C});
 }
-template <int NW, int RP, int SUB, int S, int MINB, bool NORM>
+template <int NW, int RP, int SUB, int S, int MINB, bool NORM, bool PIPE = false>
 __global__ void __launch_bounds__(NW * 32 + 32, MINB) pair_kernel_culled_ws_list(ProblemList L) {
-    pair_items_culled_ws<0, 0, NW, RP, SUB, NORM, S>(L);
+    pair_items_culled_ws<0, 0, NW, RP, SUB, NORM, S, PIPE>(L);
 }
 
 // (static: each translation unit that launches them has its own copy)

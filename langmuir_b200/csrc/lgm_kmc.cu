@@ -70,10 +70,12 @@ constexpr int kBalanceTries = 1024;
 constexpr int kNT = 128, kRP = 4, kSUB = 32;
 constexpr int kTile = kNT * 2 * kRP;
 constexpr int kCullPerItem = 2;  // source chunks per work item of the culled pair sum
-// Tile of the culled pair sum: 64 threads, 2 target pairs each (the shape the
-// API's autotuner picks for the 256x256x16 and 128x128x64 workloads).
-constexpr int kCNT = 64, kCRP = 2;
-constexpr int kCTile = kCNT * 2 * kCRP;
+// The culled pair sum: the warp-specialised kernel (lgm_cull.cuh) with 4
+// target warps of 2 target pairs per thread, a producer warp, 4 stages and 4
+// resident CTAs per SM; items taken largest first.
+constexpr int kCNW = 4, kCRP = 2, kCStages = 4, kCMinBlocks = 4;
+constexpr int kCThreads = kCNW * 32 + 32;
+constexpr int kCTile = kCNW * 32 * 2 * kCRP;
 // Replicas with room for fewer source chunks than this keep the unculled
 // skip tile: with a handful of chunks the boxes and the cull only add launches.
 constexpr int kCullMinChunks = 8;
@@ -133,7 +135,9 @@ struct Dev {
     Box *cbox, *gbox;
     int32_t* live;
     int4* items;
-    int32_t *item_count, *tile_first, *tile_items;
+    int32_t *item_count, *tile_first, *tile_items;  // item_count[2]: written, taken
+    int32_t *chist, *corder;  // item costs' histogram and the largest-first order
+                              // (corder null for a batch's replicas: the batch's)
     int src_cap;   // source records capacity (multiple of CH)
     int tpad_cap;  // per-term target block capacity
     unsigned* err;
@@ -1024,14 +1028,20 @@ __host__ __device__ __forceinline__ CullArgs cull_args(const Dev& D) {
     C.c2 = D.cutoff2; C.tile_size = kCTile;
     C.per_item = kCullPerItem; C.max_items = D.max_items;
     C.live = D.live; C.live_stride = D.src_cap / CH;
-    C.items = D.items; C.item_count = D.item_count;
+    C.items = D.items; C.item_count = D.item_count; C.work = D.item_count + 1;
     C.tile_first = D.tile_first; C.tile_items = D.tile_items;
+    // costs from the pair kernel's warp segments; a standalone replica orders
+    // its own items (a batch orders all its culled replicas' items at once)
+    C.warp_targets = 64 * kCRP;
+    C.hist = D.chist;
+    C.order = D.corder;
     return C;
 }
 __global__ void __launch_bounds__(CH) k_chunk_boxes(Dev D) {
     chunk_boxes_body(pair_args(D), cull_args(D), (int)blockIdx.x);
 }
 __global__ void __launch_bounds__(kCullThreads) k_cull(Dev D) { cull_body(cull_args(D), (int)blockIdx.x); }
+__global__ void __launch_bounds__(1024) k_order_items(Dev D) { order_items_body(cull_args(D)); }
 __global__ void k_tscatter(Dev D) { tscatter_body(D, LGM_THREAD_INDEX); }
 __global__ void k_trank(Dev D) { trank_body(D, LGM_THREAD_INDEX); }
 __global__ void __launch_bounds__(kGuardThreads) k_guard(Dev D) {
@@ -1104,6 +1114,31 @@ __global__ void __launch_bounds__(1024) kb_item_offsets(const Dev* R, const int*
         offs[i] = i < n ? *R[list[i]].item_count : 0;
     __syncthreads();
     block_exclusive_scan(offs, n + 1);
+    if (threadIdx.x == 0) offs[n + 1] = 0;  // the next item to take (ProblemList::work)
+}
+// order[] = all culled replicas' items (numbered as ProblemList numbers them)
+// by decreasing cost, from the batch's cost histogram.  One block.
+__global__ void __launch_bounds__(1024) kb_order_items(ProblemList L, const int32_t* hist,
+                                                       int32_t* order) {
+    __shared__ int s_off[kCostBuckets];
+    const int total = L.count();
+    for (int b = (int)threadIdx.x; b < kCostBuckets; b += (int)blockDim.x) s_off[b] = hist[b];
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int run = 0;
+        for (int b = kCostBuckets - 1; b >= 0; --b) {
+            const int h = s_off[b];
+            s_off[b] = run;
+            run += h;
+        }
+    }
+    __syncthreads();
+    for (int g = (int)threadIdx.x; g < total; g += (int)blockDim.x) {
+        int prob, local;
+        L.resolve(g, prob, local);  // L.order is null here: g's own item
+        const int c = min(L.C(prob).items[local].w, kCostBuckets - 1);
+        order[atomicAdd(&s_off[c], 1)] = g;
+    }
 }
 __global__ void __launch_bounds__(kGuardThreads) kb_guard(const Dev* R, const int4* map) {
     __shared__ double2 red[32];
@@ -1610,12 +1645,14 @@ using KPairFn = void (*)(PairArgs);
 
 using KCulledFn = void (*)(PairArgs, CullArgs);
 KCulledFn kmc_pair_culled(int gauss) {
-    return gauss ? &pair_kernel_culled<1, 0, kCNT, kCRP, kSUB, true>
-                 : &pair_kernel_culled<0, 0, kCNT, kCRP, kSUB, true>;
+    return gauss ? &pair_kernel_culled_ws<1, 0, kCNW, kCRP, kSUB, kCStages, kCMinBlocks, true>
+                 : &pair_kernel_culled_ws<0, 0, kCNW, kCRP, kSUB, kCStages, kCMinBlocks, true>;
 }
+size_t kmc_culled_smem(int tab_k) { return ws_smem_bytes(kCStages, tab_k, 4); }
 
 // the culled replicas of a batch (point charges), one persistent launch
-constexpr auto kBatchCulled = &pair_kernel_culled_list<kCNT, kCRP, kSUB, true>;
+constexpr auto kBatchCulled =
+    &pair_kernel_culled_ws_list<kCNW, kCRP, kSUB, kCStages, kCMinBlocks, true>;
 
 KPairFn kmc_pair(int gauss, int sorted = 1) {
     if (sorted)
@@ -1647,7 +1684,8 @@ lgm_status enqueue_step(lgm_kmc* k) {
         if (D.culled) {
             k_chunk_boxes<<<D.src_cap / CH, CH, 0, st>>>(D);
             k_cull<<<k->cull_tiles, kCullThreads, 0, st>>>(D);
-            kmc_pair_culled(D.gauss)<<<k->cull_grid, kCNT, pair_smem_bytes(A.tab_k), st>>>(
+            k_order_items<<<1, 1024, 0, st>>>(D);
+            kmc_pair_culled(D.gauss)<<<k->cull_grid, kCThreads, kmc_culled_smem(A.tab_k), st>>>(
                 A, cull_args(D));
         } else {
             kmc_pair(D.gauss, D.sorted)<<<dim3(k->pair_tiles, D.splits), kNT,
@@ -1859,7 +1897,8 @@ static lgm_status kmc_create_impl(const lgm_params* pin, int32_t device, uint32_
         DA(D.cbox, src_chunks); DA(D.gbox, (size_t)src_chunks * kGroupsPerChunk);
         DA(D.live, (size_t)k->cull_tiles * src_chunks);
         DA(D.items, (size_t)k->cull_tiles * D.max_items);
-        DA(D.item_count, 1); DA(D.tile_first, k->cull_tiles); DA(D.tile_items, k->cull_tiles);
+        DA(D.item_count, 2); DA(D.tile_first, k->cull_tiles); DA(D.tile_items, k->cull_tiles);
+        DA(D.chist, kCostBuckets); DA(D.corder, (size_t)k->cull_tiles * D.max_items);
     }
     DA(D.Vt, 2 * ncap); DA(D.Nt, 2 * ncap);
     DA(D.err, 1);
@@ -1904,14 +1943,14 @@ static lgm_status kmc_create_impl(const lgm_params* pin, int32_t device, uint32_
             cudaFuncSetAttribute(kmc_pair(1, sorted), cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)pair_smem_bytes(kmax));
         cudaFuncSetAttribute(kmc_pair_culled(1), cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)pair_smem_bytes(kmax));
+                             (int)kmc_culled_smem(kmax));
     }
     cudaMemcpy(crank_d, crank.data(), sizeof(int32_t) * crank.size(), cudaMemcpyHostToDevice);
     D.cell_rank = crank_d;
     if (D.culled) {
         int cbps = 1;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&cbps, kmc_pair_culled(D.gauss), kCNT,
-                                                      pair_smem_bytes(D.gauss ? D.gtab_k : 0));
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&cbps, kmc_pair_culled(D.gauss), kCThreads,
+                                                      kmc_culled_smem(D.gauss ? D.gtab_k : 0));
         k->cull_grid = n_sms * std::max(1, cbps);
     }
     {
@@ -2205,7 +2244,9 @@ struct lgm_kmc_batch {
     // work items (lgm_cull.cuh, ProblemList); the others take the items kernel
     std::vector<int> culled;
     int* d_culled = nullptr;
-    int32_t* d_coffs = nullptr;      // [culled + 1] work-item offsets
+    int32_t* d_coffs = nullptr;      // [culled + 2] work-item offsets, next item taken
+    int32_t* d_chist = nullptr;      // [kCostBuckets] the culled items' costs
+    int32_t* d_corder = nullptr;     // the culled items, largest first
     PairArgs* d_cpargs = nullptr;    // [count], filled for the culled replicas
     CullArgs* d_cargs = nullptr;     // [count]
     int2 *map_box = nullptr, *map_cull = nullptr;
@@ -2307,8 +2348,11 @@ lgm_status enqueue_batch_pair(lgm_kmc_batch* b, cudaStream_t st) {
         kb_chunk_boxes<<<b->nb_box, CH, 0, st>>>(b->d_reps, b->map_box);
         kb_cull<<<b->nb_cull, kCullThreads, 0, st>>>(b->d_reps, b->map_cull);
         kb_item_offsets<<<1, 1024, 0, st>>>(b->d_reps, b->d_culled, n, b->d_coffs);
-        kBatchCulled<<<b->cull_grid, kCNT, pair_smem_bytes(0), st>>>(
-            ProblemList{b->d_cpargs, b->d_cargs, b->d_culled, b->d_coffs, n});
+        kb_order_items<<<1, 1024, 0, st>>>(
+            ProblemList{b->d_cpargs, b->d_cargs, b->d_culled, b->d_coffs, n, nullptr},
+            b->d_chist, b->d_corder);
+        kBatchCulled<<<b->cull_grid, kCThreads, kmc_culled_smem(0), st>>>(
+            ProblemList{b->d_cpargs, b->d_cargs, b->d_culled, b->d_coffs, n, b->d_corder});
     }
     return enqueue_batch_items(b, st);
 }
@@ -2453,17 +2497,34 @@ lgm_status partition_batch(lgm_kmc_batch* b) {
     // culled pair sums for the per-phase replicas with room for enough chunks
     // (point charges: the Gaussian tables differ between replicas)
     b->culled.clear();
-    for (int r = 0; r < (int)b->hD.size(); ++r) b->hD[r].culled = 0;
+    for (int r = 0; r < (int)b->hD.size(); ++r) {
+        b->hD[r].culled = 0;
+        b->hD[r].chist = b->reps[r]->D.chist;
+        b->hD[r].corder = b->reps[r]->D.corder;
+    }
     for (int r : b->classic)
         if (b->reps[r]->cull_ok && !b->gauss) {
             b->hD[r].culled = 1;
             b->culled.push_back(r);
         }
+    // the culled items' cost histogram and order are the batch's
+    for (int32_t** p : {&b->d_coffs, &b->d_chist, &b->d_corder}) {
+        if (*p) cudaFree(*p);
+        *p = nullptr;
+    }
+    size_t order_cap = 1;
+    for (int r : b->culled) order_cap += (size_t)b->reps[r]->cull_tiles * b->hD[r].max_items;
+    if (cudaMalloc(&b->d_coffs, sizeof(int32_t) * (b->culled.size() + 2)) != cudaSuccess ||
+        cudaMalloc(&b->d_chist, sizeof(int32_t) * kCostBuckets) != cudaSuccess ||
+        cudaMalloc(&b->d_corder, sizeof(int32_t) * order_cap) != cudaSuccess)
+        return bfail(b, LGM_ERR_CUDA, "work-item offsets");
     std::vector<int2> box, cull;
     std::vector<PairArgs> cpargs(b->hD.size());
     std::vector<CullArgs> cargs(b->hD.size());
     for (int r : b->culled) {
-        const Dev& D = b->hD[r];
+        Dev& D = b->hD[r];
+        D.chist = b->d_chist;
+        D.corder = nullptr;
         for (int c = 0; c < D.src_cap / CH; ++c) box.push_back(make_int2(r, c));
         for (int t = 0; t < b->reps[r]->cull_tiles; ++t) cull.push_back(make_int2(r, t));
         cpargs[r] = pair_args(D);
@@ -2503,16 +2564,14 @@ lgm_status partition_batch(lgm_kmc_batch* b) {
         !upload(&b->map_cull, cull) || !upload(&b->d_cpargs, cpargs) ||
         !upload(&b->d_cargs, cargs))
         return bfail(b, LGM_ERR_CUDA, "block maps");
-    if (b->d_coffs) cudaFree(b->d_coffs);
-    b->d_coffs = nullptr;
-    if (cudaMalloc(&b->d_coffs, sizeof(int32_t) * (b->culled.size() + 1)) != cudaSuccess)
-        return bfail(b, LGM_ERR_CUDA, "work-item offsets");
+
     b->nb_box = (int)box.size();
     b->nb_cull = (int)cull.size();
     if (!b->culled.empty()) {
         int dev_sms = 0, cbps = 1;
         cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, b->device);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&cbps, kBatchCulled, kCNT, pair_smem_bytes(0));
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&cbps, kBatchCulled, kCThreads,
+                                                      kmc_culled_smem(0));
         b->cull_grid = std::max(1, dev_sms) * std::max(1, cbps);
     }
     b->nb_guard = (int)guard.size();
@@ -2591,7 +2650,8 @@ lgm_status lgm_kmc_batch_destroy(lgm_kmc_batch* b) {
     if (b->graph) cudaGraphDestroy(b->graph);
     void* ptrs[] = {b->d_reps, b->d_pargs, b->d_items, b->map_car, b->map_pack, b->map_fin,
                     b->map_guard, b->map_bins, b->d_fused, b->d_classic, b->d_culled,
-                    b->d_coffs, b->d_cpargs, b->d_cargs, b->map_box, b->map_cull};
+                    b->d_coffs, b->d_cpargs, b->d_cargs, b->map_box, b->map_cull,
+                    b->d_chist, b->d_corder};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (b->fork) cudaEventDestroy(b->fork);
