@@ -630,13 +630,16 @@ def other_kernels_run(L, args, fp32_peak):
     dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
     st = torch.cuda.Stream(dev)
     out = {}
-    # gauss2, config 3
+    # gauss2, config 3, FP32 rsqrt path and FP64 table path
     w = WORKLOADS["cfg3_gauss"]
     s_all, q_all, n = make_inputs(w, 5)
-    with L.Coulomb(w["X"], w["Y"], w["Z"], cutoff=w["cutoff"], sigma=w["sigma"],
-                   device=dev.index) as ctx:
-        out["gauss2_cfg3"] = dict(workload=w["desc"], **_kernel_leg(
-            L, ctx, args, w, s_all, q_all, n, L.GAUSS, 1, dev, st, fp32_peak))
+    for key, path, what in (("gauss2_cfg3", L.PATH_RSQRT, ""),
+                            ("gauss2_table64_cfg3", L.PATH_TABLE64,
+                             ", FP64 w(k) table, every term added in FP64")):
+        with L.Coulomb(w["X"], w["Y"], w["Z"], cutoff=w["cutoff"], sigma=w["sigma"],
+                       device=dev.index, path=path) as ctx:
+            out[key] = dict(workload=w["desc"] + what, **_kernel_leg(
+                L, ctx, args, w, s_all, q_all, n, L.GAUSS, 1, dev, st, fp32_peak))
     # cfg2 through the FP32 1/sqrt(k) table and through the FP64 table
     w = WORKLOADS["cfg2_3d_eh_images"]
     s_all, q_all, n = make_inputs(w, 7)

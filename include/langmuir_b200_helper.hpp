@@ -43,6 +43,12 @@ public:
     OpenClHelper(const OpenClHelper&) = delete;
     OpenClHelper& operator=(const OpenClHelper&) = delete;
 
+    // Extension (no reference counterpart): how the kernels accumulate --
+    // LGM_PATH_RSQRT (default), LGM_PATH_TABLE or LGM_PATH_TABLE64 (FP64
+    // terms: every potential within the reference's 1e-4 % acceptance test).
+    // Takes effect at the next initializeOpenCL.
+    void setAccumulationPath(lgm_path path) { m_path = path; }
+
     // openclhelper.cpp:17-187: okCL is false until the device is set up; a
     // failure with use.opencl set is an error (the reference's qFatal).
     void initializeOpenCL(int gpuID = -1) {
@@ -61,6 +67,7 @@ public:
         cfg.work_z = p.workZ;
         cfg.work_size = p.workSize;
         cfg.opencl_threshold = p.openclThreshold;
+        cfg.path = m_path;
         lgm_destroy(m_ctx);
         lgm_destroy(m_ctx64);
         m_ctx = m_ctx64 = nullptr;
@@ -228,6 +235,7 @@ private:
     lgm_ctx* m_ctx64 = nullptr;  // FP64 sums for compareHostAndDeviceForAllCarriers
     lgm_config m_cfg{};
     int m_device = -1;
+    lgm_path m_path = LGM_PATH_RSQRT;
     lgm_kind m_kind = LGM_POINT;
     std::vector<int32_t> m_s, m_q;
     std::vector<double> m_o;

@@ -129,20 +129,45 @@ __global__ void prep_sources_sorted(const int32_t* __restrict__ s, const int32_t
 // x' = -1 - x (distance x_i + x_j + 1, cubicgrid.cpp:117-120); a right image
 // at x' = 2X - 1 - x.  all_sites != 0: target g is lattice site g (kernel 1).
 __global__ void prep_targets(const int32_t* __restrict__ ts, int t, int t_pad, int all_sites,
-                             unsigned terms, int X, int Y, int XY, int volume,
-                             const int32_t* __restrict__ perm, float4* __restrict__ tgt,
-                             unsigned* err) {
-    const int g = blockIdx.x * blockDim.x + threadIdx.x;  // physical slot
-    if (g >= t_pad) return;
-    int x = 0, y = 0, z = 0;
-    if (g < t) {
-        const int tg = perm[g];                           // the target in this slot
-        const int sg = all_sites ? tg : ts[tg];
+                             unsigned terms, int X, int Y, int XY, int volume, int shift,
+                             const int32_t* __restrict__ tkey, const int32_t* __restrict__ ttmp,
+                             const int32_t* __restrict__ bins_end, int32_t* __restrict__ perm,
+                             float4* __restrict__ tgt, unsigned* err) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;  // scatter slot
+    if (j >= t_pad) return;
+    // The target scattered to slot j goes to physical slot g: its bin's start
+    // plus its rank inside the bin by index (perm[g] = target).  A target's
+    // sum is split into the work items of its tile (the culled tiles), so its
+    // tile, and with it the rounding of the item partials' sum, must not
+    // depend on the scatter's order: with this rank the sums are a function
+    // of the target list and the source set.  bins_end[b] is the end of bin b
+    // after the scatter.
+    // Every site (kernel 1): a cell's bin holds all its sites, and the rank
+    // by index is the site's raster position inside the (edge-clipped) cell.
+    int g = j, x = 0, y = 0, z = 0;
+    if (j < t) {
+        const int i = ttmp[j];
+        const int b = tkey[i];
+        const int lo = b > 0 ? bins_end[b - 1] : 0;
+        const int sg = all_sites ? i : ts[i];
         if (sg < 0 || sg >= volume + kDrainIds) {
             atomicOr(err, DEVERR_TARGET_RANGE);
         } else {
             z = sg / XY; y = sg / X - z * Y; x = sg % X;
         }
+        int rank = 0;
+        if (all_sites) {
+            const int c = 1 << shift;
+            const int x0 = (x >> shift) << shift, y0 = (y >> shift) << shift;
+            const int z0 = (z >> shift) << shift;
+            const int cw = min(c, X - x0), ch = min(c, Y - y0);
+            rank = ((z - z0) * ch + (y - y0)) * cw + (x - x0);
+        } else {
+            const int hi = bins_end[b];
+            for (int k = lo; k < hi; ++k) rank += ttmp[k] < i;
+        }
+        g = lo + rank;
+        perm[g] = i;
     }
     int slot = 0;
     for (int term = 0; term < 3; ++term) {
@@ -238,27 +263,10 @@ __global__ void scatter_both(const int32_t* __restrict__ tkey, int t, int32_t* _
     if (g < n) stmp[atomicAdd(&sbins[skey[g]], 1)] = g;
 }
 
-// perm[slot] = target in spatial order: the target scattered to slot j goes
-// to its bin's start plus its rank inside the bin by index.  A target's sum
-// is split into the work items of its tile (the culled tiles), so its tile,
-// and with it the rounding of the item partials' sum, must not depend on the
-// scatter's order: with this rank the sums are a function of the target list
-// and the source set.  bins_end[b] is the end of bin b after the scatter.
-__global__ void rank_targets(const int32_t* __restrict__ tkey, const int32_t* __restrict__ ttmp,
-                             const int32_t* __restrict__ bins_end, int t,
-                             int32_t* __restrict__ perm) {
-    const int j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= t) return;
-    const int i = ttmp[j];
-    const int b = tkey[i];
-    const int lo = b > 0 ? bins_end[b - 1] : 0, hi = bins_end[b];
-    int rank = 0;
-    for (int k = lo; k < hi; ++k) rank += ttmp[k] < i;
-    perm[lo + rank] = i;
-}
-
 // out[perm[g]] = prefactor * (sum of the item partials of the direct slot -
-// those of the image slots) of target g, for the culled pair sums.
+// those of the image slots) of target g, for the culled pair sums.  The
+// terms' partial streams are read side by side, four items at a time (up to
+// twelve loads in flight); each stream is still added in item order.
 __global__ void finalize_items(const double* __restrict__ part,
                                const int* __restrict__ tile_first,
                                const int* __restrict__ tile_items, int tile_size, int t,
@@ -266,11 +274,36 @@ __global__ void finalize_items(const double* __restrict__ part,
                                const int32_t* __restrict__ perm, double* __restrict__ out) {
     const int g = blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= t) return;
-    double total = 0.0;
-    for (int slot = 0; slot < nterms; ++slot) {
-        const double s = item_sum(part, tile_first, tile_items, tile_size, slot * t_pad + g);
-        total = (slot == 0) ? s : total - s;
+    const double* q[3];
+    int n[3];
+    int nmax = 0;
+#pragma unroll
+    for (int slot = 0; slot < 3; ++slot) {
+        n[slot] = 0;
+        q[slot] = part;
+        if (slot < nterms) {
+            const int p = slot * t_pad + g;
+            const int tile = p / tile_size, loc = p - tile * tile_size;
+            n[slot] = tile_items[tile];
+            q[slot] = part + (size_t)tile_first[tile] * tile_size + loc;
+            nmax = max(nmax, n[slot]);
+        }
     }
+    double sum[3] = {0.0, 0.0, 0.0};
+    for (int i = 0; i < nmax; i += 4) {
+        double v[3][4];
+#pragma unroll
+        for (int slot = 0; slot < 3; ++slot)
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+                v[slot][u] = i + u < n[slot] ? q[slot][(size_t)(i + u) * tile_size] : 0.0;
+#pragma unroll
+        for (int slot = 0; slot < 3; ++slot)
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+                if (i + u < n[slot]) sum[slot] += v[slot][u];
+    }
+    const double total = sum[0] - sum[1] - sum[2];
     out[perm[g]] = prefactor * total;
 }
 
@@ -383,16 +416,22 @@ const Variant kVariants[] = {
     // warp-specialised: (target warps, target pairs, run, chunks per item,
     // stages, CTAs per SM); the register bound counts the producer warp
     LGM_VARIANT_CULL_WS(4, 4, 32, 2, 4, 4, false), LGM_VARIANT_CULL_WS(8, 2, 32, 2, 4, 3, false),
-    LGM_VARIANT_CULL_WS(4, 2, 32, 2, 4, 5, false), LGM_VARIANT_CULL_WS(3, 4, 32, 2, 4, 5, false),
-    LGM_VARIANT_CULL_WS(7, 2, 32, 2, 4, 3, false), LGM_VARIANT_CULL_WS(4, 4, 32, 4, 4, 4, false),
-    // the same with the next source's r^2 ahead of each vote
-    LGM_VARIANT_CULL_WS(4, 2, 32, 2, 4, 5, true), LGM_VARIANT_CULL_WS(7, 2, 32, 2, 4, 3, true),
-    LGM_VARIANT_CULL_WS(4, 2, 32, 2, 4, 4, true), LGM_VARIANT_CULL_WS(2, 2, 32, 2, 4, 8, true),
+    LGM_VARIANT_CULL_WS(4, 2, 32, 2, 4, 5, false), LGM_VARIANT_CULL_WS(7, 2, 32, 2, 4, 3, false),
+    LGM_VARIANT_CULL_WS(4, 4, 32, 4, 4, 4, false),
+    // with the next source's r^2 ahead of each vote (PIPE); 4 CTAs of 4
+    // target warps and 2 target pairs per thread measured best on the
+    // 256x256x16 and 128x128x64 workloads (96 registers; the 5-CTA bound of
+    // 72 registers was 36% slower)
+    LGM_VARIANT_CULL_WS(4, 2, 32, 2, 4, 4, true), LGM_VARIANT_CULL_WS(4, 2, 32, 2, 4, 4, false),
+    LGM_VARIANT_CULL_WS(2, 2, 32, 2, 4, 6, true), LGM_VARIANT_CULL_WS(3, 2, 32, 2, 4, 5, true),
+    LGM_VARIANT_CULL_WS(4, 2, 32, 1, 4, 4, true), LGM_VARIANT_CULL_WS(4, 2, 32, 2, 6, 4, true),
 };
 constexpr int kNumVariants = (int)(sizeof(kVariants) / sizeof(kVariants[0]));
 static_assert(kNumVariants <= (int)(sizeof(lgm_ctx::bps) / sizeof(lgm_ctx::bps[0])),
               "lgm_ctx::bps holds every variant");
-constexpr int kDefaultVariant = 14;  // culled, 128 threads, 4 target pairs, runs of 32, 2 chunks per item
+// warp-specialised culled, 4 target warps, 2 target pairs, runs of 32, 2
+// chunks per item, PIPE
+constexpr int kDefaultVariant = 26;
 
 const void* kernel_of(const Variant& V, int fi) {
     return V.cull ? reinterpret_cast<const void*>(V.cfn[fi])
@@ -462,11 +501,10 @@ lgm_status prep(lgm_ctx* c, unsigned terms, const int32_t* d_src, const int32_t*
     bins_scan2<<<2, kScanThreads, 0, st>>>(c->d_bins, c->d_sbins, c->ncells + 1);
     scatter_both<<<tb, 256, 0, st>>>(c->d_key, t, c->d_bins, c->d_ttmp, c->d_skey, n, c->d_sbins,
                                      c->d_stmp);
-    rank_targets<<<(t + 255) / 256, 256, 0, st>>>(c->d_key, c->d_ttmp, c->d_bins, t, c->d_perm);
     LGM_CUDA(c, cudaGetLastError());
-    prep_targets<<<(sh.t_pad + 255) / 256, 256, 0, st>>>(d_tgt_site, t, sh.t_pad, all_sites, terms,
-                                                          cf.grid_x, cf.grid_y, c->xy, c->volume,
-                                                          c->d_perm, c->d_tgt, c->d_err);
+    prep_targets<<<(sh.t_pad + 255) / 256, 256, 0, st>>>(
+        d_tgt_site, t, sh.t_pad, all_sites, terms, cf.grid_x, cf.grid_y, c->xy, c->volume,
+        c->cell_shift, c->d_key, c->d_ttmp, c->d_bins, c->d_perm, c->d_tgt, c->d_err);
     prep_sources_sorted<<<(sh.n_pad + 255) / 256, 256, 0, st>>>(
         d_src, d_q, n, sh.n_pad, c->d_skey, c->d_stmp, c->d_sbins, cf.grid_x, cf.grid_y, c->xy,
         c->volume, c->d_geo, c->d_qq, c->d_err);

@@ -71,8 +71,9 @@ constexpr int kNT = 128, kRP = 4, kSUB = 32;
 constexpr int kTile = kNT * 2 * kRP;
 constexpr int kCullPerItem = 2;  // source chunks per work item of the culled pair sum
 // The culled pair sum: the warp-specialised kernel (lgm_cull.cuh) with 4
-// target warps of 2 target pairs per thread, a producer warp, 4 stages and 4
-// resident CTAs per SM; items taken largest first.
+// target warps of 2 target pairs per thread, a producer warp, 4 stages, 4
+// resident CTAs per SM and the next source's r^2 ahead of each vote; items
+// taken largest first (the API's default variant).
 constexpr int kCNW = 4, kCRP = 2, kCStages = 4, kCMinBlocks = 4;
 constexpr int kCThreads = kCNW * 32 + 32;
 constexpr int kCTile = kCNW * 32 * 2 * kCRP;
@@ -1645,14 +1646,15 @@ using KPairFn = void (*)(PairArgs);
 
 using KCulledFn = void (*)(PairArgs, CullArgs);
 KCulledFn kmc_pair_culled(int gauss) {
-    return gauss ? &pair_kernel_culled_ws<1, 0, kCNW, kCRP, kSUB, kCStages, kCMinBlocks, true>
-                 : &pair_kernel_culled_ws<0, 0, kCNW, kCRP, kSUB, kCStages, kCMinBlocks, true>;
+    return gauss
+               ? &pair_kernel_culled_ws<1, 0, kCNW, kCRP, kSUB, kCStages, kCMinBlocks, true, true>
+               : &pair_kernel_culled_ws<0, 0, kCNW, kCRP, kSUB, kCStages, kCMinBlocks, true, true>;
 }
 size_t kmc_culled_smem(int tab_k) { return ws_smem_bytes(kCStages, tab_k, 4); }
 
 // the culled replicas of a batch (point charges), one persistent launch
 constexpr auto kBatchCulled =
-    &pair_kernel_culled_ws_list<kCNW, kCRP, kSUB, kCStages, kCMinBlocks, true>;
+    &pair_kernel_culled_ws_list<kCNW, kCRP, kSUB, kCStages, kCMinBlocks, true, true>;
 
 KPairFn kmc_pair(int gauss, int sorted = 1) {
     if (sorted)

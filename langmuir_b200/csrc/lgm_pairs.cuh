@@ -353,11 +353,14 @@ __device__ __forceinline__ void block_exclusive_scan(int32_t* a, int n) {
     __syncthreads();
 }
 
-// Morton (Z-order) rank of every lattice cell -- cubes of 2^shift sites,
-// the shift the smallest that keeps the cells at most 65536 -- for sorting
-// targets in spatial order.  Host side; returns the rank table.
+// Morton (Z-order) rank of every lattice cell -- cubes of 2^shift sites, the
+// shift the smallest from 3 up that keeps the cells at most 65536 -- for
+// sorting targets and sources in spatial order.  Cells of 8^3 sites rather
+// than 4^3 cut the bins (and the scans over them) eightfold for a slightly
+// coarser order: on 256x256x16 with 2% charges the culled sums examine 0.4%
+// more pairs.  Host side; returns the rank table.
 inline std::vector<int32_t> cell_ranks(int X, int Y, int Z, int* shift, int* cx, int* cy) {
-    int sh = 2;
+    int sh = 3;
     auto cells = [&](int d) { return (d + (1 << sh) - 1) >> sh; };
     while ((long long)cells(X) * cells(Y) * cells(Z) > 65536) ++sh;
     *shift = sh;

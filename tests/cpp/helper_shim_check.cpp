@@ -5,8 +5,10 @@
 // "site future_site", then nd defect sites.  Output: okCL, status, then one
 // line per carrier: opencl_id p_current p_future.  With --compare, instead
 // compareHostAndDeviceForAllCarriers: "failed N", then per carrier
-// "opencl_id gpu1 gpu2 cpu1 cpu2 gpu cpu failed".
+// "opencl_id gpu1 gpu2 cpu1 cpu2 gpu cpu failed".  A second argument selects
+// the accumulation path (lgm_path: 0 rsqrt, 1 table, 2 FP64 table).
 #include <cstdio>
+#include <cstdlib>
 #include <string>
 #include <vector>
 
@@ -63,6 +65,7 @@ int main(int argc, char** argv) {
         w.d.push_back(s);
     }
     langmuir_b200::OpenClHelper<World> helper(w);
+    if (argc > 2) helper.setAccumulationPath((lgm_path)std::atoi(argv[2]));
     helper.initializeOpenCL(0);
     const bool on = helper.toggleOpenCL(true);
     std::printf("okCL %d use %d status %d\n", (int)w.p.okCL, (int)on, (int)helper.lastStatus());

@@ -107,3 +107,31 @@ def test_shim_compare_host_and_device(shim_exe, oracle_mod):
     rule = ((gpu - cpu) > 1e-4) | (pdiff(gpu1, cpu1) > 1e-4) | (pdiff(gpu2, cpu2) > 1e-4)
     assert np.array_equal(flag.astype(bool), rule)
     assert failed == int(rule.sum())
+
+
+@pytest.mark.gpu
+def test_shim_compare_flags_no_carrier_on_a_cfg2_world_with_fp64_terms(shim_exe, oracle_mod):
+    """On a 256x256x16 world with 1% electrons and 1% holes, each with one
+    proposed hop, compareHostAndDeviceForAllCarriers under the FP64-table
+    accumulation (LGM_PATH_TABLE64) flags no carrier: every potential is within
+    the reference's 1e-4 % of the FP64 sums (chargeagent.cpp:364-370).  The
+    FP32 rsqrt path, run on the same world for contrast, stays within its
+    stated 1e-6 N bound but may flag carriers whose potential nearly cancels."""
+    X, Y, Z, c = 256, 256, 16, 50
+    rng = np.random.default_rng(21)
+    orc = oracle_mod.Oracle(X, Y, Z, cutoff=c)
+    n = int(0.01 * X * Y * Z)
+    sites = rng.choice(X * Y * Z, 2 * n, replace=False)
+    e, h = sites[:n], sites[n:]
+    ef = [int(rng.choice(orc.neighbors(int(s)))) for s in e]
+    hf = [int(rng.choice(orc.neighbors(int(s)))) for s in h]
+    failed = {}
+    for path in (2, 0):
+        rc, out = run_shim(shim_exe, X, Y, Z, c, e, ef, h, hf, [], 0, "--compare", str(path))
+        assert rc == 0, out
+        rows = out.strip().splitlines()
+        assert rows[0] == "okCL 1 use 1 status 0"
+        failed[path] = int(rows[1].split()[1])
+        assert len(rows) == 2 + 2 * n
+    assert failed[2] == 0
+    print("carriers flagged: FP64 table", failed[2], "FP32 rsqrt", failed[0])
