@@ -418,10 +418,10 @@ const Variant kVariants[] = {
     LGM_VARIANT_CULL_WS(4, 4, 32, 2, 4, 4, false), LGM_VARIANT_CULL_WS(8, 2, 32, 2, 4, 3, false),
     LGM_VARIANT_CULL_WS(4, 2, 32, 2, 4, 5, false), LGM_VARIANT_CULL_WS(7, 2, 32, 2, 4, 3, false),
     LGM_VARIANT_CULL_WS(4, 4, 32, 4, 4, 4, false),
-    // with the next source's r^2 ahead of each vote (PIPE); 4 CTAs of 4
-    // target warps and 2 target pairs per thread measured best on the
-    // 256x256x16 and 128x128x64 workloads (96 registers; the 5-CTA bound of
-    // 72 registers was 36% slower)
+    // 4 CTAs of 4 target warps and 2 target pairs per thread measured best on
+    // the 256x256x16 and 128x128x64 workloads (96 registers; the 5-CTA bound
+    // of 72 registers was 36% slower); the next source's r^2 ahead of each
+    // vote (PIPE) measured the same
     LGM_VARIANT_CULL_WS(4, 2, 32, 2, 4, 4, true), LGM_VARIANT_CULL_WS(4, 2, 32, 2, 4, 4, false),
     LGM_VARIANT_CULL_WS(2, 2, 32, 2, 4, 6, true), LGM_VARIANT_CULL_WS(3, 2, 32, 2, 4, 5, true),
     LGM_VARIANT_CULL_WS(4, 2, 32, 1, 4, 4, true), LGM_VARIANT_CULL_WS(4, 2, 32, 2, 6, 4, true),
@@ -430,8 +430,8 @@ constexpr int kNumVariants = (int)(sizeof(kVariants) / sizeof(kVariants[0]));
 static_assert(kNumVariants <= (int)(sizeof(lgm_ctx::bps) / sizeof(lgm_ctx::bps[0])),
               "lgm_ctx::bps holds every variant");
 // warp-specialised culled, 4 target warps, 2 target pairs, runs of 32, 2
-// chunks per item, PIPE
-constexpr int kDefaultVariant = 26;
+// chunks per item
+constexpr int kDefaultVariant = 27;
 
 const void* kernel_of(const Variant& V, int fi) {
     return V.cull ? reinterpret_cast<const void*>(V.cfn[fi])
@@ -576,14 +576,14 @@ lgm_status launch_culled(lgm_ctx* c, int kind, int v, const Shape& sh, const Pai
     C.warp_targets = 64 * V.rp;
     C.hist = c->d_cost_hist;
     C.order = c->d_order;
+    C.done = c->d_item_count + 2;
     if (c->counting) {
         LGM_CUDA(c, cudaMemsetAsync(c->d_examined, 0, sizeof(unsigned long long), st));
         C.examined = c->d_examined;
         c->count_pending = true;
     }
     chunk_boxes_kernel<<<sh.n_chunks, CH, 0, st>>>(P, C);
-    cull_kernel<<<tiles, kCullThreads, 0, st>>>(C);
-    order_items_kernel<<<1, 1024, 0, st>>>(C);
+    cull_kernel<<<tiles, kCullThreads, 0, st>>>(C);  // its last block orders the items
     // timing on: the events bracket the pair kernel alone (recorded again here)
     if (c->timing) LGM_CUDA(c, cudaEventRecord(c->ev_pair0, st));
     const int grid = c->sm_count * std::max(1, c->bps[v][fi]);
@@ -1000,7 +1000,7 @@ lgm_status lgm_create(const lgm_config* cfg, int32_t device, lgm_ctx** out) {
         c->bins_stride = (c->ncells + 2 + 3) / 4 * 4;
         if ((e = cudaMalloc(&c->d_cell_rank, sizeof(int32_t) * rank.size())) != cudaSuccess ||
             (e = cudaMalloc(&c->d_bins, sizeof(int32_t) * 2 * c->bins_stride)) != cudaSuccess ||
-            (e = cudaMalloc(&c->d_item_count, 2 * sizeof(int32_t))) != cudaSuccess ||
+            (e = cudaMalloc(&c->d_item_count, 3 * sizeof(int32_t))) != cudaSuccess ||
             (e = cudaMalloc(&c->d_cost_hist, kCostBuckets * sizeof(int32_t))) != cudaSuccess)
             return bail("cudaMalloc", e);
         // the source bins follow the target bins, 16-byte aligned (the scan reads int4)

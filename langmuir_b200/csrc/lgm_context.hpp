@@ -57,7 +57,8 @@ struct lgm_ctx {
     int4* d_items = nullptr; size_t items_cap = 0;
     int32_t* d_tile_first = nullptr; size_t tfirst_cap = 0;
     int32_t* d_tile_items = nullptr; size_t titems_cap = 0;
-    int32_t* d_item_count = nullptr;                  // [2]: items written, next item taken
+    int32_t* d_item_count = nullptr;                  // [3]: items written, next item taken,
+                                                      // tiles culled
     int32_t* d_cost_hist = nullptr;                   // [kCostBuckets] items per cost
     int32_t* d_order = nullptr; size_t order_cap = 0; // items by decreasing cost
 

@@ -118,6 +118,9 @@ struct CullArgs {
     int warp_targets = 0;
     int* hist = nullptr;
     int* order = nullptr;
+    // with order: culled tiles so far (zeroed by chunk_boxes block 0); the
+    // cull's last block to finish writes order[]
+    int* done = nullptr;
 };
 
 // One block of CH threads per source chunk: group and chunk boxes of the
@@ -131,6 +134,7 @@ __device__ __forceinline__ void chunk_boxes_body(const PairArgs& A, const CullAr
         if (threadIdx.x == 0) {
             if (C.item_count) *C.item_count = 0;
             if (C.work) *C.work = 0;
+            if (C.done) *C.done = 0;
         }
         if (C.hist)
             for (int b = (int)threadIdx.x; b < kCostBuckets; b += (int)blockDim.x) C.hist[b] = 0;
@@ -160,6 +164,46 @@ __device__ __forceinline__ void chunk_boxes_body(const PairArgs& A, const CullAr
     }
 }
 
+// order[] = the items by decreasing cost (a counting sort over the cost
+// classes; the order inside a class is arbitrary and changes no sum: an
+// item's partials go to its own slot whichever CTA computes it).  One block;
+// the reads bypass L1 (the other blocks' writes are in L2).
+__device__ __forceinline__ void order_items_body(const CullArgs& C) {
+    __shared__ int s_off[kCostBuckets];
+    const int nit = __ldcg(C.item_count);
+    for (int b = (int)threadIdx.x; b < kCostBuckets; b += (int)blockDim.x)
+        s_off[b] = __ldcg(&C.hist[b]);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int run = 0;
+        for (int b = kCostBuckets - 1; b >= 0; --b) {
+            const int h = s_off[b];
+            s_off[b] = run;
+            run += h;
+        }
+    }
+    __syncthreads();
+    for (int g = (int)threadIdx.x; g < nit; g += (int)blockDim.x) {
+        const int c = min(__ldcg(&C.items[g]).w, kCostBuckets - 1);
+        C.order[atomicAdd(&s_off[c], 1)] = g;
+    }
+}
+
+// The cull's last block to finish (every block fences its items and costs,
+// then counts itself in C.done) writes the order.
+__device__ __forceinline__ void cull_last_orders(const CullArgs& C) {
+    __shared__ int s_last;
+    __syncthreads();  // every thread's items and histogram adds are issued
+    if (threadIdx.x == 0) {
+        __threadfence();
+        s_last = atomicAdd(C.done, 1) == (int)gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    order_items_body(C);
+}
+
 // One block of kCullThreads per target tile: the tile's box, its live chunks
 // in source order, and its work items.
 __device__ __forceinline__ void cull_body(const CullArgs& C, const int tile) {
@@ -173,6 +217,7 @@ __device__ __forceinline__ void cull_body(const CullArgs& C, const int tile) {
     constexpr int nw = kCullThreads / 32;
     if (tile * C.tile_size >= t_phys) {
         if (tid == 0) C.tile_items[tile] = 0;
+        if (C.order) cull_last_orders(C);
         return;
     }
     // The boxes of the tile's warp segments (one segment: the whole tile),
@@ -223,16 +268,15 @@ __device__ __forceinline__ void cull_body(const CullArgs& C, const int tile) {
     const int nit = L == 0 ? 0 : (L + per - 1) / per;
     __syncthreads();  // the last round's live entries are visible to the block
     if (C.hist) {
-        // item cost: the (segment, group) pairs within the cutoff; the live
-        // list was written by this block (visible after the barriers above)
-        const int work = L * kGroupsPerChunk * nseg;
-        for (int w = tid; w < work; w += kCullThreads) {
-            const int li = w / (kGroupsPerChunk * nseg);
-            const int r = w - li * (kGroupsPerChunk * nseg);
-            const int g = r / nseg, sg = r - g * nseg;
-            const int chunk = live[li];
-            if (box_gap2(s_seg[sg], C.gbox[(size_t)chunk * kGroupsPerChunk + g]) < C.c2)
-                atomicAdd(&s_cost[li / per], 1);
+        // item cost: the (segment, group) pairs within the cutoff, one thread
+        // per (live chunk, group); the live list was written by this block
+        // (visible after the barriers above)
+        for (int w = tid; w < L * kGroupsPerChunk; w += kCullThreads) {
+            const int li = w / kGroupsPerChunk, g = w - li * kGroupsPerChunk;
+            const Box gb = C.gbox[(size_t)live[li] * kGroupsPerChunk + g];
+            int n = 0;
+            for (int sg = 0; sg < nseg; ++sg) n += box_gap2(s_seg[sg], gb) < C.c2;
+            if (n) atomicAdd(&s_cost[li / per], n);
         }
     }
     if (tid == 0) {
@@ -246,29 +290,7 @@ __device__ __forceinline__ void cull_body(const CullArgs& C, const int tile) {
         C.items[s_base + i] = make_int4(tile, i * per, min(per, L - i * per), s_cost[i]);
         if (C.hist) atomicAdd(&C.hist[min(s_cost[i], kCostBuckets - 1)], 1);
     }
-}
-
-// order[] = the items by decreasing cost (a counting sort over the cost
-// classes; the order inside a class is arbitrary and changes no sum: an
-// item's partials go to its own slot whichever CTA computes it).  One block.
-__device__ __forceinline__ void order_items_body(const CullArgs& C) {
-    __shared__ int s_off[kCostBuckets];
-    const int nit = *C.item_count;
-    for (int b = (int)threadIdx.x; b < kCostBuckets; b += (int)blockDim.x) s_off[b] = C.hist[b];
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        int run = 0;
-        for (int b = kCostBuckets - 1; b >= 0; --b) {
-            const int h = s_off[b];
-            s_off[b] = run;
-            run += h;
-        }
-    }
-    __syncthreads();
-    for (int g = (int)threadIdx.x; g < nit; g += (int)blockDim.x) {
-        const int c = min(C.items[g].w, kCostBuckets - 1);
-        C.order[atomicAdd(&s_off[c], 1)] = g;
-    }
+    if (C.order) cull_last_orders(C);
 }
 
 // The pair sum over the work items (see the file comment).  KIND 0 point, 1

@@ -71,9 +71,8 @@ constexpr int kNT = 128, kRP = 4, kSUB = 32;
 constexpr int kTile = kNT * 2 * kRP;
 constexpr int kCullPerItem = 2;  // source chunks per work item of the culled pair sum
 // The culled pair sum: the warp-specialised kernel (lgm_cull.cuh) with 4
-// target warps of 2 target pairs per thread, a producer warp, 4 stages, 4
-// resident CTAs per SM and the next source's r^2 ahead of each vote; items
-// taken largest first (the API's default variant).
+// target warps of 2 target pairs per thread, a producer warp, 4 stages and 4
+// resident CTAs per SM; items taken largest first (the API's default variant).
 constexpr int kCNW = 4, kCRP = 2, kCStages = 4, kCMinBlocks = 4;
 constexpr int kCThreads = kCNW * 32 + 32;
 constexpr int kCTile = kCNW * 32 * 2 * kCRP;
@@ -136,7 +135,8 @@ struct Dev {
     Box *cbox, *gbox;
     int32_t* live;
     int4* items;
-    int32_t *item_count, *tile_first, *tile_items;  // item_count[2]: written, taken
+    int32_t *item_count, *tile_first, *tile_items;  // item_count[3]: written, taken, tiles
+                                                    // culled
     int32_t *chist, *corder;  // item costs' histogram and the largest-first order
                               // (corder null for a batch's replicas: the batch's)
     int src_cap;   // source records capacity (multiple of CH)
@@ -336,35 +336,49 @@ __device__ __forceinline__ void finalize_body(const Dev& D, const int g) {
     if (g >= t) return;
     double v = 0.0, n = 0.0;
     if (D.culled) {
-        // the partials of the tile's work items, in item (= chunk) order
-        for (int slot = 0; slot < D.nterms; ++slot) {
-            const int p = slot * tpad + g;
-            const int tile = p / kCTile, loc = p - tile * kCTile;
-            const int ni = D.tile_items[tile];
-            const size_t f = (size_t)D.tile_first[tile] * kCTile + loc;
-            double s = 0.0, m = 0.0;
-            int i = 0;
-            for (; i + 4 <= ni; i += 4) {  // four items' loads in flight, adds in order
-                double pv[4];
-                float nv[4];
+        // the partials of the tile's work items, in item (= chunk) order; the
+        // terms' streams read side by side, four items at a time
+        const double* qp[3];
+        const float* qn[3];
+        int ni[3], nmax = 0;
 #pragma unroll
-                for (int u = 0; u < 4; ++u) {
-                    pv[u] = D.part[f + (size_t)(i + u) * kCTile];
-                    nv[u] = D.part_norm[f + (size_t)(i + u) * kCTile];
-                }
-#pragma unroll
-                for (int u = 0; u < 4; ++u) {
-                    s += pv[u];
-                    m += (double)nv[u];
-                }
+        for (int slot = 0; slot < 3; ++slot) {
+            ni[slot] = 0;
+            qp[slot] = D.part;
+            qn[slot] = D.part_norm;
+            if (slot < D.nterms) {
+                const int p = slot * tpad + g;
+                const int tile = p / kCTile, loc = p - tile * kCTile;
+                ni[slot] = D.tile_items[tile];
+                const size_t f = (size_t)D.tile_first[tile] * kCTile + loc;
+                qp[slot] = D.part + f;
+                qn[slot] = D.part_norm + f;
+                nmax = max(nmax, ni[slot]);
             }
-            for (; i < ni; ++i) {
-                s += D.part[f + (size_t)i * kCTile];
-                m += (double)D.part_norm[f + (size_t)i * kCTile];
-            }
-            v = slot == 0 ? s : v - s;
-            n += m;
         }
+        double s[3] = {0.0, 0.0, 0.0}, m[3] = {0.0, 0.0, 0.0};
+        for (int i = 0; i < nmax; i += 4) {
+            double pv[3][4];
+            float nv[3][4];
+#pragma unroll
+            for (int slot = 0; slot < 3; ++slot)
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const bool on = i + u < ni[slot];
+                    pv[slot][u] = on ? qp[slot][(size_t)(i + u) * kCTile] : 0.0;
+                    nv[slot][u] = on ? qn[slot][(size_t)(i + u) * kCTile] : 0.f;
+                }
+#pragma unroll
+            for (int slot = 0; slot < 3; ++slot)
+#pragma unroll
+                for (int u = 0; u < 4; ++u)
+                    if (i + u < ni[slot]) {
+                        s[slot] += pv[slot][u];
+                        m[slot] += (double)nv[slot][u];
+                    }
+        }
+        v = s[0] - s[1] - s[2];
+        n = m[0] + m[1] + m[2];
         const int target = D.tperm[g];
         D.Vt[target] = D.prefactor * v;
         D.Nt[target] = D.prefactor * n;
@@ -1036,13 +1050,13 @@ __host__ __device__ __forceinline__ CullArgs cull_args(const Dev& D) {
     C.warp_targets = 64 * kCRP;
     C.hist = D.chist;
     C.order = D.corder;
+    C.done = D.item_count + 2;
     return C;
 }
 __global__ void __launch_bounds__(CH) k_chunk_boxes(Dev D) {
     chunk_boxes_body(pair_args(D), cull_args(D), (int)blockIdx.x);
 }
 __global__ void __launch_bounds__(kCullThreads) k_cull(Dev D) { cull_body(cull_args(D), (int)blockIdx.x); }
-__global__ void __launch_bounds__(1024) k_order_items(Dev D) { order_items_body(cull_args(D)); }
 __global__ void k_tscatter(Dev D) { tscatter_body(D, LGM_THREAD_INDEX); }
 __global__ void k_trank(Dev D) { trank_body(D, LGM_THREAD_INDEX); }
 __global__ void __launch_bounds__(kGuardThreads) k_guard(Dev D) {
@@ -1108,24 +1122,22 @@ __global__ void kb_tested_pairs(const Dev* R, const int* list, int n, unsigned l
         atomicAdd(out, (unsigned long long)dyn[0] * CH * (unsigned long long)dyn[1]);
     }
 }
-// offs[i] = work items of culled replicas list[0 .. i-1], i <= n (one block)
-__global__ void __launch_bounds__(1024) kb_item_offsets(const Dev* R, const int* list, int n,
-                                                        int32_t* offs) {
-    for (int i = (int)threadIdx.x; i <= n; i += (int)blockDim.x)
-        offs[i] = i < n ? *R[list[i]].item_count : 0;
-    __syncthreads();
-    block_exclusive_scan(offs, n + 1);
-    if (threadIdx.x == 0) offs[n + 1] = 0;  // the next item to take (ProblemList::work)
-}
-// order[] = all culled replicas' items (numbered as ProblemList numbers them)
-// by decreasing cost, from the batch's cost histogram.  One block.
-__global__ void __launch_bounds__(1024) kb_order_items(ProblemList L, const int32_t* hist,
-                                                       int32_t* order) {
+// One block, after the culls: offs[i] = work items of culled replicas
+// list[0 .. i-1] (i <= n) and offs[n + 1] = 0, the next item to take
+// (ProblemList::work); then order[] = all those items, numbered as
+// ProblemList numbers them, by decreasing cost (the batch's histogram).
+__global__ void __launch_bounds__(1024) kb_item_order(ProblemList L, const Dev* R,
+                                                      const int32_t* hist, int32_t* offs,
+                                                      int32_t* order) {
     __shared__ int s_off[kCostBuckets];
-    const int total = L.count();
+    const int n = L.n;
+    for (int i = (int)threadIdx.x; i <= n; i += (int)blockDim.x)
+        offs[i] = i < n ? *R[L.list[i]].item_count : 0;
     for (int b = (int)threadIdx.x; b < kCostBuckets; b += (int)blockDim.x) s_off[b] = hist[b];
     __syncthreads();
+    block_exclusive_scan(offs, n + 1);
     if (threadIdx.x == 0) {
+        offs[n + 1] = 0;
         int run = 0;
         for (int b = kCostBuckets - 1; b >= 0; --b) {
             const int h = s_off[b];
@@ -1134,6 +1146,7 @@ __global__ void __launch_bounds__(1024) kb_order_items(ProblemList L, const int3
         }
     }
     __syncthreads();
+    const int total = L.count();
     for (int g = (int)threadIdx.x; g < total; g += (int)blockDim.x) {
         int prob, local;
         L.resolve(g, prob, local);  // L.order is null here: g's own item
@@ -1646,15 +1659,14 @@ using KPairFn = void (*)(PairArgs);
 
 using KCulledFn = void (*)(PairArgs, CullArgs);
 KCulledFn kmc_pair_culled(int gauss) {
-    return gauss
-               ? &pair_kernel_culled_ws<1, 0, kCNW, kCRP, kSUB, kCStages, kCMinBlocks, true, true>
-               : &pair_kernel_culled_ws<0, 0, kCNW, kCRP, kSUB, kCStages, kCMinBlocks, true, true>;
+    return gauss ? &pair_kernel_culled_ws<1, 0, kCNW, kCRP, kSUB, kCStages, kCMinBlocks, true>
+                 : &pair_kernel_culled_ws<0, 0, kCNW, kCRP, kSUB, kCStages, kCMinBlocks, true>;
 }
 size_t kmc_culled_smem(int tab_k) { return ws_smem_bytes(kCStages, tab_k, 4); }
 
 // the culled replicas of a batch (point charges), one persistent launch
 constexpr auto kBatchCulled =
-    &pair_kernel_culled_ws_list<kCNW, kCRP, kSUB, kCStages, kCMinBlocks, true, true>;
+    &pair_kernel_culled_ws_list<kCNW, kCRP, kSUB, kCStages, kCMinBlocks, true>;
 
 KPairFn kmc_pair(int gauss, int sorted = 1) {
     if (sorted)
@@ -1686,7 +1698,6 @@ lgm_status enqueue_step(lgm_kmc* k) {
         if (D.culled) {
             k_chunk_boxes<<<D.src_cap / CH, CH, 0, st>>>(D);
             k_cull<<<k->cull_tiles, kCullThreads, 0, st>>>(D);
-            k_order_items<<<1, 1024, 0, st>>>(D);
             kmc_pair_culled(D.gauss)<<<k->cull_grid, kCThreads, kmc_culled_smem(A.tab_k), st>>>(
                 A, cull_args(D));
         } else {
@@ -1899,7 +1910,7 @@ static lgm_status kmc_create_impl(const lgm_params* pin, int32_t device, uint32_
         DA(D.cbox, src_chunks); DA(D.gbox, (size_t)src_chunks * kGroupsPerChunk);
         DA(D.live, (size_t)k->cull_tiles * src_chunks);
         DA(D.items, (size_t)k->cull_tiles * D.max_items);
-        DA(D.item_count, 2); DA(D.tile_first, k->cull_tiles); DA(D.tile_items, k->cull_tiles);
+        DA(D.item_count, 3); DA(D.tile_first, k->cull_tiles); DA(D.tile_items, k->cull_tiles);
         DA(D.chist, kCostBuckets); DA(D.corder, (size_t)k->cull_tiles * D.max_items);
     }
     DA(D.Vt, 2 * ncap); DA(D.Nt, 2 * ncap);
@@ -2349,10 +2360,9 @@ lgm_status enqueue_batch_pair(lgm_kmc_batch* b, cudaStream_t st) {
         const int n = (int)b->culled.size();
         kb_chunk_boxes<<<b->nb_box, CH, 0, st>>>(b->d_reps, b->map_box);
         kb_cull<<<b->nb_cull, kCullThreads, 0, st>>>(b->d_reps, b->map_cull);
-        kb_item_offsets<<<1, 1024, 0, st>>>(b->d_reps, b->d_culled, n, b->d_coffs);
-        kb_order_items<<<1, 1024, 0, st>>>(
-            ProblemList{b->d_cpargs, b->d_cargs, b->d_culled, b->d_coffs, n, nullptr},
-            b->d_chist, b->d_corder);
+        kb_item_order<<<1, 1024, 0, st>>>(
+            ProblemList{b->d_cpargs, b->d_cargs, b->d_culled, b->d_coffs, n, nullptr}, b->d_reps,
+            b->d_chist, b->d_coffs, b->d_corder);
         kBatchCulled<<<b->cull_grid, kCThreads, kmc_culled_smem(0), st>>>(
             ProblemList{b->d_cpargs, b->d_cargs, b->d_culled, b->d_coffs, n, b->d_corder});
     }
