@@ -70,7 +70,7 @@ lgm_status grow_host(lgm_ctx* c, T** p, size_t* cap, size_t need) {
 
 // ---- prep kernels ---------------------------------------------------------
 
-// Source records (see lgm_pairs.cuh) in spatial order.  The sources were
+// Source records (see lgm_pairs.cuh) in spatial order (prep_records).  The sources were
 // counted into bins by lattice cell (bins_both) and scattered by bin
 // (scatter_both, in no particular order inside a bin); slot j of that scatter
 // takes its final place here: the bin's start plus its rank inside the bin by
@@ -96,13 +96,13 @@ __device__ __forceinline__ void source_record(int sj, int qj, int X, int XY, int
     qq[dst] = make_float2(qf, qf);
 }
 
-__global__ void prep_sources_sorted(const int32_t* __restrict__ s, const int32_t* __restrict__ q,
-                                    int n, int n_pad, const int32_t* __restrict__ key,
-                                    const int32_t* __restrict__ tmp,
-                                    const int32_t* __restrict__ bins_end, int X, int Y, int XY,
-                                    int volume, float4* __restrict__ geo,
-                                    float2* __restrict__ qq, unsigned* err) {
-    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void prep_source(const int j, const int32_t* __restrict__ s,
+                                            const int32_t* __restrict__ q, int n, int n_pad,
+                                            const int32_t* __restrict__ key,
+                                            const int32_t* __restrict__ tmp,
+                                            const int32_t* __restrict__ bins_end, int X, int Y,
+                                            int XY, int volume, float4* __restrict__ geo,
+                                            float2* __restrict__ qq, unsigned* err) {
     if (j >= n_pad) return;
     if (j >= n) {
         geo[2 * j] = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -128,13 +128,15 @@ __global__ void prep_sources_sorted(const int32_t* __restrict__ s, const int32_t
 // ones only), each block t_pad long.  A left image is the direct sum at
 // x' = -1 - x (distance x_i + x_j + 1, cubicgrid.cpp:117-120); a right image
 // at x' = 2X - 1 - x.  all_sites != 0: target g is lattice site g (kernel 1).
-__global__ void prep_targets(const int32_t* __restrict__ ts, int t, int t_pad, int all_sites,
-                             unsigned terms, int X, int Y, int XY, int volume, int shift,
-                             const int32_t* __restrict__ tkey, const int32_t* __restrict__ ttmp,
-                             const int32_t* __restrict__ bins_end, int32_t* __restrict__ perm,
-                             float4* __restrict__ tgt, unsigned* err) {
-    const int j = blockIdx.x * blockDim.x + threadIdx.x;  // scatter slot
-    if (j >= t_pad) return;
+__device__ __forceinline__ void prep_target(const int j, const int32_t* __restrict__ ts, int t,
+                                            int t_pad, int all_sites, unsigned terms, int X,
+                                            int Y, int XY, int volume, int shift,
+                                            const int32_t* __restrict__ tkey,
+                                            const int32_t* __restrict__ ttmp,
+                                            const int32_t* __restrict__ bins_end,
+                                            int32_t* __restrict__ perm, float4* __restrict__ tgt,
+                                            unsigned* err) {
+    if (j >= t_pad) return;  // j: the scatter slot
     // The target scattered to slot j goes to physical slot g: its bin's start
     // plus its rank inside the bin by index (perm[g] = target).  A target's
     // sum is split into the work items of its tile (the culled tiles), so its
@@ -182,6 +184,27 @@ __global__ void prep_targets(const int32_t* __restrict__ ts, int t, int t_pad, i
             make_float4(fx, fy, fz, g < t ? (float)(xp * xp + y * y + z * z) : -1.f);
         ++slot;
     }
+}
+
+// The target records (blocks [0, tb)) and the source records (the blocks
+// after), one launch.
+__global__ void prep_records(int tb, const int32_t* __restrict__ ts, int t, int t_pad,
+                             int all_sites, unsigned terms, int X, int Y, int XY, int volume,
+                             int shift, const int32_t* __restrict__ tkey,
+                             const int32_t* __restrict__ ttmp,
+                             const int32_t* __restrict__ tbins_end, int32_t* __restrict__ perm,
+                             float4* __restrict__ tgt, const int32_t* __restrict__ s,
+                             const int32_t* __restrict__ q, int n, int n_pad,
+                             const int32_t* __restrict__ skey, const int32_t* __restrict__ stmp,
+                             const int32_t* __restrict__ sbins_end, float4* __restrict__ geo,
+                             float2* __restrict__ qq, unsigned* err) {
+    const int b = (int)blockIdx.x;
+    if (b < tb)
+        prep_target(b * (int)blockDim.x + (int)threadIdx.x, ts, t, t_pad, all_sites, terms, X, Y,
+                    XY, volume, shift, tkey, ttmp, tbins_end, perm, tgt, err);
+    else
+        prep_source((b - tb) * (int)blockDim.x + (int)threadIdx.x, s, q, n, n_pad, skey, stmp,
+                    sbins_end, X, Y, XY, volume, geo, qq, err);
 }
 
 // out[perm[g]] = prefactor * (sum over splits of the direct block - image
@@ -253,8 +276,8 @@ __global__ void __launch_bounds__(kScanThreads) bins_scan2(int32_t* __restrict__
 }
 
 // ttmp[slot] = target and stmp[slot] = source: each takes the next slot of
-// its bin, in no particular order inside the bin; rank_targets and
-// prep_sources_sorted fix the final order.
+// its bin, in no particular order inside the bin; prep_target and
+// prep_source (prep_records) fix the final order.
 __global__ void scatter_both(const int32_t* __restrict__ tkey, int t, int32_t* __restrict__ tbins,
                              int32_t* __restrict__ ttmp, const int32_t* __restrict__ skey, int n,
                              int32_t* __restrict__ sbins, int32_t* __restrict__ stmp) {
@@ -264,47 +287,42 @@ __global__ void scatter_both(const int32_t* __restrict__ tkey, int t, int32_t* _
 }
 
 // out[perm[g]] = prefactor * (sum of the item partials of the direct slot -
-// those of the image slots) of target g, for the culled pair sums.  The
-// terms' partial streams are read side by side, four items at a time (up to
-// twelve loads in flight); each stream is still added in item order.
-__global__ void finalize_items(const double* __restrict__ part,
-                               const int* __restrict__ tile_first,
-                               const int* __restrict__ tile_items, int tile_size, int t,
-                               int t_pad, int nterms, double prefactor,
-                               const int32_t* __restrict__ perm, double* __restrict__ out) {
-    const int g = blockIdx.x * blockDim.x + threadIdx.x;
-    if (g >= t) return;
-    const double* q[3];
-    int n[3];
-    int nmax = 0;
+// those of the image slots) of target g, for the culled pair sums.  A block
+// of 32 x 3 threads takes 32 targets: warp y sums term slot y's partials of
+// each target in item order, eight items in flight; warp 0 then combines the
+// slots through shared memory.
+__global__ void __launch_bounds__(96) finalize_items(const double* __restrict__ part,
+                                                     const int* __restrict__ tile_first,
+                                                     const int* __restrict__ tile_items,
+                                                     int tile_size, int t, int t_pad, int nterms,
+                                                     double prefactor,
+                                                     const int32_t* __restrict__ perm,
+                                                     double* __restrict__ out) {
+    constexpr int kRows = 8;
+    __shared__ double s_sum[3][32];
+    const int g = blockIdx.x * 32 + (int)threadIdx.x, slot = (int)threadIdx.y;
+    double sum = 0.0;
+    if (g < t && slot < nterms) {
+        const int p = slot * t_pad + g;
+        const int tile = p / tile_size, loc = p - tile * tile_size;
+        const int n = tile_items[tile];
+        const double* q = part + (size_t)tile_first[tile] * tile_size + loc;
+        for (int i = 0; i < n; i += kRows) {
+            double v[kRows];
 #pragma unroll
-    for (int slot = 0; slot < 3; ++slot) {
-        n[slot] = 0;
-        q[slot] = part;
-        if (slot < nterms) {
-            const int p = slot * t_pad + g;
-            const int tile = p / tile_size, loc = p - tile * tile_size;
-            n[slot] = tile_items[tile];
-            q[slot] = part + (size_t)tile_first[tile] * tile_size + loc;
-            nmax = max(nmax, n[slot]);
+            for (int u = 0; u < kRows; ++u)
+                v[u] = i + u < n ? q[(size_t)(i + u) * tile_size] : 0.0;
+#pragma unroll
+            for (int u = 0; u < kRows; ++u)
+                if (i + u < n) sum += v[u];
         }
     }
-    double sum[3] = {0.0, 0.0, 0.0};
-    for (int i = 0; i < nmax; i += 4) {
-        double v[3][4];
-#pragma unroll
-        for (int slot = 0; slot < 3; ++slot)
-#pragma unroll
-            for (int u = 0; u < 4; ++u)
-                v[slot][u] = i + u < n[slot] ? q[slot][(size_t)(i + u) * tile_size] : 0.0;
-#pragma unroll
-        for (int slot = 0; slot < 3; ++slot)
-#pragma unroll
-            for (int u = 0; u < 4; ++u)
-                if (i + u < n[slot]) sum[slot] += v[slot][u];
+    s_sum[slot][threadIdx.x] = sum;
+    __syncthreads();
+    if (slot == 0 && g < t) {
+        const int x = (int)threadIdx.x;
+        out[perm[g]] = prefactor * (s_sum[0][x] - s_sum[1][x] - s_sum[2][x]);
     }
-    const double total = sum[0] - sum[1] - sum[2];
-    out[perm[g]] = prefactor * total;
 }
 
 __global__ void fill_zero(double* out, int t) {
@@ -502,12 +520,11 @@ lgm_status prep(lgm_ctx* c, unsigned terms, const int32_t* d_src, const int32_t*
     scatter_both<<<tb, 256, 0, st>>>(c->d_key, t, c->d_bins, c->d_ttmp, c->d_skey, n, c->d_sbins,
                                      c->d_stmp);
     LGM_CUDA(c, cudaGetLastError());
-    prep_targets<<<(sh.t_pad + 255) / 256, 256, 0, st>>>(
-        d_tgt_site, t, sh.t_pad, all_sites, terms, cf.grid_x, cf.grid_y, c->xy, c->volume,
-        c->cell_shift, c->d_key, c->d_ttmp, c->d_bins, c->d_perm, c->d_tgt, c->d_err);
-    prep_sources_sorted<<<(sh.n_pad + 255) / 256, 256, 0, st>>>(
-        d_src, d_q, n, sh.n_pad, c->d_skey, c->d_stmp, c->d_sbins, cf.grid_x, cf.grid_y, c->xy,
-        c->volume, c->d_geo, c->d_qq, c->d_err);
+    const int ptb = (sh.t_pad + 255) / 256, psb = (sh.n_pad + 255) / 256;
+    prep_records<<<ptb + psb, 256, 0, st>>>(
+        ptb, d_tgt_site, t, sh.t_pad, all_sites, terms, cf.grid_x, cf.grid_y, c->xy, c->volume,
+        c->cell_shift, c->d_key, c->d_ttmp, c->d_bins, c->d_perm, c->d_tgt, d_src, d_q, n,
+        sh.n_pad, c->d_skey, c->d_stmp, c->d_sbins, c->d_geo, c->d_qq, c->d_err);
     LGM_CUDA(c, cudaGetLastError());
     return LGM_OK;
 }
@@ -715,13 +732,13 @@ lgm_status launch_potentials(lgm_ctx* c, int kind, unsigned terms, const int32_t
         finalize<<<(t + 255) / 256, 256, 0, st>>>(c->d_part, splits, sh.t_phys, t, sh.t_pad,
                                                    sh.nterms, cf.electrostatic_prefactor,
                                                    c->d_perm, d_out);
-        c->last.kernel_launches = 7;  // bins, scan, scatter, two preps, pair, finalize
+        c->last.kernel_launches = 6;  // bins, scan, scatter, records, pair, finalize
     } else {
         const Variant& V = kVariants[c->last.variant];
-        finalize_items<<<(t + 255) / 256, 256, 0, st>>>(
+        finalize_items<<<(t + 31) / 32, dim3(32, 3), 0, st>>>(
             c->d_part, c->d_tile_first, c->d_tile_items, V.nt * 2 * V.rp, t, sh.t_pad, sh.nterms,
             cf.electrostatic_prefactor, c->d_perm, d_out);
-        c->last.kernel_launches = 9;  // bins, scan, scatter, two preps, boxes, cull, pair, finalize
+        c->last.kernel_launches = 8;  // bins, scan, scatter, records, boxes, cull, pair, finalize
     }
     LGM_CUDA(c, cudaGetLastError());
     c->last.pairs_tested = (int64_t)sh.nterms * t * (int64_t)n;

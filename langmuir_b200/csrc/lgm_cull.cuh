@@ -168,21 +168,38 @@ __device__ __forceinline__ void chunk_boxes_body(const PairArgs& A, const CullAr
 // classes; the order inside a class is arbitrary and changes no sum: an
 // item's partials go to its own slot whichever CTA computes it).  One block;
 // the reads bypass L1 (the other blocks' writes are in L2).
+// s_off[b] = the items of cost classes above b, from the class counts in
+// s_off (an exclusive scan in decreasing class order); every thread of a
+// block of at least kCostBuckets threads calls it.
+__device__ __forceinline__ void cost_offsets(int* s_off) {
+    static_assert(kCostBuckets == 256, "one bucket per thread of eight warps");
+    __shared__ int s_w[kCostBuckets / 32];
+    const int t = (int)threadIdx.x, lane = t & 31;
+    const int b = kCostBuckets - 1 - t;  // thread t takes class 255 - t
+    const int v = t < kCostBuckets ? s_off[b] : 0;
+    int inc = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o) inc += y;
+    }
+    if (t < kCostBuckets && lane == 31) s_w[t >> 5] = inc;
+    __syncthreads();
+    if (t < kCostBuckets) {
+        int before = 0;
+        for (int w = 0; w < (t >> 5); ++w) before += s_w[w];
+        s_off[b] = before + inc - v;
+    }
+    __syncthreads();
+}
+
 __device__ __forceinline__ void order_items_body(const CullArgs& C) {
     __shared__ int s_off[kCostBuckets];
     const int nit = __ldcg(C.item_count);
     for (int b = (int)threadIdx.x; b < kCostBuckets; b += (int)blockDim.x)
         s_off[b] = __ldcg(&C.hist[b]);
     __syncthreads();
-    if (threadIdx.x == 0) {
-        int run = 0;
-        for (int b = kCostBuckets - 1; b >= 0; --b) {
-            const int h = s_off[b];
-            s_off[b] = run;
-            run += h;
-        }
-    }
-    __syncthreads();
+    cost_offsets(s_off);
     for (int g = (int)threadIdx.x; g < nit; g += (int)blockDim.x) {
         const int c = min(__ldcg(&C.items[g]).w, kCostBuckets - 1);
         C.order[atomicAdd(&s_off[c], 1)] = g;

@@ -1020,6 +1020,51 @@ __device__ __forceinline__ void compact_inject_body(const Dev& D, int* warp_sums
 __global__ void k_choose(Dev D) { choose_body(D, LGM_THREAD_INDEX); }
 __global__ void k_pack(Dev D) { pack_body(D, LGM_THREAD_INDEX); }
 __global__ void k_finalize(Dev D) { finalize_body(D, LGM_THREAD_INDEX); }
+// finalize_body's culled branch with a block of 32 x 3 threads per 32
+// targets: warp y sums term slot y's item partials (and norms) in item order,
+// eight items in flight, and warp 0 combines the slots -- the same sums in
+// the same order, three times the threads.
+__global__ void __launch_bounds__(96) k_finalize_culled(Dev D) {
+    constexpr int kRows = 8;
+    __shared__ double s_v[3][32], s_n[3][32];
+    const int t = 2 * (D.cnt[I_NE] + D.cnt[I_NH]);
+    const int tpad = D.cnt[I_TPAD];
+    const int x = (int)threadIdx.x, slot = (int)threadIdx.y;
+    const int g = (int)blockIdx.x * 32 + x;
+    double sv = 0.0, sn = 0.0;
+    if (g < t && slot < D.nterms) {
+        const int p = slot * tpad + g;
+        const int tile = p / kCTile, loc = p - tile * kCTile;
+        const int ni = D.tile_items[tile];
+        const size_t f = (size_t)D.tile_first[tile] * kCTile + loc;
+        for (int i = 0; i < ni; i += kRows) {
+            double pv[kRows];
+            float nv[kRows];
+#pragma unroll
+            for (int u = 0; u < kRows; ++u) {
+                const bool on = i + u < ni;
+                pv[u] = on ? D.part[f + (size_t)(i + u) * kCTile] : 0.0;
+                nv[u] = on ? D.part_norm[f + (size_t)(i + u) * kCTile] : 0.f;
+            }
+#pragma unroll
+            for (int u = 0; u < kRows; ++u)
+                if (i + u < ni) {
+                    sv += pv[u];
+                    sn += (double)nv[u];
+                }
+        }
+    }
+    s_v[slot][x] = sv;
+    s_n[slot][x] = sn;
+    __syncthreads();
+    if (slot == 0 && g < t) {
+        const double v = s_v[0][x] - s_v[1][x] - s_v[2][x];
+        const double n = s_n[0][x] + s_n[1][x] + s_n[2][x];
+        const int target = D.tperm[g];
+        D.Vt[target] = D.prefactor * v;
+        D.Nt[target] = D.prefactor * n;
+    }
+}
 __global__ void k_decide(Dev D) { decide_body(D, LGM_THREAD_INDEX); }
 __global__ void k_tbins_zero(Dev D) { tbins_zero_body(D, LGM_THREAD_INDEX); }
 __global__ void k_tbins(Dev D) { tbins_body(D, LGM_THREAD_INDEX); }
@@ -1136,16 +1181,8 @@ __global__ void __launch_bounds__(1024) kb_item_order(ProblemList L, const Dev* 
     for (int b = (int)threadIdx.x; b < kCostBuckets; b += (int)blockDim.x) s_off[b] = hist[b];
     __syncthreads();
     block_exclusive_scan(offs, n + 1);
-    if (threadIdx.x == 0) {
-        offs[n + 1] = 0;
-        int run = 0;
-        for (int b = kCostBuckets - 1; b >= 0; --b) {
-            const int h = s_off[b];
-            s_off[b] = run;
-            run += h;
-        }
-    }
-    __syncthreads();
+    if (threadIdx.x == 0) offs[n + 1] = 0;
+    cost_offsets(s_off);
     const int total = L.count();
     for (int g = (int)threadIdx.x; g < total; g += (int)blockDim.x) {
         int prob, local;
@@ -1704,7 +1741,8 @@ lgm_status enqueue_step(lgm_kmc* k) {
             kmc_pair(D.gauss, D.sorted)<<<dim3(k->pair_tiles, D.splits), kNT,
                                           pair_smem_bytes(A.tab_k), st>>>(A);
         }
-        k_finalize<<<(2 * nc + blk - 1) / blk, blk, 0, st>>>(D);
+        if (D.culled) k_finalize_culled<<<(2 * nc + 31) / 32, dim3(32, 3), 0, st>>>(D);
+        else k_finalize<<<(2 * nc + blk - 1) / blk, blk, 0, st>>>(D);
     }
     k_decide<<<(nc + blk - 1) / blk, blk, 0, st>>>(D);
     if (D.coulomb) k_guard<<<2 * k->sm_count, kGuardThreads, 0, st>>>(D);
