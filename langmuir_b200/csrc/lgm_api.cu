@@ -441,8 +441,8 @@ const Variant kVariants[] = {
     // of 72 registers was 36% slower); the next source's r^2 ahead of each
     // vote (PIPE) measured the same
     LGM_VARIANT_CULL_WS(4, 2, 32, 2, 4, 4, true), LGM_VARIANT_CULL_WS(4, 2, 32, 2, 4, 4, false),
-    LGM_VARIANT_CULL_WS(2, 2, 32, 2, 4, 6, true), LGM_VARIANT_CULL_WS(3, 2, 32, 2, 4, 5, true),
-    LGM_VARIANT_CULL_WS(4, 2, 32, 1, 4, 4, true), LGM_VARIANT_CULL_WS(4, 2, 32, 2, 6, 4, true),
+    LGM_VARIANT_CULL_WS(2, 2, 32, 2, 4, 6, true), LGM_VARIANT_CULL_WS(4, 2, 32, 3, 4, 4, false),
+    LGM_VARIANT_CULL_WS(4, 2, 32, 1, 4, 4, true), LGM_VARIANT_CULL_WS(4, 2, 32, 4, 4, 4, false),
 };
 constexpr int kNumVariants = (int)(sizeof(kVariants) / sizeof(kVariants[0]));
 static_assert(kNumVariants <= (int)(sizeof(lgm_ctx::bps) / sizeof(lgm_ctx::bps[0])),
