@@ -606,14 +606,20 @@ def load_labels(path, device="cuda"):
 
 def run_pipeline(n_train=4096, n_holdout=512, n_candidates=100000, steps=50000, burn_in=10000,
                  members=4, epochs=300, top=256, seed=0, labels_cache="", lr=4e-3, log=print,
-                 **model_kw):
+                 holdout_steps=None, train_steps=None, **model_kw):
     """Generate, label, train, evaluate on kMC-labelled holdouts, screen
     candidates and re-simulate the picks.  Returns a report dict.  With
     ``labels_cache`` the training and holdout labels are read from (or, the
-    first time, written to) that prefix."""
+    first time, written to) that prefix.  ``train_steps`` / ``holdout_steps``
+    (default ``steps``) set the length of the training and holdout label runs:
+    a label's noise falls as the square root of its window, and the holdout
+    labels are the yardstick of the surrogate's error."""
     import os
+    train_steps = train_steps or steps
+    holdout_steps = holdout_steps or steps
     rep = {"config": dict(n_train=n_train, n_holdout=n_holdout, n_candidates=n_candidates,
-                          steps=steps, burn_in=burn_in, members=members, epochs=epochs, top=top,
+                          steps=steps, train_steps=train_steps, holdout_steps=holdout_steps,
+                          burn_in=burn_in, members=members, epochs=epochs, top=top,
                           seed=seed, size=128, lr=lr, **model_kw)}
     sync = torch.cuda.synchronize
     cached = labels_cache and os.path.exists(labels_cache + "_train.npz")
@@ -623,15 +629,16 @@ def run_pipeline(n_train=4096, n_holdout=512, n_candidates=100000, steps=50000, 
     else:
         ph_tr, _, _ = grf_morphologies(n_train, seed=seed * 10 + 1)
         ph_ho, _, _ = grf_morphologies(n_holdout, seed=seed * 10 + 2)
-        lab_tr = kmc_labels(ph_tr, steps=steps, burn_in=burn_in, seed=seed + 1, replica0=0)
-        log(f"labels: {n_train} morphologies x {steps} steps in {lab_tr['seconds']:.1f} s")
-        lab_ho = kmc_labels(ph_ho, steps=steps, burn_in=burn_in, seed=seed + 1, replica0=1 << 24)
+        lab_tr = kmc_labels(ph_tr, steps=train_steps, burn_in=burn_in, seed=seed + 1, replica0=0)
+        log(f"labels: {n_train} morphologies x {train_steps} steps in {lab_tr['seconds']:.1f} s")
+        lab_ho = kmc_labels(ph_ho, steps=holdout_steps, burn_in=burn_in, seed=seed + 1,
+                            replica0=1 << 24)
         if labels_cache:
             save_labels(labels_cache + "_train.npz", ph_tr, lab_tr)
             save_labels(labels_cache + "_holdout.npz", ph_ho, lab_ho)
     rep["labels_from_cache"] = bool(cached)
     rep["kmc"] = {"train_seconds": lab_tr["seconds"], "holdout_seconds": lab_ho["seconds"],
-                  "morphs_per_s": n_train / lab_tr["seconds"],
+                  "morphs_per_s": n_train / lab_tr["seconds"] * train_steps / steps,
                   "efficiency_percentiles": np.percentile(lab_tr["efficiency"], [5, 50, 95]).tolist(),
                   "generated_median": float(np.median(lab_tr["generated"]))}
     y_tr = np.stack([lab_tr["current"], lab_tr["efficiency"]], 1)
@@ -687,7 +694,11 @@ def main(argv=None):
     ap.add_argument("--train", type=int, default=4096)
     ap.add_argument("--holdout", type=int, default=512)
     ap.add_argument("--candidates", type=int, default=100000)
-    ap.add_argument("--steps", type=int, default=50000)
+    ap.add_argument("--steps", type=int, default=50000,
+                    help="kMC steps per label (the screened picks; the cost screening is set "
+                         "against)")
+    ap.add_argument("--train-steps", type=int, default=0, help="training labels (0: --steps)")
+    ap.add_argument("--holdout-steps", type=int, default=0, help="holdout labels (0: --steps)")
     ap.add_argument("--burn-in", type=int, default=10000)
     ap.add_argument("--members", type=int, default=4)
     ap.add_argument("--epochs", type=int, default=300)
@@ -700,7 +711,8 @@ def main(argv=None):
     a = ap.parse_args(argv)
     rep = run_pipeline(a.train, a.holdout, a.candidates, a.steps, a.burn_in, a.members, a.epochs,
                        seed=a.seed, labels_cache=a.labels_cache, lr=a.lr, tta=a.tta,
-                       ramp=a.ramp)
+                       ramp=a.ramp, holdout_steps=a.holdout_steps or None,
+                       train_steps=a.train_steps or None)
     arrays = rep.pop("_arrays")
     model = rep.pop("_model")
     text = json.dumps(rep, indent=1)
