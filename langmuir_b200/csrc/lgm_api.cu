@@ -251,7 +251,9 @@ __global__ void bins_both(const int32_t* __restrict__ ts, int t, int all_sites,
                           int shift, int cells_x, int cells_y,
                           const int32_t* __restrict__ cell_rank, int ncells,
                           int32_t* __restrict__ tkey, int32_t* __restrict__ tbins,
-                          int32_t* __restrict__ skey, int32_t* __restrict__ sbins) {
+                          int32_t* __restrict__ skey, int32_t* __restrict__ sbins,
+                          int32_t* __restrict__ done) {
+    __shared__ int s_last;
     const int g = blockIdx.x * blockDim.x + threadIdx.x;
     if (g < t) {
         const int b = cell_bin(all_sites ? g : ts[g], X, Y, XY, volume, shift, cells_x, cells_y,
@@ -265,15 +267,21 @@ __global__ void bins_both(const int32_t* __restrict__ ts, int t, int all_sites,
         skey[g] = b;
         atomicAdd(&sbins[b], 1);
     }
+    // The last block to finish turns both counts into exclusive scans in
+    // place (the counts were added by atomics in L2; this block read none of
+    // them before, and fences after seeing the others done).
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        s_last = atomicAdd(done, 1) == (int)gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    block_exclusive_scan(tbins, ncells + 1);
+    block_exclusive_scan(sbins, ncells + 1);
 }
 
-// Exclusive scans of the target bins (block 0) and the source bins (block 1)
-// in place, nb entries each.
-constexpr int kScanThreads = 1024;
-__global__ void __launch_bounds__(kScanThreads) bins_scan2(int32_t* __restrict__ tbins,
-                                                           int32_t* __restrict__ sbins, int nb) {
-    block_exclusive_scan(blockIdx.x == 0 ? tbins : sbins, nb);
-}
 
 // ttmp[slot] = target and stmp[slot] = source: each takes the next slot of
 // its bin, in no particular order inside the bin; prep_target and
@@ -523,13 +531,13 @@ lgm_status prep(lgm_ctx* c, unsigned terms, const int32_t* d_src, const int32_t*
     if ((s = grow_device(c, &c->d_skey, &c->skey_cap, (size_t)n)) != LGM_OK) return s;
     if ((s = grow_device(c, &c->d_stmp, &c->stmp_cap, (size_t)n)) != LGM_OK) return s;
     // targets and sources in spatial order: bins, scans, scatters
-    LGM_CUDA(c, cudaMemsetAsync(c->d_bins, 0, sizeof(int32_t) * 2 * c->bins_stride, st));
+    // both bin arrays and the bins_both block counter behind them, one memset
+    LGM_CUDA(c, cudaMemsetAsync(c->d_bins, 0, sizeof(int32_t) * (2 * c->bins_stride + 4), st));
     const int tb = (std::max(t, n) + 255) / 256;
     bins_both<<<tb, 256, 0, st>>>(d_tgt_site, t, all_sites, d_src, n, cf.grid_x, cf.grid_y, c->xy,
                                   c->volume, c->cell_shift, c->cells_x, c->cells_y,
                                   c->d_cell_rank, c->ncells, c->d_key, c->d_bins, c->d_skey,
-                                  c->d_sbins);
-    bins_scan2<<<2, kScanThreads, 0, st>>>(c->d_bins, c->d_sbins, c->ncells + 1);
+                                  c->d_sbins, c->d_bins + 2 * c->bins_stride);
     scatter_both<<<tb, 256, 0, st>>>(c->d_key, t, c->d_bins, c->d_ttmp, c->d_skey, n, c->d_sbins,
                                      c->d_stmp);
     LGM_CUDA(c, cudaGetLastError());
@@ -752,7 +760,7 @@ lgm_status launch_potentials(lgm_ctx* c, int kind, unsigned terms, const int32_t
         finalize<<<(t + 255) / 256, 256, 0, st>>>(c->d_part, splits, sh.t_phys, t, sh.t_pad,
                                                    sh.nterms, cf.electrostatic_prefactor,
                                                    c->d_perm, d_out);
-        c->last.kernel_launches = 6;  // bins, scan, scatter, records, pair, finalize
+        c->last.kernel_launches = 5;  // bins (+ scan), scatter, records, pair, finalize
     } else {
         const Variant& V = kVariants[c->last.variant];
         if (V.ws) {
@@ -764,7 +772,7 @@ lgm_status launch_potentials(lgm_ctx* c, int kind, unsigned terms, const int32_t
                 c->d_part, c->d_tile_first, c->d_tile_items, V.nt * 2 * V.rp, t, sh.t_pad,
                 sh.nterms, cf.electrostatic_prefactor, c->d_perm, d_out);
         }
-        c->last.kernel_launches = 8;  // bins, scan, scatter, records, boxes, cull, pair, finalize
+        c->last.kernel_launches = 7;  // bins (+ scan), scatter, records, boxes, cull, pair, finalize
     }
     LGM_CUDA(c, cudaGetLastError());
     c->last.pairs_tested = (int64_t)sh.nterms * t * (int64_t)n;
@@ -1042,7 +1050,8 @@ lgm_status lgm_create(const lgm_config* cfg, int32_t device, lgm_ctx** out) {
         c->ncells = (int)rank.size();
         c->bins_stride = (c->ncells + 2 + 3) / 4 * 4;
         if ((e = cudaMalloc(&c->d_cell_rank, sizeof(int32_t) * rank.size())) != cudaSuccess ||
-            (e = cudaMalloc(&c->d_bins, sizeof(int32_t) * 2 * c->bins_stride)) != cudaSuccess ||
+            (e = cudaMalloc(&c->d_bins, sizeof(int32_t) * (2 * c->bins_stride + 4))) !=
+                cudaSuccess ||
             (e = cudaMalloc(&c->d_item_count, 3 * sizeof(int32_t))) != cudaSuccess ||
             (e = cudaMalloc(&c->d_cost_hist, kCostBuckets * sizeof(int32_t))) != cudaSuccess)
             return bail("cudaMalloc", e);
