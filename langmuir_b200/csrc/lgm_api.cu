@@ -333,19 +333,6 @@ __global__ void __launch_bounds__(96) finalize_items(const double* __restrict__ 
     }
 }
 
-// out[perm[g]] = prefactor * (direct - left image - right image) from the
-// per-target item sums the warp-specialised culled kernel wrote.
-__global__ void finalize_sums(const double* __restrict__ tsum, int t, int t_pad, int nterms,
-                              double prefactor, const int32_t* __restrict__ perm,
-                              double* __restrict__ out) {
-    const int g = blockIdx.x * blockDim.x + threadIdx.x;
-    if (g >= t) return;
-    const double s0 = tsum[g];
-    const double s1 = nterms > 1 ? tsum[t_pad + g] : 0.0;
-    const double s2 = nterms > 2 ? tsum[2 * t_pad + g] : 0.0;
-    out[perm[g]] = prefactor * (s0 - s1 - s2);
-}
-
 __global__ void fill_zero(double* out, int t) {
     const int g = blockIdx.x * blockDim.x + threadIdx.x;
     if (g < t) out[g] = 0.0;
@@ -615,13 +602,6 @@ lgm_status launch_culled(lgm_ctx* c, int kind, int v, const Shape& sh, const Pai
     C.hist = c->d_cost_hist;
     C.order = c->d_order;
     C.done = c->d_item_count + 2;
-    if (V.ws) {  // the pair kernel adds each tile's item partials itself
-        if ((s = grow_device(c, &c->d_seg_done, &c->seg_cap, (size_t)tiles * kMaxSegments)) != LGM_OK)
-            return s;
-        if ((s = grow_device(c, &c->d_tsum, &c->tsum_cap, (size_t)sh.t_phys)) != LGM_OK) return s;
-        C.seg_done = c->d_seg_done;
-        C.tsum = c->d_tsum;
-    }
     if (c->counting) {
         LGM_CUDA(c, cudaMemsetAsync(c->d_examined, 0, sizeof(unsigned long long), st));
         C.examined = c->d_examined;
@@ -763,15 +743,9 @@ lgm_status launch_potentials(lgm_ctx* c, int kind, unsigned terms, const int32_t
         c->last.kernel_launches = 5;  // bins (+ scan), scatter, records, pair, finalize
     } else {
         const Variant& V = kVariants[c->last.variant];
-        if (V.ws) {
-            finalize_sums<<<(t + 255) / 256, 256, 0, st>>>(c->d_tsum, t, sh.t_pad, sh.nterms,
-                                                           cf.electrostatic_prefactor, c->d_perm,
-                                                           d_out);
-        } else {
-            finalize_items<<<(t + 31) / 32, dim3(32, 3), 0, st>>>(
-                c->d_part, c->d_tile_first, c->d_tile_items, V.nt * 2 * V.rp, t, sh.t_pad,
-                sh.nterms, cf.electrostatic_prefactor, c->d_perm, d_out);
-        }
+        finalize_items<<<(t + 31) / 32, dim3(32, 3), 0, st>>>(
+            c->d_part, c->d_tile_first, c->d_tile_items, V.nt * 2 * V.rp, t, sh.t_pad, sh.nterms,
+            cf.electrostatic_prefactor, c->d_perm, d_out);
         c->last.kernel_launches = 7;  // bins (+ scan), scatter, records, boxes, cull, pair, finalize
     }
     LGM_CUDA(c, cudaGetLastError());
@@ -1107,7 +1081,7 @@ lgm_status lgm_destroy(lgm_ctx* c) {
                         c->d_skey,  c->d_stmp,       c->d_cbox,       c->d_gbox,
                         c->d_live,  c->d_items,      c->d_tile_first, c->d_tile_items,
                         c->d_item_count, c->d_examined, c->d_rtab64,  c->d_gtab64,
-                        c->d_cost_hist,  c->d_order, c->d_seg_done, c->d_tsum};
+                        c->d_cost_hist,  c->d_order};
     for (void* p : dev_ptrs)
         if (p) cudaFree(p);
     void* host_ptrs[] = {c->h_s, c->h_q, c->h_t, c->h_o, c->h_err};

@@ -61,8 +61,6 @@ struct lgm_ctx {
                                                       // tiles culled
     int32_t* d_cost_hist = nullptr;                   // [kCostBuckets] items per cost
     int32_t* d_order = nullptr; size_t order_cap = 0; // items by decreasing cost
-    int32_t* d_seg_done = nullptr; size_t seg_cap = 0;  // items done per (tile, warp segment)
-    double* d_tsum = nullptr; size_t tsum_cap = 0;      // per physical target: its item sums
 
     // Pinned host staging for the host-buffer entry points.
     int32_t* h_s = nullptr;   size_t hs_cap = 0;

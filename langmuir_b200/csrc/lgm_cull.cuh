@@ -118,14 +118,6 @@ struct CullArgs {
     int warp_targets = 0;
     int* hist = nullptr;
     int* order = nullptr;
-    // Optional (null: off) in-kernel reduction of the warp-specialised kernel:
-    // per (tile, warp segment) the items done so far (zeroed by the cull); the
-    // warp that finishes a segment's last item sums the segment's item
-    // partials, in item order, into tsum (and tnorm) per physical target.  The
-    // cull zeroes tsum for tiles without items.
-    int* seg_done = nullptr;
-    double* tsum = nullptr;
-    double* tnorm = nullptr;
     // with order: culled tiles so far (zeroed by chunk_boxes block 0); the
     // cull's last block to finish writes order[]
     int* done = nullptr;
@@ -245,9 +237,6 @@ __device__ __forceinline__ void cull_body(const CullArgs& C, const int tile) {
         if (C.order) cull_last_orders(C);
         return;
     }
-    if (C.seg_done && tid < kMaxSegments)
-        if (tid < C.tile_size / (C.warp_targets > 0 ? C.warp_targets : C.tile_size))
-            C.seg_done[tile * kMaxSegments + tid] = 0;
     // The boxes of the tile's warp segments (one segment: the whole tile),
     // one warp of this block per segment; the tile box is their union.
     const int seg_len = C.warp_targets > 0 ? C.warp_targets : C.tile_size;
@@ -312,13 +301,6 @@ __device__ __forceinline__ void cull_body(const CullArgs& C, const int tile) {
         C.tile_first[tile] = base;
         C.tile_items[tile] = nit;
         s_base = base;
-    }
-    if (nit == 0 && C.tsum) {  // no item will sum this tile's targets
-        const int p1 = min((tile + 1) * C.tile_size, t_phys);
-        for (int p = tile * C.tile_size + tid; p < p1; p += kCullThreads) {
-            C.tsum[p] = 0.0;
-            if (C.tnorm) C.tnorm[p] = 0.0;
-        }
     }
     __syncthreads();
     for (int i = tid; i < nit; i += kCullThreads) {
@@ -728,54 +710,6 @@ __device__ __forceinline__ void pair_items_culled(const PS& P) {
     }
 }
 
-// After a warp wrote its partials of one item of tile `tile`: count the item
-// for the warp's segment, and if it was the segment's last, add the
-// segment's partials over all the tile's items, in item order, into
-// C.tsum / C.tnorm (every writer fences before counting; the last one fences
-// after, and reads past L1).
-template <bool NORM, int RP, int TS>
-__device__ __forceinline__ void segment_sum(const PairArgs& A, const CullArgs& C, const int tile,
-                                            const int warp, const int base, const int t_phys,
-                                            const int lane) {
-    int last = 0;
-    __threadfence();  // this lane's partials before the count
-    __syncwarp();
-    if (lane == 0)
-        last = atomicAdd(&C.seg_done[tile * kMaxSegments + warp], 1) == C.tile_items[tile] - 1;
-    if (!__shfl_sync(0xffffffffu, last, 0)) return;
-    __threadfence();
-    const int ni = C.tile_items[tile];
-    const size_t f = (size_t)C.tile_first[tile] * TS;
-#pragma unroll
-    for (int q = 0; q < 2 * RP; ++q) {
-        const int p = base + warp * (64 * RP) + q * 32 + lane;
-        if (p >= t_phys) continue;
-        const double* src = A.part + f + (p - base);
-        double sv = 0.0, sn = 0.0;
-        int i = 0;
-        for (; i + 4 <= ni; i += 4) {  // four items' loads in flight, adds in order
-            double v[4];
-            float w[4];
-#pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                v[u] = __ldcg(src + (size_t)(i + u) * TS);
-                if (NORM) w[u] = __ldcg(A.part_norm + f + (p - base) + (size_t)(i + u) * TS);
-            }
-#pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                sv += v[u];
-                if (NORM) sn += (double)w[u];
-            }
-        }
-        for (; i < ni; ++i) {
-            sv += __ldcg(src + (size_t)i * TS);
-            if (NORM) sn += (double)__ldcg(A.part_norm + f + (p - base) + (size_t)i * TS);
-        }
-        C.tsum[p] = sv;
-        if (NORM) C.tnorm[p] = sn;
-    }
-}
-
 // Dynamic shared memory of the warp-specialised kernel: S stages of source
 // records and group boxes, their item records and full/empty barriers, then
 // the table (elem bytes per entry; tab_k = 0 and elem = 0: none).
@@ -950,7 +884,6 @@ __device__ __forceinline__ void pair_items_culled_ws(const PS& P) {
                     if (NORM) A.part_norm[(size_t)m.x * TS + (p - base)] = nrm[NORM ? q : 0];
                 }
             }
-            if (C.seg_done) segment_sum<NORM, RP, TS>(A, C, base / TS, warp, base, t_phys, lane);
         }
     }
 }

@@ -139,8 +139,6 @@ struct Dev {
                                                     // culled
     int32_t *chist, *corder;  // item costs' histogram and the largest-first order
                               // (corder null for a batch's replicas: the batch's)
-    int32_t* seg_done;        // items done per (tile, warp segment)
-    double *tsum, *tnorm;     // per physical target: its item partials' sum and norm
     int src_cap;   // source records capacity (multiple of CH)
     int tpad_cap;  // per-term target block capacity
     unsigned* err;
@@ -338,15 +336,49 @@ __device__ __forceinline__ void finalize_body(const Dev& D, const int g) {
     if (g >= t) return;
     double v = 0.0, n = 0.0;
     if (D.culled) {
-        // the per-target sums of the tile's item partials, added in item
-        // (= chunk) order by the pair kernel
-        const double s0 = D.tsum[g], m0 = D.tnorm[g];
-        const double s1 = D.nterms > 1 ? D.tsum[tpad + g] : 0.0;
-        const double m1 = D.nterms > 1 ? D.tnorm[tpad + g] : 0.0;
-        const double s2 = D.nterms > 2 ? D.tsum[2 * tpad + g] : 0.0;
-        const double m2 = D.nterms > 2 ? D.tnorm[2 * tpad + g] : 0.0;
-        v = s0 - s1 - s2;
-        n = m0 + m1 + m2;
+        // the partials of the tile's work items, in item (= chunk) order; the
+        // terms' streams read side by side, four items at a time
+        const double* qp[3];
+        const float* qn[3];
+        int ni[3], nmax = 0;
+#pragma unroll
+        for (int slot = 0; slot < 3; ++slot) {
+            ni[slot] = 0;
+            qp[slot] = D.part;
+            qn[slot] = D.part_norm;
+            if (slot < D.nterms) {
+                const int p = slot * tpad + g;
+                const int tile = p / kCTile, loc = p - tile * kCTile;
+                ni[slot] = D.tile_items[tile];
+                const size_t f = (size_t)D.tile_first[tile] * kCTile + loc;
+                qp[slot] = D.part + f;
+                qn[slot] = D.part_norm + f;
+                nmax = max(nmax, ni[slot]);
+            }
+        }
+        double s[3] = {0.0, 0.0, 0.0}, m[3] = {0.0, 0.0, 0.0};
+        for (int i = 0; i < nmax; i += 4) {
+            double pv[3][4];
+            float nv[3][4];
+#pragma unroll
+            for (int slot = 0; slot < 3; ++slot)
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const bool on = i + u < ni[slot];
+                    pv[slot][u] = on ? qp[slot][(size_t)(i + u) * kCTile] : 0.0;
+                    nv[slot][u] = on ? qn[slot][(size_t)(i + u) * kCTile] : 0.f;
+                }
+#pragma unroll
+            for (int slot = 0; slot < 3; ++slot)
+#pragma unroll
+                for (int u = 0; u < 4; ++u)
+                    if (i + u < ni[slot]) {
+                        s[slot] += pv[slot][u];
+                        m[slot] += (double)nv[slot][u];
+                    }
+        }
+        v = s[0] - s[1] - s[2];
+        n = m[0] + m[1] + m[2];
         const int target = D.tperm[g];
         D.Vt[target] = D.prefactor * v;
         D.Nt[target] = D.prefactor * n;
@@ -988,6 +1020,51 @@ __device__ __forceinline__ void compact_inject_body(const Dev& D, int* warp_sums
 __global__ void k_choose(Dev D) { choose_body(D, LGM_THREAD_INDEX); }
 __global__ void k_pack(Dev D) { pack_body(D, LGM_THREAD_INDEX); }
 __global__ void k_finalize(Dev D) { finalize_body(D, LGM_THREAD_INDEX); }
+// finalize_body's culled branch with a block of 32 x 3 threads per 32
+// targets: warp y sums term slot y's item partials (and norms) in item order,
+// eight items in flight, and warp 0 combines the slots -- the same sums in
+// the same order, three times the threads.
+__global__ void __launch_bounds__(96) k_finalize_culled(Dev D) {
+    constexpr int kRows = 8;
+    __shared__ double s_v[3][32], s_n[3][32];
+    const int t = 2 * (D.cnt[I_NE] + D.cnt[I_NH]);
+    const int tpad = D.cnt[I_TPAD];
+    const int x = (int)threadIdx.x, slot = (int)threadIdx.y;
+    const int g = (int)blockIdx.x * 32 + x;
+    double sv = 0.0, sn = 0.0;
+    if (g < t && slot < D.nterms) {
+        const int p = slot * tpad + g;
+        const int tile = p / kCTile, loc = p - tile * kCTile;
+        const int ni = D.tile_items[tile];
+        const size_t f = (size_t)D.tile_first[tile] * kCTile + loc;
+        for (int i = 0; i < ni; i += kRows) {
+            double pv[kRows];
+            float nv[kRows];
+#pragma unroll
+            for (int u = 0; u < kRows; ++u) {
+                const bool on = i + u < ni;
+                pv[u] = on ? D.part[f + (size_t)(i + u) * kCTile] : 0.0;
+                nv[u] = on ? D.part_norm[f + (size_t)(i + u) * kCTile] : 0.f;
+            }
+#pragma unroll
+            for (int u = 0; u < kRows; ++u)
+                if (i + u < ni) {
+                    sv += pv[u];
+                    sn += (double)nv[u];
+                }
+        }
+    }
+    s_v[slot][x] = sv;
+    s_n[slot][x] = sn;
+    __syncthreads();
+    if (slot == 0 && g < t) {
+        const double v = s_v[0][x] - s_v[1][x] - s_v[2][x];
+        const double n = s_n[0][x] + s_n[1][x] + s_n[2][x];
+        const int target = D.tperm[g];
+        D.Vt[target] = D.prefactor * v;
+        D.Nt[target] = D.prefactor * n;
+    }
+}
 __global__ void k_decide(Dev D) { decide_body(D, LGM_THREAD_INDEX); }
 __global__ void k_tbins_zero(Dev D) { tbins_zero_body(D, LGM_THREAD_INDEX); }
 __global__ void k_tbins(Dev D) { tbins_body(D, LGM_THREAD_INDEX); }
@@ -1019,9 +1096,6 @@ __host__ __device__ __forceinline__ CullArgs cull_args(const Dev& D) {
     C.hist = D.chist;
     C.order = D.corder;
     C.done = D.item_count + 2;
-    C.seg_done = D.seg_done;  // the pair kernel adds each tile's item partials itself
-    C.tsum = D.tsum;
-    C.tnorm = D.tnorm;
     return C;
 }
 __global__ void __launch_bounds__(CH) k_chunk_boxes(Dev D) {
@@ -1667,7 +1741,8 @@ lgm_status enqueue_step(lgm_kmc* k) {
             kmc_pair(D.gauss, D.sorted)<<<dim3(k->pair_tiles, D.splits), kNT,
                                           pair_smem_bytes(A.tab_k), st>>>(A);
         }
-        k_finalize<<<(2 * nc + blk - 1) / blk, blk, 0, st>>>(D);
+        if (D.culled) k_finalize_culled<<<(2 * nc + 31) / 32, dim3(32, 3), 0, st>>>(D);
+        else k_finalize<<<(2 * nc + blk - 1) / blk, blk, 0, st>>>(D);
     }
     k_decide<<<(nc + blk - 1) / blk, blk, 0, st>>>(D);
     if (D.coulomb) k_guard<<<2 * k->sm_count, kGuardThreads, 0, st>>>(D);
@@ -1875,8 +1950,6 @@ static lgm_status kmc_create_impl(const lgm_params* pin, int32_t device, uint32_
         DA(D.items, (size_t)k->cull_tiles * D.max_items);
         DA(D.item_count, 3); DA(D.tile_first, k->cull_tiles); DA(D.tile_items, k->cull_tiles);
         DA(D.chist, kCostBuckets); DA(D.corder, (size_t)k->cull_tiles * D.max_items);
-        DA(D.seg_done, (size_t)k->cull_tiles * kMaxSegments);
-        DA(D.tsum, tphys_cap); DA(D.tnorm, tphys_cap);
     }
     DA(D.Vt, 2 * ncap); DA(D.Nt, 2 * ncap);
     DA(D.err, 1);
