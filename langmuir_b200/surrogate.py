@@ -663,8 +663,10 @@ def run_pipeline(n_train=4096, n_holdout=512, n_candidates=100000, steps=50000, 
     sync()
     screen_s = time.perf_counter() - t0
     picks = torch.unique(torch.cat([top_idx, unc_idx])).cpu()
-    lab_pk = kmc_labels(cand[picks.to(cand.device)], steps=steps, burn_in=burn_in, seed=seed + 1,
-                        replica0=1 << 25)
+    # the picks are labelled as the holdouts are, so that both judge the
+    # surrogate on labels of one protocol
+    lab_pk = kmc_labels(cand[picks.to(cand.device)], steps=holdout_steps, burn_in=burn_in,
+                        seed=seed + 1, replica0=1 << 25)
     pk_mean = cmean[picks.to(cmean.device)].cpu().numpy()
     is_top = torch.isin(picks, top_idx.cpu()).numpy()
     is_unc = torch.isin(picks, unc_idx.cpu()).numpy()
