@@ -200,9 +200,19 @@ __device__ __forceinline__ void order_items_body(const CullArgs& C) {
         s_off[b] = __ldcg(&C.hist[b]);
     __syncthreads();
     cost_offsets(s_off);
-    for (int g = (int)threadIdx.x; g < nit; g += (int)blockDim.x) {
-        const int c = min(__ldcg(&C.items[g]).w, kCostBuckets - 1);
-        C.order[atomicAdd(&s_off[c], 1)] = g;
+    const int nt = (int)blockDim.x;
+    for (int g0 = (int)threadIdx.x; g0 < nit; g0 += 4 * nt) {  // four item loads in flight
+        int c[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int g = g0 + u * nt;
+            c[u] = g < nit ? min(__ldcg(&C.items[g]).w, kCostBuckets - 1) : 0;
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int g = g0 + u * nt;
+            if (g < nit) C.order[atomicAdd(&s_off[c[u]], 1)] = g;
+        }
     }
 }
 

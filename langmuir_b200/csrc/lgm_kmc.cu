@@ -1182,12 +1182,24 @@ __global__ void __launch_bounds__(1024) kb_item_order(ProblemList L, const Dev* 
     __syncthreads();
     block_exclusive_scan(offs, n + 1);
     if (threadIdx.x == 0) offs[n + 1] = 0;
-    cost_offsets(s_off);
-    const int total = L.count();
+    // the offsets in shared memory for the items' replica searches (up to
+    // kOffsInShared replicas; more search global memory)
+    constexpr int kOffsInShared = 2048;
+    __shared__ int s_offs[kOffsInShared];
+    const bool in_smem = n + 1 <= kOffsInShared;
+    if (in_smem)
+        for (int i = (int)threadIdx.x; i <= n; i += (int)blockDim.x) s_offs[i] = offs[i];
+    cost_offsets(s_off);  // (its barriers also publish s_offs)
+    const int* so = in_smem ? s_offs : offs;
+    const int total = so[n];
     for (int g = (int)threadIdx.x; g < total; g += (int)blockDim.x) {
-        int prob, local;
-        L.resolve(g, prob, local);  // L.order is null here: g's own item
-        const int c = min(L.C(prob).items[local].w, kCostBuckets - 1);
+        int lo = 0, hi = n;  // the last replica whose first item is at or before g
+        while (hi - lo > 1) {
+            const int mid = (lo + hi) >> 1;
+            if (so[mid] <= g) lo = mid;
+            else hi = mid;
+        }
+        const int c = min(L.C(L.list[lo]).items[g - so[lo]].w, kCostBuckets - 1);
         order[atomicAdd(&s_off[c], 1)] = g;
     }
 }
