@@ -435,22 +435,22 @@ const Variant kVariants[] = {
     LGM_VARIANT(128, 4, 32),       LGM_VARIANT(256, 2, 16),       LGM_VARIANT_SKIP(128, 4, 32),
     LGM_VARIANT_SKIP(128, 4, 16),  LGM_VARIANT_SKIP(128, 2, 32),  LGM_VARIANT_SKIP(64, 4, 32),
     LGM_VARIANT_SKIP(64, 3, 32),   LGM_VARIANT_SKIP(128, 3, 32),
-    LGM_VARIANT_CULL(128, 4, 32, 2), LGM_VARIANT_CULL(128, 4, 32, 1),
-    LGM_VARIANT_CULL(128, 4, 32, 4), LGM_VARIANT_CULL(128, 2, 32, 2),
-    LGM_VARIANT_CULL(64, 4, 32, 2),  LGM_VARIANT_CULL(128, 4, 16, 2),
-    LGM_VARIANT_CULL(64, 2, 32, 2),
+    LGM_VARIANT_CULL(128, 4, 16, 2), LGM_VARIANT_CULL(128, 4, 16, 1),
+    LGM_VARIANT_CULL(128, 4, 16, 4), LGM_VARIANT_CULL(128, 2, 16, 2),
+    LGM_VARIANT_CULL(64, 4, 16, 2),  LGM_VARIANT_CULL(128, 4, 8, 2),
+    LGM_VARIANT_CULL(64, 2, 16, 2),
     // warp-specialised: (target warps, target pairs, run, chunks per item,
     // stages, CTAs per SM); the register bound counts the producer warp
-    LGM_VARIANT_CULL_WS(4, 4, 32, 2, 4, 4, false), LGM_VARIANT_CULL_WS(8, 2, 32, 2, 4, 3, false),
-    LGM_VARIANT_CULL_WS(4, 2, 32, 2, 4, 5, false), LGM_VARIANT_CULL_WS(7, 2, 32, 2, 4, 3, false),
-    LGM_VARIANT_CULL_WS(4, 4, 32, 4, 4, 4, false),
+    LGM_VARIANT_CULL_WS(4, 4, 16, 2, 4, 4, false), LGM_VARIANT_CULL_WS(8, 2, 16, 2, 4, 3, false),
+    LGM_VARIANT_CULL_WS(4, 2, 16, 2, 4, 5, false), LGM_VARIANT_CULL_WS(7, 2, 16, 2, 4, 3, false),
+    LGM_VARIANT_CULL_WS(4, 4, 16, 4, 4, 4, false),
     // 4 CTAs of 4 target warps and 2 target pairs per thread measured best on
     // the 256x256x16 and 128x128x64 workloads (96 registers; the 5-CTA bound
     // of 72 registers was 36% slower); the next source's r^2 ahead of each
     // vote (PIPE) measured the same
-    LGM_VARIANT_CULL_WS(4, 2, 32, 2, 4, 4, true), LGM_VARIANT_CULL_WS(4, 2, 32, 2, 4, 4, false),
-    LGM_VARIANT_CULL_WS(2, 2, 32, 2, 4, 6, true), LGM_VARIANT_CULL_WS(4, 2, 32, 3, 4, 4, false),
-    LGM_VARIANT_CULL_WS(4, 2, 32, 1, 4, 4, true), LGM_VARIANT_CULL_WS(4, 2, 32, 4, 4, 4, false),
+    LGM_VARIANT_CULL_WS(4, 2, 16, 2, 4, 4, true), LGM_VARIANT_CULL_WS(4, 2, 16, 2, 4, 4, false),
+    LGM_VARIANT_CULL_WS(2, 2, 16, 2, 4, 6, true), LGM_VARIANT_CULL_WS(4, 2, 16, 3, 4, 4, false),
+    LGM_VARIANT_CULL_WS(4, 2, 16, 1, 4, 4, true), LGM_VARIANT_CULL_WS(4, 2, 16, 4, 4, 4, false),
 };
 constexpr int kNumVariants = (int)(sizeof(kVariants) / sizeof(kVariants[0]));
 static_assert(kNumVariants <= (int)(sizeof(lgm_ctx::bps) / sizeof(lgm_ctx::bps[0])),

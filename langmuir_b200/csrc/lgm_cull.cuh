@@ -33,8 +33,8 @@
 
 namespace lgm {
 
-constexpr int kGroup = 32;                    // sources per group box
-constexpr int kGroupsPerChunk = CH / kGroup;  // 4
+constexpr int kGroup = 16;                    // sources per group box
+constexpr int kGroupsPerChunk = CH / kGroup;  // 8
 constexpr int kCullThreads = 256;             // threads of the cull kernel
 constexpr int kMaxItemsPerTile = 32;          // items a tile's chunk list is cut into, at most
 constexpr int kMaxSegments = 16;              // warp target segments of a tile, at most
@@ -123,7 +123,7 @@ struct CullArgs {
     int* done = nullptr;
 };
 
-// One block of CH threads per source chunk: group and chunk boxes of the
+// One block of CH threads per source chunk: group (kGroup) and chunk boxes of the
 // records with a nonzero charge.  Block 0 also zeroes the item counter for
 // the cull that follows.
 __device__ __forceinline__ void chunk_boxes_body(const PairArgs& A, const CullArgs& C,
@@ -146,12 +146,21 @@ __device__ __forceinline__ void chunk_boxes_body(const PairArgs& A, const CullAr
     const int x = (int)(-0.5f * g0.x), y = (int)(-0.5f * g0.z), z = (int)(-0.5f * g1.x);
     int xl = valid ? x : 32767, yl = valid ? y : 32767, zl = valid ? z : 32767;
     int xh = valid ? x : -32768, yh = valid ? y : -32768, zh = valid ? z : -32768;
-    warp_box(xl, yl, zl, xh, yh, zh);
-    const int warp = (int)threadIdx.x >> 5;
-    if ((threadIdx.x & 31) == 0) {
+    // min and max over each aligned group of kGroup lanes
+#pragma unroll
+    for (int o = kGroup / 2; o > 0; o >>= 1) {
+        xl = min(xl, __shfl_xor_sync(0xffffffffu, xl, o));
+        yl = min(yl, __shfl_xor_sync(0xffffffffu, yl, o));
+        zl = min(zl, __shfl_xor_sync(0xffffffffu, zl, o));
+        xh = max(xh, __shfl_xor_sync(0xffffffffu, xh, o));
+        yh = max(yh, __shfl_xor_sync(0xffffffffu, yh, o));
+        zh = max(zh, __shfl_xor_sync(0xffffffffu, zh, o));
+    }
+    const int grp = (int)threadIdx.x / kGroup;
+    if ((threadIdx.x % kGroup) == 0) {
         const Box b = make_box(xl, yl, zl, xh, yh, zh);
-        C.gbox[chunk * kGroupsPerChunk + warp] = b;
-        s_g[warp] = b;
+        C.gbox[chunk * kGroupsPerChunk + grp] = b;
+        s_g[grp] = b;
     }
     __syncthreads();
     if (threadIdx.x == 0) {
