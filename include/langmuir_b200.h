@@ -198,11 +198,14 @@ typedef struct lgm_peaks {
 } lgm_peaks;
 lgm_status lgm_probe_peaks(int32_t device, lgm_peaks* out);
 
-/* Failure-detection self test (no reference counterpart): a kernel whose
- * bulk-copy pipeline stages are armed but never filled runs the pair kernels'
- * bounded wait with `wait_limit` tries (1 .. 2^20) and their drain; the wait
- * runs out, the device error word reports it, and the call returns
- * LGM_ERR_TIMEOUT with the context still usable.  Nothing faults or hangs. */
+/* Failure-detection self test (no reference counterpart): kernels whose
+ * bulk-copy pipeline stages are armed but never filled -- the two-stage
+ * pipeline of the classic tiles and the four-stage ring of the
+ * warp-specialised culled kernel -- run the pair kernels' bounded waits with
+ * `wait_limit` tries (1 .. 2^20) and their drains; the waits run out, the
+ * device error word reports it, and the call returns LGM_ERR_TIMEOUT with the
+ * context still usable (LGM_ERR_STATE if either kernel reported anything
+ * else).  Nothing faults or hangs. */
 lgm_status lgm_selftest_timeout(int32_t device, int32_t wait_limit);
 
 /* Launch statistics of the last pair-sum launch on the context. */

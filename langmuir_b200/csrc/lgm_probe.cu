@@ -151,6 +151,31 @@ __global__ void __launch_bounds__(128) selftest_wait_timeout(unsigned* err, int 
     if (!__syncthreads_and(mine) && threadIdx.x == 0) lgm::mbar_drain_stages(bars, 0u, 2u, limit);
 }
 
+// The same for the warp-specialised kernels' ring of four stages: all four
+// are armed, no copy comes, every target warp's bounded wait on stage 0 runs
+// out and leaves as a warp (the warp-uniform vote of pair_items_culled_ws),
+// and the producer thread waits (bounded) for the ring's four phases before
+// leaving (mbar_drain_ring).
+__global__ void __launch_bounds__(160) selftest_ring_timeout(unsigned* err, int limit) {
+    constexpr int S = 4;
+    __shared__ __align__(8) uint64_t full[S];
+    const int warp = (int)threadIdx.x >> 5;
+    if (threadIdx.x == 0) {
+        for (int i = 0; i < S; ++i) {
+            lgm::mbar_init(&full[i], 1);
+        }
+        lgm::fence_mbar_init();
+        for (int i = 0; i < S; ++i) lgm::mbar_arrive_expect_tx(&full[i], 5184u);
+    }
+    __syncthreads();
+    if (warp == 4) {  // the producer warp
+        if ((threadIdx.x & 31) == 0) lgm::mbar_drain_ring(full, S, 0u, (uint32_t)S, limit);
+        return;
+    }
+    if (!__all_sync(0xffffffffu, lgm::mbar_wait_bounded(&full[0], 0u, err, limit))) return;
+    atomicOr(err, lgm::DEVERR_STATE);  // a stage that no copy filled completed
+}
+
 }  // namespace
 
 extern "C" lgm_status lgm_selftest_timeout(int32_t device, int32_t wait_limit) {
@@ -166,13 +191,23 @@ extern "C" lgm_status lgm_selftest_timeout(int32_t device, int32_t wait_limit) {
     if (cudaMemset(d_err, 0, sizeof(unsigned)) != cudaSuccess) {
         st = LGM_ERR_CUDA;
     } else {
+        // the two-stage pipeline, then the four-stage ring: each must report
+        // the timeout and nothing else
+        unsigned h_ring = 0;
         selftest_wait_timeout<<<2, 128>>>(d_err, wait_limit);
-        if (cudaGetLastError() != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess ||
-            cudaMemcpy(&h_err, d_err, sizeof h_err, cudaMemcpyDeviceToHost) != cudaSuccess)
+        bool ok = cudaGetLastError() == cudaSuccess && cudaDeviceSynchronize() == cudaSuccess &&
+                  cudaMemcpy(&h_err, d_err, sizeof h_err, cudaMemcpyDeviceToHost) == cudaSuccess &&
+                  cudaMemset(d_err, 0, sizeof(unsigned)) == cudaSuccess;
+        if (ok) {
+            selftest_ring_timeout<<<2, 160>>>(d_err, wait_limit);
+            ok = cudaGetLastError() == cudaSuccess && cudaDeviceSynchronize() == cudaSuccess &&
+                 cudaMemcpy(&h_ring, d_err, sizeof h_ring, cudaMemcpyDeviceToHost) == cudaSuccess;
+        }
+        if (!ok)
             st = LGM_ERR_CUDA;
-        else if (h_err & lgm::DEVERR_TIMEOUT)
+        else if (h_err == lgm::DEVERR_TIMEOUT && h_ring == lgm::DEVERR_TIMEOUT)
             st = LGM_ERR_TIMEOUT;
-        else if (h_err)
+        else
             st = LGM_ERR_STATE;
     }
     cudaFree(d_err);
