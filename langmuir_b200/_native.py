@@ -109,6 +109,7 @@ SIGNATURES = {
                                                    ctypes.c_int32, _vp, _vp]),
     "lgm_last_launch": (ctypes.c_int32, [_vp, ctypes.POINTER(LaunchInfo)]),
     "lgm_set_timing": (ctypes.c_int32, [_vp, ctypes.c_int32]),
+    "lgm_set_launch_overlap": (ctypes.c_int32, [_vp, ctypes.c_int32]),
     "lgm_set_counting": (ctypes.c_int32, [_vp, ctypes.c_int32]),
     "lgm_probe_peaks": (ctypes.c_int32, [ctypes.c_int32, _vp]),
     "lgm_selftest_timeout": (ctypes.c_int32, [ctypes.c_int32, ctypes.c_int32]),

@@ -122,12 +122,18 @@ class Coulomb:
             N.lib().lgm_variant_items(v, ctypes.byref(k), ctypes.byref(st))
             out.append({"threads": a.value, "target_pairs": b.value, "run": c.value,
                         "warp_skip": bool(f.value & 1), "culled": bool(f.value & 2),
-                        "warp_specialised": bool(f.value & 4), "chunks_per_item": k.value,
+                        "warp_specialised": bool(f.value & 4),
+                        "warp_items": bool(f.value & 8), "chunks_per_item": k.value,
                         "stages": st.value})
         return out
 
     def set_timing(self, on: bool = True):
         self._check(N.lib().lgm_set_timing(self._h, int(bool(on))))
+
+    def set_launch_overlap(self, on: bool = True):
+        """Programmatic stream serialization between the call's kernels
+        (lgm_set_launch_overlap); on by default, the same results either way."""
+        self._check(N.lib().lgm_set_launch_overlap(self._h, int(bool(on))))
 
     def set_counting(self, on: bool = True):
         """Culled pair sums count the pairs they examine (lgm_set_counting)."""

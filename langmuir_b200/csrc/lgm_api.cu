@@ -198,6 +198,8 @@ __global__ void prep_records(int tb, const int32_t* __restrict__ ts, int t, int 
                              const int32_t* __restrict__ skey, const int32_t* __restrict__ stmp,
                              const int32_t* __restrict__ sbins_end, float4* __restrict__ geo,
                              float2* __restrict__ qq, unsigned* err) {
+    pdl_wait();
+    pdl_trigger();
     const int b = (int)blockIdx.x;
     if (b < tb)
         prep_target(b * (int)blockDim.x + (int)threadIdx.x, ts, t, t_pad, all_sites, terms, X, Y,
@@ -207,12 +209,25 @@ __global__ void prep_records(int tb, const int32_t* __restrict__ ts, int t, int 
                     sbins_end, X, Y, XY, volume, geo, qq, err);
 }
 
+// The last kernel of a call clears both bin arrays (their last reader,
+// prep_records, has completed), so the next call's bins_both counts into
+// zeros without a memset of its own.  Thread i of the grid (one row of the
+// block) clears entries i, i + stride, ...
+__device__ __forceinline__ void zero_bins(int32_t* __restrict__ bins, int nbins) {
+    const int stride = (int)(gridDim.x * blockDim.x);
+    for (int i = (int)(blockIdx.x * blockDim.x + threadIdx.x); i < nbins; i += stride) bins[i] = 0;
+}
+
 // out[perm[g]] = prefactor * (sum over splits of the direct block - image
 // blocks) of physical slot g.
 __global__ void finalize(const double* __restrict__ part, int splits, int t_phys, int t,
                          int t_pad, int nterms, double prefactor,
-                         const int32_t* __restrict__ perm, double* __restrict__ out) {
+                         const int32_t* __restrict__ perm, double* __restrict__ out,
+                         int32_t* __restrict__ bins, int nbins) {
+    pdl_wait();
+    pdl_trigger();
     const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    zero_bins(bins, nbins);
     if (g >= t) return;
     double total = 0.0;
     for (int slot = 0; slot < nterms; ++slot) {
@@ -254,6 +269,8 @@ __global__ void bins_both(const int32_t* __restrict__ ts, int t, int all_sites,
                           int32_t* __restrict__ skey, int32_t* __restrict__ sbins,
                           int32_t* __restrict__ done) {
     __shared__ int s_last;
+    pdl_wait();
+    pdl_trigger();
     const int g = blockIdx.x * blockDim.x + threadIdx.x;
     if (g < t) {
         const int b = cell_bin(all_sites ? g : ts[g], X, Y, XY, volume, shift, cells_x, cells_y,
@@ -280,6 +297,7 @@ __global__ void bins_both(const int32_t* __restrict__ ts, int t, int all_sites,
     __threadfence();
     block_exclusive_scan(tbins, ncells + 1);
     block_exclusive_scan(sbins, ncells + 1);
+    if (threadIdx.x == 0) *done = 0;  // every block has counted itself: ready for the next call
 }
 
 
@@ -289,6 +307,8 @@ __global__ void bins_both(const int32_t* __restrict__ ts, int t, int all_sites,
 __global__ void scatter_both(const int32_t* __restrict__ tkey, int t, int32_t* __restrict__ tbins,
                              int32_t* __restrict__ ttmp, const int32_t* __restrict__ skey, int n,
                              int32_t* __restrict__ sbins, int32_t* __restrict__ stmp) {
+    pdl_wait();
+    pdl_trigger();
     const int g = blockIdx.x * blockDim.x + threadIdx.x;
     if (g < t) ttmp[atomicAdd(&tbins[tkey[g]], 1)] = g;
     if (g < n) stmp[atomicAdd(&sbins[skey[g]], 1)] = g;
@@ -305,10 +325,14 @@ __global__ void __launch_bounds__(96) finalize_items(const double* __restrict__ 
                                                      int tile_size, int t, int t_pad, int nterms,
                                                      double prefactor,
                                                      const int32_t* __restrict__ perm,
-                                                     double* __restrict__ out) {
+                                                     double* __restrict__ out,
+                                                     int32_t* __restrict__ bins, int nbins) {
     constexpr int kRows = 8;
     __shared__ double s_sum[3][32];
+    pdl_wait();
+    pdl_trigger();
     const int g = blockIdx.x * 32 + (int)threadIdx.x, slot = (int)threadIdx.y;
+    if (slot == 0) zero_bins(bins, nbins);
     double sum = 0.0;
     if (g < t && slot < nterms) {
         const int p = slot * t_pad + g;
@@ -334,6 +358,8 @@ __global__ void __launch_bounds__(96) finalize_items(const double* __restrict__ 
 }
 
 __global__ void fill_zero(double* out, int t) {
+    pdl_wait();
+    pdl_trigger();
     const int g = blockIdx.x * blockDim.x + threadIdx.x;
     if (g < t) out[g] = 0.0;
 }
@@ -349,6 +375,8 @@ pair_kernel_f64(const float4* __restrict__ geo, const float2* __restrict__ qq, i
                 int splits, const float4* __restrict__ tgt, int t_phys, double* __restrict__ part,
                 int c2, int kind, double erffactor) {
     __shared__ int4 s_g[kF64Tile];  // x, y, z, q
+    pdl_wait();
+    pdl_trigger();
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     const int split = blockIdx.y;
     const int j_begin = (int)((long long)split * n_pad / splits);
@@ -386,6 +414,27 @@ pair_kernel_f64(const float4* __restrict__ geo, const float2* __restrict__ qq, i
 
 // ---- launch plumbing --------------------------------------------------------
 
+// Launches a kernel of a call's chain.  With overlap on it carries the
+// programmatic stream serialization attribute: the kernel may be scheduled
+// while the one ahead of it in the stream is still running, and waits for it
+// in pdl_wait() (lgm_device.cuh) before touching memory, so the launch
+// latency between the chain's kernels overlaps the kernel ahead.
+template <typename... P, typename... A>
+cudaError_t launch_chain(bool overlap, void (*k)(P...), dim3 grid, dim3 block, size_t smem,
+                         cudaStream_t st, A... args) {
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cfg.attrs = at;
+    cfg.numAttrs = overlap ? 1 : 0;
+    return cudaLaunchKernelEx(&cfg, k, static_cast<P>(args)...);
+}
+
 using PairFn = void (*)(PairArgs);
 using CulledFn = void (*)(PairArgs, CullArgs);
 
@@ -400,6 +449,7 @@ struct Variant {
     PairFn fn[4];
     CulledFn cfn[4];  // [3]: the FP64-table path (culled variants only)
     int ws = 0;       // warp-specialised culled kernel: its stages (0: not)
+    int wi = 0;       // warp-item culled kernel: stages per warp (0: not)
 };
 #define LGM_VARIANT_S(NT, RP, SUB, SK)                                                    \
     Variant {                                                                             \
@@ -429,6 +479,27 @@ struct Variant {
              &pair_kernel_culled_ws<0, 2, NW, RP, SUB, S, MINB>},                             \
             S                                                                                 \
     }
+// VOTE: sources per warp vote of the MUFU path (0: none; lgm_cull.cuh)
+#define LGM_VARIANT_CULL_WSV(NW, RP, SUB, K, S, MINB, VOTE)                                  \
+    Variant {                                                                                 \
+        NW * 32, RP, SUB, 1, 1, K, {nullptr, nullptr, nullptr, nullptr},                      \
+            {&pair_kernel_culled_ws<0, 0, NW, RP, SUB, S, MINB, false, false, VOTE>,          \
+             &pair_kernel_culled_ws<1, 0, NW, RP, SUB, S, MINB, false, false, VOTE>,          \
+             &pair_kernel_culled_ws<0, 1, NW, RP, SUB, S, MINB>,                              \
+             &pair_kernel_culled_ws<0, 2, NW, RP, SUB, S, MINB>},                             \
+            S                                                                                 \
+    }
+// warp items (lgm_cull.cuh pair_items_warp): NW independent warps per CTA,
+// S stages per warp, at least MINB CTAs per SM
+#define LGM_VARIANT_CULL_WI(NW, RP, SUB, K, S, MINB, VOTE)                                   \
+    Variant {                                                                                 \
+        NW * 32, RP, SUB, 1, 1, K, {nullptr, nullptr, nullptr, nullptr},                      \
+            {&pair_kernel_warp_items<0, 0, NW, RP, SUB, S, MINB, VOTE>,                       \
+             &pair_kernel_warp_items<1, 0, NW, RP, SUB, S, MINB, VOTE>,                       \
+             &pair_kernel_warp_items<0, 1, NW, RP, SUB, S, MINB>,                             \
+             &pair_kernel_warp_items<0, 2, NW, RP, SUB, S, MINB>},                            \
+            0, S                                                                              \
+    }
 const Variant kVariants[] = {
     LGM_VARIANT(128, 4, 16),       LGM_VARIANT(128, 4, 8),        LGM_VARIANT(128, 2, 16),
     LGM_VARIANT(128, 8, 16),       LGM_VARIANT(256, 4, 16),       LGM_VARIANT(64, 4, 16),
@@ -451,13 +522,21 @@ const Variant kVariants[] = {
     LGM_VARIANT_CULL_WS(4, 2, 16, 2, 4, 4, true), LGM_VARIANT_CULL_WS(4, 2, 16, 2, 4, 4, false),
     LGM_VARIANT_CULL_WS(2, 2, 16, 2, 4, 6, true), LGM_VARIANT_CULL_WS(4, 2, 16, 3, 4, 4, false),
     LGM_VARIANT_CULL_WS(4, 2, 16, 1, 4, 4, true), LGM_VARIANT_CULL_WS(4, 2, 16, 4, 4, 4, false),
+    // one vote per 2 or 4 sources, or none
+    LGM_VARIANT_CULL_WSV(4, 2, 16, 2, 4, 4, 2), LGM_VARIANT_CULL_WSV(4, 2, 16, 2, 4, 4, 0),
+    LGM_VARIANT_CULL_WSV(4, 2, 16, 2, 4, 4, 4),
+    // warp items: (warps, target pairs, run, chunks per item, stages per warp,
+    // CTAs per SM, sources per vote)
+    LGM_VARIANT_CULL_WI(4, 2, 16, 2, 2, 5, 2), LGM_VARIANT_CULL_WI(4, 2, 16, 2, 3, 3, 2),
+    LGM_VARIANT_CULL_WI(4, 2, 16, 1, 2, 5, 2), LGM_VARIANT_CULL_WI(2, 2, 16, 2, 3, 7, 2),
 };
 constexpr int kNumVariants = (int)(sizeof(kVariants) / sizeof(kVariants[0]));
 static_assert(kNumVariants <= (int)(sizeof(lgm_ctx::bps) / sizeof(lgm_ctx::bps[0])),
               "lgm_ctx::bps holds every variant");
-// warp-specialised culled, 4 target warps, 2 target pairs, runs of 32, 2
-// chunks per item
-constexpr int kDefaultVariant = 27;
+// warp-specialised culled, 4 target warps, 2 target pairs, runs of 16, 2
+// chunks per item, one vote per 2 sources (2% faster than a vote per source
+// on the 256x256x16 and 128x128x64 workloads, the same bits)
+constexpr int kDefaultVariant = 32;
 
 const void* kernel_of(const Variant& V, int fi) {
     return V.cull ? reinterpret_cast<const void*>(V.cfn[fi])
@@ -469,6 +548,7 @@ const void* kernel_of(const Variant& V, int fi) {
 int variant_threads(const Variant& V) { return V.nt + (V.ws ? 32 : 0); }
 size_t variant_smem(const Variant& V, int fi, int tab_k) {
     if (V.ws) return ws_smem_bytes(V.ws, tab_k, fi == 3 ? 8 : 4);
+    if (V.wi) return wi_smem_bytes(V.nt / 32, V.wi, tab_k, fi == 3 ? 8 : 4);
     return fi == 3 ? pair_smem_bytes64(tab_k) : pair_smem_bytes(tab_k);
 }
 
@@ -517,23 +597,27 @@ lgm_status prep(lgm_ctx* c, unsigned terms, const int32_t* d_src, const int32_t*
     if ((s = grow_device(c, &c->d_ttmp, &c->ttmp_cap, (size_t)t)) != LGM_OK) return s;
     if ((s = grow_device(c, &c->d_skey, &c->skey_cap, (size_t)n)) != LGM_OK) return s;
     if ((s = grow_device(c, &c->d_stmp, &c->stmp_cap, (size_t)n)) != LGM_OK) return s;
-    // targets and sources in spatial order: bins, scans, scatters
-    // both bin arrays and the bins_both block counter behind them, one memset
-    LGM_CUDA(c, cudaMemsetAsync(c->d_bins, 0, sizeof(int32_t) * (2 * c->bins_stride + 4), st));
+    // targets and sources in spatial order: bins, scans, scatters.  Both bin
+    // arrays and the bins_both block counter behind them start at zero: the
+    // last kernel of the previous call cleared them (bins_both's last block
+    // clears the counter), else one memset does.
+    if (!c->bins_clean)
+        LGM_CUDA(c, cudaMemsetAsync(c->d_bins, 0, sizeof(int32_t) * (2 * c->bins_stride + 4), st));
+    c->bins_clean = false;
+    const bool ov = c->overlap;
     const int tb = (std::max(t, n) + 255) / 256;
-    bins_both<<<tb, 256, 0, st>>>(d_tgt_site, t, all_sites, d_src, n, cf.grid_x, cf.grid_y, c->xy,
-                                  c->volume, c->cell_shift, c->cells_x, c->cells_y,
-                                  c->d_cell_rank, c->ncells, c->d_key, c->d_bins, c->d_skey,
-                                  c->d_sbins, c->d_bins + 2 * c->bins_stride);
-    scatter_both<<<tb, 256, 0, st>>>(c->d_key, t, c->d_bins, c->d_ttmp, c->d_skey, n, c->d_sbins,
-                                     c->d_stmp);
-    LGM_CUDA(c, cudaGetLastError());
+    LGM_CUDA(c, launch_chain(ov, bins_both, tb, 256, 0, st, d_tgt_site, t, all_sites, d_src, n,
+                             cf.grid_x, cf.grid_y, c->xy, c->volume, c->cell_shift, c->cells_x,
+                             c->cells_y, c->d_cell_rank, c->ncells, c->d_key, c->d_bins,
+                             c->d_skey, c->d_sbins, c->d_bins + 2 * c->bins_stride));
+    LGM_CUDA(c, launch_chain(ov, scatter_both, tb, 256, 0, st, c->d_key, t, c->d_bins, c->d_ttmp,
+                             c->d_skey, n, c->d_sbins, c->d_stmp));
     const int ptb = (sh.t_pad + 255) / 256, psb = (sh.n_pad + 255) / 256;
-    prep_records<<<ptb + psb, 256, 0, st>>>(
-        ptb, d_tgt_site, t, sh.t_pad, all_sites, terms, cf.grid_x, cf.grid_y, c->xy, c->volume,
-        c->cell_shift, c->d_key, c->d_ttmp, c->d_bins, c->d_perm, c->d_tgt, d_src, d_q, n,
-        sh.n_pad, c->d_skey, c->d_stmp, c->d_sbins, c->d_geo, c->d_qq, c->d_err);
-    LGM_CUDA(c, cudaGetLastError());
+    LGM_CUDA(c, launch_chain(ov, prep_records, ptb + psb, 256, 0, st, ptb, d_tgt_site, t, sh.t_pad,
+                             all_sites, terms, cf.grid_x, cf.grid_y, c->xy, c->volume,
+                             c->cell_shift, c->d_key, c->d_ttmp, c->d_bins, c->d_perm, c->d_tgt,
+                             d_src, d_q, n, sh.n_pad, c->d_skey, c->d_stmp, c->d_sbins, c->d_geo,
+                             c->d_qq, c->d_err));
     return LGM_OK;
 }
 
@@ -578,6 +662,14 @@ lgm_status launch_culled(lgm_ctx* c, int kind, int v, const Shape& sh, const Pai
     if ((s = grow_device(c, &c->d_tile_items, &c->titems_cap, (size_t)tiles)) != LGM_OK) return s;
     if ((s = grow_device(c, &c->d_part, &c->part_cap, item_cap * TS)) != LGM_OK) return s;
     if ((s = grow_device(c, &c->d_order, &c->order_cap, item_cap)) != LGM_OK) return s;
+    const int nseg = TS / (64 * V.rp);
+    if (V.wi) {
+        if ((s = grow_device(c, &c->d_segmask, &c->segmask_cap,
+                             (size_t)tiles * sh.n_chunks * nseg)) != LGM_OK)
+            return s;
+        if ((s = grow_device(c, &c->d_wcost, &c->wcost_cap, item_cap * nseg)) != LGM_OK) return s;
+        if ((s = grow_device(c, &c->d_wlist, &c->wlist_cap, item_cap * nseg)) != LGM_OK) return s;
+    }
     PairArgs P = A;
     P.part = c->d_part;
     CullArgs C;
@@ -602,18 +694,26 @@ lgm_status launch_culled(lgm_ctx* c, int kind, int v, const Shape& sh, const Pai
     C.hist = c->d_cost_hist;
     C.order = c->d_order;
     C.done = c->d_item_count + 2;
+    if (V.wi) {  // warp items: the cull lists them largest first in place of order[]
+        C.order = nullptr;
+        C.segmask = c->d_segmask;
+        C.wcost = c->d_wcost;
+        C.wlist = c->d_wlist;
+    }
     if (c->counting) {
         LGM_CUDA(c, cudaMemsetAsync(c->d_examined, 0, sizeof(unsigned long long), st));
         C.examined = c->d_examined;
         c->count_pending = true;
     }
-    chunk_boxes_kernel<<<sh.n_chunks, CH, 0, st>>>(P, C);
-    cull_kernel<<<tiles, kCullThreads, 0, st>>>(C);  // its last block orders the items
+    const bool ov = c->overlap;
+    LGM_CUDA(c, launch_chain(ov, chunk_boxes_kernel, sh.n_chunks, CH, 0, st, P, C));
+    // its last block orders the items
+    LGM_CUDA(c, launch_chain(ov, cull_kernel, tiles, kCullThreads, 0, st, C));
     // timing on: the events bracket the pair kernel alone (recorded again here)
     if (c->timing) LGM_CUDA(c, cudaEventRecord(c->ev_pair0, st));
     const int grid = c->sm_count * std::max(1, c->bps[v][fi]);
-    V.cfn[fi]<<<grid, variant_threads(V), variant_smem(V, fi, P.tab_k), st>>>(P, C);
-    LGM_CUDA(c, cudaGetLastError());
+    LGM_CUDA(c, launch_chain(ov, V.cfn[fi], grid, variant_threads(V),
+                             variant_smem(V, fi, P.tab_k), st, P, C));
     c->last.ctas = grid;
     c->last.threads = variant_threads(V);
     c->last.targets_per_thread = 2 * V.rp;
@@ -664,8 +764,7 @@ lgm_status launch_pair(lgm_ctx* c, int kind, int v, const Shape& sh, cudaStream_
     }
     const Variant& V = kVariants[v];
     dim3 grid(tiles, splits);
-    V.fn[fi]<<<grid, V.nt, pair_smem_bytes(A.tab_k), st>>>(A);
-    LGM_CUDA(c, cudaGetLastError());
+    LGM_CUDA(c, launch_chain(c->overlap, V.fn[fi], grid, V.nt, pair_smem_bytes(A.tab_k), st, A));
     c->last.ctas = grid.x * grid.y;
     c->last.threads = V.nt;
     c->last.targets_per_thread = 2 * V.rp;
@@ -701,8 +800,7 @@ lgm_status launch_potentials(lgm_ctx* c, int kind, unsigned terms, const int32_t
     c->count_pending = false;
     if (t == 0) return LGM_OK;
     if (n == 0) {
-        fill_zero<<<(t + 255) / 256, 256, 0, st>>>(d_out, t);
-        LGM_CUDA(c, cudaGetLastError());
+        LGM_CUDA(c, launch_chain(c->overlap, fill_zero, (t + 255) / 256, 256, 0, st, d_out, t));
         c->last.kernel_launches = 1;
         return LGM_OK;
     }
@@ -720,11 +818,10 @@ lgm_status launch_potentials(lgm_ctx* c, int kind, unsigned terms, const int32_t
         if ((s = grow_device(c, &c->d_part, &c->part_cap, (size_t)splits * sh.t_phys)) != LGM_OK)
             return s;
         dim3 grid(ctas, splits);
-        pair_kernel_f64<<<grid, kF64Threads, 0, st>>>(c->d_geo, c->d_qq, sh.n_pad, splits, c->d_tgt,
-                                                      sh.t_phys, c->d_part,
-                                                      cf.electrostatic_cutoff * cf.electrostatic_cutoff,
-                                                      kind, erffactor);
-        LGM_CUDA(c, cudaGetLastError());
+        LGM_CUDA(c, launch_chain(c->overlap, pair_kernel_f64, grid, kF64Threads, 0, st, c->d_geo,
+                                 c->d_qq, sh.n_pad, splits, c->d_tgt, sh.t_phys, c->d_part,
+                                 cf.electrostatic_cutoff * cf.electrostatic_cutoff, kind,
+                                 erffactor));
         c->last.ctas = grid.x * grid.y;
         c->last.threads = kF64Threads;
         c->last.targets_per_thread = 1;
@@ -736,19 +833,22 @@ lgm_status launch_potentials(lgm_ctx* c, int kind, unsigned terms, const int32_t
         LGM_CUDA(c, cudaEventRecord(c->ev_pair1, st));
         c->timed_pending = true;
     }
+    // the last kernel also clears both bin arrays for the next call
+    const int nbins = 2 * c->bins_stride;
     if (splits > 0) {
-        finalize<<<(t + 255) / 256, 256, 0, st>>>(c->d_part, splits, sh.t_phys, t, sh.t_pad,
-                                                   sh.nterms, cf.electrostatic_prefactor,
-                                                   c->d_perm, d_out);
+        LGM_CUDA(c, launch_chain(c->overlap, finalize, (t + 255) / 256, 256, 0, st, c->d_part,
+                                 splits, sh.t_phys, t, sh.t_pad, sh.nterms,
+                                 cf.electrostatic_prefactor, c->d_perm, d_out, c->d_bins, nbins));
         c->last.kernel_launches = 5;  // bins (+ scan), scatter, records, pair, finalize
     } else {
         const Variant& V = kVariants[c->last.variant];
-        finalize_items<<<(t + 31) / 32, dim3(32, 3), 0, st>>>(
-            c->d_part, c->d_tile_first, c->d_tile_items, V.nt * 2 * V.rp, t, sh.t_pad, sh.nterms,
-            cf.electrostatic_prefactor, c->d_perm, d_out);
+        LGM_CUDA(c, launch_chain(c->overlap, finalize_items, (t + 31) / 32, dim3(32, 3), 0, st,
+                                 c->d_part, c->d_tile_first, c->d_tile_items, V.nt * 2 * V.rp, t,
+                                 sh.t_pad, sh.nterms, cf.electrostatic_prefactor, c->d_perm, d_out,
+                                 c->d_bins, nbins));
         c->last.kernel_launches = 7;  // bins (+ scan), scatter, records, boxes, cull, pair, finalize
     }
-    LGM_CUDA(c, cudaGetLastError());
+    c->bins_clean = true;
     c->last.pairs_tested = (int64_t)sh.nterms * t * (int64_t)n;
     c->last.splits = splits;
     return LGM_OK;
@@ -1081,7 +1181,8 @@ lgm_status lgm_destroy(lgm_ctx* c) {
                         c->d_skey,  c->d_stmp,       c->d_cbox,       c->d_gbox,
                         c->d_live,  c->d_items,      c->d_tile_first, c->d_tile_items,
                         c->d_item_count, c->d_examined, c->d_rtab64,  c->d_gtab64,
-                        c->d_cost_hist,  c->d_order};
+                        c->d_cost_hist,  c->d_order,     c->d_segmask,    c->d_wcost,
+                        c->d_wlist};
     for (void* p : dev_ptrs)
         if (p) cudaFree(p);
     void* host_ptrs[] = {c->h_s, c->h_q, c->h_t, c->h_o, c->h_err};
@@ -1128,6 +1229,12 @@ lgm_status lgm_set_counting(lgm_ctx* c, int32_t enable) {
     return LGM_OK;
 }
 
+lgm_status lgm_set_launch_overlap(lgm_ctx* c, int32_t enable) {
+    if (!c) return LGM_ERR_INVALID_ARGUMENT;
+    c->overlap = enable != 0;
+    return LGM_OK;
+}
+
 lgm_status lgm_set_timing(lgm_ctx* c, int32_t enable) {
     if (!c) return LGM_ERR_INVALID_ARGUMENT;
     LGM_CUDA(c, cudaSetDevice(c->device));
@@ -1154,14 +1261,15 @@ lgm_status lgm_variant_flags(int32_t v, int32_t* flags) {
     if (v < 0 || v >= kNumVariants || !flags) return LGM_ERR_INVALID_ARGUMENT;
     *flags = (kVariants[v].skip ? LGM_VARIANT_WARP_SKIP : 0) |
              (kVariants[v].cull ? LGM_VARIANT_CULLED : 0) |
-             (kVariants[v].ws ? LGM_VARIANT_WARP_SPECIALISED : 0);
+             (kVariants[v].ws ? LGM_VARIANT_WARP_SPECIALISED : 0) |
+             (kVariants[v].wi ? LGM_VARIANT_WARP_ITEMS : 0);
     return LGM_OK;
 }
 
 lgm_status lgm_variant_items(int32_t v, int32_t* chunks_per_item, int32_t* stages) {
     if (v < 0 || v >= kNumVariants) return LGM_ERR_INVALID_ARGUMENT;
     if (chunks_per_item) *chunks_per_item = kVariants[v].cull ? kVariants[v].per_item : 0;
-    if (stages) *stages = kVariants[v].ws;
+    if (stages) *stages = kVariants[v].ws ? kVariants[v].ws : kVariants[v].wi;
     return LGM_OK;
 }
 

@@ -61,6 +61,10 @@ struct lgm_ctx {
                                                       // tiles culled
     int32_t* d_cost_hist = nullptr;                   // [kCostBuckets] items per cost
     int32_t* d_order = nullptr; size_t order_cap = 0; // items by decreasing cost
+    // warp items (warp-item variants): segment group masks, costs, ordered list
+    uint8_t* d_segmask = nullptr; size_t segmask_cap = 0;
+    int32_t* d_wcost = nullptr; size_t wcost_cap = 0;
+    int4* d_wlist = nullptr; size_t wlist_cap = 0;
 
     // Pinned host staging for the host-buffer entry points.
     int32_t* h_s = nullptr;   size_t hs_cap = 0;
@@ -78,6 +82,11 @@ struct lgm_ctx {
     bool count_pending = false;
     bool timing = false;
     cudaEvent_t ev_pair0 = nullptr, ev_pair1 = nullptr;  // bracket the pair kernel
+    // the call's kernels launched with programmatic stream serialization
+    // (lgm_set_launch_overlap), and both bin arrays known to be zero (the
+    // last kernel of a completed launch sequence clears them)
+    bool overlap = true;
+    bool bins_clean = false;
     bool timed_pending = false;
 
     std::string err;

@@ -131,4 +131,17 @@ __device__ __forceinline__ void fma_if_below(float& acc, float q, float w, unsig
 
 __device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
 
+// Programmatic dependent launch.  A kernel launched with the programmatic
+// stream serialization attribute may be scheduled before the kernel ahead of
+// it in the stream has finished; pdl_wait() blocks until that kernel has
+// completed and its memory operations are visible (a no-op for a kernel
+// launched without the attribute).  Every kernel of a call's chain calls it
+// before its first global memory access.  pdl_trigger() lets the next kernel
+// of the stream be scheduled once every CTA of this grid has called it (or
+// exited); it changes when the next kernel starts waiting, never what it sees.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() {
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 }  // namespace lgm

@@ -75,6 +75,7 @@ constexpr int kCullPerItem = 2;  // source chunks per work item of the culled pa
 // resident CTAs per SM; items taken largest first (the API's default variant).
 constexpr int kCNW = 4, kCRP = 2, kCStages = 4, kCMinBlocks = 4;
 constexpr int kCSUB = kGroup;  // FP32 runs of the culled sum: one source group
+constexpr int kCVote = 2;      // sources per warp vote of the culled sum (the same bits)
 constexpr int kCThreads = kCNW * 32 + 32;
 constexpr int kCTile = kCNW * 32 * 2 * kCRP;
 // Replicas with room for fewer source chunks than this keep the unculled
@@ -1709,14 +1710,14 @@ using KPairFn = void (*)(PairArgs);
 
 using KCulledFn = void (*)(PairArgs, CullArgs);
 KCulledFn kmc_pair_culled(int gauss) {
-    return gauss ? &pair_kernel_culled_ws<1, 0, kCNW, kCRP, kCSUB, kCStages, kCMinBlocks, true>
-                 : &pair_kernel_culled_ws<0, 0, kCNW, kCRP, kCSUB, kCStages, kCMinBlocks, true>;
+    return gauss ? &pair_kernel_culled_ws<1, 0, kCNW, kCRP, kCSUB, kCStages, kCMinBlocks, true, false, kCVote>
+                 : &pair_kernel_culled_ws<0, 0, kCNW, kCRP, kCSUB, kCStages, kCMinBlocks, true, false, kCVote>;
 }
 size_t kmc_culled_smem(int tab_k) { return ws_smem_bytes(kCStages, tab_k, 4); }
 
 // the culled replicas of a batch (point charges), one persistent launch
 constexpr auto kBatchCulled =
-    &pair_kernel_culled_ws_list<kCNW, kCRP, kCSUB, kCStages, kCMinBlocks, true>;
+    &pair_kernel_culled_ws_list<kCNW, kCRP, kCSUB, kCStages, kCMinBlocks, true, false, kCVote>;
 
 KPairFn kmc_pair(int gauss, int sorted = 1) {
     if (sorted)

@@ -286,6 +286,8 @@ __device__ __forceinline__ void pair_tile(PairArgs A, const int tile, const int 
 // Grid form: blockIdx.x = target tile, blockIdx.y = source split.
 template <int KIND, int PATH, int NT, int RP, int SUB, bool NORM = false, bool SKIP = false>
 __global__ void __launch_bounds__(NT) pair_kernel(PairArgs A) {
+    pdl_wait();
+    pdl_trigger();
     pair_tile<KIND, PATH, NT, RP, SUB, NORM, SKIP>(A, blockIdx.x, blockIdx.y);
 }
 
