@@ -662,6 +662,7 @@ lgm_status launch_culled(lgm_ctx* c, int kind, int v, const Shape& sh, const Pai
     if ((s = grow_device(c, &c->d_tile_items, &c->titems_cap, (size_t)tiles)) != LGM_OK) return s;
     if ((s = grow_device(c, &c->d_part, &c->part_cap, item_cap * TS)) != LGM_OK) return s;
     if ((s = grow_device(c, &c->d_order, &c->order_cap, item_cap)) != LGM_OK) return s;
+    if ((s = grow_device(c, &c->d_oitems, &c->oitems_cap, item_cap)) != LGM_OK) return s;
     const int nseg = TS / (64 * V.rp);
     if (V.wi) {
         if ((s = grow_device(c, &c->d_segmask, &c->segmask_cap,
@@ -693,9 +694,11 @@ lgm_status launch_culled(lgm_ctx* c, int kind, int v, const Shape& sh, const Pai
     C.warp_targets = 64 * V.rp;
     C.hist = c->d_cost_hist;
     C.order = c->d_order;
+    C.oitems = c->d_oitems;
     C.done = c->d_item_count + 2;
     if (V.wi) {  // warp items: the cull lists them largest first in place of order[]
         C.order = nullptr;
+        C.oitems = nullptr;
         C.segmask = c->d_segmask;
         C.wcost = c->d_wcost;
         C.wlist = c->d_wlist;
@@ -1182,7 +1185,7 @@ lgm_status lgm_destroy(lgm_ctx* c) {
                         c->d_live,  c->d_items,      c->d_tile_first, c->d_tile_items,
                         c->d_item_count, c->d_examined, c->d_rtab64,  c->d_gtab64,
                         c->d_cost_hist,  c->d_order,     c->d_segmask,    c->d_wcost,
-                        c->d_wlist};
+                        c->d_wlist,      c->d_oitems};
     for (void* p : dev_ptrs)
         if (p) cudaFree(p);
     void* host_ptrs[] = {c->h_s, c->h_q, c->h_t, c->h_o, c->h_err};

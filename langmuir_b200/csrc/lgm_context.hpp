@@ -61,6 +61,7 @@ struct lgm_ctx {
                                                       // tiles culled
     int32_t* d_cost_hist = nullptr;                   // [kCostBuckets] items per cost
     int32_t* d_order = nullptr; size_t order_cap = 0; // items by decreasing cost
+    int4* d_oitems = nullptr; size_t oitems_cap = 0;  // their records in that order
     // warp items (warp-item variants): segment group masks, costs, ordered list
     uint8_t* d_segmask = nullptr; size_t segmask_cap = 0;
     int32_t* d_wcost = nullptr; size_t wcost_cap = 0;

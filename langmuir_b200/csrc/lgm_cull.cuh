@@ -118,6 +118,9 @@ struct CullArgs {
     int warp_targets = 0;
     int* hist = nullptr;
     int* order = nullptr;
+    // Optional with order: the item records in order[]'s order, .w = the
+    // item's index (one load fewer for the kernels that take items in turn)
+    int4* oitems = nullptr;
     // with order: culled tiles so far (zeroed by chunk_boxes block 0); the
     // cull's last block to finish writes order[]
     int* done = nullptr;
@@ -246,16 +249,20 @@ __device__ __forceinline__ void order_items_body(const CullArgs& C) {
         return;
     }
     for (int g0 = (int)threadIdx.x; g0 < nit; g0 += 4 * nt) {  // four item loads in flight
-        int c[4];
+        int4 r[4];
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
             const int g = g0 + u * nt;
-            c[u] = g < nit ? min(__ldcg(&C.items[g]).w, kCostBuckets - 1) : 0;
+            r[u] = g < nit ? __ldcg(&C.items[g]) : make_int4(0, 0, 0, 0);
         }
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
             const int g = g0 + u * nt;
-            if (g < nit) C.order[atomicAdd(&s_off[c[u]], 1)] = g;
+            if (g < nit) {
+                const int pos = atomicAdd(&s_off[min(r[u].w, kCostBuckets - 1)], 1);
+                C.order[pos] = g;
+                if (C.oitems) C.oitems[pos] = make_int4(r[u].x, r[u].y, r[u].z, g);
+            }
         }
     }
 }
@@ -312,7 +319,7 @@ __device__ __forceinline__ void cull_body(const CullArgs& C, const int tile) {
         if (lane == 0) s_seg[sg] = make_box(xl, yl, zl, xh, yh, zh);
     }
     if (tid < kMaxItemsPerTile) s_cost[tid] = 0;
-    if (C.segmask)
+    if (C.hist)
         for (int w = tid; w < kMaxItemsPerTile * kMaxSegments; w += kCullThreads) s_wcost[w] = 0;
     __syncthreads();
     Box tb = s_seg[0];
@@ -361,15 +368,25 @@ __device__ __forceinline__ void cull_body(const CullArgs& C, const int tile) {
             }
         }
     } else if (C.hist) {
-        // item cost: the (segment, group) pairs within the cutoff, one thread
-        // per (live chunk, group); the live list was written by this block
-        // (visible after the barriers above)
+        // item cost: the groups within the cutoff of each warp segment, one
+        // thread per (live chunk, group); the live list was written by this
+        // block (visible after the barriers above).  A CTA takes an item as
+        // long as its busiest warp does: cost 4 x the most groups of one
+        // segment + their mean over the segments.
         for (int w = tid; w < L * kGroupsPerChunk; w += kCullThreads) {
             const int li = w / kGroupsPerChunk, g = w - li * kGroupsPerChunk;
             const Box gb = C.gbox[(size_t)live[li] * kGroupsPerChunk + g];
-            int n = 0;
-            for (int sg = 0; sg < nseg; ++sg) n += box_gap2(s_seg[sg], gb) < C.c2;
-            if (n) atomicAdd(&s_cost[li / per], n);
+            for (int sg = 0; sg < nseg; ++sg)
+                if (box_gap2(s_seg[sg], gb) < C.c2) atomicAdd(&s_wcost[(li / per) * nseg + sg], 1);
+        }
+        __syncthreads();
+        for (int i = tid; i < nit; i += kCullThreads) {
+            int mx = 0, sum = 0;
+            for (int sg = 0; sg < nseg; ++sg) {
+                mx = max(mx, s_wcost[i * nseg + sg]);
+                sum += s_wcost[i * nseg + sg];
+            }
+            s_cost[i] = 4 * mx + sum / nseg;
         }
     }
     if (tid == 0) {
@@ -417,6 +434,17 @@ struct OneProblem {
         prob = 0;
         local = c.order ? c.order[g] : g;
     }
+    // the record of item g (in taking order) and its problem and local index
+    __device__ __forceinline__ int4 item(int g, int& prob, int& local) const {
+        prob = 0;
+        if (c.oitems) {
+            const int4 r = c.oitems[g];
+            local = r.w;
+            return r;
+        }
+        local = c.order ? c.order[g] : g;
+        return c.items[local];
+    }
     __device__ __forceinline__ const PairArgs& A(int) const { return a; }
     __device__ __forceinline__ const CullArgs& C(int) const { return c; }
     __device__ __forceinline__ const PairArgs& first() const { return a; }
@@ -442,6 +470,10 @@ struct ProblemList {
         }
         prob = list[lo];
         local = g - offs[lo];
+    }
+    __device__ __forceinline__ int4 item(int g, int& prob, int& local) const {
+        resolve(g, prob, local);
+        return ca[prob].items[local];
     }
     __device__ __forceinline__ const PairArgs& A(int p) const { return pa[p]; }
     __device__ __forceinline__ const CullArgs& C(int p) const { return ca[p]; }
@@ -869,9 +901,10 @@ inline size_t ws_smem_bytes(int S, int tab_k, int elem) {
 // the tile's targets as in pair_items_culled (TS = NW * 64 RP); one producer
 // warp (its lane 0) takes items from an atomic counter -- whichever CTA is
 // free takes the next item -- and streams their chunks through an S-stage
-// ring: stage records {local item, chunk position, chunks, problem}, full
-// barriers (the bulk copies) and empty barriers (one arrival per consumer
-// warp).  Consumer warps never wait for one another: a warp whose groups are
+// ring: stage records {local item, chunk position, chunks, problem} and the
+// item's tile, full barriers (the bulk copies) and empty barriers (one
+// arrival per consumer warp).  The producer claims the next item only when
+// the consumers are on the last chunk it issued (see the claim below).  Consumer warps never wait for one another: a warp whose groups are
 // all beyond the cutoff of its targets passes a chunk at once, and may run up
 // to S chunks ahead of the slowest warp.  After the last item the producer
 // posts a record with item -1 (no copy) that ends the consumers.  Every wait
@@ -900,6 +933,7 @@ __device__ __forceinline__ void pair_items_culled_ws(const PS& P) {
     float* s_tab = reinterpret_cast<float*>(smem + S * ws_stage_bytes());
     double* s_tab64 = reinterpret_cast<double*>(smem + S * ws_stage_bytes());
     __shared__ Box s_wbox[NW];
+    __shared__ int s_tile[S];  // the tile of each stage's item
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     if (tid == 0) {
@@ -922,15 +956,22 @@ __device__ __forceinline__ void pair_items_culled_ws(const PS& P) {
         uint32_t k = 0;  // stages issued
         bool ok = true;
         for (;;) {
+            // Claim the next item only once the target warps have released
+            // every chunk but the last one issued.  Claimed but unstarted
+            // items are what the other CTAs wait for at the end of the
+            // kernel: taken early, the largest items would pile up three to
+            // a CTA in the first microseconds.  The claim and the first copy
+            // take less than a chunk's sums.
+            if (k >= 2 && !mbar_wait_bounded(&s_empty[(k - 2) % S], ((k - 2) / S) & 1u, err)) {
+                ok = false;
+                break;
+            }
             const int g = atomicAdd(P.work(), 1);
             const bool done = g >= nit;
             if (done) pdl_trigger();  // no item left: the next kernel may be scheduled
             int prob = 0, local = -1;
             int4 r = make_int4(0, 0, 1, 0);
-            if (!done) {
-                P.resolve(g, prob, local);
-                r = P.C(prob).items[local];
-            }
+            if (!done) r = P.item(g, prob, local);
             for (int c = 0; c < r.z; ++c, ++k) {
                 const int st = (int)(k % S);
                 if (k >= (uint32_t)S && !mbar_wait_bounded(&s_empty[st], (k / S - 1) & 1u, err)) {
@@ -938,6 +979,7 @@ __device__ __forceinline__ void pair_items_culled_ws(const PS& P) {
                     break;
                 }
                 s_rec[st] = make_int4(local, c, r.z, prob);
+                s_tile[st] = r.x;
                 if (done) {
                     mbar_arrive(&s_full[st]);  // the end record: no copy
                 } else {
@@ -980,7 +1022,7 @@ __device__ __forceinline__ void pair_items_culled_ws(const PS& P) {
         const PairArgs& A = P.A(m.w);
         const CullArgs& C = P.C(m.w);
         if (m.y == 0) {  // the item's first chunk: its tile's targets of this warp
-            base = C.items[m.x].x * TS;
+            base = s_tile[st] * TS;
             t_phys = A.dyn ? A.dyn[1] : A.t_phys;
             c2 = C.c2;
             tab_k = A.tab_k;
