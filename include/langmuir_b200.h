@@ -272,18 +272,10 @@ lgm_status lgm_variant_info(int32_t variant, int32_t* threads, int32_t* target_p
  * The sums equal those of the other culled variants bit for bit.  `threads`
  * of lgm_variant_info counts the target warps' threads only. */
 #define LGM_VARIANT_WARP_SPECIALISED 4
-/* LGM_VARIANT_WARP_ITEMS (with LGM_VARIANT_CULLED): the work items are split
- * per warp segment of targets (64 * target_pairs targets), and every warp of
- * a CTA takes them on its own from a shared counter, largest first, staging
- * only the chunks its segment has a live group in through its own ring of
- * stages (its lane 0 issues the copies); no warp waits for another.  The sums
- * equal those of the other culled variants bit for bit. */
-#define LGM_VARIANT_WARP_ITEMS 8
 lgm_status lgm_variant_flags(int32_t variant, int32_t* flags);
 /* Culled variants: source chunks per work item (at least; more when a
  * tile's live chunks exceed 32 items) and, warp-specialised, the stages of
- * the copy ring, or, warp items, the stages of each warp's ring (0
- * otherwise); both 0 for the other variants. */
+ * the copy ring (0 otherwise); both 0 for the other variants. */
 lgm_status lgm_variant_items(int32_t variant, int32_t* chunks_per_item, int32_t* stages);
 
 #ifdef __cplusplus

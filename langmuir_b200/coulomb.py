@@ -122,8 +122,7 @@ class Coulomb:
             N.lib().lgm_variant_items(v, ctypes.byref(k), ctypes.byref(st))
             out.append({"threads": a.value, "target_pairs": b.value, "run": c.value,
                         "warp_skip": bool(f.value & 1), "culled": bool(f.value & 2),
-                        "warp_specialised": bool(f.value & 4),
-                        "warp_items": bool(f.value & 8), "chunks_per_item": k.value,
+                        "warp_specialised": bool(f.value & 4), "chunks_per_item": k.value,
                         "stages": st.value})
         return out
 

@@ -317,7 +317,7 @@ __global__ void scatter_both(const int32_t* __restrict__ tkey, int t, int32_t* _
 // out[perm[g]] = prefactor * (sum of the item partials of the direct slot -
 // those of the image slots) of target g, for the culled pair sums.  A block
 // of 32 x 3 threads takes 32 targets: warp y sums term slot y's partials of
-// each target in item order, eight items in flight; warp 0 then combines the
+// each target in item order, sixteen items in flight; warp 0 then combines the
 // slots through shared memory.
 __global__ void __launch_bounds__(96) finalize_items(const double* __restrict__ part,
                                                      const int* __restrict__ tile_first,
@@ -327,11 +327,12 @@ __global__ void __launch_bounds__(96) finalize_items(const double* __restrict__ 
                                                      const int32_t* __restrict__ perm,
                                                      double* __restrict__ out,
                                                      int32_t* __restrict__ bins, int nbins) {
-    constexpr int kRows = 8;
+    constexpr int kRows = 16;  // loads in flight (a tile has at most 32 items)
     __shared__ double s_sum[3][32];
     pdl_wait();
     pdl_trigger();
     const int g = blockIdx.x * 32 + (int)threadIdx.x, slot = (int)threadIdx.y;
+    const int dst = slot == 0 && g < t ? perm[g] : 0;  // loaded ahead of the sums
     if (slot == 0) zero_bins(bins, nbins);
     double sum = 0.0;
     if (g < t && slot < nterms) {
@@ -353,7 +354,7 @@ __global__ void __launch_bounds__(96) finalize_items(const double* __restrict__ 
     __syncthreads();
     if (slot == 0 && g < t) {
         const int x = (int)threadIdx.x;
-        out[perm[g]] = prefactor * (s_sum[0][x] - s_sum[1][x] - s_sum[2][x]);
+        out[dst] = prefactor * (s_sum[0][x] - s_sum[1][x] - s_sum[2][x]);
     }
 }
 
@@ -449,7 +450,6 @@ struct Variant {
     PairFn fn[4];
     CulledFn cfn[4];  // [3]: the FP64-table path (culled variants only)
     int ws = 0;       // warp-specialised culled kernel: its stages (0: not)
-    int wi = 0;       // warp-item culled kernel: stages per warp (0: not)
 };
 #define LGM_VARIANT_S(NT, RP, SUB, SK)                                                    \
     Variant {                                                                             \
@@ -489,17 +489,6 @@ struct Variant {
              &pair_kernel_culled_ws<0, 2, NW, RP, SUB, S, MINB>},                             \
             S                                                                                 \
     }
-// warp items (lgm_cull.cuh pair_items_warp): NW independent warps per CTA,
-// S stages per warp, at least MINB CTAs per SM
-#define LGM_VARIANT_CULL_WI(NW, RP, SUB, K, S, MINB, VOTE)                                   \
-    Variant {                                                                                 \
-        NW * 32, RP, SUB, 1, 1, K, {nullptr, nullptr, nullptr, nullptr},                      \
-            {&pair_kernel_warp_items<0, 0, NW, RP, SUB, S, MINB, VOTE>,                       \
-             &pair_kernel_warp_items<1, 0, NW, RP, SUB, S, MINB, VOTE>,                       \
-             &pair_kernel_warp_items<0, 1, NW, RP, SUB, S, MINB>,                             \
-             &pair_kernel_warp_items<0, 2, NW, RP, SUB, S, MINB>},                            \
-            0, S                                                                              \
-    }
 const Variant kVariants[] = {
     LGM_VARIANT(128, 4, 16),       LGM_VARIANT(128, 4, 8),        LGM_VARIANT(128, 2, 16),
     LGM_VARIANT(128, 8, 16),       LGM_VARIANT(256, 4, 16),       LGM_VARIANT(64, 4, 16),
@@ -525,10 +514,6 @@ const Variant kVariants[] = {
     // one vote per 2 or 4 sources, or none
     LGM_VARIANT_CULL_WSV(4, 2, 16, 2, 4, 4, 2), LGM_VARIANT_CULL_WSV(4, 2, 16, 2, 4, 4, 0),
     LGM_VARIANT_CULL_WSV(4, 2, 16, 2, 4, 4, 4),
-    // warp items: (warps, target pairs, run, chunks per item, stages per warp,
-    // CTAs per SM, sources per vote)
-    LGM_VARIANT_CULL_WI(4, 2, 16, 2, 2, 5, 2), LGM_VARIANT_CULL_WI(4, 2, 16, 2, 3, 3, 2),
-    LGM_VARIANT_CULL_WI(4, 2, 16, 1, 2, 5, 2), LGM_VARIANT_CULL_WI(2, 2, 16, 2, 3, 7, 2),
 };
 constexpr int kNumVariants = (int)(sizeof(kVariants) / sizeof(kVariants[0]));
 static_assert(kNumVariants <= (int)(sizeof(lgm_ctx::bps) / sizeof(lgm_ctx::bps[0])),
@@ -548,7 +533,6 @@ const void* kernel_of(const Variant& V, int fi) {
 int variant_threads(const Variant& V) { return V.nt + (V.ws ? 32 : 0); }
 size_t variant_smem(const Variant& V, int fi, int tab_k) {
     if (V.ws) return ws_smem_bytes(V.ws, tab_k, fi == 3 ? 8 : 4);
-    if (V.wi) return wi_smem_bytes(V.nt / 32, V.wi, tab_k, fi == 3 ? 8 : 4);
     return fi == 3 ? pair_smem_bytes64(tab_k) : pair_smem_bytes(tab_k);
 }
 
@@ -663,14 +647,6 @@ lgm_status launch_culled(lgm_ctx* c, int kind, int v, const Shape& sh, const Pai
     if ((s = grow_device(c, &c->d_part, &c->part_cap, item_cap * TS)) != LGM_OK) return s;
     if ((s = grow_device(c, &c->d_order, &c->order_cap, item_cap)) != LGM_OK) return s;
     if ((s = grow_device(c, &c->d_oitems, &c->oitems_cap, item_cap)) != LGM_OK) return s;
-    const int nseg = TS / (64 * V.rp);
-    if (V.wi) {
-        if ((s = grow_device(c, &c->d_segmask, &c->segmask_cap,
-                             (size_t)tiles * sh.n_chunks * nseg)) != LGM_OK)
-            return s;
-        if ((s = grow_device(c, &c->d_wcost, &c->wcost_cap, item_cap * nseg)) != LGM_OK) return s;
-        if ((s = grow_device(c, &c->d_wlist, &c->wlist_cap, item_cap * nseg)) != LGM_OK) return s;
-    }
     PairArgs P = A;
     P.part = c->d_part;
     CullArgs C;
@@ -696,13 +672,6 @@ lgm_status launch_culled(lgm_ctx* c, int kind, int v, const Shape& sh, const Pai
     C.order = c->d_order;
     C.oitems = c->d_oitems;
     C.done = c->d_item_count + 2;
-    if (V.wi) {  // warp items: the cull lists them largest first in place of order[]
-        C.order = nullptr;
-        C.oitems = nullptr;
-        C.segmask = c->d_segmask;
-        C.wcost = c->d_wcost;
-        C.wlist = c->d_wlist;
-    }
     if (c->counting) {
         LGM_CUDA(c, cudaMemsetAsync(c->d_examined, 0, sizeof(unsigned long long), st));
         C.examined = c->d_examined;
@@ -1184,8 +1153,7 @@ lgm_status lgm_destroy(lgm_ctx* c) {
                         c->d_skey,  c->d_stmp,       c->d_cbox,       c->d_gbox,
                         c->d_live,  c->d_items,      c->d_tile_first, c->d_tile_items,
                         c->d_item_count, c->d_examined, c->d_rtab64,  c->d_gtab64,
-                        c->d_cost_hist,  c->d_order,     c->d_segmask,    c->d_wcost,
-                        c->d_wlist,      c->d_oitems};
+                        c->d_cost_hist,  c->d_order,     c->d_oitems};
     for (void* p : dev_ptrs)
         if (p) cudaFree(p);
     void* host_ptrs[] = {c->h_s, c->h_q, c->h_t, c->h_o, c->h_err};
@@ -1264,15 +1232,14 @@ lgm_status lgm_variant_flags(int32_t v, int32_t* flags) {
     if (v < 0 || v >= kNumVariants || !flags) return LGM_ERR_INVALID_ARGUMENT;
     *flags = (kVariants[v].skip ? LGM_VARIANT_WARP_SKIP : 0) |
              (kVariants[v].cull ? LGM_VARIANT_CULLED : 0) |
-             (kVariants[v].ws ? LGM_VARIANT_WARP_SPECIALISED : 0) |
-             (kVariants[v].wi ? LGM_VARIANT_WARP_ITEMS : 0);
+             (kVariants[v].ws ? LGM_VARIANT_WARP_SPECIALISED : 0);
     return LGM_OK;
 }
 
 lgm_status lgm_variant_items(int32_t v, int32_t* chunks_per_item, int32_t* stages) {
     if (v < 0 || v >= kNumVariants) return LGM_ERR_INVALID_ARGUMENT;
     if (chunks_per_item) *chunks_per_item = kVariants[v].cull ? kVariants[v].per_item : 0;
-    if (stages) *stages = kVariants[v].ws ? kVariants[v].ws : kVariants[v].wi;
+    if (stages) *stages = kVariants[v].ws;
     return LGM_OK;
 }
 

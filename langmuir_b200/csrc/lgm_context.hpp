@@ -62,10 +62,6 @@ struct lgm_ctx {
     int32_t* d_cost_hist = nullptr;                   // [kCostBuckets] items per cost
     int32_t* d_order = nullptr; size_t order_cap = 0; // items by decreasing cost
     int4* d_oitems = nullptr; size_t oitems_cap = 0;  // their records in that order
-    // warp items (warp-item variants): segment group masks, costs, ordered list
-    uint8_t* d_segmask = nullptr; size_t segmask_cap = 0;
-    int32_t* d_wcost = nullptr; size_t wcost_cap = 0;
-    int4* d_wlist = nullptr; size_t wlist_cap = 0;
 
     // Pinned host staging for the host-buffer entry points.
     int32_t* h_s = nullptr;   size_t hs_cap = 0;

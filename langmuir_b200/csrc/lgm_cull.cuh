@@ -39,6 +39,7 @@ constexpr int kCullThreads = 256;             // threads of the cull kernel
 constexpr int kMaxItemsPerTile = 32;          // items a tile's chunk list is cut into, at most
 constexpr int kMaxSegments = 16;              // warp target segments of a tile, at most
 constexpr int kCostBuckets = 256;             // item cost classes of the largest-first order
+constexpr int kLiveSmem = 1024;               // live chunks the cull keeps in shared memory
 
 // A box of lattice coordinates [lo, hi] per axis (inclusive).  Empty: lo > hi.
 struct __align__(16) Box {
@@ -124,19 +125,6 @@ struct CullArgs {
     // with order: culled tiles so far (zeroed by chunk_boxes block 0); the
     // cull's last block to finish writes order[]
     int* done = nullptr;
-    // Optional warp items (segmask null: off; needs hist and done).  A warp
-    // item is one warp segment (warp_targets targets) of one item; with
-    // nseg = tile_size / warp_targets segments per tile, warp item
-    // item * nseg + sg.  segmask[(tile * live_stride + li) * nseg + sg]: the
-    // groups (bit g) of the tile's live chunk li whose box comes within the
-    // cutoff of segment sg's box; wcost[item * nseg + sg]: those groups over
-    // the item's chunks (the warp item's cost; hist then counts warp items);
-    // and the cull's last block writes wlist[] = {item, tile, first live
-    // index, chunk count * 16 + sg}, the warp items by decreasing cost, in
-    // place of order[].
-    uint8_t* segmask = nullptr;
-    int* wcost = nullptr;
-    int4* wlist = nullptr;
 };
 
 // One block of CH threads per source chunk: group (kGroup) and chunk boxes of the
@@ -226,37 +214,16 @@ __device__ __forceinline__ void order_items_body(const CullArgs& C) {
     __syncthreads();
     cost_offsets(s_off);
     const int nt = (int)blockDim.x;
-    if (C.wlist) {  // warp items: their records by decreasing cost
-        const int nseg = C.tile_size / C.warp_targets;
-        const int nw = nit * nseg;
-        for (int g0 = (int)threadIdx.x; g0 < nw; g0 += 4 * nt) {
-            int c[4];
-            int4 r[4];
+    constexpr int kLoads = 8;  // item loads in flight per thread
+    for (int g0 = (int)threadIdx.x; g0 < nit; g0 += kLoads * nt) {
+        int4 r[kLoads];
 #pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                const int g = g0 + u * nt;
-                c[u] = g < nw ? min(__ldcg(&C.wcost[g]), kCostBuckets - 1) : 0;
-                r[u] = g < nw ? __ldcg(&C.items[g / nseg]) : make_int4(0, 0, 0, 0);
-            }
-#pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                const int g = g0 + u * nt;
-                if (g < nw)
-                    C.wlist[atomicAdd(&s_off[c[u]], 1)] =
-                        make_int4(g / nseg, r[u].x, r[u].y, r[u].z * 16 + g % nseg);
-            }
-        }
-        return;
-    }
-    for (int g0 = (int)threadIdx.x; g0 < nit; g0 += 4 * nt) {  // four item loads in flight
-        int4 r[4];
-#pragma unroll
-        for (int u = 0; u < 4; ++u) {
+        for (int u = 0; u < kLoads; ++u) {
             const int g = g0 + u * nt;
             r[u] = g < nit ? __ldcg(&C.items[g]) : make_int4(0, 0, 0, 0);
         }
 #pragma unroll
-        for (int u = 0; u < 4; ++u) {
+        for (int u = 0; u < kLoads; ++u) {
             const int g = g0 + u * nt;
             if (g < nit) {
                 const int pos = atomicAdd(&s_off[min(r[u].w, kCostBuckets - 1)], 1);
@@ -288,7 +255,8 @@ __device__ __forceinline__ void cull_body(const CullArgs& C, const int tile) {
     __shared__ Box s_seg[kMaxSegments];
     __shared__ int s_wcount[kCullThreads / 32];
     __shared__ int s_cost[kMaxItemsPerTile];
-    __shared__ int s_wcost[kMaxItemsPerTile * kMaxSegments];  // warp items: their costs
+    __shared__ int s_wcost[kMaxItemsPerTile * kMaxSegments];  // per (item, segment) groups
+    __shared__ int s_live[kLiveSmem];  // the live list, when it fits
     __shared__ int s_base;
     const int n_chunks = C.dyn ? C.dyn[0] : C.n_chunks;
     const int t_phys = C.dyn ? C.dyn[1] : C.t_phys;
@@ -296,7 +264,7 @@ __device__ __forceinline__ void cull_body(const CullArgs& C, const int tile) {
     constexpr int nw = kCullThreads / 32;
     if (tile * C.tile_size >= t_phys) {
         if (tid == 0) C.tile_items[tile] = 0;
-        if (C.order || C.wlist) cull_last_orders(C);
+        if (C.order) cull_last_orders(C);
         return;
     }
     // The boxes of the tile's warp segments (one segment: the whole tile),
@@ -342,42 +310,48 @@ __device__ __forceinline__ void cull_body(const CullArgs& C, const int tile) {
             before += w < warp ? s_wcount[w] : 0;
             total += s_wcount[w];
         }
-        if (on) live[L + before + __popc(m & ((1u << lane) - 1u))] = c;
+        if (on) {
+            const int li = L + before + __popc(m & ((1u << lane) - 1u));
+            live[li] = c;
+            if (li < kLiveSmem) s_live[li] = c;
+        }
         L += total;
     }
     const int per = max(C.per_item, (L + C.max_items - 1) / C.max_items);
     const int nit = L == 0 ? 0 : (L + per - 1) / per;
+    if (tid == 0) {  // the tile's first item: the claim's round trip overlaps the costs
+        const int base = nit ? atomicAdd(C.item_count, nit) : 0;
+        C.tile_first[tile] = base;
+        C.tile_items[tile] = nit;
+        s_base = base;
+    }
     __syncthreads();  // the last round's live entries are visible to the block
-    if (C.segmask) {
-        // warp items: one thread per (live chunk, segment) -- the segment's
-        // live groups of the chunk, and their count added to the warp item's
-        // cost; the live list was written by this block (visible after the
-        // barriers above)
-        uint8_t* sm = C.segmask + (size_t)tile * C.live_stride * nseg;
-        for (int w = tid; w < L * nseg; w += kCullThreads) {
-            const int li = w / nseg, sg = w - li * nseg;
-            const Box* gb = C.gbox + (size_t)live[li] * kGroupsPerChunk;
-            unsigned m = 0;
-#pragma unroll
-            for (int g = 0; g < kGroupsPerChunk; ++g)
-                m |= (box_gap2(s_seg[sg], gb[g]) < C.c2 ? 1u : 0u) << g;
-            sm[(size_t)li * nseg + sg] = (uint8_t)m;
-            if (m) {
-                atomicAdd(&s_wcost[(li / per) * nseg + sg], __popc(m));
-                atomicAdd(&s_cost[li / per], __popc(m));
-            }
-        }
-    } else if (C.hist) {
+    if (C.hist) {
         // item cost: the groups within the cutoff of each warp segment, one
-        // thread per (live chunk, group); the live list was written by this
-        // block (visible after the barriers above).  A CTA takes an item as
-        // long as its busiest warp does: cost 4 x the most groups of one
-        // segment + their mean over the segments.
-        for (int w = tid; w < L * kGroupsPerChunk; w += kCullThreads) {
-            const int li = w / kGroupsPerChunk, g = w - li * kGroupsPerChunk;
-            const Box gb = C.gbox[(size_t)live[li] * kGroupsPerChunk + g];
-            for (int sg = 0; sg < nseg; ++sg)
-                if (box_gap2(s_seg[sg], gb) < C.c2) atomicAdd(&s_wcost[(li / per) * nseg + sg], 1);
+        // thread per (live chunk, group), four group boxes in flight.  A CTA
+        // takes an item as long as its busiest warp does: cost 4 x the most
+        // groups of one segment + their mean over the segments.
+        const int nw = L * kGroupsPerChunk;
+        for (int w0 = tid; w0 < nw; w0 += 4 * kCullThreads) {
+            Box gb[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int w = w0 + u * kCullThreads;
+                if (w < nw) {
+                    const int li = w / kGroupsPerChunk;
+                    const int ch = L <= kLiveSmem ? s_live[li] : live[li];
+                    gb[u] = C.gbox[(size_t)ch * kGroupsPerChunk + (w - li * kGroupsPerChunk)];
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int w = w0 + u * kCullThreads;
+                if (w < nw) {
+                    const int it = (w / kGroupsPerChunk) / per;
+                    for (int sg = 0; sg < nseg; ++sg)
+                        if (box_gap2(s_seg[sg], gb[u]) < C.c2) atomicAdd(&s_wcost[it * nseg + sg], 1);
+                }
+            }
         }
         __syncthreads();
         for (int i = tid; i < nit; i += kCullThreads) {
@@ -389,25 +363,12 @@ __device__ __forceinline__ void cull_body(const CullArgs& C, const int tile) {
             s_cost[i] = 4 * mx + sum / nseg;
         }
     }
-    if (tid == 0) {
-        const int base = nit ? atomicAdd(C.item_count, nit) : 0;
-        C.tile_first[tile] = base;
-        C.tile_items[tile] = nit;
-        s_base = base;
-    }
     __syncthreads();
     for (int i = tid; i < nit; i += kCullThreads) {
         C.items[s_base + i] = make_int4(tile, i * per, min(per, L - i * per), s_cost[i]);
-        if (C.hist && !C.segmask) atomicAdd(&C.hist[min(s_cost[i], kCostBuckets - 1)], 1);
+        if (C.hist) atomicAdd(&C.hist[min(s_cost[i], kCostBuckets - 1)], 1);
     }
-    if (C.segmask) {
-        for (int w = tid; w < nit * nseg; w += kCullThreads) {  // w = i * nseg + sg
-            const int cw = s_wcost[w];
-            C.wcost[(size_t)s_base * nseg + w] = cw;
-            atomicAdd(&C.hist[min(cw, kCostBuckets - 1)], 1);
-        }
-    }
-    if (C.order || C.wlist) cull_last_orders(C);
+    if (C.order) cull_last_orders(C);
 }
 
 // The pair sum over the work items (see the file comment).  KIND 0 point, 1
@@ -1075,155 +1036,6 @@ __device__ __forceinline__ void pair_items_culled_ws(const PS& P) {
             }
         }
     }
-}
-
-// Dynamic shared memory of the warp-item kernel: NW warps x S stages of source
-// records, their full barriers, then the table (elem bytes per entry).
-inline size_t wi_smem_bytes(int NW, int S, int tab_k, int elem) {
-    return (size_t)NW * S * (pair_stage_bytes() + sizeof(uint64_t)) + (size_t)(tab_k + 1) * elem +
-           16;
-}
-
-// The pair sum over warp items (CullArgs::wlist).  Every warp of the CTA works
-// alone: it takes the next warp item -- one 64 RP-target segment of one item,
-// largest first -- from the shared counter, stages the item's chunks in which
-// the segment has a live group (segmask) through its own S-stage ring (bulk
-// copies issued by its lane 0 onto full barriers), and writes the segment's
-// partials to the item's slot.  A segment's chunks and FP32 runs are added in
-// the order of the other culled kernels, and a chunk the segment has no live
-// group in adds nothing there either: the sums are the same bits.  There is
-// no producer warp and no barrier between warps, so no warp waits for a
-// slower one; the next item's counter value is fetched while this one runs.
-// Every wait is bounded: on a timeout the warp raises DEVERR_TIMEOUT, waits
-// (bounded) for its copies in flight, and leaves.
-template <int KIND, int PATH, int NW, int RP, int SUB, bool NORM, int S, int VOTE>
-__device__ __forceinline__ void pair_items_warp(const PairArgs& A, const CullArgs& C) {
-    static_assert(kGroup % SUB == 0, "an FP32 run lies inside one group");
-    static_assert(PATH != 2 || !NORM, "the FP64-table path carries no FP32 run norms");
-    constexpr int SEG = 64 * RP;
-    constexpr uint32_t kStage = (uint32_t)pair_stage_bytes();
-    constexpr uint32_t kGeoBytes = CH * 2 * sizeof(float4);
-    extern __shared__ __align__(128) unsigned char smem[];
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    unsigned char* wbase = smem + (size_t)warp * S * kStage;
-    uint64_t* s_full = reinterpret_cast<uint64_t*>(smem + (size_t)NW * S * kStage) + warp * S;
-    unsigned char* tab_base = smem + (size_t)NW * S * (kStage + sizeof(uint64_t));
-    const float* s_tab = reinterpret_cast<const float*>(tab_base);
-    const double* s_tab64 = reinterpret_cast<const double*>(tab_base);
-    if (lane == 0) {
-        for (int i = 0; i < S; ++i) mbar_init(&s_full[i], 1);
-        fence_mbar_init();
-    }
-    if (PATH == 2) {
-        for (int k = tid; k <= A.tab_k; k += NW * 32)
-            reinterpret_cast<double*>(tab_base)[k] = A.tab64[k];
-    } else if (KIND == 1 || PATH == 1) {
-        for (int k = tid; k <= A.tab_k; k += NW * 32) reinterpret_cast<float*>(tab_base)[k] = A.tab[k];
-    }
-    __syncthreads();
-
-    const int nseg = C.tile_size / SEG;
-    const int nwi = *C.item_count * nseg;
-    const int t_phys = A.dyn ? A.dyn[1] : A.t_phys;
-    const unsigned ulim = __float_as_uint(A.c2 - 0.5f);
-    auto geo = [&](uint32_t k) { return reinterpret_cast<const float4*>(wbase + (k % S) * kStage); };
-    auto qq = [&](uint32_t k) {
-        return reinterpret_cast<const float2*>(wbase + (k % S) * kStage + kGeoBytes);
-    };
-    uint32_t k_issue = 0, k_cons = 0;  // stages issued and consumed (the same in every lane)
-    bool failed = false;
-    int nxt = 0;
-    if (lane == 0) nxt = atomicAdd(C.work, 1);
-    for (;;) {
-        const int g = __shfl_sync(0xffffffffu, nxt, 0);
-        if (g >= nwi) break;
-        const int4 W = C.wlist[g];
-        if (lane == 0) nxt = atomicAdd(C.work, 1);  // the item after this one
-        const int item = W.x, tile = W.y, first = W.z, count = W.w >> 4, sg = W.w & 15;
-        const int base = tile * C.tile_size + sg * SEG;
-        float2 tx[RP], ty[RP], tz[RP], tt[RP];
-#pragma unroll
-        for (int q = 0; q < RP; ++q) {
-            const int p0 = base + 2 * q * 32 + lane, p1 = p0 + 32;
-            const float4 a = p0 < t_phys ? A.tgt[p0] : make_float4(0.f, 0.f, 0.f, -1.f);
-            const float4 b = p1 < t_phys ? A.tgt[p1] : make_float4(0.f, 0.f, 0.f, -1.f);
-            tx[q] = f2(a.x, b.x); ty[q] = f2(a.y, b.y); tz[q] = f2(a.z, b.z); tt[q] = f2(a.w, b.w);
-        }
-        double acc64[2 * RP];
-        float nrm[NORM ? 2 * RP : 1];
-#pragma unroll
-        for (int q = 0; q < 2 * RP; ++q) acc64[q] = 0.0;
-#pragma unroll
-        for (int q = 0; q < (NORM ? 2 * RP : 1); ++q) nrm[q] = 0.f;
-        // the item's chunks 32 at a time: lane c holds chunk c's id and this
-        // segment's group mask; the live ones go through the ring in order
-        for (int c0 = 0; c0 < count && !failed; c0 += 32) {
-            const int c = c0 + lane;
-            int cid = 0;
-            unsigned m = 0;
-            if (c < count) {
-                const size_t li = (size_t)tile * C.live_stride + first + c;
-                cid = C.live[li];
-                m = C.segmask[li * nseg + sg];
-            }
-            const unsigned live = __ballot_sync(0xffffffffu, m != 0);
-            const int nl = __popc(live);
-            // the lanes of the live chunks not yet issued / not yet consumed
-            unsigned to_issue = live, to_cons = live;
-            auto issue = [&]() {  // the next live chunk into stage k_issue % S
-                const int chunk = __shfl_sync(0xffffffffu, cid, __ffs(to_issue) - 1);
-                to_issue &= to_issue - 1u;
-                if (lane == 0) {
-                    uint64_t* bar = &s_full[k_issue % S];
-                    unsigned char* dst = wbase + (k_issue % S) * kStage;
-                    fence_proxy_async_smem();
-                    mbar_arrive_expect_tx(bar, kStage);
-                    bulk_g2s(dst, A.geo + (size_t)chunk * CH * 2, kGeoBytes, bar);
-                    bulk_g2s(dst + kGeoBytes, A.qq + (size_t)chunk * CH,
-                             (uint32_t)(CH * sizeof(float2)), bar);
-                }
-                ++k_issue;
-            };
-            for (int j = 0; j < min(S, nl); ++j) issue();
-            for (int j = 0; j < nl; ++j) {
-                const unsigned gm = __shfl_sync(0xffffffffu, m, __ffs(to_cons) - 1);
-                to_cons &= to_cons - 1u;
-                if (!__all_sync(0xffffffffu,
-                                mbar_wait_bounded(&s_full[k_cons % S], (k_cons / S) & 1u, A.err))) {
-                    failed = true;
-                    break;
-                }
-                if (C.examined && lane == 0)
-                    atomicAdd(C.examined, (unsigned long long)__popc(gm) * kGroup * SEG);
-                chunk_pairs<KIND, PATH, RP, SUB, NORM, false, VOTE>(
-                    geo(k_cons), qq(k_cons), gm, tx, ty, tz, tt, acc64, nrm, ulim, A.tab_k, s_tab,
-                    s_tab64);
-                __syncwarp();  // every lane is done with the stage
-                ++k_cons;
-                if (j + S < nl) issue();
-            }
-        }
-        if (failed) break;
-        double* out = A.part + (size_t)item * C.tile_size + sg * SEG;
-#pragma unroll
-        for (int q = 0; q < 2 * RP; ++q) {
-            if (base + q * 32 + lane < t_phys) {
-                out[q * 32 + lane] = acc64[q];
-                if (NORM)
-                    A.part_norm[(size_t)item * C.tile_size + sg * SEG + q * 32 + lane] =
-                        nrm[NORM ? q : 0];
-            }
-        }
-    }
-    if (!failed) pdl_trigger();  // no item left for this warp
-    // after a timeout: let this warp's copies still in flight land first
-    if (failed && lane == 0) mbar_drain_ring(s_full, S, k_cons, k_issue);
-}
-
-template <int KIND, int PATH, int NW, int RP, int SUB, int S, int MINB, int VOTE = 1>
-__global__ void __launch_bounds__(NW * 32, MINB) pair_kernel_warp_items(PairArgs A, CullArgs C) {
-    pdl_wait();
-    pair_items_warp<KIND, PATH, NW, RP, SUB, false, S, VOTE>(A, C);
 }
 
 template <int KIND, int PATH, int NT, int RP, int SUB, bool NORM = false>

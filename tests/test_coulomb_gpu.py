@@ -450,13 +450,11 @@ def test_culled_sums_examine_fewer_pairs(lgm, oracle_mod):
 
 def test_warp_specialised_culled_sums_equal_the_culled_sums(lgm, oracle_mod):
     """A warp-specialised culled variant (producer warp, ring of stages, items
-    taken from a counter) and a warp-item variant (every warp takes its own
-    segment of an item, staging only the chunks that segment has a live group
-    in) add every target's terms in the order of a culled variant with the
-    same tile, FP32 run and chunks per item: the sums are equal bit for bit,
-    for every path and kind, with images at both electrodes (a group one warp
-    shape skips adds +0 in the other), and with the same warp shape so are the
-    pairs examined."""
+    taken from a counter) adds every target's terms in the order of a culled
+    variant with the same tile, FP32 run and chunks per item: the sums are
+    equal bit for bit, for every path and kind, with images at both
+    electrodes (a group one warp shape skips adds +0 in the other), and with
+    the same warp shape so are the pairs examined."""
     X, Y, Z, c = 128, 128, 16, 40
     rng = np.random.default_rng(12)
     orc = oracle_mod.Oracle(X, Y, Z, cutoff=c, sigma=1.0)
@@ -470,11 +468,9 @@ def test_warp_specialised_culled_sums_equal_the_culled_sums(lgm, oracle_mod):
             vs = ctx.variants()
             shape = lambda v: (vs[v]["threads"] * vs[v]["target_pairs"], vs[v]["run"],
                                vs[v]["chunks_per_item"])
-            for w in [i for i, v in enumerate(vs) if v["warp_specialised"] or v["warp_items"]]:
-                # a warp-item variant's twin may be warp-specialised
-                twins = [i for i, v in enumerate(vs) if v["culled"] and not v["warp_items"]
-                         and (vs[w]["warp_items"] or not v["warp_specialised"])
-                         and shape(i) == shape(w)][:2]
+            for w in [i for i, v in enumerate(vs) if v["warp_specialised"]]:
+                twins = [i for i, v in enumerate(vs) if v["culled"] and
+                         not v["warp_specialised"] and shape(i) == shape(w)]
                 for t in twins:
                     got = []
                     for v in (t, w):
