@@ -1019,14 +1019,22 @@ __device__ __forceinline__ void compact_inject_body(const Dev& D, int* warp_sums
 
 // Single-replica kernels: the Dev travels by value.
 #define LGM_THREAD_INDEX (int)(blockIdx.x * blockDim.x + threadIdx.x)
-__global__ void k_choose(Dev D) { choose_body(D, LGM_THREAD_INDEX); }
-__global__ void k_pack(Dev D) { pack_body(D, LGM_THREAD_INDEX); }
-__global__ void k_finalize(Dev D) { finalize_body(D, LGM_THREAD_INDEX); }
+__global__ void k_choose(Dev D) {
+    pdl_wait();
+    pdl_trigger(); choose_body(D, LGM_THREAD_INDEX); }
+__global__ void k_pack(Dev D) {
+    pdl_wait();
+    pdl_trigger(); pack_body(D, LGM_THREAD_INDEX); }
+__global__ void k_finalize(Dev D) {
+    pdl_wait();
+    pdl_trigger(); finalize_body(D, LGM_THREAD_INDEX); }
 // finalize_body's culled branch with a block of 32 x 3 threads per 32
 // targets: warp y sums term slot y's item partials (and norms) in item order,
 // eight items in flight, and warp 0 combines the slots -- the same sums in
 // the same order, three times the threads.
 __global__ void __launch_bounds__(96) k_finalize_culled(Dev D) {
+    pdl_wait();
+    pdl_trigger();
     constexpr int kRows = 8;
     __shared__ double s_v[3][32], s_n[3][32];
     const int t = 2 * (D.cnt[I_NE] + D.cnt[I_NH]);
@@ -1067,10 +1075,18 @@ __global__ void __launch_bounds__(96) k_finalize_culled(Dev D) {
         D.Nt[target] = D.prefactor * n;
     }
 }
-__global__ void k_decide(Dev D) { decide_body(D, LGM_THREAD_INDEX); }
-__global__ void k_tbins_zero(Dev D) { tbins_zero_body(D, LGM_THREAD_INDEX); }
-__global__ void k_tbins(Dev D) { tbins_body(D, LGM_THREAD_INDEX); }
+__global__ void k_decide(Dev D) {
+    pdl_wait();
+    pdl_trigger(); decide_body(D, LGM_THREAD_INDEX); }
+__global__ void k_tbins_zero(Dev D) {
+    pdl_wait();
+    pdl_trigger(); tbins_zero_body(D, LGM_THREAD_INDEX); }
+__global__ void k_tbins(Dev D) {
+    pdl_wait();
+    pdl_trigger(); tbins_body(D, LGM_THREAD_INDEX); }
 __global__ void __launch_bounds__(1024) k_tbins_scan(Dev D) {
+    pdl_wait();
+    pdl_trigger();
     if (blockIdx.x == 0) block_exclusive_scan(D.bins, D.ncells + 1);
     else block_exclusive_scan(D.sbins, 3 * (D.ncells + 1));
 }
@@ -1101,23 +1117,49 @@ __host__ __device__ __forceinline__ CullArgs cull_args(const Dev& D) {
     return C;
 }
 __global__ void __launch_bounds__(CH) k_chunk_boxes(Dev D) {
+    pdl_wait();
+    pdl_trigger();
     chunk_boxes_body(pair_args(D), cull_args(D), (int)blockIdx.x);
 }
-__global__ void __launch_bounds__(kCullThreads) k_cull(Dev D) { cull_body(cull_args(D), (int)blockIdx.x); }
-__global__ void k_tscatter(Dev D) { tscatter_body(D, LGM_THREAD_INDEX); }
-__global__ void k_trank(Dev D) { trank_body(D, LGM_THREAD_INDEX); }
+__global__ void __launch_bounds__(kCullThreads) k_cull(Dev D) {
+    pdl_wait();
+    pdl_trigger(); cull_body(cull_args(D), (int)blockIdx.x); }
+__global__ void k_tscatter(Dev D) {
+    pdl_wait();
+    pdl_trigger(); tscatter_body(D, LGM_THREAD_INDEX); }
+__global__ void k_trank(Dev D) {
+    pdl_wait();
+    pdl_trigger(); trank_body(D, LGM_THREAD_INDEX); }
 __global__ void __launch_bounds__(kGuardThreads) k_guard(Dev D) {
+    pdl_wait();
+    pdl_trigger();
     __shared__ double2 red[32];
     guard_body(D, blockIdx.x, gridDim.x, red);
 }
-__global__ void k_hmap(Dev D) { hmap_body(D, LGM_THREAD_INDEX, true); }
-__global__ void k_recomb_propose(Dev D) { recomb_propose_body(D, LGM_THREAD_INDEX); }
-__global__ void k_recomb_resolve(Dev D) { recomb_resolve_body(D, LGM_THREAD_INDEX); }
-__global__ void k_recomb_reset(Dev D) { recomb_reset_body(D, LGM_THREAD_INDEX); }
-__global__ void k_claim(Dev D) { claim_body(D, LGM_THREAD_INDEX); }
-__global__ void k_move(Dev D) { move_body(D, LGM_THREAD_INDEX); }
-__global__ void k_unclaim(Dev D) { unclaim_body(D, LGM_THREAD_INDEX); }
+__global__ void k_hmap(Dev D) {
+    pdl_wait();
+    pdl_trigger(); hmap_body(D, LGM_THREAD_INDEX, true); }
+__global__ void k_recomb_propose(Dev D) {
+    pdl_wait();
+    pdl_trigger(); recomb_propose_body(D, LGM_THREAD_INDEX); }
+__global__ void k_recomb_resolve(Dev D) {
+    pdl_wait();
+    pdl_trigger(); recomb_resolve_body(D, LGM_THREAD_INDEX); }
+__global__ void k_recomb_reset(Dev D) {
+    pdl_wait();
+    pdl_trigger(); recomb_reset_body(D, LGM_THREAD_INDEX); }
+__global__ void k_claim(Dev D) {
+    pdl_wait();
+    pdl_trigger(); claim_body(D, LGM_THREAD_INDEX); }
+__global__ void k_move(Dev D) {
+    pdl_wait();
+    pdl_trigger(); move_body(D, LGM_THREAD_INDEX); }
+__global__ void k_unclaim(Dev D) {
+    pdl_wait();
+    pdl_trigger(); unclaim_body(D, LGM_THREAD_INDEX); }
 __global__ void __launch_bounds__(kCompactThreads) k_compact_inject(Dev D) {
+    pdl_wait();
+    pdl_trigger();
     __shared__ int warp_sums[32];
     __shared__ double red[32];
     compact_inject_body(D, warp_sums, red);
@@ -1726,51 +1768,71 @@ KPairFn kmc_pair(int gauss, int sorted = 1) {
     return gauss ? &pair_kernel<1, 0, kNT, kRP, kSUB, true> : &pair_kernel<0, 0, kNT, kRP, kSUB, true>;
 }
 
+// Launches one kernel of the step with programmatic stream serialization:
+// it may be scheduled while the kernel ahead of it is running and waits for
+// it in pdl_wait() (every k_* kernel and the pair kernels call it first), so
+// the launch gaps inside the captured graph overlap the kernel ahead.
+template <typename... P, typename... Args>
+cudaError_t kl(void (*f)(P...), dim3 grid, dim3 block, size_t smem, cudaStream_t st,
+               Args... args) {
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, f, static_cast<P>(args)...);
+}
+
 // One step: kernels in order on k->stream (captured into the graph).
 lgm_status enqueue_step(lgm_kmc* k) {
     const Dev& D = k->D;
     cudaStream_t st = k->stream;
     const int nc = std::max(1, D.cap_e + D.cap_h);
     const int blk = 256;
-    k_choose<<<(nc + blk - 1) / blk, blk, 0, st>>>(D);
+    const int g1 = (nc + blk - 1) / blk;
+    KCUDA(k, kl(k_choose, g1, blk, 0, st, D));
     if (D.coulomb) {
         if (D.sorted) {
             const int nz = D.culled ? 3 * (D.ncells + 1) : D.ncells + 1;
             const int nb = std::max(2 * nc, nc + (D.dq != 0 ? D.nd : 0));
-            k_tbins_zero<<<(nz + blk - 1) / blk, blk, 0, st>>>(D);
-            k_tbins<<<(nb + blk - 1) / blk, blk, 0, st>>>(D);
-            k_tbins_scan<<<D.culled ? 2 : 1, 1024, 0, st>>>(D);
-            k_tscatter<<<(nb + blk - 1) / blk, blk, 0, st>>>(D);
-            if (D.culled) k_trank<<<(2 * nc + blk - 1) / blk, blk, 0, st>>>(D);
+            KCUDA(k, kl(k_tbins_zero, (nz + blk - 1) / blk, blk, 0, st, D));
+            KCUDA(k, kl(k_tbins, (nb + blk - 1) / blk, blk, 0, st, D));
+            KCUDA(k, kl(k_tbins_scan, D.culled ? 2 : 1, 1024, 0, st, D));
+            KCUDA(k, kl(k_tscatter, (nb + blk - 1) / blk, blk, 0, st, D));
+            if (D.culled) KCUDA(k, kl(k_trank, (2 * nc + blk - 1) / blk, blk, 0, st, D));
         }
         const int npack = std::max(D.src_cap, D.tpad_cap);
-        k_pack<<<(npack + blk - 1) / blk, blk, 0, st>>>(D);
+        KCUDA(k, kl(k_pack, (npack + blk - 1) / blk, blk, 0, st, D));
         const PairArgs A = pair_args(D);
         if (D.culled) {
-            k_chunk_boxes<<<D.src_cap / CH, CH, 0, st>>>(D);
-            k_cull<<<k->cull_tiles, kCullThreads, 0, st>>>(D);
-            kmc_pair_culled(D.gauss)<<<k->cull_grid, kCThreads, kmc_culled_smem(A.tab_k), st>>>(
-                A, cull_args(D));
+            KCUDA(k, kl(k_chunk_boxes, D.src_cap / CH, CH, 0, st, D));
+            KCUDA(k, kl(k_cull, k->cull_tiles, kCullThreads, 0, st, D));
+            KCUDA(k, kl(kmc_pair_culled(D.gauss), k->cull_grid, kCThreads,
+                        kmc_culled_smem(A.tab_k), st, A, cull_args(D)));
         } else {
-            kmc_pair(D.gauss, D.sorted)<<<dim3(k->pair_tiles, D.splits), kNT,
-                                          pair_smem_bytes(A.tab_k), st>>>(A);
+            KCUDA(k, kl(kmc_pair(D.gauss, D.sorted), dim3(k->pair_tiles, D.splits), kNT,
+                        pair_smem_bytes(A.tab_k), st, A));
         }
-        if (D.culled) k_finalize_culled<<<(2 * nc + 31) / 32, dim3(32, 3), 0, st>>>(D);
-        else k_finalize<<<(2 * nc + blk - 1) / blk, blk, 0, st>>>(D);
+        if (D.culled) KCUDA(k, kl(k_finalize_culled, (2 * nc + 31) / 32, dim3(32, 3), 0, st, D));
+        else KCUDA(k, kl(k_finalize, (2 * nc + blk - 1) / blk, blk, 0, st, D));
     }
-    k_decide<<<(nc + blk - 1) / blk, blk, 0, st>>>(D);
-    if (D.coulomb) k_guard<<<2 * k->sm_count, kGuardThreads, 0, st>>>(D);
+    KCUDA(k, kl(k_decide, g1, blk, 0, st, D));
+    if (D.coulomb) KCUDA(k, kl(k_guard, 2 * k->sm_count, kGuardThreads, 0, st, D));
     if (D.solar && D.rec_rate > 0) {
-        k_hmap<<<(nc + blk - 1) / blk, blk, 0, st>>>(D);
-        k_recomb_propose<<<(nc + blk - 1) / blk, blk, 0, st>>>(D);
-        k_recomb_resolve<<<(nc + blk - 1) / blk, blk, 0, st>>>(D);
-        k_recomb_reset<<<(nc + blk - 1) / blk, blk, 0, st>>>(D);
+        KCUDA(k, kl(k_hmap, g1, blk, 0, st, D));
+        KCUDA(k, kl(k_recomb_propose, g1, blk, 0, st, D));
+        KCUDA(k, kl(k_recomb_resolve, g1, blk, 0, st, D));
+        KCUDA(k, kl(k_recomb_reset, g1, blk, 0, st, D));
     }
-    k_claim<<<(nc + blk - 1) / blk, blk, 0, st>>>(D);
-    k_move<<<(nc + blk - 1) / blk, blk, 0, st>>>(D);
-    k_unclaim<<<(nc + blk - 1) / blk, blk, 0, st>>>(D);
-    k_compact_inject<<<1, kCompactThreads, 0, st>>>(D);
-    KCUDA(k, cudaGetLastError());
+    KCUDA(k, kl(k_claim, g1, blk, 0, st, D));
+    KCUDA(k, kl(k_move, g1, blk, 0, st, D));
+    KCUDA(k, kl(k_unclaim, g1, blk, 0, st, D));
+    KCUDA(k, kl(k_compact_inject, 1, kCompactThreads, 0, st, D));
     return LGM_OK;
 }
 
