@@ -110,7 +110,10 @@ int32_t lgm_abi_version(void);
  * lattice sites [0, volume); targets may also be the electrode ids
  * [volume, volume + 35) that the reference packs for drains
  * (openclhelper.cpp:411-424), whose values are defined but meaningless.
- * Host buffers, synchronous. */
+ * Host buffers, synchronous.  A site outside its range returns
+ * LGM_ERR_OUT_OF_RANGE naming the first bad one (sources before targets) and
+ * leaves out untouched; the check runs on the device with the sums, so the
+ * call still does its device work first. */
 lgm_status lgm_potentials(lgm_ctx* ctx, lgm_kind kind, uint32_t terms,
                           const int32_t* src_site, const int32_t* src_q, int32_t n,
                           const int32_t* tgt_site, int32_t t, double* out);

@@ -21,6 +21,16 @@ def _i32(a) -> np.ndarray:
     return np.ascontiguousarray(np.asarray(a, dtype=np.int32).ravel())
 
 
+def _out(out, n: int) -> np.ndarray:
+    """A caller's output array (float64, C-contiguous, n long), or a new one."""
+    if out is None:
+        return np.empty(n, dtype=np.float64)
+    if (not isinstance(out, np.ndarray) or out.dtype != np.float64 or out.shape != (n,)
+            or not out.flags.c_contiguous):
+        raise ValueError(f"out must be a C-contiguous float64 array of length {n}")
+    return out
+
+
 class Coulomb:
     """One B200 context: lattice, cutoff, prefactor, sigma, precision, path."""
 
@@ -66,18 +76,21 @@ class Coulomb:
         N.check(st, self._h)
 
     # -- host-buffer entry points ----------------------------------------------
-    def potentials(self, src_site, src_q, tgt_site, kind=N.POINT, terms=N.TERM_DIRECT):
+    def potentials(self, src_site, src_q, tgt_site, kind=N.POINT, terms=N.TERM_DIRECT, out=None):
+        """Potentials at the targets (lgm_potentials).  out: a float64 array
+        of len(tgt_site) to fill and return (a caller stepping a simulation
+        reuses one), else a new one."""
         s, q, t = _i32(src_site), _i32(src_q), _i32(tgt_site)
         if len(s) != len(q):
             raise ValueError("src_site and src_q differ in length")
-        out = np.empty(len(t), dtype=np.float64)
+        out = _out(out, len(t))
         self._check(N.lib().lgm_potentials(self._h, int(kind), int(terms), s, q, len(s), t,
                                            len(t), out))
         return out
 
-    def kernel2(self, s, q, n, kind=N.POINT):
+    def kernel2(self, s, q, n, kind=N.POINT, out=None):
         s, q = _i32(s), _i32(q)
-        out = np.empty(len(s), dtype=np.float64)
+        out = _out(out, len(s))
         self._check(N.lib().lgm_coulomb_kernel2(self._h, int(kind), s, q, int(n), len(s), out))
         return out
 

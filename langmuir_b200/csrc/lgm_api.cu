@@ -223,11 +223,13 @@ __device__ __forceinline__ void zero_bins(int32_t* __restrict__ bins, int nbins)
 __global__ void finalize(const double* __restrict__ part, int splits, int t_phys, int t,
                          int t_pad, int nterms, double prefactor,
                          const int32_t* __restrict__ perm, double* __restrict__ out,
-                         int32_t* __restrict__ bins, int nbins) {
+                         int32_t* __restrict__ bins, int nbins, const unsigned* err,
+                         unsigned* err_out) {
     pdl_wait();
     pdl_trigger();
     const int g = blockIdx.x * blockDim.x + threadIdx.x;
     zero_bins(bins, nbins);
+    if (err_out && g == 0) *err_out = *err;
     if (g >= t) return;
     double total = 0.0;
     for (int slot = 0; slot < nterms; ++slot) {
@@ -326,7 +328,8 @@ __global__ void __launch_bounds__(96) finalize_items(const double* __restrict__ 
                                                      double prefactor,
                                                      const int32_t* __restrict__ perm,
                                                      double* __restrict__ out,
-                                                     int32_t* __restrict__ bins, int nbins) {
+                                                     int32_t* __restrict__ bins, int nbins,
+                                                     const unsigned* err, unsigned* err_out) {
     constexpr int kRows = 16;  // loads in flight (a tile has at most 32 items)
     __shared__ double s_sum[3][32];
     pdl_wait();
@@ -334,6 +337,7 @@ __global__ void __launch_bounds__(96) finalize_items(const double* __restrict__ 
     const int g = blockIdx.x * 32 + (int)threadIdx.x, slot = (int)threadIdx.y;
     const int dst = slot == 0 && g < t ? perm[g] : 0;  // loaded ahead of the sums
     if (slot == 0) zero_bins(bins, nbins);
+    if (err_out && g == 0 && slot == 0) *err_out = *err;
     double sum = 0.0;
     if (g < t && slot < nterms) {
         const int p = slot * t_pad + g;
@@ -358,10 +362,11 @@ __global__ void __launch_bounds__(96) finalize_items(const double* __restrict__ 
     }
 }
 
-__global__ void fill_zero(double* out, int t) {
+__global__ void fill_zero(double* out, int t, const unsigned* err, unsigned* err_out) {
     pdl_wait();
     pdl_trigger();
     const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (err_out && g == 0) *err_out = *err;
     if (g < t) out[g] = 0.0;
 }
 
@@ -762,7 +767,8 @@ int choose_variant(const lgm_ctx* c, int kind, const Shape& sh) {
 // all lattice sites when all_sites).  Everything on `st`.
 lgm_status launch_potentials(lgm_ctx* c, int kind, unsigned terms, const int32_t* d_src,
                              const int32_t* d_q, int n, const int32_t* d_tgt_site, int t,
-                             int all_sites, double* d_out, cudaStream_t st) {
+                             int all_sites, double* d_out, cudaStream_t st,
+                             unsigned* err_out = nullptr) {
     const lgm_config& cf = c->cfg;
     c->last = lgm_launch_info{};
     c->last.pair_kernel_ms = -1.f;
@@ -772,7 +778,8 @@ lgm_status launch_potentials(lgm_ctx* c, int kind, unsigned terms, const int32_t
     c->count_pending = false;
     if (t == 0) return LGM_OK;
     if (n == 0) {
-        LGM_CUDA(c, launch_chain(c->overlap, fill_zero, (t + 255) / 256, 256, 0, st, d_out, t));
+        LGM_CUDA(c, launch_chain(c->overlap, fill_zero, (t + 255) / 256, 256, 0, st, d_out, t,
+                                 c->d_err, err_out));
         c->last.kernel_launches = 1;
         return LGM_OK;
     }
@@ -810,14 +817,15 @@ lgm_status launch_potentials(lgm_ctx* c, int kind, unsigned terms, const int32_t
     if (splits > 0) {
         LGM_CUDA(c, launch_chain(c->overlap, finalize, (t + 255) / 256, 256, 0, st, c->d_part,
                                  splits, sh.t_phys, t, sh.t_pad, sh.nterms,
-                                 cf.electrostatic_prefactor, c->d_perm, d_out, c->d_bins, nbins));
+                                 cf.electrostatic_prefactor, c->d_perm, d_out, c->d_bins, nbins,
+                                 c->d_err, err_out));
         c->last.kernel_launches = 5;  // bins (+ scan), scatter, records, pair, finalize
     } else {
         const Variant& V = kVariants[c->last.variant];
         LGM_CUDA(c, launch_chain(c->overlap, finalize_items, (t + 31) / 32, dim3(32, 3), 0, st,
                                  c->d_part, c->d_tile_first, c->d_tile_items, V.nt * 2 * V.rp, t,
                                  sh.t_pad, sh.nterms, cf.electrostatic_prefactor, c->d_perm, d_out,
-                                 c->d_bins, nbins));
+                                 c->d_bins, nbins, c->d_err, err_out));
         c->last.kernel_launches = 7;  // bins (+ scan), scatter, records, boxes, cull, pair, finalize
     }
     c->bins_clean = true;
@@ -826,10 +834,9 @@ lgm_status launch_potentials(lgm_ctx* c, int kind, unsigned terms, const int32_t
     return LGM_OK;
 }
 
-lgm_status check_device_error(lgm_ctx* c, cudaStream_t st) {
-    LGM_CUDA(c, cudaMemcpyAsync(c->h_err, c->d_err, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
-    LGM_CUDA(c, cudaStreamSynchronize(st));
-    const unsigned e = *c->h_err;
+// The status of device error word e (read back into c->h_err); a nonzero word
+// is cleared on the device for the next call.
+lgm_status device_error_status(lgm_ctx* c, cudaStream_t st, unsigned e) {
     if (e == 0) return LGM_OK;
     LGM_CUDA(c, cudaMemsetAsync(c->d_err, 0, sizeof(unsigned), st));
     LGM_CUDA(c, cudaStreamSynchronize(st));
@@ -839,6 +846,12 @@ lgm_status check_device_error(lgm_ctx* c, cudaStream_t st) {
     if (e & DEVERR_TARGET_RANGE)
         return fail(c, LGM_ERR_OUT_OF_RANGE, "a target site lies outside [0, volume + 35)");
     return fail(c, LGM_ERR_STATE, "device reported an inconsistent state");
+}
+
+lgm_status check_device_error(lgm_ctx* c, cudaStream_t st) {
+    LGM_CUDA(c, cudaMemcpyAsync(c->h_err, c->d_err, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+    LGM_CUDA(c, cudaStreamSynchronize(st));
+    return device_error_status(c, st, *c->h_err);
 }
 
 lgm_status check_common(lgm_ctx* c, int kind, unsigned terms, int n, int t) {
@@ -859,30 +872,6 @@ lgm_status check_common(lgm_ctx* c, int kind, unsigned terms, int n, int t) {
     return LGM_OK;
 }
 
-// Host-side range checks for the host-buffer entry points (the reference
-// would index garbage; here the call fails before any work).
-// Copies site ids into a pinned staging buffer and checks each one against
-// [0, lim) in the same pass; the first bad id gives the error that
-// check_sites would give.  `what` names the role in the message, and `base`
-// is the index of src[0] in the caller's array.
-lgm_status stage_sites(lgm_ctx* c, const int32_t* src, int n, int32_t lim, const char* what,
-                       int32_t* dst, int base = 0) {
-    bool bad = false;
-    for (int j = 0; j < n; ++j) {
-        const int32_t v = src[j];
-        bad |= (v < 0) | (v >= lim);
-        dst[j] = v;
-    }
-    if (!bad) return LGM_OK;
-    for (int j = 0; j < n; ++j)
-        if (src[j] < 0 || src[j] >= lim) {
-            char b[128];
-            std::snprintf(b, sizeof b, "%s %d: site %d outside [0, %d)", what, base + j, src[j],
-                          lim);
-            return fail(c, LGM_ERR_OUT_OF_RANGE, b);
-        }
-    return LGM_OK;
-}
 
 lgm_status check_sites(lgm_ctx* c, const int32_t* src, int n, const int32_t* tgt, int t) {
     for (int j = 0; j < n; ++j)
@@ -1330,39 +1319,44 @@ lgm_status lgm_potentials(lgm_ctx* c, lgm_kind kind, uint32_t terms, const int32
         return fail(c, LGM_ERR_INVALID_ARGUMENT, "null buffer");
     LGM_CUDA(c, cudaSetDevice(c->device));
     cudaStream_t st = c->stream;
-    const size_t nn = std::max(n, 1), tt = std::max(t, 1);
-    if ((s = grow_host(c, &c->h_s, &c->hs_cap, nn)) != LGM_OK) return s;
-    if ((s = grow_host(c, &c->h_q, &c->hq_cap, nn)) != LGM_OK) return s;
-    if ((s = grow_host(c, &c->h_t, &c->ht_cap, tt)) != LGM_OK) return s;
-    if ((s = grow_host(c, &c->h_o, &c->ho_cap, tt)) != LGM_OK) return s;
-    if ((s = grow_device(c, &c->d_s, &c->s_cap, nn)) != LGM_OK) return s;
-    if ((s = grow_device(c, &c->d_q, &c->q_cap, nn)) != LGM_OK) return s;
-    if ((s = grow_device(c, &c->d_t, &c->t_cap, tt)) != LGM_OK) return s;
-    if ((s = grow_device(c, &c->d_o, &c->o_cap, tt)) != LGM_OK) return s;
-    // Sites are checked while they are staged (sources first, then targets,
-    // as check_sites orders its errors).  When the sources are the first n
-    // targets (kernel 2: w aliases s, openclhelper.cpp:154) they are staged
-    // and copied once, as part of the targets.
+    if (t == 0) return check_sites(c, src_site, n, nullptr, 0);
+    // One pinned staging buffer and one device buffer, laid out [targets t]
+    // [charges n][sources n, unless they are the first n targets], cross in
+    // one copy; the results come back in one copy with the device error word
+    // behind them (written by the call's last kernel).
     const bool alias = tgt_site == src_site && n <= t;
-    if (alias) {
-        if ((s = stage_sites(c, src_site, n, c->volume, "source", c->h_t)) != LGM_OK) return s;
-    } else {
-        if ((s = stage_sites(c, src_site, n, c->volume, "source", c->h_s)) != LGM_OK) return s;
-        LGM_CUDA(c, cudaMemcpyAsync(c->d_s, c->h_s, sizeof(int32_t) * n, cudaMemcpyHostToDevice,
-                                    st));
+    const size_t words = (size_t)t + n + (alias ? 0 : n);
+    if ((s = grow_host(c, &c->h_t, &c->ht_cap, words)) != LGM_OK) return s;
+    if ((s = grow_host(c, &c->h_o, &c->ho_cap, (size_t)t + 1)) != LGM_OK) return s;
+    if ((s = grow_device(c, &c->d_t, &c->t_cap, words)) != LGM_OK) return s;
+    if ((s = grow_device(c, &c->d_o, &c->o_cap, (size_t)t + 1)) != LGM_OK) return s;
+    // The sites are checked on the device (prep_records), which gives each an
+    // empty record and raises an error bit; only then are they checked here,
+    // for the first bad one (sources first, then targets, as check_sites
+    // reports them).  When the sources are the first n targets (kernel 2: w
+    // aliases s, openclhelper.cpp:154) they cross once, as targets.
+    std::memcpy(c->h_t, tgt_site, sizeof(int32_t) * t);
+    if (n > 0) std::memcpy(c->h_t + t, src_q, sizeof(int32_t) * n);
+    if (!alias && n > 0) std::memcpy(c->h_t + t + n, src_site, sizeof(int32_t) * n);
+    LGM_CUDA(c, cudaMemcpyAsync(c->d_t, c->h_t, sizeof(int32_t) * words, cudaMemcpyHostToDevice,
+                                st));
+    const int32_t* d_src = alias ? c->d_t : c->d_t + t + n;
+    unsigned* d_err_out = reinterpret_cast<unsigned*>(c->d_o + t);
+    if ((s = launch_potentials(c, kind, terms, d_src, c->d_t + t, n, c->d_t, t, 0, c->d_o, st,
+                               d_err_out)) != LGM_OK)
+        return s;
+    LGM_CUDA(c, cudaMemcpyAsync(c->h_o, c->d_o, sizeof(double) * ((size_t)t + 1),
+                                cudaMemcpyDeviceToHost, st));
+    LGM_CUDA(c, cudaStreamSynchronize(st));
+    const unsigned e = *reinterpret_cast<const unsigned*>(c->h_o + t);
+    if (e != 0) {
+        const lgm_status ds = device_error_status(c, st, e);  // clears the device word
+        if (e & (DEVERR_SOURCE_RANGE | DEVERR_TARGET_RANGE)) {
+            const lgm_status hs = check_sites(c, src_site, n, tgt_site, t);
+            if (hs != LGM_OK) return hs;
+        }
+        return ds;
     }
-    std::memcpy(c->h_q, src_q, sizeof(int32_t) * n);
-    LGM_CUDA(c, cudaMemcpyAsync(c->d_q, c->h_q, sizeof(int32_t) * n, cudaMemcpyHostToDevice, st));
-    const int t0 = alias ? n : 0;  // aliased: the first n are staged and in range already
-    if ((s = stage_sites(c, tgt_site + t0, t - t0, c->volume + kDrainIds, "target", c->h_t + t0,
-                         t0)) != LGM_OK)
-        return s;
-    LGM_CUDA(c, cudaMemcpyAsync(c->d_t, c->h_t, sizeof(int32_t) * t, cudaMemcpyHostToDevice, st));
-    if ((s = launch_potentials(c, kind, terms, alias ? c->d_t : c->d_s, c->d_q, n, c->d_t, t, 0,
-                               c->d_o, st)) != LGM_OK)
-        return s;
-    LGM_CUDA(c, cudaMemcpyAsync(c->h_o, c->d_o, sizeof(double) * t, cudaMemcpyDeviceToHost, st));
-    if ((s = check_device_error(c, st)) != LGM_OK) return s;
     std::memcpy(out, c->h_o, sizeof(double) * t);
     return LGM_OK;
 }

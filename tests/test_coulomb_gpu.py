@@ -533,3 +533,21 @@ def test_bounded_wait_runs_out_and_the_context_stays_usable(lgm, oracle_mod):
     s, q, n = packed_case(orc, rng, 300, 280, 0, 0)
     with lgm.Coulomb(X, Y, Z, cutoff=c) as ctx:
         assert_close(ctx.kernel2(s, q, n), orc.kernel2(s, q, n), norm_of(orc, s, q, n), TOL32)
+
+
+def test_out_array_reused(lgm):
+    """A caller's result array is filled in place, call after call, with the
+    same values as a fresh one; a wrong one is refused before any work."""
+    rng = np.random.default_rng(5)
+    s = rng.choice(16 * 16 * 4, 60, replace=False).astype(np.int32)
+    q = np.where(np.arange(60) % 2 == 0, 1, -1).astype(np.int32)
+    out = np.full(60, np.nan)
+    with lgm.Coulomb(16, 16, 4, cutoff=10) as ctx:
+        want = ctx.potentials(s[:30], q[:30], s)
+        for _ in range(2):
+            got = ctx.potentials(s[:30], q[:30], s, out=out)
+            assert got is out
+            np.testing.assert_array_equal(out, want)
+        np.testing.assert_array_equal(ctx.kernel2(s, q, 30, out=out), ctx.kernel2(s, q, 30))
+        with pytest.raises(ValueError):
+            ctx.potentials(s[:30], q[:30], s, out=np.empty(59))
