@@ -46,7 +46,7 @@ FLOP_PER_TEST = 8
 FLOP_PER_CONTRIB = 3
 # DRAM bytes per launch of the pair kernel from one ncu capture of this
 # workload: dram__bytes_read.sum + dram__bytes_write.sum.
-PAIR_KERNEL_DRAM_BYTES = 2878976
+PAIR_KERNEL_DRAM_BYTES = 2034176
 
 
 def make_inputs(w, seed):
