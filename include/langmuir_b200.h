@@ -44,8 +44,8 @@ typedef int32_t lgm_status;
  * Gaussian-smeared charges (gauss1/gauss2, kernel.cl:139,296). */
 typedef enum lgm_kind { LGM_POINT = 0, LGM_GAUSS = 1 } lgm_kind;
 
-/* Pair-sum arithmetic.  FP32C: FP32 terms, FP32 runs of 8 positive terms
- * folded into FP64 accumulators.  FP64: every term in FP64 (the guard-band and
+/* Pair-sum arithmetic.  FP32C: FP32 terms, FP32 runs of up to 32 terms (16,
+ * one source group, in the default variants) folded into FP64 accumulators.  FP64: every term in FP64 (the guard-band and
  * reference-precision path). */
 typedef enum lgm_precision { LGM_PREC_FP32C = 0, LGM_PREC_FP64 = 1 } lgm_precision;
 
@@ -262,7 +262,7 @@ lgm_status lgm_variant_info(int32_t variant, int32_t* threads, int32_t* target_p
  * every pair and the sums are unchanged. */
 #define LGM_VARIANT_WARP_SKIP 1
 /* LGM_VARIANT_CULLED: the sources are sorted by lattice cell as well; each
- * source chunk (128 sources) and each group of 32 gets a bounding box, a cull
+ * source chunk (128 sources) and each group of 16 gets a bounding box, a cull
  * pass lists per tile of targets the chunks whose box comes within the cutoff,
  * and a persistent kernel sums over those work items only, a warp skipping any
  * group whose box lies beyond the cutoff of its own targets.  Skipped pairs

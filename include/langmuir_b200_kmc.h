@@ -258,7 +258,7 @@ lgm_status lgm_kmc_batch_tuning(const lgm_kmc_batch* b, int32_t* threads, int32_
 lgm_status lgm_kmc_batch_time_pair(lgm_kmc_batch* b, int32_t reps, float* ms);
 /* Runs the batched pair sum once more (as lgm_kmc_batch_time_pair) and counts
  * the source-target pairs it examined: for culled replicas, the pairs of the
- * 32-source groups whose boxes lie within the cutoff of a warp's targets; for
+ * 16-source groups whose boxes lie within the cutoff of a warp's targets; for
  * the others, every target against every packed source.  Measurement aid. */
 lgm_status lgm_kmc_batch_count_pairs(lgm_kmc_batch* b, uint64_t* pairs);
 /* How many replicas of the batch take the culled pair sum. */

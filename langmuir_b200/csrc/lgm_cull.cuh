@@ -7,14 +7,14 @@
 // visited at all:
 //
 //   chunk_boxes  the bounding box of every source chunk (CH = 128 sources)
-//                and of each of its four groups of 32;
+//                and of each of its eight groups of 16;
 //   cull         per target tile (the targets of one CTA), the ordered list
 //                of source chunks whose box comes within the cutoff of the
 //                tile's box, cut into work items of at most `per_item` chunks;
 //   pair         a persistent kernel: CTA b takes items b, b + G, b + 2G, ...
 //                and streams their chunks through shared memory (bulk TMA, two
 //                stages, the next item's chunks prefetched across the item
-//                boundary).  Each warp skips a 32-source group whose box lies
+//                boundary).  Each warp skips a 16-source group whose box lies
 //                beyond the cutoff of its own targets' box, and inside a live
 //                group the warp still votes per source (the SKIP tile of
 //                lgm_pairs.cuh);
