@@ -571,7 +571,11 @@ constexpr int kGuardThreads = 1024;
 constexpr int kGuardSplits = 16;
 // Blocks per replica of the batched guard: flagged decisions of one replica
 // are spread over them (a replica with M charges flags ~1e-3 M per step).
-constexpr int kGuardBlocksPerReplica = 12;
+constexpr int kGuardBlocksPerReplica = 48;
+// The batch's guard blocks: most replicas flag no decision in a step, and a
+// block with nothing to do costs its launch and retirement, so they are
+// small; a replica gets one block per 512 charges of capacity.
+constexpr int kGuardThreadsBatch = 256;
 // Indices per thread of the batched element-wise kernels (see LGM_BATCH_LOOP).
 constexpr int kItemsPerThread = 4;
 
@@ -1247,7 +1251,7 @@ __global__ void __launch_bounds__(1024) kb_item_order(ProblemList L, const Dev* 
         order[atomicAdd(&s_off[c], 1)] = g;
     }
 }
-__global__ void __launch_bounds__(kGuardThreads) kb_guard(const Dev* R, const int4* map) {
+__global__ void __launch_bounds__(kGuardThreadsBatch) kb_guard(const Dev* R, const int4* map) {
     __shared__ double2 red[32];
     const int4 m = map[blockIdx.x];
     guard_body(R[m.x], m.y, m.z, red);
@@ -2540,7 +2544,7 @@ lgm_status enqueue_batch_step(lgm_kmc_batch* b) {
         kb_finalize<<<b->nb_fin, 256, 0, st>>>(b->d_reps, b->map_fin);
     }
     kb_decide<<<b->nb_car, 256, 0, st>>>(b->d_reps, b->map_car);
-    if (b->coulomb) kb_guard<<<b->nb_guard, kGuardThreads, 0, st>>>(b->d_reps, b->map_guard);
+    if (b->coulomb) kb_guard<<<b->nb_guard, kGuardThreadsBatch, 0, st>>>(b->d_reps, b->map_guard);
     if (b->recomb) {
         kb_hmap<<<b->nb_car, 256, 0, st>>>(b->d_reps, b->map_car);
         kb_recomb_propose<<<b->nb_car, 256, 0, st>>>(b->d_reps, b->map_car);
@@ -2670,8 +2674,8 @@ lgm_status partition_batch(lgm_kmc_batch* b) {
         // a culled replica's source sort also walks the defects
         add(fin, r, D.culled ? std::max(2 * ncap, ncap + (D.dq != 0 ? D.nd : 0)) : 2 * ncap);
         add(bins, r, D.culled ? 3 * (D.ncells + 1) : D.ncells + 1);
-        // flagged decisions grow with the charge count: one block per 2048 of capacity
-        const int ng = std::min(kGuardBlocksPerReplica, std::max(1, (ncap + 2047) / 2048));
+        // flagged decisions grow with the charge count: one block per 512 of capacity
+        const int ng = std::min(kGuardBlocksPerReplica, std::max(1, (ncap + 511) / 512));
         for (int i = 0; i < ng; ++i) guard.push_back(make_int4(r, i, ng, 0));
         max_cap = std::max(max_cap, std::max(D.cap_e, D.cap_h));
     }
