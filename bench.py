@@ -932,10 +932,11 @@ def main():
         for _ in range(k_e2e):
             ctx.potentials(h_s[:n], h_q[:n], h_s, kind, w["terms"], out=h_o)
         dt = (time.perf_counter() - t0) / k_e2e
-        # host->device per call: the T int32 site ids (the sources are their
-        # first n, copied once) and the n int32 charges; device->host: T doubles
+        # host->device per call, one copy: the T int32 site ids (the sources are
+        # their first n) and the n int32 charges; device->host, one copy: T
+        # doubles and the device error word behind them (one more double)
         e2e = {"value": pairs_per_step / dt, "unit": "pair-evals/s",
-               "h2d_bytes_per_step": int(4 * (n + T)), "d2h_bytes_per_step": int(8 * T)}
+               "h2d_bytes_per_step": int(4 * (n + T)), "d2h_bytes_per_step": int(8 * (T + 1))}
 
     # the fused kMC step on the same lattice and occupancy: hops per second
     kmc = None

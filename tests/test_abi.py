@@ -148,3 +148,16 @@ def test_variant_table():
         flags.append(f.value)
     assert 0 in flags and 1 in flags  # plain and warp-skip tiles both present
     assert N.lib().lgm_variant_flags(n, C.byref(f)) == N.ERR_INVALID_ARGUMENT
+
+
+def test_out_array_checks():
+    """The Python wrapper's result arrays: a caller's float64 array of the
+    right length is used as it is; anything else is refused before any call."""
+    import numpy as np
+    from langmuir_b200.coulomb import _out
+    a = np.zeros(5)
+    assert _out(a, 5) is a
+    assert _out(None, 3).shape == (3,)
+    for bad in (np.zeros(4), np.zeros(5, np.float32), np.zeros(10)[::2], [0.0] * 5):
+        with pytest.raises(ValueError):
+            _out(bad, 5)
